@@ -1,0 +1,235 @@
+/*
+ * sieb200.h — C ABI of the B200-native dense method-of-moments library.
+ *
+ * Each entry point replaces one piece of the SIE-GSTC solver's public C++
+ * surface (paths relative to that project). All arguments are plain pointers
+ * and sizes; complex numbers are interleaved (re, im) doubles or floats;
+ * dense matrices are column-major. Functions never throw, abort or trap:
+ * they return a status code and leave a message for sieb200_last_error().
+ *
+ * Pointers documented as "host" may be any host memory; pointers documented
+ * as "device" must be CUDA device (or managed) memory on the context's GPU.
+ */
+#ifndef SIEB200_H
+#define SIEB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status ---- */
+/* Replaces the C++ exceptions of src/sie_mom/solvers/gstc_sie.cu:71-179
+ * (std::invalid_argument), include/sie_mom/cuda/dense_lu_solver.cuh:97-111
+ * (singular LU, std::runtime_error) and gstc_sie.cu:474-503 (non-finite). */
+enum {
+    SIEB200_OK = 0,
+    SIEB200_INVALID_ARG = 1,
+    SIEB200_OVERFLOW = 2,
+    SIEB200_SINGULAR = 3,
+    SIEB200_NONFINITE = 4,
+    SIEB200_NOT_CONVERGED = 5,
+    SIEB200_CUDA_ERROR = 6,
+    SIEB200_TIMEOUT = 7,
+    SIEB200_NO_DEVICE = 8,
+    SIEB200_OUT_OF_MEMORY = 9
+};
+
+/* Thread-local message of the last failing call on this host thread. */
+const char* sieb200_last_error(void);
+int sieb200_version(void);
+
+/* ----------------------------------------------------------- context ---- */
+/* Owns one CUDA stream, device workspaces, LU factors and library handles.
+ * One context per host thread; contexts on the same device are independent.
+ * Replaces the per-call RAII buffers of include/sie_mom/cuda/device_buffer.cuh:46-172. */
+typedef struct sieb200_ctx sieb200_ctx;
+int sieb200_ctx_create(int device, sieb200_ctx** out);
+int sieb200_ctx_destroy(sieb200_ctx* ctx);
+int sieb200_ctx_synchronize(sieb200_ctx* ctx);
+/* cudaStream_t of the context (as void*), for callers that order their own
+ * work against it. */
+void* sieb200_ctx_stream(sieb200_ctx* ctx);
+
+/* -------------------------------------------------------------- mesh ---- */
+/* Unique edges in first-appearance order over (face, local edge
+ * (le, le+1 mod 3)), key (min, max); faces_edges[3f+le] = edge index.
+ * Replaces ObjMeshLoader::buildEdgesAndMapping (src/sie_mom/mesh/obj_mesh_loader.cpp:360-386)
+ * and SphericalSurface::buildEdgesAndMapping (src/sie_mom/mesh/spherical_surface.cpp:100-136).
+ * edges_out: host, 2*3*num_faces ints capacity; faces_edges_out: host, 3*num_faces. */
+int sieb200_build_edges(const int32_t* faces, int64_t num_faces, int32_t* edges_out,
+                        int32_t* faces_edges_out, int64_t* num_edges_out);
+
+/* Dunavant rule `rule` (1..20) as the kernels use it: points (xi, eta) and
+ * weights rounded to float, in the expansion order of
+ * src/sie_mom/quadrature/triangle_dunavant_rule.cpp:135-256, as
+ * make_quadrature (include/sie_mom/quadrature/triangle_dunavant_rule.hpp:82-101)
+ * returns them. Returns the point count (pts: 2*count floats, w: count), or
+ * -1 for an invalid rule; NULL outputs only query the count. */
+int sieb200_quadrature_rule(int rule, float* pts, float* w);
+
+/* MeshData (include/sie_mom/mesh/spherical_surface.hpp:10-15); host pointers,
+ * vertices as nV x 3 doubles, faces and faces_edges as nF x 3 ints. */
+typedef struct {
+    const double* vertices;
+    int64_t num_vertices;
+    const int32_t* faces;
+    int64_t num_faces;
+    const int32_t* faces_edges;
+    int64_t num_edges;
+} sieb200_mesh;
+
+/* --------------------------------------------------------- options ---- */
+enum { SIEB200_PEC_EFIE = 0, SIEB200_PMCHWT = 1, SIEB200_GSTC = 2 };
+enum {
+    SIEB200_SOLVER_LU_FP64 = 0,     /* own FP64 blocked LU (drop-in for the cuSOLVER path) */
+    SIEB200_SOLVER_LU_CUSOLVER = 1, /* cusolverDnZgetrf/Zgetrs, as dense_lu_solver.cuh */
+    SIEB200_SOLVER_MIXED_IR = 2,    /* split-FP32 tensor-core LU + FP64 GMRES refinement */
+    SIEB200_SOLVER_GMRES_C64 = 3    /* GMRES on a complex64 copy of Z, FP64 residual */
+};
+enum { SIEB200_BASIS_FACE = 0, SIEB200_BASIS_SPHERICAL = 1 };
+
+/* Mirrors GstcSieOptions (include/sie_mom/solvers/gstc_sie.hpp:32-57),
+ * DielectricOptions (include/sie_mom/solvers/dielectric/dielectric_solver.hpp:30-44)
+ * and PecOptions (include/sie_mom/solvers/pec_solver.hpp:16-29).
+ * Fill with sieb200_options_default(formulation, &opt) first: it sets the
+ * reference's per-solver defaults (rule 7 / 17 / 17, threshold 0.1 lambda0,
+ * vacuum constants of pec_solver.hpp:26-27 or gstc_sie.hpp:55-56). */
+typedef struct {
+    int formulation;
+    double frequency_hz;
+    double eps_r_interior, mu_r_interior;
+    double eps_r_exterior, mu_r_exterior;
+    int quadrature_rule;
+    double singularity_threshold_lambda0;
+    double vacuum_permittivity, vacuum_permeability;
+    int basis;               /* GSTC frame */
+    int tensors_are_uniform; /* GSTC: 32 complex values instead of 32 per face */
+    int compute_residual;
+    int solver;              /* SIEB200_SOLVER_* */
+    double tolerance;        /* refinement / GMRES target on the scaled system */
+    int max_iterations;
+    int restart;
+} sieb200_options;
+int sieb200_options_default(int formulation, sieb200_options* out);
+
+/* Excitation (include/sie_mom/excitation/excitation.hpp:19-30): kind 0 is a
+ * plane wave (a = real E0, b = propagation direction), kind 1 a dipole
+ * (a = effective moment, b = position, is_magnetic). region 1 interior,
+ * 2 exterior. The wavenumber and impedance are bound from the region's
+ * medium as prepare_source does (src/sie_mom/excitation/excitation.cu:110-137). */
+typedef struct {
+    int kind;
+    int region;
+    double a[3];
+    double b[3];
+    int is_magnetic;
+} sieb200_source;
+
+/* Metrics (gstc_sie.hpp:108-202, dielectric_solver.hpp:49-67, pec_solver.hpp:31-44)
+ * plus the refinement counters of the mixed solver. Residuals refer to the
+ * internally scaled system, as in the reference. */
+typedef struct {
+    int64_t matrix_dimension;
+    int64_t dense_matrix_bytes;
+    double assembly_seconds;
+    double factorization_seconds;
+    double solve_seconds;
+    double residual_seconds;
+    int residual_computed;
+    double rhs_norm;
+    double absolute_residual;
+    double relative_residual;
+    double maximum_coefficient[4]; /* per current block [J1, M1, J2, M2] / [J, M] / [J] */
+    int refinement_iterations;
+    int solver;
+} sieb200_metrics;
+
+/* ------------------------------------------------------------ solvers --- */
+/* PEC T-EFIE: solve_pec_dense (include/sie_mom/solvers/pec_solver.hpp:57-61).
+ * current_out: host, num_edges complex (exterior J2). */
+int sieb200_solve_pec_dense(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                            const sieb200_source* source, double* current_out,
+                            sieb200_metrics* metrics);
+
+/* T-PMCHWT: solve_dielectric_dense (include/sie_mom/solvers/dielectric/dielectric_solver.hpp:92-96).
+ * currents_out: host, 2*num_edges complex [J, M], physical (M x eta0). */
+int sieb200_solve_dielectric_dense(sieb200_ctx* ctx, const sieb200_mesh* mesh,
+                                   const sieb200_options* opt, const sieb200_source* source,
+                                   double* currents_out, sieb200_metrics* metrics);
+
+/* SIE-GSTC batch: solve_gstc_dense_batch (include/sie_mom/solvers/gstc_sie.hpp:226-239)
+ * and, with num_cases = 1, solve_gstc_dense (gstc_sie.hpp:214-219).
+ * tensors: host, 32 complex per face (Lambda row-major then its inverse) or
+ * 32 if tensors_are_uniform. Each case has up to one interior and one
+ * exterior source: sources[2*c] (interior, kind < 0 = absent) and
+ * sources[2*c+1] (exterior). currents_out: host, num_cases x 4*num_edges
+ * complex [J1, M1, J2, M2], physical. metrics: num_cases entries. */
+int sieb200_solve_gstc_dense_batch(sieb200_ctx* ctx, const sieb200_mesh* mesh,
+                                   const double* tensors, const sieb200_options* opt,
+                                   const sieb200_source* sources, int num_cases,
+                                   double* currents_out, sieb200_metrics* metrics);
+
+/* ------------------------------------------------- assembly building blocks */
+/* Dense system matrix exactly as the reference kernels place it
+ * (PEC: sie_kernels_assembly.cuh:610-705; PMCHWT: dielectric_kernels.cu:23-149;
+ * GSTC: sie_kernels_assembly.cuh:156-272 + 460-594), eta0-scaled.
+ * Z: complex128, N x N column-major with leading dimension N; device memory
+ * when z_on_device != 0, else host. tensors: GSTC only (host). */
+int sieb200_assemble_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                            const double* tensors, double* Z, int z_on_device);
+
+/* Right-hand sides of num_sources sources as num_sources columns of length N
+ * (sie_kernels_utils.cuh:184-232, dielectric_solver.cu:399-530, pec_solver.cu:242-264).
+ * For GSTC, each column receives one source in its region's rows. */
+int sieb200_assemble_rhs(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                         const sieb200_source* sources, int num_sources, double* B,
+                         int b_on_device);
+
+/* ---------------------------------------------------------- dense LA ---- */
+/* DenseLuSolver (include/sie_mom/cuda/dense_lu_solver.cuh:17-184) as an
+ * object: factorize a device complex128 matrix with the selected method, then
+ * solve any number of right-hand sides. For SIEB200_SOLVER_MIXED_IR the
+ * solver keeps its own split-FP32 factors plus a pointer to the FP64 matrix
+ * (which must stay alive and unchanged) for the refinement residual. */
+typedef struct sieb200_dense_solver sieb200_dense_solver;
+int sieb200_dense_solver_create(sieb200_ctx* ctx, int64_t n, int method,
+                                sieb200_dense_solver** out);
+int sieb200_dense_solver_destroy(sieb200_dense_solver* s);
+/* A: device, n x n complex128, leading dimension lda. The FP64 methods factor
+ * in place (as cusolverDnZgetrf does); the mixed method leaves A intact. */
+int sieb200_dense_solver_factorize(sieb200_dense_solver* s, double* A, int64_t lda);
+/* B: device, n x nrhs complex128 (ldb), overwritten with the solution.
+ * tolerance/max_iterations apply to the mixed method (relative residual of
+ * each column); iterations_out (optional) receives the refinement count. */
+int sieb200_dense_solver_solve(sieb200_dense_solver* s, int64_t nrhs, double* B, int64_t ldb,
+                               double tolerance, int max_iterations, int* iterations_out);
+/* Conjugate-transpose solve A^H X = B with the same factors (adjoint). */
+int sieb200_dense_solver_solve_adjoint(sieb200_dense_solver* s, int64_t nrhs, double* B,
+                                       int64_t ldb, double tolerance, int max_iterations,
+                                       int* iterations_out);
+
+/* Complex matvec y = A x (+ beta y) on device data: A complex128 (prec 0) or
+ * complex64 (prec 1), n x n, lda; x, y complex128. Replaces the cublasZgemv
+ * residual of src/sie_mom/solvers/gstc_sie.cu:398-457. */
+int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
+                   const double* x, double beta, double* y);
+
+/* --------------------------------------------------------- far field ---- */
+/* Schelkunoff radiation vectors of the exterior RWG currents at the 7-point
+ * rule, as MetasurfaceFarFieldEvaluator does
+ * (applications/anisotropic_gstc_sphere/plot_far_field.py:118-220).
+ * j_cur, m_cur: host, num_edges complex each (m_cur may be NULL).
+ * Directions: host, ndir x 3 unit vectors each. Outputs: host, ndir complex
+ * F_theta and F_phi, ndir real radiation intensities U. */
+int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,
+                      const double* m_cur, double k0, double eta0, int64_t ndir,
+                      const double* r_hat, const double* theta_hat, const double* phi_hat,
+                      double* f_theta, double* f_phi, double* intensity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIEB200_H */

@@ -1,0 +1,143 @@
+"""Test infrastructure only: ctypes access to the CPU oracle (sieoracle.c) and,
+when it has been built, to the reference harness (_ref/libsieref.so).
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg import this.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libsieoracle.so"
+REF_SO = HERE / "_ref" / "libsieref.so"
+
+_P = ctypes.c_void_p
+_f = ctypes.c_float
+_d = ctypes.c_double
+_i = ctypes.c_int
+
+_ASSEMBLE = [_i, _P, _P, _P, _i, _i, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, _P, _i, _i, _P, _i]
+
+
+def _build_oracle() -> None:
+    src = HERE / "sieoracle.c"
+    if ORACLE_SO.exists() and ORACLE_SO.stat().st_mtime >= src.stat().st_mtime:
+        return
+    subprocess.run(["make", "-s", "-C", str(HERE), str(ORACLE_SO)], check=True,
+                   capture_output=True)
+
+
+def oracle() -> ctypes.CDLL:
+    _build_oracle()
+    lib = ctypes.CDLL(str(ORACLE_SO))
+    lib.so_rule.argtypes = [_i, _P, _P]
+    lib.so_build_edges.argtypes = [_P, _i, _P, _P]
+    lib.so_wilton.argtypes = [_P, _P, _P]
+    lib.so_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.so_assemble.argtypes = _ASSEMBLE
+    lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P]
+    lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
+    return lib
+
+
+def reference() -> ctypes.CDLL | None:
+    if not REF_SO.exists():
+        return None
+    lib = ctypes.CDLL(str(REF_SO))
+    lib.ref_dunavant.argtypes = [_i, _P, _P]
+    lib.ref_icosphere.argtypes = [_f, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
+                                  _P, _P, _P, _P]
+    lib.ref_wilton.argtypes = [_P, _P, _P]
+    lib.ref_phi0.argtypes = [_P, _P]
+    lib.ref_phi0.restype = _d
+    lib.ref_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.ref_assemble.argtypes = _ASSEMBLE
+    lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P]
+    lib.ref_lu_solve.argtypes = [_i, _P, _P, _P, _i, _i]
+    lib.ref_lu_solve.restype = _d
+    lib.ref_max_threads.restype = _i
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def dimension(kind: int, ne: int) -> int:
+    return ne * (1, 2, 4)[kind]
+
+
+def kernel_scalars(kind: int, frequency_hz: float, eps_r=(1.0, 1.0), mu_r=(1.0, 1.0),
+                   threshold_lambda0: float = 0.1, eps0: float | None = None,
+                   mu0: float | None = None) -> dict:
+    """The float kernel arguments the reference solvers pass
+    (pec_solver.cu:338-359, dielectric_solver.cu:312-321, gstc_sie.cu:281-290):
+    eps_r/mu_r = (interior, exterior)."""
+    if eps0 is None:
+        eps0 = 8.8541878188e-12 if kind == 2 else 8.8541878128e-12
+    if mu0 is None:
+        mu0 = 1.25663706127e-6 if kind == 2 else 1.25663706212e-6
+    omega = 2.0 * np.pi * frequency_hz
+    k1 = omega * np.sqrt(mu_r[0] * mu0 * eps_r[0] * eps0)
+    k2 = omega * np.sqrt(mu_r[1] * mu0 * eps_r[1] * eps0)
+    if kind == 2:
+        thr = threshold_lambda0 * (1.0 / np.sqrt(mu0 * eps0)) / frequency_hz
+    else:
+        thr = threshold_lambda0 * 2.0 * np.pi / (omega * np.sqrt(mu0 * eps0))
+    if kind == 0:
+        k1 = k2
+    return dict(k1=k1, k2=k2, mu_r1=mu_r[0], mu_r2=mu_r[1], eps_r1=eps_r[0], eps_r2=eps_r[1],
+                mu0=mu0, eps0=eps0, omega=omega, thr=thr)
+
+
+def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, uniform=False,
+             basis=0, threads=0, fn="so_assemble") -> np.ndarray:
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
+    ne = int(mesh.edges.shape[0])
+    N = dimension(kind, ne)
+    Z = np.zeros((N, N), dtype=np.complex128, order="F")
+    t = None if tensors is None else np.ascontiguousarray(tensors, dtype=np.complex128)
+    s = scalars
+    getattr(lib, fn)(kind, _p(V), _p(F), _p(FE), F.shape[0], ne, rule, s["k1"], s["k2"], s["mu_r1"],
+                     s["mu_r2"], s["eps_r1"], s["eps_r2"], s["mu0"], s["eps0"], s["omega"], s["thr"],
+                     _p(t), int(uniform), int(basis), _p(Z), int(threads))
+    return Z
+
+
+def rhs(lib, kind: int, mesh, rule: int, source: dict, k: float, eta: float, mu0: float,
+        eps0: float) -> np.ndarray:
+    """source: {'kind': 0|1, 'a': (3,), 'b': (3,), 'is_magnetic': bool, 'region': 1|2}."""
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
+    ne = int(mesh.edges.shape[0])
+    b = np.zeros(dimension(kind, ne), dtype=np.complex128)
+    a = np.ascontiguousarray(source["a"], dtype=np.float64)
+    bb = np.ascontiguousarray(source["b"], dtype=np.float64)
+    lib.so_rhs(kind, source["kind"], _p(V), _p(F), _p(FE), F.shape[0], ne, rule, _p(a), _p(bb),
+               int(source.get("is_magnetic", 0)), k, eta, source["region"], mu0, eps0, _p(b))
+    return b
+
+
+def far_field(lib, mesh, j, m, k0, eta0, r_hat, theta_hat, phi_hat):
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    j = np.ascontiguousarray(j, dtype=np.complex128)
+    m = None if m is None else np.ascontiguousarray(m, dtype=np.complex128)
+    rh, th, ph = (np.ascontiguousarray(x, dtype=np.float64) for x in (r_hat, theta_hat, phi_hat))
+    nd = rh.shape[0]
+    ft = np.zeros(nd, np.complex128)
+    fp = np.zeros(nd, np.complex128)
+    U = np.zeros(nd)
+    rc = lib.so_far_field(_p(V), _p(F), F.shape[0], int(mesh.edges.shape[0]), _p(j), _p(m), k0, eta0,
+                          nd, _p(rh), _p(th), _p(ph), _p(ft), _p(fp), _p(U))
+    if rc != 0:
+        raise ValueError("oracle far field: edge numbering mismatch")
+    return ft, fp, U

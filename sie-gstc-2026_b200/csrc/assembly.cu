@@ -1,0 +1,832 @@
+// Dense RWG-Galerkin impedance-matrix assembly (PEC T-EFIE, T-PMCHWT, SIE-GSTC).
+//
+// Reference behaviour (paths relative to the SIE-GSTC project):
+//   per face pair TL/TK      include/sie_mom/cuda/dunavant_quadrature.cuh:207-324
+//   singular extraction      dunavant_quadrature.cuh:769-875,
+//                            include/sie_mom/cuda/semi_analytic_integrals.cuh:35-92, 563-667
+//   Green kernels            include/sie_mom/cuda/green_functions_utils.cuh:236-361
+//   block placement          include/sie_mom/cuda/sie_kernels_assembly.cuh:156-272, 610-705,
+//                            src/sie_mom/solvers/dielectric/dielectric_kernels.cu:23-149
+//   GSTC jump-condition mass sie_kernels_assembly.cuh:460-594,
+//                            include/sie_mom/cuda/gstc_tensor_utils.cuh:72-309,
+//                            dunavant_quadrature.cuh:1422-1508
+//
+// B200 design. The reference runs one thread per face pair with 72 global
+// complex atomics per pair. Here:
+//   1. face_prep      one thread per face builds a geometry record and the
+//                     face's quadrature points (double) once.
+//   2. pair_regular   one CTA per test face; its 8 warps stream the source
+//                     faces, one warp per face pair, lanes over the Q*Q point
+//                     pairs. Instead of 9 RWG products per point pair, every
+//                     lane accumulates 8 (TL) + 10 (TK) complex moments of the
+//                     kernel in triangle-local coordinates; a warp butterfly
+//                     reduces them and 9 lanes expand them into the 3x3 blocks:
+//                       rho_m . rho_n  = (p-A_j).(q-B_i)
+//                       (rho_m x rho_n) . R = (rho_m x rho_n) . (v_j - v_i),
+//                     so the inner loop is bound by the Green-kernel
+//                     evaluation (sqrt, division, sincos) on the FP64 pipe.
+//   3. pair_singular  one warp per near pair (centroid distance below the
+//                     threshold, decided in float as the reference does) adds
+//                     the analytic (Wilton) part, lanes over outer points.
+//   4. mass_face      GSTC only: one thread per (face, tensor).
+//   5. gather         one thread per (test edge, source edge) sums the <= 2x2
+//                     incident face pairs and writes every block of Z exactly
+//                     once per slab: deterministic, no atomics.
+// Face-pair blocks live in a workspace processed in slabs of test faces, so
+// the largest meshes stream through a bounded buffer.
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sieb200 {
+
+namespace {
+
+constexpr int kMaxQ = 80;      // Dunavant rule 20 has 79 points
+constexpr int kWarps = 8;      // warps per CTA in pair_regular
+constexpr double kPi = 3.14159265358979323846;
+
+struct FaceGeom {
+    d3 v[3];
+    d3 c;        // centroid ((v0 + v1) + v2) / 3, as the reference forms it
+    d3 fv[3];    // free vertex of local edge j
+    d3 A[3];     // fv[j] - c
+    double len[3];
+    double area;
+    int idx[3];
+    int edge[3];
+};
+
+__device__ __forceinline__ d3 ldg3(const d3* p) {
+    return mk3(__ldg(&p->x), __ldg(&p->y), __ldg(&p->z));
+}
+
+// Reference-exact (no FMA contraction) centroid and distance, so that the
+// float threshold test takes the same branch as the reference kernels
+// (sie_kernels_assembly.cuh:195-199).
+__device__ __forceinline__ float centroid_distance(const FaceGeom& a, const FaceGeom& b) {
+    const double dx = __dsub_rn(a.c.x, b.c.x), dy = __dsub_rn(a.c.y, b.c.y),
+                 dz = __dsub_rn(a.c.z, b.c.z);
+    const double s = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return (float)__dsqrt_rn(s);
+}
+
+__global__ void face_prep_kernel(const double* __restrict__ V, const int* __restrict__ F,
+                                 const int* __restrict__ FE, int nf, const float* __restrict__ qpts,
+                                 int Q, FaceGeom* __restrict__ geom, d3* __restrict__ qp) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    FaceGeom g;
+    for (int a = 0; a < 3; ++a) {
+        g.idx[a] = F[3 * f + a];
+        g.edge[a] = FE[3 * f + a];
+        g.v[a] = mk3(V[3 * g.idx[a]], V[3 * g.idx[a] + 1], V[3 * g.idx[a] + 2]);
+    }
+    g.c = mk3(__ddiv_rn(__dadd_rn(__dadd_rn(g.v[0].x, g.v[1].x), g.v[2].x), 3.0),
+              __ddiv_rn(__dadd_rn(__dadd_rn(g.v[0].y, g.v[1].y), g.v[2].y), 3.0),
+              __ddiv_rn(__dadd_rn(__dadd_rn(g.v[0].z, g.v[1].z), g.v[2].z), 3.0));
+    // mesh_geometry.cuh:51-80: local edge e runs A->B, free vertex opposite,
+    // sign +1 iff global index of A > global index of B.
+    const int EA[3] = {0, 1, 2}, EB[3] = {1, 2, 0}, EF[3] = {2, 0, 1};
+    for (int e = 0; e < 3; ++e) {
+        const d3 ev = g.v[EB[e]] - g.v[EA[e]];
+        const double l = sqrt(ev.x * ev.x + ev.y * ev.y + ev.z * ev.z);
+        g.len[e] = (g.idx[EA[e]] > g.idx[EB[e]] ? 1.0 : -1.0) * l;
+        g.fv[e] = g.v[EF[e]];
+        g.A[e] = g.fv[e] - g.c;
+    }
+    const d3 cr = cross3(g.v[1] - g.v[0], g.v[2] - g.v[0]);
+    g.area = 0.5 * sqrt(dot3(cr, cr));
+    geom[f] = g;
+    // mesh_geometry.cuh:211-222 with float reference coordinates.
+    for (int q = 0; q < Q; ++q) {
+        const double xi = (double)qpts[2 * q], eta = (double)qpts[2 * q + 1];
+        const double zeta = 1.0 - xi - eta;
+        qp[(size_t)f * Q + q] = mk3(g.v[0].x * zeta + g.v[1].x * xi + g.v[2].x * eta,
+                                    g.v[0].y * zeta + g.v[1].y * xi + g.v[2].y * eta,
+                                    g.v[0].z * zeta + g.v[1].z * xi + g.v[2].z * eta);
+    }
+}
+
+// Near pairs: count (list == nullptr) or fill.
+__global__ void near_pairs_kernel(const FaceGeom* __restrict__ geom, int nf, float thr,
+                                  int m0, int m1, unsigned long long* counter, int2* list,
+                                  unsigned long long capacity) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long span = (long long)(m1 - m0) * nf;
+    if (id >= span) return;
+    const int m = m0 + (int)(id / nf), n = (int)(id % nf);
+    if (centroid_distance(geom[m], geom[n]) < thr) {
+        const unsigned long long slot = atomicAdd(counter, 1ull);
+        if (list && slot < capacity) list[slot] = make_int2(m, n);
+    }
+}
+
+template <int NK, bool TK>
+struct Moments {
+    cplx S0[NK], Sp[NK][3], Sq[NK][3], Spq[NK];
+    cplx T0[TK ? NK : 1], Tp[TK ? NK : 1][3], Tq[TK ? NK : 1][3], Tpq[TK ? NK : 1][3];
+};
+
+__device__ __forceinline__ void warp_sum(double& v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+}
+__device__ __forceinline__ void warp_sum(cplx& v) {
+    warp_sum(v.re);
+    warp_sum(v.im);
+}
+
+// One point pair: kernel values for wavenumber k (standard or extracted form)
+// green_functions_utils.cuh:236-288 / 295-361. Returns G (TL kernel) and g
+// with TK kernel = g * (r_p - r_q).
+__device__ __forceinline__ void green_std(double R, double inv_R, double i4pR, double k, cplx& G,
+                                          cplx& g) {
+    double s, c;
+    sincos(k * R, &s, &c);
+    G = cx(c * i4pR, -s * i4pR);
+    const cplx wg = cx(inv_R * G.re - k * G.im, inv_R * G.im + k * G.re);
+    g = wg * inv_R;
+}
+
+__device__ __forceinline__ void green_reg(double R, double k, cplx& G, cplx& g) {
+    if (R < 1e-9) {
+        G = cx(0.0, -k / (4.0 * kPi));
+        g = cx(0.0, 0.0);
+        return;
+    }
+    const double i4p = 1.0 / (4.0 * kPi);
+    const double inv_R = 1.0 / R, inv_R2 = inv_R * inv_R, inv_R3 = inv_R2 * inv_R;
+    const double i4pR = i4p * inv_R;
+    double s, c;
+    sincos(k * R, &s, &c);
+    G = cx((c - 1.0) * i4pR, -s * i4pR);
+    cplx K = cx(inv_R3, k * inv_R2) * cx(c, -s);
+    K.re += -(inv_R3 + k * k * 0.5 * inv_R);
+    g = K * i4p;
+}
+
+template <int NK, bool TK>
+__device__ __forceinline__ void accumulate(Moments<NK, TK>& M, const d3& pl, const d3& ql,
+                                           double pq, const d3& pxq, double ww, int a,
+                                           cplx G, cplx g) {
+    const cplx Gw = G * ww;
+    M.S0[a] += Gw;
+    M.Sp[a][0] += Gw * pl.x; M.Sp[a][1] += Gw * pl.y; M.Sp[a][2] += Gw * pl.z;
+    M.Sq[a][0] += Gw * ql.x; M.Sq[a][1] += Gw * ql.y; M.Sq[a][2] += Gw * ql.z;
+    M.Spq[a] += Gw * pq;
+    if (TK) {
+        const cplx gw = g * ww;
+        M.T0[a] += gw;
+        M.Tp[a][0] += gw * pl.x; M.Tp[a][1] += gw * pl.y; M.Tp[a][2] += gw * pl.z;
+        M.Tq[a][0] += gw * ql.x; M.Tq[a][1] += gw * ql.y; M.Tq[a][2] += gw * ql.z;
+        M.Tpq[a][0] += gw * pxq.x; M.Tpq[a][1] += gw * pxq.y; M.Tpq[a][2] += gw * pxq.z;
+    }
+}
+
+// Regular (or extracted-kernel) double quadrature of all face pairs (m, n)
+// with m in [m0, m1). Output blocks: NB = NK (TL only) or 2*NK (TL then TK),
+// each 3x3 complex, per pair at pairs[((m-m0)*nf + n) * NB*9].
+template <int NK, bool TK>
+__global__ void __launch_bounds__(kWarps * 32, 1)
+pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                    const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
+                    float thr, cplx* __restrict__ pairs) {
+    constexpr int NB = TK ? 2 * NK : NK;
+    __shared__ d3 s_tp[kMaxQ], s_tl[kMaxQ];
+    __shared__ double s_w[kMaxQ];
+    __shared__ d3 s_sp[kWarps][kMaxQ], s_sl[kWarps][kMaxQ];
+
+    const int m = m0 + blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const FaceGeom& gm = geom[m];
+    const d3 cm = gm.c;
+    for (int t = threadIdx.x; t < Q; t += blockDim.x) {
+        const d3 r = qp[(size_t)m * Q + t];
+        s_tp[t] = r;
+        s_tl[t] = r - cm;
+        s_w[t] = (double)qw_g[t];
+    }
+    __syncthreads();
+    const double kk[2] = {k0, k1};
+    const int QQ = Q * Q;
+
+    for (int n = warp; n < nf; n += kWarps) {
+        const FaceGeom& gn = geom[n];
+        const d3 cn = gn.c;
+        for (int t = lane; t < Q; t += 32) {
+            const d3 r = ldg3(&qp[(size_t)n * Q + t]);
+            s_sp[warp][t] = r;
+            s_sl[warp][t] = r - cn;
+        }
+        __syncwarp();
+        const bool regular = centroid_distance(gm, gn) < thr;  // warp-uniform
+        const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] &&
+                           gm.idx[2] == gn.idx[2];
+
+        Moments<NK, TK> M;
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            M.S0[a] = cx(0, 0); M.Spq[a] = cx(0, 0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { M.Sp[a][c] = cx(0, 0); M.Sq[a][c] = cx(0, 0); }
+            if (TK) {
+                M.T0[a] = cx(0, 0);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    M.Tp[a][c] = cx(0, 0); M.Tq[a][c] = cx(0, 0); M.Tpq[a][c] = cx(0, 0);
+                }
+            }
+        }
+
+        for (int idx = lane; idx < QQ; idx += 32) {
+            const int p = idx / Q, q = idx - p * Q;
+            const d3 rp = s_tp[p], rq = s_sp[warp][q];
+            const d3 pl = s_tl[p], ql = s_sl[warp][q];
+            const double ww = s_w[p] * s_w[q];
+            const d3 Rv = rp - rq;
+            const double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+            const double pq = dot3(pl, ql);
+            const d3 pxq = TK ? cross3(pl, ql) : mk3(0, 0, 0);
+            if (!regular) {
+                if (R < 1e-12) continue;
+                const double inv_R = 1.0 / R;
+                const double i4pR = 1.0 / (4.0 * kPi * R);
+#pragma unroll
+                for (int a = 0; a < NK; ++a) {
+                    cplx G, g;
+                    green_std(R, inv_R, i4pR, kk[a], G, g);
+                    accumulate<NK, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < NK; ++a) {
+                    cplx G, g;
+                    green_reg(R, kk[a], G, g);
+                    accumulate<NK, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
+                }
+            }
+        }
+        // Butterfly: every lane ends with the totals.
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            warp_sum(M.S0[a]); warp_sum(M.Spq[a]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { warp_sum(M.Sp[a][c]); warp_sum(M.Sq[a][c]); }
+            if (TK) {
+                warp_sum(M.T0[a]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    warp_sum(M.Tp[a][c]); warp_sum(M.Tq[a][c]); warp_sum(M.Tpq[a][c]);
+                }
+            }
+        }
+        if (lane < 9) {
+            const int j = lane / 3, i = lane - 3 * j;
+            const d3 A = gm.A[j], B = gn.A[i];
+            const d3 d = gm.fv[j] - gn.fv[i];
+            const double scale = gm.len[j] * gn.len[i];
+            const double AB = dot3(A, B);
+            cplx* out = pairs + ((size_t)blockIdx.x * nf + n) * (NB * 9);
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                // TL_ji = l_j l_i [ 1/4 (Spq - Sp.B - A.Sq + (A.B) S0) - S0 / k^2 ]
+                cplx t = M.Spq[a];
+                t = t - (M.Sp[a][0] * B.x + M.Sp[a][1] * B.y + M.Sp[a][2] * B.z);
+                t = t - (M.Sq[a][0] * A.x + M.Sq[a][1] * A.y + M.Sq[a][2] * A.z);
+                t += M.S0[a] * AB;
+                const cplx tl = (t * 0.25 - M.S0[a] * (1.0 / (kk[a] * kk[a]))) * scale;
+                out[a * 9 + lane] = tl;
+                if (TK) {
+                    cplx tk = cx(0, 0);
+                    if (!coinc) {
+                        // TK_ji = l_j l_i / 4 [ Tpq.d - (Tp x B).d - (A x Tq).d + ((A x B).d) T0 ]
+                        const d3 BxD = cross3(B, d);   // (Tp x B).d = Tp . (B x d)
+                        const d3 DxA = cross3(d, A);   // (A x Tq).d = Tq . (d x A)
+                        const double axbd = dot3(cross3(A, B), d);
+                        cplx u = M.Tpq[a][0] * d.x + M.Tpq[a][1] * d.y + M.Tpq[a][2] * d.z;
+                        u = u - (M.Tp[a][0] * BxD.x + M.Tp[a][1] * BxD.y + M.Tp[a][2] * BxD.z);
+                        u = u - (M.Tq[a][0] * DxA.x + M.Tq[a][1] * DxA.y + M.Tq[a][2] * DxA.z);
+                        u += M.T0[a] * axbd;
+                        tk = u * (0.25 * scale);
+                    }
+                    out[(NK + a) * 9 + lane] = tk;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------ Wilton ----
+struct Pots {
+    double phi0, phi2, d;
+    d3 phi1b, phi3b, r_pi;
+};
+
+__device__ __forceinline__ d3 normalize3(d3 a) {
+    const double inv = 1.0 / sqrt(dot3(a, a));
+    return a * inv;
+}
+
+// semi_analytic_integrals.cuh:35-92 and 563-667 in one pass.
+__device__ Pots wilton(const d3 r, const d3 tri[3]) {
+    Pots P;
+    const d3 n = normalize3(cross3(tri[1] - tri[0], tri[2] - tri[0]));
+    P.d = dot3(r - tri[0], n);
+    P.r_pi = r - n * P.d;
+    const double ad = fabs(P.d);
+    const double eps9f = (double)1e-9f;
+    P.phi0 = 0.0;
+    P.phi2 = 0.0;
+    P.phi1b = mk3(0, 0, 0);
+    P.phi3b = mk3(0, 0, 0);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const d3 vs = tri[e], ve = tri[(e + 1) % 3];
+        const d3 th = normalize3(ve - vs);
+        const d3 u = cross3(th, n);
+        const d3 rs = vs - n * dot3(n, vs);
+        const d3 re = ve - n * dot3(n, ve);
+        const d3 to_s = rs - P.r_pi;
+        const double su = dot3(to_s, u);
+        const double p0 = fabs(su);
+        const double orient = su >= 0.0 ? 1.0 : -1.0;
+        const double lp = dot3(re - P.r_pi, th);
+        const double lm = dot3(rs - P.r_pi, th);
+        const double Pp = hypot(p0, lp), Pm = hypot(p0, lm);
+        const double R0 = hypot(p0, ad);
+        const double Rp = hypot(Pp, ad), Rm = hypot(Pm, ad);
+        const double logt = (log(Rp) + log1p(lp / Rp)) - (log(Rm) + log1p(lm / Rm));
+        double at = 0.0;
+        if (ad > eps9f || ad > 1e-6)
+            at = atan2(p0 * lp, R0 * R0 + ad * Rp) - atan2(p0 * lm, R0 * R0 + ad * Rm);
+        if (p0 > eps9f) P.phi0 += orient * (p0 * logt - (ad > eps9f ? ad * at : 0.0));
+        P.phi1b = P.phi1b + u * ((R0 * R0) * logt + (lp * Rp) - (lm * Rm));
+        double term = 0.0;
+        if (ad > 1e-6)
+            term = (1.0 / ad) * at;
+        else if (p0 > 1e-9)
+            term = -((lp / (p0 * Pp)) - (lm / (p0 * Pm)));
+        P.phi2 += orient * term;
+        P.phi3b = P.phi3b - u * logt;
+    }
+    P.phi1b = P.phi1b * 0.5;
+    return P;
+}
+
+__device__ __forceinline__ d3 psi1(const Pots& P, d3 fv) {
+    return (P.phi1b + P.r_pi * P.phi0) - fv * P.phi0;
+}
+
+// semi_analytic_integrals.cuh:481-498 (k^2/2 formed in float).
+__device__ __forceinline__ d3 upsilon(const Pots& P, d3 fv, d3 r, float k) {
+    const d3 phi3 = P.phi3b + (P.r_pi - fv) * P.phi2;
+    const d3 ps = psi1(P, fv);
+    const float k2o2 = __fmul_rn(__fmul_rn(k, k), 0.5f);
+    const d3 comb = phi3 + ps * (double)k2o2;
+    return cross3(r - fv, comb) * -1.0;
+}
+
+// Singular (extracted) part of the near pairs, added to the pair blocks.
+// dunavant_quadrature.cuh:769-875. Lanes over outer points p.
+template <int NK>
+__global__ void pair_singular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                     const float* __restrict__ qw_g, int Q, int nf, int m0,
+                                     const int2* __restrict__ list, int count, double k0,
+                                     double k1, bool with_tk, cplx* __restrict__ pairs) {
+    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp_global >= count) return;
+    const int2 mn = list[warp_global];
+    const FaceGeom gm = geom[mn.x];
+    const FaceGeom gn = geom[mn.y];
+    const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] && gm.idx[2] == gn.idx[2];
+    const double kk[2] = {k0, k1};
+    double tl[NK][9], tk[NK][9];
+#pragma unroll
+    for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int t = 0; t < 9; ++t) { tl[a][t] = 0.0; tk[a][t] = 0.0; }
+
+    for (int p = lane; p < Q; p += 32) {
+        const d3 rp = qp[(size_t)mn.x * Q + p];
+        const double wp = (double)qw_g[p];
+        const Pots P = wilton(rp, gn.v);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const d3 rm = rp - gm.fv[j];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const d3 ps = psi1(P, gn.fv[i]);
+                const double db = 0.25 * dot3(rm, ps);
+#pragma unroll
+                for (int a = 0; a < NK; ++a) {
+                    tl[a][j * 3 + i] += (db - 1.0 / (kk[a] * kk[a]) * P.phi0) * wp;
+                    if (with_tk && !coinc) {
+                        const d3 up = upsilon(P, gn.fv[i], rp, (float)kk[a]);
+                        tk[a][j * 3 + i] += 0.25 * dot3(rm, up) * wp;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int t = 0; t < 9; ++t) { warp_sum(tl[a][t]); warp_sum(tk[a][t]); }
+    if (lane < 9) {
+        const int j = lane / 3, i = lane - 3 * j;
+        const double as = 1.0 / (4.0 * kPi * gn.area);
+        const double s = as * gm.len[j] * gn.len[i];
+        const int NB = with_tk ? 2 * NK : NK;
+        cplx* out = pairs + ((size_t)(mn.x - m0) * nf + mn.y) * (NB * 9);
+        double tlv[NK], tkv[NK];
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            // select entry `lane` without dynamic register indexing
+            tlv[a] = 0.0; tkv[a] = 0.0;
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+                if (t == lane) { tlv[a] = tl[a][t]; tkv[a] = tk[a][t]; }
+            out[a * 9 + lane].re += tlv[a] * s;
+            if (with_tk) out[(NK + a) * 9 + lane].re += tkv[a] * s;
+        }
+    }
+}
+
+// ------------------------------------------------------------ GSTC mass --
+// One thread per (face, tensor t in 0..7): tensors 0..3 are the Y blocks
+// (ee, em, me, mm) after the perp transform, 4..7 the Z blocks.
+__global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                 const float* __restrict__ qw_g, int Q, int nf,
+                                 const cplx* __restrict__ tensors, int uniform, int basis,
+                                 cplx* __restrict__ mass) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nf * 8) return;
+    const int f = id >> 3, t = id & 7;
+    const FaceGeom g = geom[f];
+    // Frame: gstc_tensor_utils.cuh:72-147.
+    d3 u, w;
+    if (basis == 0) {
+        const d3 e1 = g.v[1] - g.v[0], e2 = g.v[2] - g.v[0];
+        const d3 nn = cross3(e1, e2);
+        const double l1 = sqrt(dot3(e1, e1)), ln = sqrt(dot3(nn, nn));
+        if (l1 < 1e-20 || ln < 1e-20) {
+            u = mk3(1, 0, 0); w = mk3(0, 1, 0);
+        } else {
+            const d3 nh = nn * (1.0 / ln);
+            u = e1 * (1.0 / l1);
+            w = cross3(nh, u);
+        }
+    } else {
+        const d3 c = mk3((g.v[0].x + g.v[1].x + g.v[2].x) / 3.0, (g.v[0].y + g.v[1].y + g.v[2].y) / 3.0,
+                         (g.v[0].z + g.v[1].z + g.v[2].z) / 3.0);
+        const double r = sqrt(dot3(c, c));
+        if (r < 1e-12) {
+            u = mk3(1, 0, 0); w = mk3(0, 1, 0);
+        } else {
+            double ct = c.z / r;
+            ct = ct > 1.0 ? 1.0 : (ct < -1.0 ? -1.0 : ct);
+            const double th = acos(ct), ph = atan2(c.y, c.x);
+            const double cth = cos(th), sth = sin(th), cph = cos(ph), sph = sin(ph);
+            u = mk3(cth * cph, cth * sph, -sth);
+            w = mk3(-sph, cph, 0.0);
+        }
+    }
+    // Lift the 2x2 block (gstc_tensor_utils.cuh:184-238).
+    const cplx* tp = tensors + (uniform ? 0 : (size_t)f * 32) + (t >= 4 ? 16 : 0);
+    const int blk = t & 3, r0 = (blk >> 1) * 2, c0 = (blk & 1) * 2;
+    const cplx t00 = tp[r0 * 4 + c0], t01 = tp[r0 * 4 + c0 + 1];
+    const cplx t10 = tp[(r0 + 1) * 4 + c0], t11 = tp[(r0 + 1) * 4 + c0 + 1];
+    const double uc[3] = {u.x, u.y, u.z}, wc[3] = {w.x, w.y, w.z};
+    cplx T[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            cplx s = cx(0, 0);
+            s += t00 * (uc[i] * uc[j]);
+            s += t01 * (uc[i] * wc[j]);
+            s += t10 * (wc[i] * uc[j]);
+            s += t11 * (wc[i] * wc[j]);
+            T[i][j] = s;
+        }
+    if (t < 4) {
+        // Y_perp = -[n]x Y [n]x with float-cast entries (gstc_tensor_utils.cuh:269-309).
+        const d3 n = normalize3(cross3(g.v[1] - g.v[0], g.v[2] - g.v[0]));
+        const double N[3][3] = {{0.0, (double)(float)(-n.z), (double)(float)n.y},
+                                {(double)(float)n.z, 0.0, (double)(float)(-n.x)},
+                                {(double)(float)(-n.y), (double)(float)n.x, 0.0}};
+        cplx tmp[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                cplx s = cx(0, 0);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s += T[r][k] * N[k][c];
+                tmp[r][c] = s;
+            }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                cplx s = cx(0, 0);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s += tmp[k][c] * N[r][k];
+                T[r][c] = cx(-s.re, -s.im);
+            }
+    }
+    // Mass quadrature with float geometry (dunavant_quadrature.cuh:1422-1508).
+    const float area = (float)g.area;
+    float el[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) el[i] = (float)g.len[i];
+    cplx R[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) R[e] = cx(0, 0);
+    for (int p = 0; p < Q; ++p) {
+        const double wp = (double)qw_g[p];
+        const d3 rp = qp[(size_t)f * Q + p];
+        d3 rho[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) rho[i] = rp - g.fv[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const cplx tx = T[0][0] * rho[i].x + (T[0][1] * rho[i].y + T[0][2] * rho[i].z);
+                const cplx ty = T[1][0] * rho[i].x + (T[1][1] * rho[i].y + T[1][2] * rho[i].z);
+                const cplx tz = T[2][0] * rho[i].x + (T[2][1] * rho[i].y + T[2][2] * rho[i].z);
+                const cplx ig = tx * rho[j].x + (ty * rho[j].y + tz * rho[j].z);
+                R[j * 3 + i] += ig * wp;
+            }
+    }
+    const float sc = __fdiv_rn(1.f, __fmul_rn(4.f, area));
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float fs = __fmul_rn(__fmul_rn(sc, el[j]), el[i]);
+            mass[((size_t)f * 8 + t) * 9 + j * 3 + i] = R[j * 3 + i] * (double)fs;
+        }
+}
+
+// ------------------------------------------------------------ gather ----
+struct GatherParams {
+    int formulation;
+    int nf, ne;
+    int m0, m1;
+    int NB;
+    cplx c_jj[2], c_mm[2];
+    double s_jm, s_mm;
+    double me, me2;  // mass scales (float eta0, eta0^2)
+};
+
+// One thread per (test edge te, source edge se); te fastest for coalesced
+// column-major stores. Sums the incident face pairs with the test face in
+// [m0, m1) and adds into Z (zeroed before the first slab).
+__global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __restrict__ mass,
+                              const int* __restrict__ inc, GatherParams P, cplx* __restrict__ Z,
+                              int64_t ldz) {
+    const int te = blockIdx.x * blockDim.x + threadIdx.x;
+    const int se = blockIdx.y * blockDim.y + threadIdx.y;
+    if (te >= P.ne || se >= P.ne) return;
+    const int it[2] = {inc[2 * te], inc[2 * te + 1]};
+    const int is[2] = {inc[2 * se], inc[2 * se + 1]};
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+        if (it[a] >= 0 && it[a] / 3 >= P.m0 && it[a] / 3 < P.m1) any = true;
+    if (!any) return;
+
+    cplx acc[4] = {cx(0, 0), cx(0, 0), cx(0, 0), cx(0, 0)};
+    cplx mass_acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) mass_acc[k] = cx(0, 0);
+    bool has_mass = false;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (it[a] < 0) continue;
+        const int m = it[a] / 3, j = it[a] - 3 * m;
+        if (m < P.m0 || m >= P.m1) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            if (is[b] < 0) continue;
+            const int n = is[b] / 3, i = is[b] - 3 * n;
+            const cplx* blk = pairs + ((size_t)(m - P.m0) * P.nf + n) * (P.NB * 9) + j * 3 + i;
+            for (int k = 0; k < P.NB; ++k) acc[k] += blk[k * 9];
+            if (P.formulation == SIEB200_GSTC && m == n) {
+                has_mass = true;
+                const cplx* mb = mass + (size_t)m * 72 + j * 3 + i;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) mass_acc[k] += mb[k * 9];
+            }
+        }
+    }
+    const int64_t E = P.ne;
+    auto at = [&](int64_t r, int64_t c) -> cplx& { return Z[r + c * ldz]; };
+    if (P.formulation == SIEB200_PEC_EFIE) {
+        at(te, se) += P.c_jj[1] * acc[0];
+    } else if (P.formulation == SIEB200_PMCHWT) {
+        // acc: TL1, TL2, TK1, TK2
+        const cplx jj = P.c_jj[0] * acc[0] + P.c_jj[1] * acc[1];
+        const cplx tk = acc[2] + acc[3];
+        const cplx jm = tk * P.s_jm;
+        const cplx mm = (P.c_mm[0] * acc[0] + P.c_mm[1] * acc[1]) * P.s_mm;
+        at(te, se) += jj;
+        at(te, se + E) += jm;
+        at(te + E, se) += cx(-jm.re, -jm.im);
+        at(te + E, se + E) += mm;
+    } else {
+        cplx blk[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) blk[r][c] = cx(0, 0);
+#pragma unroll
+        for (int reg = 0; reg < 2; ++reg) {
+            const cplx tl = acc[reg], tk = acc[2 + reg];
+            const cplx jm = tk * P.s_jm;
+            const int o = 2 * reg;
+            blk[o][o] = P.c_jj[reg] * tl;
+            blk[o][o + 1] = jm;
+            blk[o + 1][o] = cx(-jm.re, -jm.im);
+            blk[o + 1][o + 1] = P.c_mm[reg] * tl;
+        }
+        if (has_mass) {
+            // A_M'' pattern with the 1/2 and 1/8 factors (sie_kernels_assembly.cuh:565-592).
+            const cplx Yee = mass_acc[0], Yem = mass_acc[1], Yme = mass_acc[2], Ymm = mass_acc[3];
+            const cplx Zee = mass_acc[4], Zem = mass_acc[5], Zme = mass_acc[6], Zmm = mass_acc[7];
+            const double f = 0.5, fq = 0.125;
+            const cplx ap = Zee * f + Ymm * fq, am = Zee * f - Ymm * fq;
+            const cplx bp = Zem * f + Yme * fq, bm = Zem * f - Yme * fq;
+            const cplx cp = Zme * f + Yem * fq, cm = Zme * f - Yem * fq;
+            const cplx dp = Zmm * f + Yee * fq, dm = Zmm * f - Yee * fq;
+            const double s1 = 1.0, se_ = P.me, s2 = P.me2;
+            blk[0][0] += ap * s1; blk[0][1] += bm * se_; blk[0][2] += am * s1; blk[0][3] += bp * se_;
+            blk[1][0] += cm * se_; blk[1][1] += dp * s2; blk[1][2] += cp * se_; blk[1][3] += dm * s2;
+            blk[2][0] += am * s1; blk[2][1] += bp * se_; blk[2][2] += ap * s1; blk[2][3] += bm * se_;
+            blk[3][0] += cp * se_; blk[3][1] += dm * s2; blk[3][2] += cm * se_; blk[3][3] += dp * s2;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) at(te + r * E, se + c * E) += blk[r][c];
+    }
+}
+
+}  // namespace
+
+int64_t system_dimension(int formulation, int64_t ne) {
+    return formulation == SIEB200_PEC_EFIE ? ne : (formulation == SIEB200_PMCHWT ? 2 * ne : 4 * ne);
+}
+
+int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                    const double* host_tensors, cplx* dZ, int64_t ldz) {
+    AssemblyParams ap;
+    SIEB_RETURN_IF(make_assembly_params(opt, &ap));
+    const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges, nv = (int)mesh.num_vertices;
+    const int64_t N = system_dimension(opt.formulation, ne);
+    SIEB_CHECK(ldz >= N, SIEB200_INVALID_ARG, "leading dimension of Z is smaller than N");
+    float pts[2 * kMaxQ], wts[kMaxQ];
+    const int Q = expand_rule(opt.quadrature_rule, pts, wts);
+    SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
+    cudaStream_t st = ctx->stream;
+
+    // Edge -> (face*3 + local edge) incidences; at most two per edge.
+    std::vector<int> inc(2 * (size_t)ne, -1);
+    for (int f = 0; f < nf; ++f)
+        for (int le = 0; le < 3; ++le) {
+            const int e = mesh.faces_edges[3 * f + le];
+            SIEB_CHECK(e >= 0 && e < ne, SIEB200_INVALID_ARG, "faces_edges entry out of range");
+            if (inc[2 * e] < 0) inc[2 * e] = 3 * f + le;
+            else if (inc[2 * e + 1] < 0) inc[2 * e + 1] = 3 * f + le;
+            else {
+                set_error("non-manifold mesh: an edge is shared by more than two faces");
+                return SIEB200_INVALID_ARG;
+            }
+        }
+
+    // Upload mesh, rule, incidences.
+    const size_t vbytes = sizeof(double) * 3 * nv, fbytes = sizeof(int) * 3 * nf;
+    SIEB_RETURN_IF(ctx->faces.reserve(vbytes + 2 * fbytes + 16 * 3));
+    char* fb = ctx->faces.as<char>();
+    double* dV = reinterpret_cast<double*>(fb);
+    int* dF = reinterpret_cast<int*>(fb + ((vbytes + 15) / 16) * 16);
+    int* dFE = dF + 3 * nf + 4;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dV, mesh.vertices, vbytes, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dF, mesh.faces, fbytes, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dFE, mesh.faces_edges, fbytes, cudaMemcpyHostToDevice, st));
+    SIEB_RETURN_IF(ctx->qw.reserve(sizeof(float) * 3 * kMaxQ));
+    float* dpts = ctx->qw.as<float>();
+    float* dw = dpts + 2 * kMaxQ;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dpts, pts, sizeof(float) * 2 * Q, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dw, wts, sizeof(float) * Q, cudaMemcpyHostToDevice, st));
+    SIEB_RETURN_IF(ctx->inc.reserve(sizeof(int) * inc.size()));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(ctx->inc.ptr, inc.data(), sizeof(int) * inc.size(),
+                                  cudaMemcpyHostToDevice, st));
+
+    SIEB_RETURN_IF(ctx->geom.reserve(sizeof(FaceGeom) * nf));
+    SIEB_RETURN_IF(ctx->qpts.reserve(sizeof(d3) * (size_t)nf * Q));
+    FaceGeom* geom = ctx->geom.as<FaceGeom>();
+    d3* qp = ctx->qpts.as<d3>();
+    face_prep_kernel<<<(nf + 127) / 128, 128, 0, st>>>(dV, dF, dFE, nf, dpts, Q, geom, qp);
+    SIEB_TRY_CUDA(cudaGetLastError());
+
+    // GSTC mass blocks.
+    cplx* dmass = nullptr;
+    if (opt.formulation == SIEB200_GSTC) {
+        const size_t ntens = opt.tensors_are_uniform ? 32 : (size_t)nf * 32;
+        SIEB_RETURN_IF(ctx->tens.reserve(sizeof(cplx) * ntens));
+        SIEB_TRY_CUDA(cudaMemcpyAsync(ctx->tens.ptr, host_tensors, sizeof(cplx) * ntens,
+                                      cudaMemcpyHostToDevice, st));
+        SIEB_RETURN_IF(ctx->mass.reserve(sizeof(cplx) * 72 * (size_t)nf));
+        dmass = ctx->mass.as<cplx>();
+        mass_face_kernel<<<(nf * 8 + 127) / 128, 128, 0, st>>>(
+            geom, qp, dw, Q, nf, ctx->tens.as<cplx>(), opt.tensors_are_uniform, ap.basis, dmass);
+        SIEB_TRY_CUDA(cudaGetLastError());
+    }
+
+    // Slabs of test faces bounded by the pair-block workspace.
+    const bool tk = opt.formulation != SIEB200_PEC_EFIE;
+    const int NK = ap.nk;
+    const int NB = tk ? 2 * NK : NK;
+    const size_t pair_bytes = sizeof(cplx) * 9 * NB;
+    size_t budget = (size_t)8 << 30;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 3);
+    int slab = (int)std::max<size_t>(1, std::min<size_t>(nf, budget / (pair_bytes * nf)));
+    SIEB_RETURN_IF(ctx->pairs.reserve(pair_bytes * (size_t)slab * nf));
+    cplx* pairs = ctx->pairs.as<cplx>();
+    SIEB_RETURN_IF(ctx->counter.reserve(sizeof(unsigned long long)));
+    unsigned long long* counter = ctx->counter.as<unsigned long long>();
+
+    SIEB_TRY_CUDA(cudaMemset2DAsync(dZ, sizeof(cplx) * ldz, 0, sizeof(cplx) * N, N, st));
+
+    GatherParams gp;
+    gp.formulation = opt.formulation;
+    gp.nf = nf;
+    gp.ne = ne;
+    gp.NB = NB;
+    gp.c_jj[0] = ap.c_jj[0]; gp.c_jj[1] = ap.c_jj[1];
+    gp.c_mm[0] = ap.c_mm[0]; gp.c_mm[1] = ap.c_mm[1];
+    gp.s_jm = ap.s_jm; gp.s_mm = ap.s_mm;
+    gp.me = ap.mass_eta0; gp.me2 = ap.mass_eta0_sq;
+
+    for (int m0 = 0; m0 < nf; m0 += slab) {
+        const int m1 = std::min(nf, m0 + slab);
+        const int rows = m1 - m0;
+        if (opt.formulation == SIEB200_PEC_EFIE)
+            pair_regular_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, pairs);
+        else
+            pair_regular_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
+        SIEB_TRY_CUDA(cudaGetLastError());
+
+        // Near-pair list of this slab: count, size, fill.
+        const long long span = (long long)rows * nf;
+        const int nb = (int)((span + 255) / 256);
+        SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+        near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter, nullptr, 0);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        unsigned long long count = 0;
+        SIEB_TRY_CUDA(cudaMemcpyAsync(&count, counter, sizeof(count), cudaMemcpyDeviceToHost, st));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+        if (count > 0) {
+            SIEB_RETURN_IF(ctx->near_list.reserve(sizeof(int2) * count));
+            SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+            near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter,
+                                                  ctx->near_list.as<int2>(), count);
+            SIEB_TRY_CUDA(cudaGetLastError());
+            const int threads = 128;
+            const int blocks = (int)((count * 32 + threads - 1) / threads);
+            if (opt.formulation == SIEB200_PEC_EFIE)
+                pair_singular_kernel<1><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],
+                    ap.k[1], false, pairs);
+            else
+                pair_singular_kernel<2><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[0],
+                    ap.k[1], true, pairs);
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
+        gp.m0 = m0;
+        gp.m1 = m1;
+        const dim3 gb(32, 8), gg((ne + 31) / 32, (ne + 7) / 8);
+        gather_kernel<<<gg, gb, 0, st>>>(pairs, dmass, ctx->inc.as<int>(), gp, dZ, ldz);
+        SIEB_TRY_CUDA(cudaGetLastError());
+    }
+    return SIEB200_OK;
+}
+
+}  // namespace sieb200

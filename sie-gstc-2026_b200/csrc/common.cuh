@@ -1,0 +1,128 @@
+// Shared types and helpers of the sieb200 CUDA library (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/sieb200.h"
+
+namespace sieb200 {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+struct Status {
+    int code;
+    std::string msg;
+};
+
+#define SIEB_TRY_CUDA(expr)                                                              \
+    do {                                                                                  \
+        cudaError_t _e = (expr);                                                          \
+        if (_e != cudaSuccess) {                                                          \
+            ::sieb200::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));    \
+            return _e == cudaErrorMemoryAllocation ? SIEB200_OUT_OF_MEMORY                \
+                                                   : SIEB200_CUDA_ERROR;                  \
+        }                                                                                 \
+    } while (0)
+
+#define SIEB_CHECK(cond, code, msg)               \
+    do {                                          \
+        if (!(cond)) {                            \
+            ::sieb200::set_error(msg);            \
+            return (code);                        \
+        }                                         \
+    } while (0)
+
+#define SIEB_RETURN_IF(st)          \
+    do {                            \
+        int _s = (st);              \
+        if (_s != SIEB200_OK) return _s; \
+    } while (0)
+
+// ------------------------------------------------------------------ math
+struct cplx {
+    double re, im;
+};
+
+__host__ __device__ inline cplx cx(double r, double i) { return {r, i}; }
+__host__ __device__ inline cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ inline cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__host__ __device__ inline cplx operator*(cplx a, cplx b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__host__ __device__ inline cplx operator*(cplx a, double s) { return {a.re * s, a.im * s}; }
+__host__ __device__ inline cplx& operator+=(cplx& a, cplx b) {
+    a.re += b.re;
+    a.im += b.im;
+    return a;
+}
+
+struct d3 {
+    double x, y, z;
+};
+__host__ __device__ inline d3 mk3(double x, double y, double z) { return {x, y, z}; }
+__host__ __device__ inline d3 operator+(d3 a, d3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__host__ __device__ inline d3 operator-(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__host__ __device__ inline d3 operator*(d3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__host__ __device__ inline double dot3(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ inline d3 cross3(d3 a, d3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// ------------------------------------------------------------------ context
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t n);  // grows, never shrinks; contents not preserved
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+    ~DeviceBuffer() { release(); }
+};
+
+}  // namespace sieb200
+
+struct sieb200_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void* cusolver = nullptr;  // cusolverDnHandle_t, created on first use
+    int sm_count = 0;
+    // Assembly workspaces (reused across calls).
+    sieb200::DeviceBuffer faces, geom, qpts, qw, pairs, near_list, counter, inc, mass, zbuf,
+        rhsbuf, srcbuf, tens;
+};
+
+namespace sieb200 {
+
+// Physical scalars of one assembly, already rounded the way the reference
+// kernels see them (their float kernel arguments).
+struct AssemblyParams {
+    int formulation = 0;
+    int nk = 1;                 // wavenumbers evaluated (1 for PEC, 2 otherwise)
+    double k[2] = {0, 0};       // float-valued
+    float threshold = 0.f;      // float centroid-distance threshold
+    // PEC: Z = c_tl[1] * TL2.
+    // PMCHWT: jj = c_jj[0] TL1 + c_jj[1] TL2; jm = s_jm (TK1+TK2); mj = -jm;
+    //         mm = s_mm (c_mm[0] TL1 + c_mm[1] TL2).
+    // GSTC:  per region r: jj = c_jj[r] TL_r, jm = s_jm TK_r, mj = -jm, mm = c_mm[r] TL_r.
+    cplx c_jj[2] = {}, c_mm[2] = {};
+    double s_jm = 0, s_mm = 1;
+    // GSTC mass-block scales (float eta0 and eta0^2).
+    double mass_eta0 = 1, mass_eta0_sq = 1;
+    int basis = 0;
+};
+
+int make_assembly_params(const sieb200_options& opt, AssemblyParams* out);
+int expand_rule(int rule, float* pts, float* w);  // returns Q or -1
+
+// Assembly on the context stream into a device column-major N x N matrix.
+int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                    const double* host_tensors, cplx* dZ, int64_t ldz);
+int assemble_rhs_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                        const sieb200_source* sources, int nsrc, cplx* dB, int64_t ldb);
+
+int64_t system_dimension(int formulation, int64_t num_edges);
+
+}  // namespace sieb200

@@ -1,0 +1,165 @@
+// Dense complex linear algebra on the context stream: the reference's
+// cuSolverDn LU (include/sie_mom/cuda/dense_lu_solver.cuh:17-184), the
+// FP64 matvec that replaces its cublasZgemv residual
+// (src/sie_mom/solvers/gstc_sie.cu:398-457), and the solver object that
+// dispatches to the mixed-precision path (mixed.cu).
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "dense.cuh"
+
+namespace sieb200 {
+
+namespace {
+
+// y = A x (+ beta y). Column-major A, one thread per row, a column chunk per
+// grid.y; deterministic two-pass reduction over chunks.
+template <class TA>
+__global__ void gemv_partial_kernel(int64_t n, const TA* __restrict__ A, int64_t lda,
+                                    const cplx* __restrict__ x, int64_t cols_per_chunk,
+                                    cplx* __restrict__ partial) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.y * cols_per_chunk;
+    const int64_t c1 = min(n, c0 + cols_per_chunk);
+    if (i >= n) return;
+    double re = 0.0, im = 0.0;
+    int64_t c = c0;
+    for (; c + 4 <= c1; c += 4) {
+        TA a[4];
+        cplx xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = A[i + (c + u) * lda];
+            xv[u] = x[c + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double ar = (double)a[u].x, ai = (double)a[u].y;
+            re += ar * xv[u].re - ai * xv[u].im;
+            im += ar * xv[u].im + ai * xv[u].re;
+        }
+    }
+    for (; c < c1; ++c) {
+        const TA a = A[i + c * lda];
+        const cplx xv = x[c];
+        re += (double)a.x * xv.re - (double)a.y * xv.im;
+        im += (double)a.x * xv.im + (double)a.y * xv.re;
+    }
+    partial[(int64_t)blockIdx.y * n + i] = cx(re, im);
+}
+
+__global__ void gemv_finish_kernel(int64_t n, int chunks, const cplx* __restrict__ partial,
+                                   double beta, cplx* __restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cplx s = beta != 0.0 ? y[i] * beta : cx(0, 0);
+    for (int k = 0; k < chunks; ++k) s += partial[(int64_t)k * n + i];
+    y[i] = s;
+}
+
+}  // namespace
+
+int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec, const cplx* x,
+                double beta, cplx* y, DeviceBuffer& scratch) {
+    const int threads = 256;
+    const int64_t row_blocks = (n + threads - 1) / threads;
+    // Aim for ~4 CTAs per SM.
+    int64_t chunks = std::max<int64_t>(1, (int64_t)ctx->sm_count * 4 / std::max<int64_t>(1, row_blocks));
+    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / 64));
+    const int64_t cpc = (n + chunks - 1) / chunks;
+    chunks = (n + cpc - 1) / cpc;
+    SIEB_RETURN_IF(scratch.reserve(sizeof(cplx) * n * chunks));
+    const dim3 grid((unsigned)row_blocks, (unsigned)chunks);
+    if (prec == 0)
+        gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(
+            n, static_cast<const double2*>(A), lda, x, cpc, scratch.as<cplx>());
+    else
+        gemv_partial_kernel<float2><<<grid, threads, 0, ctx->stream>>>(
+            n, static_cast<const float2*>(A), lda, x, cpc, scratch.as<cplx>());
+    SIEB_TRY_CUDA(cudaGetLastError());
+    gemv_finish_kernel<<<(unsigned)row_blocks, threads, 0, ctx->stream>>>(n, (int)chunks,
+                                                                          scratch.as<cplx>(), beta, y);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
+static int cusolver_handle(sieb200_ctx* ctx, cusolverDnHandle_t* h) {
+    if (!ctx->cusolver) {
+        cusolverDnHandle_t hh = nullptr;
+        SIEB_CHECK(cusolverDnCreate(&hh) == CUSOLVER_STATUS_SUCCESS, SIEB200_CUDA_ERROR,
+                   "cusolverDnCreate failed");
+        SIEB_CHECK(cusolverDnSetStream(hh, ctx->stream) == CUSOLVER_STATUS_SUCCESS,
+                   SIEB200_CUDA_ERROR, "cusolverDnSetStream failed");
+        ctx->cusolver = hh;
+    }
+    *h = static_cast<cusolverDnHandle_t>(ctx->cusolver);
+    return SIEB200_OK;
+}
+
+void destroy_cusolver(sieb200_ctx* ctx) {
+    if (ctx->cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(ctx->cusolver));
+    ctx->cusolver = nullptr;
+}
+
+int DenseSolver::factorize(double* A_, int64_t lda_) {
+    A = A_;
+    lda = lda_;
+    factored = false;
+    if (method == SIEB200_SOLVER_LU_CUSOLVER) {
+        cusolverDnHandle_t h;
+        SIEB_RETURN_IF(cusolver_handle(ctx, &h));
+        int lwork = 0;
+        SIEB_CHECK(cusolverDnZgetrf_bufferSize(h, (int)n, (int)n, reinterpret_cast<cuDoubleComplex*>(A),
+                                               (int)lda, &lwork) == CUSOLVER_STATUS_SUCCESS,
+                   SIEB200_CUDA_ERROR, "cusolverDnZgetrf_bufferSize failed");
+        SIEB_RETURN_IF(work.reserve(sizeof(cuDoubleComplex) * (size_t)std::max(lwork, 1)));
+        SIEB_RETURN_IF(ipiv.reserve(sizeof(int) * (n + 1)));
+        int* d_info = ipiv.as<int>() + n;
+        SIEB_CHECK(cusolverDnZgetrf(h, (int)n, (int)n, reinterpret_cast<cuDoubleComplex*>(A), (int)lda,
+                                    work.as<cuDoubleComplex>(), ipiv.as<int>(), d_info) ==
+                       CUSOLVER_STATUS_SUCCESS,
+                   SIEB200_CUDA_ERROR, "cusolverDnZgetrf failed");
+        int info = 0;
+        SIEB_TRY_CUDA(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (info > 0) {
+            set_error("LU factorization failed: matrix is singular (U(" + std::to_string(info) + "," +
+                      std::to_string(info) + ") is zero)");
+            return SIEB200_SINGULAR;
+        }
+        SIEB_CHECK(info == 0, SIEB200_INVALID_ARG, "cusolverDnZgetrf reported an invalid argument");
+        factored = true;
+        return SIEB200_OK;
+    }
+    if (method == SIEB200_SOLVER_LU_FP64 || method == SIEB200_SOLVER_MIXED_IR) {
+        const int st = mixed_factorize(this);
+        if (st == SIEB200_OK) factored = true;
+        return st;
+    }
+    set_error("unsupported dense solver method");
+    return SIEB200_INVALID_ARG;
+}
+
+int DenseSolver::solve(int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol, int maxit,
+                       int* iters) {
+    SIEB_CHECK(factored, SIEB200_INVALID_ARG, "dense solver: factorize() has not succeeded");
+    if (iters) *iters = 0;
+    if (method == SIEB200_SOLVER_LU_CUSOLVER) {
+        cusolverDnHandle_t h;
+        SIEB_RETURN_IF(cusolver_handle(ctx, &h));
+        int* d_info = ipiv.as<int>() + n;
+        SIEB_CHECK(cusolverDnZgetrs(h, adjoint ? CUBLAS_OP_C : CUBLAS_OP_N, (int)n, (int)nrhs,
+                                    reinterpret_cast<cuDoubleComplex*>(A), (int)lda, ipiv.as<int>(),
+                                    reinterpret_cast<cuDoubleComplex*>(B), (int)ldb,
+                                    d_info) == CUSOLVER_STATUS_SUCCESS,
+                   SIEB200_CUDA_ERROR, "cusolverDnZgetrs failed");
+        return SIEB200_OK;
+    }
+    return mixed_solve(this, nrhs, B, ldb, adjoint, tol, maxit, iters);
+}
+
+}  // namespace sieb200

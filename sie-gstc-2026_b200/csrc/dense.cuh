@@ -1,0 +1,45 @@
+// Dense solver object shared by dense.cu (cuSOLVER reference path) and
+// mixed.cu (own FP64 LU and split-FP32 tensor-core LU + GMRES refinement).
+#pragma once
+
+#include "common.cuh"
+
+namespace sieb200 {
+
+struct DenseSolver {
+    sieb200_ctx* ctx = nullptr;
+    int64_t n = 0;
+    int method = 0;
+    double* A = nullptr;  // FP64 matrix (cuSOLVER/own FP64: factors in place; mixed: original)
+    int64_t lda = 0;
+    bool factored = false;
+    DeviceBuffer ipiv, work;
+    // Own LU state (mixed.cu).
+    DeviceBuffer lu;       // factors: complex64 (mixed) or complex128 (own FP64), n x n
+    DeviceBuffer perm;     // row permutation, LAPACK-style swaps
+    DeviceBuffer panel;    // panel / tournament workspace
+    DeviceBuffer gemm_a, gemm_b;  // split-TF32 operand staging
+    DeviceBuffer krylov;   // GMRES basis and small dense work
+    DeviceBuffer vec;      // residual / work vectors
+    DeviceBuffer flags;    // triangular-solve progress flags and error word
+    DeviceBuffer gemv_scratch;
+    void* gemm_state = nullptr;
+
+    int factorize(double* A, int64_t lda);
+    int solve(int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol, int maxit, int* iters);
+};
+
+int mixed_factorize(DenseSolver* s);
+int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
+                int maxit, int* iters);
+void mixed_release(DenseSolver* s);
+
+int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec, const cplx* x,
+                double beta, cplx* y, DeviceBuffer& scratch);
+void destroy_cusolver(sieb200_ctx* ctx);
+
+}  // namespace sieb200
+
+struct sieb200_dense_solver {
+    sieb200::DenseSolver impl;
+};

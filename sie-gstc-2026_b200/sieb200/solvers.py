@@ -1,0 +1,358 @@
+"""Reference-shaped solver API over the C ABI.
+
+Names, argument meaning and error behaviour follow the SIE-GSTC solver's C++
+API (paths relative to that project):
+    solve_pec_dense           include/sie_mom/solvers/pec_solver.hpp:57-61
+    solve_dielectric_dense    include/sie_mom/solvers/dielectric/dielectric_solver.hpp:92-96
+    solve_gstc_dense          include/sie_mom/solvers/gstc_sie.hpp:214-219
+    solve_gstc_dense_batch    include/sie_mom/solvers/gstc_sie.hpp:226-239
+    DenseLuSolver             include/sie_mom/cuda/dense_lu_solver.cuh:17-184
+Invalid inputs raise ValueError (the reference's std::invalid_argument);
+singular or non-finite results raise SiebError (std::runtime_error).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .mesh import MeshData
+
+SOLVERS = {"lu_fp64": _lib.SOLVER_LU_FP64, "lu_cusolver": _lib.SOLVER_LU_CUSOLVER,
+           "mixed_ir": _lib.SOLVER_MIXED_IR}
+
+
+@dataclass
+class IsotropicMedium:
+    relative_permittivity: float = 1.0
+    relative_permeability: float = 1.0
+
+
+INTERIOR, EXTERIOR = 1, 2
+
+
+@dataclass
+class PlaneWaveExcitation:
+    electric_amplitude: Sequence[float] = (1.0, 0.0, 0.0)
+    propagation_direction: Sequence[float] = (0.0, 0.0, 1.0)
+    region: int = EXTERIOR
+
+    def as_c(self) -> _lib.Source:
+        s = _lib.Source()
+        s.kind, s.region, s.is_magnetic = 0, int(self.region), 0
+        s.a[:] = [float(x) for x in self.electric_amplitude]
+        s.b[:] = [float(x) for x in self.propagation_direction]
+        return s
+
+
+@dataclass
+class DipoleExcitation:
+    effective_moment: Sequence[float] = (0.0, 0.0, 1.0)
+    position: Sequence[float] = (0.0, 0.0, 0.0)
+    is_magnetic: bool = False
+    region: int = INTERIOR
+
+    def as_c(self) -> _lib.Source:
+        s = _lib.Source()
+        s.kind, s.region, s.is_magnetic = 1, int(self.region), int(bool(self.is_magnetic))
+        s.a[:] = [float(x) for x in self.effective_moment]
+        s.b[:] = [float(x) for x in self.position]
+        return s
+
+
+@dataclass
+class PecOptions:
+    frequency_hz: float = 0.0
+    exterior: IsotropicMedium = field(default_factory=IsotropicMedium)
+    quadrature_rule: int = 7
+    singularity_threshold_lambda0: float = 0.1
+    compute_residual: bool = True
+    vacuum_permittivity: float = 8.8541878128e-12
+    vacuum_permeability: float = 1.25663706212e-6
+    solver: str = "lu_cusolver"
+    tolerance: float = 1e-10
+    max_iterations: int = 50
+
+
+@dataclass
+class DielectricOptions:
+    frequency_hz: float = 0.0
+    interior: IsotropicMedium = field(default_factory=IsotropicMedium)
+    exterior: IsotropicMedium = field(default_factory=IsotropicMedium)
+    quadrature_rule: int = 17
+    singularity_threshold_lambda0: float = 0.1
+    compute_residual: bool = True
+    vacuum_permittivity: float = 8.8541878128e-12
+    vacuum_permeability: float = 1.25663706212e-6
+    solver: str = "lu_cusolver"
+    tolerance: float = 1e-10
+    max_iterations: int = 50
+
+
+@dataclass
+class GstcSieOptions:
+    frequency_hz: float = 0.0
+    interior: IsotropicMedium = field(default_factory=IsotropicMedium)
+    exterior: IsotropicMedium = field(default_factory=IsotropicMedium)
+    quadrature_rule: int = 17
+    singularity_threshold_lambda0: float = 0.1
+    tensors_are_uniform: bool = False
+    compute_residual: bool = True
+    basis: str = "face"
+    vacuum_permittivity: float = 8.8541878188e-12
+    vacuum_permeability: float = 1.25663706127e-6
+    solver: str = "lu_cusolver"
+    tolerance: float = 1e-10
+    max_iterations: int = 50
+
+
+def to_c_options(opt, formulation: int) -> _lib.Options:
+    o = _lib.default_options(formulation)
+    o.frequency_hz = float(opt.frequency_hz)
+    if formulation != _lib.PEC_EFIE:
+        o.eps_r_interior = float(opt.interior.relative_permittivity)
+        o.mu_r_interior = float(opt.interior.relative_permeability)
+    o.eps_r_exterior = float(opt.exterior.relative_permittivity)
+    o.mu_r_exterior = float(opt.exterior.relative_permeability)
+    o.quadrature_rule = int(opt.quadrature_rule)
+    o.singularity_threshold_lambda0 = float(opt.singularity_threshold_lambda0)
+    o.vacuum_permittivity = float(opt.vacuum_permittivity)
+    o.vacuum_permeability = float(opt.vacuum_permeability)
+    o.compute_residual = int(bool(opt.compute_residual))
+    if opt.solver not in SOLVERS:
+        raise ValueError(f"unknown solver {opt.solver!r}; choose one of {sorted(SOLVERS)}")
+    o.solver = SOLVERS[opt.solver]
+    o.tolerance = float(opt.tolerance)
+    o.max_iterations = int(opt.max_iterations)
+    if formulation == _lib.GSTC:
+        if opt.basis not in ("face", "spherical"):
+            raise ValueError("unsupported GSTC basis type")
+        o.basis = 0 if opt.basis == "face" else 1
+        o.tensors_are_uniform = int(bool(opt.tensors_are_uniform))
+    return o
+
+
+class Context:
+    """One CUDA stream plus reusable device workspaces (sieb200_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.lib().sieb200_ctx_create(int(device), ctypes.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return _lib.lib().sieb200_ctx_stream(self._h) or 0
+
+    def synchronize(self) -> None:
+        _lib.check(_lib.lib().sieb200_ctx_synchronize(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().sieb200_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_tls = threading.local()
+
+
+def default_context() -> Context:
+    ctx = getattr(_tls, "ctx", None)
+    if ctx is None:
+        ctx = Context(0)
+        _tls.ctx = ctx
+    return ctx
+
+
+@dataclass
+class SolveResult:
+    currents: np.ndarray
+    metrics: dict
+
+
+def _metrics(m: _lib.Metrics) -> dict:
+    return m.as_dict()
+
+
+def solve_pec_dense(mesh: MeshData, options: PecOptions, source, ctx: Optional[Context] = None) -> SolveResult:
+    ctx = ctx or default_context()
+    o = to_c_options(options, _lib.PEC_EFIE)
+    out = np.zeros(mesh.num_edges, dtype=np.complex128)
+    m = _lib.Metrics()
+    src = source.as_c()
+    _lib.check(_lib.lib().sieb200_solve_pec_dense(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
+                                                  ctypes.byref(src), out.ctypes.data, ctypes.byref(m)))
+    return SolveResult(out, _metrics(m))
+
+
+def solve_dielectric_dense(mesh: MeshData, options: DielectricOptions, source,
+                           ctx: Optional[Context] = None) -> SolveResult:
+    ctx = ctx or default_context()
+    o = to_c_options(options, _lib.PMCHWT)
+    out = np.zeros(2 * mesh.num_edges, dtype=np.complex128)
+    m = _lib.Metrics()
+    src = source.as_c()
+    _lib.check(_lib.lib().sieb200_solve_dielectric_dense(ctx.handle, ctypes.byref(mesh.as_c()),
+                                                         ctypes.byref(o), ctypes.byref(src),
+                                                         out.ctypes.data, ctypes.byref(m)))
+    return SolveResult(out, _metrics(m))
+
+
+@dataclass
+class GstcExcitationCase:
+    interior: Optional[object] = None
+    exterior: Optional[object] = None
+
+
+def _tensor_array(mesh: MeshData, tensors, uniform: bool) -> np.ndarray:
+    t = np.ascontiguousarray(np.asarray(tensors, dtype=np.complex128).reshape(-1))
+    expected = 32 if uniform else 32 * mesh.num_faces
+    if t.size != expected:
+        raise ValueError(f"GSTC tensor count mismatch: expected {expected}, got {t.size}")
+    return t
+
+
+def solve_gstc_dense_batch(mesh: MeshData, tensors, options: GstcSieOptions,
+                           cases: Sequence[GstcExcitationCase], ctx: Optional[Context] = None):
+    ctx = ctx or default_context()
+    if len(cases) == 0:
+        raise ValueError("SIE batch must contain at least one excitation case")
+    o = to_c_options(options, _lib.GSTC)
+    t = _tensor_array(mesh, tensors, options.tensors_are_uniform)
+    srcs = (_lib.Source * (2 * len(cases)))()
+    for c, case in enumerate(cases):
+        for slot, s in enumerate((case.interior, case.exterior)):
+            if s is None:
+                srcs[2 * c + slot].kind = -1
+            else:
+                srcs[2 * c + slot] = s.as_c()
+    N = 4 * mesh.num_edges
+    out = np.zeros((len(cases), N), dtype=np.complex128)
+    ms = (_lib.Metrics * len(cases))()
+    _lib.check(_lib.lib().sieb200_solve_gstc_dense_batch(
+        ctx.handle, ctypes.byref(mesh.as_c()), t.ctypes.data, ctypes.byref(o), srcs, len(cases),
+        out.ctypes.data, ms))
+    return [SolveResult(out[c], _metrics(ms[c])) for c in range(len(cases))]
+
+
+def solve_gstc_dense(mesh: MeshData, tensors, options: GstcSieOptions, source,
+                     ctx: Optional[Context] = None) -> SolveResult:
+    case = GstcExcitationCase(interior=source if source.region == INTERIOR else None,
+                              exterior=source if source.region == EXTERIOR else None)
+    return solve_gstc_dense_batch(mesh, tensors, options, [case], ctx)[0]
+
+
+def _formulation_of(options) -> int:
+    if isinstance(options, PecOptions):
+        return _lib.PEC_EFIE
+    if isinstance(options, DielectricOptions):
+        return _lib.PMCHWT
+    if isinstance(options, GstcSieOptions):
+        return _lib.GSTC
+    raise TypeError("options must be PecOptions, DielectricOptions or GstcSieOptions")
+
+
+def system_dimension(options, mesh: MeshData) -> int:
+    return {0: 1, 1: 2, 2: 4}[_formulation_of(options)] * mesh.num_edges
+
+
+def assemble_matrix(mesh: MeshData, options, tensors=None, ctx: Optional[Context] = None) -> np.ndarray:
+    """Dense eta0-scaled system matrix, column-major (returned as a numpy
+    array with Fortran order)."""
+    ctx = ctx or default_context()
+    f = _formulation_of(options)
+    o = to_c_options(options, f)
+    N = system_dimension(options, mesh)
+    Z = np.zeros((N, N), dtype=np.complex128, order="F")
+    t = _tensor_array(mesh, tensors, options.tensors_are_uniform) if f == _lib.GSTC else None
+    _lib.check(_lib.lib().sieb200_assemble_matrix(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
+                                                  _lib.ptr(t), Z.ctypes.data, 0))
+    return Z
+
+
+def assemble_matrix_device(mesh: MeshData, options, out_ptr: int, tensors=None,
+                           ctx: Optional[Context] = None) -> None:
+    """Assemble into caller-owned device memory (N*N complex128, ld = N)."""
+    ctx = ctx or default_context()
+    f = _formulation_of(options)
+    o = to_c_options(options, f)
+    t = _tensor_array(mesh, tensors, options.tensors_are_uniform) if f == _lib.GSTC else None
+    _lib.check(_lib.lib().sieb200_assemble_matrix(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
+                                                  _lib.ptr(t), out_ptr, 1))
+
+
+def assemble_rhs(mesh: MeshData, options, sources: Sequence, ctx: Optional[Context] = None) -> np.ndarray:
+    """One column per source, shape (N, nsrc), column-major."""
+    ctx = ctx or default_context()
+    f = _formulation_of(options)
+    o = to_c_options(options, f)
+    N = system_dimension(options, mesh)
+    arr = (_lib.Source * len(sources))(*[s.as_c() for s in sources])
+    B = np.zeros((N, len(sources)), dtype=np.complex128, order="F")
+    _lib.check(_lib.lib().sieb200_assemble_rhs(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
+                                               arr, len(sources), B.ctypes.data, 0))
+    return B
+
+
+class DenseLuSolver:
+    """Factorize once, solve many (dense_lu_solver.cuh:17-184).
+
+    Works on device memory addresses (e.g. torch tensors' data_ptr()); the
+    FP64 methods factor in place, the mixed method keeps the matrix intact
+    and refines every solve to `tolerance` against it."""
+
+    def __init__(self, n: int, method: str = "lu_cusolver", ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        if method not in SOLVERS:
+            raise ValueError(f"unknown method {method!r}")
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.lib().sieb200_dense_solver_create(self.ctx.handle, int(n), SOLVERS[method],
+                                                          ctypes.byref(self._h)))
+        self.n = n
+        self.last_iterations = 0
+
+    def factorize(self, a_ptr: int, lda: Optional[int] = None) -> None:
+        _lib.check(_lib.lib().sieb200_dense_solver_factorize(self._h, a_ptr, int(lda or self.n)))
+
+    def solve(self, b_ptr: int, nrhs: int = 1, ldb: Optional[int] = None, tolerance: float = 1e-10,
+              max_iterations: int = 50, adjoint: bool = False) -> int:
+        it = ctypes.c_int(0)
+        fn = (_lib.lib().sieb200_dense_solver_solve_adjoint if adjoint
+              else _lib.lib().sieb200_dense_solver_solve)
+        _lib.check(fn(self._h, int(nrhs), b_ptr, int(ldb or self.n), float(tolerance),
+                      int(max_iterations), ctypes.byref(it)))
+        self.last_iterations = it.value
+        return it.value
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().sieb200_dense_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def matvec(n: int, a_ptr: int, x_ptr: int, y_ptr: int, lda: Optional[int] = None, prec: int = 0,
+           beta: float = 0.0, ctx: Optional[Context] = None) -> None:
+    ctx = ctx or default_context()
+    _lib.check(_lib.lib().sieb200_matvec(ctx.handle, int(n), a_ptr, int(lda or n), int(prec), x_ptr,
+                                         float(beta), y_ptr))
