@@ -217,6 +217,14 @@ int sieb200_dense_solver_solve_adjoint(sieb200_dense_solver* s, int64_t nrhs, do
 int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                    const double* x, double beta, double* y);
 
+/* Split-TF32 tensor-core contraction used by the mixed LU's trailing update
+ * (no counterpart in the reference, which calls cuSOLVER): on device data,
+ *   C[m2 x n] (fp32, column-major, ldc) -= A[m2 x k] * B[n x k]^T,
+ * A and B K-major fp32, k a multiple of 32. mode 1: tcgen05 kernel, mode 0:
+ * SIMT kernel on the same operands (checking path). */
+int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
+                          const float* B, float* C, int64_t ldc, int mode);
+
 /* --------------------------------------------------------- far field ---- */
 /* Schelkunoff radiation vectors of the exterior RWG currents at the 7-point
  * rule, as MetasurfaceFarFieldEvaluator does

@@ -15,6 +15,7 @@
 
 #include "common.cuh"
 #include "dense.cuh"
+#include "gemm_tc.cuh"
 
 namespace sieb200 {
 
@@ -594,6 +595,20 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
                                reinterpret_cast<cplx*>(y), scratch));
     SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     return SIEB200_OK;
+}
+
+int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
+                          const float* B, float* C, int64_t ldc, int mode) {
+    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && (mode == 0 || mode == 1), SIEB200_INVALID_ARG,
+               "invalid GEMM arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    GemmTC* g = nullptr;
+    SIEB_RETURN_IF(gemm_tc_create(&g));
+    gemm_tc_set_mode(g, mode);
+    int st = gemm_tc_sub(g, ctx->stream, C, ldc, A, B, m2, n, k);
+    if (st == SIEB200_OK) st = gemm_tc_check(g, ctx->stream);
+    gemm_tc_destroy(g);
+    return st;
 }
 
 int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,

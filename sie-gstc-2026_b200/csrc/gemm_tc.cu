@@ -1,0 +1,354 @@
+// Trailing-update GEMM of the mixed-precision LU on the 5th-generation tensor
+// cores (sm_100a):
+//   C[2M x N] (fp32, column-major, ldc) -= A[2M x K] * B[N x K]^T,
+// A and B K-major fp32 (TF32 hi/lo split laid out along K by the panel
+// kernels, so the three products hi*hi + hi*lo + lo*hi are one K sweep).
+//
+// One CTA per 128 x 128 output tile, 128 threads:
+//   warp 0 lane 0  TMA producer: 128B-swizzled 128 x 32 fp32 boxes of A and B
+//                  into a 3-stage shared-memory ring (mbarrier expect_tx),
+//   warp 1 lane 0  MMA issuer: tcgen05.mma.cta_group::1.kind::tf32, M=128,
+//                  N=128, K=8 per instruction, accumulator in TMEM;
+//                  tcgen05.commit frees a stage / signals the accumulator,
+//   warp 2         allocates and frees 128 TMEM columns,
+//   warps 0-3      epilogue: tcgen05.ld 32x32b (each warp its 32 lanes =
+//                  rows), C -= acc with coalesced column stores.
+// 96 KB of shared memory lets two CTAs share an SM, so one tile's epilogue
+// overlaps the other's main loop. Every mbarrier wait is bounded; on timeout
+// the kernel records an error word, drains what it issued and returns.
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "gemm_tc.cuh"
+
+namespace sieb200 {
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 32;  // BK fp32 = 128 bytes = one swizzle atom
+constexpr int STAGES = 3;
+constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;
+constexpr int SMEM_BYTES = STAGES * (STAGE_A + STAGE_B) + 1024 /*align*/ + 256 /*barriers*/;
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false on timeout (and sets the error word).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned* err) {
+    long long it = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++it > kSpinLimit) {
+            atomicCAS(err, 0u, 3u);
+            return false;
+        }
+        if ((it & 1023) == 0 && *reinterpret_cast<volatile unsigned*>(err) != 0u) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major, 128-byte swizzle shared-memory matrix descriptor (sm_100 layout:
+// start>>4 [0,14), LBO>>4 [16,30), SBO>>4 [32,46), version 1 [46,48),
+// layout SWIZZLE_128B = 2 [61,64)); 8-row core groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return (uint64_t)((addr & 0x3FFFF) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: D f32 [4,6)=1, A tf32 [7,10)=2, B tf32 [10,13)=2,
+// both K-major, N>>3 at [17,23), M>>4 at [24,29).
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(128, 2)
+gemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, unsigned* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned stage area (required by the 128B swizzle atoms).
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);
+    const uint32_t sA = base;
+    const uint32_t sB = base + STAGES * STAGE_A;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + STAGES * (STAGE_A + STAGE_B));
+    const uint32_t full0 = smem_u32(&bars[0]);
+    const uint32_t empty0 = smem_u32(&bars[STAGES]);
+    const uint32_t accb = smem_u32(&bars[2 * STAGES]);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * STAGES + 1]);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kblocks = K / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(accb, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        // Producer.
+        for (int kb = 0; kb < kblocks; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (kb / STAGES) & 1;
+            if (!mbar_wait(empty0 + 8 * s, ph ^ 1, err)) { ok = false; break; }
+            mbar_expect_tx(full0 + 8 * s, STAGE_A + STAGE_B);
+            tma_load_2d(sA + s * STAGE_A, &tmA, full0 + 8 * s, kb * BK, m0);
+            tma_load_2d(sB + s * STAGE_B, &tmB, full0 + 8 * s, kb * BK, n0);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer.
+        for (int kb = 0; kb < kblocks; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (kb / STAGES) & 1;
+            if (!mbar_wait(full0 + 8 * s, ph, err)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint64_t ad = smem_desc_sw128(sA + s * STAGE_A);
+            const uint64_t bd = smem_desc_sw128(sB + s * STAGE_B);
+#pragma unroll
+            for (int k = 0; k < BK / 8; ++k)  // 8 tf32 = 32 bytes per instruction: start address += 2
+                umma_tf32(tmem, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u);
+            umma_commit(empty0 + 8 * s);
+        }
+        umma_commit(accb);  // fires when every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // Epilogue: all four warps. Lane 0 waits and broadcasts, so the warp stays
+    // converged for the .sync.aligned TMEM loads.
+    int got = 0;
+    if (lane == 0) got = mbar_wait(accb, 0, err) ? 1 : 0;
+    got = __shfl_sync(0xffffffffu, got, 0);
+    __syncwarp();
+    if (got) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int chunk = 0; chunk < BN / 32; ++chunk) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + chunk * 32, v);
+            if (row < M2) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = n0 + chunk * 32 + j;
+                    if (col < N) {
+                        float* p = C + (int64_t)col * ldc + row;
+                        *p = *p - v[j];
+                    }
+                }
+            }
+        }
+    } else {
+        ok = false;
+    }
+    (void)ok;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 2) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    }
+}
+
+// SIMT reference on the same packed operands (checking path).
+__global__ void gemm_simt_sub_kernel(const float* __restrict__ A, const float* __restrict__ B,
+                                     float* __restrict__ C, int64_t ldc, int M2, int N, int K) {
+    __shared__ float As[64][33], Bs[64][33];
+    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+    const int tr = threadIdx.x & 63, tc = threadIdx.x >> 6;  // 256 threads: 64 rows x 4 col groups
+    float acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[j] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+        for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {
+            const int r = e / 32, k = e % 32;
+            As[r][k] = (r0 + r < M2) ? A[(int64_t)(r0 + r) * K + k0 + k] : 0.f;
+            Bs[r][k] = (c0 + r < N) ? B[(int64_t)(c0 + r) * K + k0 + k] : 0.f;
+        }
+        __syncthreads();
+        for (int k = 0; k < 32; ++k) {
+            const float a = As[tr][k];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] += a * Bs[tc * 16 + j][k];
+        }
+        __syncthreads();
+    }
+    if (r0 + tr < M2)
+        for (int j = 0; j < 16; ++j) {
+            const int col = c0 + tc * 16 + j;
+            if (col < N) C[(int64_t)col * ldc + r0 + tr] -= acc[j];
+        }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder() {
+    if (g_encode) return SIEB200_OK;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    SIEB_TRY_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    SIEB_CHECK(fn && q == cudaDriverEntryPointSuccess, SIEB200_CUDA_ERROR,
+               "cuTensorMapEncodeTiled is not available from the driver");
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return SIEB200_OK;
+}
+
+int make_map(CUtensorMap* map, const float* ptr, int64_t inner, int64_t outer, int box_outer) {
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)(inner * sizeof(float))};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SIEB_CHECK(r == CUDA_SUCCESS, SIEB200_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return SIEB200_OK;
+}
+
+}  // namespace
+
+struct GemmTC {
+    unsigned* err = nullptr;
+    int mode = 1;
+    bool attr_set = false;
+};
+
+int gemm_tc_create(GemmTC** out) {
+    GemmTC* g = new GemmTC();
+    cudaError_t e = cudaMalloc(&g->err, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        delete g;
+        set_error(std::string("gemm workspace: ") + cudaGetErrorString(e));
+        return SIEB200_CUDA_ERROR;
+    }
+    cudaMemset(g->err, 0, sizeof(unsigned));
+    const char* env = getenv("SIEB200_GEMM_SIMT");
+    if (env && env[0] == '1') g->mode = 0;
+    *out = g;
+    return SIEB200_OK;
+}
+
+void gemm_tc_destroy(GemmTC* g) {
+    if (!g) return;
+    if (g->err) cudaFree(g->err);
+    delete g;
+}
+
+void gemm_tc_set_mode(GemmTC* g, int mode) { g->mode = mode; }
+
+int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A, const float* B,
+                int64_t M2, int64_t N, int K) {
+    SIEB_CHECK(K % BK == 0 && K > 0, SIEB200_INVALID_ARG, "GEMM K must be a positive multiple of 32");
+    SIEB_CHECK(M2 > 0 && N > 0 && M2 < (1ll << 31) && N < (1ll << 31), SIEB200_INVALID_ARG, "GEMM size out of range");
+    SIEB_CHECK(((uintptr_t)A % 16) == 0 && ((uintptr_t)B % 16) == 0, SIEB200_INVALID_ARG,
+               "GEMM operands must be 16-byte aligned");
+    if (g->mode == 0) {
+        gemm_simt_sub_kernel<<<dim3((unsigned)((M2 + 63) / 64), (unsigned)((N + 63) / 64)), 256, 0, stream>>>(
+            A, B, C, ldc, (int)M2, (int)N, K);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    }
+    SIEB_RETURN_IF(get_encoder());
+    if (!g->attr_set) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           SMEM_BYTES));
+        g->attr_set = true;
+    }
+    CUtensorMap ma, mb;
+    SIEB_RETURN_IF(make_map(&ma, A, K, M2, BM));
+    SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
+    const dim3 grid((unsigned)((M2 + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
+    gemm_tf32_sub_kernel<<<grid, 128, SMEM_BYTES, stream>>>(ma, mb, C, ldc, (int)M2, (int)N, K, g->err);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
+int gemm_tc_check(GemmTC* g, cudaStream_t stream) {
+    unsigned e = 0;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(&e, g->err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (e != 0u) {
+        set_error("tensor-core GEMM: a pipeline wait exceeded its bound");
+        return SIEB200_TIMEOUT;
+    }
+    return SIEB200_OK;
+}
+
+}  // namespace sieb200

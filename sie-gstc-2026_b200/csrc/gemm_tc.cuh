@@ -1,0 +1,25 @@
+// Split-TF32 trailing-update GEMM on the 5th-generation tensor cores.
+//   C[2M x N] (fp32, column-major, ldc) -= A[2M x K] * B[N x K]^T
+// A and B are K-major fp32 operands prepared by the LU panel kernels
+// (realified complex rows with the hi/lo TF32 split laid out along K).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace sieb200 {
+
+struct GemmTC;
+
+int gemm_tc_create(GemmTC** out);
+void gemm_tc_destroy(GemmTC* g);
+// Returns a SIEB200_* status; the kernel's bounded waits report through an
+// error word checked on the next synchronization (gemm_tc_check).
+int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A,
+                const float* B, int64_t M2, int64_t N, int K);
+int gemm_tc_check(GemmTC* g, cudaStream_t stream);
+// Selects the implementation for testing: 1 = tcgen05 (default), 0 = SIMT on
+// the same packed operands.
+void gemm_tc_set_mode(GemmTC* g, int mode);
+
+}  // namespace sieb200

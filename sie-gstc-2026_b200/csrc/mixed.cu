@@ -1,23 +1,897 @@
-// Own LU factorizations (FP64 and split-FP32 tensor-core) and GMRES-based
-// iterative refinement. Filled in by the blocked-LU implementation.
+// Mixed-precision dense solver: randomized butterfly transform + blocked LU
+// without pivoting in complex64 with split-TF32 tensor-core trailing updates,
+// wrapped in FP64 restarted GMRES (right preconditioned) against the intact
+// complex128 system. Replaces the cusolverDnZgetrf/Zgetrs path of
+// include/sie_mom/cuda/dense_lu_solver.cuh:42-166 for the solves/s metric.
+//
+// Method (published): Parker's random butterfly transform makes Gaussian
+// elimination without pivoting safe with high probability; Baboulin,
+// Dongarra et al. ("Accelerating linear system solutions using randomization
+// techniques", ACM TOMS 2013) pair it with iterative refinement. Here:
+//   W = U^T A V  (depth-2 recursive butterflies, random diagonals exp(r/10),
+//                 r uniform in [-1/2, 1/2], fixed seed), A padded to a
+//                 multiple of 4 with an identity block,
+//   W = L U      (no pivoting, block size NB; diagonal blocks factored and
+//                 inverted in one CTA each; panels by explicit block inverses;
+//                 trailing update on the tensor cores, or SIMT for checking),
+//   M^{-1} r = V U^{-1} L^{-1} U^T r  (single-kernel blocked triangular
+//                 solves with progress flags, FP64 arithmetic on c64 factors),
+//   GMRES(m) in FP64 on A M^{-1} until ||b - A x|| <= tol ||b||.
+// Every spin-wait is bounded: on timeout the kernel records an error word and
+// returns; the host reports SIEB200_TIMEOUT.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "dense.cuh"
+#include "gemm_tc.cuh"
 
 namespace sieb200 {
 
+namespace {
+
+constexpr int NB = 64;  // LU block size (complex columns)
+// Dynamic shared memory of the block kernels (two NB x (NB+1) complex64
+// tiles, or one plus a 32-row slab).
+constexpr int kSmemDiag = 2 * NB * (NB + 1) * (int)sizeof(float2);
+constexpr int kSmemPanel = (NB + 32) * (NB + 1) * (int)sizeof(float2);
+
+struct MixedState {
+    int64_t n = 0, np = 0, ldw = 0, nbl = 0;
+    float2* W = nullptr;        // factors, np x np, ld = ldw
+    float2* Linv = nullptr;     // inverse unit-lower diagonal blocks, NB x NB each (col-major)
+    float2* Uinv = nullptr;     // inverse upper diagonal blocks
+    float* Apack = nullptr;     // split realified L21: (2*np) x (6*NB), K-major
+    float* Bpack = nullptr;     // split U12 columns: np x (6*NB), K-major
+    float2* panel = nullptr;    // NB x np scratch for U12 / np x NB for L21
+    double* diag = nullptr;     // butterfly diagonals: U (level1 a,b; level2 e,f) and V, 4*np each
+    unsigned* err = nullptr;    // error word (nonzero = failure code)
+    unsigned* tri_flags = nullptr;   // per block progress flags (2 * nbl) + 2 tickets
+    cplx* vecs = nullptr;       // FP64 work vectors
+    int use_tc = 1;
+    GemmTC* gemm = nullptr;
+};
+
+// ------------------------------------------------------------ butterflies
+__device__ __forceinline__ double rbt_value(uint64_t seed, int64_t i) {
+    // splitmix64 -> uniform r in [-1/2, 1/2] -> exp(r / 10)
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+    return exp(u / 10.0);
+}
+
+__global__ void rbt_init_kernel(double* diag, int64_t np, uint64_t seed) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 8 * np) return;
+    diag[i] = rbt_value(seed, i);
+}
+
+// Index quadruple of a depth-2 butterfly: {i, i+q, i+2q, i+3q}, q = np/4.
+// Transposed application T^T = L1^T L2^T (first the two level-2 blocks, then
+// level 1) of a butterfly with diagonals d = [a (h), b (h), e (h), f (h)],
+// h = np/2: level-2 block s pairs (s h + i, s h + i + q) with e[s q + i],
+// f[s q + i]; level 1 pairs (i', i' + h) with a[i'], b[i'].
+template <class T>
+__device__ __forceinline__ void bfly_T4(T x[4], const double* d, int64_t np, int64_t i) {
+    const int64_t h = np / 2, q = np / 4;
+    const double r = 0.70710678118654752440;
+    const double* a = d;
+    const double* b = d + h;
+    const double* e = d + 2 * h;
+    const double* f = d + 3 * h;
+    // level-2 transpose: halves s = 0 (x0,x1) and s = 1 (x2,x3)
+    T z[4];
+    z[0] = (x[0] + x[1]) * (e[i] * r);
+    z[1] = (x[0] - x[1]) * (f[i] * r);
+    z[2] = (x[2] + x[3]) * (e[q + i] * r);
+    z[3] = (x[2] - x[3]) * (f[q + i] * r);
+    // level-1 transpose: pairs (i, i+h) -> (z0, z2), (i+q, i+q+h) -> (z1, z3)
+    x[0] = (z[0] + z[2]) * (a[i] * r);
+    x[2] = (z[0] - z[2]) * (b[i] * r);
+    x[1] = (z[1] + z[3]) * (a[i + q] * r);
+    x[3] = (z[1] - z[3]) * (b[i + q] * r);
+}
+
+// Forward application T = L2 L1 (level 1, then level 2).
+template <class T>
+__device__ __forceinline__ void bfly_N4(T x[4], const double* d, int64_t np, int64_t i) {
+    const int64_t h = np / 2, q = np / 4;
+    const double r = 0.70710678118654752440;
+    const double* a = d;
+    const double* b = d + h;
+    const double* e = d + 2 * h;
+    const double* f = d + 3 * h;
+    T z[4];
+    z[0] = (x[0] * a[i] + x[2] * b[i]) * r;
+    z[2] = (x[0] * a[i] - x[2] * b[i]) * r;
+    z[1] = (x[1] * a[i + q] + x[3] * b[i + q]) * r;
+    z[3] = (x[1] * a[i + q] - x[3] * b[i + q]) * r;
+    x[0] = (z[0] * e[i] + z[1] * f[i]) * r;
+    x[1] = (z[0] * e[i] - z[1] * f[i]) * r;
+    x[2] = (z[2] * e[q + i] + z[3] * f[q + i]) * r;
+    x[3] = (z[2] * e[q + i] - z[3] * f[q + i]) * r;
+}
+
+// W = U^T A_pad V, read A (c128, n x n, lda) once, write W (c64).
+__global__ void rbt_matrix_kernel(const cplx* __restrict__ A, int64_t lda, int64_t n, int64_t np,
+                                  const double* __restrict__ du, const double* __restrict__ dv,
+                                  float2* __restrict__ W, int64_t ldw) {
+    const int64_t q = np / 4;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = blockIdx.y;
+    if (i >= q || j >= q) return;
+    cplx blk[4][4];  // [row s][col t]
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int64_t c = j + t * q;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int64_t r = i + s * q;
+            cplx v;
+            if (r < n && c < n) v = A[r + c * lda];
+            else v = cx(r == c ? 1.0 : 0.0, 0.0);
+            blk[s][t] = v;
+        }
+    }
+    // rows: U^T on each column
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        cplx x[4] = {blk[0][t], blk[1][t], blk[2][t], blk[3][t]};
+        bfly_T4(x, du, np, i);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) blk[s][t] = x[s];
+    }
+    // columns: (row) * V = (V^T row^T)^T
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        cplx x[4] = {blk[s][0], blk[s][1], blk[s][2], blk[s][3]};
+        bfly_T4(x, dv, np, j);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) blk[s][t] = x[t];
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            W[(i + s * q) + (j + t * q) * ldw] = make_float2((float)blk[s][t].re, (float)blk[s][t].im);
+}
+
+// y = U^T x_pad (vector); x has n entries (rest treated as 0).
+__global__ void rbt_vec_T_kernel(const cplx* __restrict__ x, int64_t n, int64_t np,
+                                 const double* __restrict__ d, cplx* __restrict__ y) {
+    const int64_t q = np / 4;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q) return;
+    cplx v[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int64_t r = i + s * q;
+        v[s] = r < n ? x[r] : cx(0, 0);
+    }
+    bfly_T4(v, d, np, i);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) y[i + s * q] = v[s];
+}
+
+// x = V y (first n entries kept).
+__global__ void rbt_vec_N_kernel(const cplx* __restrict__ y, int64_t n, int64_t np,
+                                 const double* __restrict__ d, cplx* __restrict__ x) {
+    const int64_t q = np / 4;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q) return;
+    cplx v[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) v[s] = y[i + s * q];
+    bfly_N4(v, d, np, i);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int64_t r = i + s * q;
+        if (r < n) x[r] = v[s];
+    }
+}
+
+// ------------------------------------------------------------ block LU
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 crecipf(float2 a) {
+    const float d = a.x * a.x + a.y * a.y;
+    return make_float2(a.x / d, -a.y / d);
+}
+
+// Factor the kb x kb diagonal block in place without pivoting (one CTA,
+// block in shared memory), then form inv(L11) (unit lower) and inv(U11).
+__global__ void __launch_bounds__(256) diag_lu_kernel(float2* __restrict__ W, int64_t ldw,
+                                                      int64_t k0, int kb, float2* __restrict__ Linv,
+                                                      float2* __restrict__ Uinv,
+                                                      unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2(*A)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);             // [col][row]
+    float2(*X)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e % kb, c = e / kb;
+        A[c][r] = W[(k0 + r) + (k0 + c) * ldw];
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        const float2 piv = A[j][j];
+        const float pm = piv.x * piv.x + piv.y * piv.y;
+        if (!(pm > 1e-30f) || !isfinite(pm)) {
+            if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
+            return;
+        }
+        const float2 ip = crecipf(piv);
+        __syncthreads();
+        for (int r = j + 1 + tid; r < kb; r += blockDim.x) A[j][r] = cmulf(A[j][r], ip);
+        __syncthreads();
+        const int rows = kb - j - 1;
+        for (int e = tid; e < rows * rows; e += blockDim.x) {
+            const int r = j + 1 + e % rows, c = j + 1 + e / rows;
+            A[c][r] = csubf(A[c][r], cmulf(A[j][r], A[c][j]));
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < kb * kb; e += blockDim.x) {
+        const int r = e % kb, c = e / kb;
+        W[(k0 + r) + (k0 + c) * ldw] = A[c][r];
+    }
+    // inv(L11): solve L X = I column by column (thread per column).
+    for (int c = tid; c < kb; c += blockDim.x) {
+        for (int r = 0; r < kb; ++r) {
+            float2 s = make_float2(r == c ? 1.f : 0.f, 0.f);
+            for (int k = c; k < r; ++k) s = csubf(s, cmulf(A[k][r], X[c][k]));
+            X[c][r] = r < c ? make_float2(0.f, 0.f) : s;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
+        Linv[r + c * NB] = (r < kb && c < kb) ? X[c][r] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    // inv(U11): solve U X = I (thread per column), backward.
+    for (int c = tid; c < kb; c += blockDim.x) {
+        for (int r = kb - 1; r >= 0; --r) {
+            float2 s = make_float2(r == c ? 1.f : 0.f, 0.f);
+            if (r <= c) {
+                for (int k = r + 1; k <= c; ++k) s = csubf(s, cmulf(A[k][r], X[c][k]));
+                X[c][r] = cmulf(s, crecipf(A[r][r]));
+            } else {
+                X[c][r] = make_float2(0.f, 0.f);
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
+        Uinv[r + c * NB] = (r < kb && c < kb) ? X[c][r] : make_float2(0.f, 0.f);
+    }
+}
+
+__device__ __forceinline__ float tf32_hi(float x) {
+    uint32_t y;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
+    return __uint_as_float(y);
+}
+
+// L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
+// writes L21 back into W and the split realified rows into Apack.
+// One CTA per 32 rows; inv(U11) staged in shared memory.
+__global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0,
+                                                      int kb, int64_t r0, int64_t np,
+                                                      const float2* __restrict__ Uinv,
+                                                      float* __restrict__ Apack, int pack) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2(*Ui)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
+    float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [row][col], 32 rows
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += blockDim.x) Ui[e / NB][e % NB] = Uinv[e];
+    const int64_t rb = r0 + (int64_t)blockIdx.x * 32;
+    for (int e = tid; e < 32 * kb; e += blockDim.x) {
+        const int r = e % 32, c = e / 32;
+        const int64_t gr = rb + r;
+        Ar[r][c] = gr < np ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int K3 = 6 * NB;
+    for (int e = tid; e < 32 * kb; e += blockDim.x) {
+        const int r = e % 32, c = e / 32;
+        const int64_t gr = rb + r;
+        if (gr >= np) continue;
+        float2 s = make_float2(0.f, 0.f);
+        for (int k = 0; k <= c; ++k) s = make_float2(s.x + Ar[r][k].x * Ui[c][k].x - Ar[r][k].y * Ui[c][k].y,
+                                                     s.y + Ar[r][k].x * Ui[c][k].y + Ar[r][k].y * Ui[c][k].x);
+        W[gr + (k0 + c) * ldw] = s;
+        if (pack) {
+            // realified row 2i: [Re, -Im], row 2i+1: [Im, Re]; split [hi | hi | lo]
+            const int64_t i = gr - r0;
+            float* row0 = Apack + (2 * i) * K3;
+            float* row1 = row0 + K3;
+            const float v00 = s.x, v01 = -s.y, v10 = s.y, v11 = s.x;
+            const float h00 = tf32_hi(v00), h01 = tf32_hi(v01), h10 = tf32_hi(v10), h11 = tf32_hi(v11);
+            row0[2 * c] = h00; row0[2 * c + 1] = h01;
+            row0[2 * NB + 2 * c] = h00; row0[2 * NB + 2 * c + 1] = h01;
+            row0[4 * NB + 2 * c] = v00 - h00; row0[4 * NB + 2 * c + 1] = v01 - h01;
+            row1[2 * c] = h10; row1[2 * c + 1] = h11;
+            row1[2 * NB + 2 * c] = h10; row1[2 * NB + 2 * c + 1] = h11;
+            row1[4 * NB + 2 * c] = v10 - h10; row1[4 * NB + 2 * c + 1] = v11 - h11;
+        }
+    }
+    if (pack && kb < NB) {
+        // zero the unused K slots of these rows
+        for (int e = tid; e < 32 * (NB - kb); e += blockDim.x) {
+            const int r = e % 32, c = kb + e / 32;
+            const int64_t gr = rb + r;
+            if (gr >= np) continue;
+            const int64_t i = gr - r0;
+            for (int h = 0; h < 2; ++h) {
+                float* row = Apack + (2 * i + h) * K3;
+                for (int s = 0; s < 3; ++s) { row[s * 2 * NB + 2 * c] = 0.f; row[s * 2 * NB + 2 * c + 1] = 0.f; }
+            }
+        }
+    }
+}
+
+// U12 = inv(L11) * A12 for columns [c0, np) of the panel rows [k0, k0+kb);
+// writes U12 back into W and the split columns into Bpack. One CTA per 32 cols.
+__global__ void __launch_bounds__(256) panel_U_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0,
+                                                      int kb, int64_t c0, int64_t np,
+                                                      const float2* __restrict__ Linv,
+                                                      float* __restrict__ Bpack, int pack) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2(*Li)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
+    float2(*Ac)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [col][row], 32 cols
+    const int tid = threadIdx.x;
+    for (int e = tid; e < NB * NB; e += blockDim.x) Li[e / NB][e % NB] = Linv[e];
+    const int64_t cb = c0 + (int64_t)blockIdx.x * 32;
+    for (int e = tid; e < 32 * kb; e += blockDim.x) {
+        const int r = e % kb, c = e / kb;
+        const int64_t gc = cb + c;
+        Ac[c][r] = gc < np ? W[(k0 + r) + gc * ldw] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int K3 = 6 * NB;
+    for (int e = tid; e < 32 * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
+        const int64_t gc = cb + c;
+        if (gc >= np) continue;
+        float2 s = make_float2(0.f, 0.f);
+        if (r < kb)
+            for (int k = 0; k <= r; ++k) s = make_float2(s.x + Li[k][r].x * Ac[c][k].x - Li[k][r].y * Ac[c][k].y,
+                                                         s.y + Li[k][r].x * Ac[c][k].y + Li[k][r].y * Ac[c][k].x);
+        if (r < kb) W[(k0 + r) + gc * ldw] = s;
+        if (pack) {
+            float* col = Bpack + (gc - c0) * K3;
+            const float h0 = tf32_hi(s.x), h1 = tf32_hi(s.y);
+            col[2 * r] = h0; col[2 * r + 1] = h1;
+            col[2 * NB + 2 * r] = s.x - h0; col[2 * NB + 2 * r + 1] = s.y - h1;
+            col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
+        }
+    }
+}
+
+// SIMT trailing update C -= L21 U12 in complex64 (checking path).
+__global__ void __launch_bounds__(256) trailing_simt_kernel(float2* __restrict__ W, int64_t ldw,
+                                                            int64_t k0, int kb, int64_t s0, int64_t np) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2(*Ls)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [row][k]
+    float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + 64;   // [col][k]
+    const int64_t rb = s0 + (int64_t)blockIdx.x * 64, cb = s0 + (int64_t)blockIdx.y * 64;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 64 * kb; e += blockDim.x) {
+        const int r = e % 64, k = e / 64;
+        Ls[r][k] = rb + r < np ? W[(rb + r) + (k0 + k) * ldw] : make_float2(0.f, 0.f);
+        const int c = e % 64, kk = e / 64;
+        Us[c][kk] = cb + c < np ? W[(k0 + kk) + (cb + c) * ldw] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int e = tid; e < 64 * 64; e += blockDim.x) {
+        const int r = e % 64, c = e / 64;
+        if (rb + r >= np || cb + c >= np) continue;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int k = 0; k < kb; ++k) {
+            acc.x += Ls[r][k].x * Us[c][k].x - Ls[r][k].y * Us[c][k].y;
+            acc.y += Ls[r][k].x * Us[c][k].y + Ls[r][k].y * Us[c][k].x;
+        }
+        float2& w = W[(rb + r) + (cb + c) * ldw];
+        w = make_float2(w.x - acc.x, w.y - acc.y);
+    }
+}
+
+// ------------------------------------------------------------ triangular solves
+// Blocked forward (lower = 1) or backward solve on the factors, one CTA per
+// block row, tickets in launch order, FP64 arithmetic. x has np entries; the
+// solve is in place in x. flags: nbl words (cleared by the host), ticket at
+// flags[nbl].
+__global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
+                                                   int nbl, int lower, const float2* __restrict__ Dinv,
+                                                   cplx* __restrict__ x, unsigned* __restrict__ flags,
+                                                   unsigned* __restrict__ err, long long spin_limit) {
+    __shared__ int s_blk, s_abort;
+    __shared__ double s_re[NB][4], s_im[NB][4];
+    __shared__ cplx s_x[NB];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_blk = (int)atomicAdd(&flags[nbl], 1u);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int t = s_blk;
+    if (t >= nbl) return;
+    const int bi = lower ? t : nbl - 1 - t;
+    const int64_t r0 = (int64_t)bi * NB;
+    const int rows = (int)(np - r0 < NB ? np - r0 : NB);
+    const int r = tid & (NB - 1);   // row within block
+    const int part = tid >> 6;      // 4 partitions of the K dimension
+    double acc_re = 0.0, acc_im = 0.0;
+    for (int step = 0; step < t; ++step) {
+        const int bj = lower ? step : nbl - 1 - step;
+        if (tid == 0) {
+            // Block bj was handed out before this one, so its CTA is running;
+            // the wait is still bounded and reports through err.
+            long long it = 0;
+            while (atomicAdd(&flags[bj], 0u) == 0u) {
+                if (++it > spin_limit || atomicAdd(err, 0u) != 0u) {
+                    atomicCAS(err, 0u, 2u);
+                    s_abort = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (s_abort) return;
+        const int64_t c0 = (int64_t)bj * NB;
+        const int cols = (int)(np - c0 < NB ? np - c0 : NB);
+        if (r < rows) {
+            for (int c = part; c < cols; c += 4) {
+                const float2 a = W[(r0 + r) + (c0 + c) * ldw];
+                // produced by another CTA: read through L2, never a stale L1 line
+                const double xr = __ldcg(&x[c0 + c].re), xi = __ldcg(&x[c0 + c].im);
+                acc_re += (double)a.x * xr - (double)a.y * xi;
+                acc_im += (double)a.x * xi + (double)a.y * xr;
+            }
+        }
+        __syncthreads();
+    }
+    s_re[r][part] = acc_re;
+    s_im[r][part] = acc_im;
+    __syncthreads();
+    if (tid < NB) {
+        const cplx b = tid < rows ? cx(__ldcg(&x[r0 + tid].re), __ldcg(&x[r0 + tid].im)) : cx(0, 0);
+        const double sr = s_re[tid][0] + s_re[tid][1] + s_re[tid][2] + s_re[tid][3];
+        const double si = s_im[tid][0] + s_im[tid][1] + s_im[tid][2] + s_im[tid][3];
+        s_x[tid] = cx(b.re - sr, b.im - si);
+    }
+    __syncthreads();
+    // x_i = Dinv * s  (Dinv: NB x NB col-major, this block)
+    const float2* D = Dinv + (size_t)bi * NB * NB;
+    if (tid < rows) {
+        double re = 0.0, im = 0.0;
+        for (int c = 0; c < rows; ++c) {
+            const float2 a = D[tid + c * NB];
+            re += (double)a.x * s_x[c].re - (double)a.y * s_x[c].im;
+            im += (double)a.x * s_x[c].im + (double)a.y * s_x[c].re;
+        }
+        __stcg(&x[r0 + tid].re, re);
+        __stcg(&x[r0 + tid].im, im);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(&flags[bi], 1u);
+}
+
+// ------------------------------------------------------------ small vector ops
+__global__ void dot_partial_kernel(int64_t n, int k, const cplx* __restrict__ V, int64_t ldv,
+                                   const cplx* __restrict__ w, cplx* __restrict__ out) {
+    // out[blockIdx.y + k * blockIdx.x] = sum over this block's slice of conj(V_j) w
+    const int j = blockIdx.y;
+    __shared__ double sr[8], si[8];
+    double re = 0, im = 0;
+    const cplx* v = V + (int64_t)j * ldv;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const cplx a = v[i], b = w[i];
+        re += a.re * b.re + a.im * b.im;
+        im += a.re * b.im - a.im * b.re;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sr[threadIdx.x >> 5] = re; si[threadIdx.x >> 5] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tre = 0, tim = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { tre += sr[q]; tim += si[q]; }
+        out[(int64_t)blockIdx.x * k + j] = cx(tre, tim);
+    }
+}
+
+__global__ void dot_finish_kernel(int k, int parts, const cplx* __restrict__ partial, cplx* __restrict__ h) {
+    const int j = threadIdx.x;
+    if (j >= k) return;
+    cplx s = cx(0, 0);
+    for (int p = 0; p < parts; ++p) s += partial[(int64_t)p * k + j];
+    h[j] = s;
+}
+
+// w -= V[:, 0:k] h
+__global__ void axpy_multi_kernel(int64_t n, int k, const cplx* __restrict__ V, int64_t ldv,
+                                  const cplx* __restrict__ h, cplx* __restrict__ w) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cplx s = w[i];
+    for (int j = 0; j < k; ++j) s = s - V[i + (int64_t)j * ldv] * h[j];
+    w[i] = s;
+}
+
+__global__ void scale_copy_kernel(int64_t n, const cplx* __restrict__ x, double s, cplx* __restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = x[i] * s;
+}
+
+__global__ void combo_kernel(int64_t n, int k, const cplx* __restrict__ V, int64_t ldv,
+                             const cplx* __restrict__ y, cplx* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    cplx s = cx(0, 0);
+    for (int j = 0; j < k; ++j) s += V[i + (int64_t)j * ldv] * y[j];
+    out[i] = s;
+}
+
+__global__ void add_kernel(int64_t n, const cplx* __restrict__ a, cplx* __restrict__ x) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += a[i];
+}
+
+__global__ void conj_kernel(int64_t n, cplx* __restrict__ x) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i].im = -x[i].im;
+}
+
+// Adjoint support: W^H solves are done on the conjugate transpose factors.
+__global__ void conj_transpose_c64_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
+                                          float2* __restrict__ WT) {
+    __shared__ float2 tile[32][33];
+    const int64_t bx = (int64_t)blockIdx.x * 32, by = (int64_t)blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = bx + threadIdx.x, c = by + j;
+        if (r < np && c < np) tile[j][threadIdx.x] = W[r + c * ldw];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = by + threadIdx.x, c = bx + j;
+        if (r < np && c < np) {
+            const float2 v = tile[threadIdx.x][j];
+            WT[r + c * ldw] = make_float2(v.x, -v.y);
+        }
+    }
+}
+
+inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ------------------------------------------------------------ host side
+
+static MixedState* state_of(DenseSolver* s) { return static_cast<MixedState*>(s->gemm_state); }
+
+void mixed_release(DenseSolver* s) {
+    MixedState* st = state_of(s);
+    if (st) {
+        if (st->gemm) gemm_tc_destroy(st->gemm);
+        delete st;
+    }
+    s->gemm_state = nullptr;
+    s->lu.release(); s->perm.release(); s->panel.release(); s->gemm_a.release(); s->gemm_b.release();
+    s->krylov.release(); s->vec.release(); s->flags.release(); s->gemv_scratch.release();
+}
+
+static int check_err(DenseSolver* s, const char* what) {
+    MixedState* st = state_of(s);
+    unsigned e = 0;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(&e, st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->ctx->stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(s->ctx->stream));
+    if (e == 1u) {
+        set_error(std::string(what) + ": zero or non-finite pivot in the unpivoted LU of the randomized matrix");
+        return SIEB200_SINGULAR;
+    }
+    if (e == 2u) {
+        set_error(std::string(what) + ": a triangular-solve block waited past its bound");
+        return SIEB200_TIMEOUT;
+    }
+    if (e != 0u) {
+        set_error(std::string(what) + ": device error word " + std::to_string(e));
+        return SIEB200_CUDA_ERROR;
+    }
+    return SIEB200_OK;
+}
+
 int mixed_factorize(DenseSolver* s) {
-    (void)s;
-    set_error("own LU factorization is not built into this library yet");
-    return SIEB200_INVALID_ARG;
+    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG,
+               "own FP64 LU is not available in this build; use SIEB200_SOLVER_LU_CUSOLVER");
+    sieb200_ctx* ctx = s->ctx;
+    cudaStream_t stream = ctx->stream;
+    MixedState* st = state_of(s);
+    if (!st) {
+        st = new MixedState();
+        s->gemm_state = st;
+    }
+    const int64_t n = s->n;
+    const int64_t np = ((n + 3) / 4) * 4;
+    const int64_t ldw = ((np + 31) / 32) * 32;
+    const int64_t nbl = (np + NB - 1) / NB;
+    st->n = n; st->np = np; st->ldw = ldw; st->nbl = nbl;
+    const char* env = getenv("SIEB200_TRAILING_SIMT");
+    st->use_tc = (env && env[0] == '1') ? 0 : 1;
+
+    // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
+    const size_t bW = sizeof(float2) * ldw * np;
+    const size_t bInv = sizeof(float2) * NB * NB * nbl;
+    const size_t bDiag = sizeof(double) * 8 * np;
+    const size_t bFlags = sizeof(unsigned) * (4 * nbl + 16);
+    auto up = [](size_t b) { return ((b + 255) / 256) * 256; };
+    SIEB_RETURN_IF(s->lu.reserve(up(bW) + 2 * up(bInv) + up(bDiag) + up(bFlags)));
+    char* base = s->lu.as<char>();
+    st->W = reinterpret_cast<float2*>(base);
+    st->Linv = reinterpret_cast<float2*>(base + up(bW));
+    st->Uinv = reinterpret_cast<float2*>(base + up(bW) + up(bInv));
+    st->diag = reinterpret_cast<double*>(base + up(bW) + 2 * up(bInv));
+    st->err = reinterpret_cast<unsigned*>(base + up(bW) + 2 * up(bInv) + up(bDiag));
+    st->tri_flags = st->err + 16;
+    const int K3 = 6 * NB;
+    SIEB_RETURN_IF(s->gemm_a.reserve(sizeof(float) * 2 * np * K3));
+    SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * K3));
+    st->Apack = s->gemm_a.as<float>();
+    st->Bpack = s->gemm_b.as<float>();
+    if (st->use_tc && !st->gemm) SIEB_RETURN_IF(gemm_tc_create(&st->gemm));
+
+    static bool attrs_set = false;
+    if (!attrs_set) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_L_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        attrs_set = true;
+    }
+    SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
+    rbt_init_kernel<<<blocks_for(8 * np, 256), 256, 0, stream>>>(st->diag, np, 0x5EB200ull);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    const int64_t q = np / 4;
+    rbt_matrix_kernel<<<dim3(blocks_for(q, 128), (unsigned)q), 128, 0, stream>>>(
+        reinterpret_cast<const cplx*>(s->A), s->lda, n, np, st->diag, st->diag + 4 * np, st->W, ldw);
+    SIEB_TRY_CUDA(cudaGetLastError());
+
+    for (int64_t bk = 0; bk < nbl; ++bk) {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        float2* Li = st->Linv + (size_t)bk * NB * NB;
+        float2* Ui = st->Uinv + (size_t)bk * NB * NB;
+        diag_lu_kernel<<<1, 256, kSmemDiag, stream>>>(st->W, ldw, k0, kb, Li, Ui, st->err);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        const int64_t s0 = k0 + kb;
+        if (s0 >= np) break;
+        const int64_t m = np - s0;
+        panel_L_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Ui, st->Apack,
+                                                             st->use_tc);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        panel_U_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Li, st->Bpack,
+                                                             st->use_tc);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        if (st->use_tc) {
+            float* C = reinterpret_cast<float*>(st->W + s0 + s0 * ldw);
+            SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, st->Apack, st->Bpack, 2 * m, m, K3));
+        } else {
+            trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
+                st->W, ldw, k0, kb, s0, np);
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
+    }
+    return check_err(s, "mixed LU factorization");
+}
+
+// Apply M^{-1} = V U^{-1} L^{-1} U^T to r (length n) into z (length n).
+static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, bool adjoint) {
+    MixedState* st = state_of(s);
+    cudaStream_t stream = s->ctx->stream;
+    const int64_t n = st->n, np = st->np, q = np / 4;
+    const double* du = st->diag;
+    const double* dv = st->diag + 4 * np;
+    // Adjoint: (V W^{-1} U^T)^H = U W^{-H} V^T, with W^H = U^H L^H.
+    const double* d_first = adjoint ? dv : du;
+    const double* d_last = adjoint ? du : dv;
+    rbt_vec_T_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(r, n, np, d_first, work);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    const long long spin = 1ll << 26;
+    unsigned* fl = st->tri_flags;
+    const int nbl = (int)st->nbl;
+    if (!adjoint) {
+        SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
+        trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, 1, st->Linv, work, fl, st->err, spin);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
+        trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, 0, st->Uinv, work, fl, st->err, spin);
+        SIEB_TRY_CUDA(cudaGetLastError());
+    } else {
+        // W^H y = c  <=>  conj(W)^T y = c: solve with conj on both sides using
+        // the transposed factors held in s->panel (built on first use).
+        return SIEB200_INVALID_ARG;
+    }
+    rbt_vec_N_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(work, n, np, d_last, z);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
+static double host_norm2(const std::vector<cplx>& v) {
+    long double s = 0;
+    for (const cplx& c : v) s += (long double)c.re * c.re + (long double)c.im * c.im;
+    return std::sqrt((double)s);
+}
+
+// Restarted right-preconditioned GMRES on A x = b (FP64, A the intact
+// complex128 matrix), started from x = M^{-1} b.
+static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int maxit, int* iters) {
+    (void)ldb_unused;
+    MixedState* st = state_of(s);
+    sieb200_ctx* ctx = s->ctx;
+    cudaStream_t stream = ctx->stream;
+    const int64_t n = st->n, np = st->np;
+    const int m = 20;  // restart length
+    const int parts = 64;
+    // vectors: x, r, w, z, work(np), V (n x (m+1)), partial, h
+    const size_t vbytes = sizeof(cplx) * (5 * np + (int64_t)(m + 1) * n + parts * (m + 1) + (m + 2));
+    SIEB_RETURN_IF(s->krylov.reserve(vbytes));
+    cplx* x = s->krylov.as<cplx>();
+    cplx* r = x + np;
+    cplx* w = r + np;
+    cplx* z = w + np;
+    cplx* work = z + np;
+    cplx* V = work + np;
+    cplx* partial = V + (int64_t)(m + 1) * n;
+    cplx* h = partial + parts * (m + 1);
+    const double* A = s->A;
+    const int64_t lda = s->lda;
+
+    // ||b||
+    std::vector<cplx> hb(n);
+    SIEB_TRY_CUDA(cudaMemcpyAsync(hb.data(), b, sizeof(cplx) * n, cudaMemcpyDeviceToHost, stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+    const double bnorm = host_norm2(hb);
+    SIEB_CHECK(bnorm > 0 && std::isfinite(bnorm), SIEB200_INVALID_ARG, "right-hand side norm must be finite and nonzero");
+
+    SIEB_RETURN_IF(apply_precond(s, b, x, work, false));
+    int total = 0;
+    std::vector<cplx> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), hh(m + 2);
+    for (int outer = 0; outer < 1000; ++outer) {
+        // r = b - A x
+        SIEB_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
+        SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));  // r = A x - b
+        dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, r, n, r, partial);
+        dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
+        cplx rr;
+        SIEB_TRY_CUDA(cudaMemcpyAsync(&rr, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+        const double beta = std::sqrt(std::max(rr.re, 0.0));
+        if (!std::isfinite(beta)) {
+            set_error("GMRES refinement produced a non-finite residual");
+            return SIEB200_NONFINITE;
+        }
+        if (beta <= tol * bnorm) break;
+        if (total >= maxit) {
+            if (iters) *iters = total;
+            set_error("GMRES refinement did not reach the tolerance within max_iterations");
+            return SIEB200_NOT_CONVERGED;
+        }
+        // r holds A x - b: v1 = -r / beta
+        scale_copy_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, r, -1.0 / beta, V);
+        std::fill(g.begin(), g.end(), cx(0, 0));
+        g[0] = cx(beta, 0);
+        int j = 0;
+        double est = beta;
+        for (; j < m && total < maxit; ++j, ++total) {
+            cplx* vj = V + (int64_t)j * n;
+            SIEB_RETURN_IF(apply_precond(s, vj, z, work, false));
+            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, z, 0.0, w, s->gemv_scratch));
+            // Classical Gram-Schmidt with one reorthogonalization (CGS2).
+            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
+            for (int pass = 0; pass < 2; ++pass) {
+                dot_partial_kernel<<<dim3(parts, j + 1), 256, 0, stream>>>(n, j + 1, V, n, w, partial);
+                dot_finish_kernel<<<1, 64, 0, stream>>>(j + 1, parts, partial, h);
+                axpy_multi_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j + 1, V, n, h, w);
+                SIEB_TRY_CUDA(cudaGetLastError());
+                SIEB_TRY_CUDA(cudaMemcpyAsync(hh.data(), h, sizeof(cplx) * (j + 1), cudaMemcpyDeviceToHost,
+                                              stream));
+                SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+                for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = H[(size_t)i * m + j] + hh[i];
+            }
+            dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, w, n, w, partial);
+            dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
+            cplx ww;
+            SIEB_TRY_CUDA(cudaMemcpyAsync(&ww, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
+            SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+            const double hn = std::sqrt(std::max(ww.re, 0.0));
+            cplx hj1 = cx(hn, 0);
+            if (j + 1 <= m)
+                scale_copy_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, w, hn > 0 ? 1.0 / hn : 0.0,
+                                                                           V + (int64_t)(j + 1) * n);
+            // Givens on column j
+            for (int i = 0; i < j; ++i) {
+                const cplx a = H[(size_t)i * m + j], bb = H[(size_t)(i + 1) * m + j];
+                // [c s; -conj(s) c] with real c
+                const cplx t1 = cx(cs[i].re * a.re + (sn[i] * bb).re, cs[i].re * a.im + (sn[i] * bb).im);
+                const cplx conj_s = cx(sn[i].re, -sn[i].im);
+                const cplx t2 = cx(-(conj_s * a).re + cs[i].re * bb.re, -(conj_s * a).im + cs[i].re * bb.im);
+                H[(size_t)i * m + j] = t1;
+                H[(size_t)(i + 1) * m + j] = t2;
+            }
+            const cplx a = H[(size_t)j * m + j];
+            const double an = std::hypot(a.re, a.im), bn = hn;
+            const double den = std::hypot(an, bn);
+            if (den == 0.0) { cs[j] = cx(1, 0); sn[j] = cx(0, 0); }
+            else if (an == 0.0) { cs[j] = cx(0, 0); sn[j] = cx(1, 0); }
+            else {
+                cs[j] = cx(an / den, 0);
+                // s = (a/|a|) * conj(b) / den with b = hn real
+                sn[j] = cx(a.re / an * bn / den, a.im / an * bn / den);
+            }
+            H[(size_t)j * m + j] = cx(cs[j].re * a.re + sn[j].re * hn, cs[j].re * a.im + sn[j].im * hn);
+            (void)hj1;
+            const cplx gj = g[j];
+            const cplx conj_s = cx(sn[j].re, -sn[j].im);
+            g[j] = cx(cs[j].re * gj.re, cs[j].re * gj.im);
+            g[j + 1] = cx(-(conj_s * gj).re, -(conj_s * gj).im);
+            est = std::hypot(g[j + 1].re, g[j + 1].im);
+            if (est <= 0.5 * tol * bnorm || hn == 0.0) { ++j; ++total; break; }
+        }
+        // y = H^{-1} g (upper triangular j x j)
+        std::vector<cplx> y(j);
+        for (int i = j - 1; i >= 0; --i) {
+            cplx sacc = g[i];
+            for (int k = i + 1; k < j; ++k) sacc = sacc - H[(size_t)i * m + k] * y[k];
+            const cplx d = H[(size_t)i * m + i];
+            const double dd = d.re * d.re + d.im * d.im;
+            y[i] = cx((sacc.re * d.re + sacc.im * d.im) / dd, (sacc.im * d.re - sacc.re * d.im) / dd);
+        }
+        SIEB_TRY_CUDA(cudaMemcpyAsync(h, y.data(), sizeof(cplx) * j, cudaMemcpyHostToDevice, stream));
+        combo_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j, V, n, h, w);
+        SIEB_RETURN_IF(apply_precond(s, w, z, work, false));
+        add_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, z, x);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        SIEB_RETURN_IF(check_err(s, "GMRES refinement"));
+    }
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b, x, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
+    if (iters) *iters = total;
+    return check_err(s, "GMRES refinement");
 }
 
 int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
                 int maxit, int* iters) {
-    (void)s; (void)nrhs; (void)B; (void)ldb; (void)adjoint; (void)tol; (void)maxit; (void)iters;
-    set_error("own LU solve is not built into this library yet");
-    return SIEB200_INVALID_ARG;
+    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG, "unsupported solver method");
+    SIEB_CHECK(!adjoint, SIEB200_INVALID_ARG, "adjoint solve of the mixed method is not available yet");
+    if (!(tol > 0)) tol = 1e-10;
+    if (maxit <= 0) maxit = 50;
+    int total = 0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+        int it = 0;
+        const int st = gmres_ir(s, reinterpret_cast<cplx*>(B) + c * ldb, ldb, tol, maxit, &it);
+        total = std::max(total, it);
+        if (st != SIEB200_OK) {
+            if (iters) *iters = total;
+            return st;
+        }
+    }
+    if (iters) *iters = total;
+    return SIEB200_OK;
 }
-
-void mixed_release(DenseSolver* s) { (void)s; }
 
 }  // namespace sieb200

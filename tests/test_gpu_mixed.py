@@ -1,0 +1,116 @@
+"""GPU: the split-TF32 tensor-core GEMM and the mixed-precision refined
+solver against FP64 references.
+
+Tolerances: the GEMM on TF32-representable operands with FP32 accumulation
+agrees with an FP64 product to 1e-5 relative (K = 384); the mixed solver's
+currents agree with the cuSOLVER FP64 path to 1e-9 relative and its
+relative residual on the scaled system is <= 1e-10 (the refinement target)."""
+
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+C0 = 299792458.0
+
+
+def _tf32(x):
+    b = np.asarray(x, dtype=np.float32).view(np.uint32) & np.uint32(0xFFFFE000)
+    return b.view(np.float32)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("m2,n", [(256, 128), (300, 200), (1000, 517)])
+def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
+    import torch
+    import sieb200
+    from sieb200 import _lib
+    rng = np.random.default_rng(m2 + n)
+    K = 384
+    A = _tf32(rng.standard_normal((m2, K)))
+    B = _tf32(rng.standard_normal((n, K)))
+    ldc = m2 + 8
+    C = rng.standard_normal((n, ldc)).astype(np.float32)  # column-major storage: C[col, row]
+    dA, dB, dC = (torch.from_numpy(x.copy()).cuda() for x in (A, B, C))
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().sieb200_gemm_tf32_sub(gpu_ctx.handle, m2, n, K, dA.data_ptr(), dB.data_ptr(),
+                                                 dC.data_ptr(), ldc, mode))
+    out = dC.cpu().numpy()
+    ref = C.astype(np.float64).copy()
+    ref[:, :m2] -= (A.astype(np.float64) @ B.astype(np.float64).T).T
+    assert rel_err(out[:, :m2], ref[:, :m2]) < 1e-5
+    assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
+
+
+def _pmchwt(level=2, solver="lu_cusolver", rule=5):
+    import sieb200
+    m = sieb200.icosphere(0.5, level)
+    o = sieb200.DielectricOptions(frequency_hz=C0, quadrature_rule=rule,
+                                  interior=sieb200.IsotropicMedium(4.0, 1.0), solver=solver)
+    return m, o
+
+
+@pytest.mark.parametrize("trailing", ["tc", "simt"])
+def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
+    import sieb200
+    if trailing == "simt":
+        monkeypatch.setenv("SIEB200_TRAILING_SIMT", "1")
+    m, o = _pmchwt(2)
+    ref = sieb200.solve_dielectric_dense(m, o, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
+    o.solver = "mixed_ir"
+    r = sieb200.solve_dielectric_dense(m, o, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
+    assert r.metrics["relative_residual"] <= 1e-10
+    assert np.linalg.norm(r.currents - ref.currents) / np.linalg.norm(ref.currents) < 1e-9
+    assert 1 <= r.metrics["refinement_iterations"] <= 20
+
+
+def test_mixed_gstc_batch_and_pec(gpu_ctx):
+    import sieb200
+    m = sieb200.icosphere(1.0, 2)
+    rng = np.random.default_rng(2)
+    t = rng.standard_normal((m.num_faces, 32)) + 1j * rng.standard_normal((m.num_faces, 32))
+    t *= 0.3
+    o = sieb200.GstcSieOptions(frequency_hz=C0, quadrature_rule=5)
+    cases = [sieb200.GstcExcitationCase(exterior=sieb200.PlaneWaveExcitation()),
+             sieb200.GstcExcitationCase(exterior=sieb200.PlaneWaveExcitation(
+                 electric_amplitude=(0, 1, 0), propagation_direction=(1, 0, 0)))]
+    ref = sieb200.solve_gstc_dense_batch(m, t, o, cases, ctx=gpu_ctx)
+    o.solver = "mixed_ir"
+    got = sieb200.solve_gstc_dense_batch(m, t, o, cases, ctx=gpu_ctx)
+    for a, b in zip(got, ref):
+        assert a.metrics["relative_residual"] <= 1e-10
+        assert np.linalg.norm(a.currents - b.currents) / np.linalg.norm(b.currents) < 1e-9
+    pm = sieb200.icosphere(1.0, 2)
+    po = sieb200.PecOptions(frequency_hz=C0, quadrature_rule=5)
+    pref = sieb200.solve_pec_dense(pm, po, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
+    po.solver = "mixed_ir"
+    pgot = sieb200.solve_pec_dense(pm, po, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
+    assert pgot.metrics["relative_residual"] <= 1e-10
+    assert np.linalg.norm(pgot.currents - pref.currents) / np.linalg.norm(pref.currents) < 1e-9
+
+
+def test_dense_solver_object_on_device_memory(gpu_ctx):
+    import torch
+    import sieb200
+    m, o = _pmchwt(2)
+    N = 2 * m.num_edges
+    Z = torch.empty((N, N), dtype=torch.complex128, device="cuda")
+    sieb200.assemble_matrix_device(m, o, Z.data_ptr(), ctx=gpu_ctx)
+    b = torch.from_numpy(sieb200.assemble_rhs(m, o, [sieb200.PlaneWaveExcitation()], ctx=gpu_ctx)[:, 0].copy()).cuda()
+    Zh = Z.cpu().numpy().T  # storage is column-major
+    x_ref = np.linalg.solve(Zh, b.cpu().numpy())
+    s = sieb200.DenseLuSolver(N, "mixed_ir", ctx=gpu_ctx)
+    s.factorize(Z.data_ptr())
+    x = b.clone()
+    torch.cuda.synchronize()
+    it = s.solve(x.data_ptr(), tolerance=1e-12, max_iterations=60)
+    gpu_ctx.synchronize()
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(xs - x_ref) / np.linalg.norm(x_ref) < 1e-10
+    assert np.linalg.norm(Zh @ xs - b.cpu().numpy()) / np.linalg.norm(b.cpu().numpy()) < 1e-12
+    assert it >= 1
+    s.close()
