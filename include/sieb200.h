@@ -225,6 +225,19 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode);
 
+/* Per-context kernel timing (no counterpart in the reference, which times
+ * phases with std::chrono): when enabled, the library brackets each launch
+ * of the listed kernels with CUDA events on the context stream and
+ * accumulates launch count, device milliseconds and algorithmic work.
+ * kernel 0: split-TF32 trailing GEMM (work = 2*m2*n*k TF32 flops and
+ * 4*(2*m2*n + (m2 + n)*k) bytes per launch); 1: triangular solves
+ * (work = bytes of factors read); 2: FP64 matvec (bytes of Z read). */
+int sieb200_profile_enable(sieb200_ctx* ctx, int enable);
+/* Number of CUDA kernels the library has launched in this process. */
+int64_t sieb200_launch_count(void);
+int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,
+                         double* flops, double* bytes);
+
 /* --------------------------------------------------------- far field ---- */
 /* Schelkunoff radiation vectors of the exterior RWG currents at the 7-point
  * rule, as MetasurfaceFarFieldEvaluator does

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -47,6 +48,43 @@ double seconds_since(Clock::time_point t0) {
 }  // namespace
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void Profiler::begin(cudaStream_t s, int kernel, double flops, double bytes, cudaEvent_t* end_out) {
+    *end_out = nullptr;
+    if (!enabled) return;
+    Pending p{kernel, nullptr, nullptr, flops, bytes};
+    if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaEventRecord(p.a, s);
+    pending.push_back(p);
+    *end_out = p.b;
+}
+
+void Profiler::end(cudaStream_t s, cudaEvent_t e) {
+    if (e) cudaEventRecord(e, s);
+}
+
+void Profiler::collect() {
+    for (Pending& p : pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            KernelProfile& kp = k[p.kernel];
+            kp.launches += 1;
+            kp.ms += ms;
+            kp.flops += p.flops;
+            kp.bytes += p.bytes;
+        }
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+    cudaGetLastError();
+}
 
 int DeviceBuffer::reserve(size_t n) {
     if (n <= bytes && ptr) return SIEB200_OK;
@@ -594,6 +632,28 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
     SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, prec, reinterpret_cast<const cplx*>(x), beta,
                                reinterpret_cast<cplx*>(y), scratch));
     SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
+int64_t sieb200_launch_count(void) { return (int64_t)g_launches.load(); }
+
+int sieb200_profile_enable(sieb200_ctx* ctx, int enable) {
+    SIEB_CHECK(ctx, SIEB200_INVALID_ARG, "context must not be null");
+    ctx->prof.collect();
+    ctx->prof.enabled = enable != 0;
+    for (auto& k : ctx->prof.k) k = KernelProfile();
+    return SIEB200_OK;
+}
+
+int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,
+                         double* flops, double* bytes) {
+    SIEB_CHECK(ctx && kernel >= 0 && kernel < 3, SIEB200_INVALID_ARG, "invalid profile query");
+    ctx->prof.collect();
+    const KernelProfile& k = ctx->prof.k[kernel];
+    if (launches) *launches = k.launches;
+    if (total_ms) *total_ms = k.ms;
+    if (flops) *flops = k.flops;
+    if (bytes) *bytes = k.bytes;
     return SIEB200_OK;
 }
 

@@ -740,6 +740,7 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
     FaceGeom* geom = ctx->geom.as<FaceGeom>();
     d3* qp = ctx->qpts.as<d3>();
     face_prep_kernel<<<(nf + 127) / 128, 128, 0, st>>>(dV, dF, dFE, nf, dpts, Q, geom, qp);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
 
     // GSTC mass blocks.
@@ -753,6 +754,7 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
         dmass = ctx->mass.as<cplx>();
         mass_face_kernel<<<(nf * 8 + 127) / 128, 128, 0, st>>>(
             geom, qp, dw, Q, nf, ctx->tens.as<cplx>(), opt.tensors_are_uniform, ap.basis, dmass);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
     }
 
@@ -791,6 +793,7 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
         else
             pair_regular_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
 
         // Near-pair list of this slab: count, size, fill.
@@ -798,6 +801,7 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
         const int nb = (int)((span + 255) / 256);
         SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
         near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter, nullptr, 0);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         unsigned long long count = 0;
         SIEB_TRY_CUDA(cudaMemcpyAsync(&count, counter, sizeof(count), cudaMemcpyDeviceToHost, st));
@@ -807,6 +811,7 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
             SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
             near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter,
                                                   ctx->near_list.as<int2>(), count);
+            SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             const int threads = 128;
             const int blocks = (int)((count * 32 + threads - 1) / threads);
@@ -818,12 +823,14 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
                 pair_singular_kernel<2><<<blocks, threads, 0, st>>>(
                     geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[0],
                     ap.k[1], true, pairs);
+            SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
         }
         gp.m0 = m0;
         gp.m1 = m1;
         const dim3 gb(32, 8), gg((ne + 31) / 32, (ne + 7) / 8);
         gather_kernel<<<gg, gb, 0, st>>>(pairs, dmass, ctx->inc.as<int>(), gp, dZ, ldz);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
     }
     return SIEB200_OK;

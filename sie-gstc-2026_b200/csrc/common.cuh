@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/sieb200.h"
 
@@ -40,6 +41,10 @@ struct Status {
         int _s = (st);              \
         if (_s != SIEB200_OK) return _s; \
     } while (0)
+
+// Process-wide count of kernels this library has launched (host side).
+void note_launch();
+#define SIEB_NOTE_LAUNCH() ::sieb200::note_launch()
 
 // ------------------------------------------------------------------ math
 struct cplx {
@@ -84,8 +89,31 @@ struct DeviceBuffer {
 
 }  // namespace sieb200
 
+namespace sieb200 {
+// Event-pair profiler of selected kernels on the context stream.
+struct KernelProfile {
+    int64_t launches = 0;
+    double ms = 0.0, flops = 0.0, bytes = 0.0;
+};
+struct Profiler {
+    bool enabled = false;
+    struct Pending {
+        int kernel;
+        cudaEvent_t a, b;
+        double flops, bytes;
+    };
+    std::vector<Pending> pending;
+    KernelProfile k[3];
+    // Returns an event pair recorded around a launch (nullptr events when off).
+    void begin(cudaStream_t s, int kernel, double flops, double bytes, cudaEvent_t* end_out);
+    void end(cudaStream_t s, cudaEvent_t e);
+    void collect();  // synchronizes the recorded events and accumulates
+};
+}  // namespace sieb200
+
 struct sieb200_ctx {
     int device = 0;
+    sieb200::Profiler prof;
     cudaStream_t stream = nullptr;
     void* cusolver = nullptr;  // cusolverDnHandle_t, created on first use
     int sm_count = 0;

@@ -74,15 +74,21 @@ int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int pre
     chunks = (n + cpc - 1) / cpc;
     SIEB_RETURN_IF(scratch.reserve(sizeof(cplx) * n * chunks));
     const dim3 grid((unsigned)row_blocks, (unsigned)chunks);
+    cudaEvent_t ev;
+    ctx->prof.begin(ctx->stream, 2, 8.0 * (double)n * (double)n,
+                    (prec == 0 ? 16.0 : 8.0) * (double)n * (double)n + 16.0 * 3.0 * n, &ev);
     if (prec == 0)
         gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(
             n, static_cast<const double2*>(A), lda, x, cpc, scratch.as<cplx>());
     else
         gemv_partial_kernel<float2><<<grid, threads, 0, ctx->stream>>>(
             n, static_cast<const float2*>(A), lda, x, cpc, scratch.as<cplx>());
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     gemv_finish_kernel<<<(unsigned)row_blocks, threads, 0, ctx->stream>>>(n, (int)chunks,
                                                                           scratch.as<cplx>(), beta, y);
+    SIEB_NOTE_LAUNCH();
+    ctx->prof.end(ctx->stream, ev);
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }

@@ -322,6 +322,7 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
     if (g->mode == 0) {
         gemm_simt_sub_kernel<<<dim3((unsigned)((M2 + 63) / 64), (unsigned)((N + 63) / 64)), 256, 0, stream>>>(
             A, B, C, ldc, (int)M2, (int)N, K);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     }
@@ -336,6 +337,7 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
     SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
     const dim3 grid((unsigned)((M2 + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
     gemm_tf32_sub_kernel<<<grid, 128, SMEM_BYTES, stream>>>(ma, mb, C, ldc, (int)M2, (int)N, K, g->err);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }

@@ -666,10 +666,12 @@ int mixed_factorize(DenseSolver* s) {
     }
     SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
     rbt_init_kernel<<<blocks_for(8 * np, 256), 256, 0, stream>>>(st->diag, np, 0x5EB200ull);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     const int64_t q = np / 4;
     rbt_matrix_kernel<<<dim3(blocks_for(q, 128), (unsigned)q), 128, 0, stream>>>(
         reinterpret_cast<const cplx*>(s->A), s->lda, n, np, st->diag, st->diag + 4 * np, st->W, ldw);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
 
     for (int64_t bk = 0; bk < nbl; ++bk) {
@@ -678,22 +680,30 @@ int mixed_factorize(DenseSolver* s) {
         float2* Li = st->Linv + (size_t)bk * NB * NB;
         float2* Ui = st->Uinv + (size_t)bk * NB * NB;
         diag_lu_kernel<<<1, 256, kSmemDiag, stream>>>(st->W, ldw, k0, kb, Li, Ui, st->err);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         const int64_t s0 = k0 + kb;
         if (s0 >= np) break;
         const int64_t m = np - s0;
         panel_L_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Ui, st->Apack,
                                                              st->use_tc);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         panel_U_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Li, st->Bpack,
                                                              st->use_tc);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         if (st->use_tc) {
             float* C = reinterpret_cast<float*>(st->W + s0 + s0 * ldw);
+            cudaEvent_t ev;
+            ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * m * K3,
+                            4.0 * (2.0 * (2.0 * m) * m + (2.0 * m + m) * K3), &ev);
             SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, st->Apack, st->Bpack, 2 * m, m, K3));
+            ctx->prof.end(stream, ev);
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
+            SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
         }
     }
@@ -711,23 +721,31 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     const double* d_first = adjoint ? dv : du;
     const double* d_last = adjoint ? du : dv;
     rbt_vec_T_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(r, n, np, d_first, work);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     const long long spin = 1ll << 26;
     unsigned* fl = st->tri_flags;
     const int nbl = (int)st->nbl;
     if (!adjoint) {
-        SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
-        trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, 1, st->Linv, work, fl, st->err, spin);
-        SIEB_TRY_CUDA(cudaGetLastError());
-        SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
-        trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, 0, st->Uinv, work, fl, st->err, spin);
-        SIEB_TRY_CUDA(cudaGetLastError());
+        // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
+        const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
+        for (int lower = 1; lower >= 0; --lower) {
+            SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
+            cudaEvent_t ev;
+            s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
+            trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, lower, lower ? st->Linv : st->Uinv,
+                                                 work, fl, st->err, spin);
+            SIEB_NOTE_LAUNCH();
+            s->ctx->prof.end(stream, ev);
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
     } else {
         // W^H y = c  <=>  conj(W)^T y = c: solve with conj on both sides using
         // the transposed factors held in s->panel (built on first use).
         return SIEB200_INVALID_ARG;
     }
     rbt_vec_N_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(work, n, np, d_last, z);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }
@@ -777,7 +795,9 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         SIEB_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
         SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));  // r = A x - b
         dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, r, n, r, partial);
+        SIEB_NOTE_LAUNCH();
         dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
+        SIEB_NOTE_LAUNCH();
         cplx rr;
         SIEB_TRY_CUDA(cudaMemcpyAsync(&rr, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
         SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
@@ -794,6 +814,7 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         }
         // r holds A x - b: v1 = -r / beta
         scale_copy_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, r, -1.0 / beta, V);
+        SIEB_NOTE_LAUNCH();
         std::fill(g.begin(), g.end(), cx(0, 0));
         g[0] = cx(beta, 0);
         int j = 0;
@@ -806,8 +827,11 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
             for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
             for (int pass = 0; pass < 2; ++pass) {
                 dot_partial_kernel<<<dim3(parts, j + 1), 256, 0, stream>>>(n, j + 1, V, n, w, partial);
+                SIEB_NOTE_LAUNCH();
                 dot_finish_kernel<<<1, 64, 0, stream>>>(j + 1, parts, partial, h);
+                SIEB_NOTE_LAUNCH();
                 axpy_multi_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j + 1, V, n, h, w);
+                SIEB_NOTE_LAUNCH();
                 SIEB_TRY_CUDA(cudaGetLastError());
                 SIEB_TRY_CUDA(cudaMemcpyAsync(hh.data(), h, sizeof(cplx) * (j + 1), cudaMemcpyDeviceToHost,
                                               stream));
@@ -815,15 +839,19 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
                 for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = H[(size_t)i * m + j] + hh[i];
             }
             dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, w, n, w, partial);
+            SIEB_NOTE_LAUNCH();
             dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
+            SIEB_NOTE_LAUNCH();
             cplx ww;
             SIEB_TRY_CUDA(cudaMemcpyAsync(&ww, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
             SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
             const double hn = std::sqrt(std::max(ww.re, 0.0));
             cplx hj1 = cx(hn, 0);
-            if (j + 1 <= m)
+            if (j + 1 <= m) {
                 scale_copy_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, w, hn > 0 ? 1.0 / hn : 0.0,
                                                                            V + (int64_t)(j + 1) * n);
+                SIEB_NOTE_LAUNCH();
+            }
             // Givens on column j
             for (int i = 0; i < j; ++i) {
                 const cplx a = H[(size_t)i * m + j], bb = H[(size_t)(i + 1) * m + j];
@@ -864,8 +892,10 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         }
         SIEB_TRY_CUDA(cudaMemcpyAsync(h, y.data(), sizeof(cplx) * j, cudaMemcpyHostToDevice, stream));
         combo_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j, V, n, h, w);
+        SIEB_NOTE_LAUNCH();
         SIEB_RETURN_IF(apply_precond(s, w, z, work, false));
         add_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, z, x);
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         SIEB_RETURN_IF(check_err(s, "GMRES refinement"));
     }

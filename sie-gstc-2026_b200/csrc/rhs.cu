@@ -375,9 +375,11 @@ int assemble_rhs_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb20
     SIEB_TRY_CUDA(cudaMemset2DAsync(dB, sizeof(cplx) * ldb, 0, sizeof(cplx) * N, nsrc, st));
     rhs_face_kernel<<<dim3((nf + 127) / 128, nsrc), 128, 0, st>>>(dV, dF, nf, dq, dq + 160, Q, dsrc,
                                                                   nsrc, ctx->rhsbuf.as<cplx>());
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     rhs_gather_kernel<<<dim3((ne + 127) / 128, nsrc), 128, 0, st>>>(
         ctx->rhsbuf.as<cplx>(), dinc, nf, ne, dsrc, nsrc, N, dB, ldb);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }
@@ -413,6 +415,7 @@ int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j
         reinterpret_cast<int*>(b + oFE), nf, reinterpret_cast<cplx*>(b + oJ),
         m_cur ? reinterpret_cast<cplx*>(b + oM) : nullptr, reinterpret_cast<d3*>(b + oRq),
         reinterpret_cast<cplx*>(b + oCj), reinterpret_cast<cplx*>(b + oCm));
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     if (ndir > 0) {
         double* dd = reinterpret_cast<double*>(b + oDir);
@@ -421,6 +424,7 @@ int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j
             reinterpret_cast<cplx*>(b + oCm), M, k0, eta0, dd, dd + 3 * ndir, dd + 6 * ndir,
             reinterpret_cast<cplx*>(b + oOut), reinterpret_cast<cplx*>(b + oOut) + ndir,
             reinterpret_cast<double*>(b + oU));
+        SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         SIEB_TRY_CUDA(cudaMemcpyAsync(f_theta, b + oOut, sizeof(cplx) * ndir, cudaMemcpyDeviceToHost, st));
         SIEB_TRY_CUDA(cudaMemcpyAsync(f_phi, b + oOut + sizeof(cplx) * ndir, sizeof(cplx) * ndir, cudaMemcpyDeviceToHost, st));

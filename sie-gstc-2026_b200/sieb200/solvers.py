@@ -156,6 +156,18 @@ class Context:
     def synchronize(self) -> None:
         _lib.check(_lib.lib().sieb200_ctx_synchronize(self._h))
 
+    def profile(self, enable: bool = True) -> None:
+        """Start (and reset) or stop event timing of the library's hot kernels."""
+        _lib.check(_lib.lib().sieb200_profile_enable(self._h, int(bool(enable))))
+
+    def profile_read(self, kernel: int) -> dict:
+        """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec."""
+        n = ctypes.c_int64()
+        ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().sieb200_profile_read(self._h, int(kernel), ctypes.byref(n), ctypes.byref(ms),
+                                                   ctypes.byref(fl), ctypes.byref(by)))
+        return {"launches": n.value, "ms": ms.value, "flops": fl.value, "bytes": by.value}
+
     def close(self) -> None:
         if self._h:
             _lib.lib().sieb200_ctx_destroy(self._h)
