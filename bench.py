@@ -359,10 +359,14 @@ def run(args):
             "refinement_iterations": max(iters), "assembly_seconds": t_asm,
             "assembly_green_evals_per_s": evals / t_asm,
         }
-        print(json.dumps(out))
+        print(json.dumps(out), flush=True)
+    torch.cuda.synchronize()
     if world > 1:
         dist.destroy_process_group()
-    ctx.close()
+    # Leave without running destructors of tensors that were used on the
+    # library's stream after that stream is gone.
+    sys.stderr.flush()
+    os._exit(0)
 
 
 def main():
