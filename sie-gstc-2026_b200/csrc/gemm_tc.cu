@@ -194,27 +194,40 @@ gemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_const
 
     // Epilogue: all four warps. Lane 0 waits and broadcasts, so the warp stays
     // converged for the .sync.aligned TMEM loads.
+    const int row = m0 + warp * 32 + lane;
+    const bool row_ok = row < M2;
+    // Software-pipelined: the 32 C values of the next chunk are in flight
+    // while the current chunk is combined and stored; the first chunk is
+    // fetched before the accumulator is ready.
+    float cur[32], nxt[32];
+    auto load_chunk = [&](int chunk, float (&dst)[32]) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const int col = n0 + chunk * 32 + j;
+            dst[j] = (row_ok && col < N) ? __ldcs(C + (int64_t)col * ldc + row) : 0.f;
+        }
+    };
+    load_chunk(0, cur);
     int got = 0;
     if (lane == 0) got = mbar_wait(accb, 0, err) ? 1 : 0;
     got = __shfl_sync(0xffffffffu, got, 0);
     __syncwarp();
     if (got) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
         for (int chunk = 0; chunk < BN / 32; ++chunk) {
+            if (chunk + 1 < BN / 32) load_chunk(chunk + 1, nxt);
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + chunk * 32, v);
-            if (row < M2) {
+            if (row_ok) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int col = n0 + chunk * 32 + j;
-                    if (col < N) {
-                        float* p = C + (int64_t)col * ldc + row;
-                        *p = *p - v[j];
-                    }
+                    if (col < N) __stcs(C + (int64_t)col * ldc + row, cur[j] - v[j]);
                 }
             }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) cur[j] = nxt[j];
         }
     } else {
         ok = false;

@@ -222,58 +222,81 @@ __global__ void __launch_bounds__(256) diag_lu_kernel(float2* __restrict__ W, in
         A[c][r] = W[(k0 + r) + (k0 + c) * ldw];
     }
     __syncthreads();
+    // Elimination with one barrier per step: step j updates the trailing
+    // block from the unscaled column j times 1/pivot and scales column j-1
+    // (which nobody reads at step j).
+    float2 ip_prev = make_float2(0.f, 0.f);
     for (int j = 0; j < kb; ++j) {
         const float2 piv = A[j][j];
         const float pm = piv.x * piv.x + piv.y * piv.y;
-        if (!(pm > 1e-30f) || !isfinite(pm)) {
+        if (!(pm > 1e-30f) || !isfinite(pm)) {  // block-uniform decision
             if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
             return;
         }
         const float2 ip = crecipf(piv);
-        __syncthreads();
-        for (int r = j + 1 + tid; r < kb; r += blockDim.x) A[j][r] = cmulf(A[j][r], ip);
-        __syncthreads();
+        if (j > 0)
+            for (int r = j + tid; r < kb; r += blockDim.x) A[j - 1][r] = cmulf(A[j - 1][r], ip_prev);
         const int rows = kb - j - 1;
         for (int e = tid; e < rows * rows; e += blockDim.x) {
             const int r = j + 1 + e % rows, c = j + 1 + e / rows;
-            A[c][r] = csubf(A[c][r], cmulf(A[j][r], A[c][j]));
+            A[c][r] = csubf(A[c][r], cmulf(cmulf(A[j][r], ip), A[c][j]));
         }
+        ip_prev = ip;
         __syncthreads();
     }
+    // (the last column has no entries below the diagonal: nothing to scale)
     for (int e = tid; e < kb * kb; e += blockDim.x) {
         const int r = e % kb, c = e / kb;
         W[(k0 + r) + (k0 + c) * ldw] = A[c][r];
     }
-    // inv(L11): solve L X = I column by column (thread per column).
-    for (int c = tid; c < kb; c += blockDim.x) {
-        for (int r = 0; r < kb; ++r) {
-            float2 s = make_float2(r == c ? 1.f : 0.f, 0.f);
-            for (int k = c; k < r; ++k) s = csubf(s, cmulf(A[k][r], X[c][k]));
-            X[c][r] = r < c ? make_float2(0.f, 0.f) : s;
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int r = e % NB, c = e / NB;
-        Linv[r + c * NB] = (r < kb && c < kb) ? X[c][r] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    // inv(U11): solve U X = I (thread per column), backward.
-    for (int c = tid; c < kb; c += blockDim.x) {
-        for (int r = kb - 1; r >= 0; --r) {
-            float2 s = make_float2(r == c ? 1.f : 0.f, 0.f);
-            if (r <= c) {
-                for (int k = r + 1; k <= c; ++k) s = csubf(s, cmulf(A[k][r], X[c][k]));
-                X[c][r] = cmulf(s, crecipf(A[r][r]));
-            } else {
-                X[c][r] = make_float2(0.f, 0.f);
+    // Triangular inverses, rows in sequence, columns in parallel: thread
+    // (c, part) owns column c and a quarter of the inner sum; the four
+    // quarters are adjacent lanes and meet by shuffles.
+    const int c = tid >> 2, part = tid & 3;
+    // inv(L11): X(r, c) = delta(r, c) - sum_{c <= k < r} L(r, k) X(k, c).
+    for (int r = 0; r < kb; ++r) {
+        float sx = 0.f, sy = 0.f;
+        if (c < r)
+            for (int k = c + part; k < r; k += 4) {
+                const float2 l = A[k][r], x = X[c][k];
+                sx += l.x * x.x - l.y * x.y;
+                sy += l.x * x.y + l.y * x.x;
             }
-        }
+        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
+        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
+        sx += __shfl_xor_sync(0xffffffffu, sx, 2);
+        sy += __shfl_xor_sync(0xffffffffu, sy, 2);
+        if (part == 0 && c < kb)
+            X[c][r] = c < r ? make_float2(-sx, -sy) : make_float2(c == r ? 1.f : 0.f, 0.f);
+        __syncthreads();
+    }
+    for (int e = tid; e < NB * NB; e += blockDim.x) {
+        const int rr = e % NB, cc = e / NB;
+        Linv[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
     }
     __syncthreads();
+    // inv(U11): X(r, c) = (delta(r, c) - sum_{r < k <= c} U(r, k) X(k, c)) / U(r, r).
+    for (int r = kb - 1; r >= 0; --r) {
+        float sx = 0.f, sy = 0.f;
+        if (c > r && c < kb)
+            for (int k = r + 1 + part; k <= c; k += 4) {
+                const float2 u = A[k][r], x = X[c][k];
+                sx += u.x * x.x - u.y * x.y;
+                sy += u.x * x.y + u.y * x.x;
+            }
+        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
+        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
+        sx += __shfl_xor_sync(0xffffffffu, sx, 2);
+        sy += __shfl_xor_sync(0xffffffffu, sy, 2);
+        if (part == 0 && c < kb) {
+            const float2 rhs = make_float2((c == r ? 1.f : 0.f) - sx, -sy);
+            X[c][r] = c >= r ? cmulf(rhs, crecipf(A[r][r])) : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+    }
     for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int r = e % NB, c = e / NB;
-        Uinv[r + c * NB] = (r < kb && c < kb) ? X[c][r] : make_float2(0.f, 0.f);
+        const int rr = e % NB, cc = e / NB;
+        Uinv[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
     }
 }
 
@@ -303,41 +326,46 @@ __global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, in
     }
     __syncthreads();
     const int K3 = 6 * NB;
-    for (int e = tid; e < 32 * kb; e += blockDim.x) {
-        const int r = e % 32, c = e / 32;
-        const int64_t gr = rb + r;
-        if (gr >= np) continue;
+    // L21 rows into registers (thread: row r, columns c = cg + 8u)...
+    const int r = tid & 31, cg = tid >> 5;
+    float2 res[NB / 8];
+#pragma unroll
+    for (int u = 0; u < NB / 8; ++u) {
+        const int c = cg + 8 * u;
         float2 s = make_float2(0.f, 0.f);
-        for (int k = 0; k <= c; ++k) s = make_float2(s.x + Ar[r][k].x * Ui[c][k].x - Ar[r][k].y * Ui[c][k].y,
-                                                     s.y + Ar[r][k].x * Ui[c][k].y + Ar[r][k].y * Ui[c][k].x);
-        W[gr + (k0 + c) * ldw] = s;
-        if (pack) {
-            // realified row 2i: [Re, -Im], row 2i+1: [Im, Re]; split [hi | hi | lo]
-            const int64_t i = gr - r0;
-            float* row0 = Apack + (2 * i) * K3;
-            float* row1 = row0 + K3;
-            const float v00 = s.x, v01 = -s.y, v10 = s.y, v11 = s.x;
-            const float h00 = tf32_hi(v00), h01 = tf32_hi(v01), h10 = tf32_hi(v10), h11 = tf32_hi(v11);
-            row0[2 * c] = h00; row0[2 * c + 1] = h01;
-            row0[2 * NB + 2 * c] = h00; row0[2 * NB + 2 * c + 1] = h01;
-            row0[4 * NB + 2 * c] = v00 - h00; row0[4 * NB + 2 * c + 1] = v01 - h01;
-            row1[2 * c] = h10; row1[2 * c + 1] = h11;
-            row1[2 * NB + 2 * c] = h10; row1[2 * NB + 2 * c + 1] = h11;
-            row1[4 * NB + 2 * c] = v10 - h10; row1[4 * NB + 2 * c + 1] = v11 - h11;
-        }
+        if (c < kb)
+            for (int k = 0; k <= c; ++k)
+                s = make_float2(s.x + Ar[r][k].x * Ui[c][k].x - Ar[r][k].y * Ui[c][k].y,
+                                s.y + Ar[r][k].x * Ui[c][k].y + Ar[r][k].y * Ui[c][k].x);
+        res[u] = s;
     }
-    if (pack && kb < NB) {
-        // zero the unused K slots of these rows
-        for (int e = tid; e < 32 * (NB - kb); e += blockDim.x) {
-            const int r = e % 32, c = kb + e / 32;
-            const int64_t gr = rb + r;
-            if (gr >= np) continue;
-            const int64_t i = gr - r0;
-            for (int h = 0; h < 2; ++h) {
-                float* row = Apack + (2 * i + h) * K3;
-                for (int s = 0; s < 3; ++s) { row[s * 2 * NB + 2 * c] = 0.f; row[s * 2 * NB + 2 * c + 1] = 0.f; }
-            }
-        }
+    __syncthreads();
+    // ... back through shared memory (zero beyond kb) ...
+#pragma unroll
+    for (int u = 0; u < NB / 8; ++u) Ar[r][cg + 8 * u] = res[u];
+    __syncthreads();
+    // ... to W (rows fastest: coalesced columns) ...
+    for (int e = tid; e < 32 * kb; e += blockDim.x) {
+        const int rr = e % 32, c = e / 32;
+        const int64_t gr = rb + rr;
+        if (gr < np) W[gr + (k0 + c) * ldw] = Ar[rr][c];
+    }
+    if (!pack) return;
+    // ... and to the split realified rows (K fastest: coalesced rows).
+    // row 2i: [Re, -Im] per column, row 2i+1: [Im, Re]; layout [hi | hi | lo].
+    for (int e = tid; e < 32 * 2 * NB; e += blockDim.x) {
+        const int rr = e / (2 * NB), kk = e % (2 * NB);
+        const int64_t gr = rb + rr;
+        if (gr >= np) continue;
+        const int c = kk >> 1, h = kk & 1;
+        const float2 s = Ar[rr][c];
+        const float v0 = h == 0 ? s.x : -s.y;   // real row
+        const float v1 = h == 0 ? s.y : s.x;    // imaginary row
+        const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
+        float* row0 = Apack + (2 * (gr - r0)) * K3;
+        float* row1 = row0 + K3;
+        row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
+        row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
     }
 }
 
@@ -408,20 +436,35 @@ __global__ void __launch_bounds__(256) trailing_simt_kernel(float2* __restrict__
 }
 
 // ------------------------------------------------------------ triangular solves
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Blocked forward (lower = 1) or backward solve on the factors, one CTA per
-// block row, tickets in launch order, FP64 arithmetic. x has np entries; the
-// solve is in place in x. flags: nbl words (cleared by the host), ticket at
-// flags[nbl].
+// block row in solve order (tickets handed out in launch order), FP64
+// arithmetic on the complex64 factors; in place in x (np entries).
+// progress[0]: number of blocks completed in solve order (blocks finish in
+// order, so a single counter suffices); progress[1]: ticket counter. Both are
+// cleared by the host. A CTA waits only for blocks with smaller tickets,
+// whose CTAs are already running; every wait is bounded and reports through
+// err. While waiting, the next factor tile (and, from the start, the
+// diagonal inverse) are already in registers, so the critical path per block
+// is the x read, two 64-wide reductions and the release of the counter.
 __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
                                                    int nbl, int lower, const float2* __restrict__ Dinv,
-                                                   cplx* __restrict__ x, unsigned* __restrict__ flags,
+                                                   cplx* __restrict__ x, unsigned* __restrict__ progress,
                                                    unsigned* __restrict__ err, long long spin_limit) {
-    __shared__ int s_blk, s_abort;
+    __shared__ int s_blk, s_ready, s_abort;
     __shared__ double s_re[NB][4], s_im[NB][4];
     __shared__ cplx s_x[NB];
     const int tid = threadIdx.x;
     if (tid == 0) {
-        s_blk = (int)atomicAdd(&flags[nbl], 1u);
+        s_blk = (int)atomicAdd(&progress[1], 1u);
         s_abort = 0;
     }
     __syncthreads();
@@ -431,38 +474,65 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
     const int64_t r0 = (int64_t)bi * NB;
     const int rows = (int)(np - r0 < NB ? np - r0 : NB);
     const int r = tid & (NB - 1);   // row within block
-    const int part = tid >> 6;      // 4 partitions of the K dimension
-    double acc_re = 0.0, acc_im = 0.0;
-    for (int step = 0; step < t; ++step) {
+    const int part = tid >> 6;      // 4 partitions of the inner dimension
+    // Diagonal inverse of this block, row r, columns part, part+4, ...
+    const float2* D = Dinv + (size_t)bi * NB * NB;
+    float2 dreg[NB / 4];
+#pragma unroll
+    for (int u = 0; u < NB / 4; ++u) dreg[u] = D[r + (part + 4 * u) * NB];
+
+    auto load_w = [&](int step, float2 (&dst)[NB / 4]) {
         const int bj = lower ? step : nbl - 1 - step;
+        const int64_t c0 = (int64_t)bj * NB;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = part + 4 * u;
+            dst[u] = (r < rows && c0 + c < np) ? W[(r0 + r) + (c0 + c) * ldw] : make_float2(0.f, 0.f);
+        }
+    };
+    double acc_re = 0.0, acc_im = 0.0;
+    auto accumulate = [&](int step, const float2 (&w)[NB / 4]) {
+        const int bj = lower ? step : nbl - 1 - step;
+        const int64_t c0 = (int64_t)bj * NB;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = part + 4 * u;
+            if (c0 + c < np) {
+                // produced by another CTA: read through L2, never a stale L1 line
+                const double xr = __ldcg(&x[c0 + c].re), xi = __ldcg(&x[c0 + c].im);
+                acc_re += (double)w[u].x * xr - (double)w[u].y * xi;
+                acc_im += (double)w[u].x * xi + (double)w[u].y * xr;
+            }
+        }
+    };
+
+    float2 wpre[NB / 4], wtmp[NB / 4];
+    int done = 0;
+    while (done < t) {
+        load_w(done, wpre);  // in flight while the counter is awaited
         if (tid == 0) {
-            // Block bj was handed out before this one, so its CTA is running;
-            // the wait is still bounded and reports through err.
             long long it = 0;
-            while (atomicAdd(&flags[bj], 0u) == 0u) {
-                if (++it > spin_limit || atomicAdd(err, 0u) != 0u) {
+            unsigned p;
+            while ((p = ld_acquire_gpu(&progress[0])) <= (unsigned)done) {
+                if (++it > spin_limit || ((it & 255) == 0 && ld_acquire_gpu(err) != 0u)) {
                     atomicCAS(err, 0u, 2u);
                     s_abort = 1;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
-            __threadfence();
+            s_ready = (int)min(p, (unsigned)t);
         }
         __syncthreads();
         if (s_abort) return;
-        const int64_t c0 = (int64_t)bj * NB;
-        const int cols = (int)(np - c0 < NB ? np - c0 : NB);
-        if (r < rows) {
-            for (int c = part; c < cols; c += 4) {
-                const float2 a = W[(r0 + r) + (c0 + c) * ldw];
-                // produced by another CTA: read through L2, never a stale L1 line
-                const double xr = __ldcg(&x[c0 + c].re), xi = __ldcg(&x[c0 + c].im);
-                acc_re += (double)a.x * xr - (double)a.y * xi;
-                acc_im += (double)a.x * xi + (double)a.y * xr;
-            }
+        const int ready = s_ready;
+        accumulate(done, wpre);
+        for (int step = done + 1; step < ready; ++step) {
+            load_w(step, wtmp);
+            accumulate(step, wtmp);
         }
-        __syncthreads();
+        done = ready;
+        __syncthreads();  // s_ready is rewritten on the next pass
     }
     s_re[r][part] = acc_re;
     s_im[r][part] = acc_im;
@@ -471,24 +541,27 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
         const cplx b = tid < rows ? cx(__ldcg(&x[r0 + tid].re), __ldcg(&x[r0 + tid].im)) : cx(0, 0);
         const double sr = s_re[tid][0] + s_re[tid][1] + s_re[tid][2] + s_re[tid][3];
         const double si = s_im[tid][0] + s_im[tid][1] + s_im[tid][2] + s_im[tid][3];
-        s_x[tid] = cx(b.re - sr, b.im - si);
+        s_x[tid] = tid < rows ? cx(b.re - sr, b.im - si) : cx(0, 0);
     }
     __syncthreads();
-    // x_i = Dinv * s  (Dinv: NB x NB col-major, this block)
-    const float2* D = Dinv + (size_t)bi * NB * NB;
+    // x_i = Dinv * s  (Dinv: NB x NB column-major, this block)
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int u = 0; u < NB / 4; ++u) {
+        const int c = part + 4 * u;
+        re += (double)dreg[u].x * s_x[c].re - (double)dreg[u].y * s_x[c].im;
+        im += (double)dreg[u].x * s_x[c].im + (double)dreg[u].y * s_x[c].re;
+    }
+    s_re[r][part] = re;
+    s_im[r][part] = im;
+    __syncthreads();
     if (tid < rows) {
-        double re = 0.0, im = 0.0;
-        for (int c = 0; c < rows; ++c) {
-            const float2 a = D[tid + c * NB];
-            re += (double)a.x * s_x[c].re - (double)a.y * s_x[c].im;
-            im += (double)a.x * s_x[c].im + (double)a.y * s_x[c].re;
-        }
-        __stcg(&x[r0 + tid].re, re);
-        __stcg(&x[r0 + tid].im, im);
+        __stcg(&x[r0 + tid].re, s_re[tid][0] + s_re[tid][1] + s_re[tid][2] + s_re[tid][3]);
+        __stcg(&x[r0 + tid].im, s_im[tid][0] + s_im[tid][1] + s_im[tid][2] + s_im[tid][3]);
     }
     __threadfence();
     __syncthreads();
-    if (tid == 0) atomicExch(&flags[bi], 1u);
+    if (tid == 0) st_release_gpu(&progress[0], (unsigned)(t + 1));
 }
 
 // ------------------------------------------------------------ small vector ops
