@@ -37,7 +37,7 @@ namespace {
 constexpr int NB = 64;  // LU block size (complex columns)
 // Dynamic shared memory of the block kernels (two NB x (NB+1) complex64
 // tiles, or one plus a 32-row slab).
-constexpr int kSmemDiag = 2 * NB * (NB + 1) * (int)sizeof(float2);
+constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
 constexpr int kSmemPanel = (NB + 32) * (NB + 1) * (int)sizeof(float2);
 
 struct MixedState {
@@ -216,87 +216,116 @@ __global__ void __launch_bounds__(256) diag_lu_kernel(float2* __restrict__ W, in
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2(*A)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);             // [col][row]
     float2(*X)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;
+    float2* Tb = reinterpret_cast<float2*>(dyn_smem) + 2 * NB * (NB + 1);             // NB*NB/4
+    __shared__ float2 colbuf[2][NB], rowbuf[2][NB];
     const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int r = e % kb, c = e / kb;
-        A[c][r] = W[(k0 + r) + (k0 + c) * ldw];
+    // Elimination in registers: thread (r, g) owns row r, columns g + 4u. The
+    // block is padded to NB x NB with the identity (kb < NB only at the end).
+    const int r = tid & (NB - 1), g = tid >> 6;
+    float2 a[NB / 4];
+#pragma unroll
+    for (int u = 0; u < NB / 4; ++u) {
+        const int c = g + 4 * u;
+        a[u] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
     }
-    __syncthreads();
-    // Elimination with one barrier per step: step j updates the trailing
-    // block from the unscaled column j times 1/pivot and scales column j-1
-    // (which nobody reads at step j).
-    float2 ip_prev = make_float2(0.f, 0.f);
-    for (int j = 0; j < kb; ++j) {
-        const float2 piv = A[j][j];
+    // One barrier per step; the pivot column and row go through
+    // double-buffered shared slots.
+#pragma unroll 1
+    for (int j = 0; j < NB; ++j) {
+        const int buf = j & 1;
+        if (g == (j & 3)) {
+#pragma unroll
+            for (int u = 0; u < NB / 4; ++u)  // static indices keep a[] in registers
+                if (u == (j >> 2)) colbuf[buf][r] = a[u];
+        }
+        if (r == j) {
+#pragma unroll
+            for (int u = 0; u < NB / 4; ++u) rowbuf[buf][g + 4 * u] = a[u];
+        }
+        __syncthreads();
+        const float2 piv = rowbuf[buf][j];
         const float pm = piv.x * piv.x + piv.y * piv.y;
         if (!(pm > 1e-30f) || !isfinite(pm)) {  // block-uniform decision
             if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
             return;
         }
-        const float2 ip = crecipf(piv);
-        if (j > 0)
-            for (int r = j + tid; r < kb; r += blockDim.x) A[j - 1][r] = cmulf(A[j - 1][r], ip_prev);
-        const int rows = kb - j - 1;
-        for (int e = tid; e < rows * rows; e += blockDim.x) {
-            const int r = j + 1 + e % rows, c = j + 1 + e / rows;
-            A[c][r] = csubf(A[c][r], cmulf(cmulf(A[j][r], ip), A[c][j]));
-        }
-        ip_prev = ip;
-        __syncthreads();
-    }
-    // (the last column has no entries below the diagonal: nothing to scale)
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int r = e % kb, c = e / kb;
-        W[(k0 + r) + (k0 + c) * ldw] = A[c][r];
-    }
-    // Triangular inverses, rows in sequence, columns in parallel: thread
-    // (c, part) owns column c and a quarter of the inner sum; the four
-    // quarters are adjacent lanes and meet by shuffles.
-    const int c = tid >> 2, part = tid & 3;
-    // inv(L11): X(r, c) = delta(r, c) - sum_{c <= k < r} L(r, k) X(k, c).
-    for (int r = 0; r < kb; ++r) {
-        float sx = 0.f, sy = 0.f;
-        if (c < r)
-            for (int k = c + part; k < r; k += 4) {
-                const float2 l = A[k][r], x = X[c][k];
-                sx += l.x * x.x - l.y * x.y;
-                sy += l.x * x.y + l.y * x.x;
+        if (r > j) {
+            const float2 l = cmulf(colbuf[buf][r], crecipf(piv));
+#pragma unroll
+            for (int u = 0; u < NB / 4; ++u) {
+                const int c = g + 4 * u;
+                if (c > j) a[u] = csubf(a[u], cmulf(l, rowbuf[buf][c]));
+                else if (c == j) a[u] = l;
             }
-        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
-        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
-        sx += __shfl_xor_sync(0xffffffffu, sx, 2);
-        sy += __shfl_xor_sync(0xffffffffu, sy, 2);
-        if (part == 0 && c < kb)
-            X[c][r] = c < r ? make_float2(-sx, -sy) : make_float2(c == r ? 1.f : 0.f, 0.f);
-        __syncthreads();
+        }
     }
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int rr = e % NB, cc = e / NB;
-        Linv[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < NB / 4; ++u) {
+        const int c = g + 4 * u;
+        A[c][r] = a[u];
+        if (r < kb && c < kb) W[(k0 + r) + (k0 + c) * ldw] = a[u];
     }
     __syncthreads();
-    // inv(U11): X(r, c) = (delta(r, c) - sum_{r < k <= c} U(r, k) X(k, c)) / U(r, r).
-    for (int r = kb - 1; r >= 0; --r) {
-        float sx = 0.f, sy = 0.f;
-        if (c > r && c < kb)
-            for (int k = r + 1 + part; k <= c; k += 4) {
-                const float2 u = A[k][r], x = X[c][k];
-                sx += u.x * x.x - u.y * x.y;
-                sy += u.x * x.y + u.y * x.x;
-            }
-        sx += __shfl_xor_sync(0xffffffffu, sx, 1);
-        sy += __shfl_xor_sync(0xffffffffu, sy, 1);
-        sx += __shfl_xor_sync(0xffffffffu, sx, 2);
-        sy += __shfl_xor_sync(0xffffffffu, sy, 2);
-        if (part == 0 && c < kb) {
-            const float2 rhs = make_float2((c == r ? 1.f : 0.f) - sx, -sy);
-            X[c][r] = c >= r ? cmulf(rhs, crecipf(A[r][r])) : make_float2(0.f, 0.f);
+    // Triangular inverses by recursive doubling: at level s the inverses of
+    // the s x s diagonal blocks are known, and each 2s block completes with
+    //   lower: X21 = -X22 (L21 X11),   upper: X12 = -X11 (U12 X22),
+    // two parallel s x s products and two barriers per level.
+    for (int lower = 1; lower >= 0; --lower) {
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+            const int rr = e & (NB - 1), cc = e >> 6;
+            X[cc][rr] = rr != cc ? make_float2(0.f, 0.f)
+                                 : (lower ? make_float2(1.f, 0.f) : crecipf(A[rr][rr]));
         }
         __syncthreads();
-    }
-    for (int e = tid; e < NB * NB; e += blockDim.x) {
-        const int rr = e % NB, cc = e / NB;
-        Uinv[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
+        for (int l = 0; (1 << l) < NB; ++l) {
+            const int s = 1 << l, work = (NB / 2) << l;  // (NB / 2s) blocks of s*s
+            for (int e = tid; e < work; e += blockDim.x) {
+                const int b = e >> (2 * l), rem = e & ((1 << (2 * l)) - 1);
+                const int i = rem & (s - 1), j = rem >> l, base = b * 2 * s;
+                float2 acc = make_float2(0.f, 0.f);
+                if (lower) {  // T = L21 X11, X11 lower: k >= j
+                    for (int k = j; k < s; ++k)
+                        acc = make_float2(acc.x + A[base + k][base + s + i].x * X[base + j][base + k].x -
+                                                  A[base + k][base + s + i].y * X[base + j][base + k].y,
+                                          acc.y + A[base + k][base + s + i].x * X[base + j][base + k].y +
+                                                  A[base + k][base + s + i].y * X[base + j][base + k].x);
+                } else {      // T = U12 X22, X22 upper: k <= j
+                    for (int k = 0; k <= j; ++k)
+                        acc = make_float2(acc.x + A[base + s + k][base + i].x * X[base + s + j][base + s + k].x -
+                                                  A[base + s + k][base + i].y * X[base + s + j][base + s + k].y,
+                                          acc.y + A[base + s + k][base + i].x * X[base + s + j][base + s + k].y +
+                                                  A[base + s + k][base + i].y * X[base + s + j][base + s + k].x);
+                }
+                Tb[e] = acc;
+            }
+            __syncthreads();
+            for (int e = tid; e < work; e += blockDim.x) {
+                const int b = e >> (2 * l), rem = e & ((1 << (2 * l)) - 1);
+                const int i = rem & (s - 1), j = rem >> l, base = b * 2 * s;
+                const float2* T = Tb + (b << (2 * l));
+                float2 acc = make_float2(0.f, 0.f);
+                if (lower) {  // X21 = -X22 T, X22 lower: k <= i
+                    for (int k = 0; k <= i; ++k) {
+                        const float2 x = X[base + s + k][base + s + i], t = T[k + (j << l)];
+                        acc = make_float2(acc.x + x.x * t.x - x.y * t.y, acc.y + x.x * t.y + x.y * t.x);
+                    }
+                    X[base + j][base + s + i] = make_float2(-acc.x, -acc.y);
+                } else {      // X12 = -X11 T, X11 upper: k >= i
+                    for (int k = i; k < s; ++k) {
+                        const float2 x = X[base + k][base + i], t = T[k + (j << l)];
+                        acc = make_float2(acc.x + x.x * t.x - x.y * t.y, acc.y + x.x * t.y + x.y * t.x);
+                    }
+                    X[base + s + j][base + i] = make_float2(-acc.x, -acc.y);
+                }
+            }
+            __syncthreads();
+        }
+        float2* out = lower ? Linv : Uinv;
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+            const int rr = e & (NB - 1), cc = e >> 6;
+            out[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
     }
 }
 
@@ -459,10 +488,10 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
                                                    int nbl, int lower, const float2* __restrict__ Dinv,
                                                    cplx* __restrict__ x, unsigned* __restrict__ progress,
                                                    unsigned* __restrict__ err, long long spin_limit) {
-    __shared__ int s_blk, s_ready, s_abort;
-    __shared__ double s_re[NB][4], s_im[NB][4];
-    __shared__ cplx s_x[NB];
-    const int tid = threadIdx.x;
+    __shared__ int s_blk;
+    __shared__ volatile int s_abort;
+    __shared__ cplx s_y[NB];
+    const int tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) {
         s_blk = (int)atomicAdd(&progress[1], 1u);
         s_abort = 0;
@@ -473,9 +502,9 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
     const int bi = lower ? t : nbl - 1 - t;
     const int64_t r0 = (int64_t)bi * NB;
     const int rows = (int)(np - r0 < NB ? np - r0 : NB);
-    const int r = tid & (NB - 1);   // row within block
-    const int part = tid >> 6;      // 4 partitions of the inner dimension
-    // Diagonal inverse of this block, row r, columns part, part+4, ...
+    // Thread (r, part): row r of the block, inner columns part + 4u. A warp
+    // holds 8 whole rows, so every reduction is a pair of shuffles.
+    const int r = tid >> 2, part = tid & 3;
     const float2* D = Dinv + (size_t)bi * NB * NB;
     float2 dreg[NB / 4];
 #pragma unroll
@@ -506,60 +535,67 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
         }
     };
 
+    // Each warp follows the counter on its own (lane 0 polls, the warp reads
+    // the answer by shuffle): no CTA barrier between arrivals.
     float2 wpre[NB / 4], wtmp[NB / 4];
     int done = 0;
-    while (done < t) {
+    bool aborted = false;
+    while (done < t && !aborted) {
         load_w(done, wpre);  // in flight while the counter is awaited
-        if (tid == 0) {
+        int ready = 0;
+        if (lane == 0) {
             long long it = 0;
             unsigned p;
             while ((p = ld_acquire_gpu(&progress[0])) <= (unsigned)done) {
-                if (++it > spin_limit || ((it & 255) == 0 && ld_acquire_gpu(err) != 0u)) {
+                if (s_abort || ++it > spin_limit || ((it & 255) == 0 && ld_acquire_gpu(err) != 0u)) {
                     atomicCAS(err, 0u, 2u);
                     s_abort = 1;
+                    p = 0;
                     break;
                 }
                 __nanosleep(32);
             }
-            s_ready = (int)min(p, (unsigned)t);
+            ready = p == 0 ? -1 : (int)min(p, (unsigned)t);
         }
-        __syncthreads();
-        if (s_abort) return;
-        const int ready = s_ready;
+        ready = __shfl_sync(0xffffffffu, ready, 0);
+        if (ready < 0) {
+            aborted = true;
+            break;
+        }
         accumulate(done, wpre);
         for (int step = done + 1; step < ready; ++step) {
             load_w(step, wtmp);
             accumulate(step, wtmp);
         }
         done = ready;
-        __syncthreads();  // s_ready is rewritten on the next pass
     }
-    s_re[r][part] = acc_re;
-    s_im[r][part] = acc_im;
-    __syncthreads();
-    if (tid < NB) {
-        const cplx b = tid < rows ? cx(__ldcg(&x[r0 + tid].re), __ldcg(&x[r0 + tid].im)) : cx(0, 0);
-        const double sr = s_re[tid][0] + s_re[tid][1] + s_re[tid][2] + s_re[tid][3];
-        const double si = s_im[tid][0] + s_im[tid][1] + s_im[tid][2] + s_im[tid][3];
-        s_x[tid] = tid < rows ? cx(b.re - sr, b.im - si) : cx(0, 0);
+    acc_re += __shfl_xor_sync(0xffffffffu, acc_re, 1);
+    acc_im += __shfl_xor_sync(0xffffffffu, acc_im, 1);
+    acc_re += __shfl_xor_sync(0xffffffffu, acc_re, 2);
+    acc_im += __shfl_xor_sync(0xffffffffu, acc_im, 2);
+    if (part == 0) {
+        const cplx b = r < rows ? cx(__ldcg(&x[r0 + r].re), __ldcg(&x[r0 + r].im)) : cx(0, 0);
+        s_y[r] = r < rows ? cx(b.re - acc_re, b.im - acc_im) : cx(0, 0);
     }
     __syncthreads();
-    // x_i = Dinv * s  (Dinv: NB x NB column-major, this block)
+    if (s_abort) return;  // block-uniform
+    // x_i = Dinv * y  (Dinv: NB x NB column-major, this block)
     double re = 0.0, im = 0.0;
 #pragma unroll
     for (int u = 0; u < NB / 4; ++u) {
-        const int c = part + 4 * u;
-        re += (double)dreg[u].x * s_x[c].re - (double)dreg[u].y * s_x[c].im;
-        im += (double)dreg[u].x * s_x[c].im + (double)dreg[u].y * s_x[c].re;
+        const cplx yv = s_y[part + 4 * u];
+        re += (double)dreg[u].x * yv.re - (double)dreg[u].y * yv.im;
+        im += (double)dreg[u].x * yv.im + (double)dreg[u].y * yv.re;
     }
-    s_re[r][part] = re;
-    s_im[r][part] = im;
-    __syncthreads();
-    if (tid < rows) {
-        __stcg(&x[r0 + tid].re, s_re[tid][0] + s_re[tid][1] + s_re[tid][2] + s_re[tid][3]);
-        __stcg(&x[r0 + tid].im, s_im[tid][0] + s_im[tid][1] + s_im[tid][2] + s_im[tid][3]);
+    re += __shfl_xor_sync(0xffffffffu, re, 1);
+    im += __shfl_xor_sync(0xffffffffu, im, 1);
+    re += __shfl_xor_sync(0xffffffffu, re, 2);
+    im += __shfl_xor_sync(0xffffffffu, im, 2);
+    if (part == 0 && r < rows) {
+        __stcg(&x[r0 + r].re, re);
+        __stcg(&x[r0 + r].im, im);
+        __threadfence();  // each writer publishes its own stores at gpu scope
     }
-    __threadfence();
     __syncthreads();
     if (tid == 0) st_release_gpu(&progress[0], (unsigned)(t + 1));
 }
@@ -829,8 +865,10 @@ static double host_norm2(const std::vector<cplx>& v) {
     return std::sqrt((double)s);
 }
 
-// Restarted right-preconditioned GMRES on A x = b (FP64, A the intact
-// complex128 matrix), started from x = M^{-1} b.
+// Restarted flexible GMRES on A x = b (FP64, A the intact complex128 matrix)
+// with right preconditioner M^{-1}, started from x = 0. The preconditioned
+// directions z_j = M^{-1} v_j are kept, so the update x += Z y costs no
+// further preconditioner application.
 static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int maxit, int* iters) {
     (void)ldb_unused;
     MixedState* st = state_of(s);
@@ -839,16 +877,17 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     const int64_t n = st->n, np = st->np;
     const int m = 20;  // restart length
     const int parts = 64;
-    // vectors: x, r, w, z, work(np), V (n x (m+1)), partial, h
-    const size_t vbytes = sizeof(cplx) * (5 * np + (int64_t)(m + 1) * n + parts * (m + 1) + (m + 2));
+    // vectors: x, r, w, work(np), V (n x (m+1)), Z (n x m), partial, h
+    const size_t vbytes =
+        sizeof(cplx) * (4 * np + (int64_t)(m + 1) * n + (int64_t)m * n + parts * (m + 1) + (m + 2));
     SIEB_RETURN_IF(s->krylov.reserve(vbytes));
     cplx* x = s->krylov.as<cplx>();
     cplx* r = x + np;
     cplx* w = r + np;
-    cplx* z = w + np;
-    cplx* work = z + np;
+    cplx* work = w + np;
     cplx* V = work + np;
-    cplx* partial = V + (int64_t)(m + 1) * n;
+    cplx* Zb = V + (int64_t)(m + 1) * n;
+    cplx* partial = Zb + (int64_t)m * n;
     cplx* h = partial + parts * (m + 1);
     const double* A = s->A;
     const int64_t lda = s->lda;
@@ -860,13 +899,18 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     const double bnorm = host_norm2(hb);
     SIEB_CHECK(bnorm > 0 && std::isfinite(bnorm), SIEB200_INVALID_ARG, "right-hand side norm must be finite and nonzero");
 
-    SIEB_RETURN_IF(apply_precond(s, b, x, work, false));
+    SIEB_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(cplx) * n, stream));
     int total = 0;
     std::vector<cplx> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), hh(m + 2);
     for (int outer = 0; outer < 1000; ++outer) {
-        // r = b - A x
-        SIEB_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
-        SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));  // r = A x - b
+        // r = A x - b (for x = 0 simply -b)
+        if (outer == 0) {
+            scale_copy_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, b, -1.0, r);
+            SIEB_NOTE_LAUNCH();
+        } else {
+            SIEB_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
+            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));
+        }
         dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, r, n, r, partial);
         SIEB_NOTE_LAUNCH();
         dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
@@ -894,8 +938,9 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         double est = beta;
         for (; j < m && total < maxit; ++j, ++total) {
             cplx* vj = V + (int64_t)j * n;
-            SIEB_RETURN_IF(apply_precond(s, vj, z, work, false));
-            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, z, 0.0, w, s->gemv_scratch));
+            cplx* zj = Zb + (int64_t)j * n;
+            SIEB_RETURN_IF(apply_precond(s, vj, zj, work, false));
+            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
             // Classical Gram-Schmidt with one reorthogonalization (CGS2).
             for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
             for (int pass = 0; pass < 2; ++pass) {
@@ -964,10 +1009,9 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
             y[i] = cx((sacc.re * d.re + sacc.im * d.im) / dd, (sacc.im * d.re - sacc.re * d.im) / dd);
         }
         SIEB_TRY_CUDA(cudaMemcpyAsync(h, y.data(), sizeof(cplx) * j, cudaMemcpyHostToDevice, stream));
-        combo_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j, V, n, h, w);
+        combo_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j, Zb, n, h, w);
         SIEB_NOTE_LAUNCH();
-        SIEB_RETURN_IF(apply_precond(s, w, z, work, false));
-        add_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, z, x);
+        add_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, w, x);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         SIEB_RETURN_IF(check_err(s, "GMRES refinement"));
