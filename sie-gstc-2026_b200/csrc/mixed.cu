@@ -203,8 +203,8 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 crecipf(float2 a) {
-    const float d = a.x * a.x + a.y * a.y;
-    return make_float2(a.x / d, -a.y / d);
+    const float inv = __frcp_rn(a.x * a.x + a.y * a.y);
+    return make_float2(a.x * inv, -a.y * inv);
 }
 
 // Factor the kb x kb diagonal block in place without pivoting (one CTA,
@@ -338,16 +338,15 @@ __device__ __forceinline__ float tf32_hi(float x) {
 // L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
 // writes L21 back into W and the split realified rows into Apack.
 // One CTA per 32 rows; inv(U11) staged in shared memory.
-__global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0,
-                                                      int kb, int64_t r0, int64_t np,
-                                                      const float2* __restrict__ Uinv,
-                                                      float* __restrict__ Apack, int pack) {
+__device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                             int64_t r0, int64_t np, const float2* __restrict__ Uinv,
+                                             float* __restrict__ Apack, int pack, int bx) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2(*Ui)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
     float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [row][col], 32 rows
     const int tid = threadIdx.x;
     for (int e = tid; e < NB * NB; e += blockDim.x) Ui[e / NB][e % NB] = Uinv[e];
-    const int64_t rb = r0 + (int64_t)blockIdx.x * 32;
+    const int64_t rb = r0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * kb; e += blockDim.x) {
         const int r = e % 32, c = e / 32;
         const int64_t gr = rb + r;
@@ -400,16 +399,15 @@ __global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, in
 
 // U12 = inv(L11) * A12 for columns [c0, np) of the panel rows [k0, k0+kb);
 // writes U12 back into W and the split columns into Bpack. One CTA per 32 cols.
-__global__ void __launch_bounds__(256) panel_U_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0,
-                                                      int kb, int64_t c0, int64_t np,
-                                                      const float2* __restrict__ Linv,
-                                                      float* __restrict__ Bpack, int pack) {
+__device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                             int64_t c0, int64_t np, const float2* __restrict__ Linv,
+                                             float* __restrict__ Bpack, int pack, int bx) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2(*Li)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
     float2(*Ac)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [col][row], 32 cols
     const int tid = threadIdx.x;
     for (int e = tid; e < NB * NB; e += blockDim.x) Li[e / NB][e % NB] = Linv[e];
-    const int64_t cb = c0 + (int64_t)blockIdx.x * 32;
+    const int64_t cb = c0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * kb; e += blockDim.x) {
         const int r = e % kb, c = e / kb;
         const int64_t gc = cb + c;
@@ -434,6 +432,18 @@ __global__ void __launch_bounds__(256) panel_U_kernel(float2* __restrict__ W, in
             col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
         }
     }
+}
+
+// Both panels of one block step in one launch: CTAs [0, nL) form L21 rows,
+// the rest U12 columns (disjoint regions of W).
+__global__ void __launch_bounds__(256) panel_LU_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                       int64_t s0, int64_t np, const float2* __restrict__ Linv,
+                                                       const float2* __restrict__ Uinv, float* __restrict__ Apack,
+                                                       float* __restrict__ Bpack, int pack, int nL) {
+    if ((int)blockIdx.x < nL)
+        panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x);
+    else
+        panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x - nL);
 }
 
 // SIMT trailing update C -= L21 U12 in complex64 (checking path).
@@ -535,31 +545,34 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
         }
     };
 
-    // Each warp follows the counter on its own (lane 0 polls, the warp reads
-    // the answer by shuffle): no CTA barrier between arrivals.
+    // One poller per CTA. The counter is read with acquire semantics and the
+    // answer handed to the CTA through a barrier; a CTA far behind the
+    // frontier backs off in proportion to its distance, so the next block in
+    // line is the only fast poller on the counter's cache line.
     float2 wpre[NB / 4], wtmp[NB / 4];
     int done = 0;
-    bool aborted = false;
-    while (done < t && !aborted) {
+    while (done < t) {
         load_w(done, wpre);  // in flight while the counter is awaited
-        int ready = 0;
-        if (lane == 0) {
+        if (tid == 0) {
             long long it = 0;
             unsigned p;
+            int ready = -1;
             while ((p = ld_acquire_gpu(&progress[0])) <= (unsigned)done) {
-                if (s_abort || ++it > spin_limit || ((it & 255) == 0 && ld_acquire_gpu(err) != 0u)) {
+                if (++it > spin_limit || ((it & 63) == 0 && ld_acquire_gpu(err) != 0u)) {
                     atomicCAS(err, 0u, 2u);
-                    s_abort = 1;
                     p = 0;
                     break;
                 }
-                __nanosleep(32);
+                const unsigned gap = (unsigned)t - p;  // blocks still ahead of this one
+                __nanosleep(gap <= 1 ? 20 : (gap < 64 ? 200 * gap : 12800));
             }
-            ready = p == 0 ? -1 : (int)min(p, (unsigned)t);
+            if (p != 0) ready = (int)min(p, (unsigned)t);
+            s_blk = ready;  // reused as the broadcast slot
         }
-        ready = __shfl_sync(0xffffffffu, ready, 0);
+        __syncthreads();
+        const int ready = s_blk;
         if (ready < 0) {
-            aborted = true;
+            s_abort = 1;
             break;
         }
         accumulate(done, wpre);
@@ -568,6 +581,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
             accumulate(step, wtmp);
         }
         done = ready;
+        __syncthreads();  // the broadcast slot is rewritten on the next pass
     }
     acc_re += __shfl_xor_sync(0xffffffffu, acc_re, 1);
     acc_im += __shfl_xor_sync(0xffffffffu, acc_im, 1);
@@ -594,8 +608,9 @@ __global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W,
     if (part == 0 && r < rows) {
         __stcg(&x[r0 + r].re, re);
         __stcg(&x[r0 + r].im, im);
-        __threadfence();  // each writer publishes its own stores at gpu scope
     }
+    // Barrier, then one gpu-scope release by thread 0: the writes of the
+    // whole CTA happen before the release through the barrier.
     __syncthreads();
     if (tid == 0) st_release_gpu(&progress[0], (unsigned)(t + 1));
 }
@@ -769,8 +784,7 @@ int mixed_factorize(DenseSolver* s) {
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_L_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_LU_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
         attrs_set = true;
     }
     SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
@@ -794,12 +808,9 @@ int mixed_factorize(DenseSolver* s) {
         const int64_t s0 = k0 + kb;
         if (s0 >= np) break;
         const int64_t m = np - s0;
-        panel_L_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Ui, st->Apack,
-                                                             st->use_tc);
-        SIEB_NOTE_LAUNCH();
-        SIEB_TRY_CUDA(cudaGetLastError());
-        panel_U_kernel<<<blocks_for(m, 32), 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Li, st->Bpack,
-                                                             st->use_tc);
+        const int nL = (int)blocks_for(m, 32);
+        panel_LU_kernel<<<2 * nL, 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Li, Ui, st->Apack,
+                                                              st->Bpack, st->use_tc, nL);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         if (st->use_tc) {
