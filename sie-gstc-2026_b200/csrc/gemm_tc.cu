@@ -27,6 +27,7 @@
 
 #include "common.cuh"
 #include "gemm_tc.cuh"
+#include "sm100.cuh"
 
 namespace sieb200 {
 
@@ -37,30 +38,6 @@ constexpr int STAGES = 3;
 constexpr int STAGE_A = BM * BK * 4, STAGE_B = BN * BK * 4;
 constexpr int SMEM_BYTES = STAGES * (STAGE_A + STAGE_B) + 1024 /*align*/ + 256 /*barriers*/;
 constexpr long long kSpinLimit = 1ll << 26;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
 // Bounded wait: false on timeout (and sets the error word).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned* err) {
@@ -73,13 +50,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigne
         if ((it & 1023) == 0 && *reinterpret_cast<volatile unsigned*>(err) != 0u) return false;
     }
     return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
-        : "memory");
 }
 
 // K-major, 128-byte swizzle shared-memory matrix descriptor (sm_100 layout:
@@ -270,32 +240,36 @@ __global__ void gemm_simt_sub_kernel(const float* __restrict__ A, const float* _
         }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-
-int get_encoder() {
-    if (g_encode) return SIEB200_OK;
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    SIEB_TRY_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-    SIEB_CHECK(fn && q == cudaDriverEntryPointSuccess, SIEB200_CUDA_ERROR,
-               "cuTensorMapEncodeTiled is not available from the driver");
-    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    return SIEB200_OK;
-}
-
 int make_map(CUtensorMap* map, const float* ptr, int64_t inner, int64_t outer, int box_outer) {
-    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
-    const cuuint64_t strides[1] = {(cuuint64_t)(inner * sizeof(float))};
-    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_outer};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), dims, strides, box,
-                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    SIEB_CHECK(r == CUDA_SUCCESS, SIEB200_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
-    return SIEB200_OK;
+    return encode_tensor_map_2d(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, ptr, (uint64_t)inner, (uint64_t)outer,
+                                (uint64_t)inner * sizeof(float), BK, (uint32_t)box_outer, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 }  // namespace
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType type, const void* base, uint64_t inner,
+                         uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner, uint32_t box_outer,
+                         CUtensorMapSwizzle swizzle) {
+    if (!g_encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SIEB_TRY_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        SIEB_CHECK(fn && q == cudaDriverEntryPointSuccess, SIEB200_CUDA_ERROR,
+                   "cuTensorMapEncodeTiled is not available from the driver");
+        g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)row_stride_bytes};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = g_encode(map, type, 2, const_cast<void*>(base), dims, strides, box, estr,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SIEB_CHECK(r == CUDA_SUCCESS, SIEB200_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return SIEB200_OK;
+}
 
 struct GemmTC {
     unsigned* err = nullptr;
@@ -339,7 +313,6 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     }
-    SIEB_RETURN_IF(get_encoder());
     if (!g->attr_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            SMEM_BYTES));

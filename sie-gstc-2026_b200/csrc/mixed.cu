@@ -29,6 +29,7 @@
 
 #include "dense.cuh"
 #include "gemm_tc.cuh"
+#include "sm100.cuh"
 
 namespace sieb200 {
 
@@ -39,13 +40,15 @@ constexpr int NB = 64;  // LU block size (complex columns)
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
 constexpr int kSmemPanel = (NB + 32) * (NB + 1) * (int)sizeof(float2);
+constexpr int kDiagThreads = 1024;  // diagonal-block kernel: 16 column groups of NB rows
+static_assert(kDiagThreads % NB == 0 && NB % (kDiagThreads / NB) == 0, "diag thread layout");
 
 struct MixedState {
     int64_t n = 0, np = 0, ldw = 0, nbl = 0;
     float2* W = nullptr;        // factors, np x np, ld = ldw
     float2* Linv = nullptr;     // inverse unit-lower diagonal blocks, NB x NB each (col-major)
     float2* Uinv = nullptr;     // inverse upper diagonal blocks
-    float* Apack = nullptr;     // split realified L21: (2*np) x (6*NB), K-major
+    float* Apack[2] = {nullptr, nullptr};  // split realified L21: (2*np) x (6*NB), K-major; by step parity
     float* Bpack = nullptr;     // split U12 columns: np x (6*NB), K-major
     float2* panel = nullptr;    // NB x np scratch for U12 / np x NB for L21
     double* diag = nullptr;     // butterfly diagonals: U (level1 a,b; level2 e,f) and V, 4*np each
@@ -54,6 +57,11 @@ struct MixedState {
     cplx* vecs = nullptr;       // FP64 work vectors
     int use_tc = 1;
     GemmTC* gemm = nullptr;
+    CUtensorMap tmW;                       // W for the triangular solves' tile loads
+    const void* tm_base = nullptr;
+    int64_t tm_np = 0;
+    cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
+    cudaEvent_t ev_cols = nullptr, ev_panel = nullptr;
 };
 
 // ------------------------------------------------------------ butterflies
@@ -209,59 +217,64 @@ __device__ __forceinline__ float2 crecipf(float2 a) {
 
 // Factor the kb x kb diagonal block in place without pivoting (one CTA,
 // block in shared memory), then form inv(L11) (unit lower) and inv(U11).
-__global__ void __launch_bounds__(256) diag_lu_kernel(float2* __restrict__ W, int64_t ldw,
-                                                      int64_t k0, int kb, float2* __restrict__ Linv,
-                                                      float2* __restrict__ Uinv,
-                                                      unsigned* __restrict__ err) {
+__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(float2* __restrict__ W, int64_t ldw,
+                                                               int64_t k0, int kb, float2* __restrict__ Linv,
+                                                               float2* __restrict__ Uinv,
+                                                               unsigned* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2(*A)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);             // [col][row]
     float2(*X)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;
     float2* Tb = reinterpret_cast<float2*>(dyn_smem) + 2 * NB * (NB + 1);             // NB*NB/4
     __shared__ float2 colbuf[2][NB], rowbuf[2][NB];
+    constexpr int G = kDiagThreads / NB;  // column groups
+    constexpr int CPT = NB / G;           // columns per thread
     const int tid = threadIdx.x;
-    // Elimination in registers: thread (r, g) owns row r, columns g + 4u. The
-    // block is padded to NB x NB with the identity (kb < NB only at the end).
-    const int r = tid & (NB - 1), g = tid >> 6;
-    float2 a[NB / 4];
+    // Elimination in registers: thread (r, g) owns row r, columns g + G u.
+    // The block is padded to NB x NB with the identity (kb < NB only at the
+    // end). Many warps with few columns each keep the latency-bound chain of
+    // NB steps short.
+    const int r = tid & (NB - 1), g = tid / NB;
+    float2 a[CPT];
 #pragma unroll
-    for (int u = 0; u < NB / 4; ++u) {
-        const int c = g + 4 * u;
+    for (int u = 0; u < CPT; ++u) {
+        const int c = g + G * u;
         a[u] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
     }
     // One barrier per step; the pivot column and row go through
-    // double-buffered shared slots.
+    // double-buffered shared slots. Step j = jg + G uj is written as two
+    // loops so that the pivot column's register a[uj] has a static index.
+#pragma unroll
+    for (int uj = 0; uj < CPT; ++uj) {
 #pragma unroll 1
-    for (int j = 0; j < NB; ++j) {
-        const int buf = j & 1;
-        if (g == (j & 3)) {
+        for (int jg = 0; jg < G; ++jg) {
+            const int j = jg + G * uj;
+            const int buf = j & 1;
+            if (g == jg) colbuf[buf][r] = a[uj];
+            if (r == j) {
 #pragma unroll
-            for (int u = 0; u < NB / 4; ++u)  // static indices keep a[] in registers
-                if (u == (j >> 2)) colbuf[buf][r] = a[u];
-        }
-        if (r == j) {
+                for (int u = 0; u < CPT; ++u) rowbuf[buf][g + G * u] = a[u];
+            }
+            __syncthreads();
+            const float2 piv = rowbuf[buf][j];
+            const float pm = piv.x * piv.x + piv.y * piv.y;
+            if (!(pm > 1e-30f) || !isfinite(pm)) {  // block-uniform decision
+                if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
+                return;
+            }
+            if (r > j) {
+                const float2 l = cmulf(colbuf[buf][r], crecipf(piv));
 #pragma unroll
-            for (int u = 0; u < NB / 4; ++u) rowbuf[buf][g + 4 * u] = a[u];
-        }
-        __syncthreads();
-        const float2 piv = rowbuf[buf][j];
-        const float pm = piv.x * piv.x + piv.y * piv.y;
-        if (!(pm > 1e-30f) || !isfinite(pm)) {  // block-uniform decision
-            if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
-            return;
-        }
-        if (r > j) {
-            const float2 l = cmulf(colbuf[buf][r], crecipf(piv));
-#pragma unroll
-            for (int u = 0; u < NB / 4; ++u) {
-                const int c = g + 4 * u;
-                if (c > j) a[u] = csubf(a[u], cmulf(l, rowbuf[buf][c]));
-                else if (c == j) a[u] = l;
+                for (int u = 0; u < CPT; ++u) {
+                    const int c = g + G * u;
+                    if (c > j) a[u] = csubf(a[u], cmulf(l, rowbuf[buf][c]));
+                    else if (c == j) a[u] = l;
+                }
             }
         }
     }
 #pragma unroll
-    for (int u = 0; u < NB / 4; ++u) {
-        const int c = g + 4 * u;
+    for (int u = 0; u < CPT; ++u) {
+        const int c = g + G * u;
         A[c][r] = a[u];
         if (r < kb && c < kb) W[(k0 + r) + (k0 + c) * ldw] = a[u];
     }
@@ -434,16 +447,18 @@ __device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw
     }
 }
 
-// Both panels of one block step in one launch: CTAs [0, nL) form L21 rows,
-// the rest U12 columns (disjoint regions of W).
-__global__ void __launch_bounds__(256) panel_LU_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                                       int64_t s0, int64_t np, const float2* __restrict__ Linv,
-                                                       const float2* __restrict__ Uinv, float* __restrict__ Apack,
-                                                       float* __restrict__ Bpack, int pack, int nL) {
-    if ((int)blockIdx.x < nL)
-        panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x);
-    else
-        panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x - nL);
+// The two panels of a block step are separate launches: L21 is formed on
+// the lookahead stream as soon as its columns are updated, U12 once the
+// trailing update of its rows has finished.
+__global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                      int64_t s0, int64_t np, const float2* __restrict__ Uinv,
+                                                      float* __restrict__ Apack, int pack) {
+    panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x);
+}
+__global__ void __launch_bounds__(256) panel_U_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                      int64_t s0, int64_t np, const float2* __restrict__ Linv,
+                                                      float* __restrict__ Bpack, int pack) {
+    panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x);
 }
 
 // SIMT trailing update C -= L21 U12 in complex64 (checking path).
@@ -484,135 +499,258 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Blocked forward (lower = 1) or backward solve on the factors, one CTA per
-// block row in solve order (tickets handed out in launch order), FP64
-// arithmetic on the complex64 factors; in place in x (np entries).
-// progress[0]: number of blocks completed in solve order (blocks finish in
-// order, so a single counter suffices); progress[1]: ticket counter. Both are
-// cleared by the host. A CTA waits only for blocks with smaller tickets,
-// whose CTAs are already running; every wait is bounded and reports through
-// err. While waiting, the next factor tile (and, from the start, the
-// diagonal inverse) are already in registers, so the critical path per block
-// is the x read, two 64-wide reductions and the release of the counter.
-__global__ void __launch_bounds__(256) trsv_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
-                                                   int nbl, int lower, const float2* __restrict__ Dinv,
-                                                   cplx* __restrict__ x, unsigned* __restrict__ progress,
-                                                   unsigned* __restrict__ err, long long spin_limit) {
-    __shared__ int s_blk;
+// Blocked forward (lower = 1) or backward solve on the factors, in place in
+// x (np entries), FP64 arithmetic on the complex64 factors.
+//
+// One CTA per 128-row block (two NB sub-blocks), taken in solve order by
+// ticket. Warp 8 streams the CTA's factor tiles (128 rows x 32 columns,
+// 32 KB) by TMA into a 4-stage shared-memory ring, in the order in which
+// their x entries are published, independently of that publication; warps
+// 0-7 wait (one poller per warp) until the sub-block a tile multiplies has
+// been published, then accumulate. The two diagonal sub-blocks are solved
+// inside the CTA: the first with its explicit inverse, published at once,
+// then the coupling block and the second inverse.
+//
+// progress[0]: number of NB sub-blocks published in solve order; progress[1]:
+// ticket counter; both cleared by the host. A CTA waits only for CTAs with
+// smaller tickets, which are already running. Every wait is bounded by
+// timeout_ns from the CTA's start; on timeout the error word is set, the CTA
+// still consumes every tile its producer issues (so no copy is in flight at
+// exit) and returns without publishing.
+constexpr int TR_ROWS = 2 * NB;       // rows per CTA
+constexpr int TR_COLS = 32;           // columns per streamed tile
+constexpr int TR_STAGES = 4;
+constexpr int TR_TILE = TR_ROWS * TR_COLS;           // float2 per tile
+constexpr int TR_TILE_BYTES = TR_TILE * 8;           // 32 KB
+constexpr int TR_DLD = NB + 4;        // staged inverses [col][row]: conflict-free half-warps
+constexpr int TR_CONSUMERS = 256;
+constexpr int TR_THREADS = TR_CONSUMERS + 32;
+constexpr int kSmemTrsv = 1024 + TR_STAGES * TR_TILE_BYTES + 2 * NB * TR_DLD * 8 +
+                          (2 * TR_ROWS + NB) * (int)sizeof(cplx) + 2 * TR_STAGES * 8;
+
+__device__ __forceinline__ void consumer_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// Bounded mbarrier wait; false once the deadline has passed.
+__device__ __forceinline__ bool tr_wait(uint32_t bar, uint32_t parity, uint64_t deadline) {
+    int it = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if ((++it & 255) == 0 && global_ns() > deadline) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(TR_THREADS, 1)
+trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, int lower,
+                const float2* __restrict__ Dinv, cplx* __restrict__ x, unsigned* __restrict__ progress,
+                unsigned* __restrict__ err, unsigned long long timeout_ns) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];  // aligned to 1024 below
+    const uint32_t raw = smem_u32(dyn_smem);
+    unsigned char* base = dyn_smem + (((raw + 1023u) & ~1023u) - raw);
+    const uint32_t ring = smem_u32(base);
+    const float2* ringp = reinterpret_cast<const float2*>(base);
+    float2* Ds = reinterpret_cast<float2*>(base + TR_STAGES * TR_TILE_BYTES);  // 2 x [NB cols][TR_DLD]
+    cplx* red = reinterpret_cast<cplx*>(Ds + 2 * NB * TR_DLD);                  // TR_ROWS
+    cplx* ys = red + TR_ROWS;                                                      // TR_ROWS
+    cplx* xs = ys + TR_ROWS;                                                       // NB
+    const uint32_t full0 = smem_u32(xs + NB), empty0 = full0 + 8 * TR_STAGES;
+    __shared__ int s_t, s_go;
     __shared__ volatile int s_abort;
-    __shared__ cplx s_y[NB];
-    const int tid = threadIdx.x, lane = tid & 31;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
-        s_blk = (int)atomicAdd(&progress[1], 1u);
+        s_t = (int)atomicAdd(&progress[1], 1u);
         s_abort = 0;
+        for (int st = 0; st < TR_STAGES; ++st) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, TR_CONSUMERS / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
-    const int t = s_blk;
-    if (t >= nbl) return;
-    const int bi = lower ? t : nbl - 1 - t;
-    const int64_t r0 = (int64_t)bi * NB;
-    const int rows = (int)(np - r0 < NB ? np - r0 : NB);
-    // Thread (r, part): row r of the block, inner columns part + 4u. A warp
-    // holds 8 whole rows, so every reduction is a pair of shuffles.
-    const int r = tid >> 2, part = tid & 3;
-    const float2* D = Dinv + (size_t)bi * NB * NB;
-    float2 dreg[NB / 4];
-#pragma unroll
-    for (int u = 0; u < NB / 4; ++u) dreg[u] = D[r + (part + 4 * u) * NB];
-
-    auto load_w = [&](int step, float2 (&dst)[NB / 4]) {
-        const int bj = lower ? step : nbl - 1 - step;
-        const int64_t c0 = (int64_t)bj * NB;
-#pragma unroll
-        for (int u = 0; u < NB / 4; ++u) {
-            const int c = part + 4 * u;
-            dst[u] = (r < rows && c0 + c < np) ? W[(r0 + r) + (c0 + c) * ldw] : make_float2(0.f, 0.f);
-        }
-    };
-    double acc_re = 0.0, acc_im = 0.0;
-    auto accumulate = [&](int step, const float2 (&w)[NB / 4]) {
-        const int bj = lower ? step : nbl - 1 - step;
-        const int64_t c0 = (int64_t)bj * NB;
-#pragma unroll
-        for (int u = 0; u < NB / 4; ++u) {
-            const int c = part + 4 * u;
-            if (c0 + c < np) {
-                // produced by another CTA: read through L2, never a stale L1 line
-                const double xr = __ldcg(&x[c0 + c].re), xi = __ldcg(&x[c0 + c].im);
-                acc_re += (double)w[u].x * xr - (double)w[u].y * xi;
-                acc_im += (double)w[u].x * xi + (double)w[u].y * xr;
-            }
-        }
+    const uint64_t deadline = global_ns() + timeout_ns;
+    const int ncta = (int)((np + TR_ROWS - 1) / TR_ROWS);
+    const int t = s_t;
+    if (t >= ncta) return;  // block-uniform
+    const int rb = lower ? t : ncta - 1 - t;
+    const int64_t R0 = (int64_t)rb * TR_ROWS;
+    const int sbA = 2 * rb, sbB = 2 * rb + 1;
+    const bool has_bot = sbB < nsb;
+    // Streamed tiles: the off-diagonal ones in publication order, then the
+    // two tiles holding the coupling block between the sub-blocks.
+    const int ntile_all = (int)((np + TR_COLS - 1) / TR_COLS);
+    int n_off;
+    if (lower) {
+        n_off = (int)(R0 / TR_COLS);
+    } else {
+        const int kmin = (int)((R0 + TR_ROWS) / TR_COLS);
+        n_off = ntile_all > kmin ? ntile_all - kmin : 0;
+    }
+    const int n_tiles = n_off + (has_bot ? 2 : 0);
+    const int k_intra = (int)((lower ? R0 : R0 + NB) / TR_COLS);
+    auto tile_k = [&](int i) -> int {
+        if (i < n_off) return lower ? i : ntile_all - 1 - i;
+        return k_intra + (i - n_off);
     };
 
-    // One poller per CTA. The counter is read with acquire semantics and the
-    // answer handed to the CTA through a barrier; a CTA far behind the
-    // frontier backs off in proportion to its distance, so the next block in
-    // line is the only fast poller on the counter's cache line.
-    float2 wpre[NB / 4], wtmp[NB / 4];
-    int done = 0;
-    while (done < t) {
-        load_w(done, wpre);  // in flight while the counter is awaited
-        if (tid == 0) {
-            long long it = 0;
-            unsigned p;
-            int ready = -1;
-            while ((p = ld_acquire_gpu(&progress[0])) <= (unsigned)done) {
-                if (++it > spin_limit || ((it & 63) == 0 && ld_acquire_gpu(err) != 0u)) {
+    if (warp == TR_CONSUMERS / 32) {  // producer
+        if (lane == 0) {
+            for (int i = 0; i < n_tiles; ++i) {
+                const int st = i % TR_STAGES;
+                const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
+                if (!tr_wait(empty0 + 8 * st, ph ^ 1u, deadline)) {
                     atomicCAS(err, 0u, 2u);
-                    p = 0;
+                    s_abort = 1;
                     break;
                 }
-                const unsigned gap = (unsigned)t - p;  // blocks still ahead of this one
-                __nanosleep(gap <= 1 ? 20 : (gap < 64 ? 200 * gap : 12800));
+                mbar_expect_tx(full0 + 8 * st, TR_TILE_BYTES);
+                tma_load_2d(ring + st * TR_TILE_BYTES, &tmW, full0 + 8 * st, (int)R0, tile_k(i) * TR_COLS);
             }
-            if (p != 0) ready = (int)min(p, (unsigned)t);
-            s_blk = ready;  // reused as the broadcast slot
         }
-        __syncthreads();
-        const int ready = s_blk;
-        if (ready < 0) {
+        return;
+    }
+
+    // Consumers. Inverses of the two diagonal sub-blocks into shared memory.
+    for (int e = tid; e < NB * NB; e += TR_CONSUMERS) {
+        const int r = e & (NB - 1), c = e >> 6;
+        Ds[c * TR_DLD + r] = Dinv[(size_t)sbA * NB * NB + e];
+        Ds[(NB + c) * TR_DLD + r] = has_bot ? Dinv[(size_t)sbB * NB * NB + e] : make_float2(0.f, 0.f);
+    }
+    // Thread (r, h): row r of the block, columns h*16 .. h*16+15 of a tile.
+    const int r = tid & (TR_ROWS - 1), h = tid >> 7;
+    const int64_t grow = R0 + r;
+    cplx b = cx(0, 0);  // written only by this CTA: final from the start
+    if (h == 0 && grow < np) b = cx(__ldcg(&x[grow].re), __ldcg(&x[grow].im));
+    double acc_re = 0.0, acc_im = 0.0;
+    unsigned seen = 0;
+    for (int i = 0; i < n_off; ++i) {
+        const int st = i % TR_STAGES;
+        const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
+        const int k = tile_k(i);
+        const int sb = (k * TR_COLS) / NB;
+        const unsigned need = lower ? (unsigned)sb + 1u : (unsigned)(nsb - sb);
+        bool ok = !s_abort;
+        if (ok && seen < need) {
+            if (lane == 0) {
+                int it = 0;
+                unsigned p = seen;
+                while (true) {
+                    p = ld_acquire_gpu(&progress[0]);
+                    if (p >= need) break;
+                    if (need - p > 4) __nanosleep(256);
+                    if ((++it & 63) == 0 &&
+                        (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
+                        atomicCAS(err, 0u, 2u);
+                        s_abort = 1;
+                        break;
+                    }
+                }
+                seen = p;
+            }
+            seen = __shfl_sync(0xffffffffu, seen, 0);
+            ok = seen >= need;
+            __syncwarp();
+        }
+        // Every issued tile is waited for and released, also after an abort,
+        // so that no copy is in flight when the CTA exits.
+        if (!tr_wait(full0 + 8 * st, ph, deadline)) {
+            if (lane == 0) atomicCAS(err, 0u, 2u);
             s_abort = 1;
-            break;
+            ok = false;
         }
-        accumulate(done, wpre);
-        for (int step = done + 1; step < ready; ++step) {
-            load_w(step, wtmp);
-            accumulate(step, wtmp);
-        }
-        done = ready;
-        __syncthreads();  // the broadcast slot is rewritten on the next pass
-    }
-    acc_re += __shfl_xor_sync(0xffffffffu, acc_re, 1);
-    acc_im += __shfl_xor_sync(0xffffffffu, acc_im, 1);
-    acc_re += __shfl_xor_sync(0xffffffffu, acc_re, 2);
-    acc_im += __shfl_xor_sync(0xffffffffu, acc_im, 2);
-    if (part == 0) {
-        const cplx b = r < rows ? cx(__ldcg(&x[r0 + r].re), __ldcg(&x[r0 + r].im)) : cx(0, 0);
-        s_y[r] = r < rows ? cx(b.re - acc_re, b.im - acc_im) : cx(0, 0);
-    }
-    __syncthreads();
-    if (s_abort) return;  // block-uniform
-    // x_i = Dinv * y  (Dinv: NB x NB column-major, this block)
-    double re = 0.0, im = 0.0;
+        if (ok) {
+            const float2* tile = ringp + st * TR_TILE;
+            const int64_t c0 = (int64_t)k * TR_COLS + h * 16;
+            double xr[16], xi[16];
 #pragma unroll
-    for (int u = 0; u < NB / 4; ++u) {
-        const cplx yv = s_y[part + 4 * u];
-        re += (double)dreg[u].x * yv.re - (double)dreg[u].y * yv.im;
-        im += (double)dreg[u].x * yv.im + (double)dreg[u].y * yv.re;
+            for (int u = 0; u < 16; ++u) {
+                const bool in = c0 + u < np;
+                xr[u] = in ? __ldcg(&x[c0 + u].re) : 0.0;
+                xi[u] = in ? __ldcg(&x[c0 + u].im) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const float2 w = tile[(h * 16 + u) * TR_ROWS + r];
+                acc_re += (double)w.x * xr[u] - (double)w.y * xi[u];
+                acc_im += (double)w.x * xi[u] + (double)w.y * xr[u];
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * st);
+    }
+    if (h == 1) red[r] = cx(acc_re, acc_im);
+    consumer_bar();
+    if (h == 0) ys[r] = cx(b.re - acc_re - red[r].re, b.im - acc_im - red[r].im);
+    if (tid == 0) s_go = !s_abort;
+    consumer_bar();
+    if (!s_go) return;  // block-uniform
+
+    // Diagonal phase. Thread (dr, part): row dr of a sub-block, columns part + 4u.
+    const int dr = tid >> 2, part = tid & 3;
+    auto solve_sub = [&](int which) {
+        const float2* D = Ds + which * NB * TR_DLD;
+        const cplx* y = ys + which * NB;
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = part + 4 * u;
+            const float2 d = D[c * TR_DLD + dr];
+            const cplx yv = y[c];
+            re += (double)d.x * yv.re - (double)d.y * yv.im;
+            im += (double)d.x * yv.im + (double)d.y * yv.re;
+        }
+        re += __shfl_xor_sync(0xffffffffu, re, 1);
+        im += __shfl_xor_sync(0xffffffffu, im, 1);
+        re += __shfl_xor_sync(0xffffffffu, re, 2);
+        im += __shfl_xor_sync(0xffffffffu, im, 2);
+        const int64_t gr = R0 + which * NB + dr;
+        if (part == 0) {
+            xs[dr] = cx(re, im);
+            if (gr < np) {
+                __stcg(&x[gr].re, re);
+                __stcg(&x[gr].im, im);
+            }
+        }
+        // The barrier orders every store of the sub-block before the release.
+        consumer_bar();
+        const int sb = which ? sbB : sbA;
+        if (tid == 0) st_release_gpu(&progress[0], lower ? (unsigned)sb + 1u : (unsigned)(nsb - sb));
+    };
+    if (!has_bot) {
+        solve_sub(0);
+        return;
+    }
+    const int first = lower ? 0 : 1, second = 1 - first;
+    solve_sub(first);
+    // Coupling block: rows of `second` x columns of `first`, in the last two tiles.
+    bool ok = true;
+    for (int j = 0; j < 2; ++j) {
+        const int i = n_off + j;
+        ok = tr_wait(full0 + 8 * (i % TR_STAGES), (uint32_t)(i / TR_STAGES) & 1u, deadline) && ok;
+    }
+    if (!ok && tid == 0) atomicCAS(err, 0u, 2u);
+    const int roff = second * NB;
+    double re = 0.0, im = 0.0;
+    if (ok) {
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = part + 4 * u;
+            const float2* tile = ringp + ((n_off + (c >> 5)) % TR_STAGES) * TR_TILE;
+            const float2 w = tile[(c & 31) * TR_ROWS + roff + dr];
+            const cplx xv = xs[c];
+            re += (double)w.x * xv.re - (double)w.y * xv.im;
+            im += (double)w.x * xv.im + (double)w.y * xv.re;
+        }
     }
     re += __shfl_xor_sync(0xffffffffu, re, 1);
     im += __shfl_xor_sync(0xffffffffu, im, 1);
     re += __shfl_xor_sync(0xffffffffu, re, 2);
     im += __shfl_xor_sync(0xffffffffu, im, 2);
-    if (part == 0 && r < rows) {
-        __stcg(&x[r0 + r].re, re);
-        __stcg(&x[r0 + r].im, im);
-    }
-    // Barrier, then one gpu-scope release by thread 0: the writes of the
-    // whole CTA happen before the release through the barrier.
-    __syncthreads();
-    if (tid == 0) st_release_gpu(&progress[0], (unsigned)(t + 1));
+    if (part == 0) ys[roff + dr] = cx(ys[roff + dr].re - re, ys[roff + dr].im - im);
+    if (tid == 0) s_go = ok;
+    consumer_bar();
+    if (!s_go) return;  // block-uniform
+    solve_sub(second);
 }
 
 // ------------------------------------------------------------ small vector ops
@@ -714,6 +852,9 @@ void mixed_release(DenseSolver* s) {
     MixedState* st = state_of(s);
     if (st) {
         if (st->gemm) gemm_tc_destroy(st->gemm);
+        if (st->ev_cols) cudaEventDestroy(st->ev_cols);
+        if (st->ev_panel) cudaEventDestroy(st->ev_panel);
+        if (st->side) cudaStreamDestroy(st->side);
         delete st;
     }
     s->gemm_state = nullptr;
@@ -774,17 +915,27 @@ int mixed_factorize(DenseSolver* s) {
     st->err = reinterpret_cast<unsigned*>(base + up(bW) + 2 * up(bInv) + up(bDiag));
     st->tri_flags = st->err + 16;
     const int K3 = 6 * NB;
-    SIEB_RETURN_IF(s->gemm_a.reserve(sizeof(float) * 2 * np * K3));
+    const size_t bApack = ((sizeof(float) * 2 * np * K3 + 255) / 256) * 256;
+    SIEB_RETURN_IF(s->gemm_a.reserve(2 * bApack));
     SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * K3));
-    st->Apack = s->gemm_a.as<float>();
+    st->Apack[0] = s->gemm_a.as<float>();
+    st->Apack[1] = reinterpret_cast<float*>(s->gemm_a.as<char>() + bApack);
     st->Bpack = s->gemm_b.as<float>();
     if (st->use_tc && !st->gemm) SIEB_RETURN_IF(gemm_tc_create(&st->gemm));
+    if (!st->side) {
+        int least = 0, greatest = 0;
+        SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_panel, cudaEventDisableTiming));
+    }
 
     static bool attrs_set = false;
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_LU_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_L_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
         attrs_set = true;
     }
     SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
@@ -797,34 +948,64 @@ int mixed_factorize(DenseSolver* s) {
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
 
-    for (int64_t bk = 0; bk < nbl; ++bk) {
+    // Diagonal block bk and its L21 panel (into the A pack of step bk).
+    auto diag_and_L = [&](int64_t bk, cudaStream_t sm) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
-        float2* Li = st->Linv + (size_t)bk * NB * NB;
-        float2* Ui = st->Uinv + (size_t)bk * NB * NB;
-        diag_lu_kernel<<<1, 256, kSmemDiag, stream>>>(st->W, ldw, k0, kb, Li, Ui, st->err);
+        diag_lu_kernel<<<1, kDiagThreads, kSmemDiag, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
+                                                            st->Uinv + (size_t)bk * NB * NB, st->err);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         const int64_t s0 = k0 + kb;
+        if (s0 < np) {
+            panel_L_kernel<<<(unsigned)blocks_for(np - s0, 32), 256, kSmemPanel, sm>>>(
+                st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Apack[bk & 1], st->use_tc);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
+        return SIEB200_OK;
+    };
+    auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B) -> int {
+        const int64_t m = np - s0;
+        float* C = reinterpret_cast<float*>(st->W + s0 + c0 * ldw);
+        cudaEvent_t ev;
+        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * K3,
+                        4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K3), &ev);
+        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K3));
+        ctx->prof.end(stream, ev);
+        return SIEB200_OK;
+    };
+
+    // Right-looking block LU with a lookahead of one block: after the update
+    // of the next block's columns, its diagonal factorization and L21 panel
+    // run on the side stream while the rest of the trailing update runs here.
+    SIEB_RETURN_IF(diag_and_L(0, stream));
+    for (int64_t bk = 0; bk < nbl; ++bk) {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        const int64_t s0 = k0 + kb;
         if (s0 >= np) break;
         const int64_t m = np - s0;
-        const int nL = (int)blocks_for(m, 32);
-        panel_LU_kernel<<<2 * nL, 256, kSmemPanel, stream>>>(st->W, ldw, k0, kb, s0, np, Li, Ui, st->Apack,
-                                                              st->Bpack, st->use_tc, nL);
+        panel_U_kernel<<<(unsigned)blocks_for(m, 32), 256, kSmemPanel, stream>>>(
+            st->W, ldw, k0, kb, s0, np, st->Linv + (size_t)bk * NB * NB, st->Bpack, st->use_tc);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         if (st->use_tc) {
-            float* C = reinterpret_cast<float*>(st->W + s0 + s0 * ldw);
-            cudaEvent_t ev;
-            ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * m * K3,
-                            4.0 * (2.0 * (2.0 * m) * m + (2.0 * m + m) * K3), &ev);
-            SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, st->Apack, st->Bpack, 2 * m, m, K3));
-            ctx->prof.end(stream, ev);
+            const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
+            const float* A = st->Apack[bk & 1];
+            SIEB_RETURN_IF(gemm(s0, s0, n1, A, st->Bpack));
+            SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
+            SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
+            SIEB_RETURN_IF(diag_and_L(bk + 1, st->side));
+            SIEB_TRY_CUDA(cudaEventRecord(st->ev_panel, st->side));
+            if (m > n1) SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3));
+            SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
+            SIEB_RETURN_IF(diag_and_L(bk + 1, stream));
         }
     }
     return check_err(s, "mixed LU factorization");
@@ -843,18 +1024,35 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     rbt_vec_T_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(r, n, np, d_first, work);
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
-    const long long spin = 1ll << 26;
     unsigned* fl = st->tri_flags;
     const int nbl = (int)st->nbl;
     if (!adjoint) {
+        if (st->tm_base != st->W || st->tm_np != np) {
+            // W as 8-byte elements: rows inner, 128 x 32 boxes; rows/columns
+            // beyond np read as zero.
+            SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->W, (uint64_t)np,
+                                                (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
+                                                TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
+            st->tm_base = st->W;
+            st->tm_np = np;
+        }
+        static bool attr_set = false;
+        if (!attr_set) {
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSmemTrsv));
+            attr_set = true;
+        }
+        const unsigned ncta = (unsigned)((np + TR_ROWS - 1) / TR_ROWS);
+        const unsigned long long timeout_ns = 2000000000ull;
         // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
         const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
         for (int lower = 1; lower >= 0; --lower) {
-            SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * (nbl + 1), stream));
+            SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * 2, stream));
             cudaEvent_t ev;
             s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
-            trsv_kernel<<<nbl, 256, 0, stream>>>(st->W, st->ldw, np, nbl, lower, lower ? st->Linv : st->Uinv,
-                                                 work, fl, st->err, spin);
+            trsv_tma_kernel<<<ncta, TR_THREADS, kSmemTrsv, stream>>>(st->tmW, np, nbl, lower,
+                                                                     lower ? st->Linv : st->Uinv, work, fl,
+                                                                     st->err, timeout_ns);
             SIEB_NOTE_LAUNCH();
             s->ctx->prof.end(stream, ev);
             SIEB_TRY_CUDA(cudaGetLastError());

@@ -114,3 +114,33 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
     assert np.linalg.norm(Zh @ xs - b.cpu().numpy()) / np.linalg.norm(b.cpu().numpy()) < 1e-12
     assert it >= 1
     s.close()
+
+
+@pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
+def test_mixed_ragged_sizes_one_step(n, gpu_ctx):
+    """Sizes that leave partial sub-blocks, a last row block with one
+    sub-block, and fewer rows than one block. One preconditioned step must
+    already reach 1e-5 (the factors are single precision), and the full
+    refinement 1e-12: a wrong triangular solve fails the first bound."""
+    import torch
+    import sieb200
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()  # column-major storage
+    s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+    s.factorize(Z.data_ptr())
+    x = torch.from_numpy(b.copy()).cuda()
+    torch.cuda.synchronize()
+    it = s.solve(x.data_ptr(), tolerance=1e-5, max_iterations=1)
+    gpu_ctx.synchronize()
+    xs = x.cpu().numpy()
+    assert it == 1
+    assert np.linalg.norm(A @ xs - b) / np.linalg.norm(b) <= 1e-5
+    x = torch.from_numpy(b.copy()).cuda()
+    torch.cuda.synchronize()
+    s.solve(x.data_ptr(), tolerance=1e-12, max_iterations=20)
+    gpu_ctx.synchronize()
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(A @ xs - b) / np.linalg.norm(b) <= 1e-12
+    s.close()
