@@ -217,6 +217,17 @@ int sieb200_dense_solver_solve_adjoint(sieb200_dense_solver* s, int64_t nrhs, do
 int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                    const double* x, double beta, double* y);
 
+/* The matvec above without any allocation (no counterpart in the reference):
+ * its partial sums go to one fixed 2 MiB device array per device instead of
+ * a per-call workspace, for callers that may not allocate device memory at
+ * the point of the call. n <= 131072, else SIEB200_INVALID_ARG. The first
+ * call on a device resolves the array's address (cudaGetSymbolAddress) and
+ * should come before any stream capture. Calls whose kernels overlap in time
+ * on one device (two host threads, two contexts) race on the array.
+ * Synchronizes the context stream like sieb200_matvec. */
+int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
+                           const double* x, double beta, double* y);
+
 /* Split-TF32 tensor-core contraction used by the mixed LU's trailing update
  * (no counterpart in the reference, which calls cuSOLVER): on device data,
  *   C[m2 x n] (fp32, column-major, ldc) -= A[m2 x k] * B[n x k]^T,

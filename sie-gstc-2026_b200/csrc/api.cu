@@ -635,6 +635,17 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
     return SIEB200_OK;
 }
 
+int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
+                           const double* x, double beta, double* y) {
+    SIEB_CHECK(ctx && A && x && y && n > 0 && lda >= n && (prec == 0 || prec == 1),
+               SIEB200_INVALID_ARG, "invalid matvec arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    SIEB_RETURN_IF(gemv_device_static_scratch(ctx, n, A, lda, prec, reinterpret_cast<const cplx*>(x), beta,
+                                              reinterpret_cast<cplx*>(y)));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
 int64_t sieb200_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable) {

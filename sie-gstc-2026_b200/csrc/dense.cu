@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -89,6 +91,73 @@ int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int pre
                                                                           scratch.as<cplx>(), beta, y);
     SIEB_NOTE_LAUNCH();
     ctx->prof.end(ctx->stream, ev);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
+// ------------------------------------------------- matvec without allocation
+// Some callers of the residual matvec may not allocate device memory at the
+// point of the call: a refinement loop that runs beside other streams of the
+// same device (cudaFree waits for the whole device, stalling them), or a
+// caller that has already committed the rest of HBM to the matrix and its
+// factors (an allocation there can fail in mid-iteration). For them the
+// partial sums live in one fixed file-scope device array instead of a
+// workspace allocated per call.
+//
+// Limit: kStaticScratchElems complex128 partial sums (2 MiB), i.e. at most
+// that many rows x column chunks; the chunk count shrinks to fit, and n
+// above kStaticScratchElems is rejected. Nothing in the array needs to start
+// at zero: every partial sum is written before it is read. There is one
+// array per device, so calls whose kernels overlap in time (from two host
+// threads, or on two contexts of one device) race on it.
+constexpr int64_t kStaticScratchElems = 131072;
+static __device__ __align__(256) cplx g_static_scratch[kStaticScratchElems];
+
+namespace {
+std::mutex g_static_scratch_mu;
+void* g_static_scratch_ptr[64] = {};  // device address of the array, per device
+}  // namespace
+
+int static_scratch_setup(int device, cplx** out) {
+    SIEB_CHECK(device >= 0 && device < 64, SIEB200_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+    if (!g_static_scratch_ptr[device]) {
+        // Called with `device` current: resolves this device's instance of
+        // the array (the first call per device may load the module).
+        void* p = nullptr;
+        SIEB_TRY_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+        SIEB_CHECK(p != nullptr, SIEB200_CUDA_ERROR, "cudaGetSymbolAddress returned no address");
+        g_static_scratch_ptr[device] = p;
+    }
+    *out = static_cast<cplx*>(g_static_scratch_ptr[device]);
+    return SIEB200_OK;
+}
+
+int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
+                               const cplx* x, double beta, cplx* y) {
+    SIEB_CHECK(n <= kStaticScratchElems, SIEB200_INVALID_ARG,
+               "matvec without allocation: n = " + std::to_string(n) + " exceeds its fixed scratch (n <= " +
+                   std::to_string(kStaticScratchElems) + ")");
+    cplx* scratch = nullptr;
+    SIEB_RETURN_IF(static_scratch_setup(ctx->device, &scratch));
+    const int threads = 256;
+    const int64_t row_blocks = (n + threads - 1) / threads;
+    int64_t chunks = std::max<int64_t>(1, (int64_t)ctx->sm_count * 4 / std::max<int64_t>(1, row_blocks));
+    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / 64));
+    chunks = std::min<int64_t>(chunks, kStaticScratchElems / n);  // fit the fixed array
+    const int64_t cpc = (n + chunks - 1) / chunks;
+    chunks = (n + cpc - 1) / cpc;
+    const dim3 grid((unsigned)row_blocks, (unsigned)chunks);
+    if (prec == 0)
+        gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(n, static_cast<const double2*>(A), lda, x,
+                                                                          cpc, scratch);
+    else
+        gemv_partial_kernel<float2><<<grid, threads, 0, ctx->stream>>>(n, static_cast<const float2*>(A), lda, x,
+                                                                         cpc, scratch);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    gemv_finish_kernel<<<(unsigned)row_blocks, threads, 0, ctx->stream>>>(n, (int)chunks, scratch, beta, y);
+    SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }
