@@ -254,6 +254,8 @@ def run(args):
     gemm = ctx.profile_read(0)
     trsv = ctx.profile_read(1)
     gemv = ctx.profile_read(2)
+    prof = {name: ctx.profile_read(i) for i, name in
+            [(3, "diag_lu"), (4, "panel_L"), (5, "panel_U"), (6, "factorization"), (7, "refined_solve")]}
     ctx.profile(False)
 
     # Accuracy of the mixed solution against the FP64 matrix.
@@ -342,6 +344,10 @@ def run(args):
             "hbm_frac": gemm_gbs / peaks["hbm_gbs"], "time_share": shares,
             "trsv_gbs": trsv["bytes"] / (trsv["ms"] / 1e3) / 1e9 if trsv["ms"] > 0 else None,
             "fp64_matvec_gbs": gemv["bytes"] / (gemv["ms"] / 1e3) / 1e9 if gemv["ms"] > 0 else None,
+            # mean device time per launch (ms) of the chain kernels and of the
+            # two phases of a step (spans on the launching streams)
+            "mean_ms": {k: (v["ms"] / v["launches"] if v["launches"] else None)
+                        for k, v in [("tf32_gemm", gemm), ("trsv", trsv), *prof.items()]},
         }
         value = world * args.steps / t_mixed
         out = {

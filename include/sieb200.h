@@ -242,7 +242,10 @@ int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const 
  * accumulates launch count, device milliseconds and algorithmic work.
  * kernel 0: split-TF32 trailing GEMM (work = 2*m2*n*k TF32 flops and
  * 4*(2*m2*n + (m2 + n)*k) bytes per launch); 1: triangular solves
- * (work = bytes of factors read); 2: FP64 matvec (bytes of Z read). */
+ * (work = bytes of factors read); 2: FP64 matvec (bytes of Z read);
+ * 3: diagonal-block LU + inverses; 4: L21 panels; 5: U12 panels;
+ * 6: whole mixed factorizations; 7: whole refined solves (spans on the
+ * context stream; 3 and 4 run on the solver's lookahead stream). */
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable);
 /* Number of CUDA kernels the library has launched in this process. */
 int64_t sieb200_launch_count(void);

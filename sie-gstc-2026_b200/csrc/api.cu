@@ -56,7 +56,20 @@ void Profiler::begin(cudaStream_t s, int kernel, double flops, double bytes, cud
     *end_out = nullptr;
     if (!enabled) return;
     Pending p{kernel, nullptr, nullptr, flops, bytes};
-    if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) {
+    auto take = [&](cudaEvent_t* e) {
+        if (!pool.empty()) {
+            *e = pool.back();
+            pool.pop_back();
+            return true;
+        }
+        return cudaEventCreate(e) == cudaSuccess;
+    };
+    if (!take(&p.a)) {
+        cudaGetLastError();
+        return;
+    }
+    if (!take(&p.b)) {
+        pool.push_back(p.a);
         cudaGetLastError();
         return;
     }
@@ -79,8 +92,8 @@ void Profiler::collect() {
             kp.flops += p.flops;
             kp.bytes += p.bytes;
         }
-        cudaEventDestroy(p.a);
-        cudaEventDestroy(p.b);
+        pool.push_back(p.a);
+        pool.push_back(p.b);
     }
     pending.clear();
     cudaGetLastError();
@@ -413,6 +426,9 @@ int sieb200_ctx_destroy(sieb200_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     destroy_cusolver(ctx);
+    ctx->prof.collect();
+    for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
+    ctx->prof.pool.clear();
     ctx->faces.release(); ctx->geom.release(); ctx->qpts.release(); ctx->qw.release();
     ctx->pairs.release(); ctx->near_list.release(); ctx->counter.release(); ctx->inc.release();
     ctx->mass.release(); ctx->zbuf.release(); ctx->rhsbuf.release(); ctx->srcbuf.release();
@@ -658,7 +674,7 @@ int sieb200_profile_enable(sieb200_ctx* ctx, int enable) {
 
 int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,
                          double* flops, double* bytes) {
-    SIEB_CHECK(ctx && kernel >= 0 && kernel < 3, SIEB200_INVALID_ARG, "invalid profile query");
+    SIEB_CHECK(ctx && kernel >= 0 && kernel < Profiler::kKinds, SIEB200_INVALID_ARG, "invalid profile query");
     ctx->prof.collect();
     const KernelProfile& k = ctx->prof.k[kernel];
     if (launches) *launches = k.launches;

@@ -103,7 +103,9 @@ struct Profiler {
         double flops, bytes;
     };
     std::vector<Pending> pending;
-    KernelProfile k[3];
+    std::vector<cudaEvent_t> pool;  // events reused across collections
+    static constexpr int kKinds = 8;
+    KernelProfile k[kKinds];
     // Returns an event pair recorded around a launch (nullptr events when off).
     void begin(cudaStream_t s, int kernel, double flops, double bytes, cudaEvent_t* end_out);
     void end(cudaStream_t s, cudaEvent_t e);

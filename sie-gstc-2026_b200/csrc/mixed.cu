@@ -39,7 +39,7 @@ constexpr int NB = 64;  // LU block size (complex columns)
 // Dynamic shared memory of the block kernels (two NB x (NB+1) complex64
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
-constexpr int kSmemPanel = (NB + 32) * (NB + 1) * (int)sizeof(float2);
+constexpr int kSmemPanel = (NB * (NB + 4) + 32 * (NB + 1)) * (int)sizeof(float2);
 constexpr int kDiagThreads = 1024;  // diagonal-block kernel: 16 column groups of NB rows
 static_assert(kDiagThreads % NB == 0 && NB % (kDiagThreads / NB) == 0, "diag thread layout");
 
@@ -350,40 +350,46 @@ __device__ __forceinline__ float tf32_hi(float x) {
 
 // L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
 // writes L21 back into W and the split realified rows into Apack.
-// One CTA per 32 rows; inv(U11) staged in shared memory.
+// One CTA per 32 rows. Thread (ty, tx) computes rows 2ty, 2ty+1 and columns
+// 4tx .. 4tx+3 with k outermost; inv(U11) is upper triangular, so the k
+// loop stops at the thread's last column (tx is warp-uniform up to a pair).
 __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
                                              int64_t r0, int64_t np, const float2* __restrict__ Uinv,
                                              float* __restrict__ Apack, int pack, int bx) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    float2(*Ui)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
-    float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [row][col], 32 rows
+    float2(*Us)[NB + 4] = reinterpret_cast<float2(*)[NB + 4]>(dyn_smem);                       // [k][c]
+    float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * 8);   // [row][k]
     const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) Ui[e / NB][e % NB] = Uinv[e];
+    for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];  // Uinv[k + c*NB]
     const int64_t rb = r0 + (int64_t)bx * 32;
-    for (int e = tid; e < 32 * kb; e += blockDim.x) {
+    for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % 32, c = e / 32;
         const int64_t gr = rb + r;
-        Ar[r][c] = gr < np ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+        Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    const int K3 = 6 * NB;
-    // L21 rows into registers (thread: row r, columns c = cg + 8u)...
-    const int r = tid & 31, cg = tid >> 5;
-    float2 res[NB / 8];
+    const int ty = tid & 15, tx = tid >> 4;
+    float2 acc[2][4];
 #pragma unroll
-    for (int u = 0; u < NB / 8; ++u) {
-        const int c = cg + 8 * u;
-        float2 s = make_float2(0.f, 0.f);
-        if (c < kb)
-            for (int k = 0; k <= c; ++k)
-                s = make_float2(s.x + Ar[r][k].x * Ui[c][k].x - Ar[r][k].y * Ui[c][k].y,
-                                s.y + Ar[r][k].x * Ui[c][k].y + Ar[r][k].y * Ui[c][k].x);
-        res[u] = s;
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+    const int kend = min(kb, 4 * tx + 4);
+    for (int k = 0; k < kend; ++k) {
+        const float2 a0 = Ar[2 * ty][k], a1 = Ar[2 * ty + 1][k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float2 u = Us[k][4 * tx + j];
+            acc[0][j] = make_float2(acc[0][j].x + a0.x * u.x - a0.y * u.y, acc[0][j].y + a0.x * u.y + a0.y * u.x);
+            acc[1][j] = make_float2(acc[1][j].x + a1.x * u.x - a1.y * u.y, acc[1][j].y + a1.x * u.y + a1.y * u.x);
+        }
     }
     __syncthreads();
-    // ... back through shared memory (zero beyond kb) ...
+    // ... back through shared memory ...
 #pragma unroll
-    for (int u = 0; u < NB / 8; ++u) Ar[r][cg + 8 * u] = res[u];
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) Ar[2 * ty + i][4 * tx + j] = acc[i][j];
     __syncthreads();
     // ... to W (rows fastest: coalesced columns) ...
     for (int e = tid; e < 32 * kb; e += blockDim.x) {
@@ -394,14 +400,15 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
     if (!pack) return;
     // ... and to the split realified rows (K fastest: coalesced rows).
     // row 2i: [Re, -Im] per column, row 2i+1: [Im, Re]; layout [hi | hi | lo].
+    const int K3 = 6 * NB;
     for (int e = tid; e < 32 * 2 * NB; e += blockDim.x) {
         const int rr = e / (2 * NB), kk = e % (2 * NB);
         const int64_t gr = rb + rr;
         if (gr >= np) continue;
         const int c = kk >> 1, h = kk & 1;
-        const float2 s = Ar[rr][c];
-        const float v0 = h == 0 ? s.x : -s.y;   // real row
-        const float v1 = h == 0 ? s.y : s.x;    // imaginary row
+        const float2 v = Ar[rr][c];
+        const float v0 = h == 0 ? v.x : -v.y;   // real row
+        const float v1 = h == 0 ? v.y : v.x;    // imaginary row
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
         float* row0 = Apack + (2 * (gr - r0)) * K3;
         float* row1 = row0 + K3;
@@ -411,37 +418,59 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
 }
 
 // U12 = inv(L11) * A12 for columns [c0, np) of the panel rows [k0, k0+kb);
-// writes U12 back into W and the split columns into Bpack. One CTA per 32 cols.
+// writes U12 back into W and the split columns into Bpack. One CTA per 32
+// columns. Thread (ty, tx) computes rows 4ty .. 4ty+3 and columns 2tx,
+// 2tx+1 with k outermost; inv(L11) is lower triangular, so the k loop stops
+// at the thread's last row (ty is warp-uniform up to a pair).
 __device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
                                              int64_t c0, int64_t np, const float2* __restrict__ Linv,
                                              float* __restrict__ Bpack, int pack, int bx) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    float2(*Li)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);        // [col][row]
-    float2(*Ac)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;   // [col][row], 32 cols
+    float2(*Ls)[NB + 4] = reinterpret_cast<float2(*)[NB + 4]>(dyn_smem);                       // [k][r]
+    float2(*Ac)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * 8);   // [col][k]
     const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) Li[e / NB][e % NB] = Linv[e];
+    for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];  // Linv[r + k*NB]
     const int64_t cb = c0 + (int64_t)bx * 32;
-    for (int e = tid; e < 32 * kb; e += blockDim.x) {
-        const int r = e % kb, c = e / kb;
+    for (int e = tid; e < 32 * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
-        Ac[c][r] = gc < np ? W[(k0 + r) + gc * ldw] : make_float2(0.f, 0.f);
+        Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : make_float2(0.f, 0.f);
     }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    float2 acc[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j] = make_float2(0.f, 0.f);
+    const int kend = min(kb, 4 * ty + 4);
+    for (int k = 0; k < kend; ++k) {
+        const float2 b0 = Ac[2 * tx][k], b1 = Ac[2 * tx + 1][k];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 l = Ls[k][4 * ty + i];
+            acc[i][0] = make_float2(acc[i][0].x + l.x * b0.x - l.y * b0.y, acc[i][0].y + l.x * b0.y + l.y * b0.x);
+            acc[i][1] = make_float2(acc[i][1].x + l.x * b1.x - l.y * b1.y, acc[i][1].y + l.x * b1.y + l.y * b1.x);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) Ac[2 * tx + j][4 * ty + i] = acc[i][j];
     __syncthreads();
     const int K3 = 6 * NB;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
         if (gc >= np) continue;
-        float2 s = make_float2(0.f, 0.f);
-        if (r < kb)
-            for (int k = 0; k <= r; ++k) s = make_float2(s.x + Li[k][r].x * Ac[c][k].x - Li[k][r].y * Ac[c][k].y,
-                                                         s.y + Li[k][r].x * Ac[c][k].y + Li[k][r].y * Ac[c][k].x);
-        if (r < kb) W[(k0 + r) + gc * ldw] = s;
+        const float2 v = Ac[c][r];
+        if (r < kb) W[(k0 + r) + gc * ldw] = v;
         if (pack) {
             float* col = Bpack + (gc - c0) * K3;
-            const float h0 = tf32_hi(s.x), h1 = tf32_hi(s.y);
+            const float h0 = tf32_hi(v.x), h1 = tf32_hi(v.y);
             col[2 * r] = h0; col[2 * r + 1] = h1;
-            col[2 * NB + 2 * r] = s.x - h0; col[2 * NB + 2 * r + 1] = s.y - h1;
+            col[2 * NB + 2 * r] = v.x - h0; col[2 * NB + 2 * r + 1] = v.y - h1;
             col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
         }
     }
@@ -526,7 +555,7 @@ constexpr int TR_DLD = NB + 4;        // staged inverses [col][row]: conflict-fr
 constexpr int TR_CONSUMERS = 256;
 constexpr int TR_THREADS = TR_CONSUMERS + 32;
 constexpr int kSmemTrsv = 1024 + TR_STAGES * TR_TILE_BYTES + 2 * NB * TR_DLD * 8 +
-                          (2 * TR_ROWS + NB) * (int)sizeof(cplx) + 2 * TR_STAGES * 8;
+                          (2 * TR_ROWS + 3 * NB) * (int)sizeof(cplx) + 2 * TR_STAGES * 8;
 
 __device__ __forceinline__ void consumer_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
@@ -552,7 +581,8 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     cplx* red = reinterpret_cast<cplx*>(Ds + 2 * NB * TR_DLD);                  // TR_ROWS
     cplx* ys = red + TR_ROWS;                                                      // TR_ROWS
     cplx* xs = ys + TR_ROWS;                                                       // NB
-    const uint32_t full0 = smem_u32(xs + NB), empty0 = full0 + 8 * TR_STAGES;
+    cplx* xstage = xs + NB;                                                        // 2 x NB
+    const uint32_t full0 = smem_u32(xstage + 2 * NB), empty0 = full0 + 8 * TR_STAGES;
     __shared__ int s_t, s_go;
     __shared__ volatile int s_abort;
 
@@ -622,61 +652,71 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     cplx b = cx(0, 0);  // written only by this CTA: final from the start
     if (h == 0 && grow < np) b = cx(__ldcg(&x[grow].re), __ldcg(&x[grow].im));
     double acc_re = 0.0, acc_im = 0.0;
+    // Off-diagonal tiles in groups of one NB sub-block (two tiles, or one at
+    // a ragged end): warp 0 waits until the sub-block is published and
+    // stages its NB x entries in shared memory (double-buffered by group
+    // parity), so both tiles cost one L2 round trip; one consumer barrier
+    // per group hands them to all warps.
     unsigned seen = 0;
-    for (int i = 0; i < n_off; ++i) {
-        const int st = i % TR_STAGES;
-        const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
-        const int k = tile_k(i);
-        const int sb = (k * TR_COLS) / NB;
+    for (int i = 0, g = 0; i < n_off; ++g) {
+        const int sb = (tile_k(i) * TR_COLS) / NB;
+        const int cnt = (i + 1 < n_off && (tile_k(i + 1) * TR_COLS) / NB == sb) ? 2 : 1;
         const unsigned need = lower ? (unsigned)sb + 1u : (unsigned)(nsb - sb);
-        bool ok = !s_abort;
-        if (ok && seen < need) {
-            if (lane == 0) {
-                int it = 0;
-                unsigned p = seen;
-                while (true) {
-                    p = ld_acquire_gpu(&progress[0]);
-                    if (p >= need) break;
-                    if (need - p > 4) __nanosleep(256);
-                    if ((++it & 63) == 0 &&
-                        (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
-                        atomicCAS(err, 0u, 2u);
-                        s_abort = 1;
-                        break;
+        cplx* xg = xstage + (g & 1) * NB;
+        if (warp == 0) {
+            bool okp = !s_abort;
+            if (okp && seen < need) {
+                if (lane == 0) {
+                    int it = 0;
+                    unsigned p = seen;
+                    while (true) {
+                        p = ld_acquire_gpu(&progress[0]);
+                        if (p >= need) break;
+                        if (need - p > 4) __nanosleep(256);
+                        if ((++it & 63) == 0 &&
+                            (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
+                            atomicCAS(err, 0u, 2u);
+                            s_abort = 1;
+                            break;
+                        }
                     }
+                    seen = p;
                 }
-                seen = p;
+                seen = __shfl_sync(0xffffffffu, seen, 0);
+                okp = seen >= need;
+                __syncwarp();
             }
-            seen = __shfl_sync(0xffffffffu, seen, 0);
-            ok = seen >= need;
+            for (int e = lane; e < NB; e += 32) {
+                const int64_t c = (int64_t)sb * NB + e;
+                xg[e] = (okp && c < np) ? cx(__ldcg(&x[c].re), __ldcg(&x[c].im)) : cx(0, 0);
+            }
+        }
+        consumer_bar();
+        for (int j = 0; j < cnt; ++j, ++i) {
+            const int st = i % TR_STAGES;
+            const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
+            // Every issued tile is waited for and released, also after an
+            // abort, so that no copy is in flight when the CTA exits.
+            bool ok = !s_abort;
+            if (!tr_wait(full0 + 8 * st, ph, deadline)) {
+                if (lane == 0) atomicCAS(err, 0u, 2u);
+                s_abort = 1;
+                ok = false;
+            }
+            if (ok) {
+                const float2* tile = ringp + st * TR_TILE;
+                const cplx* xt = xg + (tile_k(i) * TR_COLS - sb * NB) + h * 16;
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const float2 w = tile[(h * 16 + u) * TR_ROWS + r];
+                    const cplx xv = xt[u];
+                    acc_re += (double)w.x * xv.re - (double)w.y * xv.im;
+                    acc_im += (double)w.x * xv.im + (double)w.y * xv.re;
+                }
+            }
             __syncwarp();
+            if (lane == 0) mbar_arrive(empty0 + 8 * st);
         }
-        // Every issued tile is waited for and released, also after an abort,
-        // so that no copy is in flight when the CTA exits.
-        if (!tr_wait(full0 + 8 * st, ph, deadline)) {
-            if (lane == 0) atomicCAS(err, 0u, 2u);
-            s_abort = 1;
-            ok = false;
-        }
-        if (ok) {
-            const float2* tile = ringp + st * TR_TILE;
-            const int64_t c0 = (int64_t)k * TR_COLS + h * 16;
-            double xr[16], xi[16];
-#pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                const bool in = c0 + u < np;
-                xr[u] = in ? __ldcg(&x[c0 + u].re) : 0.0;
-                xi[u] = in ? __ldcg(&x[c0 + u].im) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 16; ++u) {
-                const float2 w = tile[(h * 16 + u) * TR_ROWS + r];
-                acc_re += (double)w.x * xr[u] - (double)w.y * xi[u];
-                acc_im += (double)w.x * xi[u] + (double)w.y * xr[u];
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty0 + 8 * st);
     }
     if (h == 1) red[r] = cx(acc_re, acc_im);
     consumer_bar();
@@ -938,6 +978,8 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
         attrs_set = true;
     }
+    cudaEvent_t ev_fact;
+    ctx->prof.begin(stream, 6, (8.0 / 3.0) * 4.0 * (double)np * np * np, 0.0, &ev_fact);
     SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
     rbt_init_kernel<<<blocks_for(8 * np, 256), 256, 0, stream>>>(st->diag, np, 0x5EB200ull);
     SIEB_NOTE_LAUNCH();
@@ -952,15 +994,20 @@ int mixed_factorize(DenseSolver* s) {
     auto diag_and_L = [&](int64_t bk, cudaStream_t sm) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
+        cudaEvent_t ev;
+        ctx->prof.begin(sm, 3, 8.0 * NB * NB * NB, 3.0 * 8.0 * NB * NB, &ev);
         diag_lu_kernel<<<1, kDiagThreads, kSmemDiag, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
                                                             st->Uinv + (size_t)bk * NB * NB, st->err);
         SIEB_NOTE_LAUNCH();
+        ctx->prof.end(sm, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
         const int64_t s0 = k0 + kb;
         if (s0 < np) {
+            ctx->prof.begin(sm, 4, 4.0 * NB * NB * (double)(np - s0), 8.0 * 2.0 * NB * (double)(np - s0), &ev);
             panel_L_kernel<<<(unsigned)blocks_for(np - s0, 32), 256, kSmemPanel, sm>>>(
                 st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Apack[bk & 1], st->use_tc);
             SIEB_NOTE_LAUNCH();
+            ctx->prof.end(sm, ev);
             SIEB_TRY_CUDA(cudaGetLastError());
         }
         return SIEB200_OK;
@@ -986,9 +1033,12 @@ int mixed_factorize(DenseSolver* s) {
         const int64_t s0 = k0 + kb;
         if (s0 >= np) break;
         const int64_t m = np - s0;
+        cudaEvent_t evu;
+        ctx->prof.begin(stream, 5, 4.0 * NB * NB * (double)m, 8.0 * 2.0 * NB * (double)m, &evu);
         panel_U_kernel<<<(unsigned)blocks_for(m, 32), 256, kSmemPanel, stream>>>(
             st->W, ldw, k0, kb, s0, np, st->Linv + (size_t)bk * NB * NB, st->Bpack, st->use_tc);
         SIEB_NOTE_LAUNCH();
+        ctx->prof.end(stream, evu);
         SIEB_TRY_CUDA(cudaGetLastError());
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
@@ -1008,6 +1058,7 @@ int mixed_factorize(DenseSolver* s) {
             SIEB_RETURN_IF(diag_and_L(bk + 1, stream));
         }
     }
+    ctx->prof.end(stream, ev_fact);
     return check_err(s, "mixed LU factorization");
 }
 
@@ -1239,7 +1290,10 @@ int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoi
     int total = 0;
     for (int64_t c = 0; c < nrhs; ++c) {
         int it = 0;
+        cudaEvent_t ev;
+        s->ctx->prof.begin(s->ctx->stream, 7, 0.0, 0.0, &ev);
         const int st = gmres_ir(s, reinterpret_cast<cplx*>(B) + c * ldb, ldb, tol, maxit, &it);
+        s->ctx->prof.end(s->ctx->stream, ev);
         total = std::max(total, it);
         if (st != SIEB200_OK) {
             if (iters) *iters = total;

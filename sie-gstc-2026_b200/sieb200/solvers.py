@@ -161,7 +161,9 @@ class Context:
         _lib.check(_lib.lib().sieb200_profile_enable(self._h, int(bool(enable))))
 
     def profile_read(self, kernel: int) -> dict:
-        """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec."""
+        """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec,
+        3: diagonal-block LU, 4: L21 panels, 5: U12 panels, 6: whole mixed
+        factorizations, 7: whole refined solves."""
         n = ctypes.c_int64()
         ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _lib.check(_lib.lib().sieb200_profile_read(self._h, int(kernel), ctypes.byref(n), ctypes.byref(ms),
