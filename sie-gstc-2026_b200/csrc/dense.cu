@@ -63,7 +63,50 @@ __global__ void gemv_finish_kernel(int64_t n, int chunks, const cplx* __restrict
     y[i] = s;
 }
 
+// y = A^H x (+ beta y): one warp per output entry, reading column i of the
+// column-major A contiguously; FP64 accumulation, warp-shuffle reduction.
+template <class TA>
+__global__ void gemv_h_kernel(int64_t n, const TA* __restrict__ A, int64_t lda, const cplx* __restrict__ x,
+                              double beta, cplx* __restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;  // warp-uniform
+    const TA* col = A + i * lda;
+    double re = 0.0, im = 0.0;
+    for (int64_t k = lane; k < n; k += 32) {
+        const TA a = col[k];
+        const cplx xv = x[k];
+        // conj(a) * x
+        re += (double)a.x * xv.re + (double)a.y * xv.im;
+        im += (double)a.x * xv.im - (double)a.y * xv.re;
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) {
+        const cplx old = beta != 0.0 ? y[i] * beta : cx(0, 0);
+        y[i] = cx(old.re + re, old.im + im);
+    }
+}
+
 }  // namespace
+
+int gemv_h_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, const cplx* x, double beta,
+                  cplx* y) {
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((n + 7) / 8);
+    cudaEvent_t ev;
+    ctx->prof.begin(ctx->stream, 2, 8.0 * (double)n * (double)n, 16.0 * (double)n * (double)n + 16.0 * 3.0 * n,
+                    &ev);
+    gemv_h_kernel<double2><<<blocks, threads, 0, ctx->stream>>>(n, static_cast<const double2*>(A), lda, x, beta,
+                                                                 y);
+    SIEB_NOTE_LAUNCH();
+    ctx->prof.end(ctx->stream, ev);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
 
 int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec, const cplx* x,
                 double beta, cplx* y, DeviceBuffer& scratch) {

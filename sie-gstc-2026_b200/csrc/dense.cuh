@@ -36,6 +36,9 @@ void mixed_release(DenseSolver* s);
 
 int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec, const cplx* x,
                 double beta, cplx* y, DeviceBuffer& scratch);
+// y = A^H x (+ beta y), A complex128 column-major.
+int gemv_h_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, const cplx* x, double beta,
+                  cplx* y);
 // Same product with its partial sums in a fixed device array (no allocation).
 int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                                const cplx* x, double beta, cplx* y);

@@ -60,6 +60,14 @@ struct MixedState {
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
     int64_t tm_np = 0;
+    // Conjugate-transpose solves (W^H = U^H L^H): W^H and the conjugate
+    // transposes of the diagonal-block inverses, built on first use after a
+    // factorization (in the solver's panel workspace).
+    bool adj_ready = false;
+    float2* WH = nullptr;
+    float2* LinvH = nullptr;
+    float2* UinvH = nullptr;
+    CUtensorMap tmWH;
     cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
     cudaEvent_t ev_cols = nullptr, ev_panel = nullptr;
 };
@@ -880,6 +888,17 @@ __global__ void conj_transpose_c64_kernel(const float2* __restrict__ W, int64_t 
     }
 }
 
+// Conjugate transpose of each NB x NB block (column-major) of `in`, one CTA per block.
+__global__ void conj_transpose_blocks_kernel(const float2* __restrict__ in, float2* __restrict__ out) {
+    const float2* src = in + (size_t)blockIdx.x * NB * NB;
+    float2* dst = out + (size_t)blockIdx.x * NB * NB;
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
+        const float2 v = src[c + r * NB];
+        dst[e] = make_float2(v.x, -v.y);
+    }
+}
+
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -937,6 +956,7 @@ int mixed_factorize(DenseSolver* s) {
     const int64_t ldw = ((np + 31) / 32) * 32;
     const int64_t nbl = (np + NB - 1) / NB;
     st->n = n; st->np = np; st->ldw = ldw; st->nbl = nbl;
+    st->adj_ready = false;
     const char* env = getenv("SIEB200_TRAILING_SIMT");
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
 
@@ -1062,7 +1082,8 @@ int mixed_factorize(DenseSolver* s) {
     return check_err(s, "mixed LU factorization");
 }
 
-// Apply M^{-1} = V U^{-1} L^{-1} U^T to r (length n) into z (length n).
+// Apply M^{-1} = V U^{-1} L^{-1} U^T (or its conjugate transpose) to r
+// (length n) into z (length n).
 static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, bool adjoint) {
     MixedState* st = state_of(s);
     cudaStream_t stream = s->ctx->stream;
@@ -1077,41 +1098,59 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     SIEB_TRY_CUDA(cudaGetLastError());
     unsigned* fl = st->tri_flags;
     const int nbl = (int)st->nbl;
-    if (!adjoint) {
-        if (st->tm_base != st->W || st->tm_np != np) {
-            // W as 8-byte elements: rows inner, 128 x 32 boxes; rows/columns
-            // beyond np read as zero.
-            SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->W, (uint64_t)np,
-                                                (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
-                                                TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
-            st->tm_base = st->W;
-            st->tm_np = np;
-        }
-        static bool attr_set = false;
-        if (!attr_set) {
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               kSmemTrsv));
-            attr_set = true;
-        }
-        const unsigned ncta = (unsigned)((np + TR_ROWS - 1) / TR_ROWS);
-        const unsigned long long timeout_ns = 2000000000ull;
-        // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
-        const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
-        for (int lower = 1; lower >= 0; --lower) {
-            SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * 2, stream));
-            cudaEvent_t ev;
-            s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
-            trsv_tma_kernel<<<ncta, TR_THREADS, kSmemTrsv, stream>>>(st->tmW, np, nbl, lower,
-                                                                     lower ? st->Linv : st->Uinv, work, fl,
-                                                                     st->err, timeout_ns);
-            SIEB_NOTE_LAUNCH();
-            s->ctx->prof.end(stream, ev);
-            SIEB_TRY_CUDA(cudaGetLastError());
-        }
-    } else {
-        // W^H y = c  <=>  conj(W)^T y = c: solve with conj on both sides using
-        // the transposed factors held in s->panel (built on first use).
-        return SIEB200_INVALID_ARG;
+    if (st->tm_base != st->W || st->tm_np != np) {
+        // W as 8-byte elements: rows inner, 128 x 32 boxes; rows/columns
+        // beyond np read as zero.
+        SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->W, (uint64_t)np,
+                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
+                                            TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
+        st->tm_base = st->W;
+        st->tm_np = np;
+    }
+    if (adjoint && !st->adj_ready) {
+        // W^H y = c is U^H (lower) then L^H (unit upper): the same two block
+        // solves on the conjugate transpose of W, with the conjugate
+        // transposes of the diagonal-block inverses.
+        const size_t bW = ((sizeof(float2) * st->ldw * np + 255) / 256) * 256;
+        const size_t bInv = sizeof(float2) * NB * NB * nbl;
+        SIEB_RETURN_IF(s->panel.reserve(bW + 2 * bInv));
+        st->WH = s->panel.as<float2>();
+        st->LinvH = reinterpret_cast<float2*>(s->panel.as<char>() + bW);
+        st->UinvH = st->LinvH + (size_t)NB * NB * nbl;
+        conj_transpose_c64_kernel<<<dim3(blocks_for(np, 32), blocks_for(np, 32)), dim3(32, 8), 0, stream>>>(
+            st->W, st->ldw, np, st->WH);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        conj_transpose_blocks_kernel<<<nbl, 256, 0, stream>>>(st->Linv, st->LinvH);
+        SIEB_NOTE_LAUNCH();
+        conj_transpose_blocks_kernel<<<nbl, 256, 0, stream>>>(st->Uinv, st->UinvH);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmWH, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->WH, (uint64_t)np,
+                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
+                                            TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
+        st->adj_ready = true;
+    }
+    static bool attr_set = false;
+    if (!attr_set) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemTrsv));
+        attr_set = true;
+    }
+    const unsigned ncta = (unsigned)((np + TR_ROWS - 1) / TR_ROWS);
+    const unsigned long long timeout_ns = 2000000000ull;
+    // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
+    const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
+    for (int lower = 1; lower >= 0; --lower) {
+        const float2* dinv = adjoint ? (lower ? st->UinvH : st->LinvH) : (lower ? st->Linv : st->Uinv);
+        SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * 2, stream));
+        cudaEvent_t ev;
+        s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
+        trsv_tma_kernel<<<ncta, TR_THREADS, kSmemTrsv, stream>>>(adjoint ? st->tmWH : st->tmW, np, nbl, lower,
+                                                                 dinv, work, fl, st->err, timeout_ns);
+        SIEB_NOTE_LAUNCH();
+        s->ctx->prof.end(stream, ev);
+        SIEB_TRY_CUDA(cudaGetLastError());
     }
     rbt_vec_N_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(work, n, np, d_last, z);
     SIEB_NOTE_LAUNCH();
@@ -1125,11 +1164,12 @@ static double host_norm2(const std::vector<cplx>& v) {
     return std::sqrt((double)s);
 }
 
-// Restarted flexible GMRES on A x = b (FP64, A the intact complex128 matrix)
+// Restarted flexible GMRES on A x = b or A^H x = b (FP64, A the intact complex128 matrix)
 // with right preconditioner M^{-1}, started from x = 0. The preconditioned
 // directions z_j = M^{-1} v_j are kept, so the update x += Z y costs no
 // further preconditioner application.
-static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int maxit, int* iters) {
+static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int maxit, bool adjoint,
+                    int* iters) {
     (void)ldb_unused;
     MixedState* st = state_of(s);
     sieb200_ctx* ctx = s->ctx;
@@ -1169,7 +1209,10 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
             SIEB_NOTE_LAUNCH();
         } else {
             SIEB_TRY_CUDA(cudaMemcpyAsync(r, b, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, stream));
-            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));
+            if (adjoint)
+                SIEB_RETURN_IF(gemv_h_device(ctx, n, A, lda, x, -1.0, r));
+            else
+                SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, x, -1.0, r, s->gemv_scratch));
         }
         dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, r, n, r, partial);
         SIEB_NOTE_LAUNCH();
@@ -1199,8 +1242,11 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         for (; j < m && total < maxit; ++j, ++total) {
             cplx* vj = V + (int64_t)j * n;
             cplx* zj = Zb + (int64_t)j * n;
-            SIEB_RETURN_IF(apply_precond(s, vj, zj, work, false));
-            SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
+            SIEB_RETURN_IF(apply_precond(s, vj, zj, work, adjoint));
+            if (adjoint)
+                SIEB_RETURN_IF(gemv_h_device(ctx, n, A, lda, zj, 0.0, w));
+            else
+                SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
             // Classical Gram-Schmidt with one reorthogonalization (CGS2).
             for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
             for (int pass = 0; pass < 2; ++pass) {
@@ -1284,7 +1330,6 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
 int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
                 int maxit, int* iters) {
     SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG, "unsupported solver method");
-    SIEB_CHECK(!adjoint, SIEB200_INVALID_ARG, "adjoint solve of the mixed method is not available yet");
     if (!(tol > 0)) tol = 1e-10;
     if (maxit <= 0) maxit = 50;
     int total = 0;
@@ -1292,7 +1337,7 @@ int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoi
         int it = 0;
         cudaEvent_t ev;
         s->ctx->prof.begin(s->ctx->stream, 7, 0.0, 0.0, &ev);
-        const int st = gmres_ir(s, reinterpret_cast<cplx*>(B) + c * ldb, ldb, tol, maxit, &it);
+        const int st = gmres_ir(s, reinterpret_cast<cplx*>(B) + c * ldb, ldb, tol, maxit, adjoint, &it);
         s->ctx->prof.end(s->ctx->stream, ev);
         total = std::max(total, it);
         if (st != SIEB200_OK) {
