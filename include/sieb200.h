@@ -188,6 +188,19 @@ int sieb200_assemble_rhs(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb2
                          const sieb200_source* sources, int num_sources, double* B,
                          int b_on_device);
 
+/* Adjoint contraction of the SIE-GSTC system with respect to its per-face
+ * tensor records (no counterpart in the reference, which has no adjoint):
+ * s[32 f + k] = lambda^H (dZ / d record[f][k]) x, with record[f] the 32
+ * complex values of face f (Lambda row-major, then its inverse) and Z the
+ * eta0-scaled matrix sieb200_assemble_matrix builds. Z is linear in the
+ * records (only the jump-condition mass blocks of face f depend on
+ * record[f]). With lambda solving Z^H lambda = dL/dx (torch convention,
+ * x.grad), dL/d record = -conj(s). lambda, x: 4*num_edges complex; s_out:
+ * 32*num_faces complex (for uniform tensors sum over faces); device memory
+ * when on_device != 0, else host. */
+int sieb200_gstc_tensor_gradient(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                                 const double* lambda, const double* x, int on_device, double* s_out);
+
 /* ---------------------------------------------------------- dense LA ---- */
 /* DenseLuSolver (include/sie_mom/cuda/dense_lu_solver.cuh:17-184) as an
  * object: factorize a device complex128 matrix with the selected method, then
@@ -263,6 +276,15 @@ int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* 
                       const double* m_cur, double k0, double eta0, int64_t ndir,
                       const double* r_hat, const double* theta_hat, const double* phi_hat,
                       double* f_theta, double* f_phi, double* intensity);
+
+/* The same far field as an explicit operator, for differentiable objectives
+ * (no counterpart in the reference): A is (2*ndir) x (2*num_edges) complex,
+ * row-major, rows F_theta(d) then F_phi(d), columns J(e) then M(e) of the
+ * exterior currents, so that [F_theta; F_phi] = A [J; M]. Directions: host;
+ * A: device memory when a_on_device != 0, else host. */
+int sieb200_far_field_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, double k0, double eta0, int64_t ndir,
+                             const double* r_hat, const double* theta_hat, const double* phi_hat, int a_on_device,
+                             double* A);
 
 #ifdef __cplusplus
 }

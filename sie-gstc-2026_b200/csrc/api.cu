@@ -20,6 +20,8 @@
 
 namespace sieb200 {
 
+int far_field_matrix_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, double k0, double eta0, int64_t ndir,
+                            const double* rh, const double* th, const double* ph, cplx* dA);
 int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j_cur,
                      const double* m_cur, double k0, double eta0, int64_t ndir, const double* rh,
                      const double* th, const double* ph, double* f_theta, double* f_phi,
@@ -580,6 +582,34 @@ int sieb200_assemble_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, const si
     return SIEB200_OK;
 }
 
+int sieb200_gstc_tensor_gradient(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                                 const double* lambda, const double* x, int on_device, double* s_out) {
+    SIEB_RETURN_IF(validate(mesh, opt, nullptr, false));
+    SIEB_CHECK(ctx && lambda && x && s_out, SIEB200_INVALID_ARG, "invalid gradient arguments");
+    SIEB_CHECK(opt->formulation == SIEB200_GSTC, SIEB200_INVALID_ARG,
+               "the tensor gradient exists for the GSTC formulation only");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    const int64_t N = system_dimension(opt->formulation, mesh->num_edges);
+    const int64_t ns = 32 * mesh->num_faces;
+    if (on_device) {
+        SIEB_RETURN_IF(tensor_gradient_device(ctx, *mesh, *opt, reinterpret_cast<const cplx*>(lambda),
+                                              reinterpret_cast<const cplx*>(x), reinterpret_cast<cplx*>(s_out)));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+        return SIEB200_OK;
+    }
+    DeviceBuffer tmp;
+    SIEB_RETURN_IF(tmp.reserve(sizeof(cplx) * (2 * N + ns)));
+    cplx* dl = tmp.as<cplx>();
+    cplx* dx = dl + N;
+    cplx* ds = dx + N;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dl, lambda, sizeof(cplx) * N, cudaMemcpyHostToDevice, ctx->stream));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dx, x, sizeof(cplx) * N, cudaMemcpyHostToDevice, ctx->stream));
+    SIEB_RETURN_IF(tensor_gradient_device(ctx, *mesh, *opt, dl, dx, ds));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(s_out, ds, sizeof(cplx) * ns, cudaMemcpyDeviceToHost, ctx->stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
 int sieb200_assemble_rhs(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
                          const sieb200_source* sources, int num_sources, double* B, int b_on_device) {
     SIEB_RETURN_IF(validate(mesh, opt, nullptr, false));
@@ -709,6 +739,26 @@ int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* 
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     return far_field_device(ctx, *mesh, j_cur, m_cur, k0, eta0, ndir, r_hat, theta_hat, phi_hat,
                             f_theta, f_phi, intensity);
+}
+
+int sieb200_far_field_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, double k0, double eta0, int64_t ndir,
+                             const double* r_hat, const double* theta_hat, const double* phi_hat, int a_on_device,
+                             double* A) {
+    SIEB_CHECK(ctx && mesh && mesh->vertices && mesh->faces && mesh->faces_edges && A && r_hat && theta_hat &&
+                   phi_hat && ndir > 0 && ndir < (1 << 24) && mesh->num_edges > 0,
+               SIEB200_INVALID_ARG, "invalid far-field matrix arguments");
+    SIEB_CHECK(k0 > 0 && eta0 > 0, SIEB200_INVALID_ARG, "k0 and eta0 must be positive");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    if (a_on_device)
+        return sieb200::far_field_matrix_device(ctx, *mesh, k0, eta0, ndir, r_hat, theta_hat, phi_hat,
+                                                reinterpret_cast<sieb200::cplx*>(A));
+    const size_t bytes = sizeof(sieb200::cplx) * 2 * (size_t)ndir * 2 * (size_t)mesh->num_edges;
+    sieb200::DeviceBuffer tmp;
+    SIEB_RETURN_IF(tmp.reserve(bytes));
+    SIEB_RETURN_IF(sieb200::far_field_matrix_device(ctx, *mesh, k0, eta0, ndir, r_hat, theta_hat, phi_hat,
+                                                    tmp.as<sieb200::cplx>()));
+    SIEB_TRY_CUDA(cudaMemcpy(A, tmp.ptr, bytes, cudaMemcpyDeviceToHost));
+    return SIEB200_OK;
 }
 
 }  // extern "C"

@@ -463,16 +463,13 @@ __global__ void pair_singular_kernel(const FaceGeom* __restrict__ geom, const d3
 }
 
 // ------------------------------------------------------------ GSTC mass --
-// One thread per (face, tensor t in 0..7): tensors 0..3 are the Y blocks
-// (ee, em, me, mm) after the perp transform, 4..7 the Z blocks.
-__global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
-                                 const float* __restrict__ qw_g, int Q, int nf,
-                                 const cplx* __restrict__ tensors, int uniform, int basis,
-                                 cplx* __restrict__ mass) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= nf * 8) return;
-    const int f = id >> 3, t = id & 7;
-    const FaceGeom g = geom[f];
+// Mass block of tensor t (0..3: the Y blocks ee, em, me, mm after the perp
+// transform; 4..7 the Z blocks) of face g for the 2x2 tensor block
+// (t00 t01; t10 t11): out[j*3+i] for local test edge j and source edge i.
+// Linear in the four tensor entries.
+__device__ void mass_tensor_block(const FaceGeom& g, const d3* __restrict__ qpf, const float* __restrict__ qw_g,
+                                  int Q, int basis, int t, cplx t00, cplx t01, cplx t10, cplx t11,
+                                  cplx (&out)[9]) {
     // Frame: gstc_tensor_utils.cuh:72-147.
     d3 u, w;
     if (basis == 0) {
@@ -502,10 +499,6 @@ __global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __
         }
     }
     // Lift the 2x2 block (gstc_tensor_utils.cuh:184-238).
-    const cplx* tp = tensors + (uniform ? 0 : (size_t)f * 32) + (t >= 4 ? 16 : 0);
-    const int blk = t & 3, r0 = (blk >> 1) * 2, c0 = (blk & 1) * 2;
-    const cplx t00 = tp[r0 * 4 + c0], t01 = tp[r0 * 4 + c0 + 1];
-    const cplx t10 = tp[(r0 + 1) * 4 + c0], t11 = tp[(r0 + 1) * 4 + c0 + 1];
     const double uc[3] = {u.x, u.y, u.z}, wc[3] = {w.x, w.y, w.z};
     cplx T[3][3];
 #pragma unroll
@@ -555,7 +548,7 @@ __global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __
     for (int e = 0; e < 9; ++e) R[e] = cx(0, 0);
     for (int p = 0; p < Q; ++p) {
         const double wp = (double)qw_g[p];
-        const d3 rp = qp[(size_t)f * Q + p];
+        const d3 rp = qpf[p];
         d3 rho[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) rho[i] = rp - g.fv[i];
@@ -576,8 +569,102 @@ __global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const float fs = __fmul_rn(__fmul_rn(sc, el[j]), el[i]);
-            mass[((size_t)f * 8 + t) * 9 + j * 3 + i] = R[j * 3 + i] * (double)fs;
+            out[j * 3 + i] = R[j * 3 + i] * (double)fs;
         }
+}
+
+// One thread per (face, tensor t in 0..7).
+__global__ void mass_face_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                 const float* __restrict__ qw_g, int Q, int nf,
+                                 const cplx* __restrict__ tensors, int uniform, int basis,
+                                 cplx* __restrict__ mass) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nf * 8) return;
+    const int f = id >> 3, t = id & 7;
+    const cplx* tp = tensors + (uniform ? 0 : (size_t)f * 32) + (t >= 4 ? 16 : 0);
+    const int blk = t & 3, r0 = (blk >> 1) * 2, c0 = (blk & 1) * 2;
+    cplx out[9];
+    mass_tensor_block(geom[f], qp + (size_t)f * Q, qw_g, Q, basis, t, tp[r0 * 4 + c0], tp[r0 * 4 + c0 + 1],
+                      tp[(r0 + 1) * 4 + c0], tp[(r0 + 1) * 4 + c0 + 1], out);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) mass[((size_t)f * 8 + t) * 9 + e] = out[e];
+}
+
+// A_M'' block pattern of the 8 mass values of one (test, source) edge pair
+// with the 1/2 and 1/8 factors and the eta0 scales of the M rows/columns
+// (sie_kernels_assembly.cuh:565-592), added into the 4x4 region block.
+__device__ __forceinline__ void add_mass_pattern(const cplx (&mv)[8], double me, double me2, cplx (&blk)[4][4]) {
+    const cplx Yee = mv[0], Yem = mv[1], Yme = mv[2], Ymm = mv[3];
+    const cplx Zee = mv[4], Zem = mv[5], Zme = mv[6], Zmm = mv[7];
+    const double f = 0.5, fq = 0.125;
+    const cplx ap = Zee * f + Ymm * fq, am = Zee * f - Ymm * fq;
+    const cplx bp = Zem * f + Yme * fq, bm = Zem * f - Yme * fq;
+    const cplx cp = Zme * f + Yem * fq, cm = Zme * f - Yem * fq;
+    const cplx dp = Zmm * f + Yee * fq, dm = Zmm * f - Yee * fq;
+    const double s1 = 1.0, se_ = me, s2 = me2;
+    blk[0][0] += ap * s1; blk[0][1] += bm * se_; blk[0][2] += am * s1; blk[0][3] += bp * se_;
+    blk[1][0] += cm * se_; blk[1][1] += dp * s2; blk[1][2] += cp * se_; blk[1][3] += dm * s2;
+    blk[2][0] += am * s1; blk[2][1] += bp * se_; blk[2][2] += ap * s1; blk[2][3] += bm * se_;
+    blk[3][0] += cp * se_; blk[3][1] += dm * s2; blk[3][2] += cm * se_; blk[3][3] += dp * s2;
+}
+
+// Adjoint contraction for the GSTC tensors: s[f*32 + k] = lambda^H
+// (dZ / d record[f][k]) x, record[f] = (Lambda, Lambda^{-1}) row-major.
+// Z depends on the record only through the face's own mass blocks, and
+// linearly, so dZ / d entry is the mass block of a unit entry placed by the
+// A_M'' pattern on the face's 3 x 3 local edge pairs. One thread per (face, t).
+__global__ void tensor_grad_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                   const float* __restrict__ qw_g, int Q, int nf, int ne,
+                                   const int* __restrict__ FE, int basis, double me, double me2,
+                                   const cplx* __restrict__ lam, const cplx* __restrict__ x,
+                                   cplx* __restrict__ s_out) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= nf * 8) return;
+    const int f = id >> 3, t = id & 7;
+    // Pattern coefficients of tensor t: the 4x4 region block of a unit value.
+    cplx mv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) mv[k] = cx(k == t ? 1.0 : 0.0, 0.0);
+    cplx C[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) C[r][c] = cx(0, 0);
+    add_mass_pattern(mv, me, me2, C);
+    // G[j][i] = sum_{r,c} C[r][c] conj(lambda[e_j + r E]) x[e_i + c E].
+    const int64_t E = ne;
+    int e[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[k] = FE[3 * f + k];
+    cplx G[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            cplx acc = cx(0, 0);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const cplx lv = lam[e[j] + r * E];
+                const cplx lc = cx(lv.re, -lv.im);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc += C[r][c] * (lc * x[e[i] + c * E]);
+            }
+            G[j * 3 + i] = acc;
+        }
+    const int blk = t & 3, r0 = (blk >> 1) * 2, c0 = (blk & 1) * 2;
+    const FaceGeom g = geom[f];
+#pragma unroll 1
+    for (int ab = 0; ab < 4; ++ab) {
+        const cplx one = cx(1, 0), zero = cx(0, 0);
+        cplx out[9];
+        mass_tensor_block(g, qp + (size_t)f * Q, qw_g, Q, basis, t, ab == 0 ? one : zero, ab == 1 ? one : zero,
+                          ab == 2 ? one : zero, ab == 3 ? one : zero, out);
+        cplx sacc = cx(0, 0);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sacc += G[k] * out[k];
+        const int a = ab >> 1, b = ab & 1;
+        s_out[(size_t)f * 32 + (t >= 4 ? 16 : 0) + (r0 + a) * 4 + (c0 + b)] = sacc;
+    }
 }
 
 // ------------------------------------------------------------ gather ----
@@ -662,21 +749,7 @@ __global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __rest
             blk[o + 1][o] = cx(-jm.re, -jm.im);
             blk[o + 1][o + 1] = P.c_mm[reg] * tl;
         }
-        if (has_mass) {
-            // A_M'' pattern with the 1/2 and 1/8 factors (sie_kernels_assembly.cuh:565-592).
-            const cplx Yee = mass_acc[0], Yem = mass_acc[1], Yme = mass_acc[2], Ymm = mass_acc[3];
-            const cplx Zee = mass_acc[4], Zem = mass_acc[5], Zme = mass_acc[6], Zmm = mass_acc[7];
-            const double f = 0.5, fq = 0.125;
-            const cplx ap = Zee * f + Ymm * fq, am = Zee * f - Ymm * fq;
-            const cplx bp = Zem * f + Yme * fq, bm = Zem * f - Yme * fq;
-            const cplx cp = Zme * f + Yem * fq, cm = Zme * f - Yem * fq;
-            const cplx dp = Zmm * f + Yee * fq, dm = Zmm * f - Yee * fq;
-            const double s1 = 1.0, se_ = P.me, s2 = P.me2;
-            blk[0][0] += ap * s1; blk[0][1] += bm * se_; blk[0][2] += am * s1; blk[0][3] += bp * se_;
-            blk[1][0] += cm * se_; blk[1][1] += dp * s2; blk[1][2] += cp * se_; blk[1][3] += dm * s2;
-            blk[2][0] += am * s1; blk[2][1] += bp * se_; blk[2][2] += ap * s1; blk[2][3] += bm * se_;
-            blk[3][0] += cp * se_; blk[3][1] += dm * s2; blk[3][2] += cm * se_; blk[3][3] += dp * s2;
-        }
+        if (has_mass) add_mass_pattern(mass_acc, P.me, P.me2, blk);
 #pragma unroll
         for (int c = 0; c < 4; ++c)
 #pragma unroll
@@ -690,18 +763,13 @@ int64_t system_dimension(int formulation, int64_t ne) {
     return formulation == SIEB200_PEC_EFIE ? ne : (formulation == SIEB200_PMCHWT ? 2 * ne : 4 * ne);
 }
 
-int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
-                    const double* host_tensors, cplx* dZ, int64_t ldz) {
-    AssemblyParams ap;
-    SIEB_RETURN_IF(make_assembly_params(opt, &ap));
+// Mesh, rule and incidences to the device, then the per-face geometry
+// records and quadrature points (shared by assembly and the adjoint
+// contraction).
+static int prepare_faces(sieb200_ctx* ctx, const sieb200_mesh& mesh, const float* pts, const float* wts, int Q,
+                         FaceGeom** geom_out, d3** qp_out, float** dw_out, int** dFE_out) {
     const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges, nv = (int)mesh.num_vertices;
-    const int64_t N = system_dimension(opt.formulation, ne);
-    SIEB_CHECK(ldz >= N, SIEB200_INVALID_ARG, "leading dimension of Z is smaller than N");
-    float pts[2 * kMaxQ], wts[kMaxQ];
-    const int Q = expand_rule(opt.quadrature_rule, pts, wts);
-    SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
     cudaStream_t st = ctx->stream;
-
     // Edge -> (face*3 + local edge) incidences; at most two per edge.
     std::vector<int> inc(2 * (size_t)ne, -1);
     for (int f = 0; f < nf; ++f)
@@ -739,9 +807,34 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
     SIEB_RETURN_IF(ctx->qpts.reserve(sizeof(d3) * (size_t)nf * Q));
     FaceGeom* geom = ctx->geom.as<FaceGeom>();
     d3* qp = ctx->qpts.as<d3>();
+    *geom_out = geom;
+    *qp_out = qp;
+    *dw_out = dw;
+    *dFE_out = dFE;
     face_prep_kernel<<<(nf + 127) / 128, 128, 0, st>>>(dV, dF, dFE, nf, dpts, Q, geom, qp);
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
+
+    return SIEB200_OK;
+}
+
+int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                    const double* host_tensors, cplx* dZ, int64_t ldz) {
+    AssemblyParams ap;
+    SIEB_RETURN_IF(make_assembly_params(opt, &ap));
+    const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges, nv = (int)mesh.num_vertices;
+    const int64_t N = system_dimension(opt.formulation, ne);
+    SIEB_CHECK(ldz >= N, SIEB200_INVALID_ARG, "leading dimension of Z is smaller than N");
+    float pts[2 * kMaxQ], wts[kMaxQ];
+    const int Q = expand_rule(opt.quadrature_rule, pts, wts);
+    SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
+    cudaStream_t st = ctx->stream;
+
+    FaceGeom* geom = nullptr;
+    d3* qp = nullptr;
+    float* dw = nullptr;
+    int* dFE = nullptr;
+    SIEB_RETURN_IF(prepare_faces(ctx, mesh, pts, wts, Q, &geom, &qp, &dw, &dFE));
 
     // GSTC mass blocks.
     cplx* dmass = nullptr;
@@ -833,6 +926,29 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
     }
+    return SIEB200_OK;
+}
+
+int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                           const cplx* d_lam, const cplx* d_x, cplx* d_s) {
+    SIEB_CHECK(opt.formulation == SIEB200_GSTC, SIEB200_INVALID_ARG,
+               "the tensor gradient exists for the GSTC formulation only");
+    AssemblyParams ap;
+    SIEB_RETURN_IF(make_assembly_params(opt, &ap));
+    const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges;
+    float pts[2 * kMaxQ], wts[kMaxQ];
+    const int Q = expand_rule(opt.quadrature_rule, pts, wts);
+    SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
+    FaceGeom* geom = nullptr;
+    d3* qp = nullptr;
+    float* dw = nullptr;
+    int* dFE = nullptr;
+    SIEB_RETURN_IF(prepare_faces(ctx, mesh, pts, wts, Q, &geom, &qp, &dw, &dFE));
+    tensor_grad_kernel<<<(nf * 8 + 127) / 128, 128, 0, ctx->stream>>>(geom, qp, dw, Q, nf, ne, dFE, ap.basis,
+                                                                       ap.mass_eta0, ap.mass_eta0_sq, d_lam, d_x,
+                                                                       d_s);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }
 

@@ -150,6 +150,10 @@ int expand_rule(int rule, float* pts, float* w);  // returns Q or -1
 // Assembly on the context stream into a device column-major N x N matrix.
 int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
                     const double* host_tensors, cplx* dZ, int64_t ldz);
+// s[f*32 + k] = lambda^H (dZ / d record[f][k]) x for the GSTC system (device
+// vectors of length 4 ne, s: num_faces x 32).
+int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                           const cplx* d_lam, const cplx* d_x, cplx* d_s);
 int assemble_rhs_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
                         const sieb200_source* sources, int nsrc, cplx* dB, int64_t ldb);
 

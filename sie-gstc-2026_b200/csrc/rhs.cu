@@ -212,6 +212,66 @@ __global__ void ff_samples_kernel(const double* __restrict__ V, const int* __res
         }
 }
 
+// Far-field operator as a matrix: rows (F_theta of direction d, then F_phi),
+// columns (J of edge e, then M of edge e), row-major with 2*ne columns, so
+// that [F_theta; F_phi] = A [J; M] with the same radiation vectors and
+// coefficients as ff_samples_kernel / ff_directions_kernel. One thread per
+// (direction, edge); the edge's incident faces and the 7-point rule are
+// evaluated on the fly.
+__global__ void ff_matrix_kernel(const double* __restrict__ V, const int* __restrict__ F,
+                                 const int* __restrict__ inc, int ne, int64_t ndir, double k0, double eta0,
+                                 const double* __restrict__ rh, const double* __restrict__ th,
+                                 const double* __restrict__ ph, cplx* __restrict__ A) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t d = blockIdx.y;
+    if (e >= ne) return;
+    const double s15 = sqrt(15.0);
+    const double a1 = (6.0 - s15) / 21.0, w1 = (155.0 - s15) / 1200.0;
+    const double a2 = (6.0 + s15) / 21.0, w2 = (155.0 + s15) / 1200.0;
+    const double nodes[7][2] = {{1.0 / 3.0, 1.0 / 3.0}, {a1, a1}, {1.0 - 2.0 * a1, a1},
+                                {a1, 1.0 - 2.0 * a1}, {a2, a2}, {1.0 - 2.0 * a2, a2},
+                                {a2, 1.0 - 2.0 * a2}};
+    const double wq[7] = {0.225, w1, w1, w1, w2, w2, w2};
+    const int EA[3] = {0, 1, 2}, EB[3] = {1, 2, 0}, EF[3] = {2, 0, 1};
+    const d3 r = mk3(rh[3 * d], rh[3 * d + 1], rh[3 * d + 2]);
+    cplx N[3] = {cx(0, 0), cx(0, 0), cx(0, 0)};
+    for (int a = 0; a < 2; ++a) {
+        const int fi = inc[2 * e + a];
+        if (fi < 0) continue;
+        const int f = fi / 3, le = fi - 3 * f;
+        int idx[3];
+        d3 v[3];
+        for (int b = 0; b < 3; ++b) {
+            idx[b] = F[3 * f + b];
+            v[b] = mk3(V[3 * idx[b]], V[3 * idx[b] + 1], V[3 * idx[b] + 2]);
+        }
+        const d3 ev = v[EB[le]] - v[EA[le]];
+        const double len = (idx[EA[le]] > idx[EB[le]] ? 1.0 : -1.0) * sqrt(dot3(ev, ev));
+        for (int q = 0; q < 7; ++q) {
+            const double xi = nodes[q][0], eta = nodes[q][1], zeta = 1.0 - xi - eta;
+            const d3 rq = v[0] * zeta + v[1] * xi + v[2] * eta;
+            const d3 rho = rq - v[EF[le]];
+            double sn, cs;
+            sincos(k0 * dot3(r, rq), &sn, &cs);
+            const double wgt = 0.5 * len * wq[q];
+            const cplx ph_ = cx(cs * wgt, sn * wgt);
+            N[0] += ph_ * rho.x;
+            N[1] += ph_ * rho.y;
+            N[2] += ph_ * rho.z;
+        }
+    }
+    const double* t = th + 3 * d;
+    const double* p = ph + 3 * d;
+    const cplx nt = N[0] * t[0] + N[1] * t[1] + N[2] * t[2];
+    const cplx np = N[0] * p[0] + N[1] * p[1] + N[2] * p[2];
+    const cplx coeff = cx(0.0, -k0 / (4.0 * 3.14159265358979323846));
+    const int64_t cols = 2 * (int64_t)ne;
+    A[d * cols + e] = coeff * (nt * eta0);
+    A[(ndir + d) * cols + e] = coeff * (np * eta0);
+    A[d * cols + ne + e] = coeff * np;
+    A[(ndir + d) * cols + ne + e] = cx(0, 0) - coeff * nt;
+}
+
 __global__ void ff_directions_kernel(const d3* __restrict__ rq, const cplx* __restrict__ cj,
                                      const cplx* __restrict__ cm, int64_t M, double k0, double eta0,
                                      const double* __restrict__ rh, const double* __restrict__ th,
@@ -430,6 +490,45 @@ int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j
         SIEB_TRY_CUDA(cudaMemcpyAsync(f_phi, b + oOut + sizeof(cplx) * ndir, sizeof(cplx) * ndir, cudaMemcpyDeviceToHost, st));
         SIEB_TRY_CUDA(cudaMemcpyAsync(intensity, b + oU, sizeof(double) * ndir, cudaMemcpyDeviceToHost, st));
     }
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    return SIEB200_OK;
+}
+
+int far_field_matrix_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, double k0, double eta0, int64_t ndir,
+                            const double* rh, const double* th, const double* ph, cplx* dA) {
+    const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges, nv = (int)mesh.num_vertices;
+    cudaStream_t st = ctx->stream;
+    std::vector<int> inc(2 * (size_t)ne, -1);
+    for (int f = 0; f < nf; ++f)
+        for (int le = 0; le < 3; ++le) {
+            const int e = mesh.faces_edges[3 * f + le];
+            SIEB_CHECK(e >= 0 && e < ne, SIEB200_INVALID_ARG, "faces_edges entry out of range");
+            if (inc[2 * e] < 0) inc[2 * e] = 3 * f + le;
+            else if (inc[2 * e + 1] < 0) inc[2 * e + 1] = 3 * f + le;
+            else {
+                set_error("non-manifold mesh: an edge is shared by more than two faces");
+                return SIEB200_INVALID_ARG;
+            }
+        }
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += ((bytes + 255) / 256) * 256; return o; };
+    const size_t oV = take(sizeof(double) * 3 * nv), oF = take(sizeof(int) * 3 * nf),
+                 oI = take(sizeof(int) * 2 * ne), oDir = take(sizeof(double) * 9 * ndir);
+    DeviceBuffer buf;
+    SIEB_RETURN_IF(buf.reserve(off));
+    char* b = buf.as<char>();
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b + oV, mesh.vertices, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b + oF, mesh.faces, sizeof(int) * 3 * nf, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b + oI, inc.data(), sizeof(int) * 2 * ne, cudaMemcpyHostToDevice, st));
+    double* dd = reinterpret_cast<double*>(b + oDir);
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dd, rh, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dd + 3 * ndir, th, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dd + 6 * ndir, ph, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, st));
+    ff_matrix_kernel<<<dim3((unsigned)((ne + 127) / 128), (unsigned)ndir), 128, 0, st>>>(
+        reinterpret_cast<double*>(b + oV), reinterpret_cast<int*>(b + oF), reinterpret_cast<int*>(b + oI), ne,
+        ndir, k0, eta0, dd, dd + 3 * ndir, dd + 6 * ndir, dA);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
     SIEB_TRY_CUDA(cudaStreamSynchronize(st));
     return SIEB200_OK;
 }

@@ -8,6 +8,8 @@ raise.
 
 from ._lib import (GSTC, PEC_EFIE, PMCHWT, SOLVER_LU_CUSOLVER, SOLVER_LU_FP64, SOLVER_MIXED_IR,
                    InvalidArgument, SiebError, exported_symbols, lib, library_path)
+from .adjoint import (FarFieldConeObjective, cone_directions, far_field_matrix, gstc_solve, omega_records,
+                      physical_exterior, tensor_gradient)
 from .farfield import MetasurfaceFarFieldEvaluator, bistatic_rcs, far_field, spherical_frames
 from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, load_obj, make_mesh, \
     revolved_spindle, save_obj
