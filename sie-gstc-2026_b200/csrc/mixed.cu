@@ -1175,7 +1175,10 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     sieb200_ctx* ctx = s->ctx;
     cudaStream_t stream = ctx->stream;
     const int64_t n = st->n, np = st->np;
-    const int m = 20;  // restart length
+    // Restart length: the whole iteration budget up to 100 directions (V and
+    // Z together hold 2 n m complex128); restarts slow FGMRES down sharply on
+    // ill-conditioned systems.
+    const int m = std::max(1, std::min(maxit, 100));
     const int parts = 64;
     // vectors: x, r, w, work(np), V (n x (m+1)), Z (n x m), partial, h
     const size_t vbytes =
