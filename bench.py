@@ -319,6 +319,11 @@ def run(args):
     solver.close()
 
     # CPU baseline (rank 0, one GPU only): the reference's CPU solve of this system.
+    adjoint = adjoint_section(ctx, args.adjoint_steps, max_over_ranks) if args.adjoint_steps > 0 else None
+    if adjoint is not None:
+        adjoint["grads_per_s"] *= world
+        adjoint["fp64_grads_per_s"] *= world
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -364,6 +369,7 @@ def run(args):
             "relative_residual": rel_res, "rel_diff_vs_fp64_lu": rel_diff,
             "refinement_iterations": max(iters), "assembly_seconds": t_asm,
             "assembly_green_evals_per_s": evals / t_asm,
+            "adjoint": adjoint,
         }
         print(json.dumps(out), flush=True)
     torch.cuda.synchronize()
@@ -375,6 +381,68 @@ def run(args):
     os._exit(0)
 
 
+ADJOINT_WORKLOAD = ("SIE-GSTC adjoint synthesis: circular-arc spindle (arc radius 1.5 m, half-angle 60 deg), "
+                    "revolved mesh 9800 faces / 14700 RWG edges (N=58800), f=300 MHz, Dunavant rule 5; "
+                    "omega parameters (B, X, chi) per face (29400 reals, seeded, |chi^2-BX|>=0.25); "
+                    "objective = far-field power in a 10 deg cone about +z; x-polarised plane wave along +z")
+
+
+def adjoint_section(ctx, steps: int, max_over_ranks):
+    """Gradients/s of a far-field objective with respect to the per-face omega
+    parameters: assembly, factorization and refined solve forward, one
+    conjugate-transpose solve plus the tensor contraction backward."""
+    import torch
+    import sieb200
+    m = sieb200.revolved_spindle()
+    o = sieb200.GstcSieOptions(frequency_hz=3e8, quadrature_rule=5)
+    rng = np.random.default_rng(20260)
+    nf = m.num_faces
+    B, X, chi = (rng.uniform(-2, 2, nf) for _ in range(3))
+    bad = np.abs(chi ** 2 - B * X) < 0.25
+    while bad.any():
+        B[bad], X[bad], chi[bad] = (rng.uniform(-2, 2, int(bad.sum())) for _ in range(3))
+        bad = np.abs(chi ** 2 - B * X) < 0.25
+    params = [torch.tensor(v, dtype=torch.float64, requires_grad=True) for v in (B, X, chi)]
+    b = torch.from_numpy(sieb200.assemble_rhs(m, o, [sieb200.PlaneWaveExcitation()], ctx=ctx)[:, 0].copy()).cuda()
+    obj = sieb200.FarFieldConeObjective(m, o, half_angle_deg=10.0, ctx=ctx)
+
+    def grad(method):
+        for p in params:
+            p.grad = None
+        x = sieb200.gstc_solve(sieb200.omega_records(*params), b, m, o, method=method, tolerance=1e-10, ctx=ctx)
+        L = obj(x)
+        L.backward()
+        return float(L.detach()), torch.cat([p.grad for p in params]).clone()
+
+    def timed(method, n):
+        out = None
+        t = []
+        for _ in range(n):
+            torch.cuda.synchronize()
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = grad(method)
+            c.record()
+            c.synchronize()
+            t.append(a.elapsed_time(c) / 1e3)
+        return out, t
+
+    grad("mixed_ir")  # warm-up (workspaces, module loading)
+    (L_mx, g_mx), t_mx = timed("mixed_ir", steps)
+    (L_64, g_64), t_64 = timed("lu_cusolver", 1)
+    t_mx_s = max_over_ranks(statistics.mean(t_mx))
+    t_64_s = max_over_ranks(statistics.mean(t_64))
+    return {
+        "workload": ADJOINT_WORKLOAD, "N": 4 * m.num_edges, "method": "mixed_ir (split-TF32 LU + FP64 FGMRES, "
+        "adjoint: conjugate-transpose FGMRES on the same factors)",
+        "grads_per_s": 1.0 / t_mx_s, "ms_per_grad": 1e3 * t_mx_s, "steps": steps,
+        "fp64_grads_per_s": 1.0 / t_64_s, "speedup_vs_fp64": t_64_s / t_mx_s,
+        "objective": L_mx, "objective_rel_diff_vs_fp64": abs(L_mx - L_64) / abs(L_64),
+        "grad_rel_diff_vs_fp64": float((g_mx - g_64).norm() / g_64.norm()),
+        "timing": "CUDA events around device-synchronized gradient evaluations",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -383,6 +451,8 @@ def main():
     ap.add_argument("--impl", default="sieb200", choices=["sieb200", "reference"])
     ap.add_argument("--rule", type=int, default=17)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline solve")
+    ap.add_argument("--adjoint-steps", type=int, default=2,
+                    help="timed adjoint gradients on the spindle workload (0 skips them)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
