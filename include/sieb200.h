@@ -244,8 +244,10 @@ int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t l
 /* Split-TF32 tensor-core contraction used by the mixed LU's trailing update
  * (no counterpart in the reference, which calls cuSOLVER): on device data,
  *   C[m2 x n] (fp32, column-major, ldc) -= A[m2 x k] * B[n x k]^T,
- * A and B K-major fp32, k a multiple of 32. mode 1: tcgen05 kernel, mode 0:
- * SIMT kernel on the same operands (checking path). */
+ * A and B K-major fp32, k a multiple of 32. mode 2: persistent tcgen05
+ * kernel with TMA C epilogue (what the LU uses; C and ldc*4 16-byte aligned,
+ * else mode 1), mode 1: one-CTA-per-tile tcgen05 kernel, mode 0: SIMT kernel
+ * on the same operands (checking path). */
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode);
 

@@ -716,7 +716,7 @@ int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double
 
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode) {
-    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && (mode == 0 || mode == 1), SIEB200_INVALID_ARG,
+    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 2, SIEB200_INVALID_ARG,
                "invalid GEMM arguments");
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     GemmTC* g = nullptr;

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -210,6 +211,168 @@ gemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_const
     }
 }
 
+// Persistent variant: one CTA per SM walks the output tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (row tiles fastest, so the CTAs in flight share
+// B tiles and all of A stays in L2). 192 threads:
+//   warp 0 lane 0  TMA producer of A and B boxes into a 4-stage ring,
+//   warp 1         TMEM owner (256 columns: two 128-column accumulators);
+//                  lane 0 issues the MMAs, alternating accumulators by tile,
+//   warps 2-5      epilogue: the C tile (128 x 128 fp32, 64 KB) comes in by
+//                  TMA while the tile's MMAs run; each warp reads its 32 TMEM
+//                  lanes, subtracts in shared memory, releases the
+//                  accumulator, and one thread stores the tile by TMA and
+//                  starts loading the next one.
+// So a tile's C traffic overlaps the next tile's main loop inside one CTA.
+// Every mbarrier wait is bounded and reports through the error word.
+constexpr int P_STAGES = 4;
+constexpr int P_THREADS = 192;
+constexpr int C_TILE_BYTES = BM * BN * 4;
+constexpr int P_SMEM_BYTES = P_STAGES * (STAGE_A + STAGE_B) + C_TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+
+__device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__global__ void __launch_bounds__(P_THREADS, 1)
+gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                                const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, unsigned* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - raw);
+    const uint32_t sA = base;
+    const uint32_t sB = base + P_STAGES * STAGE_A;
+    const uint32_t sC = base + P_STAGES * (STAGE_A + STAGE_B);
+    float* cs = reinterpret_cast<float*>(gbase + P_STAGES * (STAGE_A + STAGE_B));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + P_STAGES * (STAGE_A + STAGE_B) + C_TILE_BYTES);
+    const uint32_t full0 = smem_u32(&bars[0]);
+    const uint32_t empty0 = smem_u32(&bars[P_STAGES]);
+    const uint32_t accf0 = smem_u32(&bars[2 * P_STAGES]);      // accumulator b ready (MMA -> epilogue)
+    const uint32_t acce0 = smem_u32(&bars[2 * P_STAGES + 2]);  // accumulator b drained (epilogue -> MMA)
+    const uint32_t cfull = smem_u32(&bars[2 * P_STAGES + 4]);  // C tile in shared memory
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * P_STAGES + 5]);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = (M2 + BM - 1) / BM, nt = (N + BN - 1) / BN;
+    const int tiles = mt * nt;
+    const int kblocks = K / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < P_STAGES; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accf0 + 8 * b, 1);
+            mbar_init(acce0 + 8 * b, 4);
+        }
+        mbar_init(cfull, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int g = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                const int m0 = (t % mt) * BM, n0 = (t / mt) * BN;
+                for (int kb = 0; kb < kblocks; ++kb, ++g) {
+                    const int s = g % P_STAGES;
+                    const uint32_t ph = (uint32_t)(g / P_STAGES) & 1u;
+                    if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) { ok = false; break; }
+                    mbar_expect_tx(full0 + 8 * s, STAGE_A + STAGE_B);
+                    tma_load_2d(sA + s * STAGE_A, &tmA, full0 + 8 * s, kb * BK, m0);
+                    tma_load_2d(sB + s * STAGE_B, &tmB, full0 + 8 * s, kb * BK, n0);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int g = 0, li = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++li) {
+                const int b = li & 1;
+                const uint32_t u = (uint32_t)(li >> 1);
+                if (!mbar_wait(acce0 + 8 * b, (u & 1u) ^ 1u, err)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                for (int kb = 0; kb < kblocks; ++kb, ++g) {
+                    const int s = g % P_STAGES;
+                    const uint32_t ph = (uint32_t)(g / P_STAGES) & 1u;
+                    if (!mbar_wait(full0 + 8 * s, ph, err)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint64_t ad = smem_desc_sw128(sA + s * STAGE_A);
+                    const uint64_t bd = smem_desc_sw128(sB + s * STAGE_B);
+#pragma unroll
+                    for (int k = 0; k < BK / 8; ++k)
+                        umma_tf32(acc, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u);
+                    umma_commit(empty0 + 8 * s);
+                }
+                if (ok) umma_commit(accf0 + 8 * b);  // fires when the tile's MMAs have completed
+            }
+        }
+    } else {
+        const int q = warp & 3;            // TMEM lane quarter of this warp
+        const int et = threadIdx.x - 64;   // 0..127
+        const int rt = q * 32 + lane;      // row of the tile
+        const bool e0 = et == 0;
+        int t = blockIdx.x;
+        if (e0 && t < tiles) {
+            mbar_expect_tx(cfull, C_TILE_BYTES);
+            tma_load_2d(sC, &tmC, cfull, (t % mt) * BM, (t / mt) * BN);
+        }
+        for (int li = 0; t < tiles; t += gridDim.x, ++li) {
+            const int b = li & 1;
+            const uint32_t u = (uint32_t)(li >> 1);
+            const bool okc = mbar_wait(cfull, (uint32_t)li & 1u, err);
+            int got = 0;
+            if (lane == 0) got = mbar_wait(accf0 + 8 * b, u & 1u, err) ? 1 : 0;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            __syncwarp();
+            if (got && okc) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+                for (int chunk = 0; chunk < BN / 32; ++chunk) {
+                    float v[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + chunk * 32), v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] -= v[j];
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce0 + 8 * b);
+            // Generic-proxy writes of the tile, then the async-proxy store.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            epilogue_bar();
+            if (e0) {
+                tma_store_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
+                bulk_commit();
+                bulk_wait_read_all();  // the buffer is free once the store has read it
+                const int tn = t + gridDim.x;
+                if (tn < tiles) {
+                    mbar_expect_tx(cfull, C_TILE_BYTES);
+                    tma_load_2d(sC, &tmC, cfull, (tn % mt) * BM, (tn / mt) * BN);
+                }
+            }
+        }
+        if (e0) bulk_wait_all();
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+    }
+}
+
 // SIMT reference on the same packed operands (checking path).
 __global__ void gemm_simt_sub_kernel(const float* __restrict__ A, const float* __restrict__ B,
                                      float* __restrict__ C, int64_t ldc, int M2, int N, int K) {
@@ -273,8 +436,9 @@ int encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType type, const void*
 
 struct GemmTC {
     unsigned* err = nullptr;
-    int mode = 1;
-    bool attr_set = false;
+    int mode = 2;
+    bool attr_set = false, attr_set_p = false;
+    int sms = 148;
 };
 
 int gemm_tc_create(GemmTC** out) {
@@ -288,6 +452,10 @@ int gemm_tc_create(GemmTC** out) {
     cudaMemset(g->err, 0, sizeof(unsigned));
     const char* env = getenv("SIEB200_GEMM_SIMT");
     if (env && env[0] == '1') g->mode = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
     *out = g;
     return SIEB200_OK;
 }
@@ -301,7 +469,7 @@ void gemm_tc_destroy(GemmTC* g) {
 void gemm_tc_set_mode(GemmTC* g, int mode) { g->mode = mode; }
 
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A, const float* B,
-                int64_t M2, int64_t N, int K) {
+                int64_t M2, int64_t N, int K, int max_ctas) {
     SIEB_CHECK(K % BK == 0 && K > 0, SIEB200_INVALID_ARG, "GEMM K must be a positive multiple of 32");
     SIEB_CHECK(M2 > 0 && N > 0 && M2 < (1ll << 31) && N < (1ll << 31), SIEB200_INVALID_ARG, "GEMM size out of range");
     SIEB_CHECK(((uintptr_t)A % 16) == 0 && ((uintptr_t)B % 16) == 0, SIEB200_INVALID_ARG,
@@ -313,14 +481,34 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     }
+    CUtensorMap ma, mb;
+    SIEB_RETURN_IF(make_map(&ma, A, K, M2, BM));
+    SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
+    // The persistent kernel moves C by TMA: its base and column stride must
+    // be 16-byte aligned (otherwise the per-tile kernel below is used).
+    if (g->mode == 2 && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
+        if (!g->attr_set_p) {
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            g->attr_set_p = true;
+        }
+        CUtensorMap mc;
+        SIEB_RETURN_IF(encode_tensor_map_2d(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, C, (uint64_t)M2, (uint64_t)N,
+                                            (uint64_t)ldc * sizeof(float), BM, BN, CU_TENSOR_MAP_SWIZZLE_NONE));
+        const int64_t tiles = ((M2 + BM - 1) / BM) * ((N + BN - 1) / BN);
+        const int cap = max_ctas > 0 ? std::min(max_ctas, g->sms) : g->sms;
+        const unsigned grid = (unsigned)std::min<int64_t>(tiles, std::max(1, cap));
+        gemm_tf32_sub_persistent_kernel<<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2, (int)N, K,
+                                                                                 g->err);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    }
     if (!g->attr_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            SMEM_BYTES));
         g->attr_set = true;
     }
-    CUtensorMap ma, mb;
-    SIEB_RETURN_IF(make_map(&ma, A, K, M2, BM));
-    SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
     const dim3 grid((unsigned)((M2 + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
     gemm_tf32_sub_kernel<<<grid, 128, SMEM_BYTES, stream>>>(ma, mb, C, ldc, (int)M2, (int)N, K, g->err);
     SIEB_NOTE_LAUNCH();

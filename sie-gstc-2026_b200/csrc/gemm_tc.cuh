@@ -15,11 +15,14 @@ int gemm_tc_create(GemmTC** out);
 void gemm_tc_destroy(GemmTC* g);
 // Returns a SIEB200_* status; the kernel's bounded waits report through an
 // error word checked on the next synchronization (gemm_tc_check).
+// max_ctas > 0 caps the persistent kernel's grid, leaving the other SMs to
+// concurrent work on other streams.
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A,
-                const float* B, int64_t M2, int64_t N, int K);
+                const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0);
 int gemm_tc_check(GemmTC* g, cudaStream_t stream);
-// Selects the implementation for testing: 1 = tcgen05 (default), 0 = SIMT on
-// the same packed operands.
+// Selects the implementation: 2 = persistent tcgen05 kernel with TMA C
+// epilogue (default), 1 = one CTA per tile tcgen05 kernel, 0 = SIMT on the
+// same packed operands (checking path).
 void gemm_tc_set_mode(GemmTC* g, int mode);
 
 }  // namespace sieb200

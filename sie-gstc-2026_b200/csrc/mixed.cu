@@ -1032,13 +1032,17 @@ int mixed_factorize(DenseSolver* s) {
         }
         return SIEB200_OK;
     };
-    auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B) -> int {
+    // The trailing update proper leaves kSideSMs SMs to the lookahead stream
+    // (the persistent GEMM holds its SMs for the whole launch).
+    constexpr int kSideSMs = 20;
+    auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B,
+                    int max_ctas) -> int {
         const int64_t m = np - s0;
         float* C = reinterpret_cast<float*>(st->W + s0 + c0 * ldw);
         cudaEvent_t ev;
         ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * K3,
                         4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K3), &ev);
-        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K3));
+        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K3, max_ctas));
         ctx->prof.end(stream, ev);
         return SIEB200_OK;
     };
@@ -1063,12 +1067,13 @@ int mixed_factorize(DenseSolver* s) {
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
             const float* A = st->Apack[bk & 1];
-            SIEB_RETURN_IF(gemm(s0, s0, n1, A, st->Bpack));
+            SIEB_RETURN_IF(gemm(s0, s0, n1, A, st->Bpack, 0));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
             SIEB_RETURN_IF(diag_and_L(bk + 1, st->side));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_panel, st->side));
-            if (m > n1) SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3));
+            if (m > n1)
+                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3, ctx->sm_count - kSideSMs));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(

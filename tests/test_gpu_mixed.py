@@ -23,8 +23,8 @@ def _tf32(x):
     return b.view(np.float32)
 
 
-@pytest.mark.parametrize("mode", [0, 1])
-@pytest.mark.parametrize("m2,n", [(256, 128), (300, 200), (1000, 517)])
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("m2,n", [(256, 128), (300, 200), (1000, 517), (4096, 1500)])
 def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
     import torch
     import sieb200
