@@ -1032,9 +1032,11 @@ int mixed_factorize(DenseSolver* s) {
         }
         return SIEB200_OK;
     };
-    // The trailing update proper leaves kSideSMs SMs to the lookahead stream
-    // (the persistent GEMM holds its SMs for the whole launch).
-    constexpr int kSideSMs = 20;
+    // The trailing update proper leaves SMs to the lookahead stream (the
+    // persistent GEMM holds its SMs for the whole launch): 20 while the
+    // update is short enough for the diagonal block and L21 panel to be on
+    // the critical path, 6 once it is long (m > 8192) and they hide anyway.
+    auto side_sms = [](int64_t m) { return m > 8192 ? 6 : 20; };
     auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B,
                     int max_ctas) -> int {
         const int64_t m = np - s0;
@@ -1073,7 +1075,7 @@ int mixed_factorize(DenseSolver* s) {
             SIEB_RETURN_IF(diag_and_L(bk + 1, st->side));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_panel, st->side));
             if (m > n1)
-                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3, ctx->sm_count - kSideSMs));
+                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3, ctx->sm_count - side_sms(m)));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
