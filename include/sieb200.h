@@ -87,7 +87,8 @@ enum {
     SIEB200_SOLVER_LU_FP64 = 0,     /* own FP64 blocked LU (drop-in for the cuSOLVER path) */
     SIEB200_SOLVER_LU_CUSOLVER = 1, /* cusolverDnZgetrf/Zgetrs, as dense_lu_solver.cuh */
     SIEB200_SOLVER_MIXED_IR = 2,    /* split-FP32 tensor-core LU + FP64 GMRES refinement */
-    SIEB200_SOLVER_GMRES_C64 = 3    /* GMRES on a complex64 copy of Z, FP64 residual */
+    SIEB200_SOLVER_GMRES_C64 = 3    /* Jacobi-preconditioned GMRES, complex64 copy of Z for the
+                                       Krylov products, FP64 residual (gmres_solver.cuh:258-520) */
 };
 enum { SIEB200_BASIS_FACE = 0, SIEB200_BASIS_SPHERICAL = 1 };
 
@@ -187,6 +188,16 @@ int sieb200_assemble_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, const si
 int sieb200_assemble_rhs(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
                          const sieb200_source* sources, int num_sources, double* B,
                          int b_on_device);
+
+/* Matrix-free product y = Z x (sie_kernels_matvec.cuh:9-141 Calderon and
+ * 143-327 mass blocks, there for GSTC with unscaled blocks and complex64
+ * vectors): Z is the eta0-scaled matrix sieb200_assemble_matrix builds, for
+ * every formulation, recomputed by the same quadrature kernels and contracted
+ * with x slab by slab instead of stored (a pair-block workspace bounded by
+ * the free memory replaces the N x N matrix). x, y: N complex128, device when
+ * on_device != 0, else host. */
+int sieb200_matvec_matrix_free(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                               const double* tensors, const double* x, double* y, int on_device);
 
 /* Adjoint contraction of the SIE-GSTC system with respect to its per-face
  * tensor records (no counterpart in the reference, which has no adjoint):

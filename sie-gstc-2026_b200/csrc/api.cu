@@ -291,7 +291,7 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
     const int64_t ne = mesh->num_edges;
     const int64_t N = system_dimension(o->formulation, ne);
     const int method = o->solver;
-    SIEB_CHECK(method >= 0 && method <= 2, SIEB200_INVALID_ARG, "unsupported solver method");
+    SIEB_CHECK(method >= 0 && method <= 3, SIEB200_INVALID_ARG, "unsupported solver method");
     cudaStream_t st = ctx->stream;
 
     DeviceBuffer Zb, Zcopy, Bb, Srcb, Xb, Rb;
@@ -318,7 +318,7 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
     SIEB_RETURN_IF(Bb.reserve(sizeof(cplx) * N * ncols));
     SIEB_TRY_CUDA(cudaMemcpyAsync(Bb.ptr, hb.data(), sizeof(cplx) * N * ncols, cudaMemcpyHostToDevice, st));
 
-    const bool in_place = method != SIEB200_SOLVER_MIXED_IR;
+    const bool in_place = method != SIEB200_SOLVER_MIXED_IR && method != SIEB200_SOLVER_GMRES_C64;
     if (o->compute_residual && in_place) {
         SIEB_RETURN_IF(Zcopy.reserve(sizeof(cplx) * N * N));
         SIEB_TRY_CUDA(cudaMemcpyAsync(Zcopy.ptr, Zb.ptr, sizeof(cplx) * N * N, cudaMemcpyDeviceToDevice, st));
@@ -582,6 +582,29 @@ int sieb200_assemble_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, const si
     return SIEB200_OK;
 }
 
+int sieb200_matvec_matrix_free(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
+                               const double* tensors, const double* x, double* y, int on_device) {
+    SIEB_RETURN_IF(validate(mesh, opt, tensors));
+    SIEB_CHECK(ctx && x && y, SIEB200_INVALID_ARG, "invalid matrix-free product arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    const int64_t N = system_dimension(opt->formulation, mesh->num_edges);
+    if (on_device) {
+        SIEB_RETURN_IF(matvec_free_device(ctx, *mesh, *opt, tensors, reinterpret_cast<const cplx*>(x),
+                                          reinterpret_cast<cplx*>(y)));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+        return SIEB200_OK;
+    }
+    DeviceBuffer tmp;
+    SIEB_RETURN_IF(tmp.reserve(sizeof(cplx) * 2 * N));
+    cplx* dx = tmp.as<cplx>();
+    cplx* dy = dx + N;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dx, x, sizeof(cplx) * N, cudaMemcpyHostToDevice, ctx->stream));
+    SIEB_RETURN_IF(matvec_free_device(ctx, *mesh, *opt, tensors, dx, dy));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(y, dy, sizeof(cplx) * N, cudaMemcpyDeviceToHost, ctx->stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
 int sieb200_gstc_tensor_gradient(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,
                                  const double* lambda, const double* x, int on_device, double* s_out) {
     SIEB_RETURN_IF(validate(mesh, opt, nullptr, false));
@@ -631,7 +654,7 @@ int sieb200_assemble_rhs(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb2
 
 int sieb200_dense_solver_create(sieb200_ctx* ctx, int64_t n, int method, sieb200_dense_solver** out) {
     SIEB_CHECK(ctx && out && n > 0, SIEB200_INVALID_ARG, "invalid dense solver arguments");
-    SIEB_CHECK(method >= 0 && method <= 2, SIEB200_INVALID_ARG, "unsupported dense solver method");
+    SIEB_CHECK(method >= 0 && method <= 3, SIEB200_INVALID_ARG, "unsupported dense solver method");
     SIEB_CHECK(n <= std::numeric_limits<int>::max(), SIEB200_OVERFLOW, "matrix dimension exceeds the int limit");
     sieb200_dense_solver* s = new sieb200_dense_solver();
     s->impl.ctx = ctx;

@@ -678,22 +678,19 @@ struct GatherParams {
     double me, me2;  // mass scales (float eta0, eta0^2)
 };
 
-// One thread per (test edge te, source edge se); te fastest for coalesced
-// column-major stores. Sums the incident face pairs with the test face in
-// [m0, m1) and adds into Z (zeroed before the first slab).
-__global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __restrict__ mass,
-                              const int* __restrict__ inc, GatherParams P, cplx* __restrict__ Z,
-                              int64_t ldz) {
-    const int te = blockIdx.x * blockDim.x + threadIdx.x;
-    const int se = blockIdx.y * blockDim.y + threadIdx.y;
-    if (te >= P.ne || se >= P.ne) return;
+// The region block (1x1 PEC, 2x2 PMCHWT, 4x4 GSTC) of Z at test edge te and
+// source edge se from the face-pair blocks of the test faces in [m0, m1);
+// false when te has no incident face in the slab.
+__device__ __forceinline__ bool edge_pair_block(const cplx* __restrict__ pairs, const cplx* __restrict__ mass,
+                                                const int* __restrict__ inc, const GatherParams& P, int te, int se,
+                                                cplx (&blk)[4][4]) {
     const int it[2] = {inc[2 * te], inc[2 * te + 1]};
     const int is[2] = {inc[2 * se], inc[2 * se + 1]};
     bool any = false;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
         if (it[a] >= 0 && it[a] / 3 >= P.m0 && it[a] / 3 < P.m1) any = true;
-    if (!any) return;
+    if (!any) return false;
 
     cplx acc[4] = {cx(0, 0), cx(0, 0), cx(0, 0), cx(0, 0)};
     cplx mass_acc[8];
@@ -709,8 +706,10 @@ __global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __rest
         for (int b = 0; b < 2; ++b) {
             if (is[b] < 0) continue;
             const int n = is[b] / 3, i = is[b] - 3 * n;
-            const cplx* blk = pairs + ((size_t)(m - P.m0) * P.nf + n) * (P.NB * 9) + j * 3 + i;
-            for (int k = 0; k < P.NB; ++k) acc[k] += blk[k * 9];
+            const cplx* pb = pairs + ((size_t)(m - P.m0) * P.nf + n) * (P.NB * 9) + j * 3 + i;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < P.NB) acc[k] += pb[k * 9];
             if (P.formulation == SIEB200_GSTC && m == n) {
                 has_mass = true;
                 const cplx* mb = mass + (size_t)m * 72 + j * 3 + i;
@@ -719,26 +718,21 @@ __global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __rest
             }
         }
     }
-    const int64_t E = P.ne;
-    auto at = [&](int64_t r, int64_t c) -> cplx& { return Z[r + c * ldz]; };
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) blk[r][c] = cx(0, 0);
     if (P.formulation == SIEB200_PEC_EFIE) {
-        at(te, se) += P.c_jj[1] * acc[0];
+        blk[0][0] = P.c_jj[1] * acc[0];
     } else if (P.formulation == SIEB200_PMCHWT) {
         // acc: TL1, TL2, TK1, TK2
-        const cplx jj = P.c_jj[0] * acc[0] + P.c_jj[1] * acc[1];
         const cplx tk = acc[2] + acc[3];
         const cplx jm = tk * P.s_jm;
-        const cplx mm = (P.c_mm[0] * acc[0] + P.c_mm[1] * acc[1]) * P.s_mm;
-        at(te, se) += jj;
-        at(te, se + E) += jm;
-        at(te + E, se) += cx(-jm.re, -jm.im);
-        at(te + E, se + E) += mm;
+        blk[0][0] = P.c_jj[0] * acc[0] + P.c_jj[1] * acc[1];
+        blk[0][1] = jm;
+        blk[1][0] = cx(-jm.re, -jm.im);
+        blk[1][1] = (P.c_mm[0] * acc[0] + P.c_mm[1] * acc[1]) * P.s_mm;
     } else {
-        cplx blk[4][4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) blk[r][c] = cx(0, 0);
 #pragma unroll
         for (int reg = 0; reg < 2; ++reg) {
             const cplx tl = acc[reg], tk = acc[2 + reg];
@@ -750,10 +744,75 @@ __global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __rest
             blk[o + 1][o + 1] = P.c_mm[reg] * tl;
         }
         if (has_mass) add_mass_pattern(mass_acc, P.me, P.me2, blk);
+    }
+    return true;
+}
+
+__device__ __forceinline__ int region_count(int formulation) {
+    return formulation == SIEB200_PEC_EFIE ? 1 : (formulation == SIEB200_PMCHWT ? 2 : 4);
+}
+
+// One thread per (test edge te, source edge se); te fastest for coalesced
+// column-major stores. Sums the incident face pairs with the test face in
+// [m0, m1) and adds into Z (zeroed before the first slab).
+__global__ void gather_kernel(const cplx* __restrict__ pairs, const cplx* __restrict__ mass,
+                              const int* __restrict__ inc, GatherParams P, cplx* __restrict__ Z,
+                              int64_t ldz) {
+    const int te = blockIdx.x * blockDim.x + threadIdx.x;
+    const int se = blockIdx.y * blockDim.y + threadIdx.y;
+    if (te >= P.ne || se >= P.ne) return;
+    cplx blk[4][4];
+    if (!edge_pair_block(pairs, mass, inc, P, te, se, blk)) return;
+    const int64_t E = P.ne;
+    const int nr = region_count(P.formulation);
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+    for (int c = 0; c < 4; ++c)
 #pragma unroll
-            for (int r = 0; r < 4; ++r) at(te + r * E, se + c * E) += blk[r][c];
+        for (int r = 0; r < 4; ++r)
+            if (c < nr && r < nr) Z[(te + r * E) + (se + c * E) * ldz] += blk[r][c];
+}
+
+// Matrix-free product: y += (the slab's rows of Z) x without storing Z. One
+// warp per test edge: lanes stride over the source edges, each forming the
+// same region block as gather_kernel, then a warp reduction; the warp owns
+// its y entries, and slabs run in order, so the sum is deterministic.
+__global__ void gather_matvec_kernel(const cplx* __restrict__ pairs, const cplx* __restrict__ mass,
+                                     const int* __restrict__ inc, GatherParams P, const cplx* __restrict__ x,
+                                     cplx* __restrict__ y) {
+    const int te = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (te >= P.ne) return;  // warp-uniform
+    const int64_t E = P.ne;
+    const int nr = region_count(P.formulation);
+    cplx acc[4] = {cx(0, 0), cx(0, 0), cx(0, 0), cx(0, 0)};
+    bool mine = false;
+    for (int se = lane; se < P.ne; se += 32) {
+        cplx blk[4][4];
+        if (!edge_pair_block(pairs, mass, inc, P, te, se, blk)) break;  // same answer for every se
+        mine = true;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (c >= nr) break;
+            const cplx xv = x[se + c * E];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[r] += blk[r][c] * xv;  // rows >= nr of blk are zero
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        double re = acc[r].re, im = acc[r].im;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        acc[r] = cx(re, im);
+    }
+    mine = __any_sync(0xffffffffu, mine);
+    if (mine && lane == 0) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (r < nr) y[te + r * E] += acc[r];
     }
 }
 
@@ -818,13 +877,16 @@ static int prepare_faces(sieb200_ctx* ctx, const sieb200_mesh& mesh, const float
     return SIEB200_OK;
 }
 
-int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
-                    const double* host_tensors, cplx* dZ, int64_t ldz) {
+// Assembly of Z (dx == nullptr) or, matrix-free, y = Z x with the same face
+// pair blocks contracted against x slab by slab instead of written to Z.
+static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                             const double* host_tensors, cplx* dZ, int64_t ldz, const cplx* dx, cplx* dy) {
     AssemblyParams ap;
     SIEB_RETURN_IF(make_assembly_params(opt, &ap));
     const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges, nv = (int)mesh.num_vertices;
+    (void)nv;
     const int64_t N = system_dimension(opt.formulation, ne);
-    SIEB_CHECK(ldz >= N, SIEB200_INVALID_ARG, "leading dimension of Z is smaller than N");
+    SIEB_CHECK(dx || ldz >= N, SIEB200_INVALID_ARG, "leading dimension of Z is smaller than N");
     float pts[2 * kMaxQ], wts[kMaxQ];
     const int Q = expand_rule(opt.quadrature_rule, pts, wts);
     SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
@@ -865,7 +927,10 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
     SIEB_RETURN_IF(ctx->counter.reserve(sizeof(unsigned long long)));
     unsigned long long* counter = ctx->counter.as<unsigned long long>();
 
-    SIEB_TRY_CUDA(cudaMemset2DAsync(dZ, sizeof(cplx) * ldz, 0, sizeof(cplx) * N, N, st));
+    if (dx)
+        SIEB_TRY_CUDA(cudaMemsetAsync(dy, 0, sizeof(cplx) * N, st));
+    else
+        SIEB_TRY_CUDA(cudaMemset2DAsync(dZ, sizeof(cplx) * ldz, 0, sizeof(cplx) * N, N, st));
 
     GatherParams gp;
     gp.formulation = opt.formulation;
@@ -921,12 +986,26 @@ int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_op
         }
         gp.m0 = m0;
         gp.m1 = m1;
-        const dim3 gb(32, 8), gg((ne + 31) / 32, (ne + 7) / 8);
-        gather_kernel<<<gg, gb, 0, st>>>(pairs, dmass, ctx->inc.as<int>(), gp, dZ, ldz);
+        if (dx) {
+            gather_matvec_kernel<<<(ne + 7) / 8, 256, 0, st>>>(pairs, dmass, ctx->inc.as<int>(), gp, dx, dy);
+        } else {
+            const dim3 gb(32, 8), gg((ne + 31) / 32, (ne + 7) / 8);
+            gather_kernel<<<gg, gb, 0, st>>>(pairs, dmass, ctx->inc.as<int>(), gp, dZ, ldz);
+        }
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
     }
     return SIEB200_OK;
+}
+
+int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                    const double* host_tensors, cplx* dZ, int64_t ldz) {
+    return assemble_or_apply(ctx, mesh, opt, host_tensors, dZ, ldz, nullptr, nullptr);
+}
+
+int matvec_free_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                       const double* host_tensors, const cplx* dx, cplx* dy) {
+    return assemble_or_apply(ctx, mesh, opt, host_tensors, nullptr, 0, dx, dy);
 }
 
 int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,

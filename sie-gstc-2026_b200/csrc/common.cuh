@@ -150,6 +150,9 @@ int expand_rule(int rule, float* pts, float* w);  // returns Q or -1
 // Assembly on the context stream into a device column-major N x N matrix.
 int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
                     const double* host_tensors, cplx* dZ, int64_t ldz);
+// y = Z x without storing Z (device vectors of length N), Z as assemble_device builds it.
+int matvec_free_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
+                       const double* host_tensors, const cplx* dx, cplx* dy);
 // s[f*32 + k] = lambda^H (dZ / d record[f][k]) x for the GSTC system (device
 // vectors of length 4 ne, s: num_faces x 32).
 int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,

@@ -253,6 +253,11 @@ int DenseSolver::factorize(double* A_, int64_t lda_) {
         factored = true;
         return SIEB200_OK;
     }
+    if (method == SIEB200_SOLVER_GMRES_C64) {
+        const int st = gmres_c64_prepare(this);
+        if (st == SIEB200_OK) factored = true;
+        return st;
+    }
     if (method == SIEB200_SOLVER_LU_FP64 || method == SIEB200_SOLVER_MIXED_IR) {
         const int st = mixed_factorize(this);
         if (st == SIEB200_OK) factored = true;

@@ -30,6 +30,7 @@ struct DenseSolver {
 };
 
 int mixed_factorize(DenseSolver* s);
+int gmres_c64_prepare(DenseSolver* s);
 int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
                 int maxit, int* iters);
 void mixed_release(DenseSolver* s);

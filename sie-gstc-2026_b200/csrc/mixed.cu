@@ -63,6 +63,7 @@ struct MixedState {
     // Conjugate-transpose solves (W^H = U^H L^H): W^H and the conjugate
     // transposes of the diagonal-block inverses, built on first use after a
     // factorization (in the solver's panel workspace).
+    cplx* dinv = nullptr;               // GMRES_C64: inverse diagonal of Z
     bool adj_ready = false;
     float2* WH = nullptr;
     float2* LinvH = nullptr;
@@ -888,6 +889,33 @@ __global__ void conj_transpose_c64_kernel(const float2* __restrict__ W, int64_t 
     }
 }
 
+// Complex128 (ld lda) to complex64 (ld n) copy of an n x n matrix.
+__global__ void to_c64_kernel(const cplx* __restrict__ A, int64_t lda, int64_t n, float2* __restrict__ W) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c = blockIdx.y;
+    if (r >= n) return;
+    const cplx v = A[r + c * lda];
+    W[r + c * n] = make_float2((float)v.re, (float)v.im);
+}
+
+// dinv[i] = 1 / A[i][i] (Jacobi preconditioner of GMRES_C64).
+__global__ void inv_diag_kernel(const cplx* __restrict__ A, int64_t lda, int64_t n, cplx* __restrict__ dinv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const cplx d = A[i + i * lda];
+    const double m = d.re * d.re + d.im * d.im;
+    dinv[i] = m > 0.0 ? cx(d.re / m, -d.im / m) : cx(1.0, 0.0);
+}
+
+// z = dinv .* v (or conj(dinv) .* v for the adjoint).
+__global__ void diag_scale_kernel(int64_t n, const cplx* __restrict__ dinv, const cplx* __restrict__ v, int conj_d,
+                                  cplx* __restrict__ z) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const cplx d = conj_d ? cx(dinv[i].re, -dinv[i].im) : dinv[i];
+    z[i] = d * v[i];
+}
+
 // Conjugate transpose of each NB x NB block (column-major) of `in`, one CTA per block.
 __global__ void conj_transpose_blocks_kernel(const float2* __restrict__ in, float2* __restrict__ out) {
     const float2* src = in + (size_t)blockIdx.x * NB * NB;
@@ -1089,6 +1117,36 @@ int mixed_factorize(DenseSolver* s) {
     return check_err(s, "mixed LU factorization");
 }
 
+// GMRES on a complex64 copy of Z: no factorization, the copy serves the
+// Krylov products, the FP64 matrix the restart residuals, and the inverse
+// diagonal of Z is the (right) preconditioner.
+int gmres_c64_prepare(DenseSolver* s) {
+    MixedState* st = state_of(s);
+    if (!st) {
+        st = new MixedState();
+        s->gemm_state = st;
+    }
+    const int64_t n = s->n;
+    st->n = n; st->np = n; st->ldw = n; st->nbl = 0;
+    st->adj_ready = false;
+    const size_t bW = ((sizeof(float2) * n * n + 255) / 256) * 256;
+    const size_t bD = ((sizeof(cplx) * n + 255) / 256) * 256;
+    SIEB_RETURN_IF(s->lu.reserve(bW + bD + 256));
+    st->W = s->lu.as<float2>();
+    st->dinv = reinterpret_cast<cplx*>(s->lu.as<char>() + bW);
+    st->err = reinterpret_cast<unsigned*>(s->lu.as<char>() + bW + bD);
+    cudaStream_t stream = s->ctx->stream;
+    SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, 256, stream));
+    to_c64_kernel<<<dim3(blocks_for(n, 256), (unsigned)n), 256, 0, stream>>>(reinterpret_cast<const cplx*>(s->A),
+                                                                             s->lda, n, st->W);
+    SIEB_NOTE_LAUNCH();
+    inv_diag_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(reinterpret_cast<const cplx*>(s->A), s->lda, n,
+                                                            st->dinv);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
 // Apply M^{-1} = V U^{-1} L^{-1} U^T (or its conjugate transpose) to r
 // (length n) into z (length n).
 static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, bool adjoint) {
@@ -1252,11 +1310,21 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         for (; j < m && total < maxit; ++j, ++total) {
             cplx* vj = V + (int64_t)j * n;
             cplx* zj = Zb + (int64_t)j * n;
-            SIEB_RETURN_IF(apply_precond(s, vj, zj, work, adjoint));
-            if (adjoint)
-                SIEB_RETURN_IF(gemv_h_device(ctx, n, A, lda, zj, 0.0, w));
-            else
-                SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
+            if (s->method == SIEB200_SOLVER_GMRES_C64) {
+                // Jacobi preconditioner; Krylov products with the complex64 copy
+                diag_scale_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, st->dinv, vj, adjoint ? 1 : 0, zj);
+                SIEB_NOTE_LAUNCH();
+                if (adjoint)
+                    SIEB_RETURN_IF(gemv_h_device(ctx, n, A, lda, zj, 0.0, w));
+                else
+                    SIEB_RETURN_IF(gemv_device(ctx, n, st->W, n, 1, zj, 0.0, w, s->gemv_scratch));
+            } else {
+                SIEB_RETURN_IF(apply_precond(s, vj, zj, work, adjoint));
+                if (adjoint)
+                    SIEB_RETURN_IF(gemv_h_device(ctx, n, A, lda, zj, 0.0, w));
+                else
+                    SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
+            }
             // Classical Gram-Schmidt with one reorthogonalization (CGS2).
             for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
             for (int pass = 0; pass < 2; ++pass) {
@@ -1339,7 +1407,8 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
 
 int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
                 int maxit, int* iters) {
-    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG, "unsupported solver method");
+    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR || s->method == SIEB200_SOLVER_GMRES_C64, SIEB200_INVALID_ARG,
+               "unsupported solver method");
     if (!(tol > 0)) tol = 1e-10;
     if (maxit <= 0) maxit = 50;
     int total = 0;

@@ -16,7 +16,7 @@ from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, load_obj, m
 from .solvers import (EXTERIOR, INTERIOR, Context, DenseLuSolver, DielectricOptions,
                       DipoleExcitation, GstcExcitationCase, GstcSieOptions, IsotropicMedium,
                       PecOptions, PlaneWaveExcitation, assemble_matrix, assemble_matrix_device,
-                      assemble_rhs, default_context, matvec, solve_dielectric_dense,
+                      assemble_rhs, default_context, matvec, matvec_matrix_free, solve_dielectric_dense,
                       solve_gstc_dense, solve_gstc_dense_batch, solve_pec_dense)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

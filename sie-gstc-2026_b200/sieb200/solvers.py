@@ -24,7 +24,7 @@ from . import _lib
 from .mesh import MeshData
 
 SOLVERS = {"lu_fp64": _lib.SOLVER_LU_FP64, "lu_cusolver": _lib.SOLVER_LU_CUSOLVER,
-           "mixed_ir": _lib.SOLVER_MIXED_IR}
+           "mixed_ir": _lib.SOLVER_MIXED_IR, "gmres_c64": 3}
 
 
 @dataclass
@@ -321,6 +321,24 @@ def assemble_rhs(mesh: MeshData, options, sources: Sequence, ctx: Optional[Conte
     _lib.check(_lib.lib().sieb200_assemble_rhs(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
                                                arr, len(sources), B.ctypes.data, 0))
     return B
+
+
+def matvec_matrix_free(mesh: MeshData, options, x: np.ndarray, tensors=None,
+                       ctx: Optional[Context] = None) -> np.ndarray:
+    """y = Z x with Z recomputed by the quadrature kernels, never stored
+    (sie_kernels_matvec.cuh:9-327 counterpart; host vectors)."""
+    ctx = ctx or default_context()
+    f = _formulation_of(options)
+    o = to_c_options(options, f)
+    N = system_dimension(options, mesh)
+    xv = np.ascontiguousarray(x, dtype=np.complex128).reshape(-1)
+    if xv.size != N:
+        raise ValueError(f"x must have {N} entries")
+    y = np.zeros(N, dtype=np.complex128)
+    t = _tensor_array(mesh, tensors, options.tensors_are_uniform) if f == _lib.GSTC else None
+    _lib.check(_lib.lib().sieb200_matvec_matrix_free(ctx.handle, ctypes.byref(mesh.as_c()), ctypes.byref(o),
+                                                     _lib.ptr(t), xv.ctypes.data, y.ctypes.data, 0))
+    return y
 
 
 class DenseLuSolver:
