@@ -22,7 +22,7 @@ def test_dunavant_rules_match_reference_bit_exact(golden, oracle_lib):
         oracle_lib.so_rule(rule, p.ctypes.data, w.ctypes.data)
         assert n == w_ref.size
         assert np.array_equal(p, p_ref) and np.array_equal(w, w_ref), rule
-    # published point counts (SURVEY/reference: rule 5 = 7, 7 = 13, 17 = 61, 20 = 79)
+    # published point counts (rule 5 = 7, 7 = 13, 17 = 61, 20 = 79)
     assert [oracle_lib.so_rule(r, None, None) for r in (1, 5, 7, 13, 17, 20)] == [1, 7, 13, 37, 61, 79]
 
 
