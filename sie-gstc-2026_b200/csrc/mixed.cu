@@ -40,8 +40,7 @@ constexpr int NB = 64;  // LU block size (complex columns)
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
 constexpr int kSmemPanel = (NB * (NB + 4) + 32 * (NB + 1)) * (int)sizeof(float2);
-constexpr int kDiagThreads = 1024;  // diagonal-block kernel: 16 column groups of NB rows
-static_assert(kDiagThreads % NB == 0 && NB % (kDiagThreads / NB) == 0, "diag thread layout");
+constexpr int kDiagThreads = 256;  // diagonal-block kernel: 8 warps of NB / 8 columns
 
 struct MixedState {
     int64_t n = 0, np = 0, ldw = 0, nbl = 0;
@@ -70,7 +69,7 @@ struct MixedState {
     float2* UinvH = nullptr;
     CUtensorMap tmWH;
     cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
-    cudaEvent_t ev_cols = nullptr, ev_panel = nullptr;
+    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr, ev_panel = nullptr;
 };
 
 // ------------------------------------------------------------ butterflies
@@ -224,130 +223,140 @@ __device__ __forceinline__ float2 crecipf(float2 a) {
     return make_float2(a.x * inv, -a.y * inv);
 }
 
-// Factor the kb x kb diagonal block in place without pivoting (one CTA,
-// block in shared memory), then form inv(L11) (unit lower) and inv(U11).
-__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(float2* __restrict__ W, int64_t ldw,
+__device__ __forceinline__ float2 cnegf(float2 a) { return make_float2(-a.x, -a.y); }
+// a - c x with fused multiply-adds.
+__device__ __forceinline__ float2 cfmsf(float2 a, float2 c, float2 x) {
+    return make_float2(fmaf(-c.x, x.x, fmaf(c.y, x.y, a.x)), fmaf(-c.x, x.y, fmaf(-c.y, x.x, a.y)));
+}
+__device__ __forceinline__ float2 shfl_c(float2 v, int src) {
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+// Diagonal block: LU without pivoting and both triangular inverses in one
+// pass of NB rank-1 steps over registers. Warp w holds columns
+// [kDiagCols w, kDiagCols (w+1)), lane l rows l and l+32. Step j takes the
+// coefficient column c_j = col_j / p_j (p_j the pivot, entry j zeroed) from
+// the warp that owns column j and applies  a(r, c) -= c_j(r) a(j, c)  to
+// every column c != j, restricted to rows r > j when c < j. Per column c
+// this is, in turn,
+//   * for j < c: the elimination itself (rows > j) and, in rows r < j, the
+//     accumulation of S(r, c) = -p_r inv(U~)(r, c), where U = D U~ (U~
+//     unit upper): the rows of the transposed elimination scaled by -p_r,
+//     which leaves row j of U in place at step j;
+//   * at j = c: the column becomes -l_c below the pivot (E_c = I - l_c e_c^T);
+//   * for j > c: inv(L) = E_{NB-1} ... E_0 accumulated below the diagonal.
+// So the register ends as [inv(L) strictly below | p_c | S strictly above],
+// with inv(U)(r, c) = -S(r, c) / (p_r p_c) and 1/p_c on the diagonal. The
+// block is padded to NB x NB with the identity (kb < NB only at the end).
+// A zero or non-finite pivot sets the error word and continues with a zero
+// reciprocal. The diagonal block of W itself is only read: everything after
+// the factorization takes the diagonal blocks from Linv / Uinv.
+constexpr int kDiagWarps = kDiagThreads / 32;
+constexpr int kDiagCols = NB / kDiagWarps;
+static_assert(kDiagCols % 2 == 0 && 32 % kDiagCols == 0, "diag column split");
+
+// Steps j = kDiagCols bp + u, u = 0 .. kDiagCols-1, all in row half H.
+template <int H>
+__device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, int w, int lane,
+                                           float2 (*cbuf)[NB], float2* rcps, unsigned* err) {
+    constexpr int CW = kDiagCols;
+#pragma unroll
+    for (int u = 0; u < CW; ++u) {
+        const int j = CW * bp + u, jl = j & 31, buf = u & 1;
+        const bool g0 = lane > j, g1 = lane + 32 > j;  // rows below the pivot
+        const float2 z = make_float2(0.f, 0.f);
+        float2 ca0, ca1;
+        if (w == bp) {  // publish c_j, then update this warp's other columns
+            const float2 piv = shfl_c(a[u][H], jl);
+            const float pm = piv.x * piv.x + piv.y * piv.y;
+            const bool bad = !(pm > 1e-30f) || !isfinite(pm);
+            if (bad && lane == 0) atomicCAS(err, 0u, 1u);
+            const float inv = bad ? 0.f : __frcp_rn(pm);
+            const float2 rcp = make_float2(piv.x * inv, -piv.y * inv);
+            ca0 = cmulf(a[u][0], rcp);
+            ca1 = cmulf(a[u][1], rcp);
+            if (lane == jl) {
+                if (H) ca1 = z;
+                else ca0 = z;
+            }
+            cbuf[buf][lane] = ca0;
+            cbuf[buf][lane + 32] = ca1;
+            if (lane == 0) rcps[j] = rcp;
+            a[u][0] = g0 ? cnegf(ca0) : a[u][0];
+            a[u][1] = g1 ? cnegf(ca1) : a[u][1];
+            const float2 cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+#pragma unroll
+            for (int v = 0; v < CW; ++v) {
+                if (v == u) continue;
+                const float2 x = shfl_c(a[v][H], jl);
+                if (v < u) {
+                    if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
+                    a[v][1] = cfmsf(a[v][1], cl1, x);
+                } else {
+                    a[v][0] = cfmsf(a[v][0], ca0, x);
+                    a[v][1] = cfmsf(a[v][1], ca1, x);
+                }
+            }
+        }
+        __syncthreads();
+        if (w != bp) {
+            ca0 = cbuf[buf][lane];
+            ca1 = cbuf[buf][lane + 32];
+            if (w < bp) {  // columns left of the pivot: rows below j only
+                const float2 cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+#pragma unroll
+                for (int v = 0; v < CW; ++v) {
+                    const float2 x = shfl_c(a[v][H], jl);
+                    if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
+                    a[v][1] = cfmsf(a[v][1], cl1, x);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < CW; ++v) {
+                    const float2 x = shfl_c(a[v][H], jl);
+                    a[v][0] = cfmsf(a[v][0], ca0, x);
+                    a[v][1] = cfmsf(a[v][1], ca1, x);
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __restrict__ W, int64_t ldw,
                                                                int64_t k0, int kb, float2* __restrict__ Linv,
                                                                float2* __restrict__ Uinv,
                                                                unsigned* __restrict__ err) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    float2(*A)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);             // [col][row]
-    float2(*X)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;
-    float2* Tb = reinterpret_cast<float2*>(dyn_smem) + 2 * NB * (NB + 1);             // NB*NB/4
-    __shared__ float2 colbuf[2][NB], rowbuf[2][NB];
-    constexpr int G = kDiagThreads / NB;  // column groups
-    constexpr int CPT = NB / G;           // columns per thread
-    const int tid = threadIdx.x;
-    // Elimination in registers: thread (r, g) owns row r, columns g + G u.
-    // The block is padded to NB x NB with the identity (kb < NB only at the
-    // end). Many warps with few columns each keep the latency-bound chain of
-    // NB steps short.
-    const int r = tid & (NB - 1), g = tid / NB;
-    float2 a[CPT];
+    constexpr int CW = kDiagCols;
+    __shared__ float2 cbuf[2][NB];  // c_j, double-buffered across the step barrier
+    __shared__ float2 rcps[NB];     // 1 / p_j
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float2 a[CW][2];
 #pragma unroll
-    for (int u = 0; u < CPT; ++u) {
-        const int c = g + G * u;
-        a[u] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
-    }
-    // One barrier per step; the pivot column and row go through
-    // double-buffered shared slots. Step j = jg + G uj is written as two
-    // loops so that the pivot column's register a[uj] has a static index.
+    for (int v = 0; v < CW; ++v)
 #pragma unroll
-    for (int uj = 0; uj < CPT; ++uj) {
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h, c = CW * w + v;
+            a[v][h] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
+        }
 #pragma unroll 1
-        for (int jg = 0; jg < G; ++jg) {
-            const int j = jg + G * uj;
-            const int buf = j & 1;
-            if (g == jg) colbuf[buf][r] = a[uj];
-            if (r == j) {
-#pragma unroll
-                for (int u = 0; u < CPT; ++u) rowbuf[buf][g + G * u] = a[u];
-            }
-            __syncthreads();
-            const float2 piv = rowbuf[buf][j];
-            const float pm = piv.x * piv.x + piv.y * piv.y;
-            if (!(pm > 1e-30f) || !isfinite(pm)) {  // block-uniform decision
-                if (tid == 0) atomicCAS(err, 0u, 1u);  // zero / non-finite pivot
-                return;
-            }
-            if (r > j) {
-                const float2 l = cmulf(colbuf[buf][r], crecipf(piv));
-#pragma unroll
-                for (int u = 0; u < CPT; ++u) {
-                    const int c = g + G * u;
-                    if (c > j) a[u] = csubf(a[u], cmulf(l, rowbuf[buf][c]));
-                    else if (c == j) a[u] = l;
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < CPT; ++u) {
-        const int c = g + G * u;
-        A[c][r] = a[u];
-        if (r < kb && c < kb) W[(k0 + r) + (k0 + c) * ldw] = a[u];
-    }
+    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<0>(a, bp, w, lane, cbuf, rcps, err);
+#pragma unroll 1
+    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<1>(a, bp, w, lane, cbuf, rcps, err);
     __syncthreads();
-    // Triangular inverses by recursive doubling: at level s the inverses of
-    // the s x s diagonal blocks are known, and each 2s block completes with
-    //   lower: X21 = -X22 (L21 X11),   upper: X12 = -X11 (U12 X22),
-    // two parallel s x s products and two barriers per level.
-    for (int lower = 1; lower >= 0; --lower) {
-        for (int e = tid; e < NB * NB; e += blockDim.x) {
-            const int rr = e & (NB - 1), cc = e >> 6;
-            X[cc][rr] = rr != cc ? make_float2(0.f, 0.f)
-                                 : (lower ? make_float2(1.f, 0.f) : crecipf(A[rr][rr]));
+#pragma unroll
+    for (int v = 0; v < CW; ++v) {
+        const int c = CW * w + v;
+        const float2 rc = rcps[c];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = lane + 32 * h;
+            const bool in = r < kb && c < kb;
+            const float2 one = make_float2(1.f, 0.f), z = make_float2(0.f, 0.f);
+            const float2 lv = r > c ? a[v][h] : (r == c ? one : z);
+            const float2 uv = r < c ? cnegf(cmulf(cmulf(a[v][h], rcps[r]), rc)) : (r == c ? rc : z);
+            Linv[r + c * NB] = in ? lv : z;
+            Uinv[r + c * NB] = in ? uv : z;
         }
-        __syncthreads();
-        for (int l = 0; (1 << l) < NB; ++l) {
-            const int s = 1 << l, work = (NB / 2) << l;  // (NB / 2s) blocks of s*s
-            for (int e = tid; e < work; e += blockDim.x) {
-                const int b = e >> (2 * l), rem = e & ((1 << (2 * l)) - 1);
-                const int i = rem & (s - 1), j = rem >> l, base = b * 2 * s;
-                float2 acc = make_float2(0.f, 0.f);
-                if (lower) {  // T = L21 X11, X11 lower: k >= j
-                    for (int k = j; k < s; ++k)
-                        acc = make_float2(acc.x + A[base + k][base + s + i].x * X[base + j][base + k].x -
-                                                  A[base + k][base + s + i].y * X[base + j][base + k].y,
-                                          acc.y + A[base + k][base + s + i].x * X[base + j][base + k].y +
-                                                  A[base + k][base + s + i].y * X[base + j][base + k].x);
-                } else {      // T = U12 X22, X22 upper: k <= j
-                    for (int k = 0; k <= j; ++k)
-                        acc = make_float2(acc.x + A[base + s + k][base + i].x * X[base + s + j][base + s + k].x -
-                                                  A[base + s + k][base + i].y * X[base + s + j][base + s + k].y,
-                                          acc.y + A[base + s + k][base + i].x * X[base + s + j][base + s + k].y +
-                                                  A[base + s + k][base + i].y * X[base + s + j][base + s + k].x);
-                }
-                Tb[e] = acc;
-            }
-            __syncthreads();
-            for (int e = tid; e < work; e += blockDim.x) {
-                const int b = e >> (2 * l), rem = e & ((1 << (2 * l)) - 1);
-                const int i = rem & (s - 1), j = rem >> l, base = b * 2 * s;
-                const float2* T = Tb + (b << (2 * l));
-                float2 acc = make_float2(0.f, 0.f);
-                if (lower) {  // X21 = -X22 T, X22 lower: k <= i
-                    for (int k = 0; k <= i; ++k) {
-                        const float2 x = X[base + s + k][base + s + i], t = T[k + (j << l)];
-                        acc = make_float2(acc.x + x.x * t.x - x.y * t.y, acc.y + x.x * t.y + x.y * t.x);
-                    }
-                    X[base + j][base + s + i] = make_float2(-acc.x, -acc.y);
-                } else {      // X12 = -X11 T, X11 upper: k >= i
-                    for (int k = i; k < s; ++k) {
-                        const float2 x = X[base + k][base + i], t = T[k + (j << l)];
-                        acc = make_float2(acc.x + x.x * t.x - x.y * t.y, acc.y + x.x * t.y + x.y * t.x);
-                    }
-                    X[base + s + j][base + i] = make_float2(-acc.x, -acc.y);
-                }
-            }
-            __syncthreads();
-        }
-        float2* out = lower ? Linv : Uinv;
-        for (int e = tid; e < NB * NB; e += blockDim.x) {
-            const int rr = e & (NB - 1), cc = e >> 6;
-            out[rr + cc * NB] = (rr < kb && cc < kb) ? X[cc][rr] : make_float2(0.f, 0.f);
-        }
-        __syncthreads();
     }
 }
 
@@ -940,6 +949,7 @@ void mixed_release(DenseSolver* s) {
     if (st) {
         if (st->gemm) gemm_tc_destroy(st->gemm);
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
+        if (st->ev_diag) cudaEventDestroy(st->ev_diag);
         if (st->ev_panel) cudaEventDestroy(st->ev_panel);
         if (st->side) cudaStreamDestroy(st->side);
         delete st;
@@ -1015,12 +1025,12 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_panel, cudaEventDisableTiming));
     }
 
     static bool attrs_set = false;
     if (!attrs_set) {
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_L_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
@@ -1044,11 +1054,12 @@ int mixed_factorize(DenseSolver* s) {
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, 8.0 * NB * NB * NB, 3.0 * 8.0 * NB * NB, &ev);
-        diag_lu_kernel<<<1, kDiagThreads, kSmemDiag, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
-                                                            st->Uinv + (size_t)bk * NB * NB, st->err);
+        diag_lu_kernel<<<1, kDiagThreads, 0, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
+                                                   st->Uinv + (size_t)bk * NB * NB, st->err);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
+        if (sm != stream) SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, sm));
         const int64_t s0 = k0 + kb;
         if (s0 < np) {
             ctx->prof.begin(sm, 4, 4.0 * NB * NB * (double)(np - s0), 8.0 * 2.0 * NB * (double)(np - s0), &ev);
@@ -1080,6 +1091,9 @@ int mixed_factorize(DenseSolver* s) {
     // Right-looking block LU with a lookahead of one block: after the update
     // of the next block's columns, its diagonal factorization and L21 panel
     // run on the side stream while the rest of the trailing update runs here.
+    // The next U12 panel needs only the diagonal inverses (and the trailing
+    // update), so it runs here concurrently with the L21 panel; the next
+    // block-column update then waits for both.
     SIEB_RETURN_IF(diag_and_L(0, stream));
     for (int64_t bk = 0; bk < nbl; ++bk) {
         const int64_t k0 = bk * NB;
@@ -1097,6 +1111,7 @@ int mixed_factorize(DenseSolver* s) {
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
             const float* A = st->Apack[bk & 1];
+            if (bk > 0) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
             SIEB_RETURN_IF(gemm(s0, s0, n1, A, st->Bpack, 0));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
@@ -1104,7 +1119,7 @@ int mixed_factorize(DenseSolver* s) {
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_panel, st->side));
             if (m > n1)
                 SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3, ctx->sm_count - side_sms(m)));
-            SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
+            SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
@@ -1113,6 +1128,7 @@ int mixed_factorize(DenseSolver* s) {
             SIEB_RETURN_IF(diag_and_L(bk + 1, stream));
         }
     }
+    if (st->use_tc) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));  // join the side stream
     ctx->prof.end(stream, ev_fact);
     return check_err(s, "mixed LU factorization");
 }
