@@ -45,6 +45,10 @@ C0 = 299792458.0
 METRIC = "solves/s mixed-prec+IR vs FP64 LU at rel.res≤1e-10 (1 B200); adjoint grads/s"
 WORKLOAD = ("T-PMCHWT dielectric sphere r=0.5 m, eps_r=4, mu_r=1, ka=pi; geodesic mesh 2000 faces / "
             "3000 RWG edges (N=6000); Dunavant rule 17; 1 plane-wave RHS")
+# DRAM bytes (read + write) per trailing-update launch, mean over the 185 launches of one
+# factorization of this workload, from one ncu capture
+# (profiles/gemm_tf32_sub_persistent_kernel_pmchwt_n6000.md, section 2).
+GEMM_DRAM_BYTES_PER_LAUNCH = 87.1e6
 
 
 def log(*a):
@@ -341,9 +345,12 @@ def run(args):
         gemm_tflops = gemm["flops"] / gemm_s / 1e12 if gemm_s > 0 else 0.0
         gemm_gbs = gemm["bytes"] / gemm_s / 1e9 if gemm_s > 0 else 0.0
         roofline = {
-            "kernel": "gemm_tf32_sub_kernel (split-TF32 trailing update, tcgen05)",
+            "kernel": "gemm_tf32_sub_persistent_kernel (split-TF32 trailing update, tcgen05)",
             "bound": "tensor", "achieved": gemm_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
-            "frac": gemm_tflops / tf32_peak, "traffic": None,
+            "frac": gemm_tflops / tf32_peak, "traffic": GEMM_DRAM_BYTES_PER_LAUNCH,
+            "traffic_note": "mean dram read+write bytes per trailing-update launch, ncu over the 185 "
+                            "launches of one N=6000 factorization",
+            "algorithmic_bytes_per_launch": gemm["bytes"] / gemm["launches"] if gemm["launches"] else None,
             "peak_note": f"TF32 dense = {peaks['source']} bf16 {peaks['bf16_tflops']} TFLOP/s / 2",
             "launches": gemm["launches"], "hbm_gbs_achieved": gemm_gbs,
             "hbm_frac": gemm_gbs / peaks["hbm_gbs"], "time_share": shares,
