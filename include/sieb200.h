@@ -269,10 +269,17 @@ int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const 
  * kernel 0: split-TF32 trailing GEMM (work = 2*m2*n*k TF32 flops and
  * 4*(2*m2*n + (m2 + n)*k) bytes per launch); 1: triangular solves
  * (work = bytes of factors read); 2: FP64 matvec (bytes of Z read);
- * 3: diagonal-block LU + inverses; 4: L21 panels; 5: U12 panels;
- * 6: whole mixed factorizations; 7: whole refined solves (spans on the
- * context stream; 3 and 4 run on the solver's lookahead stream). */
+ * 3: diagonal-block LU + inverses (with the previous block step's update
+ * of the block; on the solver's lookahead stream); 4: block-step panels
+ * (L21 with the previous step's update of its rows, and U12: one launch per
+ * step); 5: unused; 6: whole mixed factorizations; 7: whole refined solves
+ * (spans on the context stream unless stated). */
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable);
+/* enable = 2 also keeps a timeline: per span its kernel kind and its start
+ * and end in ms after the enable call (device timestamps, all streams).
+ * Copies up to `capacity` spans in recording order; *count = spans kept. */
+int sieb200_profile_timeline(sieb200_ctx* ctx, int64_t capacity, int* kernel, double* start_ms,
+                             double* end_ms, int64_t* count);
 /* Number of CUDA kernels the library has launched in this process. */
 int64_t sieb200_launch_count(void);
 int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,

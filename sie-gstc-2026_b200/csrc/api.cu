@@ -53,6 +53,8 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<long long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void Profiler::begin(cudaStream_t s, int kernel, double flops, double bytes, cudaEvent_t* end_out) {
     *end_out = nullptr;
@@ -93,6 +95,10 @@ void Profiler::collect() {
             kp.ms += ms;
             kp.flops += p.flops;
             kp.bytes += p.bytes;
+            float t0 = 0.f, t1 = 0.f;
+            if (timeline && base && cudaEventElapsedTime(&t0, base, p.a) == cudaSuccess &&
+                cudaEventElapsedTime(&t1, base, p.b) == cudaSuccess)
+                spans.push_back(Span{p.kernel, t0, t1});
         }
         pool.push_back(p.a);
         pool.push_back(p.b);
@@ -430,6 +436,7 @@ int sieb200_ctx_destroy(sieb200_ctx* ctx) {
     destroy_cusolver(ctx);
     ctx->prof.collect();
     for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
+    if (ctx->prof.base) cudaEventDestroy(ctx->prof.base);
     ctx->prof.pool.clear();
     ctx->faces.release(); ctx->geom.release(); ctx->qpts.release(); ctx->qw.release();
     ctx->pairs.release(); ctx->near_list.release(); ctx->counter.release(); ctx->inc.release();
@@ -718,10 +725,32 @@ int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t l
 int64_t sieb200_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable) {
-    SIEB_CHECK(ctx, SIEB200_INVALID_ARG, "context must not be null");
+    SIEB_CHECK(ctx && enable >= 0 && enable <= 2, SIEB200_INVALID_ARG, "invalid profile mode");
     ctx->prof.collect();
     ctx->prof.enabled = enable != 0;
     for (auto& k : ctx->prof.k) k = KernelProfile();
+    ctx->prof.spans.clear();
+    ctx->prof.timeline = enable == 2;
+    if (ctx->prof.timeline) {
+        SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+        if (!ctx->prof.base) SIEB_TRY_CUDA(cudaEventCreate(&ctx->prof.base));
+        SIEB_TRY_CUDA(cudaEventRecord(ctx->prof.base, ctx->stream));
+    }
+    return SIEB200_OK;
+}
+
+int sieb200_profile_timeline(sieb200_ctx* ctx, int64_t capacity, int* kernel, double* start_ms,
+                             double* end_ms, int64_t* count) {
+    SIEB_CHECK(ctx && count && capacity >= 0 && (capacity == 0 || (kernel && start_ms && end_ms)),
+               SIEB200_INVALID_ARG, "invalid timeline query");
+    ctx->prof.collect();
+    const auto& sp = ctx->prof.spans;
+    *count = (int64_t)sp.size();
+    for (int64_t i = 0; i < std::min<int64_t>(capacity, (int64_t)sp.size()); ++i) {
+        kernel[i] = sp[i].kernel;
+        start_ms[i] = sp[i].start_ms;
+        end_ms[i] = sp[i].end_ms;
+    }
     return SIEB200_OK;
 }
 

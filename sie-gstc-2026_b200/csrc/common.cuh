@@ -44,6 +44,8 @@ struct Status {
 
 // Process-wide count of kernels this library has launched (host side).
 void note_launch();
+void note_launches(long long n);  // n launches replayed from a CUDA graph
+long long launch_count();
 #define SIEB_NOTE_LAUNCH() ::sieb200::note_launch()
 
 // ------------------------------------------------------------------ math
@@ -106,6 +108,15 @@ struct Profiler {
     std::vector<cudaEvent_t> pool;  // events reused across collections
     static constexpr int kKinds = 8;
     KernelProfile k[kKinds];
+    // Optional timeline: every span's start and end relative to `base`,
+    // recorded on the context stream when the timeline was switched on.
+    struct Span {
+        int kernel;
+        float start_ms, end_ms;
+    };
+    bool timeline = false;
+    cudaEvent_t base = nullptr;
+    std::vector<Span> spans;
     // Returns an event pair recorded around a launch (nullptr events when off).
     void begin(cudaStream_t s, int kernel, double flops, double bytes, cudaEvent_t* end_out);
     void end(cudaStream_t s, cudaEvent_t e);

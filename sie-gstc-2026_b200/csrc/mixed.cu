@@ -39,7 +39,10 @@ constexpr int NB = 64;  // LU block size (complex columns)
 // Dynamic shared memory of the block kernels (two NB x (NB+1) complex64
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
-constexpr int kSmemPanel = (NB * (NB + 4) + 32 * (NB + 1)) * (int)sizeof(float2);
+constexpr int kSmemPanel = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(float2);
+// The diagonal-block kernel stages the previous step's two 64 x 64 factor
+// blocks; its size also keeps it off SMs that hold a trailing-GEMM CTA.
+constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
 constexpr int kDiagThreads = 256;  // diagonal-block kernel: 8 warps of NB / 8 columns
 
 struct MixedState {
@@ -69,8 +72,32 @@ struct MixedState {
     float2* UinvH = nullptr;
     CUtensorMap tmWH;
     cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
-    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr, ev_panel = nullptr;
+    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr;
+    // The factorization's launches as one CUDA graph (both streams and the
+    // event edges between them), captured on the second call with an
+    // unchanged key and replayed while it stays so; not while the profiler
+    // is on (its per-kernel events run eagerly).
+    struct GraphKey {
+        const void* A = nullptr;
+        int64_t lda = -1, n = -1;
+        const void* W = nullptr;
+        const void* pack = nullptr;
+        int use_tc = -1, sms = -1;
+        bool operator==(const GraphKey& o) const {
+            return A == o.A && lda == o.lda && n == o.n && W == o.W && pack == o.pack && use_tc == o.use_tc &&
+                   sms == o.sms;
+        }
+    };
+    GraphKey seen, captured;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_launches = 0;  // kernels per replay
 };
+
+static void drop_graph(MixedState* st) {
+    if (st->graph) cudaGraphExecDestroy(st->graph);
+    st->graph = nullptr;
+    st->captured = MixedState::GraphKey();
+}
 
 // ------------------------------------------------------------ butterflies
 __device__ __forceinline__ double rbt_value(uint64_t seed, int64_t i) {
@@ -322,11 +349,16 @@ __device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, in
     }
 }
 
+// With kp >= 0 the block first takes the previous block step's update,
+// A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32 FMA), from the two
+// factor blocks staged in dynamic shared memory (kSmemDiagUpd; that size
+// also keeps the kernel off SMs that hold a trailing-GEMM CTA).
 __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __restrict__ W, int64_t ldw,
                                                                int64_t k0, int kb, float2* __restrict__ Linv,
                                                                float2* __restrict__ Uinv,
-                                                               unsigned* __restrict__ err) {
+                                                               unsigned* __restrict__ err, int64_t kp) {
     constexpr int CW = kDiagCols;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ float2 cbuf[2][NB];  // c_j, double-buffered across the step barrier
     __shared__ float2 rcps[NB];     // 1 / p_j
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -338,6 +370,25 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __r
             const int r = lane + 32 * h, c = CW * w + v;
             a[v][h] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
         }
+    if (kp >= 0) {
+        float2(*Ls)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);           // [k][row]
+        float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;      // [col][k]
+        for (int e = threadIdx.x; e < NB * NB; e += kDiagThreads) {
+            const int i = e % NB, q = e / NB;  // i fastest: coalesced columns of W
+            Ls[q][i] = i < kb ? W[(k0 + i) + (kp + q) * ldw] : make_float2(0.f, 0.f);
+            Us[q][i] = q < kb ? W[(kp + i) + (k0 + q) * ldw] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        for (int kk = 0; kk < NB; ++kk) {
+            const float2 l0 = Ls[kk][lane], l1 = Ls[kk][lane + 32];
+#pragma unroll
+            for (int v = 0; v < CW; ++v) {
+                const float2 u = Us[CW * w + v][kk];
+                a[v][0] = cfmsf(a[v][0], l0, u);
+                a[v][1] = cfmsf(a[v][1], l1, u);
+            }
+        }
+    }
 #pragma unroll 1
     for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<0>(a, bp, w, lane, cbuf, rcps, err);
 #pragma unroll 1
@@ -368,25 +419,61 @@ __device__ __forceinline__ float tf32_hi(float x) {
 
 // L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
 // writes L21 back into W and the split realified rows into Apack.
+// With kp >= 0 the rows first take the previous block step's update of
+// these columns, A21 -= L21(kp) U12(kp)[:, k0:k0+kb] (FP32 FMA; the two
+// factors are the previous step's panels in W), so no separate GEMM
+// launch stands between the steps.
 // One CTA per 32 rows. Thread (ty, tx) computes rows 2ty, 2ty+1 and columns
 // 4tx .. 4tx+3 with k outermost; inv(U11) is upper triangular, so the k
 // loop stops at the thread's last column (tx is warp-uniform up to a pair).
 __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
                                              int64_t r0, int64_t np, const float2* __restrict__ Uinv,
-                                             float* __restrict__ Apack, int pack, int bx) {
+                                             float* __restrict__ Apack, int pack, int bx, int64_t kp) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2(*Us)[NB + 4] = reinterpret_cast<float2(*)[NB + 4]>(dyn_smem);                       // [k][c]
     float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * 8);   // [row][k]
+    float2(*Lr)[NB + 1] = Ar + 32;                                                             // [row][k]
     const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];  // Uinv[k + c*NB]
     const int64_t rb = r0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % 32, c = e / 32;
         const int64_t gr = rb + r;
         Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
     }
-    __syncthreads();
     const int ty = tid & 15, tx = tid >> 4;
+    if (kp >= 0) {
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+            const int kk = e % NB, c = e / NB;
+            Us[kk][c] = c < kb ? W[(kp + kk) + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+        }
+        for (int e = tid; e < 32 * NB; e += blockDim.x) {
+            const int r = e % 32, kk = e / 32;
+            const int64_t gr = rb + r;
+            Lr[r][kk] = gr < np ? W[gr + (kp + kk) * ldw] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        float2 upd[2][4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) upd[i][j] = Ar[2 * ty + i][4 * tx + j];
+        for (int kk = 0; kk < NB; ++kk) {
+            const float2 l0 = Lr[2 * ty][kk], l1 = Lr[2 * ty + 1][kk];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 u = Us[kk][4 * tx + j];
+                upd[0][j] = cfmsf(upd[0][j], l0, u);
+                upd[1][j] = cfmsf(upd[1][j], l1, u);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) Ar[2 * ty + i][4 * tx + j] = upd[i][j];
+    }
+    for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];  // Uinv[k + c*NB]
+    __syncthreads();
     float2 acc[2][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -494,18 +581,15 @@ __device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw
     }
 }
 
-// The two panels of a block step are separate launches: L21 is formed on
-// the lookahead stream as soon as its columns are updated, U12 once the
-// trailing update of its rows has finished.
-__global__ void __launch_bounds__(256) panel_L_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                                      int64_t s0, int64_t np, const float2* __restrict__ Uinv,
-                                                      float* __restrict__ Apack, int pack) {
-    panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x);
-}
-__global__ void __launch_bounds__(256) panel_U_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                                      int64_t s0, int64_t np, const float2* __restrict__ Linv,
-                                                      float* __restrict__ Bpack, int pack) {
-    panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x);
+// Both panels of a block step in one launch: CTAs [0, nL) form L21 (rows
+// below the diagonal block, with the previous step's update when kp >= 0),
+// the rest U12 (columns right of it).
+__global__ void __launch_bounds__(256, 3) panels_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                        int64_t s0, int64_t np, const float2* __restrict__ Uinv,
+                                                        const float2* __restrict__ Linv, float* __restrict__ Apack,
+                                                        float* __restrict__ Bpack, int pack, int nL, int64_t kp) {
+    if ((int)blockIdx.x < nL) panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x, kp);
+    else panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x - nL);
 }
 
 // SIMT trailing update C -= L21 U12 in complex64 (checking path).
@@ -947,10 +1031,10 @@ static MixedState* state_of(DenseSolver* s) { return static_cast<MixedState*>(s-
 void mixed_release(DenseSolver* s) {
     MixedState* st = state_of(s);
     if (st) {
+        drop_graph(st);
         if (st->gemm) gemm_tc_destroy(st->gemm);
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
-        if (st->ev_panel) cudaEventDestroy(st->ev_panel);
         if (st->side) cudaStreamDestroy(st->side);
         delete st;
     }
@@ -978,6 +1062,8 @@ static int check_err(DenseSolver* s, const char* what) {
     }
     return SIEB200_OK;
 }
+
+static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3);
 
 int mixed_factorize(DenseSolver* s) {
     SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG,
@@ -1026,16 +1112,60 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
-        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_panel, cudaEventDisableTiming));
     }
 
     static bool attrs_set = false;
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_L_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panel_U_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiagUpd));
         attrs_set = true;
     }
+
+    // Replay, capture or run eagerly (see MixedState::graph).
+    MixedState::GraphKey key;
+    key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
+    key.use_tc = st->use_tc; key.sms = ctx->sm_count;
+    const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
+    const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
+    if (graphs && st->graph && key == st->captured) {
+        SIEB_TRY_CUDA(cudaGraphLaunch(st->graph, stream));
+        note_launches(st->graph_launches);
+        return check_err(s, "mixed LU factorization");
+    }
+    const bool capture = graphs && key == st->seen;
+    st->seen = key;
+    if (capture) {
+        drop_graph(st);
+        const long long launches0 = launch_count();
+        SIEB_TRY_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = mixed_enqueue(s, st, bFlags, K3);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (rc == SIEB200_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&st->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (rc != SIEB200_OK || ce != cudaSuccess) {
+            drop_graph(st);
+            if (rc != SIEB200_OK) return rc;
+            cudaGetLastError();
+            set_error(std::string("capturing the factorization as a CUDA graph failed: ") + cudaGetErrorString(ce));
+            return SIEB200_CUDA_ERROR;
+        }
+        st->graph_launches = launch_count() - launches0;
+        st->captured = key;
+        SIEB_TRY_CUDA(cudaGraphLaunch(st->graph, stream));
+    } else {
+        SIEB_RETURN_IF(mixed_enqueue(s, st, bFlags, K3));
+    }
+    return check_err(s, "mixed LU factorization");
+}
+
+// Enqueues one mixed factorization on the context stream and the lookahead
+// stream (joined back at the end): eager or under stream capture.
+static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) {
+    sieb200_ctx* ctx = s->ctx;
+    cudaStream_t stream = ctx->stream;
+    const int64_t n = st->n, np = st->np, ldw = st->ldw, nbl = st->nbl;
     cudaEvent_t ev_fact;
     ctx->prof.begin(stream, 6, (8.0 / 3.0) * 4.0 * (double)np * np * np, 0.0, &ev_fact);
     SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
@@ -1048,34 +1178,41 @@ int mixed_factorize(DenseSolver* s) {
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
 
-    // Diagonal block bk and its L21 panel (into the A pack of step bk).
-    auto diag_and_L = [&](int64_t bk, cudaStream_t sm) -> int {
+    // Diagonal block bk (kp >= 0: after the update of step kp / NB).
+    auto diag_blk = [&](int64_t bk, int64_t kp, cudaStream_t sm) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         cudaEvent_t ev;
-        ctx->prof.begin(sm, 3, 8.0 * NB * NB * NB, 3.0 * 8.0 * NB * NB, &ev);
-        diag_lu_kernel<<<1, kDiagThreads, 0, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
-                                                   st->Uinv + (size_t)bk * NB * NB, st->err);
+        ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0),
+                        8.0 * NB * NB * (kp >= 0 ? 5.0 : 3.0), &ev);
+        diag_lu_kernel<<<1, kDiagThreads, kSmemDiagUpd, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
+                                                               st->Uinv + (size_t)bk * NB * NB, st->err, kp);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
-        if (sm != stream) SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, sm));
-        const int64_t s0 = k0 + kb;
-        if (s0 < np) {
-            ctx->prof.begin(sm, 4, 4.0 * NB * NB * (double)(np - s0), 8.0 * 2.0 * NB * (double)(np - s0), &ev);
-            panel_L_kernel<<<(unsigned)blocks_for(np - s0, 32), 256, kSmemPanel, sm>>>(
-                st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Apack[bk & 1], st->use_tc);
-            SIEB_NOTE_LAUNCH();
-            ctx->prof.end(sm, ev);
-            SIEB_TRY_CUDA(cudaGetLastError());
-        }
         return SIEB200_OK;
     };
-    // The trailing update proper leaves SMs to the lookahead stream (the
-    // persistent GEMM holds its SMs for the whole launch): 20 while the
-    // update is short enough for the diagonal block and L21 panel to be on
-    // the critical path, 6 once it is long (m > 8192) and they hide anyway.
-    auto side_sms = [](int64_t m) { return m > 8192 ? 6 : 20; };
+    // Both panels of block bk on the context stream (L21 into the A pack of
+    // step bk, after the update of step kp / NB when kp >= 0; U12 into the
+    // B pack).
+    auto panels = [&](int64_t bk, int64_t kp) -> int {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        const int64_t s0 = k0 + kb;
+        if (s0 >= np) return SIEB200_OK;
+        const int64_t m = np - s0;
+        const int nL = (int)blocks_for(m, 32);
+        cudaEvent_t ev;
+        ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m + (kp >= 0 ? 8.0 * NB * NB * (double)m : 0.0),
+                        8.0 * 4.0 * NB * (double)m + (kp >= 0 ? 8.0 * NB * (double)m : 0.0), &ev);
+        panels_kernel<<<(unsigned)(2 * nL), 256, kSmemPanel, stream>>>(
+            st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB,
+            st->Apack[bk & 1], st->Bpack, st->use_tc, nL, kp);
+        SIEB_NOTE_LAUNCH();
+        ctx->prof.end(stream, ev);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    };
     auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B,
                     int max_ctas) -> int {
         const int64_t m = np - s0;
@@ -1088,49 +1225,44 @@ int mixed_factorize(DenseSolver* s) {
         return SIEB200_OK;
     };
 
-    // Right-looking block LU with a lookahead of one block: after the update
-    // of the next block's columns, its diagonal factorization and L21 panel
-    // run on the side stream while the rest of the trailing update runs here.
-    // The next U12 panel needs only the diagonal inverses (and the trailing
-    // update), so it runs here concurrently with the L21 panel; the next
-    // block-column update then waits for both.
-    SIEB_RETURN_IF(diag_and_L(0, stream));
+    // Right-looking block LU with a lookahead of one block. Step bk: the
+    // panels of block bk are formed on the context stream; the next
+    // diagonal block takes its update from them and is factored on the side
+    // stream while the tensor-core trailing update (all columns but the
+    // next block's) runs here; then the next panels, whose L21 part applies
+    // step bk's update to the next block's remaining rows. The persistent
+    // GEMM leaves one SM to the diagonal kernel (whose shared memory keeps it
+    // off the GEMM's SMs).
+    SIEB_RETURN_IF(diag_blk(0, -1, stream));
+    SIEB_RETURN_IF(panels(0, -1));
     for (int64_t bk = 0; bk < nbl; ++bk) {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         const int64_t s0 = k0 + kb;
         if (s0 >= np) break;
         const int64_t m = np - s0;
-        cudaEvent_t evu;
-        ctx->prof.begin(stream, 5, 4.0 * NB * NB * (double)m, 8.0 * 2.0 * NB * (double)m, &evu);
-        panel_U_kernel<<<(unsigned)blocks_for(m, 32), 256, kSmemPanel, stream>>>(
-            st->W, ldw, k0, kb, s0, np, st->Linv + (size_t)bk * NB * NB, st->Bpack, st->use_tc);
-        SIEB_NOTE_LAUNCH();
-        ctx->prof.end(stream, evu);
-        SIEB_TRY_CUDA(cudaGetLastError());
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
-            const float* A = st->Apack[bk & 1];
-            if (bk > 0) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));
-            SIEB_RETURN_IF(gemm(s0, s0, n1, A, st->Bpack, 0));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
-            SIEB_RETURN_IF(diag_and_L(bk + 1, st->side));
-            SIEB_TRY_CUDA(cudaEventRecord(st->ev_panel, st->side));
+            SIEB_RETURN_IF(diag_blk(bk + 1, k0, st->side));
+            SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
             if (m > n1)
-                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, A, st->Bpack + n1 * K3, ctx->sm_count - side_sms(m)));
+                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * K3,
+                                    ctx->sm_count - 1));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
+            SIEB_RETURN_IF(panels(bk + 1, k0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
-            SIEB_RETURN_IF(diag_and_L(bk + 1, stream));
+            SIEB_RETURN_IF(diag_blk(bk + 1, -1, stream));
+            SIEB_RETURN_IF(panels(bk + 1, -1));
         }
     }
-    if (st->use_tc) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_panel, 0));  // join the side stream
     ctx->prof.end(stream, ev_fact);
-    return check_err(s, "mixed LU factorization");
+    return SIEB200_OK;
 }
 
 // GMRES on a complex64 copy of Z: no factorization, the copy serves the

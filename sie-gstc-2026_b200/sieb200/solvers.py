@@ -156,14 +156,28 @@ class Context:
     def synchronize(self) -> None:
         _lib.check(_lib.lib().sieb200_ctx_synchronize(self._h))
 
-    def profile(self, enable: bool = True) -> None:
-        """Start (and reset) or stop event timing of the library's hot kernels."""
-        _lib.check(_lib.lib().sieb200_profile_enable(self._h, int(bool(enable))))
+    def profile(self, enable: bool = True, timeline: bool = False) -> None:
+        """Start (and reset) or stop event timing of the library's hot kernels;
+        with timeline=True every span is also kept with its start and end."""
+        mode = (2 if timeline else 1) if enable else 0
+        _lib.check(_lib.lib().sieb200_profile_enable(self._h, mode))
+
+    def profile_timeline(self) -> list:
+        """[(kernel kind, start_ms, end_ms)] of the spans since profile(timeline=True),
+        times relative to that call (kinds as in profile_read)."""
+        count = ctypes.c_int64()
+        _lib.check(_lib.lib().sieb200_profile_timeline(self._h, 0, None, None, None, ctypes.byref(count)))
+        n = count.value
+        kinds = (ctypes.c_int * max(n, 1))()
+        t0 = (ctypes.c_double * max(n, 1))()
+        t1 = (ctypes.c_double * max(n, 1))()
+        _lib.check(_lib.lib().sieb200_profile_timeline(self._h, n, kinds, t0, t1, ctypes.byref(count)))
+        return [(kinds[i], t0[i], t1[i]) for i in range(min(n, count.value))]
 
     def profile_read(self, kernel: int) -> dict:
         """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec,
-        3: diagonal-block LU, 4: L21 panels, 5: U12 panels, 6: whole mixed
-        factorizations, 7: whole refined solves."""
+        3: diagonal-block LU, 4: block-step panels (L21 and U12), 5: unused,
+        6: whole mixed factorizations, 7: whole refined solves."""
         n = ctypes.c_int64()
         ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _lib.check(_lib.lib().sieb200_profile_read(self._h, int(kernel), ctypes.byref(n), ctypes.byref(ms),

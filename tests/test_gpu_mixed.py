@@ -201,3 +201,80 @@ def test_mixed_adjoint_matches_cusolver_on_pmchwt(gpu_ctx):
     assert np.linalg.norm(a - r) / np.linalg.norm(r) < 1e-9
     ref.close()
     mix.close()
+
+
+def test_profile_timeline_orders_the_block_steps(gpu_ctx):
+    """The profiler's timeline: one span per hot launch with start <= end,
+    every chain kernel inside the factorization span, one diagonal-block
+    kernel per block, one panels launch per block step and one tensor-core
+    trailing update per step but the last."""
+    import torch
+    import sieb200
+    n = 1000
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
+    Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()
+    s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+    gpu_ctx.profile(True, timeline=True)
+    s.factorize(Z.data_ptr())
+    gpu_ctx.synchronize()
+    spans = gpu_ctx.profile_timeline()
+    gpu_ctx.profile(False)
+    s.close()
+    assert spans and all(t0 <= t1 for _, t0, t1 in spans)
+    fact = [sp for sp in spans if sp[0] == 6]
+    assert len(fact) == 1
+    f0, f1 = fact[0][1], fact[0][2]
+    inner = [sp for sp in spans if sp[0] in (0, 3, 4)]
+    assert all(f0 - 1e-3 <= t0 and t1 <= f1 + 1e-3 for _, t0, t1 in inner)
+    nbl = -(-n // 64)
+    assert sum(1 for sp in spans if sp[0] == 3) == nbl
+    assert sum(1 for sp in spans if sp[0] == 4) == nbl - 1
+    # one trailing update per block step but the last (whose next block is the last one)
+    assert sum(1 for sp in spans if sp[0] == 0) == nbl - 2
+    diag = sorted(t0 for k, t0, _ in spans if k == 3)
+    assert diag == [t0 for k, t0, _ in spans if k == 3]  # recorded in step order
+
+
+def test_factorization_graph_replay_matches_eager(gpu_ctx, monkeypatch):
+    """The factorization is captured as a CUDA graph on its second call with
+    the same operand and replayed after that: the factors (seen through a
+    one-step preconditioned solve) are bit-identical to the eager run's. With
+    the profiler on it runs eagerly again and every span is recorded."""
+    import torch
+    import sieb200
+    n = 700
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()
+
+    def one_step(solver):  # one preconditioned step applies the factors once
+        x = torch.from_numpy(b.copy()).cuda()
+        torch.cuda.synchronize()
+        assert solver.solve(x.data_ptr(), tolerance=1e-5, max_iterations=1) == 1
+        gpu_ctx.synchronize()
+        return x.cpu().numpy()
+
+    monkeypatch.setenv("SIEB200_NO_GRAPHS", "1")
+    s0 = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+    s0.factorize(Z.data_ptr())
+    ref = one_step(s0)
+    s0.close()
+    monkeypatch.delenv("SIEB200_NO_GRAPHS")
+    s1 = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+    launches = []
+    for _ in range(4):  # eager, capture + launch, replay, replay
+        l0 = sieb200.lib().sieb200_launch_count()
+        s1.factorize(Z.data_ptr())
+        launches.append(sieb200.lib().sieb200_launch_count() - l0)
+        assert np.array_equal(one_step(s1), ref)
+    assert launches[0] == launches[1] == launches[2] == launches[3] > 0
+    gpu_ctx.profile(True, timeline=True)
+    s1.factorize(Z.data_ptr())
+    gpu_ctx.synchronize()
+    spans = gpu_ctx.profile_timeline()
+    gpu_ctx.profile(False)
+    assert np.array_equal(one_step(s1), ref)
+    s1.close()
+    assert sum(1 for sp in spans if sp[0] == 3) == -(-n // 64)
