@@ -88,15 +88,25 @@ struct MixedState {
                    sms == o.sms;
         }
     };
-    GraphKey seen, captured;
-    cudaGraphExec_t graph = nullptr;
-    long long graph_launches = 0;  // kernels per replay
+    // Two graphs (for example one per buffer of a caller that uploads the
+    // next system while this one is solved); the two keys seen last decide
+    // what is worth capturing.
+    struct Graph {
+        GraphKey key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;  // kernels per replay
+        uint64_t used = 0;
+    };
+    Graph graphs[2];
+    GraphKey seen[2];
+    uint64_t tick = 0;
 };
 
-static void drop_graph(MixedState* st) {
-    if (st->graph) cudaGraphExecDestroy(st->graph);
-    st->graph = nullptr;
-    st->captured = MixedState::GraphKey();
+static void drop_graphs(MixedState* st) {
+    for (auto& g : st->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = MixedState::Graph();
+    }
 }
 
 // ------------------------------------------------------------ butterflies
@@ -1031,7 +1041,7 @@ static MixedState* state_of(DenseSolver* s) { return static_cast<MixedState*>(s-
 void mixed_release(DenseSolver* s) {
     MixedState* st = state_of(s);
     if (st) {
-        drop_graph(st);
+        drop_graphs(st);
         if (st->gemm) gemm_tc_destroy(st->gemm);
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
@@ -1122,38 +1132,50 @@ int mixed_factorize(DenseSolver* s) {
         attrs_set = true;
     }
 
-    // Replay, capture or run eagerly (see MixedState::graph).
+    // Replay, capture or run eagerly (see MixedState::graphs).
     MixedState::GraphKey key;
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     key.use_tc = st->use_tc; key.sms = ctx->sm_count;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
-    if (graphs && st->graph && key == st->captured) {
-        SIEB_TRY_CUDA(cudaGraphLaunch(st->graph, stream));
-        note_launches(st->graph_launches);
-        return check_err(s, "mixed LU factorization");
+    if (graphs) {
+        for (auto& g : st->graphs) {
+            if (g.exec && g.key == key) {
+                g.used = ++st->tick;
+                SIEB_TRY_CUDA(cudaGraphLaunch(g.exec, stream));
+                note_launches(g.launches);
+                return check_err(s, "mixed LU factorization");
+            }
+        }
     }
-    const bool capture = graphs && key == st->seen;
-    st->seen = key;
+    const bool capture = graphs && (key == st->seen[0] || key == st->seen[1]);
+    if (!(key == st->seen[0])) {
+        st->seen[1] = st->seen[0];
+        st->seen[0] = key;
+    }
     if (capture) {
-        drop_graph(st);
+        MixedState::Graph& g = st->graphs[st->graphs[0].used <= st->graphs[1].used ? 0 : 1];
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = MixedState::Graph();
         const long long launches0 = launch_count();
         SIEB_TRY_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         const int rc = mixed_enqueue(s, st, bFlags, K3);
-        cudaGraph_t g = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(stream, &g);
-        if (rc == SIEB200_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&st->graph, g, 0);
-        if (g) cudaGraphDestroy(g);
+        cudaGraph_t cg = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(stream, &cg);
+        if (rc == SIEB200_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&g.exec, cg, 0);
+        if (cg) cudaGraphDestroy(cg);
         if (rc != SIEB200_OK || ce != cudaSuccess) {
-            drop_graph(st);
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g = MixedState::Graph();
             if (rc != SIEB200_OK) return rc;
             cudaGetLastError();
             set_error(std::string("capturing the factorization as a CUDA graph failed: ") + cudaGetErrorString(ce));
             return SIEB200_CUDA_ERROR;
         }
-        st->graph_launches = launch_count() - launches0;
-        st->captured = key;
-        SIEB_TRY_CUDA(cudaGraphLaunch(st->graph, stream));
+        g.key = key;
+        g.launches = launch_count() - launches0;
+        g.used = ++st->tick;
+        SIEB_TRY_CUDA(cudaGraphLaunch(g.exec, stream));
     } else {
         SIEB_RETURN_IF(mixed_enqueue(s, st, bFlags, K3));
     }

@@ -270,6 +270,11 @@ def test_factorization_graph_replay_matches_eager(gpu_ctx, monkeypatch):
         launches.append(sieb200.lib().sieb200_launch_count() - l0)
         assert np.array_equal(one_step(s1), ref)
     assert launches[0] == launches[1] == launches[2] == launches[3] > 0
+    # alternating between two copies of the operand keeps one graph for each
+    Z2 = Z.clone()
+    for i in range(6):
+        s1.factorize((Z2 if i % 2 == 0 else Z).data_ptr())
+        assert np.array_equal(one_step(s1), ref)
     gpu_ctx.profile(True, timeline=True)
     s1.factorize(Z.data_ptr())
     gpu_ctx.synchronize()
