@@ -45,10 +45,17 @@ C0 = 299792458.0
 METRIC = "solves/s mixed-prec+IR vs FP64 LU at rel.res≤1e-10 (1 B200); adjoint grads/s"
 WORKLOAD = ("T-PMCHWT dielectric sphere r=0.5 m, eps_r=4, mu_r=1, ka=pi; geodesic mesh 2000 faces / "
             "3000 RWG edges (N=6000); Dunavant rule 17; 1 plane-wave RHS")
-# DRAM bytes (read + write) per trailing-update launch, mean over the 185 launches of one
+# DRAM bytes (read + write) per trailing-update launch, mean over the 92 launches of one
 # factorization of this workload, from one ncu capture
 # (profiles/gemm_tf32_sub_persistent_kernel_pmchwt_n6000.md, section 2).
-GEMM_DRAM_BYTES_PER_LAUNCH = 87.1e6
+GEMM_DRAM_BYTES_PER_LAUNCH = 163.7e6
+# FP64 flops per Green evaluation (one point pair, one wavenumber) of the
+# T-PMCHWT regular pass, counted from the kernel's source with an FMA as 2:
+# the point-pair geometry shared by the two wavenumbers (distance, r_p.r_q,
+# r_p x r_q, weights: 23 flops, half each), the kernel values (11) and the
+# 8 TL + 10 TK complex moments (72); one sqrt, one reciprocal and one sincos
+# per evaluation are not counted.
+ASSEMBLY_FLOPS_PER_EVAL = 95
 
 
 def log(*a):
@@ -217,15 +224,17 @@ def run(args):
     mesh, opts = build_problem(args.rule)
     N = 2 * mesh.num_edges
 
-    # Assembly (reported, not part of a solve).
+    # Assembly (reported, not part of a solve): one warm-up, one timed.
     Z = torch.empty((N, N), dtype=torch.complex128, device="cuda")
-    torch.cuda.synchronize()
+    sieb200.assemble_matrix_device(mesh, opts, Z.data_ptr(), ctx=ctx)
+    ctx.synchronize()
     t0 = time.perf_counter()
     sieb200.assemble_matrix_device(mesh, opts, Z.data_ptr(), ctx=ctx)
     ctx.synchronize()
     t_asm = time.perf_counter() - t0
     Q = 61 if args.rule == 17 else sieb200.lib().sieb200_quadrature_rule(args.rule, None, None)
     evals = 2.0 * mesh.num_faces ** 2 * Q * Q  # Green evaluations (two wavenumbers)
+    fp64_peak = ctx.fp64_fma_peak()
     b = torch.from_numpy(sieb200.assemble_rhs(mesh, opts, [sieb200.PlaneWaveExcitation()], ctx=ctx)[:, 0].copy()).cuda()
     x = torch.empty_like(b)
 
@@ -387,7 +396,7 @@ def run(args):
             "kernel": "gemm_tf32_sub_persistent_kernel (split-TF32 trailing update, tcgen05)",
             "bound": "tensor", "achieved": gemm_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
             "frac": gemm_tflops / tf32_peak, "traffic": GEMM_DRAM_BYTES_PER_LAUNCH,
-            "traffic_note": "mean dram read+write bytes per trailing-update launch, ncu over the 185 "
+            "traffic_note": "mean dram read+write bytes per trailing-update launch, ncu over the 92 "
                             "launches of one N=6000 factorization",
             "algorithmic_bytes_per_launch": gemm["bytes"] / gemm["launches"] if gemm["launches"] else None,
             "peak_note": f"TF32 dense = {peaks['source']} bf16 {peaks['bf16_tflops']} TFLOP/s / 2",
@@ -417,6 +426,14 @@ def run(args):
             "relative_residual": rel_res, "rel_diff_vs_fp64_lu": rel_diff,
             "refinement_iterations": max(iters), "assembly_seconds": t_asm,
             "assembly_green_evals_per_s": evals / t_asm,
+            "assembly_roofline": {
+                "bound": "fp64 pipe", "unit": "TFLOP/s",
+                "flops_per_eval": ASSEMBLY_FLOPS_PER_EVAL,
+                "achieved": evals * ASSEMBLY_FLOPS_PER_EVAL / t_asm / 1e12,
+                "peak": fp64_peak, "peak_note": "measured FP64 FMA rate (sieb200_fp64_fma_peak)",
+                "frac": evals * ASSEMBLY_FLOPS_PER_EVAL / t_asm / 1e12 / fp64_peak,
+                "z_write_gbs": 16.0 * N * N / t_asm / 1e9,
+            },
             "adjoint": adjoint,
         }
         print(json.dumps(out), flush=True)

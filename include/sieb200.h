@@ -282,6 +282,10 @@ int sieb200_profile_timeline(sieb200_ctx* ctx, int64_t capacity, int* kernel, do
                              double* end_ms, int64_t* count);
 /* Number of CUDA kernels the library has launched in this process. */
 int64_t sieb200_launch_count(void);
+/* Measured FP64 FMA throughput of the context's device in TFLOP/s (FMA = 2
+ * flops; dependent-FMA chains on every SM, best of 5 timed launches): the
+ * denominator of the assembly's FP64-pipe roofline (no reference counterpart). */
+int sieb200_fp64_fma_peak(sieb200_ctx* ctx, double* tflops);
 int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,
                          double* flops, double* bytes);
 

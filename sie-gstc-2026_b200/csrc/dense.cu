@@ -5,6 +5,8 @@
 // dispatches to the mixed-precision path (mixed.cu).
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cusolverDn.h>
 
 #include <mutex>
@@ -283,6 +285,51 @@ int DenseSolver::solve(int64_t nrhs, double* B, int64_t ldb, bool adjoint, doubl
         return SIEB200_OK;
     }
     return mixed_solve(this, nrhs, B, ldb, adjoint, tol, maxit, iters);
+}
+
+
+// FP64 FMA throughput probe: 8 independent dependent-FMA chains per thread,
+// 4 CTAs of 256 threads per SM; the result is written only if it equals a
+// value it never takes, which keeps the chains live.
+__global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* out, int iters) {
+    const double m = 1.0000000001, c = 1e-12;
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = 1.0 + 1e-6 * (threadIdx.x + 32 * j);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fma(a[j], m, c);
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sum += a[j];
+    if (sum == -1.0) out[0] = sum;
+}
+
+int fp64_fma_rate(sieb200_ctx* ctx, double* tflops) {
+    const int iters = 8192;
+    const unsigned grid = (unsigned)ctx->sm_count * 4u;
+    DeviceBuffer sink;
+    SIEB_RETURN_IF(sink.reserve(sizeof(double)));
+    cudaEvent_t a, b;
+    SIEB_TRY_CUDA(cudaEventCreate(&a));
+    SIEB_TRY_CUDA(cudaEventCreate(&b));
+    float best = 1e30f;
+    for (int rep = 0; rep < 6; ++rep) {
+        cudaEventRecord(a, ctx->stream);
+        fp64_fma_probe_kernel<<<grid, 256, 0, ctx->stream>>>(sink.as<double>(), iters);
+        SIEB_NOTE_LAUNCH();
+        cudaEventRecord(b, ctx->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess && rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    SIEB_TRY_CUDA(cudaGetLastError());
+    const double flops = 2.0 * 8.0 * iters * (double)grid * 256.0;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return SIEB200_OK;
 }
 
 }  // namespace sieb200

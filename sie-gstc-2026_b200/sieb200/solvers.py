@@ -162,6 +162,12 @@ class Context:
         mode = (2 if timeline else 1) if enable else 0
         _lib.check(_lib.lib().sieb200_profile_enable(self._h, mode))
 
+    def fp64_fma_peak(self) -> float:
+        """Measured FP64 FMA throughput of this context's device, TFLOP/s."""
+        t = ctypes.c_double()
+        _lib.check(_lib.lib().sieb200_fp64_fma_peak(self._h, ctypes.byref(t)))
+        return t.value
+
     def profile_timeline(self) -> list:
         """[(kernel kind, start_ms, end_ms)] of the spans since profile(timeline=True),
         times relative to that call (kinds as in profile_read)."""

@@ -283,3 +283,10 @@ def test_factorization_graph_replay_matches_eager(gpu_ctx, monkeypatch):
     assert np.array_equal(one_step(s1), ref)
     s1.close()
     assert sum(1 for sp in spans if sp[0] == 3) == -(-n // 64)
+
+
+def test_fp64_fma_peak_is_plausible(gpu_ctx):
+    """The FP64 roofline denominator: a B200's 148 SMs at up to ~2 GHz give a
+    few tens of TFLOP/s of FP64 FMA, far from zero and from tensor rates."""
+    t = gpu_ctx.fp64_fma_peak()
+    assert 5.0 < t < 200.0
