@@ -636,6 +636,17 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Published solution entries: every 8-byte word of the publication buffer
+// starts as all ones (a NaN payload arithmetic does not produce) and is
+// written once; each word is single-copy atomic, so an entry whose two
+// words both differ from it is complete.
+__device__ __forceinline__ double ld_relaxed_f64(const double* p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ bool unpublished(double v) { return __double_as_longlong(v) == -1ll; }
+
 __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -652,8 +663,10 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
 // inside the CTA: the first with its explicit inverse, published at once,
 // then the coupling block and the second inverse.
 //
-// progress[0]: number of NB sub-blocks published in solve order; progress[1]:
-// ticket counter; both cleared by the host. A CTA waits only for CTAs with
+// A solved sub-block is published by writing its entries into xpub (all
+// ones beforehand, set by the host), which consumers poll entry by entry;
+// progress[0] also counts published sub-blocks; progress[1] is the ticket
+// counter; both cleared by the host. A CTA waits only for CTAs with
 // smaller tickets, which are already running. Every wait is bounded by
 // timeout_ns from the CTA's start; on timeout the error word is set, the CTA
 // still consumes every tile its producer issues (so no copy is in flight at
@@ -682,8 +695,8 @@ __device__ __forceinline__ bool tr_wait(uint32_t bar, uint32_t parity, uint64_t 
 
 __global__ void __launch_bounds__(TR_THREADS, 1)
 trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, int lower,
-                const float2* __restrict__ Dinv, cplx* __restrict__ x, unsigned* __restrict__ progress,
-                unsigned* __restrict__ err, unsigned long long timeout_ns) {
+                const float2* __restrict__ Dinv, cplx* __restrict__ x, cplx* __restrict__ xpub,
+                unsigned* __restrict__ progress, unsigned* __restrict__ err, unsigned long long timeout_ns) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];  // aligned to 1024 below
     const uint32_t raw = smem_u32(dyn_smem);
     unsigned char* base = dyn_smem + (((raw + 1023u) & ~1023u) - raw);
@@ -769,39 +782,39 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     // stages its NB x entries in shared memory (double-buffered by group
     // parity), so both tiles cost one L2 round trip; one consumer barrier
     // per group hands them to all warps.
-    unsigned seen = 0;
     for (int i = 0, g = 0; i < n_off; ++g) {
         const int sb = (tile_k(i) * TR_COLS) / NB;
         const int cnt = (i + 1 < n_off && (tile_k(i + 1) * TR_COLS) / NB == sb) ? 2 : 1;
         const unsigned need = lower ? (unsigned)sb + 1u : (unsigned)(nsb - sb);
         cplx* xg = xstage + (g & 1) * NB;
         if (warp == 0) {
+            // Each lane polls its entries of the sub-block in the publication
+            // buffer: the value is the flag, one L2 round trip per entry.
             bool okp = !s_abort;
-            if (okp && seen < need) {
-                if (lane == 0) {
+            for (int e = lane; e < NB; e += 32) {
+                const int64_t c = (int64_t)sb * NB + e;
+                cplx v = cx(0, 0);
+                if (okp && c < np) {
                     int it = 0;
-                    unsigned p = seen;
                     while (true) {
-                        p = ld_acquire_gpu(&progress[0]);
-                        if (p >= need) break;
-                        if (need - p > 4) __nanosleep(256);
-                        if ((++it & 63) == 0 &&
+                        const double vr = ld_relaxed_f64(&xpub[c].re), vi = ld_relaxed_f64(&xpub[c].im);
+                        if (!unpublished(vr) && !unpublished(vi)) {
+                            v = cx(vr, vi);
+                            break;
+                        }
+                        if (++it > 16) __nanosleep(64);
+                        if ((it & 63) == 0 &&
                             (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
                             atomicCAS(err, 0u, 2u);
                             s_abort = 1;
+                            okp = false;
                             break;
                         }
                     }
-                    seen = p;
                 }
-                seen = __shfl_sync(0xffffffffu, seen, 0);
-                okp = seen >= need;
-                __syncwarp();
+                xg[e] = v;
             }
-            for (int e = lane; e < NB; e += 32) {
-                const int64_t c = (int64_t)sb * NB + e;
-                xg[e] = (okp && c < np) ? cx(__ldcg(&x[c].re), __ldcg(&x[c].im)) : cx(0, 0);
-            }
+            __syncwarp();
         }
         consumer_bar();
         for (int j = 0; j < cnt; ++j, ++i) {
@@ -861,6 +874,8 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
             if (gr < np) {
                 __stcg(&x[gr].re, re);
                 __stcg(&x[gr].im, im);
+                __stcg(&xpub[gr].re, re);
+                __stcg(&xpub[gr].im, im);
             }
         }
         // The barrier orders every store of the sub-block before the release.
@@ -1376,13 +1391,16 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     const unsigned long long timeout_ns = 2000000000ull;
     // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
     const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
+    SIEB_RETURN_IF(s->flags.reserve(sizeof(cplx) * (size_t)np));
+    cplx* xpub = s->flags.as<cplx>();
     for (int lower = 1; lower >= 0; --lower) {
         const float2* dinv = adjoint ? (lower ? st->UinvH : st->LinvH) : (lower ? st->Linv : st->Uinv);
         SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * 2, stream));
+        SIEB_TRY_CUDA(cudaMemsetAsync(xpub, 0xFF, sizeof(cplx) * (size_t)np, stream));
         cudaEvent_t ev;
         s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
         trsv_tma_kernel<<<ncta, TR_THREADS, kSmemTrsv, stream>>>(adjoint ? st->tmWH : st->tmW, np, nbl, lower,
-                                                                 dinv, work, fl, st->err, timeout_ns);
+                                                                 dinv, work, xpub, fl, st->err, timeout_ns);
         SIEB_NOTE_LAUNCH();
         s->ctx->prof.end(stream, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
