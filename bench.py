@@ -56,6 +56,13 @@ GEMM_DRAM_BYTES_PER_LAUNCH = 163.7e6
 # 8 TL + 10 TK complex moments (72); one sqrt, one reciprocal and one sincos
 # per evaluation are not counted.
 ASSEMBLY_FLOPS_PER_EVAL = 95
+# FP64 flops per field evaluation (one observation point, one face, one
+# quadrature point) of the surface-field kernel, counted from its source with
+# an FMA as 2: G and grad G (26), then for each of the three half-RWG
+# functions rho (3), the L vector (36) and the K vector (36), plus the face's
+# edge-length scaling and E/H accumulation spread over the rule's 61 points
+# (~6); one sqrt, two divisions and one sincos are not counted.
+FIELDS_FLOPS_PER_EVAL = 257
 
 
 def log(*a):
@@ -371,6 +378,7 @@ def run(args):
     solver.close()
 
     # CPU baseline (rank 0, one GPU only): the reference's CPU solve of this system.
+    fields = fields_section(ctx, mesh, fp64_peak, with_cpu=(rank == 0 and world == 1 and not args.no_cpu))
     adjoint = adjoint_section(ctx, args.adjoint_steps, max_over_ranks) if args.adjoint_steps > 0 else None
     if adjoint is not None:
         adjoint["grads_per_s"] *= world
@@ -434,6 +442,7 @@ def run(args):
                 "frac": evals * ASSEMBLY_FLOPS_PER_EVAL / t_asm / 1e12 / fp64_peak,
                 "z_write_gbs": 16.0 * N * N / t_asm / 1e9,
             },
+            "fields": fields,
             "adjoint": adjoint,
         }
         print(json.dumps(out), flush=True)
@@ -450,6 +459,49 @@ ADJOINT_WORKLOAD = ("SIE-GSTC adjoint synthesis: circular-arc spindle (arc radiu
                     "revolved mesh 9800 faces / 14700 RWG edges (N=58800), f=300 MHz, Dunavant rule 5; "
                     "omega parameters (B, X, chi) per face (29400 reals, seeded, |chi^2-BX|>=0.25); "
                     "objective = far-field power in a 10 deg cone about +z; x-polarised plane wave along +z")
+
+
+def fields_section(ctx, mesh, fp64_peak: float, with_cpu: bool) -> dict:
+    """Surface-integral field values on a cut around the sphere: 361
+    directions (phi = 0 and 90 degrees, theta in 1-degree steps) at 0.55 m
+    (faces within 0.1 lambda of a point take the analytic part) and 3 m,
+    seeded synthetic currents, vacuum, Dunavant rule 17. Timed through the
+    public call (host points and currents in, host fields out)."""
+    import sieb200
+    th = np.radians(np.arange(181.0))
+    dirs = np.concatenate([np.column_stack([np.sin(th), np.zeros_like(th), np.cos(th)]),
+                           np.column_stack([np.zeros_like(th[1:-1]), np.sin(th[1:-1]), np.cos(th[1:-1])])])
+    pts = np.concatenate([0.55 * dirs, 3.0 * dirs])
+    rng = np.random.default_rng(5)
+    ne = mesh.num_edges
+    J = rng.standard_normal(ne) + 1j * rng.standard_normal(ne)
+    M = 377.0 * (rng.standard_normal(ne) + 1j * rng.standard_normal(ne))
+    call = lambda p: sieb200.evaluate_surface_integral_fields(mesh, J, M, p, C0, None, 17, ctx=ctx)  # noqa: E731
+    call(pts)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        call(pts)
+    t = (time.perf_counter() - t0) / reps
+    Q = 61
+    evals = float(pts.shape[0]) * mesh.num_faces * Q
+    out = {"points": int(pts.shape[0]), "faces": mesh.num_faces, "rule": 17, "seconds": t,
+           "points_per_s": pts.shape[0] / t, "evals_per_s": evals / t,
+           "roofline": {"bound": "fp64 pipe", "flops_per_eval": FIELDS_FLOPS_PER_EVAL,
+                        "achieved": evals * FIELDS_FLOPS_PER_EVAL / t / 1e12, "peak": fp64_peak,
+                        "unit": "TFLOP/s", "frac": evals * FIELDS_FLOPS_PER_EVAL / t / 1e12 / fp64_peak}}
+    if with_cpu:
+        from oracle import oracle as O
+        ref = O.reference()
+        if ref is not None:
+            sample = pts[::45]
+            t0 = time.perf_counter()
+            O.surface_fields(ref, mesh, J, M, sample, C0, rule=17)
+            tc = time.perf_counter() - t0
+            out["cpu_reference"] = {"points_per_s": sample.shape[0] / tc, "cores": 1, "kind": "reference",
+                                    "sample": f"{sample.shape[0]} of the cut's points, the reference's own "
+                                              "per-face helpers on one host thread (oracle/_ref)"}
+    return out
 
 
 def adjoint_section(ctx, steps: int, max_over_ranks):

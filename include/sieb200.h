@@ -310,6 +310,25 @@ int sieb200_far_field_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, double 
                              const double* r_hat, const double* theta_hat, const double* phi_hat, int a_on_device,
                              double* A);
 
+/* Surface-integral field values at observation points
+ * (evaluate_surface_integral_fields, include/sie_mom/solvers/
+ * surface_current_fields.hpp:12-44; kernel sie_kernels_utils.cuh:21-140):
+ *   E = +j w mu L[J] + K[M],   H = -K[J] + j w eps L[M]
+ * with w = 2 pi f, eps = eps_r eps0, mu = mu_r mu0, k = w sqrt(mu eps); each
+ * face by ordinary quadrature of the given Dunavant rule, or by quadrature of
+ * the extracted kernel plus the analytic (Wilton) part when its centroid is
+ * within 0.1 wavelength of the point. These are not the scattered or total
+ * fields by themselves (F_total = F_incident - Q in the region of the
+ * currents). j_cur, m_cur: host, num_edges physical coefficients each
+ * (complex interleaved; m_cur NULL = 0). points: host, nobs x 3. E, H: host,
+ * nobs x 3 complex interleaved. Same validation as the reference
+ * (positive finite frequency, media and vacuum constants, rule 1..20,
+ * finite points); nobs = 0 returns at once. */
+int sieb200_surface_fields(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,
+                           const double* m_cur, int64_t nobs, const double* points, double frequency_hz,
+                           double eps_r, double mu_r, double eps0, double mu0, int rule, double* E,
+                           double* H);
+
 #ifdef __cplusplus
 }
 #endif

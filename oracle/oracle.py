@@ -32,6 +32,9 @@ def _build_oracle() -> None:
                    capture_output=True)
 
 
+_FIELDS = [_P, _P, _P, _i, _i, _P, _P, _i, _P, _d, _d, _d, _d, _d, _i, _P, _P]
+
+
 def oracle() -> ctypes.CDLL:
     _build_oracle()
     lib = ctypes.CDLL(str(ORACLE_SO))
@@ -42,6 +45,7 @@ def oracle() -> ctypes.CDLL:
     lib.so_assemble.argtypes = _ASSEMBLE
     lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P]
     lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
+    lib.so_surface_fields.argtypes = _FIELDS
     return lib
 
 
@@ -58,6 +62,7 @@ def reference() -> ctypes.CDLL | None:
     lib.ref_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
     lib.ref_assemble.argtypes = _ASSEMBLE
     lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P]
+    lib.ref_surface_fields.argtypes = _FIELDS
     lib.ref_lu_solve.argtypes = [_i, _P, _P, _P, _i, _i]
     lib.ref_lu_solve.restype = _d
     lib.ref_max_threads.restype = _i
@@ -141,3 +146,23 @@ def far_field(lib, mesh, j, m, k0, eta0, r_hat, theta_hat, phi_hat):
     if rc != 0:
         raise ValueError("oracle far field: edge numbering mismatch")
     return ft, fp, U
+
+
+def surface_fields(lib, mesh, j, m, points, frequency_hz, eps_r=1.0, mu_r=1.0, eps0=8.8541878188e-12,
+                   mu0=1.25663706127e-6, rule=17):
+    """(E, H) surface-integral terms (nobs x 3 complex) from the C
+    restatement (lib = oracle()) or the reference harness (lib = reference())."""
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
+    j = np.ascontiguousarray(j, dtype=np.complex128)
+    m = None if m is None else np.ascontiguousarray(m, dtype=np.complex128)
+    P = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    E = np.zeros((P.shape[0], 3), np.complex128)
+    H = np.zeros((P.shape[0], 3), np.complex128)
+    fn = lib.so_surface_fields if hasattr(lib, "so_surface_fields") else lib.ref_surface_fields
+    rc = fn(_p(V), _p(F), _p(FE), F.shape[0], int(mesh.edges.shape[0]), _p(j), _p(m), P.shape[0], _p(P),
+            float(frequency_hz), float(eps_r), float(mu_r), float(eps0), float(mu0), int(rule), _p(E), _p(H))
+    if rc != 0:
+        raise ValueError("surface fields: invalid quadrature rule")
+    return E, H

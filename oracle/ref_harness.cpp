@@ -379,6 +379,70 @@ int ref_rhs_plane_wave(int kind, const double* V, const int* F, const int* FE, i
     return 0;
 }
 
+// Surface-integral field values Q_E = j w mu L[J] + K[M], Q_H = -K[J] + j w eps L[M]
+// at observation points, with the reference's own per-face quadrature helpers
+// (calculateScatterFieldQuadrature / calculateScatterFieldSingular,
+// dunavant_quadrature.cuh:1634-1770) in the loop of compute_scattered_fields_kernel
+// (sie_kernels_utils.cuh:21-140) and the constants of
+// surface_current_fields.cu:96-112 and :255-275. J, M, E, H complex interleaved.
+int ref_surface_fields(const double* V, const int* F, const int* FE, int nf, int ne, const double* J,
+                       const double* M, int nobs, const double* obs, double freq, double eps_r,
+                       double mu_r, double eps0, double mu0, int rule, double* E, double* H) {
+    (void)ne;
+    const Quad q = make_rule(rule);
+    const real_t pi = std::acos(real_t(-1));
+    const real_t omega = real_t(2) * pi * freq;
+    const real_t epsilon = eps_r * eps0, mu = mu_r * mu0;
+    const real_t k = omega * std::sqrt(mu * epsilon);
+    const complex__float coeff_J = make_complex(real_t(0), omega * mu);
+    const complex__float coeff_M = make_complex(real_t(1), real_t(0));
+    const complex__float coeff_J_h = make_complex(real_t(-1), real_t(0));
+    const complex__float coeff_M_h = make_complex(real_t(0), omega * epsilon);
+    for (int p = 0; p < nobs; ++p) {
+        const vec3_t obs_point = make_vec3(obs[3 * p], obs[3 * p + 1], obs[3 * p + 2]);
+        const complex__float zero = make_complex(real_t(0), real_t(0));
+        cvec3_t acc_E = make_cvec3(zero, zero, zero), acc_H = make_cvec3(zero, zero, zero);
+        for (int f = 0; f < nf; ++f) {
+            const int ti[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
+            vec3_t tv[3];
+            for (int a = 0; a < 3; ++a) tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+            const vec3_t centroid = (tv[0] + tv[1] + tv[2]) / 3.f;
+            const float dist = length(obs_point - centroid);
+            const float lambda = 2.0f * static_cast<float>(M_PI) / k;
+            const float threshold = 0.1f * lambda;
+            cvec3_t Lr[3], Kr[3];
+            if (dist < threshold) {
+                calculateScatterFieldQuadrature(obs_point, tv, ti, q.pts.data(), q.w.data(), q.n, k, true, Lr, Kr);
+                cvec3_t Ls[3], Ks[3];
+                calculateScatterFieldSingular(obs_point, tv, ti, k, Ls, Ks);
+                for (int i = 0; i < 3; ++i) {
+                    Lr[i] += Ls[i];
+                    Kr[i] += Ks[i];
+                }
+            } else {
+                calculateScatterFieldQuadrature(obs_point, tv, ti, q.pts.data(), q.w.data(), q.n, k, false, Lr, Kr);
+            }
+            for (int i = 0; i < 3; ++i) {
+                const int e = FE[3 * f + i];
+                const complex__float je = make_complex(J[2 * e], J[2 * e + 1]);
+                const complex__float me = M ? make_complex(M[2 * e], M[2 * e + 1]) : zero;
+                acc_E += complexMul(coeff_J, je) * Lr[i];
+                acc_E += complexMul(coeff_M, me) * Kr[i];
+                acc_H += complexMul(coeff_J_h, je) * Kr[i];
+                acc_H += complexMul(coeff_M_h, me) * Lr[i];
+            }
+        }
+        const cvec3_t* outs[2] = {&acc_E, &acc_H};
+        double* dst[2] = {E + 6 * (size_t)p, H + 6 * (size_t)p};
+        for (int o = 0; o < 2; ++o) {
+            dst[o][0] = outs[o]->x.x; dst[o][1] = outs[o]->x.y;
+            dst[o][2] = outs[o]->y.x; dst[o][3] = outs[o]->y.y;
+            dst[o][4] = outs[o]->z.x; dst[o][5] = outs[o]->z.y;
+        }
+    }
+    return 0;
+}
+
 // Eigen partial-pivot LU solve in complex128 (the reference host tests'
 // solver, tests/cpp/sie_dielectric_sphere_test.cpp:290). A column-major.
 // Returns seconds spent in factor+solve.

@@ -785,3 +785,169 @@ int so_far_field(const double* V, const int* F, int nf, int ne, const double* j_
     free(FE); free(rq); free(cj); free(cm);
     return 0;
 }
+
+/* ---------------------------------------- surface-integral field values -- */
+/* green_functions_utils.cuh:142-221: G and grad G of the field evaluation,
+ * standard (R < 1e-12 -> 0) or with the static and k^2 terms extracted
+ * (R < 1e-6 -> G = -jk/(4 pi), grad G = 0). */
+static void green_grad(v3 r1, v3 r2, double k, int regular, cx* G, cx g[3]) {
+    v3 Rv = vsub(r1, r2);
+    double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+    if (!regular) {
+        if (R < 1e-12) {
+            *G = CX(0.0, 0.0);
+            g[0] = g[1] = g[2] = CX(0.0, 0.0);
+            return;
+        }
+        double inv_R = 1.0 / R;
+        v3 Rh = V3(Rv.x * inv_R, Rv.y * inv_R, Rv.z * inv_R);
+        double i4pR = 1.0 / (4.0 * M_PI * R);
+        double s = sin(k * R), c = cos(k * R);
+        *G = CX(c * i4pR, -s * i4pR);
+        cx wg = cmul(CX(inv_R, k), *G);
+        g[0] = cscale(wg, Rh.x);
+        g[1] = cscale(wg, Rh.y);
+        g[2] = cscale(wg, Rh.z);
+    } else {
+        if (R < 1e-6) {
+            *G = CX(0.0, -k / (4.0 * M_PI));
+            g[0] = g[1] = g[2] = CX(0.0, 0.0);
+            return;
+        }
+        double i4p = 1.0 / (4.0 * M_PI);
+        double inv_R = 1.0 / R, inv_R2 = inv_R * inv_R, inv_R3 = inv_R2 * inv_R;
+        double i4pR = i4p * inv_R;
+        double s = sin(k * R), c = cos(k * R);
+        *G = CX((c - 1.0) * i4pR, -s * i4pR);
+        cx Kr = cmul(CX(inv_R3, k * inv_R2), CX(c, -s));
+        Kr.re += -(inv_R3 + k * k * 0.5 * inv_R);
+        cx sc = cscale(Kr, i4p);
+        g[0] = cscale(sc, Rv.x);
+        g[1] = cscale(sc, Rv.y);
+        g[2] = cscale(sc, Rv.z);
+    }
+}
+
+/* dunavant_quadrature.cuh:1634-1705: L and K integrals of the three half-RWG
+ * functions of source triangle S at obs (k arrives as float; 1/k^2 and the
+ * edge lengths are float). */
+static void field_quad(v3 obs, const tri_t* S, const float* pts, const float* wts, int Q, float k,
+                       int regular, cx L[3][3], cx K[3][3]) {
+    memset(L, 0, sizeof(cx) * 9);
+    memset(K, 0, sizeof(cx) * 9);
+    const float k_sq_inv = 1.f / (k * k);
+    for (int q = 0; q < Q; ++q) {
+        v3 rq = map_point(S, (double)pts[2 * q], (double)pts[2 * q + 1]);
+        const double w = (double)wts[q];
+        cx G, g[3];
+        green_grad(obs, rq, (double)k, regular, &G, g);
+        for (int i = 0; i < 3; ++i) {
+            v3 rho = vsub(rq, S->free_v[i]);
+            const double rc[3] = {rho.x, rho.y, rho.z};
+            for (int c = 0; c < 3; ++c) {
+                cx l1 = cscale(cscale(G, rc[c]), 0.5);
+                cx l2 = cscale(g[c], (double)(-k_sq_inv));
+                L[i][c] = cadd(L[i][c], cscale(cadd(l1, l2), w));
+            }
+            cx cr[3];
+            cr[0] = csub(cscale(g[2], rho.y), cscale(g[1], rho.z));
+            cr[1] = csub(cscale(g[0], rho.z), cscale(g[2], rho.x));
+            cr[2] = csub(cscale(g[1], rho.x), cscale(g[0], rho.y));
+            for (int c = 0; c < 3; ++c) K[i][c] = cadd(K[i][c], cscale(cscale(cr[c], 0.5), w));
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        const double el = (double)(float)S->len[i];
+        for (int c = 0; c < 3; ++c) {
+            L[i][c] = cscale(L[i][c], el);
+            K[i][c] = cscale(K[i][c], el);
+        }
+    }
+}
+
+/* dunavant_quadrature.cuh:1719-1770: the analytic (Wilton) parts that the
+ * extracted quadrature leaves out; real-valued, scaled by l_i / (8 pi A) in
+ * float. */
+static void field_singular(v3 obs, const tri_t* S, float k, cx L[3][3], cx K[3][3]) {
+    const float A = (float)(0.5f * vlen(vcross(vsub(S->v[1], S->v[0]), vsub(S->v[2], S->v[0]))));
+    const float base_scale = 1.0f / (8.0f * (float)M_PI * A);
+    pots_t P = wilton(obs, S->v);
+    const float k_sq_inv = 1.f / (k * k);
+    for (int i = 0; i < 3; ++i) {
+        v3 fv = S->free_v[i];
+        v3 Rf = vsub(obs, fv);
+        v3 ps = psi1(&P, fv);
+        v3 phi3 = vadd(P.phi3b, vscale(vsub(P.r_pi, fv), P.phi2));
+        v3 Lin = vadd(vsub(ps, vscale(vscale(Rf, 0.5), P.phi0)),
+                      vscale(vsub(phi3, vscale(Rf, P.phi2)), (double)k_sq_inv));
+        v3 Kv = upsilon(&P, fv, obs, k);
+        const float l_scale = (float)S->len[i] * base_scale;
+        v3 Lv = vscale(Lin, 2.0);
+        L[i][0] = CX(Lv.x * l_scale, 0.0); L[i][1] = CX(Lv.y * l_scale, 0.0); L[i][2] = CX(Lv.z * l_scale, 0.0);
+        K[i][0] = CX(Kv.x * l_scale, 0.0); K[i][1] = CX(Kv.y * l_scale, 0.0); K[i][2] = CX(Kv.z * l_scale, 0.0);
+    }
+}
+
+/* surface_current_fields.cu:96-112 and sie_kernels_utils.cuh:21-140: the
+ * positive surface-integral terms Q_E = j w mu L[J] + K[M] and
+ * Q_H = -K[J] + j w eps L[M] at each observation point, every face by
+ * ordinary quadrature, or by extracted quadrature plus the Wilton part when
+ * its centroid is within 0.1 lambda (float distance and threshold). J, M:
+ * physical coefficients per edge (complex interleaved). E, H out: nobs x 3
+ * complex interleaved. */
+int so_surface_fields(const double* V, const int* F, const int* FE, int nf, int ne, const double* J,
+                      const double* M, int nobs, const double* obs, double freq, double eps_r, double mu_r,
+                      double eps0, double mu0, int rule, double* E, double* H) {
+    float pts[2 * 100], wts[100];
+    const int Q = so_rule(rule, pts, wts);
+    if (Q <= 0) return -1;
+    (void)ne;
+    const double omega = 2.0 * M_PI * freq;
+    const double eps = eps_r * eps0, mu = mu_r * mu0;
+    const double k = omega * sqrt(mu * eps);
+    const cx cJ = CX(0.0, omega * mu), cM = CX(1.0, 0.0), cJh = CX(-1.0, 0.0), cMh = CX(0.0, omega * eps);
+    const float lambda = (float)((double)(2.0f * (float)M_PI) / k);
+    const float thr = 0.1f * lambda;
+    const float kf = (float)k;
+    for (int p = 0; p < nobs; ++p) {
+        v3 r = V3(obs[3 * p], obs[3 * p + 1], obs[3 * p + 2]);
+        cx e[3] = {{0, 0}, {0, 0}, {0, 0}}, h[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int f = 0; f < nf; ++f) {
+            tri_t S;
+            load_tri(V, F, f, &S);
+            const v3 c = V3((S.v[0].x + S.v[1].x + S.v[2].x) / 3.0, (S.v[0].y + S.v[1].y + S.v[2].y) / 3.0,
+                            (S.v[0].z + S.v[1].z + S.v[2].z) / 3.0);
+            const float dist = (float)vlen(vsub(r, c));
+            cx L[3][3], K[3][3];
+            if (dist < thr) {
+                cx Ls[3][3], Ks[3][3];
+                field_quad(r, &S, pts, wts, Q, kf, 1, L, K);
+                field_singular(r, &S, kf, Ls, Ks);
+                for (int i = 0; i < 3; ++i)
+                    for (int d = 0; d < 3; ++d) {
+                        L[i][d] = cadd(L[i][d], Ls[i][d]);
+                        K[i][d] = cadd(K[i][d], Ks[i][d]);
+                    }
+            } else {
+                field_quad(r, &S, pts, wts, Q, kf, 0, L, K);
+            }
+            for (int i = 0; i < 3; ++i) {
+                const int ed = FE[3 * f + i];
+                const cx je = CX(J[2 * ed], J[2 * ed + 1]);
+                const cx me = M ? CX(M[2 * ed], M[2 * ed + 1]) : CX(0.0, 0.0);
+                const cx wEJ = cmul(cJ, je), wEM = cmul(cM, me), wHJ = cmul(cJh, je), wHM = cmul(cMh, me);
+                for (int d = 0; d < 3; ++d) {
+                    e[d] = cadd(e[d], cmul(wEJ, L[i][d]));
+                    e[d] = cadd(e[d], cmul(wEM, K[i][d]));
+                    h[d] = cadd(h[d], cmul(wHJ, K[i][d]));
+                    h[d] = cadd(h[d], cmul(wHM, L[i][d]));
+                }
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            E[6 * p + 2 * d] = e[d].re; E[6 * p + 2 * d + 1] = e[d].im;
+            H[6 * p + 2 * d] = h[d].re; H[6 * p + 2 * d + 1] = h[d].im;
+        }
+    }
+    return 0;
+}

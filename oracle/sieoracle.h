@@ -24,6 +24,9 @@ int so_far_field(const double* V, const int* F, int nf, int ne, const double* j_
                  const double* m_cur, double k0, double eta0, int ndir, const double* r_hat,
                  const double* theta_hat, const double* phi_hat, double* f_theta, double* f_phi,
                  double* intensity);
+int so_surface_fields(const double* V, const int* F, const int* FE, int nf, int ne, const double* J,
+                      const double* M, int nobs, const double* obs, double freq, double eps_r, double mu_r,
+                      double eps0, double mu0, int rule, double* E, double* H);
 
 #ifdef __cplusplus
 }

@@ -819,4 +819,16 @@ int sieb200_far_field_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, double 
     return SIEB200_OK;
 }
 
+int sieb200_surface_fields(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,
+                           const double* m_cur, int64_t nobs, const double* points, double frequency_hz,
+                           double eps_r, double mu_r, double eps0, double mu0, int rule, double* E,
+                           double* H) {
+    SIEB_CHECK(ctx && mesh && mesh->vertices && mesh->faces && mesh->faces_edges && j_cur &&
+                   (nobs == 0 || (points && E && H)),
+               SIEB200_INVALID_ARG, "invalid surface-field arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    return sieb200::surface_fields_device(ctx, *mesh, j_cur, m_cur, nobs, points, frequency_hz, eps_r, mu_r,
+                                          eps0, mu0, rule, E, H);
+}
+
 }  // extern "C"

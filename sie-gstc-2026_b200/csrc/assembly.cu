@@ -1031,4 +1031,223 @@ int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sie
     return SIEB200_OK;
 }
 
+// ------------------------------------------------ surface-integral fields
+// The positive surface-integral terms at observation points,
+//   Q_E = j w mu L[J] + K[M],   Q_H = -K[J] + j w eps L[M]
+// (surface_current_fields.hpp:12-44, kernel sie_kernels_utils.cuh:21-140).
+
+// G and grad G of the field evaluation (green_functions_utils.cuh:142-221):
+// standard, or with the static and k^2/2 terms extracted.
+__device__ __forceinline__ void field_green(d3 r1, d3 r2, double k, bool regular, cplx& G, cplx g[3]) {
+    const d3 Rv = r1 - r2;
+    const double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+    if (!regular) {
+        if (R < 1e-12) {
+            G = cx(0.0, 0.0);
+            g[0] = g[1] = g[2] = cx(0.0, 0.0);
+            return;
+        }
+        const double inv_R = 1.0 / R;
+        const double i4pR = 1.0 / (4.0 * kPi * R);
+        double s, c;
+        sincos(k * R, &s, &c);
+        G = cx(c * i4pR, -s * i4pR);
+        const cplx wg = cx(inv_R, k) * G;
+        g[0] = wg * (Rv.x * inv_R);
+        g[1] = wg * (Rv.y * inv_R);
+        g[2] = wg * (Rv.z * inv_R);
+    } else {
+        if (R < 1e-6) {
+            G = cx(0.0, -k / (4.0 * kPi));
+            g[0] = g[1] = g[2] = cx(0.0, 0.0);
+            return;
+        }
+        const double i4p = 1.0 / (4.0 * kPi);
+        const double inv_R = 1.0 / R, inv_R2 = inv_R * inv_R, inv_R3 = inv_R2 * inv_R;
+        double s, c;
+        sincos(k * R, &s, &c);
+        G = cx((c - 1.0) * (i4p * inv_R), -s * (i4p * inv_R));
+        cplx Kr = cx(inv_R3, k * inv_R2) * cx(c, -s);
+        Kr.re += -(inv_R3 + k * k * 0.5 * inv_R);
+        const cplx sc = Kr * i4p;
+        g[0] = sc * Rv.x;
+        g[1] = sc * Rv.y;
+        g[2] = sc * Rv.z;
+    }
+}
+
+struct FieldConsts {
+    cplx cJ, cM, cJh, cMh;   // j w mu, 1, -1, j w eps
+    float k;                 // the wavenumber as the quadrature helpers receive it
+    float k_sq_inv;          // 1 / k^2 in float
+    float threshold;         // 0.1 lambda in float
+};
+
+// One CTA of 256 threads per observation point; threads take faces
+// f = t, t + 256, ...; per face the three half-RWG integrals
+// (dunavant_quadrature.cuh:1634-1705, plus the Wilton part of :1719-1770
+// when the face centroid is within 0.1 lambda), folded into E and H; a warp
+// butterfly and one pass over the warps in a fixed order sum them.
+__global__ void __launch_bounds__(256) surface_fields_kernel(const FaceGeom* __restrict__ geom,
+                                                            const d3* __restrict__ qp,
+                                                            const float* __restrict__ qw, int Q, int nf,
+                                                            const d3* __restrict__ obs,
+                                                            const cplx* __restrict__ J,
+                                                            const cplx* __restrict__ M, FieldConsts fc,
+                                                            cplx* __restrict__ E, cplx* __restrict__ H) {
+    const d3 r = obs[blockIdx.x];
+    const double kd = (double)fc.k;
+    cplx e[3] = {cx(0, 0), cx(0, 0), cx(0, 0)}, h[3] = {cx(0, 0), cx(0, 0), cx(0, 0)};
+    for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+        const FaceGeom g = geom[f];
+        // float distance from the centroid, formed without contraction
+        const double dx = __dsub_rn(r.x, g.c.x), dy = __dsub_rn(r.y, g.c.y), dz = __dsub_rn(r.z, g.c.z);
+        const float dist = (float)__dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                                       __dmul_rn(dz, dz)));
+        const bool near = dist < fc.threshold;
+        cplx L[3][3], K[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { L[i][c] = cx(0, 0); K[i][c] = cx(0, 0); }
+        for (int q = 0; q < Q; ++q) {
+            const d3 rq = qp[(size_t)f * Q + q];
+            const double w = (double)qw[q];
+            cplx G, gg[3];
+            field_green(r, rq, kd, near, G, gg);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const d3 rho = rq - g.fv[i];
+                const double rc[3] = {rho.x, rho.y, rho.z};
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    L[i][c] += ((G * rc[c]) * 0.5 + gg[c] * (double)(-fc.k_sq_inv)) * w;
+                const cplx cr[3] = {gg[2] * rho.y - gg[1] * rho.z, gg[0] * rho.z - gg[2] * rho.x,
+                                    gg[1] * rho.x - gg[0] * rho.y};
+#pragma unroll
+                for (int c = 0; c < 3; ++c) K[i][c] += (cr[c] * 0.5) * w;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double el = (double)(float)g.len[i];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { L[i][c] = L[i][c] * el; K[i][c] = K[i][c] * el; }
+        }
+        if (near) {
+            const float A = (float)g.area;
+            const float base = __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(8.0f, (float)kPi), A));
+            const Pots P = wilton(r, g.v);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const d3 fv = g.fv[i];
+                const d3 Rf = r - fv;
+                const d3 phi3 = P.phi3b + (P.r_pi - fv) * P.phi2;
+                const d3 Lin = (psi1(P, fv) - (Rf * 0.5) * P.phi0) + (phi3 - Rf * P.phi2) * (double)fc.k_sq_inv;
+                const d3 Kv = upsilon(P, fv, r, fc.k);
+                const double ls = (double)__fmul_rn((float)g.len[i], base);
+                const d3 Lv = Lin * 2.0;
+                L[i][0] += cx(Lv.x * ls, 0.0); L[i][1] += cx(Lv.y * ls, 0.0); L[i][2] += cx(Lv.z * ls, 0.0);
+                K[i][0] += cx(Kv.x * ls, 0.0); K[i][1] += cx(Kv.y * ls, 0.0); K[i][2] += cx(Kv.z * ls, 0.0);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int ed = g.edge[i];
+            const cplx je = J[ed], me = M ? M[ed] : cx(0, 0);
+            const cplx wEJ = fc.cJ * je, wEM = fc.cM * me, wHJ = fc.cJh * je, wHM = fc.cMh * me;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                e[c] += wEJ * L[i][c];
+                e[c] += wEM * K[i][c];
+                h[c] += wHJ * K[i][c];
+                h[c] += wHM * L[i][c];
+            }
+        }
+    }
+    __shared__ double part[8][12];
+    double v[12] = {e[0].re, e[0].im, e[1].re, e[1].im, e[2].re, e[2].im,
+                    h[0].re, h[0].im, h[1].re, h[1].im, h[2].re, h[2].im};
+#pragma unroll
+    for (int j = 0; j < 12; ++j) warp_sum(v[j]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < 12; ++j) part[warp][j] = v[j];
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w][threadIdx.x];
+        double* out = reinterpret_cast<double*>(threadIdx.x < 6 ? E : H) + 6 * (size_t)blockIdx.x;
+        out[threadIdx.x % 6] = t;
+    }
+}
+
+int surface_fields_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j_cur, const double* m_cur,
+                          int64_t nobs, const double* points, double frequency_hz, double eps_r, double mu_r,
+                          double eps0, double mu0, int rule, double* E_out, double* H_out) {
+    auto fin = [](double x) { return std::isfinite(x); };
+    SIEB_CHECK(frequency_hz > 0 && fin(frequency_hz), SIEB200_INVALID_ARG,
+               "field-evaluation frequency must be positive and finite");
+    SIEB_CHECK(eps_r > 0 && mu_r > 0 && fin(eps_r) && fin(mu_r), SIEB200_INVALID_ARG,
+               "field-evaluation relative permittivity and permeability must be positive and finite");
+    SIEB_CHECK(eps0 > 0 && mu0 > 0 && fin(eps0) && fin(mu0), SIEB200_INVALID_ARG,
+               "field-evaluation vacuum constants must be positive and finite");
+    SIEB_CHECK(rule >= 1 && rule <= 20, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
+    SIEB_CHECK(nobs >= 0 && nobs < (1ll << 31), SIEB200_INVALID_ARG, "observation point count out of range");
+    for (int64_t p = 0; p < nobs; ++p)
+        SIEB_CHECK(fin(points[3 * p]) && fin(points[3 * p + 1]) && fin(points[3 * p + 2]), SIEB200_INVALID_ARG,
+                   "non-finite observation point at index " + std::to_string(p));
+    if (nobs == 0) return SIEB200_OK;
+    SIEB_CHECK(mesh.num_vertices > 0 && mesh.num_faces > 0 && mesh.num_edges > 0, SIEB200_INVALID_ARG,
+               "field-evaluation mesh must contain vertices, faces, and edges");
+    const int nf = (int)mesh.num_faces, ne = (int)mesh.num_edges;
+    float pts[2 * kMaxQ], wts[kMaxQ];
+    const int Q = expand_rule(rule, pts, wts);
+    SIEB_CHECK(Q > 0 && Q <= kMaxQ, SIEB200_INVALID_ARG, "Dunavant quadrature rule must be in [1, 20]");
+    cudaStream_t st = ctx->stream;
+    FaceGeom* geom = nullptr;
+    d3* qp = nullptr;
+    float* dw = nullptr;
+    int* dFE = nullptr;
+    SIEB_RETURN_IF(prepare_faces(ctx, mesh, pts, wts, Q, &geom, &qp, &dw, &dFE));
+
+    // surface_current_fields.cu:96-112 (medium constants) and :255-275 (coefficients).
+    const double pi = std::acos(-1.0);
+    const double omega = 2.0 * pi * frequency_hz;
+    const double eps = eps_r * eps0, mu = mu_r * mu0;
+    const double k = omega * std::sqrt(mu * eps);
+    FieldConsts fc;
+    fc.cJ = cx(0.0, omega * mu);
+    fc.cM = cx(1.0, 0.0);
+    fc.cJh = cx(-1.0, 0.0);
+    fc.cMh = cx(0.0, omega * eps);
+    fc.k = (float)k;
+    volatile float kf = fc.k;  // float arithmetic as written, no contraction
+    fc.k_sq_inv = 1.f / (kf * kf);
+    volatile float lambda = (float)((double)(2.0f * (float)M_PI) / k);
+    fc.threshold = 0.1f * lambda;
+
+    DeviceBuffer buf;
+    const size_t b_obs = sizeof(d3) * (size_t)nobs, b_cur = sizeof(cplx) * (size_t)ne;
+    const size_t b_out = sizeof(cplx) * 3 * (size_t)nobs;
+    SIEB_RETURN_IF(buf.reserve(b_obs + 2 * b_cur + 2 * b_out));
+    char* b = buf.as<char>();
+    d3* dobs = reinterpret_cast<d3*>(b);
+    cplx* dJ = reinterpret_cast<cplx*>(b + b_obs);
+    cplx* dM = m_cur ? dJ + ne : nullptr;
+    cplx* dE = reinterpret_cast<cplx*>(b + b_obs + 2 * b_cur);
+    cplx* dH = dE + 3 * (size_t)nobs;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dobs, points, b_obs, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(dJ, j_cur, b_cur, cudaMemcpyHostToDevice, st));
+    if (m_cur) SIEB_TRY_CUDA(cudaMemcpyAsync(dM, m_cur, b_cur, cudaMemcpyHostToDevice, st));
+    surface_fields_kernel<<<(unsigned)nobs, 256, 0, st>>>(geom, qp, dw, Q, nf, dobs, dJ, dM, fc, dE, dH);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    SIEB_TRY_CUDA(cudaMemcpyAsync(E_out, dE, b_out, cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(H_out, dH, b_out, cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    return SIEB200_OK;
+}
+
 }  // namespace sieb200

@@ -166,6 +166,9 @@ int matvec_free_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200
                        const double* host_tensors, const cplx* dx, cplx* dy);
 // s[f*32 + k] = lambda^H (dZ / d record[f][k]) x for the GSTC system (device
 // vectors of length 4 ne, s: num_faces x 32).
+int surface_fields_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j_cur, const double* m_cur,
+                          int64_t nobs, const double* points, double frequency_hz, double eps_r, double mu_r,
+                          double eps0, double mu0, int rule, double* E_out, double* H_out);
 int tensor_gradient_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,
                            const cplx* d_lam, const cplx* d_x, cplx* d_s);
 int assemble_rhs_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,

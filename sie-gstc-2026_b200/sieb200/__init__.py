@@ -10,7 +10,8 @@ from ._lib import (GSTC, PEC_EFIE, PMCHWT, SOLVER_LU_CUSOLVER, SOLVER_LU_FP64, S
                    InvalidArgument, SiebError, exported_symbols, lib, library_path)
 from .adjoint import (FarFieldConeObjective, cone_directions, far_field_matrix, gstc_solve, omega_records,
                       physical_exterior, tensor_gradient)
-from .farfield import MetasurfaceFarFieldEvaluator, bistatic_rcs, far_field, spherical_frames
+from .farfield import (MetasurfaceFarFieldEvaluator, bistatic_rcs, evaluate_surface_integral_fields, far_field,
+                       spherical_frames)
 from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, load_obj, make_mesh, \
     revolved_spindle, save_obj
 from .solvers import (EXTERIOR, INTERIOR, Context, DenseLuSolver, DielectricOptions,

@@ -111,6 +111,8 @@ _SIGNATURES = {
     "sieb200_matvec_noalloc": ([_P, _I64, _P, _I64, ctypes.c_int, _P, ctypes.c_double, _P], ctypes.c_int),
     "sieb200_gstc_tensor_gradient": ([_P, _P, _P, _P, _P, ctypes.c_int, _P], ctypes.c_int),
     "sieb200_matvec_matrix_free": ([_P, _P, _P, _P, _P, _P, ctypes.c_int], ctypes.c_int),
+    "sieb200_surface_fields": ([_P, _P, _P, _P, _I64, _P, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double, ctypes.c_double, ctypes.c_int, _P, _P], ctypes.c_int),
     "sieb200_far_field_matrix": ([_P, _P, ctypes.c_double, ctypes.c_double, _I64, _P, _P, _P, ctypes.c_int, _P],
                                  ctypes.c_int),
     "sieb200_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),

@@ -53,6 +53,37 @@ def far_field(mesh: MeshData, j_exterior: np.ndarray, m_exterior: np.ndarray | N
     return ft, fp, U
 
 
+def evaluate_surface_integral_fields(mesh: MeshData, electric_currents, magnetic_currents, observation_points,
+                                     frequency_hz: float, medium=None, quadrature_rule: int = 17,
+                                     vacuum_permittivity: float = VACUUM_PERMITTIVITY,
+                                     vacuum_permeability: float = VACUUM_PERMEABILITY,
+                                     ctx: Context | None = None):
+    """The positive surface-integral terms Q_E = +j w mu L[J] + K[M] and
+    Q_H = -K[J] + j w eps L[M] at observation points, as
+    evaluate_surface_integral_fields (surface_current_fields.hpp:12-44) returns
+    them: (E, H), each (npoints, 3) complex128. electric/magnetic_currents:
+    one physical RWG coefficient per edge (M, not M / eta0; None = 0);
+    medium: an IsotropicMedium (relative constants, default vacuum). Not the
+    scattered or total fields by themselves: F_total = F_incident - Q in the
+    region the currents radiate into."""
+    import ctypes
+    ctx = ctx or default_context()
+    eps_r = 1.0 if medium is None else float(medium.relative_permittivity)
+    mu_r = 1.0 if medium is None else float(medium.relative_permeability)
+    j = np.ascontiguousarray(electric_currents, dtype=np.complex128).ravel()
+    m = None if magnetic_currents is None else np.ascontiguousarray(magnetic_currents, dtype=np.complex128).ravel()
+    if j.size != mesh.num_edges or (m is not None and m.size != mesh.num_edges):
+        raise ValueError("field evaluation requires one electric and magnetic coefficient per mesh edge")
+    pts = np.ascontiguousarray(observation_points, dtype=np.float64).reshape(-1, 3)
+    E = np.zeros((pts.shape[0], 3), dtype=np.complex128)
+    H = np.zeros((pts.shape[0], 3), dtype=np.complex128)
+    _lib.check(_lib.lib().sieb200_surface_fields(ctx.handle, ctypes.byref(mesh.as_c()), j.ctypes.data, _lib.ptr(m),
+                                                 pts.shape[0], pts.ctypes.data, float(frequency_hz), eps_r, mu_r,
+                                                 float(vacuum_permittivity), float(vacuum_permeability),
+                                                 int(quadrature_rule), E.ctypes.data, H.ctypes.data))
+    return E, H
+
+
 class MetasurfaceFarFieldEvaluator:
     """Exterior-current radiation pattern evaluator (plot_far_field.py:118-265).
 
