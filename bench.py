@@ -25,6 +25,7 @@ cores, rank 0 only.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -56,6 +57,11 @@ GEMM_DRAM_BYTES_PER_LAUNCH = 163.7e6
 # 8 TL + 10 TK complex moments (72); one sqrt, one reciprocal and one sincos
 # per evaluation are not counted.
 ASSEMBLY_FLOPS_PER_EVAL = 95
+# Rotated-testing (nTL / nTK) pair kernel: per wavenumber 15 flops of kernel
+# values and products with the weight, 30 for the 8 G-weighted and 44 for the
+# 11 g-weighted complex moments; 51 flops of point-pair geometry shared by the
+# two wavenumbers (FMA = 2; sqrt, reciprocal, sincos not counted).
+N_ASSEMBLY_FLOPS_PER_EVAL = 115
 # FP64 flops per field evaluation (one observation point, one face, one
 # quadrature point) of the surface-field kernel, counted from its source with
 # an FMA as 2: G and grad G (26), then for each of the three half-RWG
@@ -178,7 +184,7 @@ def run_reference(args):
     kh = np.array([0, 0, 1.0])
     ref.ref_rhs_plane_wave(1, V.ctypes.data, mesh.faces.ctypes.data, mesh.faces_edges.ctypes.data,
                            mesh.num_faces, mesh.num_edges, 17, E0.ctypes.data, kh.ctypes.data, k, eta, 2,
-                           s["mu0"], s["eps0"], b.ctypes.data)
+                           s["mu0"], s["eps0"], b.ctypes.data, 0, 1.0, 1.0)
     times = []
     for i in range(args.warmup + args.steps):
         secs, x, kind, desc = cpu_reference_solve(Z, b, threads)
@@ -242,6 +248,27 @@ def run(args):
     Q = 61 if args.rule == 17 else sieb200.lib().sieb200_quadrature_rule(args.rule, None, None)
     evals = 2.0 * mesh.num_faces ** 2 * Q * Q  # Green evaluations (two wavenumbers)
     fp64_peak = ctx.fp64_fma_peak()
+    # The same system with rotated (n x RWG) testing, N-PMCHWT surface form:
+    # nTL / nTK face-pair quadrature in place of TL / TK, same placement.
+    opts_n = dataclasses.replace(opts, formulation="N_PMCHWT")
+    sieb200.assemble_matrix_device(mesh, opts_n, Z.data_ptr(), ctx=ctx)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    sieb200.assemble_matrix_device(mesh, opts_n, Z.data_ptr(), ctx=ctx)
+    ctx.synchronize()
+    t_asm_n = time.perf_counter() - t0
+    variants = {
+        "n_pmchwt": {
+            "workload": "N-PMCHWT (n x RWG testing, surface nTL form) of the same sphere, rule 17",
+            "assembly_seconds": t_asm_n, "t_pmchwt_assembly_seconds": t_asm,
+            "green_evals_per_s": evals / t_asm_n,
+            "roofline": {"bound": "fp64 pipe", "unit": "TFLOP/s", "flops_per_eval": N_ASSEMBLY_FLOPS_PER_EVAL,
+                         "achieved": evals * N_ASSEMBLY_FLOPS_PER_EVAL / t_asm_n / 1e12, "peak": fp64_peak,
+                         "frac": evals * N_ASSEMBLY_FLOPS_PER_EVAL / t_asm_n / 1e12 / fp64_peak},
+        }
+    }
+    sieb200.assemble_matrix_device(mesh, opts, Z.data_ptr(), ctx=ctx)
+    ctx.synchronize()
     b = torch.from_numpy(sieb200.assemble_rhs(mesh, opts, [sieb200.PlaneWaveExcitation()], ctx=ctx)[:, 0].copy()).cuda()
     x = torch.empty_like(b)
 
@@ -444,6 +471,7 @@ def run(args):
             },
             "fields": fields,
             "adjoint": adjoint,
+            "variants": variants,
         }
         print(json.dumps(out), flush=True)
     torch.cuda.synchronize()

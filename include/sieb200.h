@@ -34,7 +34,8 @@ enum {
     SIEB200_CUDA_ERROR = 6,
     SIEB200_TIMEOUT = 7,
     SIEB200_NO_DEVICE = 8,
-    SIEB200_OUT_OF_MEMORY = 9
+    SIEB200_OUT_OF_MEMORY = 9,
+    SIEB200_UNSUPPORTED = 10     /* a reference option this library does not build */
 };
 
 /* Thread-local message of the last failing call on this host thread. */
@@ -113,7 +114,23 @@ typedef struct {
     double tolerance;        /* refinement / GMRES target on the scaled system */
     int max_iterations;
     int restart;
+    /* Testing variant within the formulation: PecFormulation
+     * (include/sie_mom/solvers/pec_solver.hpp:12) or DielectricFormulation
+     * (include/sie_mom/solvers/dielectric/dielectric_solver.hpp:15-19);
+     * SIEB200_VARIANT_* below, 0 for GSTC. */
+    int variant;
+    /* nTL integral form of the rotated variants (NtlIntegralForm,
+     * dielectric_solver.hpp:22-25; PecNtlForm, pec_solver.hpp:13):
+     * SIEB200_NTL_SURFACE (form B, the reference default) is built;
+     * SIEB200_NTL_LINE (form A) is answered with SIEB200_UNSUPPORTED. */
+    int ntl_form;
 } sieb200_options;
+enum {
+    SIEB200_VARIANT_T = 0,       /* T-EFIE / T-PMCHWT: RWG testing */
+    SIEB200_VARIANT_N = 1,       /* N-EFIE / N-PMCHWT: n x RWG testing, nTL / nTK */
+    SIEB200_VARIANT_N_JUMP = 2   /* N-MFIE (1/2 Gram - nTK) / N-Muller (nTL, nTK, Gram) */
+};
+enum { SIEB200_NTL_SURFACE = 0, SIEB200_NTL_LINE = 1 };
 int sieb200_options_default(int formulation, sieb200_options* out);
 
 /* Excitation (include/sie_mom/excitation/excitation.hpp:19-30): kind 0 is a

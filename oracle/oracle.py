@@ -21,7 +21,7 @@ _f = ctypes.c_float
 _d = ctypes.c_double
 _i = ctypes.c_int
 
-_ASSEMBLE = [_i, _P, _P, _P, _i, _i, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, _P, _i, _i, _P, _i]
+_ASSEMBLE = [_i, _P, _P, _P, _i, _i, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, _P, _i, _i, _P, _i, _i]
 
 
 def _build_oracle() -> None:
@@ -42,8 +42,9 @@ def oracle() -> ctypes.CDLL:
     lib.so_build_edges.argtypes = [_P, _i, _P, _P]
     lib.so_wilton.argtypes = [_P, _P, _P]
     lib.so_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.so_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
     lib.so_assemble.argtypes = _ASSEMBLE
-    lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P]
+    lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
     lib.so_surface_fields.argtypes = _FIELDS
     return lib
@@ -60,8 +61,9 @@ def reference() -> ctypes.CDLL | None:
     lib.ref_phi0.argtypes = [_P, _P]
     lib.ref_phi0.restype = _d
     lib.ref_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.ref_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
     lib.ref_assemble.argtypes = _ASSEMBLE
-    lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P]
+    lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.ref_surface_fields.argtypes = _FIELDS
     lib.ref_lu_solve.argtypes = [_i, _P, _P, _P, _i, _i]
     lib.ref_lu_solve.restype = _d
@@ -101,7 +103,10 @@ def kernel_scalars(kind: int, frequency_hz: float, eps_r=(1.0, 1.0), mu_r=(1.0, 
 
 
 def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, uniform=False,
-             basis=0, threads=0, fn="so_assemble") -> np.ndarray:
+             basis=0, threads=0, fn="so_assemble", variant: int = 0) -> np.ndarray:
+    """variant 1: rotated (n x RWG) testing, N-EFIE (kind 0) or N-PMCHWT
+    (kind 1), surface nTL form; variant 2: N-MFIE (kind 0) or N-Muller
+    (kind 1)."""
     V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
     F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
     FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
@@ -112,13 +117,15 @@ def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, unifo
     s = scalars
     getattr(lib, fn)(kind, _p(V), _p(F), _p(FE), F.shape[0], ne, rule, s["k1"], s["k2"], s["mu_r1"],
                      s["mu_r2"], s["eps_r1"], s["eps_r2"], s["mu0"], s["eps0"], s["omega"], s["thr"],
-                     _p(t), int(uniform), int(basis), _p(Z), int(threads))
+                     _p(t), int(uniform), int(basis), _p(Z), int(threads), int(variant))
     return Z
 
 
 def rhs(lib, kind: int, mesh, rule: int, source: dict, k: float, eta: float, mu0: float,
-        eps0: float) -> np.ndarray:
-    """source: {'kind': 0|1, 'a': (3,), 'b': (3,), 'is_magnetic': bool, 'region': 1|2}."""
+        eps0: float, variant: int = 0, eps_r_src: float = 1.0, mu_r_src: float = 1.0) -> np.ndarray:
+    """source: {'kind': 0|1, 'a': (3,), 'b': (3,), 'is_magnetic': bool, 'region': 1|2};
+    variant as for assemble(); eps_r_src, mu_r_src: the source region's medium
+    (used by N-Muller)."""
     V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
     F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
     FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
@@ -127,7 +134,8 @@ def rhs(lib, kind: int, mesh, rule: int, source: dict, k: float, eta: float, mu0
     a = np.ascontiguousarray(source["a"], dtype=np.float64)
     bb = np.ascontiguousarray(source["b"], dtype=np.float64)
     lib.so_rhs(kind, source["kind"], _p(V), _p(F), _p(FE), F.shape[0], ne, rule, _p(a), _p(bb),
-               int(source.get("is_magnetic", 0)), k, eta, source["region"], mu0, eps0, _p(b))
+               int(source.get("is_magnetic", 0)), k, eta, source["region"], mu0, eps0, _p(b),
+               int(variant), float(eps_r_src), float(mu_r_src))
     return b
 
 

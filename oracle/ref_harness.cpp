@@ -100,6 +100,66 @@ void pair_blocks(const double* V, const int* F, int m, int n, const Quad& q, flo
     }
 }
 
+// Per face pair: nTL/nTK (surface form B) for k1 and k2 as n_pmchwt_kernel
+// calls them (dielectric_kernels.cu:155-270), float centroid distance.
+void pair_blocks_n(const double* V, const int* F, int m, int n, const Quad& q, float k1, float k2,
+                   float thr, complex_t l1[3][3], complex_t l2[3][3], complex_t n1[3][3],
+                   complex_t n2[3][3]) {
+    const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
+    const int si[3] = {F[3 * n], F[3 * n + 1], F[3 * n + 2]};
+    vec3_t tv[3], sv[3];
+    for (int a = 0; a < 3; ++a) {
+        tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+        sv[a] = make_vec3(V[3 * si[a]], V[3 * si[a] + 1], V[3 * si[a] + 2]);
+    }
+    const vec3_t tc = (tv[0] + tv[1] + tv[2]) / 3.f;
+    const vec3_t sc = (sv[0] + sv[1] + sv[2]) / 3.f;
+    const float dist = length(tc - sc);
+    if (dist < thr) {
+        calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2, true,
+                                          l1, l2, n1, n2);
+        complex_t s1[3][3], s2[3][3], s3[3][3], s4[3][3];
+        calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2,
+                                                s1, s2, s3, s4);
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                complexAddInPlace(l1[j][i], s1[j][i]);
+                complexAddInPlace(l2[j][i], s2[j][i]);
+                complexAddInPlace(n1[j][i], s3[j][i]);
+                complexAddInPlace(n2[j][i], s4[j][i]);
+            }
+    } else {
+        calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2, false,
+                                          l1, l2, n1, n2);
+    }
+}
+
+// N-EFIE pair (pec_solver.cu:113-168): nTL2 at k2, extraction decided on the
+// double centroid distance, only the singular nTL2 added.
+void pair_n_efie(const double* V, const int* F, int m, int n, const Quad& q, float k2, float thr,
+                 complex_t l2[3][3]) {
+    const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
+    const int si[3] = {F[3 * n], F[3 * n + 1], F[3 * n + 2]};
+    vec3_t tv[3], sv[3];
+    for (int a = 0; a < 3; ++a) {
+        tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+        sv[a] = make_vec3(V[3 * si[a]], V[3 * si[a] + 1], V[3 * si[a] + 2]);
+    }
+    const vec3_t cm = (tv[0] + tv[1] + tv[2]) / real_t(3);
+    const vec3_t cn = (sv[0] + sv[1] + sv[2]) / real_t(3);
+    const bool extract = length(cm - cn) < thr;
+    complex_t l1[3][3], n1[3][3], n2[3][3];
+    calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2, extract,
+                                      l1, l2, n1, n2);
+    if (extract) {
+        complex_t s1[3][3], s2[3][3], s3[3][3], s4[3][3];
+        calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2,
+                                                s1, s2, s3, s4);
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) complexAddInPlace(l2[j][i], s2[j][i]);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -186,6 +246,21 @@ double ref_phi0(const double* r, const double* tri) {
 
 // Local 3x3 blocks of one face pair: out = [tl1, tl2, tk1, tk2] each 3x3
 // complex row-major (j test, i source), interleaved re/im (72 doubles).
+// nTL1, nTL2, nTK1, nTK2 of face pair (m, n), surface form B.
+void ref_pair_blocks_n(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
+                       float thr, double* out) {
+    const Quad q = make_rule(rule);
+    complex_t a[3][3], b[3][3], c[3][3], d[3][3];
+    pair_blocks_n(V, F, m, n, q, k1, k2, thr, a, b, c, d);
+    complex_t(*blk[4])[3] = {a, b, c, d};
+    for (int k = 0; k < 4; ++k)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                out[2 * (k * 9 + j * 3 + i)] = blk[k][j][i].x;
+                out[2 * (k * 9 + j * 3 + i) + 1] = blk[k][j][i].y;
+            }
+}
+
 void ref_pair_blocks(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
                      float thr, double* out) {
     const Quad q = make_rule(rule);
@@ -202,12 +277,15 @@ void ref_pair_blocks(const double* V, const int* F, int m, int n, int rule, floa
 
 // Dense system matrix as the reference kernels assemble it.
 // kind 0: PEC T-EFIE (N = ne), 1: T-PMCHWT (N = 2 ne), 2: GSTC (N = 4 ne,
-// Calderon + mass, eta0-scaled). Z is complex interleaved, column-major,
+// Calderon + mass, eta0-scaled); variant 1: N-EFIE / N-PMCHWT surface form
+// (pec_solver.cu:113-168, dielectric_kernels.cu:155-318); variant 2: N-MFIE /
+// N-Muller (pec_solver.cu:171-240, dielectric_kernels.cu:323-489). Z is complex
+// interleaved, column-major,
 // and is overwritten. Physical scalars are the float-demoted kernel arguments.
 int ref_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
                  float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                  float mu0, float eps0, float omega, float thr, const double* tensors,
-                 int tensors_uniform, int basis, double* Z, int threads) {
+                 int tensors_uniform, int basis, double* Z, int threads, int variant) {
     const Quad q = make_rule(rule);
     const size_t N = (kind == 0) ? ne : (kind == 1 ? 2 * (size_t)ne : 4 * (size_t)ne);
     std::memset(Z, 0, sizeof(double) * 2 * N * N);
@@ -217,9 +295,92 @@ int ref_assemble(int kind, const double* V, const int* F, const int* FE, int nf,
     for (int m = 0; m < nf; ++m) {
         for (int n = 0; n < nf; ++n) {
             complex_t tl1[3][3], tl2[3][3], tk1[3][3], tk2[3][3];
-            pair_blocks(V, F, m, n, q, k1, k2, thr, tl1, tl2, tk1, tk2);
             const int te[3] = {FE[3 * m], FE[3 * m + 1], FE[3 * m + 2]};
             const int se[3] = {FE[3 * n], FE[3 * n + 1], FE[3 * n + 2]};
+            if (kind == 0 && variant == 2) {
+                // N-MFIE (pec_solver.cu:171-240).
+                const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
+                const int si[3] = {F[3 * n], F[3 * n + 1], F[3 * n + 2]};
+                vec3_t tv[3], sv[3];
+                for (int a = 0; a < 3; ++a) {
+                    tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+                    sv[a] = make_vec3(V[3 * si[a]], V[3 * si[a] + 1], V[3 * si[a] + 2]);
+                }
+                if (m == n) {
+                    complex_t mass[3][3];
+                    calculateMassMatrixQuadrature(tv, ti, q.pts.data(), q.w.data(), q.n, mass);
+                    for (int j = 0; j < 3; ++j)
+                        for (int i = 0; i < 3; ++i)
+                            atomic_add(Z, cm_index(te[j], se[i], N), complexScale(mass[j][i], real_t(0.5)));
+                    continue;
+                }
+                const vec3_t cm = (tv[0] + tv[1] + tv[2]) / real_t(3);
+                const vec3_t cn = (sv[0] + sv[1] + sv[2]) / real_t(3);
+                const bool extract = length(cm - cn) < thr;
+                complex_t l1[3][3], l2[3][3], n1[3][3], n2[3][3];
+                calculateFormAQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, nullptr,
+                                                 nullptr, 0, k2, k2, extract, l1, l2, n1, n2);
+                if (extract) {
+                    complex_t s1[3][3], s2[3][3], s3[3][3], s4[3][3];
+                    calculateFormASingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(),
+                                                                 q.n, nullptr, nullptr, 0, k2, k2, s1, s2,
+                                                                 s3, s4);
+                    for (int j = 0; j < 3; ++j)
+                        for (int i = 0; i < 3; ++i) complexAddInPlace(n2[j][i], s4[j][i]);
+                }
+                for (int j = 0; j < 3; ++j)
+                    for (int i = 0; i < 3; ++i)
+                        atomic_add(Z, cm_index(te[j], se[i], N), complexScale(n2[j][i], real_t(-1)));
+                continue;
+            }
+            if (kind == 0 && variant == 1) {
+                pair_n_efie(V, F, m, n, q, k2, thr, tl2);
+                const float mu2 = (float)((double)mu_r2 * (double)mu0);
+                const complex_t factor = make_complex(real_t(0), omega * mu2);
+                for (int j = 0; j < 3; ++j)
+                    for (int i = 0; i < 3; ++i)
+                        atomic_add(Z, cm_index(te[j], se[i], N), factor * tl2[j][i]);
+                continue;
+            }
+            if (variant != 0)
+                pair_blocks_n(V, F, m, n, q, k1, k2, thr, tl1, tl2, tk1, tk2);
+            else
+                pair_blocks(V, F, m, n, q, k1, k2, thr, tl1, tl2, tk1, tk2);
+            if (kind == 1 && variant == 2) {
+                // N-Muller (dielectric_kernels.cu:433-488).
+                complex_t mass[3][3];
+                if (m == n) {
+                    const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
+                    vec3_t tv[3];
+                    for (int a = 0; a < 3; ++a)
+                        tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+                    calculateMassMatrixQuadrature(tv, ti, q.pts.data(), q.w.data(), q.n, mass);
+                }
+                const complex_t j_omega = make_complex(0.f, omega);
+                const float mu1 = mu_r1 * mu0, mu2 = mu_r2 * mu0;
+                const float eps1 = eps_r1 * eps0, eps2 = eps_r2 * eps0;
+                const float eta0 = sqrtf(mu0 / eps0);
+                const complex_t c_eps1 = j_omega * eps1, c_eps2 = j_omega * eps2;
+                for (int j = 0; j < 3; ++j)
+                    for (int i = 0; i < 3; ++i) {
+                        const complex_t z_jj = (c_eps2 * mu2) * tl2[j][i] - (c_eps1 * mu1) * tl1[j][i];
+                        const complex_t z_mm = complexScale(-1.0f, z_jj);
+                        complex_t z_jm = eps2 * tk2[j][i] - eps1 * tk1[j][i];
+                        complex_t z_mj = mu2 * tk2[j][i] - mu1 * tk1[j][i];
+                        if (m == n) {
+                            const complex_t g = mass[j][i];
+                            const float eps_factor = (eps1 + eps2) / 2.0f;
+                            const float mu_factor = (mu1 + mu2) / 2.0f;
+                            z_jm = z_jm - complexScale(eps_factor, g);
+                            z_mj = z_mj - complexScale(mu_factor, g);
+                        }
+                        atomic_add(Z, cm_index(te[j], se[i], N), z_jj);
+                        atomic_add(Z, cm_index(te[j], se[i] + ne, N), complexScale(z_jm, eta0));
+                        atomic_add(Z, cm_index(te[j] + ne, se[i], N), complexScale(z_mj, eta0));
+                        atomic_add(Z, cm_index(te[j] + ne, se[i] + ne, N), complexScale(z_mm, eta0 * eta0));
+                    }
+                continue;
+            }
             if (kind == 0) {
                 const complex_t c_efie = make_complex(0.f, omega * mu_r2 * mu0);
                 for (int j = 0; j < 3; ++j)
@@ -339,9 +500,14 @@ int ref_assemble(int kind, const double* V, const int* F, const int* FE, int nf,
 // H rows x sign*eta0); 2: GSTC (N = 4 ne, region 1 -> [J1,M1] rows,
 // region 2 -> [J2,M2] rows, H rows x eta0 from float mu0/eps0).
 // k, eta: the source medium's wavenumber and impedance (double, unrounded).
+// variant != 0: n x RWG testing (pec_solver.cu:372-386, dielectric_solver.cu:461-510);
+// variant 2: N-MFIE places V_H, N-Muller scales by the source region's
+// eps_r_src, mu_r_src.
 int ref_rhs_plane_wave(int kind, const double* V, const int* F, const int* FE, int nf, int ne,
                        int rule, const double* E0, const double* khat, double k, double eta,
-                       int region, double mu0_d, double eps0_d, double* b) {
+                       int region, double mu0_d, double eps0_d, double* b, int variant,
+                       double eps_r_src, double mu_r_src) {
+    const bool rotated = variant != 0;
     const Quad q = make_rule(rule);
     const size_t N = (kind == 0) ? ne : (kind == 1 ? 2 * (size_t)ne : 4 * (size_t)ne);
     std::memset(b, 0, sizeof(double) * 2 * N);
@@ -356,12 +522,24 @@ int ref_rhs_plane_wave(int kind, const double* V, const int* F, const int* FE, i
         for (int a = 0; a < 3; ++a)
             tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
         complex_t ve[3], vh[3];
-        calculateExcitationQuadrature<TestingFunction::RWG>(tv, ti, q.pts.data(), q.w.data(), q.n,
-                                                            pw, ve, vh);
+        if (rotated)
+            calculateExcitationQuadrature<TestingFunction::NxRWG>(tv, ti, q.pts.data(), q.w.data(),
+                                                                  q.n, pw, ve, vh);
+        else
+            calculateExcitationQuadrature<TestingFunction::RWG>(tv, ti, q.pts.data(), q.w.data(),
+                                                                q.n, pw, ve, vh);
         for (int i = 0; i < 3; ++i) {
             const size_t e = FE[3 * m + i];
-            if (kind == 0) {
+            if (kind == 0 && variant == 2) {
+                atomic_add(b, e, vh[i]);
+            } else if (kind == 0) {
                 atomic_add(b, e, ve[i]);
+            } else if (kind == 1 && variant == 2) {
+                const real_t eta0 = std::sqrt(mu0_d / eps0_d);
+                const real_t scale_e = static_cast<real_t>(eps_r_src * eps0_d);
+                const real_t scale_h = -static_cast<real_t>(mu_r_src * mu0_d) * eta0;
+                atomic_add(b, e, complexScale(ve[i], scale_e));
+                atomic_add(b, e + ne, complexScale(vh[i], scale_h));
             } else if (kind == 1) {
                 const real_t eta0 = std::sqrt(mu0_d / eps0_d);
                 const real_t sign = region == 2 ? real_t(1) : real_t(-1);

@@ -362,15 +362,147 @@ static void pair(const tri_t* T, const tri_t* S, const float* pts, const float* 
     }
 }
 
-void so_pair_blocks(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
-                    float thr, double* out) {
+/* ------------------------------------------- rotated (n x RWG) testing -- */
+static inline v3 face_normal(const tri_t* t) {
+    return vnorm(vcross(vsub(t->v[1], t->v[0]), vsub(t->v[2], t->v[0])));
+}
+
+static inline cx vdot_c(v3 a, const cx c[3]) {
+    return CX(a.x * c[0].re + a.y * c[1].re + a.z * c[2].re, a.x * c[0].im + a.y * c[1].im + a.z * c[2].im);
+}
+
+/* dunavant_quadrature.cuh:342-480 (surface form B): tau_mj = rho_mj x n_m,
+ * nTL = 1/4 (tau . rho_ni) G - 1/(2 k^2) tau . tk, nTK = 1/4 (tau x rho_ni) . tk
+ * with tk the TK kernel vector; nTK is left out on the coincident face, the
+ * gradient term of nTL is not. Blocks: tl1/tl2 = nTL, tk1/tk2 = nTK. */
+static void double_quad_n(const tri_t* T, const tri_t* S, const float* pts, const float* wts, int Q,
+                          double k1, double k2, int regular, blocks_t* B) {
+    memset(B, 0, sizeof(*B));
+    const double k[2] = {k1, k2};
+    const int coinc = same_face(T, S);
+    const v3 nm = face_normal(T);
+    for (int p = 0; p < Q; ++p) {
+        v3 rp = map_point(T, (double)pts[2 * p], (double)pts[2 * p + 1]);
+        double wp = (double)wts[p];
+        for (int q = 0; q < Q; ++q) {
+            v3 rq = map_point(S, (double)pts[2 * q], (double)pts[2 * q + 1]);
+            double wq = (double)wts[q];
+            kern_t K;
+            kernels(rp, rq, k, regular, &K);
+            double cw = wp * wq;
+            for (int j = 0; j < 3; ++j) {
+                v3 tau = vcross(vsub(rp, T->free_v[j]), nm);
+                for (int i = 0; i < 3; ++i) {
+                    v3 rn = vsub(rq, S->free_v[i]);
+                    double dtr = vdot(tau, rn);
+                    v3 km = vscale(vcross(tau, rn), 0.25);
+                    for (int a = 0; a < 2; ++a) {
+                        cx ntl = cscale(K.tl[a], 0.25 * dtr);
+                        ntl = cadd(ntl, cscale(vdot_c(tau, K.tk[a]), -0.5 / (k[a] * k[a])));
+                        cx* dl = a == 0 ? &B->tl1[j][i] : &B->tl2[j][i];
+                        *dl = cadd(*dl, cscale(ntl, cw));
+                        if (!coinc) {
+                            cx* dk = a == 0 ? &B->tk1[j][i] : &B->tk2[j][i];
+                            *dk = cadd(*dk, cscale(vdot_c(km, K.tk[a]), cw));
+                        }
+                    }
+                }
+            }
+        }
+    }
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            double s = T->len[j] * S->len[i];
+            B->tl1[j][i] = cscale(B->tl1[j][i], s);
+            B->tl2[j][i] = cscale(B->tl2[j][i], s);
+            B->tk1[j][i] = cscale(B->tk1[j][i], s);
+            B->tk2[j][i] = cscale(B->tk2[j][i], s);
+        }
+}
+
+/* dunavant_quadrature.cuh:889-1040 (singular part of form B): with
+ * phi_1 = phi_1b - d phi_0 n_n and the extracted gradient phi_3b - d phi_2 n_n,
+ * nTL += 1/2 tau . (phi_1 + 1/2 R_i phi_0 + grad / k^2) (the gradient left out
+ * on the coincident face), nTK += 1/4 tau . Upsilon_coul (not on the
+ * coincident face); e_mj e_ni / (4 pi A_n) afterwards. */
+static void singular_quad_n(const tri_t* T, const tri_t* S, const float* pts, const float* wts,
+                            int Q, double k1, double k2, blocks_t* B) {
+    memset(B, 0, sizeof(*B));
+    const int coinc = same_face(T, S);
+    const v3 nm = face_normal(T), nn = face_normal(S);
+    for (int p = 0; p < Q; ++p) {
+        v3 rp = map_point(T, (double)pts[2 * p], (double)pts[2 * p + 1]);
+        double wp = (double)wts[p];
+        pots_t P = wilton(rp, S->v);
+        v3 phi1 = vsub(P.phi1b, vscale(nn, P.d * P.phi0));
+        v3 grad = vsub(P.phi3b, vscale(nn, P.d * P.phi2));
+        for (int j = 0; j < 3; ++j) {
+            v3 tau = vcross(vsub(rp, T->free_v[j]), nm);
+            for (int i = 0; i < 3; ++i) {
+                v3 Ri = vsub(rp, S->free_v[i]);
+                v3 br = vadd(phi1, vscale(vscale(Ri, 0.5), P.phi0));
+                v3 b1 = coinc ? br : vadd(br, vscale(grad, 1.0 / (k1 * k1)));
+                v3 b2 = coinc ? br : vadd(br, vscale(grad, 1.0 / (k2 * k2)));
+                B->tl1[j][i].re += 0.5 * vdot(tau, b1) * wp;
+                B->tl2[j][i].re += 0.5 * vdot(tau, b2) * wp;
+                if (!coinc) {
+                    v3 u1 = upsilon(&P, S->free_v[i], rp, (float)k1);
+                    v3 u2 = upsilon(&P, S->free_v[i], rp, (float)k2);
+                    B->tk1[j][i].re += 0.25 * vdot(tau, u1) * wp;
+                    B->tk2[j][i].re += 0.25 * vdot(tau, u2) * wp;
+                }
+            }
+        }
+    }
+    v3 c = vcross(vsub(S->v[1], S->v[0]), vsub(S->v[2], S->v[0]));
+    double as = 1.0 / (4.0 * M_PI * (0.5 * vlen(c)));
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            double s = as * T->len[j] * S->len[i];
+            B->tl1[j][i] = cscale(B->tl1[j][i], s);
+            B->tl2[j][i] = cscale(B->tl2[j][i], s);
+            B->tk1[j][i] = cscale(B->tk1[j][i], s);
+            B->tk2[j][i] = cscale(B->tk2[j][i], s);
+        }
+}
+
+/* dielectric_kernels.cu:155-270 and pec_solver.cu:113-168: the same centroid
+ * test as pair(), form B quadratures. */
+static void pair_n(const tri_t* T, const tri_t* S, const float* pts, const float* wts, int Q,
+                   float k1, float k2, float thr, blocks_t* B) {
+    v3 tc = vadd(vadd(T->v[0], T->v[1]), T->v[2]);
+    v3 sc = vadd(vadd(S->v[0], S->v[1]), S->v[2]);
+    tc = V3(tc.x / 3.0, tc.y / 3.0, tc.z / 3.0);
+    sc = V3(sc.x / 3.0, sc.y / 3.0, sc.z / 3.0);
+    float dist = (float)vlen(vsub(tc, sc));
+    if (dist < thr) {
+        blocks_t Sg;
+        double_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, 1, B);
+        singular_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, &Sg);
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                B->tl1[j][i] = cadd(B->tl1[j][i], Sg.tl1[j][i]);
+                B->tl2[j][i] = cadd(B->tl2[j][i], Sg.tl2[j][i]);
+                B->tk1[j][i] = cadd(B->tk1[j][i], Sg.tk1[j][i]);
+                B->tk2[j][i] = cadd(B->tk2[j][i], Sg.tk2[j][i]);
+            }
+    } else {
+        double_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, 0, B);
+    }
+}
+
+static void pair_blocks_out(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
+                            float thr, int rotated, double* out) {
     float pts[2 * 80], wts[80];
     int Q = so_rule(rule, pts, wts);
     tri_t T, S;
     load_tri(V, F, m, &T);
     load_tri(V, F, n, &S);
     blocks_t B;
-    pair(&T, &S, pts, wts, Q, k1, k2, thr, &B);
+    if (rotated)
+        pair_n(&T, &S, pts, wts, Q, k1, k2, thr, &B);
+    else
+        pair(&T, &S, pts, wts, Q, k1, k2, thr, &B);
     cx(*blk[4])[3] = {B.tl1, B.tl2, B.tk1, B.tk2};
     for (int b = 0; b < 4; ++b)
         for (int j = 0; j < 3; ++j)
@@ -378,6 +510,17 @@ void so_pair_blocks(const double* V, const int* F, int m, int n, int rule, float
                 out[2 * (b * 9 + j * 3 + i)] = blk[b][j][i].re;
                 out[2 * (b * 9 + j * 3 + i) + 1] = blk[b][j][i].im;
             }
+}
+
+void so_pair_blocks(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
+                    float thr, double* out) {
+    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 0, out);
+}
+
+/* nTL1, nTL2, nTK1, nTK2 of face pair (m, n), surface form B. */
+void so_pair_blocks_n(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
+                      float thr, double* out) {
+    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 1, out);
 }
 
 /* ------------------------------------------------------- GSTC frames ---- */
@@ -471,6 +614,31 @@ static void mass8(const tri_t* T, const float* pts, const float* wts, int Q, cx 
             }
 }
 
+/* dunavant_quadrature.cuh:1261-1326: RWG Gram block <f_j, f_i> of one face;
+ * the dot product is rounded to float and multiplied by the float weight in
+ * float, the scale 1/(4A) e_j e_i is formed in float. */
+static void gram(const tri_t* T, const float* pts, const float* wts, int Q, double G[3][3]) {
+    memset(G, 0, sizeof(double) * 9);
+    v3 c = vcross(vsub(T->v[1], T->v[0]), vsub(T->v[2], T->v[0]));
+    const float area = (float)(0.5 * vlen(c));
+    float el[3];
+    for (int i = 0; i < 3; ++i) el[i] = (float)T->len[i];
+    for (int p = 0; p < Q; ++p) {
+        const float wp = wts[p];
+        v3 rp = map_point(T, (double)pts[2 * p], (double)pts[2 * p + 1]);
+        v3 rho[3];
+        for (int i = 0; i < 3; ++i) rho[i] = vsub(rp, T->free_v[i]);
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const float d = (float)vdot(rho[j], rho[i]);
+                G[j][i] += (double)(wp * d);
+            }
+    }
+    const float sc = 1.f / (4.f * area);
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) G[j][i] *= (double)(sc * el[j] * el[i]);
+}
+
 /* ------------------------------------------------------------ assembly -- */
 static inline void zadd(double* Z, size_t N, size_t r, size_t c, cx v) {
     size_t idx = c * N + r;
@@ -478,15 +646,19 @@ static inline void zadd(double* Z, size_t N, size_t r, size_t c, cx v) {
     Z[2 * idx + 1] += v.im;
 }
 
-/* kind 0: PEC T-EFIE (sie_kernels_assembly.cuh:610-705),
- * kind 1: T-PMCHWT (dielectric_kernels.cu:23-149),
+/* kind 0: PEC T-EFIE (sie_kernels_assembly.cuh:610-705), with variant 1
+ *         N-EFIE surface form (pec_solver.cu:113-168), variant 2 N-MFIE
+ *         (pec_solver.cu:171-240),
+ * kind 1: T-PMCHWT (dielectric_kernels.cu:23-149), with variant 1 N-PMCHWT
+ *         surface form (dielectric_kernels.cu:155-318: nTL/nTK in the places
+ *         of TL/TK), variant 2 N-Muller surface form (dielectric_kernels.cu:323-489),
  * kind 2: GSTC Calderon + mass, eta0-scaled (sie_kernels_assembly.cuh:156-272,
  *         460-594). Z: complex interleaved, column-major, overwritten.
  * Serial over faces so that the summation order is fixed. */
 int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
                 float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                 float mu0, float eps0, float omega, float thr, const double* tensors,
-                int tensors_uniform, int basis, double* Z, int threads) {
+                int tensors_uniform, int basis, double* Z, int threads, int variant) {
     (void)threads;
     float pts[2 * 80], wts[80];
     const int Q = so_rule(rule, pts, wts);
@@ -500,13 +672,51 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
     for (int m = 0; m < nf; ++m) {
         for (int n = 0; n < nf; ++n) {
             blocks_t B;
-            pair(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
+            if (variant != 0)
+                pair_n(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
+            else
+                pair(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
             const int* te = &FE[3 * m];
             const int* se = &FE[3 * n];
+            double G[3][3];
+            if (variant == 2 && m == n) gram(&tris[m], pts, wts, Q, G);
             for (int j = 0; j < 3; ++j)
                 for (int i = 0; i < 3; ++i) {
                     const size_t r = te[j], c = se[i];
-                    if (kind == 0) {
+                    if (kind == 0 && variant == 2) {
+                        /* pec_solver.cu:171-240: 1/2 Gram on the same face,
+                         * -nTK2 on the others (its self nTK is zero). */
+                        if (m == n)
+                            zadd(Z, N, r, c, CX(G[j][i] * 0.5, 0.0));
+                        else
+                            zadd(Z, N, r, c, cscale(B.tk2[j][i], -1.0));
+                    } else if (kind == 1 && variant == 2) {
+                        /* dielectric_kernels.cu:433-488 (N-Muller). */
+                        const float m1 = mu_r1 * mu0, m2 = mu_r2 * mu0;
+                        const float e1 = eps_r1 * eps0, e2 = eps_r2 * eps0;
+                        const float eta0 = sqrtf(mu0 / eps0);
+                        const cx w1 = CX(0.0, ((double)omega * e1) * m1);
+                        const cx w2 = CX(0.0, ((double)omega * e2) * m2);
+                        cx zjj = csub(cmul(w2, B.tl2[j][i]), cmul(w1, B.tl1[j][i]));
+                        cx zmm = cscale(zjj, -1.0);
+                        cx zjm = csub(cscale(B.tk2[j][i], (double)e2), cscale(B.tk1[j][i], (double)e1));
+                        cx zmj = csub(cscale(B.tk2[j][i], (double)m2), cscale(B.tk1[j][i], (double)m1));
+                        if (m == n) {
+                            const float ef = (e1 + e2) / 2.0f, mf = (m1 + m2) / 2.0f;
+                            zjm = csub(zjm, CX((double)ef * G[j][i], 0.0));
+                            zmj = csub(zmj, CX((double)mf * G[j][i], 0.0));
+                        }
+                        const float eta0sq = eta0 * eta0;
+                        zadd(Z, N, r, c, zjj);
+                        zadd(Z, N, r, c + E, cscale(zjm, (double)eta0));
+                        zadd(Z, N, r + E, c, cscale(zmj, (double)eta0));
+                        zadd(Z, N, r + E, c + E, cscale(zmm, (double)eta0sq));
+                    } else if (kind == 0 && variant == 1) {
+                        /* pec_solver.cu:163-167: j (omega * mu2) nTL2, mu2 rounded
+                         * to float from its double product. */
+                        const float ce = omega * (float)((double)mu_r2 * (double)mu0);
+                        zadd(Z, N, r, c, cmul(CX(0.0, (double)ce), B.tl2[j][i]));
+                    } else if (kind == 0) {
                         const float ce = omega * mu_r2 * mu0;
                         zadd(Z, N, r, c, cmul(CX(0.0, (double)ce), B.tl2[j][i]));
                     } else if (kind == 1) {
@@ -650,13 +860,17 @@ static void source_fields(int kind, v3 r, const double* a, const double* b, int 
     }
 }
 
-/* dunavant_quadrature.cuh:1543-1611 (RWG testing) with the placements of
+/* dunavant_quadrature.cuh:1543-1611 (RWG testing; variant != 0: n x RWG
+ * testing, rho x n_m; variant 2: N-MFIE tests H, N-Muller scales by the
+ * source region's eps_r_src, mu_r_src) with the placements of
  * pec_solver.cu:242-264 (kind 0), dielectric_solver.cu:399-530 (kind 1) and
  * sie_kernels_utils.cuh:184-232 (kind 2). source_kind 0: plane wave (a = E0,
  * b = k_hat), 1: dipole (a = moment, b = position). */
 int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* FE, int nf, int ne,
            int rule, const double* a, const double* b, int is_magnetic, double k, double eta,
-           int region, double mu0, double eps0, double* rhs) {
+           int region, double mu0, double eps0, double* rhs, int variant, double eps_r_src,
+           double mu_r_src) {
+    const int rotated = variant != 0;
     float pts[2 * 80], wts[80];
     const int Q = so_rule(rule, pts, wts);
     if (Q < 0) return -1;
@@ -669,6 +883,7 @@ int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* 
         float el[3];
         for (int i = 0; i < 3; ++i) el[i] = (float)T.len[i];
         cx ve[3] = {{0, 0}, {0, 0}, {0, 0}}, vh[3] = {{0, 0}, {0, 0}, {0, 0}};
+        const v3 nm = face_normal(&T);
         for (int p = 0; p < Q; ++p) {
             const float wp = wts[p];
             v3 rp = map_point(&T, (double)pts[2 * p], (double)pts[2 * p + 1]);
@@ -676,6 +891,7 @@ int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* 
             source_fields(source_kind, rp, a, b, is_magnetic, k, eta, Ei, Hi);
             for (int i = 0; i < 3; ++i) {
                 v3 t = vsub(rp, T.free_v[i]);
+                if (rotated) t = vcross(t, nm);
                 cx de = CX(t.x * Ei[0].re + t.y * Ei[1].re + t.z * Ei[2].re,
                            t.x * Ei[0].im + t.y * Ei[1].im + t.z * Ei[2].im);
                 cx dh = CX(t.x * Hi[0].re + t.y * Hi[1].re + t.z * Hi[2].re,
@@ -689,8 +905,18 @@ int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* 
             ve[i] = cscale(ve[i], (double)s);
             vh[i] = cscale(vh[i], (double)s);
             const size_t e = (size_t)FE[3 * m + i];
-            if (kind == 0) {
+            if (kind == 0 && variant == 2) {
+                rhs[2 * e] += vh[i].re; rhs[2 * e + 1] += vh[i].im;
+            } else if (kind == 0) {
                 rhs[2 * e] += ve[i].re; rhs[2 * e + 1] += ve[i].im;
+            } else if (kind == 1 && variant == 2) {
+                /* dielectric_solver.cu:461-489: eps V_E, -mu eta0 V_H of the
+                 * source region. */
+                const double eta0 = sqrt(mu0 / eps0);
+                const double sE = eps_r_src * eps0, sH = -(mu_r_src * mu0) * eta0;
+                cx a1 = cscale(ve[i], sE), a2 = cscale(vh[i], sH);
+                rhs[2 * e] += a1.re; rhs[2 * e + 1] += a1.im;
+                rhs[2 * (e + E)] += a2.re; rhs[2 * (e + E) + 1] += a2.im;
             } else if (kind == 1) {
                 const double eta0 = sqrt(mu0 / eps0);
                 const double sg = region == 2 ? 1.0 : -1.0;

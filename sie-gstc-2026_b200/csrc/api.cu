@@ -169,14 +169,22 @@ int make_assembly_params(const sieb200_options& o, AssemblyParams* ap) {
     const float omf = (float)omega, mu0f = (float)o.vacuum_permeability, eps0f = (float)o.vacuum_permittivity;
     ap->formulation = o.formulation;
     ap->basis = o.basis;
+    ap->variant = o.variant;
     if (o.formulation == SIEB200_PEC_EFIE) {
         const double lambda0 = 2.0 * pi / (omega * std::sqrt(o.vacuum_permeability * o.vacuum_permittivity));
         ap->threshold = (float)(o.singularity_threshold_lambda0 * lambda0);
         ap->nk = 1;
         ap->k[0] = ap->k[1] = (double)(float)k2;
-        // c_efie = j * (omega * mu_r2 * mu0) in float (sie_kernels_assembly.cuh:690).
-        const float ce = omf * (float)o.mu_r_exterior * mu0f;
-        ap->c_jj[1] = cx(0.0, (double)ce);
+        if (o.variant == 1) {
+            // N-EFIE: j * (omega * mu2) from the float kernel arguments omega and
+            // mu2 = mu_r2 mu0 (pec_solver.cu:163, 346-349).
+            const float ce = omf * (float)m2;
+            ap->c_jj[1] = cx(0.0, (double)ce);
+        } else {
+            // c_efie = j * (omega * mu_r2 * mu0) in float (sie_kernels_assembly.cuh:690).
+            const float ce = omf * (float)o.mu_r_exterior * mu0f;
+            ap->c_jj[1] = cx(0.0, (double)ce);
+        }
         return SIEB200_OK;
     }
     ap->nk = 2;
@@ -195,6 +203,15 @@ int make_assembly_params(const sieb200_options& o, AssemblyParams* ap) {
         ap->c_mm[1] = cx(0.0, (double)omf * (double)ep2f);
         ap->s_jm = (double)eta0f;
         ap->s_mm = (double)(eta0f * eta0f);
+        // N-Muller (dielectric_kernels.cu:443-488).
+        const float epf[2] = {ep1f, ep2f}, muf[2] = {mu1f, mu2f};
+        for (int r = 0; r < 2; ++r) {
+            ap->w_em[r] = ((double)omf * (double)epf[r]) * (double)muf[r];
+            ap->eps[r] = (double)epf[r];
+            ap->mu[r] = (double)muf[r];
+        }
+        ap->eps_f = (double)((ep1f + ep2f) / 2.0f);
+        ap->mu_f = (double)((mu1f + mu2f) / 2.0f);
         return SIEB200_OK;
     }
     // SIE-GSTC (gstc_sie.hpp:73-100; sie_kernels_assembly.cuh:225-231; sie_scaling.cuh:48-61).
@@ -236,6 +253,23 @@ int validate(const sieb200_mesh* mesh, const sieb200_options* o, const double* t
     SIEB_CHECK(o->singularity_threshold_lambda0 > 0, SIEB200_INVALID_ARG,
                "singularity threshold in lambda0 must be positive");
     SIEB_CHECK(o->basis == 0 || o->basis == 1, SIEB200_INVALID_ARG, "unsupported GSTC basis type");
+    SIEB_CHECK(o->variant >= SIEB200_VARIANT_T && o->variant <= SIEB200_VARIANT_N_JUMP, SIEB200_INVALID_ARG,
+               "unknown formulation variant");
+    SIEB_CHECK(o->formulation != SIEB200_GSTC || o->variant == SIEB200_VARIANT_T, SIEB200_INVALID_ARG,
+               "the SIE-GSTC formulation has no testing variants");
+    SIEB_CHECK(o->ntl_form == SIEB200_NTL_SURFACE || o->ntl_form == SIEB200_NTL_LINE, SIEB200_INVALID_ARG,
+               "unknown nTL integral form");
+    if (o->ntl_form == SIEB200_NTL_LINE) {
+        // pec_solver.cu:96-97 and dielectric_solver.cu:123-125 reject the line
+        // form where no nTL is line-integrated; where it would be, form A is
+        // not part of this library.
+        SIEB_CHECK(o->formulation != SIEB200_PEC_EFIE || o->variant == SIEB200_VARIANT_N, SIEB200_INVALID_ARG,
+                   "line nTL form requires N-EFIE");
+        SIEB_CHECK(o->formulation != SIEB200_PMCHWT || o->variant != SIEB200_VARIANT_T, SIEB200_INVALID_ARG,
+                   "line nTL form requires N-PMCHWT or N-Muller formulation");
+        set_error("the line (form A) nTL integral is not built; use the surface form");
+        return SIEB200_UNSUPPORTED;
+    }
     const int64_t N = system_dimension(o->formulation, mesh->num_edges);
     SIEB_CHECK(N <= std::numeric_limits<int>::max(), SIEB200_OVERFLOW,
                "SIE matrix dimension exceeds the int limit of the dense solvers");

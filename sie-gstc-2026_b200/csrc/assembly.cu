@@ -1,7 +1,13 @@
-// Dense RWG-Galerkin impedance-matrix assembly (PEC T-EFIE, T-PMCHWT, SIE-GSTC).
+// Dense RWG-Galerkin impedance-matrix assembly (PEC T-EFIE / N-EFIE / N-MFIE,
+// T-PMCHWT / N-PMCHWT / N-Muller, SIE-GSTC).
 //
 // Reference behaviour (paths relative to the SIE-GSTC project):
 //   per face pair TL/TK      include/sie_mom/cuda/dunavant_quadrature.cuh:207-324
+//   per face pair nTL/nTK    dunavant_quadrature.cuh:342-480 (surface form B),
+//                            singular part 889-1040
+//   RWG Gram (jump terms)    dunavant_quadrature.cuh:1261-1326
+//   rotated-testing blocks   src/sie_mom/solvers/dielectric/dielectric_kernels.cu:155-500,
+//                            src/sie_mom/solvers/pec_solver.cu:113-240
 //   singular extraction      dunavant_quadrature.cuh:769-875,
 //                            include/sie_mom/cuda/semi_analytic_integrals.cuh:35-92, 563-667
 //   Green kernels            include/sie_mom/cuda/green_functions_utils.cuh:236-361
@@ -78,6 +84,17 @@ __device__ __forceinline__ float centroid_distance(const FaceGeom& a, const Face
     return (float)__dsqrt_rn(s);
 }
 
+// Extraction test: the dielectric kernels compare the float-rounded centroid
+// distance (dielectric_kernels.cu:201-206), the PEC N-EFIE / N-MFIE kernels
+// the double distance against the float threshold (pec_solver.cu:134-136).
+__device__ __forceinline__ bool near_pair(const FaceGeom& a, const FaceGeom& b, float thr, int exact) {
+    if (!exact) return centroid_distance(a, b) < thr;
+    const double dx = __dsub_rn(a.c.x, b.c.x), dy = __dsub_rn(a.c.y, b.c.y),
+                 dz = __dsub_rn(a.c.z, b.c.z);
+    const double s = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    return __dsqrt_rn(s) < (double)thr;
+}
+
 __global__ void face_prep_kernel(const double* __restrict__ V, const int* __restrict__ F,
                                  const int* __restrict__ FE, int nf, const float* __restrict__ qpts,
                                  int Q, FaceGeom* __restrict__ geom, d3* __restrict__ qp) {
@@ -116,14 +133,14 @@ __global__ void face_prep_kernel(const double* __restrict__ V, const int* __rest
 }
 
 // Near pairs: count (list == nullptr) or fill.
-__global__ void near_pairs_kernel(const FaceGeom* __restrict__ geom, int nf, float thr,
+__global__ void near_pairs_kernel(const FaceGeom* __restrict__ geom, int nf, float thr, int exact,
                                   int m0, int m1, unsigned long long* counter, int2* list,
                                   unsigned long long capacity) {
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long span = (long long)(m1 - m0) * nf;
     if (id >= span) return;
     const int m = m0 + (int)(id / nf), n = (int)(id % nf);
-    if (centroid_distance(geom[m], geom[n]) < thr) {
+    if (near_pair(geom[m], geom[n], thr, exact)) {
         const unsigned long long slot = atomicAdd(counter, 1ull);
         if (list && slot < capacity) list[slot] = make_int2(m, n);
     }
@@ -462,6 +479,275 @@ __global__ void pair_singular_kernel(const FaceGeom* __restrict__ geom, const d3
     }
 }
 
+// ---------------------------------------------- rotated (n x RWG) testing --
+// Surface form B of nTL / nTK (dunavant_quadrature.cuh:342-480) with
+// tau_mj = rho_mj x n_m and the TK kernel vector g R (R = r_p - r_q):
+//   nTL = 1/4 (tau . rho_ni) G - 1/(2 k^2) tau . (g R),
+//   nTK = 1/4 (tau x rho_ni) . (g R)   (not on the coincident face).
+// With tau = t_p - t_j (t_p = p_l x n_m, t_j = A_j x n_m) and
+// rho_ni = q_l - B_i, the nine RWG pairs follow from per-warp moments:
+//   sum G tau.rho        = Stq - St.B - t_j.Sq + (t_j.B) S0
+//   sum g tau.R          = TtR - t_j.TR
+//   sum g (tau x rho).R  = U0 - B.V1 - t_j.V2 + (t_j x B).TR
+// St = sum G t_p, Sq = sum G q_l, Stq = sum G t_p.q_l, TR = sum g R,
+// TtR = sum g t_p.R, U0 = sum g (t_p x q_l).R, V1 = sum g R x t_p,
+// V2 = sum g q_l x R.
+template <int NK, bool NTK>
+struct MomentsN {
+    cplx S0[NK], St[NK][3], Sq[NK][3], Stq[NK];
+    cplx TR[NK][3], TtR[NK];
+    cplx U0[NTK ? NK : 1], V1[NTK ? NK : 1][3], V2[NTK ? NK : 1][3];
+};
+
+__device__ __forceinline__ d3 face_normal(const FaceGeom& g) {
+    return normalize3(cross3(g.v[1] - g.v[0], g.v[2] - g.v[0]));
+}
+
+// Regular (or extracted-kernel) double quadrature of the rotated-testing
+// blocks of all face pairs (m, n), m in [m0, m1). Output per pair: nTL for
+// each wavenumber, then (NTK) nTK for each, 3x3 complex each, in the slots
+// pair_regular_kernel gives TL and TK.
+template <int NK, bool NTK>
+__global__ void __launch_bounds__(kWarps * 32, 1)
+pair_regular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                      const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
+                      float thr, int exact, cplx* __restrict__ pairs) {
+    constexpr int NB = NTK ? 2 * NK : NK;
+    __shared__ d3 s_tp[kMaxQ], s_tt[kMaxQ];
+    __shared__ double s_w[kMaxQ];
+    __shared__ d3 s_sp[kWarps][kMaxQ], s_sl[kWarps][kMaxQ];
+
+    const int m = m0 + blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const FaceGeom& gm = geom[m];
+    const d3 nm = face_normal(gm);
+    for (int t = threadIdx.x; t < Q; t += blockDim.x) {
+        const d3 r = qp[(size_t)m * Q + t];
+        s_tp[t] = r;
+        s_tt[t] = cross3(r - gm.c, nm);
+        s_w[t] = (double)qw_g[t];
+    }
+    __syncthreads();
+    const double kk[2] = {k0, k1};
+    const int QQ = Q * Q;
+
+    for (int n = warp; n < nf; n += kWarps) {
+        const FaceGeom& gn = geom[n];
+        const d3 cn = gn.c;
+        for (int t = lane; t < Q; t += 32) {
+            const d3 r = ldg3(&qp[(size_t)n * Q + t]);
+            s_sp[warp][t] = r;
+            s_sl[warp][t] = r - cn;
+        }
+        __syncwarp();
+        const bool regular = near_pair(gm, gn, thr, exact);  // warp-uniform
+        const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] &&
+                           gm.idx[2] == gn.idx[2];
+
+        MomentsN<NK, NTK> M;
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            M.S0[a] = cx(0, 0); M.Stq[a] = cx(0, 0); M.TtR[a] = cx(0, 0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { M.St[a][c] = cx(0, 0); M.Sq[a][c] = cx(0, 0); M.TR[a][c] = cx(0, 0); }
+            if (NTK) {
+                M.U0[a] = cx(0, 0);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { M.V1[a][c] = cx(0, 0); M.V2[a][c] = cx(0, 0); }
+            }
+        }
+
+        for (int idx = lane; idx < QQ; idx += 32) {
+            const int p = idx / Q, q = idx - p * Q;
+            const d3 rp = s_tp[p], rq = s_sp[warp][q];
+            const d3 tp = s_tt[p], ql = s_sl[warp][q];
+            const double ww = s_w[p] * s_w[q];
+            const d3 Rv = rp - rq;
+            const double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+            if (!regular && R < 1e-12) continue;
+            const double tq = dot3(tp, ql), tR = dot3(tp, Rv);
+            double u0 = 0.0;
+            d3 v1 = mk3(0, 0, 0), v2 = mk3(0, 0, 0);
+            if (NTK) {
+                u0 = dot3(cross3(tp, ql), Rv);
+                v1 = cross3(Rv, tp);
+                v2 = cross3(ql, Rv);
+            }
+            const double inv_R = regular ? 0.0 : 1.0 / R;
+            const double i4pR = regular ? 0.0 : 1.0 / (4.0 * kPi * R);
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                cplx G, g;
+                if (regular) green_reg(R, kk[a], G, g);
+                else green_std(R, inv_R, i4pR, kk[a], G, g);
+                const cplx Gw = G * ww, gw = g * ww;
+                M.S0[a] += Gw;
+                M.St[a][0] += Gw * tp.x; M.St[a][1] += Gw * tp.y; M.St[a][2] += Gw * tp.z;
+                M.Sq[a][0] += Gw * ql.x; M.Sq[a][1] += Gw * ql.y; M.Sq[a][2] += Gw * ql.z;
+                M.Stq[a] += Gw * tq;
+                M.TR[a][0] += gw * Rv.x; M.TR[a][1] += gw * Rv.y; M.TR[a][2] += gw * Rv.z;
+                M.TtR[a] += gw * tR;
+                if (NTK) {
+                    M.U0[a] += gw * u0;
+                    M.V1[a][0] += gw * v1.x; M.V1[a][1] += gw * v1.y; M.V1[a][2] += gw * v1.z;
+                    M.V2[a][0] += gw * v2.x; M.V2[a][1] += gw * v2.y; M.V2[a][2] += gw * v2.z;
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            warp_sum(M.S0[a]); warp_sum(M.Stq[a]); warp_sum(M.TtR[a]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) { warp_sum(M.St[a][c]); warp_sum(M.Sq[a][c]); warp_sum(M.TR[a][c]); }
+            if (NTK) {
+                warp_sum(M.U0[a]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { warp_sum(M.V1[a][c]); warp_sum(M.V2[a][c]); }
+            }
+        }
+        if (lane < 9) {
+            const int j = lane / 3, i = lane - 3 * j;
+            const d3 tj = cross3(gm.A[j], nm), B = gn.A[i];
+            const double scale = gm.len[j] * gn.len[i];
+            const double tjB = dot3(tj, B);
+            const d3 tjxB = cross3(tj, B);
+            cplx* out = pairs + ((size_t)blockIdx.x * nf + n) * (NB * 9);
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                cplx s = M.Stq[a];
+                s = s - (M.St[a][0] * B.x + M.St[a][1] * B.y + M.St[a][2] * B.z);
+                s = s - (M.Sq[a][0] * tj.x + M.Sq[a][1] * tj.y + M.Sq[a][2] * tj.z);
+                s += M.S0[a] * tjB;
+                const cplx t = M.TtR[a] - (M.TR[a][0] * tj.x + M.TR[a][1] * tj.y + M.TR[a][2] * tj.z);
+                out[a * 9 + lane] = (s * 0.25 + t * (-0.5 / (kk[a] * kk[a]))) * scale;
+                if (NTK) {
+                    cplx u = cx(0, 0);
+                    if (!coinc) {
+                        u = M.U0[a];
+                        u = u - (M.V1[a][0] * B.x + M.V1[a][1] * B.y + M.V1[a][2] * B.z);
+                        u = u - (M.V2[a][0] * tj.x + M.V2[a][1] * tj.y + M.V2[a][2] * tj.z);
+                        u += M.TR[a][0] * tjxB.x + M.TR[a][1] * tjxB.y + M.TR[a][2] * tjxB.z;
+                        u = u * (0.25 * scale);
+                    }
+                    out[(NK + a) * 9 + lane] = u;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Singular (extracted) part of the rotated-testing blocks of the near pairs
+// (dunavant_quadrature.cuh:889-1040), added to the pair blocks. Per outer
+// point, with phi_1 = phi_1b - d phi_0 n_n and the extracted gradient
+// phi_3b - d phi_2 n_n:
+//   nTL += 1/2 tau . (phi_1 + 1/2 R_i phi_0 + gradient / k^2)
+//          (the gradient left out on the coincident face),
+//   nTK += 1/4 tau . Upsilon_coul (not on the coincident face),
+// then e_mj e_ni / (4 pi A_n). One warp per pair, lanes over outer points.
+template <int NK>
+__global__ void pair_singular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                       const float* __restrict__ qw_g, int Q, int nf, int m0,
+                                       const int2* __restrict__ list, int count, double k0,
+                                       double k1, bool with_ntk, cplx* __restrict__ pairs) {
+    const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp_global >= count) return;
+    const int2 mn = list[warp_global];
+    const FaceGeom gm = geom[mn.x];
+    const FaceGeom gn = geom[mn.y];
+    const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] && gm.idx[2] == gn.idx[2];
+    const d3 nm = face_normal(gm), nn = face_normal(gn);
+    const double kk[2] = {k0, k1};
+    double tl[NK][9], tk[NK][9];
+#pragma unroll
+    for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int t = 0; t < 9; ++t) { tl[a][t] = 0.0; tk[a][t] = 0.0; }
+
+    for (int p = lane; p < Q; p += 32) {
+        const d3 rp = qp[(size_t)mn.x * Q + p];
+        const double wp = (double)qw_g[p];
+        const Pots P = wilton(rp, gn.v);
+        const d3 phi1 = P.phi1b - nn * (P.d * P.phi0);
+        const d3 grad = P.phi3b - nn * (P.d * P.phi2);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const d3 tau = cross3(rp - gm.fv[j], nm);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const d3 br = phi1 + ((rp - gn.fv[i]) * 0.5) * P.phi0;
+#pragma unroll
+                for (int a = 0; a < NK; ++a) {
+                    const d3 V = coinc ? br : br + grad * (1.0 / (kk[a] * kk[a]));
+                    tl[a][j * 3 + i] += 0.5 * dot3(tau, V) * wp;
+                    if (with_ntk && !coinc) {
+                        const d3 up = upsilon(P, gn.fv[i], rp, (float)kk[a]);
+                        tk[a][j * 3 + i] += 0.25 * dot3(tau, up) * wp;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NK; ++a)
+#pragma unroll
+        for (int t = 0; t < 9; ++t) { warp_sum(tl[a][t]); warp_sum(tk[a][t]); }
+    if (lane < 9) {
+        const int j = lane / 3, i = lane - 3 * j;
+        const double as = 1.0 / (4.0 * kPi * gn.area);
+        const double s = as * gm.len[j] * gn.len[i];
+        const int NB = with_ntk ? 2 * NK : NK;
+        cplx* out = pairs + ((size_t)(mn.x - m0) * nf + mn.y) * (NB * 9);
+#pragma unroll
+        for (int a = 0; a < NK; ++a) {
+            double tlv = 0.0, tkv = 0.0;
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+                if (t == lane) { tlv = tl[a][t]; tkv = tk[a][t]; }
+            out[a * 9 + lane].re += tlv * s;
+            if (with_ntk) out[(NK + a) * 9 + lane].re += tkv * s;
+        }
+    }
+}
+
+// RWG Gram block <f_j, f_i> of each face (dunavant_quadrature.cuh:1261-1326)
+// with the reference's float dot product, weight and scale. One thread per
+// face, gram[9 f + 3 j + i].
+__global__ void gram_face_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                                 const float* __restrict__ qw_g, int Q, int nf, double* __restrict__ gram) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const FaceGeom& g = geom[f];
+    double R[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) R[e] = 0.0;
+    for (int p = 0; p < Q; ++p) {
+        const float wp = qw_g[p];
+        const d3 rp = qp[(size_t)f * Q + p];
+        d3 rho[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) rho[i] = rp - g.fv[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const double d = __dadd_rn(__dadd_rn(__dmul_rn(rho[j].x, rho[i].x), __dmul_rn(rho[j].y, rho[i].y)),
+                                           __dmul_rn(rho[j].z, rho[i].z));
+                R[j * 3 + i] += (double)__fmul_rn(wp, (float)d);
+            }
+    }
+    const float area = (float)g.area;
+    const float sc = __fdiv_rn(1.f, __fmul_rn(4.f, area));
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float fs = __fmul_rn(__fmul_rn(sc, (float)g.len[j]), (float)g.len[i]);
+            gram[(size_t)f * 9 + j * 3 + i] = R[j * 3 + i] * (double)fs;
+        }
+}
+
 // ------------------------------------------------------------ GSTC mass --
 // Mass block of tensor t (0..3: the Y blocks ee, em, me, mm after the perp
 // transform; 4..7 the Z blocks) of face g for the 2x2 tensor block
@@ -670,12 +956,18 @@ __global__ void tensor_grad_kernel(const FaceGeom* __restrict__ geom, const d3* 
 // ------------------------------------------------------------ gather ----
 struct GatherParams {
     int formulation;
+    int variant;  // 0 tangential testing; 1 N-EFIE / N-PMCHWT; 2 N-MFIE / N-Muller
     int nf, ne;
     int m0, m1;
     int NB;
     cplx c_jj[2], c_mm[2];
     double s_jm, s_mm;
     double me, me2;  // mass scales (float eta0, eta0^2)
+    // N-Muller (dielectric_kernels.cu:433-488): z_jj = w_em[1] nTL2 - w_em[0] nTL1
+    // (w_em = omega eps mu), z_jm = eps2 nTK2 - eps1 nTK1 - eps_f G,
+    // z_mj = mu2 nTK2 - mu1 nTK1 - mu_f G on the same face.
+    double w_em[2], eps[2], mu[2], eps_f, mu_f;
+    const double* gram;  // RWG Gram blocks (N-MFIE, N-Muller), 9 per face
 };
 
 // The region block (1x1 PEC, 2x2 PMCHWT, 4x4 GSTC) of Z at test edge te and
@@ -697,6 +989,7 @@ __device__ __forceinline__ bool edge_pair_block(const cplx* __restrict__ pairs, 
 #pragma unroll
     for (int k = 0; k < 8; ++k) mass_acc[k] = cx(0, 0);
     bool has_mass = false;
+    double gram_acc = 0.0;
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         if (it[a] < 0) continue;
@@ -716,14 +1009,27 @@ __device__ __forceinline__ bool edge_pair_block(const cplx* __restrict__ pairs, 
 #pragma unroll
                 for (int k = 0; k < 8; ++k) mass_acc[k] += mb[k * 9];
             }
+            if (P.variant == 2 && m == n) gram_acc += P.gram[(size_t)m * 9 + j * 3 + i];
         }
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) blk[r][c] = cx(0, 0);
-    if (P.formulation == SIEB200_PEC_EFIE) {
+    if (P.formulation == SIEB200_PEC_EFIE && P.variant == 2) {
+        // N-MFIE (pec_solver.cu:171-240): 1/2 Gram on the same face, - nTK2.
+        blk[0][0] = cx(0.5 * gram_acc, 0.0) - acc[1];
+    } else if (P.formulation == SIEB200_PEC_EFIE) {
         blk[0][0] = P.c_jj[1] * acc[0];
+    } else if (P.formulation == SIEB200_PMCHWT && P.variant == 2) {
+        // acc: nTL1, nTL2, nTK1, nTK2.
+        const cplx jj = acc[1] * cx(0.0, P.w_em[1]) - acc[0] * cx(0.0, P.w_em[0]);
+        const cplx jm = acc[3] * P.eps[1] - acc[2] * P.eps[0] - cx(P.eps_f * gram_acc, 0.0);
+        const cplx mj = acc[3] * P.mu[1] - acc[2] * P.mu[0] - cx(P.mu_f * gram_acc, 0.0);
+        blk[0][0] = jj;
+        blk[0][1] = jm * P.s_jm;
+        blk[1][0] = mj * P.s_jm;
+        blk[1][1] = jj * (-P.s_mm);
     } else if (P.formulation == SIEB200_PMCHWT) {
         // acc: TL1, TL2, TK1, TK2
         const cplx tk = acc[2] + acc[3];
@@ -913,10 +1219,24 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
         SIEB_TRY_CUDA(cudaGetLastError());
     }
 
-    // Slabs of test faces bounded by the pair-block workspace.
-    const bool tk = opt.formulation != SIEB200_PEC_EFIE;
+    // RWG Gram blocks for the jump terms of N-MFIE and N-Muller.
+    const int variant = ap.variant;
+    double* dgram = nullptr;
+    if (variant == 2) {
+        SIEB_RETURN_IF(ctx->mass.reserve(sizeof(double) * 9 * (size_t)nf));
+        dgram = ctx->mass.as<double>();
+        gram_face_kernel<<<(nf + 127) / 128, 128, 0, st>>>(geom, qp, dw, Q, nf, dgram);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+    }
+
+    // Slabs of test faces bounded by the pair-block workspace. Blocks per
+    // pair: TL (or nTL) per wavenumber, then TK (or nTK) where the
+    // formulation uses it (all but T-EFIE and N-EFIE).
+    const bool tk = !(opt.formulation == SIEB200_PEC_EFIE && variant != 2);
     const int NK = ap.nk;
     const int NB = tk ? 2 * NK : NK;
+    const int exact = (opt.formulation == SIEB200_PEC_EFIE && variant != 0) ? 1 : 0;
     const size_t pair_bytes = sizeof(cplx) * 9 * NB;
     size_t budget = (size_t)8 << 30;
     size_t free_b = 0, total_b = 0;
@@ -941,11 +1261,24 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
     gp.c_mm[0] = ap.c_mm[0]; gp.c_mm[1] = ap.c_mm[1];
     gp.s_jm = ap.s_jm; gp.s_mm = ap.s_mm;
     gp.me = ap.mass_eta0; gp.me2 = ap.mass_eta0_sq;
+    gp.variant = variant;
+    for (int r = 0; r < 2; ++r) { gp.w_em[r] = ap.w_em[r]; gp.eps[r] = ap.eps[r]; gp.mu[r] = ap.mu[r]; }
+    gp.eps_f = ap.eps_f; gp.mu_f = ap.mu_f;
+    gp.gram = dgram;
 
     for (int m0 = 0; m0 < nf; m0 += slab) {
         const int m1 = std::min(nf, m0 + slab);
         const int rows = m1 - m0;
-        if (opt.formulation == SIEB200_PEC_EFIE)
+        if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE && !tk)
+            pair_regular_n_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, exact, pairs);
+        else if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE)
+            pair_regular_n_kernel<1, true><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, exact, pairs);
+        else if (variant != 0)
+            pair_regular_n_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, exact, pairs);
+        else if (opt.formulation == SIEB200_PEC_EFIE)
             pair_regular_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, pairs);
         else
@@ -958,7 +1291,7 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
         const long long span = (long long)rows * nf;
         const int nb = (int)((span + 255) / 256);
         SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-        near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter, nullptr, 0);
+        near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, exact, m0, m1, counter, nullptr, 0);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         unsigned long long count = 0;
@@ -967,13 +1300,21 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
         if (count > 0) {
             SIEB_RETURN_IF(ctx->near_list.reserve(sizeof(int2) * count));
             SIEB_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-            near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, m0, m1, counter,
+            near_pairs_kernel<<<nb, 256, 0, st>>>(geom, nf, ap.threshold, exact, m0, m1, counter,
                                                   ctx->near_list.as<int2>(), count);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             const int threads = 128;
             const int blocks = (int)((count * 32 + threads - 1) / threads);
-            if (opt.formulation == SIEB200_PEC_EFIE)
+            if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE)
+                pair_singular_n_kernel<1><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],
+                    ap.k[1], tk, pairs);
+            else if (variant != 0)
+                pair_singular_n_kernel<2><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[0],
+                    ap.k[1], true, pairs);
+            else if (opt.formulation == SIEB200_PEC_EFIE)
                 pair_singular_kernel<1><<<blocks, threads, 0, st>>>(
                     geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],
                     ap.k[1], false, pairs);

@@ -153,6 +153,14 @@ struct AssemblyParams {
     // GSTC mass-block scales (float eta0 and eta0^2).
     double mass_eta0 = 1, mass_eta0_sq = 1;
     int basis = 0;
+    // Testing variant: 0 tangential (T-EFIE, T-PMCHWT, GSTC); 1 rotated
+    // n x RWG (N-EFIE, N-PMCHWT; nTL/nTK in the TL/TK slots, same placement);
+    // 2 N-MFIE (1/2 Gram - nTK2) or N-Muller (below).
+    int variant = 0;
+    // N-Muller: w_em[r] = omega eps_r mu_r, eps/mu per region (float-valued),
+    // eps_f/mu_f their float means; s_jm = eta0, s_mm = eta0^2 as for PMCHWT.
+    double w_em[2] = {0, 0}, eps[2] = {0, 0}, mu[2] = {0, 0};
+    double eps_f = 0, mu_f = 0;
 };
 
 int make_assembly_params(const sieb200_options& opt, AssemblyParams* out);

@@ -4,8 +4,10 @@
 // testing with float edge lengths and weights), source functors
 // include/sie_mom/excitation/source_functors.cuh:14-130, placements
 // src/sie_mom/solvers/pec_solver.cu:242-264 (PEC),
-// src/sie_mom/solvers/dielectric/dielectric_solver.cu:399-530 (T-PMCHWT) and
-// include/sie_mom/cuda/sie_kernels_utils.cuh:184-232 (SIE-GSTC).
+// src/sie_mom/solvers/dielectric/dielectric_solver.cu:399-530 (T-PMCHWT,
+// N-PMCHWT, N-Muller), pec_solver.cu:365-388 (T-EFIE, N-EFIE, N-MFIE) and
+// include/sie_mom/cuda/sie_kernels_utils.cuh:184-232 (SIE-GSTC). The rotated
+// variants test with rho x n_m (dunavant_quadrature.cuh:1569-1593).
 //
 // One thread per (face, source) computes the face's three tested values;
 // one thread per (edge, source) gathers the <= 2 incident faces and places
@@ -30,9 +32,11 @@ struct DevSource {
     int is_magnetic;
     double a[3], b[3];
     double k, eta;
-    // placement: rows get v_E * se and v_H * sh at offsets oe, oh (in units of E)
+    // placement: rows get v_E * se and v_H * sh at offsets oe, oh (in units of
+    // E; a negative offset places nothing)
     double se, sh;
     int oe, oh;
+    int rotated;  // n x RWG testing (dunavant_quadrature.cuh:1569-1593)
 };
 
 namespace {
@@ -103,6 +107,11 @@ __global__ void rhs_face_kernel(const double* __restrict__ V, const int* __restr
     const int EA[3] = {0, 1, 2}, EB[3] = {1, 2, 0}, EF[3] = {2, 0, 1};
     float el[3];
     d3 fv[3];
+    d3 nm = mk3(0, 0, 0);
+    if (S.rotated) {
+        const d3 cr = cross3(v[1] - v[0], v[2] - v[0]);
+        nm = cr * (1.0 / sqrt(dot3(cr, cr)));
+    }
     for (int e = 0; e < 3; ++e) {
         const d3 ev = v[EB[e]] - v[EA[e]];
         const double l = sqrt(ev.x * ev.x + ev.y * ev.y + ev.z * ev.z);
@@ -120,7 +129,7 @@ __global__ void rhs_face_kernel(const double* __restrict__ V, const int* __restr
         cplx E[3], H[3];
         source_fields(S, rp, E, H);
         for (int i = 0; i < 3; ++i) {
-            const d3 t = rp - fv[i];
+            const d3 t = S.rotated ? cross3(rp - fv[i], nm) : rp - fv[i];
             const cplx de = cx(t.x * E[0].re + t.y * E[1].re + t.z * E[2].re,
                                t.x * E[0].im + t.y * E[1].im + t.z * E[2].im);
             const cplx dh = cx(t.x * H[0].re + t.y * H[1].re + t.z * H[2].re,
@@ -155,7 +164,7 @@ __global__ void rhs_gather_kernel(const cplx* __restrict__ face_vals, const int*
     }
     cplx* col = B + (int64_t)s * ldb;
     // Column zeroing happens before launch; each (row) is owned by one thread.
-    col[e + (int64_t)S.oe * ne] = ve * S.se;
+    if (S.oe >= 0) col[e + (int64_t)S.oe * ne] = ve * S.se;
     if (S.oh >= 0) col[e + (int64_t)S.oh * ne] = vh * S.sh;
 }
 
@@ -370,9 +379,22 @@ int prepare_sources(const sieb200_options& opt, const sieb200_source* sources, i
             const double mn = std::hypot(in.a[0], in.a[1], in.a[2]);
             SIEB_CHECK(mn > 0 && std::isfinite(mn), SIEB200_INVALID_ARG, "dipole moment magnitude must be positive and finite");
         }
+        d.rotated = opt.variant != SIEB200_VARIANT_T;
         if (opt.formulation == SIEB200_PEC_EFIE) {
             SIEB_CHECK(in.region == 2, SIEB200_INVALID_ARG, "PEC solver requires an exterior (region 2) source");
-            d.se = 1.0; d.sh = 0.0; d.oe = 0; d.oh = -1;
+            if (opt.variant == SIEB200_VARIANT_N_JUMP) {
+                // N-MFIE: +<f x n, H_inc> (pec_solver.cu:372-377).
+                d.se = 0.0; d.sh = 1.0; d.oe = -1; d.oh = 0;
+            } else {
+                d.se = 1.0; d.sh = 0.0; d.oe = 0; d.oh = -1;
+            }
+        } else if (opt.formulation == SIEB200_PMCHWT && opt.variant == SIEB200_VARIANT_N_JUMP) {
+            // N-Muller: eps V_E and -mu eta0 V_H of the source region
+            // (dielectric_solver.cu:461-489).
+            const double eta0 = std::sqrt(opt.vacuum_permeability / opt.vacuum_permittivity);
+            d.se = eps_r * opt.vacuum_permittivity;
+            d.sh = -(mu_r * opt.vacuum_permeability) * eta0;
+            d.oe = 0; d.oh = 1;
         } else if (opt.formulation == SIEB200_PMCHWT) {
             const double eta0 = std::sqrt(opt.vacuum_permeability / opt.vacuum_permittivity);
             const double sign = in.region == 2 ? 1.0 : -1.0;

@@ -16,7 +16,9 @@ import numpy as np
 from . import _build
 
 OK, INVALID_ARG, OVERFLOW, SINGULAR, NONFINITE, NOT_CONVERGED, CUDA_ERROR, TIMEOUT, NO_DEVICE, \
-    OUT_OF_MEMORY = range(10)
+    OUT_OF_MEMORY, UNSUPPORTED = range(11)
+VARIANT_T, VARIANT_N, VARIANT_N_JUMP = 0, 1, 2
+NTL_SURFACE, NTL_LINE = 0, 1
 PEC_EFIE, PMCHWT, GSTC = 0, 1, 2
 SOLVER_LU_FP64, SOLVER_LU_CUSOLVER, SOLVER_MIXED_IR, SOLVER_GMRES_C64 = 0, 1, 2, 3
 
@@ -24,6 +26,7 @@ _STATUS_NAMES = {
     INVALID_ARG: "invalid argument", OVERFLOW: "overflow", SINGULAR: "singular matrix",
     NONFINITE: "non-finite value", NOT_CONVERGED: "not converged", CUDA_ERROR: "CUDA error",
     TIMEOUT: "timeout", NO_DEVICE: "no CUDA device", OUT_OF_MEMORY: "out of device memory",
+    UNSUPPORTED: "unsupported option",
 }
 
 
@@ -54,7 +57,7 @@ class Options(ctypes.Structure):
                 ("basis", ctypes.c_int), ("tensors_are_uniform", ctypes.c_int),
                 ("compute_residual", ctypes.c_int), ("solver", ctypes.c_int),
                 ("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int),
-                ("restart", ctypes.c_int)]
+                ("restart", ctypes.c_int), ("variant", ctypes.c_int), ("ntl_form", ctypes.c_int)]
 
 
 class Source(ctypes.Structure):

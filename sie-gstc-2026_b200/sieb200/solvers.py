@@ -65,6 +65,19 @@ class DipoleExcitation:
         return s
 
 
+# PecFormulation (pec_solver.hpp:12) and DielectricFormulation
+# (dielectric_solver.hpp:15-19) by enum name, plus the applications' CLI
+# spellings (pec_sphere_app.cpp:83-92, pmchwt_app.cpp:158-167).
+PEC_FORMULATIONS = {"TEfie": _lib.VARIANT_T, "NEfie": _lib.VARIANT_N, "NMfie": _lib.VARIANT_N_JUMP,
+                    "t-efie": _lib.VARIANT_T, "n-efie": _lib.VARIANT_N, "n-mfie": _lib.VARIANT_N_JUMP,
+                    "t": _lib.VARIANT_T, "n": _lib.VARIANT_N}
+DIELECTRIC_FORMULATIONS = {"T_PMCHWT": _lib.VARIANT_T, "N_PMCHWT": _lib.VARIANT_N,
+                           "N_Muller": _lib.VARIANT_N_JUMP, "t": _lib.VARIANT_T, "n": _lib.VARIANT_N,
+                           "muller": _lib.VARIANT_N_JUMP}
+NTL_FORMS = {"Surface": _lib.NTL_SURFACE, "Line": _lib.NTL_LINE, "surface": _lib.NTL_SURFACE,
+             "line": _lib.NTL_LINE}
+
+
 @dataclass
 class PecOptions:
     frequency_hz: float = 0.0
@@ -72,6 +85,9 @@ class PecOptions:
     quadrature_rule: int = 7
     singularity_threshold_lambda0: float = 0.1
     compute_residual: bool = True
+    formulation: str = "TEfie"
+    ntl_form: str = "Surface"
+    line_quadrature_points: int = 20
     vacuum_permittivity: float = 8.8541878128e-12
     vacuum_permeability: float = 1.25663706212e-6
     solver: str = "lu_cusolver"
@@ -89,6 +105,9 @@ class DielectricOptions:
     compute_residual: bool = True
     vacuum_permittivity: float = 8.8541878128e-12
     vacuum_permeability: float = 1.25663706212e-6
+    formulation: str = "T_PMCHWT"
+    ntl_form: str = "Surface"
+    line_quadrature_points: int = 20
     solver: str = "lu_cusolver"
     tolerance: float = 1e-10
     max_iterations: int = 50
@@ -129,6 +148,20 @@ def to_c_options(opt, formulation: int) -> _lib.Options:
     o.solver = SOLVERS[opt.solver]
     o.tolerance = float(opt.tolerance)
     o.max_iterations = int(opt.max_iterations)
+    if formulation != _lib.GSTC:
+        table = PEC_FORMULATIONS if formulation == _lib.PEC_EFIE else DIELECTRIC_FORMULATIONS
+        if opt.formulation not in table:
+            raise ValueError(f"unknown formulation {opt.formulation!r}; choose one of {sorted(table)}")
+        if opt.ntl_form not in NTL_FORMS:
+            raise ValueError("ntl_form must be 'Surface' or 'Line'")
+        o.variant = table[opt.formulation]
+        o.ntl_form = NTL_FORMS[opt.ntl_form]
+        line_integrated = (o.variant == _lib.VARIANT_N if formulation == _lib.PEC_EFIE
+                           else o.variant != _lib.VARIANT_T)
+        if o.ntl_form == _lib.NTL_LINE and line_integrated and \
+                not 1 <= int(opt.line_quadrature_points) <= 20:
+            # pec_solver.cu:91-95, dielectric_solver.cu:116-122
+            raise ValueError("Gauss-Legendre point count must be in [1, 20]")
     if formulation == _lib.GSTC:
         if opt.basis not in ("face", "spherical"):
             raise ValueError("unsupported GSTC basis type")

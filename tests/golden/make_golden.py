@@ -132,7 +132,7 @@ def main() -> None:
         kh = np.array([0.0, 0.0, 1.0])
         ref.ref_rhs_plane_wave(kind, L0.vertices.ctypes.data, L0.faces.ctypes.data,
                                L0.faces_edges.ctypes.data, 20, 30, 5, E0.ctypes.data, kh.ctypes.data,
-                               k, eta, 2, mu0, eps0, b.ctypes.data)
+                               k, eta, 2, mu0, eps0, b.ctypes.data, 0, 1.0, 1.0)
         out[f"b_{name}_L0"] = b
 
     # Far field of a seeded [J1, M1, J2, M2] vector on icosphere L1 r=0.5.
