@@ -115,8 +115,11 @@ def test_variant_solve_matches_oracle(name, solver, gpu_ctx, oracle_lib):
     r = (sieb200.solve_pec_dense if CASES[name][0] == 0 else sieb200.solve_dielectric_dense)(m, o, src,
                                                                                             ctx=gpu_ctx)
     x = _oracle_solution(oracle_lib, name, m, 5, C0, 0.1)
-    assert np.linalg.norm(r.currents - x) / np.linalg.norm(x) < X_TOL
-    assert r.metrics["relative_residual"] < 1e-10
+    # The mixed solver refines until the relative residual is below its
+    # tolerance (1e-10), so its forward error is bounded by cond(Z) * 1e-10.
+    tol = 1e-9 if solver == "mixed_ir" else X_TOL
+    assert np.linalg.norm(r.currents - x) / np.linalg.norm(x) < tol
+    assert r.metrics["relative_residual"] <= 1e-10
 
 
 def test_line_form_and_gstc_variant_are_refused(gpu_ctx):
