@@ -121,9 +121,11 @@ typedef struct {
     int variant;
     /* nTL integral form of the rotated variants (NtlIntegralForm,
      * dielectric_solver.hpp:22-25; PecNtlForm, pec_solver.hpp:13):
-     * SIEB200_NTL_SURFACE (form B, the reference default) is built;
-     * SIEB200_NTL_LINE (form A) is answered with SIEB200_UNSUPPORTED. */
+     * SIEB200_NTL_SURFACE (form B, the reference default) or SIEB200_NTL_LINE
+     * (form A: the scalar term as a Gauss-Legendre line integral along the
+     * testing edges), with line_quadrature_points (1..20, default 20). */
     int ntl_form;
+    int line_quadrature_points;
 } sieb200_options;
 enum {
     SIEB200_VARIANT_T = 0,       /* T-EFIE / T-PMCHWT: RWG testing */

@@ -21,7 +21,7 @@ _f = ctypes.c_float
 _d = ctypes.c_double
 _i = ctypes.c_int
 
-_ASSEMBLE = [_i, _P, _P, _P, _i, _i, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, _P, _i, _i, _P, _i, _i]
+_ASSEMBLE = [_i, _P, _P, _P, _i, _i, _i, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, _P, _i, _i, _P, _i, _i, _i]
 
 
 def _build_oracle() -> None:
@@ -42,7 +42,8 @@ def oracle() -> ctypes.CDLL:
     lib.so_build_edges.argtypes = [_P, _i, _P, _P]
     lib.so_wilton.argtypes = [_P, _P, _P]
     lib.so_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
-    lib.so_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.so_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _i, _P]
+    lib.so_gauss_legendre.argtypes = [_i, _P, _P]
     lib.so_assemble.argtypes = _ASSEMBLE
     lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
@@ -61,7 +62,8 @@ def reference() -> ctypes.CDLL | None:
     lib.ref_phi0.argtypes = [_P, _P]
     lib.ref_phi0.restype = _d
     lib.ref_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
-    lib.ref_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
+    lib.ref_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _i, _P]
+    lib.ref_gauss_legendre.argtypes = [_i, _P, _P]
     lib.ref_assemble.argtypes = _ASSEMBLE
     lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.ref_surface_fields.argtypes = _FIELDS
@@ -103,10 +105,11 @@ def kernel_scalars(kind: int, frequency_hz: float, eps_r=(1.0, 1.0), mu_r=(1.0, 
 
 
 def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, uniform=False,
-             basis=0, threads=0, fn="so_assemble", variant: int = 0) -> np.ndarray:
+             basis=0, threads=0, fn="so_assemble", variant: int = 0, line_points: int = 0) -> np.ndarray:
     """variant 1: rotated (n x RWG) testing, N-EFIE (kind 0) or N-PMCHWT
     (kind 1), surface nTL form; variant 2: N-MFIE (kind 0) or N-Muller
-    (kind 1)."""
+    (kind 1); line_points > 0 selects the line nTL form A with that many
+    Gauss-Legendre points (N-EFIE, N-PMCHWT, N-Muller)."""
     V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
     F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
     FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
@@ -117,7 +120,7 @@ def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, unifo
     s = scalars
     getattr(lib, fn)(kind, _p(V), _p(F), _p(FE), F.shape[0], ne, rule, s["k1"], s["k2"], s["mu_r1"],
                      s["mu_r2"], s["eps_r1"], s["eps_r2"], s["mu0"], s["eps0"], s["omega"], s["thr"],
-                     _p(t), int(uniform), int(basis), _p(Z), int(threads), int(variant))
+                     _p(t), int(uniform), int(basis), _p(Z), int(threads), int(variant), int(line_points))
     return Z
 
 

@@ -26,6 +26,7 @@
 #include "sie_mom/cuda/gstc_tensor_utils.cuh"
 #include "sie_mom/excitation/source_functors.cuh"
 #include "sie_mom/quadrature/triangle_dunavant_rule.hpp"
+#include "sie_mom/quadrature/gauss_legendre_rule.hpp"
 #include "sie_mom/mesh/spherical_surface.hpp"
 
 #include <Eigen/Dense>
@@ -50,7 +51,20 @@ inline void atomic_add(double* Z, size_t idx, const complex_t& v) {
 struct Quad {
     std::vector<float> pts, w;
     int n = 0;
+    // Gauss-Legendre line rule of the nTL form A, float as the solvers upload it
+    // (dielectric_solver.cu:179-197); empty for the surface form B.
+    std::vector<float> lt, lw;
+    int nl = 0;
 };
+
+void add_line_rule(Quad& q, int points) {
+    if (points <= 0) return;
+    std::vector<double> t(points), w(points);
+    gauss_legendre_rule(points, t.data(), w.data());
+    q.lt.assign(t.begin(), t.end());
+    q.lw.assign(w.begin(), w.end());
+    q.nl = points;
+}
 
 Quad make_rule(int rule) {
     Quad q;
@@ -116,11 +130,19 @@ void pair_blocks_n(const double* V, const int* F, int m, int n, const Quad& q, f
     const vec3_t sc = (sv[0] + sv[1] + sv[2]) / 3.f;
     const float dist = length(tc - sc);
     if (dist < thr) {
-        calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2, true,
-                                          l1, l2, n1, n2);
         complex_t s1[3][3], s2[3][3], s3[3][3], s4[3][3];
-        calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2,
-                                                s1, s2, s3, s4);
+        if (q.nl > 0) {
+            calculateFormAQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, q.lt.data(),
+                                             q.lw.data(), q.nl, k1, k2, true, l1, l2, n1, n2);
+            calculateFormASingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n,
+                                                         q.lt.data(), q.lw.data(), q.nl, k1, k2, s1, s2,
+                                                         s3, s4);
+        } else {
+            calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2,
+                                              true, l1, l2, n1, n2);
+            calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1,
+                                                    k2, s1, s2, s3, s4);
+        }
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) {
                 complexAddInPlace(l1[j][i], s1[j][i]);
@@ -128,6 +150,9 @@ void pair_blocks_n(const double* V, const int* F, int m, int n, const Quad& q, f
                 complexAddInPlace(n1[j][i], s3[j][i]);
                 complexAddInPlace(n2[j][i], s4[j][i]);
             }
+    } else if (q.nl > 0) {
+        calculateFormAQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, q.lt.data(),
+                                         q.lw.data(), q.nl, k1, k2, false, l1, l2, n1, n2);
     } else {
         calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k1, k2, false,
                                           l1, l2, n1, n2);
@@ -149,12 +174,21 @@ void pair_n_efie(const double* V, const int* F, int m, int n, const Quad& q, flo
     const vec3_t cn = (sv[0] + sv[1] + sv[2]) / real_t(3);
     const bool extract = length(cm - cn) < thr;
     complex_t l1[3][3], n1[3][3], n2[3][3];
-    calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2, extract,
-                                      l1, l2, n1, n2);
+    if (q.nl > 0)
+        calculateFormAQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, q.lt.data(),
+                                         q.lw.data(), q.nl, k2, k2, extract, l1, l2, n1, n2);
+    else
+        calculateDoubleQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2, extract,
+                                          l1, l2, n1, n2);
     if (extract) {
         complex_t s1[3][3], s2[3][3], s3[3][3], s4[3][3];
-        calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2,
-                                                s1, s2, s3, s4);
+        if (q.nl > 0)
+            calculateFormASingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n,
+                                                         q.lt.data(), q.lw.data(), q.nl, k2, k2, s1, s2,
+                                                         s3, s4);
+        else
+            calculateSingularPartQuadrature_nTL_nTK(tv, ti, sv, si, q.pts.data(), q.w.data(), q.n, k2, k2,
+                                                    s1, s2, s3, s4);
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) complexAddInPlace(l2[j][i], s2[j][i]);
     }
@@ -246,10 +280,12 @@ double ref_phi0(const double* r, const double* tri) {
 
 // Local 3x3 blocks of one face pair: out = [tl1, tl2, tk1, tk2] each 3x3
 // complex row-major (j test, i source), interleaved re/im (72 doubles).
-// nTL1, nTL2, nTK1, nTK2 of face pair (m, n), surface form B.
+// nTL1, nTL2, nTK1, nTK2 of face pair (m, n): surface form B (line_points 0)
+// or line form A with that many Gauss-Legendre points.
 void ref_pair_blocks_n(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
-                       float thr, double* out) {
-    const Quad q = make_rule(rule);
+                       float thr, int line_points, double* out) {
+    Quad q = make_rule(rule);
+    add_line_rule(q, line_points);
     complex_t a[3][3], b[3][3], c[3][3], d[3][3];
     pair_blocks_n(V, F, m, n, q, k1, k2, thr, a, b, c, d);
     complex_t(*blk[4])[3] = {a, b, c, d};
@@ -285,8 +321,9 @@ void ref_pair_blocks(const double* V, const int* F, int m, int n, int rule, floa
 int ref_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
                  float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                  float mu0, float eps0, float omega, float thr, const double* tensors,
-                 int tensors_uniform, int basis, double* Z, int threads, int variant) {
-    const Quad q = make_rule(rule);
+                 int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points) {
+    Quad q = make_rule(rule);
+    if (variant == 1 || (variant == 2 && kind == 1)) add_line_rule(q, line_points);
     const size_t N = (kind == 0) ? ne : (kind == 1 ? 2 * (size_t)ne : 4 * (size_t)ne);
     std::memset(Z, 0, sizeof(double) * 2 * N * N);
     if (threads > 0) omp_set_num_threads(threads);
@@ -642,5 +679,12 @@ double ref_lu_solve(int n, const double* A, const double* b, double* x, int nrhs
 }
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
+
+// The reference's Gauss-Legendre rule on [0, 1] (gauss_legendre_rule.cpp), doubles.
+int ref_gauss_legendre(int n, double* t, double* w) {
+    if (n < 1 || n > gauss_legendre_max_points()) return -1;
+    gauss_legendre_rule(n, t, w);
+    return n;
+}
 
 }  // extern "C"

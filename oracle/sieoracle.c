@@ -73,6 +73,20 @@ int so_rule(int rule, float* pts, float* w) {
     return o;
 }
 
+/* Gauss-Legendre rules on [0, 1] (src/sie_mom/quadrature/gauss_legendre_rule.cpp),
+ * rounded to float as the solvers upload them (pec_solver.cu:67-75). */
+#include "../sie-gstc-2026_b200/csrc/gauss_legendre_table.inc"
+
+int so_gauss_legendre(int n, float* t, float* w) {
+    if (n < 1 || n > 20) return -1;
+    const int off = n * (n - 1) / 2;
+    for (int q = 0; q < n; ++q) {
+        if (t) t[q] = (float)kGaussLegendreNodes[off + q];
+        if (w) w[q] = (float)kGaussLegendreWeights[off + q];
+    }
+    return n;
+}
+
 /* ---------------------------------------------------------------- mesh --- */
 /* src/sie_mom/mesh/obj_mesh_loader.cpp:360-386: edges numbered by first
  * appearance over (face, local edge (le, le+1 mod 3)), key (min, max).
@@ -185,6 +199,44 @@ void so_wilton(const double* r, const double* tri, double* out) {
     out[0] = P.phi0; out[1] = P.phi1b.x; out[2] = P.phi1b.y; out[3] = P.phi1b.z;
     out[4] = P.phi2; out[5] = P.phi3b.x; out[6] = P.phi3b.y; out[7] = P.phi3b.z;
     out[8] = P.r_pi.x; out[9] = P.r_pi.y; out[10] = P.r_pi.z; out[11] = P.d;
+}
+
+/* semi_analytic_integrals.cuh:108-171 (calculate_phi_0, used on the testing
+ * edges of the line form): an edge whose end is within 1e-9 of the point is
+ * skipped, and on an edge's line (R0 < 1e-8) the end distances are
+ * regularised by 1e-8. */
+static double phi0_line(v3 r, const v3 tri[3]) {
+    v3 n = vnorm(vcross(vsub(tri[1], tri[0]), vsub(tri[2], tri[0])));
+    const double d = vdot(vsub(r, tri[0]), n);
+    const v3 r_pi = vsub(r, vscale(n, d));
+    const double ad = fabs(d);
+    double phi0 = 0.0;
+    for (int e = 0; e < 3; ++e) {
+        v3 vs = tri[e], ve = tri[(e + 1) % 3];
+        v3 th = vnorm(vsub(ve, vs));
+        v3 u = vcross(th, n);
+        v3 rs = vsub(vs, vscale(n, vdot(n, vs)));
+        v3 re = vsub(ve, vscale(n, vdot(n, ve)));
+        v3 to_s = vsub(rs, r_pi);
+        double p0 = fabs(vdot(to_s, u));
+        double orient = vdot(to_s, u) >= 0.0 ? 1.0 : -1.0;
+        double lp = vdot(vsub(re, r_pi), th);
+        double lm = vdot(vsub(rs, r_pi), th);
+        double Pp = hypot(p0, lp), Pm = hypot(p0, lm);
+        double R0 = hypot(p0, ad);
+        double Rp = hypot(Pp, ad), Rm = hypot(Pm, ad);
+        if (Rp < 1e-9 || Rm < 1e-9) continue;
+        if (R0 < 1e-8) {
+            Rp = sqrt(Rp * Rp + 1e-8 * 1e-8);
+            Rm = sqrt(Rm * Rm + 1e-8 * 1e-8);
+        }
+        double logt = (log(Rp) + log1p(lp / Rp)) - (log(Rm) + log1p(lm / Rm));
+        double at = 0.0;
+        if (ad > 1e-9)
+            at = atan2(p0 * lp, R0 * R0 + ad * Rp) - atan2(p0 * lm, R0 * R0 + ad * Rm);
+        phi0 += orient * (p0 * logt - ad * at);
+    }
+    return phi0;
 }
 
 /* semi_analytic_integrals.cuh:422-427. */
@@ -466,19 +518,170 @@ static void singular_quad_n(const tri_t* T, const tri_t* S, const float* pts, co
         }
 }
 
-/* dielectric_kernels.cu:155-270 and pec_solver.cu:113-168: the same centroid
- * test as pair(), form B quadratures. */
+/* Line rule of the nTL form A (Gauss-Legendre on [0, 1], float-rounded); n = 0
+ * selects the surface form B. */
+typedef struct { const float* t; const float* w; int n; } line_t;
+
+/* dunavant_quadrature.cuh:492-692 (form A): nTL = 1/4 (tau . rho) G on both
+ * areas plus, for every source basis, the testing-edge line integral
+ * (L_e / 2A_m) (tau . nu_e) G / k^2 against the source area; nTK as in form B.
+ * n_m is the cross product divided by its length. */
+static void double_quad_a(const tri_t* T, const tri_t* S, const float* pts, const float* wts, int Q,
+                          const line_t* L, double k1, double k2, int regular, blocks_t* B) {
+    memset(B, 0, sizeof(*B));
+    const double k[2] = {k1, k2};
+    const int coinc = same_face(T, S);
+    const v3 cr = vcross(vsub(T->v[1], T->v[0]), vsub(T->v[2], T->v[0]));
+    const double twoA = vlen(cr);
+    const v3 nm = V3(cr.x / twoA, cr.y / twoA, cr.z / twoA);
+    for (int p = 0; p < Q; ++p) {
+        v3 rp = map_point(T, (double)pts[2 * p], (double)pts[2 * p + 1]);
+        double wp = (double)wts[p];
+        for (int q = 0; q < Q; ++q) {
+            v3 rq = map_point(S, (double)pts[2 * q], (double)pts[2 * q + 1]);
+            double wq = (double)wts[q];
+            kern_t K;
+            kernels(rp, rq, k, regular, &K);
+            const double aw = wp * wq, vw = 0.25 * aw;
+            for (int j = 0; j < 3; ++j) {
+                v3 tau = vcross(vsub(rp, T->free_v[j]), nm);
+                for (int i = 0; i < 3; ++i) {
+                    v3 rn = vsub(rq, S->free_v[i]);
+                    const double f = vw * vdot(tau, rn);
+                    B->tl1[j][i] = cadd(B->tl1[j][i], cscale(K.tl[0], f));
+                    B->tl2[j][i] = cadd(B->tl2[j][i], cscale(K.tl[1], f));
+                    if (!coinc) {
+                        v3 km = vscale(vcross(tau, rn), 0.25);
+                        B->tk1[j][i] = cadd(B->tk1[j][i], cscale(vdot_c(km, K.tk[0]), aw));
+                        B->tk2[j][i] = cadd(B->tk2[j][i], cscale(vdot_c(km, K.tk[1]), aw));
+                    }
+                }
+            }
+        }
+    }
+    for (int e = 0; e < 3; ++e) {
+        const v3 vA = T->v[e], vB = T->v[(e + 1) % 3];
+        const v3 E = vsub(vB, vA);
+        const double Le = vlen(E);
+        const v3 c = vcross(E, nm);
+        const v3 nu = V3(c.x / Le, c.y / Le, c.z / Le);
+        const double geom = Le / twoA;
+        for (int q = 0; q < L->n; ++q) {
+            const double t = (double)L->t[q], wl = (double)L->w[q];
+            const v3 req = V3(vA.x + t * (vB.x - vA.x), vA.y + t * (vB.y - vA.y), vA.z + t * (vB.z - vA.z));
+            for (int p = 0; p < Q; ++p) {
+                v3 rnp = map_point(S, (double)pts[2 * p], (double)pts[2 * p + 1]);
+                kern_t K;
+                kernels(req, rnp, k, regular, &K);
+                const double cw = wl * (double)wts[p];
+                for (int j = 0; j < 3; ++j) {
+                    v3 tau = vcross(vsub(req, T->free_v[j]), nm);
+                    const double ff = geom * vdot(tau, nu);
+                    const cx n1 = cscale(cscale(K.tl[0], ff / (k1 * k1)), cw);
+                    const cx n2 = cscale(cscale(K.tl[1], ff / (k2 * k2)), cw);
+                    for (int i = 0; i < 3; ++i) {
+                        B->tl1[j][i] = cadd(B->tl1[j][i], n1);
+                        B->tl2[j][i] = cadd(B->tl2[j][i], n2);
+                    }
+                }
+            }
+        }
+    }
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            double s = T->len[j] * S->len[i];
+            B->tl1[j][i] = cscale(B->tl1[j][i], s);
+            B->tl2[j][i] = cscale(B->tl2[j][i], s);
+            B->tk1[j][i] = cscale(B->tk1[j][i], s);
+            B->tk2[j][i] = cscale(B->tk2[j][i], s);
+        }
+}
+
+/* dunavant_quadrature.cuh:1040-1179 (singular part of form A): area nTL
+ * 1/4 w tau . Psi_1 (no gradient), nTK 1/4 w tau . Upsilon_coul (not on the
+ * coincident face), both scaled by e_mj e_ni / (4 pi A_n); the line part
+ * sum_e sum_q L_e w_q (tau . nu_e) phi_0(r_eq) scaled by
+ * e_mj e_ni / (8 pi A_m A_n k^2). */
+static void singular_quad_a(const tri_t* T, const tri_t* S, const float* pts, const float* wts, int Q,
+                            const line_t* L, double k1, double k2, blocks_t* B) {
+    memset(B, 0, sizeof(*B));
+    const v3 cr = vcross(vsub(T->v[1], T->v[0]), vsub(T->v[2], T->v[0]));
+    const double twoA = vlen(cr);
+    const double Am = 0.5 * twoA;
+    const v3 nm = V3(cr.x / twoA, cr.y / twoA, cr.z / twoA);
+    const double An = 0.5 * vlen(vcross(vsub(S->v[1], S->v[0]), vsub(S->v[2], S->v[0])));
+    const int coinc = same_face(T, S);
+    for (int p = 0; p < Q; ++p) {
+        v3 rp = map_point(T, (double)pts[2 * p], (double)pts[2 * p + 1]);
+        const double wp = (double)wts[p];
+        pots_t P = wilton(rp, S->v);
+        for (int j = 0; j < 3; ++j) {
+            v3 tau = vcross(vsub(rp, T->free_v[j]), nm);
+            for (int i = 0; i < 3; ++i) {
+                const double an = 0.25 * wp * vdot(tau, psi1(&P, S->free_v[i]));
+                B->tl1[j][i].re += an;
+                B->tl2[j][i].re += an;
+                if (!coinc) {
+                    v3 u1 = upsilon(&P, S->free_v[i], rp, (float)k1);
+                    v3 u2 = upsilon(&P, S->free_v[i], rp, (float)k2);
+                    B->tk1[j][i].re += 0.25 * wp * vdot(tau, u1);
+                    B->tk2[j][i].re += 0.25 * wp * vdot(tau, u2);
+                }
+            }
+        }
+    }
+    double line[3] = {0.0, 0.0, 0.0};
+    for (int e = 0; e < 3; ++e) {
+        const v3 vA = T->v[e], vB = T->v[(e + 1) % 3];
+        const v3 E = vsub(vB, vA);
+        const double Le = vlen(E);
+        const v3 c = vcross(E, nm);
+        const v3 nu = V3(c.x / Le, c.y / Le, c.z / Le);
+        for (int q = 0; q < L->n; ++q) {
+            const double t = (double)L->t[q], wl = (double)L->w[q];
+            const v3 req = V3(vA.x + t * (vB.x - vA.x), vA.y + t * (vB.y - vA.y), vA.z + t * (vB.z - vA.z));
+            const double ph0 = phi0_line(req, S->v);
+            for (int j = 0; j < 3; ++j) {
+                v3 tau = vcross(vsub(req, T->free_v[j]), nm);
+                line[j] += Le * wl * vdot(tau, nu) * ph0;
+            }
+        }
+    }
+    const double as = 1.0 / (4.0 * M_PI * An);
+    const double ls = 1.0 / (8.0 * M_PI * Am * An);
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+            const double edges = T->len[j] * S->len[i];
+            const double l1 = edges * ls * line[j] / (k1 * k1);
+            const double l2 = edges * ls * line[j] / (k2 * k2);
+            B->tl1[j][i] = cadd(cscale(B->tl1[j][i], edges * as), CX(l1, 0.0));
+            B->tl2[j][i] = cadd(cscale(B->tl2[j][i], edges * as), CX(l2, 0.0));
+            B->tk1[j][i] = cscale(B->tk1[j][i], edges * as);
+            B->tk2[j][i] = cscale(B->tk2[j][i], edges * as);
+        }
+}
+
+/* dielectric_kernels.cu:155-270 and pec_solver.cu:113-168: rotated-testing
+ * pair, form B (L->n == 0) or form A. Extraction below the threshold: the
+ * dielectric kernels compare the float-rounded centroid distance, the PEC
+ * kernels (exact != 0) the double one. */
 static void pair_n(const tri_t* T, const tri_t* S, const float* pts, const float* wts, int Q,
-                   float k1, float k2, float thr, blocks_t* B) {
+                   const line_t* L, float k1, float k2, float thr, int exact, blocks_t* B) {
     v3 tc = vadd(vadd(T->v[0], T->v[1]), T->v[2]);
     v3 sc = vadd(vadd(S->v[0], S->v[1]), S->v[2]);
     tc = V3(tc.x / 3.0, tc.y / 3.0, tc.z / 3.0);
     sc = V3(sc.x / 3.0, sc.y / 3.0, sc.z / 3.0);
-    float dist = (float)vlen(vsub(tc, sc));
-    if (dist < thr) {
-        blocks_t Sg;
-        double_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, 1, B);
-        singular_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, &Sg);
+    const double dd = vlen(vsub(tc, sc));
+    const int near = exact ? (dd < (double)thr) : ((float)dd < thr);
+    blocks_t Sg;
+    if (L->n > 0) {
+        double_quad_a(T, S, pts, wts, Q, L, (double)k1, (double)k2, near, B);
+        if (near) singular_quad_a(T, S, pts, wts, Q, L, (double)k1, (double)k2, &Sg);
+    } else {
+        double_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, near, B);
+        if (near) singular_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, &Sg);
+    }
+    if (near)
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) {
                 B->tl1[j][i] = cadd(B->tl1[j][i], Sg.tl1[j][i]);
@@ -486,21 +689,19 @@ static void pair_n(const tri_t* T, const tri_t* S, const float* pts, const float
                 B->tk1[j][i] = cadd(B->tk1[j][i], Sg.tk1[j][i]);
                 B->tk2[j][i] = cadd(B->tk2[j][i], Sg.tk2[j][i]);
             }
-    } else {
-        double_quad_n(T, S, pts, wts, Q, (double)k1, (double)k2, 0, B);
-    }
 }
 
 static void pair_blocks_out(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
-                            float thr, int rotated, double* out) {
-    float pts[2 * 80], wts[80];
+                            float thr, int rotated, int line_points, double* out) {
+    float pts[2 * 80], wts[80], lt[20], lw[20];
     int Q = so_rule(rule, pts, wts);
+    line_t L = {lt, lw, line_points > 0 ? so_gauss_legendre(line_points, lt, lw) : 0};
     tri_t T, S;
     load_tri(V, F, m, &T);
     load_tri(V, F, n, &S);
     blocks_t B;
     if (rotated)
-        pair_n(&T, &S, pts, wts, Q, k1, k2, thr, &B);
+        pair_n(&T, &S, pts, wts, Q, &L, k1, k2, thr, 0, &B);
     else
         pair(&T, &S, pts, wts, Q, k1, k2, thr, &B);
     cx(*blk[4])[3] = {B.tl1, B.tl2, B.tk1, B.tk2};
@@ -514,13 +715,14 @@ static void pair_blocks_out(const double* V, const int* F, int m, int n, int rul
 
 void so_pair_blocks(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
                     float thr, double* out) {
-    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 0, out);
+    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 0, 0, out);
 }
 
-/* nTL1, nTL2, nTK1, nTK2 of face pair (m, n), surface form B. */
+/* nTL1, nTL2, nTK1, nTK2 of face pair (m, n): surface form B (line_points 0)
+ * or line form A with that many Gauss-Legendre points. */
 void so_pair_blocks_n(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
-                      float thr, double* out) {
-    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 1, out);
+                      float thr, int line_points, double* out) {
+    pair_blocks_out(V, F, m, n, rule, k1, k2, thr, 1, line_points, out);
 }
 
 /* ------------------------------------------------------- GSTC frames ---- */
@@ -658,11 +860,17 @@ static inline void zadd(double* Z, size_t N, size_t r, size_t c, cx v) {
 int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
                 float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                 float mu0, float eps0, float omega, float thr, const double* tensors,
-                int tensors_uniform, int basis, double* Z, int threads, int variant) {
+                int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points) {
     (void)threads;
     float pts[2 * 80], wts[80];
     const int Q = so_rule(rule, pts, wts);
     if (Q < 0) return -1;
+    float lt[20], lw[20];
+    /* N-MFIE evaluates no line integral (pec_solver.cu:215-218). */
+    const int NG = (variant == 1 || (variant == 2 && kind == 1)) && line_points > 0
+                       ? so_gauss_legendre(line_points, lt, lw) : 0;
+    if (NG < 0) return -1;
+    const line_t L = {lt, lw, NG};
     const size_t E = (size_t)ne;
     const size_t N = kind == 0 ? E : (kind == 1 ? 2 * E : 4 * E);
     memset(Z, 0, sizeof(double) * 2 * N * N);
@@ -673,7 +881,7 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
         for (int n = 0; n < nf; ++n) {
             blocks_t B;
             if (variant != 0)
-                pair_n(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
+                pair_n(&tris[m], &tris[n], pts, wts, Q, &L, k1, k2, thr, kind == 0, &B);
             else
                 pair(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
             const int* te = &FE[3 * m];

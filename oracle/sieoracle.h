@@ -14,11 +14,12 @@ void so_wilton(const double* r, const double* tri, double* out);
 void so_pair_blocks(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
                     float thr, double* out);
 void so_pair_blocks_n(const double* V, const int* F, int m, int n, int rule, float k1, float k2,
-                      float thr, double* out);
+                      float thr, int line_points, double* out);
+int so_gauss_legendre(int n, float* t, float* w);
 int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
                 float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                 float mu0, float eps0, float omega, float thr, const double* tensors,
-                int tensors_uniform, int basis, double* Z, int threads, int variant);
+                int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points);
 int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* FE, int nf, int ne,
            int rule, const double* a, const double* b, int is_magnetic, double k, double eta,
            int region, double mu0, double eps0, double* rhs, int variant, double eps_r_src,

@@ -42,6 +42,8 @@ struct Rule {
 const Rule kRules[20] = {
 #include "dunavant_table.inc"
 };
+// Gauss-Legendre rules 1-20 on [0, 1]; see gen_gauss_legendre_table.py.
+#include "gauss_legendre_table.inc"
 
 using Clock = std::chrono::steady_clock;
 double seconds_since(Clock::time_point t0) {
@@ -130,6 +132,19 @@ void DeviceBuffer::release() {
     bytes = 0;
 }
 
+// Gauss-Legendre rule with n points on [0, 1], nodes ascending, rounded to
+// float as the solvers upload it (pec_solver.cu:67-75,
+// dielectric/dielectric_solver.cu:179-197). Returns n, or -1.
+int gauss_legendre_rule_f(int n, float* t, float* w) {
+    if (n < 1 || n > 20) return -1;
+    const int off = n * (n - 1) / 2;
+    for (int q = 0; q < n; ++q) {
+        t[q] = (float)kGaussLegendreNodes[off + q];
+        w[q] = (float)kGaussLegendreWeights[off + q];
+    }
+    return n;
+}
+
 // Expansion order of src/sie_mom/quadrature/triangle_dunavant_rule.cpp:135-256
 // (orbit by orbit: 1-orbits once; 3-orbits as (a,b),(b,c),(c,a); 6-orbits
 // additionally the swapped pairs), rounded to float as
@@ -170,6 +185,11 @@ int make_assembly_params(const sieb200_options& o, AssemblyParams* ap) {
     ap->formulation = o.formulation;
     ap->basis = o.basis;
     ap->variant = o.variant;
+    // The line form A integrates nTL along the testing edges for N-EFIE,
+    // N-PMCHWT and N-Muller; N-MFIE has no nTL (pec_solver.cu:215-218).
+    const bool line_integrated = o.formulation == SIEB200_PEC_EFIE ? o.variant == SIEB200_VARIANT_N
+                                                                  : o.variant != SIEB200_VARIANT_T;
+    ap->line_points = (o.ntl_form == SIEB200_NTL_LINE && line_integrated) ? o.line_quadrature_points : 0;
     if (o.formulation == SIEB200_PEC_EFIE) {
         const double lambda0 = 2.0 * pi / (omega * std::sqrt(o.vacuum_permeability * o.vacuum_permittivity));
         ap->threshold = (float)(o.singularity_threshold_lambda0 * lambda0);
@@ -260,15 +280,16 @@ int validate(const sieb200_mesh* mesh, const sieb200_options* o, const double* t
     SIEB_CHECK(o->ntl_form == SIEB200_NTL_SURFACE || o->ntl_form == SIEB200_NTL_LINE, SIEB200_INVALID_ARG,
                "unknown nTL integral form");
     if (o->ntl_form == SIEB200_NTL_LINE) {
-        // pec_solver.cu:96-97 and dielectric_solver.cu:123-125 reject the line
-        // form where no nTL is line-integrated; where it would be, form A is
-        // not part of this library.
+        // pec_solver.cu:91-97 and dielectric_solver.cu:116-125: the line form
+        // needs a line-integrated nTL and a 1-20 point Gauss-Legendre rule.
         SIEB_CHECK(o->formulation != SIEB200_PEC_EFIE || o->variant == SIEB200_VARIANT_N, SIEB200_INVALID_ARG,
                    "line nTL form requires N-EFIE");
         SIEB_CHECK(o->formulation != SIEB200_PMCHWT || o->variant != SIEB200_VARIANT_T, SIEB200_INVALID_ARG,
                    "line nTL form requires N-PMCHWT or N-Muller formulation");
-        set_error("the line (form A) nTL integral is not built; use the surface form");
-        return SIEB200_UNSUPPORTED;
+        SIEB_CHECK(o->formulation != SIEB200_GSTC, SIEB200_INVALID_ARG,
+                   "the SIE-GSTC formulation has no nTL line form");
+        SIEB_CHECK(o->line_quadrature_points >= 1 && o->line_quadrature_points <= 20, SIEB200_INVALID_ARG,
+                   "Gauss-Legendre point count must be in [1, 20]");
     }
     const int64_t N = system_dimension(o->formulation, mesh->num_edges);
     SIEB_CHECK(N <= std::numeric_limits<int>::max(), SIEB200_OVERFLOW,
@@ -540,6 +561,7 @@ int sieb200_options_default(int formulation, sieb200_options* o) {
     o->tolerance = 1e-10;
     o->max_iterations = 50;
     o->restart = 30;
+    o->line_quadrature_points = 20;
     o->solver = SIEB200_SOLVER_LU_CUSOLVER;
     if (formulation == SIEB200_GSTC) {
         o->quadrature_rule = 17;

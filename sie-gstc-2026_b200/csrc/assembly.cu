@@ -57,6 +57,7 @@ namespace {
 
 constexpr int kMaxQ = 80;      // Dunavant rule 20 has 79 points
 constexpr int kWarps = 8;      // warps per CTA in pair_regular
+constexpr int kMaxLine = 20;   // Gauss-Legendre points of the nTL line form
 constexpr double kPi = 3.14159265358979323846;
 
 struct FaceGeom {
@@ -503,11 +504,64 @@ __device__ __forceinline__ d3 face_normal(const FaceGeom& g) {
     return normalize3(cross3(g.v[1] - g.v[0], g.v[2] - g.v[0]));
 }
 
+// The line form's unit normal: cross product divided by its length
+// (dunavant_quadrature.cuh:521-525), and twice the area.
+__device__ __forceinline__ d3 face_normal_div(const FaceGeom& g) {
+    const d3 c = cross3(g.v[1] - g.v[0], g.v[2] - g.v[0]);
+    const double l = sqrt(dot3(c, c));
+    return mk3(c.x / l, c.y / l, c.z / l);
+}
+
+// semi_analytic_integrals.cuh:108-171 (calculate_phi_0, on the testing edges
+// of the line form): an edge whose end is within 1e-9 of r is skipped, and on
+// an edge's line (R0 < 1e-8) the end distances are regularised by 1e-8.
+__device__ double phi0_line(const d3 r, const d3 tri[3]) {
+    const d3 n = normalize3(cross3(tri[1] - tri[0], tri[2] - tri[0]));
+    const double d = dot3(r - tri[0], n);
+    const d3 r_pi = r - n * d;
+    const double ad = fabs(d);
+    double phi0 = 0.0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const d3 vs = tri[e], ve = tri[(e + 1) % 3];
+        const d3 th = normalize3(ve - vs);
+        const d3 u = cross3(th, n);
+        const d3 rs = vs - n * dot3(n, vs);
+        const d3 re = ve - n * dot3(n, ve);
+        const double su = dot3(rs - r_pi, u);
+        const double p0 = fabs(su);
+        const double orient = su >= 0.0 ? 1.0 : -1.0;
+        const double lp = dot3(re - r_pi, th);
+        const double lm = dot3(rs - r_pi, th);
+        const double Pp = hypot(p0, lp), Pm = hypot(p0, lm);
+        const double R0 = hypot(p0, ad);
+        double Rp = hypot(Pp, ad), Rm = hypot(Pm, ad);
+        if (Rp < 1e-9 || Rm < 1e-9) continue;
+        if (R0 < 1e-8) {
+            // Rounded product, then rounded sum, as the reference's
+            // sqrt(pow(R, 2) + pow(eps, 2)): where 1e-16 is below half an ulp
+            // of R^2 the regularisation has no effect and, on the edge line
+            // beyond its start, log1p(-1) makes the reference's value
+            // infinite; the same inputs give the same values here.
+            Rp = sqrt(__dadd_rn(__dmul_rn(Rp, Rp), 1e-8 * 1e-8));
+            Rm = sqrt(__dadd_rn(__dmul_rn(Rm, Rm), 1e-8 * 1e-8));
+        }
+        const double logt = (log(Rp) + log1p(lp / Rp)) - (log(Rm) + log1p(lm / Rm));
+        double at = 0.0;
+        if (ad > 1e-9) at = atan2(p0 * lp, R0 * R0 + ad * Rp) - atan2(p0 * lm, R0 * R0 + ad * Rm);
+        phi0 += orient * (p0 * logt - ad * at);
+    }
+    return phi0;
+}
+
 // Regular (or extracted-kernel) double quadrature of the rotated-testing
 // blocks of all face pairs (m, n), m in [m0, m1). Output per pair: nTL for
 // each wavenumber, then (NTK) nTK for each, 3x3 complex each, in the slots
 // pair_regular_kernel gives TL and TK.
-template <int NK, bool NTK>
+// FORM_A: the area part of the line form A (dunavant_quadrature.cuh:492-567):
+// nTL without the gradient term (pair_line_kernel adds the testing-edge line
+// integral), n_m as the cross product divided by its length.
+template <int NK, bool NTK, bool FORM_A>
 __global__ void __launch_bounds__(kWarps * 32, 1)
 pair_regular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
                       const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
@@ -520,7 +574,7 @@ pair_regular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ 
     const int m = m0 + blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const FaceGeom& gm = geom[m];
-    const d3 nm = face_normal(gm);
+    const d3 nm = FORM_A ? face_normal_div(gm) : face_normal(gm);
     for (int t = threadIdx.x; t < Q; t += blockDim.x) {
         const d3 r = qp[(size_t)m * Q + t];
         s_tp[t] = r;
@@ -618,8 +672,12 @@ pair_regular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ 
                 s = s - (M.St[a][0] * B.x + M.St[a][1] * B.y + M.St[a][2] * B.z);
                 s = s - (M.Sq[a][0] * tj.x + M.Sq[a][1] * tj.y + M.Sq[a][2] * tj.z);
                 s += M.S0[a] * tjB;
-                const cplx t = M.TtR[a] - (M.TR[a][0] * tj.x + M.TR[a][1] * tj.y + M.TR[a][2] * tj.z);
-                out[a * 9 + lane] = (s * 0.25 + t * (-0.5 / (kk[a] * kk[a]))) * scale;
+                if (FORM_A) {
+                    out[a * 9 + lane] = s * (0.25 * scale);
+                } else {
+                    const cplx t = M.TtR[a] - (M.TR[a][0] * tj.x + M.TR[a][1] * tj.y + M.TR[a][2] * tj.z);
+                    out[a * 9 + lane] = (s * 0.25 + t * (-0.5 / (kk[a] * kk[a]))) * scale;
+                }
                 if (NTK) {
                     cplx u = cx(0, 0);
                     if (!coinc) {
@@ -637,19 +695,23 @@ pair_regular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ 
     }
 }
 
-// Singular (extracted) part of the rotated-testing blocks of the near pairs
-// (dunavant_quadrature.cuh:889-1040), added to the pair blocks. Per outer
-// point, with phi_1 = phi_1b - d phi_0 n_n and the extracted gradient
-// phi_3b - d phi_2 n_n:
+// Singular (extracted) part of the rotated-testing blocks of the near pairs,
+// added to the pair blocks. One warp per pair, lanes over outer points.
+// Surface form B (dunavant_quadrature.cuh:889-1040), per outer point with
+// phi_1 = phi_1b - d phi_0 n_n and the extracted gradient phi_3b - d phi_2 n_n:
 //   nTL += 1/2 tau . (phi_1 + 1/2 R_i phi_0 + gradient / k^2)
 //          (the gradient left out on the coincident face),
-//   nTK += 1/4 tau . Upsilon_coul (not on the coincident face),
-// then e_mj e_ni / (4 pi A_n). One warp per pair, lanes over outer points.
-template <int NK>
+// then e_mj e_ni / (4 pi A_n). Line form A (1040-1179): nTL += 1/4 w tau . Psi_1
+// on the area, scaled alike, plus the testing-edge sum
+// sum_e sum_q L_e w_q (tau . nu_e) phi_0(r_eq) scaled by e_mj e_ni / (8 pi A_m A_n k^2)
+// (lanes over the 3 NG edge points). Both forms:
+//   nTK += 1/4 tau . Upsilon_coul (not on the coincident face).
+template <int NK, bool FORM_A>
 __global__ void pair_singular_n_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
                                        const float* __restrict__ qw_g, int Q, int nf, int m0,
                                        const int2* __restrict__ list, int count, double k0,
-                                       double k1, bool with_ntk, cplx* __restrict__ pairs) {
+                                       double k1, bool with_ntk, const float* __restrict__ gl_t,
+                                       const float* __restrict__ gl_w, int NG, cplx* __restrict__ pairs) {
     const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp_global >= count) return;
@@ -657,7 +719,8 @@ __global__ void pair_singular_n_kernel(const FaceGeom* __restrict__ geom, const 
     const FaceGeom gm = geom[mn.x];
     const FaceGeom gn = geom[mn.y];
     const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] && gm.idx[2] == gn.idx[2];
-    const d3 nm = face_normal(gm), nn = face_normal(gn);
+    const d3 nm = FORM_A ? face_normal_div(gm) : face_normal(gm);
+    const d3 nn = face_normal(gn);
     const double kk[2] = {k0, k1};
     double tl[NK][9], tk[NK][9];
 #pragma unroll
@@ -676,18 +739,45 @@ __global__ void pair_singular_n_kernel(const FaceGeom* __restrict__ geom, const 
             const d3 tau = cross3(rp - gm.fv[j], nm);
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const d3 br = phi1 + ((rp - gn.fv[i]) * 0.5) * P.phi0;
+                if (FORM_A) {
+                    const double an = 0.25 * wp * dot3(tau, psi1(P, gn.fv[i]));
 #pragma unroll
-                for (int a = 0; a < NK; ++a) {
-                    const d3 V = coinc ? br : br + grad * (1.0 / (kk[a] * kk[a]));
-                    tl[a][j * 3 + i] += 0.5 * dot3(tau, V) * wp;
-                    if (with_ntk && !coinc) {
+                    for (int a = 0; a < NK; ++a) tl[a][j * 3 + i] += an;
+                } else {
+                    const d3 br = phi1 + ((rp - gn.fv[i]) * 0.5) * P.phi0;
+#pragma unroll
+                    for (int a = 0; a < NK; ++a) {
+                        const d3 V = coinc ? br : br + grad * (1.0 / (kk[a] * kk[a]));
+                        tl[a][j * 3 + i] += 0.5 * dot3(tau, V) * wp;
+                    }
+                }
+                if (with_ntk && !coinc) {
+#pragma unroll
+                    for (int a = 0; a < NK; ++a) {
                         const d3 up = upsilon(P, gn.fv[i], rp, (float)kk[a]);
-                        tk[a][j * 3 + i] += 0.25 * dot3(tau, up) * wp;
+                        tk[a][j * 3 + i] += (FORM_A ? 0.25 * wp * dot3(tau, up) : 0.25 * dot3(tau, up) * wp);
                     }
                 }
             }
         }
+    }
+    double line[3] = {0.0, 0.0, 0.0};
+    if (FORM_A) {
+        for (int it = lane; it < 3 * NG; it += 32) {
+            const int e = it / NG, q = it - e * NG;
+            const d3 vA = gm.v[e], vB = gm.v[e == 2 ? 0 : e + 1];
+            const d3 E = vB - vA;
+            const double Le = sqrt(dot3(E, E));
+            const d3 c = cross3(E, nm);
+            const d3 nu = mk3(c.x / Le, c.y / Le, c.z / Le);
+            const double t = (double)gl_t[q], wl = (double)gl_w[q];
+            const d3 req = mk3(vA.x + t * (vB.x - vA.x), vA.y + t * (vB.y - vA.y), vA.z + t * (vB.z - vA.z));
+            const double ph0 = phi0_line(req, gn.v);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) line[j] += Le * wl * dot3(cross3(req - gm.fv[j], nm), nu) * ph0;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) warp_sum(line[j]);
     }
 #pragma unroll
     for (int a = 0; a < NK; ++a)
@@ -699,15 +789,118 @@ __global__ void pair_singular_n_kernel(const FaceGeom* __restrict__ geom, const 
         const double s = as * gm.len[j] * gn.len[i];
         const int NB = with_ntk ? 2 * NK : NK;
         cplx* out = pairs + ((size_t)(mn.x - m0) * nf + mn.y) * (NB * 9);
+        const double edges = gm.len[j] * gn.len[i];
+        const double ls = FORM_A ? 1.0 / (8.0 * kPi * gm.area * gn.area) : 0.0;
+        double lj = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+            if (jj == j) lj = line[jj];
 #pragma unroll
         for (int a = 0; a < NK; ++a) {
             double tlv = 0.0, tkv = 0.0;
 #pragma unroll
             for (int t = 0; t < 9; ++t)
                 if (t == lane) { tlv = tl[a][t]; tkv = tk[a][t]; }
-            out[a * 9 + lane].re += tlv * s;
-            if (with_ntk) out[(NK + a) * 9 + lane].re += tkv * s;
+            if (FORM_A) {
+                out[a * 9 + lane].re += tlv * (edges * as) + edges * ls * lj / (kk[a] * kk[a]);
+                if (with_ntk) out[(NK + a) * 9 + lane].re += tkv * (edges * as);
+            } else {
+                out[a * 9 + lane].re += tlv * s;
+                if (with_ntk) out[(NK + a) * 9 + lane].re += tkv * s;
+            }
         }
+    }
+}
+
+// Testing-edge line integral of the nTL form A (dunavant_quadrature.cuh:598-672),
+// added to the nTL blocks of every face pair of the slab: for each test edge
+// e (v_A -> v_B), Gauss-Legendre point t_q and source point p,
+//   nTL_ji += l_j l_i (L_e / 2A_m) (tau_j(r_eq) . nu_e) G(r_eq, r_p) w_q w_p / k^2,
+// the same for every source basis i. tau_j . nu_e is linear in t_q, so each
+// warp (one face pair) accumulates sum w G and sum w t G per edge and
+// wavenumber; 9 lanes expand them. Standard or extracted kernel as the pair's
+// area quadrature.
+template <int NK>
+__global__ void __launch_bounds__(kWarps * 32)
+pair_line_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                 const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
+                 float thr, int exact, const float* __restrict__ gl_t, const float* __restrict__ gl_w,
+                 int NG, int NB, cplx* __restrict__ pairs) {
+    __shared__ double s_w[kMaxQ];
+    __shared__ double s_t[20], s_wl[20];
+    const int m = m0 + blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t < Q; t += blockDim.x) s_w[t] = (double)qw_g[t];
+    for (int t = threadIdx.x; t < NG; t += blockDim.x) { s_t[t] = (double)gl_t[t]; s_wl[t] = (double)gl_w[t]; }
+    __syncthreads();
+    const FaceGeom& gm = geom[m];
+    const d3 nm = face_normal_div(gm);
+    const d3 cr = cross3(gm.v[1] - gm.v[0], gm.v[2] - gm.v[0]);
+    const double twoA = sqrt(dot3(cr, cr));
+    const double kk[2] = {k0, k1};
+    const int items = NG * Q;
+    for (int n = warp; n < nf; n += kWarps) {
+        const FaceGeom& gn = geom[n];
+        const bool regular = near_pair(gm, gn, thr, exact);  // warp-uniform
+        cplx M0[3][NK], M1[3][NK];
+#pragma unroll
+        for (int e = 0; e < 3; ++e)
+#pragma unroll
+            for (int a = 0; a < NK; ++a) { M0[e][a] = cx(0, 0); M1[e][a] = cx(0, 0); }
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const d3 vA = gm.v[e], vB = gm.v[e == 2 ? 0 : e + 1];
+            for (int it = lane; it < items; it += 32) {
+                const int q = it / Q, p = it - q * Q;
+                const double t = s_t[q];
+                const d3 req = mk3(vA.x + t * (vB.x - vA.x), vA.y + t * (vB.y - vA.y), vA.z + t * (vB.z - vA.z));
+                const d3 rq = ldg3(&qp[(size_t)n * Q + p]);
+                const d3 Rv = req - rq;
+                const double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+                if (!regular && R < 1e-12) continue;
+                const double w = s_wl[q] * s_w[p];
+                const double inv_R = regular ? 0.0 : 1.0 / R;
+                const double i4pR = regular ? 0.0 : 1.0 / (4.0 * kPi * R);
+#pragma unroll
+                for (int a = 0; a < NK; ++a) {
+                    cplx G, g;
+                    if (regular) green_reg(R, kk[a], G, g);
+                    else green_std(R, inv_R, i4pR, kk[a], G, g);
+                    const cplx Gw = G * w;
+                    M0[e][a] += Gw;
+                    M1[e][a] += Gw * t;
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 3; ++e)
+#pragma unroll
+            for (int a = 0; a < NK; ++a) { warp_sum(M0[e][a]); warp_sum(M1[e][a]); }
+        if (lane < 9) {
+            const int j = lane / 3, i = lane - 3 * j;
+            cplx acc[NK];
+#pragma unroll
+            for (int a = 0; a < NK; ++a) acc[a] = cx(0, 0);
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const d3 vA = gm.v[e], vB = gm.v[e == 2 ? 0 : e + 1];
+                const d3 E = vB - vA;
+                const double Le = sqrt(dot3(E, E));
+                const d3 c = cross3(E, nm);
+                const d3 nu = mk3(c.x / Le, c.y / Le, c.z / Le);
+                const double geomf = Le / twoA;
+                // tau_j(r_eq) . nu_e = c0 + t c1
+                const double c0 = dot3(cross3(vA - gm.fv[j], nm), nu);
+                const double c1 = dot3(cross3(E, nm), nu);
+#pragma unroll
+                for (int a = 0; a < NK; ++a) acc[a] += (M0[e][a] * c0 + M1[e][a] * c1) * geomf;
+            }
+            const double scale = gm.len[j] * gn.len[i];
+            cplx* out = pairs + ((size_t)blockIdx.x * nf + n) * (NB * 9);
+#pragma unroll
+            for (int a = 0; a < NK; ++a) out[a * 9 + lane] += acc[a] * (scale / (kk[a] * kk[a]));
+        }
+        __syncwarp();
     }
 }
 
@@ -1159,7 +1352,7 @@ static int prepare_faces(sieb200_ctx* ctx, const sieb200_mesh& mesh, const float
     SIEB_TRY_CUDA(cudaMemcpyAsync(dV, mesh.vertices, vbytes, cudaMemcpyHostToDevice, st));
     SIEB_TRY_CUDA(cudaMemcpyAsync(dF, mesh.faces, fbytes, cudaMemcpyHostToDevice, st));
     SIEB_TRY_CUDA(cudaMemcpyAsync(dFE, mesh.faces_edges, fbytes, cudaMemcpyHostToDevice, st));
-    SIEB_RETURN_IF(ctx->qw.reserve(sizeof(float) * 3 * kMaxQ));
+    SIEB_RETURN_IF(ctx->qw.reserve(sizeof(float) * (3 * kMaxQ + 2 * kMaxLine)));
     float* dpts = ctx->qw.as<float>();
     float* dw = dpts + 2 * kMaxQ;
     SIEB_TRY_CUDA(cudaMemcpyAsync(dpts, pts, sizeof(float) * 2 * Q, cudaMemcpyHostToDevice, st));
@@ -1237,6 +1430,17 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
     const int NK = ap.nk;
     const int NB = tk ? 2 * NK : NK;
     const int exact = (opt.formulation == SIEB200_PEC_EFIE && variant != 0) ? 1 : 0;
+    // Line form A of nTL (N-EFIE, N-PMCHWT, N-Muller): Gauss-Legendre rule on
+    // [0, 1] after the Dunavant rule in the rule buffer.
+    const int NG = ap.line_points;
+    const bool form_a = NG > 0;
+    float* dgl = ctx->qw.as<float>() + 3 * kMaxQ;
+    if (form_a) {
+        float glt[2 * kMaxLine];
+        SIEB_CHECK(NG <= kMaxLine && gauss_legendre_rule_f(NG, glt, glt + kMaxLine) == NG, SIEB200_INVALID_ARG,
+                   "Gauss-Legendre point count must be in [1, 20]");
+        SIEB_TRY_CUDA(cudaMemcpyAsync(dgl, glt, sizeof(glt), cudaMemcpyHostToDevice, st));
+    }
     const size_t pair_bytes = sizeof(cplx) * 9 * NB;
     size_t budget = (size_t)8 << 30;
     size_t free_b = 0, total_b = 0;
@@ -1269,14 +1473,20 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
     for (int m0 = 0; m0 < nf; m0 += slab) {
         const int m1 = std::min(nf, m0 + slab);
         const int rows = m1 - m0;
-        if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE && !tk)
-            pair_regular_n_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
+        if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE && !tk && form_a)
+            pair_regular_n_kernel<1, false, true><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, exact, pairs);
+        else if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE && !tk)
+            pair_regular_n_kernel<1, false, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, exact, pairs);
         else if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE)
-            pair_regular_n_kernel<1, true><<<rows, kWarps * 32, 0, st>>>(
+            pair_regular_n_kernel<1, true, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, exact, pairs);
+        else if (variant != 0 && form_a)
+            pair_regular_n_kernel<2, true, true><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, exact, pairs);
         else if (variant != 0)
-            pair_regular_n_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
+            pair_regular_n_kernel<2, true, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, exact, pairs);
         else if (opt.formulation == SIEB200_PEC_EFIE)
             pair_regular_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
@@ -1286,6 +1496,18 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
+        if (form_a) {
+            if (NK == 1)
+                pair_line_kernel<1><<<rows, kWarps * 32, 0, st>>>(geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1],
+                                                                  ap.threshold, exact, dgl, dgl + kMaxLine, NG,
+                                                                  NB, pairs);
+            else
+                pair_line_kernel<2><<<rows, kWarps * 32, 0, st>>>(geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1],
+                                                                  ap.threshold, exact, dgl, dgl + kMaxLine, NG,
+                                                                  NB, pairs);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
 
         // Near-pair list of this slab: count, size, fill.
         const long long span = (long long)rows * nf;
@@ -1306,14 +1528,22 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
             SIEB_TRY_CUDA(cudaGetLastError());
             const int threads = 128;
             const int blocks = (int)((count * 32 + threads - 1) / threads);
-            if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE)
-                pair_singular_n_kernel<1><<<blocks, threads, 0, st>>>(
+            if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE && form_a)
+                pair_singular_n_kernel<1, true><<<blocks, threads, 0, st>>>(
                     geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],
-                    ap.k[1], tk, pairs);
-            else if (variant != 0)
-                pair_singular_n_kernel<2><<<blocks, threads, 0, st>>>(
+                    ap.k[1], tk, dgl, dgl + kMaxLine, NG, pairs);
+            else if (variant != 0 && opt.formulation == SIEB200_PEC_EFIE)
+                pair_singular_n_kernel<1, false><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],
+                    ap.k[1], tk, dgl, dgl + kMaxLine, 0, pairs);
+            else if (variant != 0 && form_a)
+                pair_singular_n_kernel<2, true><<<blocks, threads, 0, st>>>(
                     geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[0],
-                    ap.k[1], true, pairs);
+                    ap.k[1], true, dgl, dgl + kMaxLine, NG, pairs);
+            else if (variant != 0)
+                pair_singular_n_kernel<2, false><<<blocks, threads, 0, st>>>(
+                    geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[0],
+                    ap.k[1], true, dgl, dgl + kMaxLine, 0, pairs);
             else if (opt.formulation == SIEB200_PEC_EFIE)
                 pair_singular_kernel<1><<<blocks, threads, 0, st>>>(
                     geom, qp, dw, Q, nf, m0, ctx->near_list.as<int2>(), (int)count, ap.k[1],

@@ -161,10 +161,13 @@ struct AssemblyParams {
     // eps_f/mu_f their float means; s_jm = eta0, s_mm = eta0^2 as for PMCHWT.
     double w_em[2] = {0, 0}, eps[2] = {0, 0}, mu[2] = {0, 0};
     double eps_f = 0, mu_f = 0;
+    // Gauss-Legendre points of the nTL line form A; 0 for the surface form B.
+    int line_points = 0;
 };
 
 int make_assembly_params(const sieb200_options& opt, AssemblyParams* out);
 int expand_rule(int rule, float* pts, float* w);  // returns Q or -1
+int gauss_legendre_rule_f(int n, float* t, float* w);  // returns n or -1
 
 // Assembly on the context stream into a device column-major N x N matrix.
 int assemble_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb200_options& opt,

@@ -57,7 +57,8 @@ class Options(ctypes.Structure):
                 ("basis", ctypes.c_int), ("tensors_are_uniform", ctypes.c_int),
                 ("compute_residual", ctypes.c_int), ("solver", ctypes.c_int),
                 ("tolerance", ctypes.c_double), ("max_iterations", ctypes.c_int),
-                ("restart", ctypes.c_int), ("variant", ctypes.c_int), ("ntl_form", ctypes.c_int)]
+                ("restart", ctypes.c_int), ("variant", ctypes.c_int), ("ntl_form", ctypes.c_int),
+                ("line_quadrature_points", ctypes.c_int)]
 
 
 class Source(ctypes.Structure):

@@ -156,6 +156,7 @@ def to_c_options(opt, formulation: int) -> _lib.Options:
             raise ValueError("ntl_form must be 'Surface' or 'Line'")
         o.variant = table[opt.formulation]
         o.ntl_form = NTL_FORMS[opt.ntl_form]
+        o.line_quadrature_points = int(opt.line_quadrature_points)
         line_integrated = (o.variant == _lib.VARIANT_N if formulation == _lib.PEC_EFIE
                            else o.variant != _lib.VARIANT_T)
         if o.ntl_form == _lib.NTL_LINE and line_integrated and \

@@ -1,6 +1,6 @@
 """Regenerate tests/golden/variants_golden.npz: the rotated-testing
-formulations (N-EFIE, N-MFIE, N-PMCHWT, N-Muller; surface nTL form) as the
-reference computes them.
+formulations (N-EFIE, N-MFIE, N-PMCHWT, N-Muller; surface nTL form B and line
+form A) as the reference computes them.
 
 Run in a checkout that has the reference sources and the harness built
 (make -C oracle):
@@ -8,7 +8,7 @@ Run in a checkout that has the reference sources and the harness built
 
 Source of truth: oracle/_ref/libsieref.so, the reference's own quadrature
 (calculateDoubleQuadrature_nTL_nTK, calculateSingularPartQuadrature_nTL_nTK,
-calculateFormAQuadrature_nTL_nTK and its singular part for N-MFIE,
+calculateFormAQuadrature_nTL_nTK and its singular part, gauss_legendre_rule,
 calculateMassMatrixQuadrature, calculateExcitationQuadrature<NxRWG>) in the
 loops of n_pmchwt_kernel / n_muller_kernel
 (src/sie_mom/solvers/dielectric/dielectric_kernels.cu:155-489) and
@@ -33,12 +33,15 @@ from oracle import oracle as O  # noqa: E402
 C0 = 299792458.0
 OUT = Path(__file__).resolve().parent / "variants_golden.npz"
 
-# name -> (kind, variant, media)
+# name -> (kind, variant, media, Gauss-Legendre points of the line form A; 0: surface form B)
 CASES = {
-    "n_efie": (0, 1, {}),
-    "n_mfie": (0, 2, {}),
-    "n_pmchwt": (1, 1, dict(eps_r=(4.0, 1.0), mu_r=(1.0, 1.0))),
-    "n_muller": (1, 2, dict(eps_r=(2.5, 1.0), mu_r=(1.5, 1.0))),
+    "n_efie": (0, 1, {}, 0),
+    "n_mfie": (0, 2, {}, 0),
+    "n_pmchwt": (1, 1, dict(eps_r=(4.0, 1.0), mu_r=(1.0, 1.0)), 0),
+    "n_muller": (1, 2, dict(eps_r=(2.5, 1.0), mu_r=(1.5, 1.0)), 0),
+    "n_efie_line": (0, 1, {}, 20),
+    "n_pmchwt_line": (1, 1, dict(eps_r=(4.0, 1.0), mu_r=(1.0, 1.0)), 10),
+    "n_muller_line": (1, 2, dict(eps_r=(2.5, 1.0), mu_r=(1.5, 1.0)), 7),
 }
 
 
@@ -58,12 +61,22 @@ def main() -> None:
     L0 = _Mesh(g, "L0")
     L1 = _Mesh(g, "L1r05")
     out = {}
-    for name, (kind, variant, media) in CASES.items():
+    # The line-form cases use the icosahedron scaled to radius 0.3 at 3 C0
+    # (same electrical size): at unit scale the reference's line form gives
+    # non-finite values (kept below as Z_n_efie_line_unit_L0).
+    L0s = _Mesh(g, "L0")
+    L0s.vertices = 0.3 * L0s.vertices
+    for name, (kind, variant, media, line_points) in CASES.items():
         # frequency C0 (lambda0 = 1 m) with a 1.5 lambda0 threshold on the
         # unit icosahedron: self and neighbouring pairs take the extracted path.
-        s = O.kernel_scalars(kind, C0, **media, threshold_lambda0=1.5)
-        out[f"Z_{name}_L0"] = O.assemble(ref, kind, L0, 5, s, fn="ref_assemble", variant=variant,
-                                         threads=1)
+        mesh, freq = (L0s, 3 * C0) if line_points else (L0, C0)
+        s = O.kernel_scalars(kind, freq, **media, threshold_lambda0=1.5)
+        out[f"Z_{name}_L0"] = O.assemble(ref, kind, mesh, 5, s, fn="ref_assemble", variant=variant,
+                                         threads=1, line_points=line_points)
+        if name == "n_efie_line":
+            su = O.kernel_scalars(kind, C0, **media, threshold_lambda0=1.5)
+            out["Z_n_efie_line_unit_L0"] = O.assemble(ref, kind, L0, 5, su, fn="ref_assemble",
+                                                      variant=variant, threads=1, line_points=line_points)
         eps_r = media.get("eps_r", (1.0, 1.0))
         mu_r = media.get("mu_r", (1.0, 1.0))
         regions = (2, 1) if kind == 1 else (2,)
@@ -74,8 +87,8 @@ def main() -> None:
             b = np.zeros(O.dimension(kind, L0.edges.shape[0]), np.complex128)
             E0 = np.array([1.0, 0.0, 0.0])
             kh = np.array([0.0, 0.0, 1.0])
-            ref.ref_rhs_plane_wave(kind, L0.vertices.ctypes.data, L0.faces.ctypes.data,
-                                   L0.faces_edges.ctypes.data, L0.faces.shape[0], L0.edges.shape[0], 5,
+            ref.ref_rhs_plane_wave(kind, mesh.vertices.ctypes.data, mesh.faces.ctypes.data,
+                                   mesh.faces_edges.ctypes.data, L0.faces.shape[0], L0.edges.shape[0], 5,
                                    E0.ctypes.data, kh.ctypes.data, k, eta, region, s["mu0"], s["eps0"],
                                    b.ctypes.data, variant, er, mr)
             out[f"b_{name}_L0_region{region}"] = b
@@ -86,9 +99,21 @@ def main() -> None:
     blocks = np.zeros((pairs.shape[0], 72))
     for p, (m, n) in enumerate(pairs):
         ref.ref_pair_blocks_n(L1.vertices.ctypes.data, L1.faces.ctypes.data, int(m), int(n), 6,
-                              s["k1"], s["k2"], s["thr"], blocks[p].ctypes.data)
+                              s["k1"], s["k2"], s["thr"], 0, blocks[p].ctypes.data)
+    blocks_line = np.zeros((pairs.shape[0], 72))
+    for p, (m, n) in enumerate(pairs):
+        ref.ref_pair_blocks_n(L1.vertices.ctypes.data, L1.faces.ctypes.data, int(m), int(n), 6,
+                              s["k1"], s["k2"], s["thr"], 12, blocks_line[p].ctypes.data)
     out["pair_n_index"] = pairs
     out["pair_n_blocks"] = blocks
+    out["pair_n_blocks_line12"] = blocks_line
+    # The reference's Gauss-Legendre rules on [0, 1] (gauss_legendre_rule.cpp).
+    for n in range(1, 21):
+        t = np.zeros(n)
+        w = np.zeros(n)
+        ref.ref_gauss_legendre(n, t.ctypes.data, w.ctypes.data)
+        out[f"gl{n}_nodes"] = t
+        out[f"gl{n}_weights"] = w
     out["pair_n_scalars"] = np.array([s["k1"], s["k2"], s["thr"]], np.float32)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")

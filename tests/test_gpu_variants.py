@@ -1,6 +1,6 @@
 """GPU parity of the rotated-testing formulations (N-EFIE, N-MFIE, N-PMCHWT,
-N-Muller; surface nTL form) through the C ABI, against the golden fixtures
-made from the reference and against the oracle.
+N-Muller; surface nTL form B and line form A) through the C ABI, against the
+golden fixtures made from the reference and against the oracle.
 
 Tolerances as for the tangential formulations: assembled Z and right-hand
 sides <= 1e-12 (max-entry error relative to the largest entry); solved
@@ -27,6 +27,9 @@ CASES = {
     "n_muller": (1, "N_Muller", dict(eps_r=(2.5, 1.0), mu_r=(1.5, 1.0))),
 }
 VARIANT = {"n_efie": 1, "n_mfie": 2, "n_pmchwt": 1, "n_muller": 2}
+# line form A: case -> (base case, Gauss-Legendre points); the fixtures use
+# the icosahedron scaled to radius 0.3 at 3 C0.
+LINE = {"n_efie_line": ("n_efie", 20), "n_pmchwt_line": ("n_pmchwt", 10), "n_muller_line": ("n_muller", 7)}
 
 
 @pytest.fixture(scope="module")
@@ -34,7 +37,7 @@ def vgolden():
     return dict(np.load(VG))
 
 
-def _opts(name, freq, rule, thr, solver="lu_cusolver", ntl_form="Surface"):
+def _opts(name, freq, rule, thr, solver="lu_cusolver", ntl_form="Surface", line_points=20):
     import sieb200
     kind, form, media = CASES[name]
     eps_r = media.get("eps_r", (1.0, 1.0))
@@ -42,11 +45,11 @@ def _opts(name, freq, rule, thr, solver="lu_cusolver", ntl_form="Surface"):
     if kind == 0:
         return sieb200.PecOptions(frequency_hz=freq, quadrature_rule=rule, singularity_threshold_lambda0=thr,
                                   exterior=sieb200.IsotropicMedium(eps_r[1], mu_r[1]), solver=solver,
-                                  formulation=form, ntl_form=ntl_form)
+                                  formulation=form, ntl_form=ntl_form, line_quadrature_points=line_points)
     return sieb200.DielectricOptions(frequency_hz=freq, quadrature_rule=rule, singularity_threshold_lambda0=thr,
                                      interior=sieb200.IsotropicMedium(eps_r[0], mu_r[0]),
                                      exterior=sieb200.IsotropicMedium(eps_r[1], mu_r[1]), solver=solver,
-                                     formulation=form, ntl_form=ntl_form)
+                                     formulation=form, ntl_form=ntl_form, line_quadrature_points=line_points)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -122,13 +125,37 @@ def test_variant_solve_matches_oracle(name, solver, gpu_ctx, oracle_lib):
     assert r.metrics["relative_residual"] <= 1e-10
 
 
-def test_line_form_and_gstc_variant_are_refused(gpu_ctx):
+@pytest.mark.parametrize("name", sorted(LINE))
+def test_line_form_assembly_matches_reference_golden(name, vgolden, gpu_ctx, mesh_l0):
     import sieb200
-    from sieb200 import _lib
+    base, lp = LINE[name]
+    m = sieb200.make_mesh(0.3 * mesh_l0.vertices, mesh_l0.faces)
+    Z = sieb200.assemble_matrix(m, _opts(base, 3 * C0, 5, 1.5, ntl_form="Line", line_points=lp), ctx=gpu_ctx)
+    assert rel_err(Z, vgolden[f"Z_{name}_L0"]) < Z_TOL
+
+
+@pytest.mark.parametrize("name,rule,thr", [("n_efie_line", 7, 0.35), ("n_pmchwt_line", 6, 0.3),
+                                           ("n_muller_line", 5, 0.3)])
+def test_line_form_assembly_matches_oracle(name, rule, thr, gpu_ctx, oracle_lib):
+    import sieb200
+    base, lp = LINE[name]
+    kind, _, media = CASES[base]
+    m = sieb200.icosphere(0.5, 1)
+    o = _opts(base, C0, rule, thr, ntl_form="Line", line_points=lp)
+    Z = sieb200.assemble_matrix(m, o, ctx=gpu_ctx)
+    s = O.kernel_scalars(kind, C0, **media, threshold_lambda0=thr)
+    Zo = O.assemble(oracle_lib, kind, m, rule, s, variant=VARIANT[base], line_points=lp)
+    assert rel_err(Z, Zo) < Z_TOL
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(Z.shape[0]) + 1j * rng.standard_normal(Z.shape[0])
+    assert rel_err(sieb200.matvec_matrix_free(m, o, x, ctx=gpu_ctx), Z @ x) < 1e-12
+
+
+def test_invalid_line_options_are_refused(gpu_ctx):
+    import sieb200
     m = sieb200.icosphere(0.5, 0)
-    with pytest.raises(sieb200.SiebError) as e:
-        sieb200.assemble_matrix(m, _opts("n_pmchwt", C0, 5, 0.1, ntl_form="Line"), ctx=gpu_ctx)
-    assert e.value.status == _lib.UNSUPPORTED
+    with pytest.raises(ValueError, match="Gauss-Legendre"):
+        sieb200.assemble_matrix(m, _opts("n_pmchwt", C0, 5, 0.1, ntl_form="Line", line_points=21), ctx=gpu_ctx)
     with pytest.raises(ValueError, match="requires N-EFIE"):
         sieb200.assemble_matrix(m, _opts("n_mfie", C0, 5, 0.1, ntl_form="Line"), ctx=gpu_ctx)
     o = sieb200.DielectricOptions(frequency_hz=C0, ntl_form="Line")
