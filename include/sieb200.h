@@ -315,6 +315,15 @@ int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double
  * j_cur, m_cur: host, num_edges complex each (m_cur may be NULL).
  * Directions: host, ndir x 3 unit vectors each. Outputs: host, ndir complex
  * F_theta and F_phi, ndir real radiation intensities U. */
+/* Incident E and H of one source (plane wave or dipole, bound to its
+ * region's medium from opt) at num_points host points (x, y, z); E and H:
+ * host, 3 complex per point. Replaces evaluate_incident_fields
+ * (src/sie_mom/excitation/excitation.cu:158-210, declared in
+ * include/sie_mom/excitation/excitation.hpp), which the apps subtract the
+ * surface integrals from for their field cuts. */
+int sieb200_incident_fields(sieb200_ctx* ctx, const sieb200_options* opt, const sieb200_source* source,
+                            int64_t num_points, const double* points, double* E, double* H);
+
 int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,
                       const double* m_cur, double k0, double eta0, int64_t ndir,
                       const double* r_hat, const double* theta_hat, const double* phi_hat,

@@ -48,6 +48,7 @@ def oracle() -> ctypes.CDLL:
     lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
     lib.so_surface_fields.argtypes = _FIELDS
+    lib.so_incident_fields.argtypes = [_i, _P, _P, _i, _d, _d, _i, _P, _P, _P]
     return lib
 
 
@@ -176,4 +177,19 @@ def surface_fields(lib, mesh, j, m, points, frequency_hz, eps_r=1.0, mu_r=1.0, e
             float(frequency_hz), float(eps_r), float(mu_r), float(eps0), float(mu0), int(rule), _p(E), _p(H))
     if rc != 0:
         raise ValueError("surface fields: invalid quadrature rule")
+    return E, H
+
+
+def incident_fields(lib, source: dict, k: float, eta: float, points):
+    """Incident (E, H) at points (n x 3 complex) of a source dict as for rhs()
+    (plane-wave direction normalised here, as the library prepares it)."""
+    P = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    a = np.ascontiguousarray(source["a"], dtype=np.float64)
+    b = np.ascontiguousarray(source["b"], dtype=np.float64)
+    if source["kind"] == 0:
+        b = b / np.linalg.norm(b)
+    E = np.zeros((P.shape[0], 3), np.complex128)
+    H = np.zeros((P.shape[0], 3), np.complex128)
+    lib.so_incident_fields(int(source["kind"]), _p(a), _p(b), int(source.get("is_magnetic", 0)), float(k),
+                           float(eta), P.shape[0], _p(P), _p(E), _p(H))
     return E, H

@@ -1068,6 +1068,22 @@ static void source_fields(int kind, v3 r, const double* a, const double* b, int 
     }
 }
 
+/* compute_incident_field_kernel (src/sie_mom/excitation/excitation.cu:140-156):
+ * the source functors at n points; E, H complex interleaved, 3 per point.
+ * b is the unit propagation direction of a plane wave. */
+int so_incident_fields(int source_kind, const double* a, const double* b, int is_magnetic, double k, double eta,
+                       int n, const double* pts, double* E, double* H) {
+    for (int i = 0; i < n; ++i) {
+        cx Ei[3], Hi[3];
+        source_fields(source_kind, V3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), a, b, is_magnetic, k, eta, Ei, Hi);
+        for (int c = 0; c < 3; ++c) {
+            E[2 * (3 * i + c)] = Ei[c].re; E[2 * (3 * i + c) + 1] = Ei[c].im;
+            H[2 * (3 * i + c)] = Hi[c].re; H[2 * (3 * i + c) + 1] = Hi[c].im;
+        }
+    }
+    return 0;
+}
+
 /* dunavant_quadrature.cuh:1543-1611 (RWG testing; variant != 0: n x RWG
  * testing, rho x n_m; variant 2: N-MFIE tests H, N-Muller scales by the
  * source region's eps_r_src, mu_r_src) with the placements of

@@ -24,6 +24,8 @@ int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* 
            int rule, const double* a, const double* b, int is_magnetic, double k, double eta,
            int region, double mu0, double eps0, double* rhs, int variant, double eps_r_src,
            double mu_r_src);
+int so_incident_fields(int source_kind, const double* a, const double* b, int is_magnetic, double k, double eta,
+                       int n, const double* pts, double* E, double* H);
 int so_far_field(const double* V, const int* F, int nf, int ne, const double* j_cur,
                  const double* m_cur, double k0, double eta0, int ndir, const double* r_hat,
                  const double* theta_hat, const double* phi_hat, double* f_theta, double* f_phi,

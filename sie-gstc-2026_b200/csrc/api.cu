@@ -26,6 +26,8 @@ int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j
                      const double* m_cur, double k0, double eta0, int64_t ndir, const double* rh,
                      const double* th, const double* ph, double* f_theta, double* f_phi,
                      double* intensity);
+int incident_fields_device(sieb200_ctx* ctx, const sieb200_options& opt, const sieb200_source& source, int64_t n,
+                           const double* points, double* E_out, double* H_out);
 
 namespace {
 thread_local std::string g_last_error;
@@ -853,6 +855,18 @@ int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* 
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     return far_field_device(ctx, *mesh, j_cur, m_cur, k0, eta0, ndir, r_hat, theta_hat, phi_hat,
                             f_theta, f_phi, intensity);
+}
+
+int sieb200_incident_fields(sieb200_ctx* ctx, const sieb200_options* opt, const sieb200_source* source,
+                            int64_t num_points, const double* points, double* E, double* H) {
+    SIEB_CHECK(ctx && opt && source && num_points >= 0 && (num_points == 0 || (points && E && H)),
+               SIEB200_INVALID_ARG, "invalid incident-field arguments");
+    SIEB_CHECK(opt->frequency_hz > 0 && std::isfinite(opt->frequency_hz), SIEB200_INVALID_ARG,
+               "SIE frequency must be positive");
+    SIEB_CHECK(opt->vacuum_permittivity > 0 && opt->vacuum_permeability > 0, SIEB200_INVALID_ARG,
+               "vacuum permittivity and permeability must be positive");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    return sieb200::incident_fields_device(ctx, *opt, *source, num_points, points, E, H);
 }
 
 int sieb200_far_field_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, double k0, double eta0, int64_t ndir,

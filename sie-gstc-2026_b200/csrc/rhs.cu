@@ -146,6 +146,23 @@ __global__ void rhs_face_kernel(const double* __restrict__ V, const int* __restr
     }
 }
 
+// Incident E and H of one source at observation points
+// (compute_incident_field_kernel, src/sie_mom/excitation/excitation.cu:140-156):
+// the same source functors as the right-hand sides, one thread per point.
+__global__ void incident_fields_kernel(const double* __restrict__ pts, int64_t n, const DevSource* __restrict__ src,
+                                       cplx* __restrict__ E, cplx* __restrict__ H) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DevSource S = *src;
+    cplx e[3], h[3];
+    source_fields(S, mk3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), e, h);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        E[3 * i + c] = e[c];
+        H[3 * i + c] = h[c];
+    }
+}
+
 __global__ void rhs_gather_kernel(const cplx* __restrict__ face_vals, const int* __restrict__ inc,
                                   int nf, int ne, const DevSource* __restrict__ src, int nsrc,
                                   int64_t N, cplx* __restrict__ B, int64_t ldb) {
@@ -463,6 +480,36 @@ int assemble_rhs_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const sieb20
         ctx->rhsbuf.as<cplx>(), dinc, nf, ne, dsrc, nsrc, N, dB, ldb);
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
+// evaluate_incident_fields (src/sie_mom/excitation/excitation.cu:158-210):
+// host points in, host E and H (3 complex per point) out; the source's k and
+// eta are bound from its region's medium as for the right-hand sides.
+int incident_fields_device(sieb200_ctx* ctx, const sieb200_options& opt, const sieb200_source& source, int64_t n,
+                           const double* points, double* E_out, double* H_out) {
+    std::vector<DevSource> ds;
+    SIEB_RETURN_IF(prepare_sources(opt, &source, 1, &ds));
+    for (int64_t i = 0; i < 3 * n; ++i)
+        SIEB_CHECK(std::isfinite(points[i]), SIEB200_INVALID_ARG, "incident-field observation point must be finite");
+    if (n == 0) return SIEB200_OK;
+    cudaStream_t st = ctx->stream;
+    const size_t pbytes = sizeof(double) * 3 * (size_t)n, fbytes = sizeof(cplx) * 3 * (size_t)n;
+    const size_t off_s = ((pbytes + 255) / 256) * 256;
+    const size_t off_e = off_s + 256, off_h = off_e + ((fbytes + 255) / 256) * 256;
+    DeviceBuffer buf;
+    SIEB_RETURN_IF(buf.reserve(off_h + fbytes));
+    char* b = buf.as<char>();
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b, points, pbytes, cudaMemcpyHostToDevice, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(b + off_s, ds.data(), sizeof(DevSource), cudaMemcpyHostToDevice, st));
+    incident_fields_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        reinterpret_cast<const double*>(b), n, reinterpret_cast<const DevSource*>(b + off_s),
+        reinterpret_cast<cplx*>(b + off_e), reinterpret_cast<cplx*>(b + off_h));
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    SIEB_TRY_CUDA(cudaMemcpyAsync(E_out, b + off_e, fbytes, cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(H_out, b + off_h, fbytes, cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
     return SIEB200_OK;
 }
 

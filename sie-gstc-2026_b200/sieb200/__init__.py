@@ -12,12 +12,13 @@ from .adjoint import (FarFieldConeObjective, cone_directions, far_field_matrix, 
                       physical_exterior, tensor_gradient)
 from .farfield import (MetasurfaceFarFieldEvaluator, bistatic_rcs, evaluate_surface_integral_fields, far_field,
                        spherical_frames)
-from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, load_obj, make_mesh, \
+from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, infer_sphere_radius, load_obj, make_mesh, \
     revolved_spindle, save_obj
 from .solvers import (EXTERIOR, INTERIOR, Context, DenseLuSolver, DielectricOptions,
                       DipoleExcitation, GstcExcitationCase, GstcSieOptions, IsotropicMedium,
                       PecOptions, PlaneWaveExcitation, assemble_matrix, assemble_matrix_device,
-                      assemble_rhs, default_context, matvec, matvec_matrix_free, solve_dielectric_dense,
+                      assemble_rhs, default_context, incident_fields, matvec, matvec_matrix_free,
+                      solve_dielectric_dense,
                       solve_gstc_dense, solve_gstc_dense_batch, solve_pec_dense)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

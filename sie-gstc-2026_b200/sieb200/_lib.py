@@ -119,6 +119,7 @@ _SIGNATURES = {
                                 ctypes.c_double, ctypes.c_double, ctypes.c_int, _P, _P], ctypes.c_int),
     "sieb200_far_field_matrix": ([_P, _P, ctypes.c_double, ctypes.c_double, _I64, _P, _P, _P, ctypes.c_int, _P],
                                  ctypes.c_int),
+    "sieb200_incident_fields": ([_P, _P, _P, _I64, _P, _P, _P], ctypes.c_int),
     "sieb200_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "sieb200_fp64_fma_peak": ([_P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "sieb200_profile_timeline": ([_P, _I64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),

@@ -190,22 +190,69 @@ def revolved_spindle(arc_radius: float = 1.5, half_angle_deg: float = 60.0, n_ax
     return make_mesh(v, f)
 
 
+def _obj_index(token: str, seen: int, where: str) -> int:
+    """obj_mesh_loader.cpp:26-66: 1-based or negative (relative) index before any '/'."""
+    text = token.split("/", 1)[0]
+    if not text:
+        raise ValueError(f"{where}: face has an empty vertex index")
+    try:
+        raw = int(text)
+    except ValueError:
+        raise ValueError(f"{where}: invalid face vertex index '{text}'") from None
+    if raw == 0:
+        raise ValueError(f"{where}: invalid face vertex index '{text}'")
+    if raw > 0:
+        return raw - 1
+    if not 0 <= seen + raw < seen:
+        raise ValueError(f"{where}: relative face vertex index is out of range")
+    return seen + raw
+
+
 def load_obj(path: str | Path) -> MeshData:
-    """Vertices (v) and triangular faces (f, 1-based, optional /vt/vn) in file
-    order, winding preserved (obj_mesh_loader.hpp:17-39 contract)."""
+    """Vertices (v) and triangular faces (f) in file order, winding preserved,
+    with the line-level checks and messages of ObjMeshLoader
+    (src/sie_mom/mesh/obj_mesh_loader.cpp:90-152): three coordinates per
+    vertex, exactly three indices per face (a trailing '#' comment ends the
+    face), no empty, zero or out-of-range index, at least one vertex and one
+    face, finite coordinates."""
+    path = str(path)
+    try:
+        text = Path(path).read_text()
+    except OSError:
+        raise RuntimeError(f"Failed to open OBJ file: {path}") from None
     verts, faces = [], []
-    for line in Path(path).read_text().splitlines():
+    for number, line in enumerate(text.splitlines(), 1):
         parts = line.split()
         if not parts or parts[0].startswith("#"):
             continue
+        where = f"{path}:{number}"
         if parts[0] == "v":
-            verts.append([float(x) for x in parts[1:4]])
+            try:
+                verts.append([float(x) for x in parts[1:4]])
+                if len(parts) < 4:
+                    raise ValueError
+            except ValueError:
+                raise RuntimeError(f"{where}: vertex requires three coordinates") from None
         elif parts[0] == "f":
-            idx = [int(p.split("/")[0]) for p in parts[1:]]
-            if len(idx) != 3:
-                raise ValueError("only triangular faces are supported")
-            faces.append([i - 1 if i > 0 else len(verts) + i for i in idx])
-    return make_mesh(np.array(verts), np.array(faces, dtype=np.int32))
+            tokens = []
+            for t in parts[1:]:
+                if t.startswith("#"):
+                    break
+                tokens.append(t)
+            if len(tokens) != 3:
+                raise RuntimeError(f"{where}: only triangular faces are supported")
+            try:
+                faces.append([_obj_index(t, len(verts), where) for t in tokens])
+            except ValueError as e:
+                raise RuntimeError(str(e)) from None
+    if not verts:
+        raise RuntimeError(f"Invalid OBJ mesh {path}: no vertices")
+    if not faces:
+        raise RuntimeError(f"Invalid OBJ mesh {path}: no faces")
+    v = np.array(verts, dtype=np.float64)
+    if not np.isfinite(v).all():
+        raise RuntimeError(f"Invalid OBJ mesh {path}: non-finite vertex coordinate")
+    return make_mesh(v, np.array(faces, dtype=np.int32))
 
 
 def save_obj(mesh: MeshData, path: str | Path) -> None:
@@ -214,3 +261,15 @@ def save_obj(mesh: MeshData, path: str | Path) -> None:
             fh.write(f"v {v[0]:.17g} {v[1]:.17g} {v[2]:.17g}\n")
         for f in mesh.faces:
             fh.write(f"f {f[0] + 1} {f[1] + 1} {f[2] + 1}\n")
+
+
+def infer_sphere_radius(mesh: MeshData, max_relative_spread: float = 1e-4) -> float:
+    """Mean vertex radius of a sphere mesh centred at the origin
+    (include/sie_mom/mesh/mesh_utils.hpp:156-182)."""
+    r = np.sqrt((np.asarray(mesh.vertices, dtype=np.float64) ** 2).sum(axis=1))
+    if not (np.isfinite(r).all() and (r > 0).all()):
+        raise RuntimeError("sphere mesh contains a non-finite or zero-radius vertex")
+    radius = float(np.sum(r.astype(np.longdouble)) / r.size)
+    if (r.max() - r.min()) / radius > max_relative_spread:
+        raise RuntimeError("mesh vertices do not lie on a common spherical radius")
+    return radius

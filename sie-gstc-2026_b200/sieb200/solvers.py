@@ -377,6 +377,22 @@ def assemble_rhs(mesh: MeshData, options, sources: Sequence, ctx: Optional[Conte
     return B
 
 
+def incident_fields(observation_points, source, options, ctx: Optional[Context] = None):
+    """Incident (E, H) of one source at observation points, each (n, 3)
+    complex128 (evaluate_incident_fields, src/sie_mom/excitation/excitation.cu:158-210);
+    the source's wavenumber and impedance come from its region's medium in
+    options."""
+    ctx = ctx or default_context()
+    o = to_c_options(options, _formulation_of(options))
+    pts = np.ascontiguousarray(observation_points, dtype=np.float64).reshape(-1, 3)
+    E = np.zeros((pts.shape[0], 3), dtype=np.complex128)
+    H = np.zeros((pts.shape[0], 3), dtype=np.complex128)
+    src = source.as_c()
+    _lib.check(_lib.lib().sieb200_incident_fields(ctx.handle, ctypes.byref(o), ctypes.byref(src), pts.shape[0],
+                                                  pts.ctypes.data, E.ctypes.data, H.ctypes.data))
+    return E, H
+
+
 def matvec_matrix_free(mesh: MeshData, options, x: np.ndarray, tensors=None,
                        ctx: Optional[Context] = None) -> np.ndarray:
     """y = Z x with Z recomputed by the quadrature kernels, never stored
