@@ -181,3 +181,64 @@ def test_metrics_and_field_writers(tmp_path):
     lines = (tmp_path / "f.csv").read_text().splitlines()
     assert lines[0].startswith("point_index,x,y,z,region,Ex_real")
     assert lines[1] == "0,1,2,3,2,0,0,0,0,0,-0.5,0,0,0,0,0,0"
+
+
+# ------------------------------------------------------------ pec_sphere_app
+PEC_BASE = ["pec", "--mesh", "m.obj", "--output-dir", "out", "--frequency-hz", "3e8"]
+
+
+def test_pec_parse_and_messages():
+    from sieb200.apps.pec_sphere_app import parse
+    a = parse(PEC_BASE + ["--formulation", "n", "--ntl-form", "line", "--line-quadrature-points", "12",
+                          "--zx-grid-size", "0", "--radial-points", "7", "--frequency-hz", "2e8Hz"])
+    assert (a.formulation, a.ntl_form, a.line_quadrature_points) == ("NEfie", "Line", 12)
+    assert a.zx_grid_size == 0 and a.radial_points == 7 and a.frequency_hz == 2e8  # stod takes the prefix
+    for extra, msg in [(["--formulation", "x"], "--formulation must be t-efie, n-efie, or n-mfie"),
+                       (["--ntl-form", "area"], "--ntl-form must be surface or line"),
+                       (["--zx-grid-size", "1"], "invalid field sampling range or point count"),
+                       (["--radial-max-radii", "0.01"], "invalid field sampling range or point count"),
+                       (["--currents-file", "c.csv", "--no-fields"], "--currents-file requires field evaluation"),
+                       (["--currents-file", "c.csv", "--export-matrix"],
+                        "--export-matrix requires solving, not --currents-file"),
+                       (["--quadrature-rule", "x"], "stoi"),
+                       (["--zz"], "unknown option: --zz"),
+                       (["--mesh"], "missing option value")]:
+        with pytest.raises(ValueError) as e:
+            parse(PEC_BASE + extra)
+        assert str(e.value) == msg
+    with pytest.raises(ValueError, match="are required"):
+        parse(["pec", "--mesh", "m.obj"])
+
+
+def test_pec_matrix_npy_and_currents_csv(tmp_path):
+    from sieb200.apps.pec_sphere_app import read_currents, write_matrix_npy
+    rng = np.random.default_rng(1)
+    Z = rng.standard_normal((5, 5)) + 1j * rng.standard_normal((5, 5))
+    write_matrix_npy(tmp_path / "m.npy", Z)
+    raw = (tmp_path / "m.npy").read_bytes()
+    assert raw[:8] == b"\x93NUMPY\x01\x00" and (10 + int.from_bytes(raw[8:10], "little")) % 16 == 0
+    back = np.load(tmp_path / "m.npy")
+    assert np.array_equal(back, Z) and back.flags["F_CONTIGUOUS"]
+    c = tmp_path / "c.csv"
+    c.write_text("edge,J2_real,J2_imag,J2_abs\n0,1.5,-2,2.5\n1,0,1e-3,1e-3\n")
+    assert np.array_equal(read_currents(str(c), 2), [1.5 - 2j, 1e-3j])
+    with pytest.raises(RuntimeError, match="edge count does not match mesh"):
+        read_currents(str(c), 3)
+    c.write_text("edge,J2_real,J2_imag,J2_abs\n1,1.5,-2,2.5\n")
+    with pytest.raises(RuntimeError, match="invalid current CSV row"):
+        read_currents(str(c), 1)
+    c.write_text("edge,J2\n")
+    with pytest.raises(RuntimeError, match="unexpected current CSV header"):
+        read_currents(str(c), 0)
+
+
+def test_pec_observations():
+    from sieb200.apps.pec_sphere_app import Arguments, make_observations
+    a = Arguments(zx_grid_size=3, radial_points=3, radial_min_radii=0.0, radial_max_radii=2.0,
+                  radial_theta_degrees=0.0)
+    o = make_observations(a, 1.0)
+    assert o.zx_count == 9 and o.points.shape == (12, 3)
+    assert np.allclose(o.points[4], [0, 0, 0]) and o.regions[4] == 1 and o.regions[0] == 2
+    assert np.allclose(o.points[9:, 2], [0.0, 1.0, 2.0]) and list(o.regions[9:]) == [1, 2, 2]
+    o = make_observations(Arguments(zx_grid_size=0, radial_points=0), 1.0)
+    assert o.points.shape == (0, 3)

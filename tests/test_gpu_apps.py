@@ -89,3 +89,37 @@ def test_anisotropic_sphere_app_end_to_end(tmp_path, gpu_ctx):
             inc = sieb200.incident_fields(P[sel], src, o, ctx=gpu_ctx)[0] if src is not None else 0.0
             assert rel_err(E_csv[sel], inc - Q) < 1e-12
         assert (d / "fields" / "sie_interior_representation_zx.csv").is_file()
+
+
+def test_pec_sphere_app_end_to_end(tmp_path, gpu_ctx):
+    import sieb200
+    from sieb200.apps.pec_sphere_app import main
+    mesh = sieb200.icosphere(0.5, 1)
+    sieb200.save_obj(mesh, tmp_path / "sphere.obj")
+    out = tmp_path / "run"
+    argv = ["pec_sphere_app", "--mesh", str(tmp_path / "sphere.obj"), "--output-dir", str(out),
+            "--frequency-hz", str(C0), "--formulation", "n-efie", "--quadrature-rule", "5",
+            "--export-matrix", "--zx-grid-size", "4", "--radial-points", "6"]
+    assert main(argv) == 0
+    m2 = sieb200.load_obj(tmp_path / "sphere.obj")
+    o = sieb200.PecOptions(frequency_hz=C0, quadrature_rule=5, formulation="NEfie")
+    r = sieb200.solve_pec_dense(m2, o, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
+    rows = np.loadtxt(out / "currents.csv", delimiter=",", skiprows=1)
+    assert rel_err(rows[:, 1] + 1j * rows[:, 2], r.currents) < 1e-12
+    assert np.allclose(rows[:, 3], np.abs(rows[:, 1] + 1j * rows[:, 2]), rtol=1e-15)
+    Z = np.load(out / "matrix.npy")
+    assert rel_err(Z, sieb200.assemble_matrix(m2, o, ctx=gpu_ctx)) < 1e-15
+    f = np.loadtxt(out / "radial_fields.csv", delimiter=",", skiprows=1)
+    assert f.shape == (6, 16)
+    P = f[:, :3]
+    Q, _ = sieb200.evaluate_surface_integral_fields(m2, r.currents, None, P, C0, ctx=gpu_ctx)
+    inc, _ = sieb200.incident_fields(P, sieb200.PlaneWaveExcitation(), o, ctx=gpu_ctx)
+    E = f[:, 4:10:2] + 1j * f[:, 5:11:2]
+    assert rel_err(E, inc - Q) < 1e-11  # the CSV carries 13 significant digits
+    # --currents-file: the saved J2 gives the same field files without a solve
+    out2 = tmp_path / "fields_only"
+    assert main(["pec_sphere_app", "--mesh", str(tmp_path / "sphere.obj"), "--output-dir", str(out2),
+                 "--frequency-hz", str(C0), "--quadrature-rule", "5", "--currents-file", str(out / "currents.csv"),
+                 "--zx-grid-size", "4", "--radial-points", "6"]) == 0
+    assert (out2 / "radial_fields.csv").read_text() == (out / "radial_fields.csv").read_text()
+    assert (out2 / "zx_fields.csv").read_text() == (out / "zx_fields.csv").read_text()
