@@ -112,7 +112,8 @@ def test_pec_sphere_app_end_to_end(tmp_path, gpu_ctx):
     f = np.loadtxt(out / "radial_fields.csv", delimiter=",", skiprows=1)
     assert f.shape == (6, 16)
     P = f[:, :3]
-    Q, _ = sieb200.evaluate_surface_integral_fields(m2, r.currents, None, P, C0, ctx=gpu_ctx)
+    Q, _ = sieb200.evaluate_surface_integral_fields(m2, r.currents, None, P, C0, o.exterior, 5,
+                                                    o.vacuum_permittivity, o.vacuum_permeability, ctx=gpu_ctx)
     inc, _ = sieb200.incident_fields(P, sieb200.PlaneWaveExcitation(), o, ctx=gpu_ctx)
     E = f[:, 4:10:2] + 1j * f[:, 5:11:2]
     assert rel_err(E, inc - Q) < 1e-11  # the CSV carries 13 significant digits
