@@ -30,7 +30,7 @@ def _blocks(parameters):
 
 
 def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: float, extraction_method: str,
-                           tensor_structure: str, device=None):
+                           tensor_structure: str, device=None, hermitian_solver: str = "auto"):
     """(records, diagnostics): records a (face_count, 32) complex128 tensor on
     `device` (default: the current CUDA device). parameters: an object or dict
     with Y_ee, Y_em, Y_me, Y_mm of shape (2, 2, face_count) (numpy arrays or
@@ -38,8 +38,9 @@ def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: 
     losslessness (extraction_method "reciprocal_lossless"), diagonal
     structure (tensor_structure "diagonal"), numerical singularity
     (s_min <= 4 eps s_max) and the two-sided inverse residual (1e-8).
-    Lossless maps are inverted as the Hermitian system (i B) X = i I (LDL^H),
-    the others by LU."""
+    Lossless maps are inverted as the Hermitian system (i B) X = i I (LDL^H
+    on the CPU, LU on CUDA; hermitian_solver "ldl" or "lu" forces one), the
+    others by LU."""
     torch = _torch()
     dev = torch.device(device) if device is not None else torch.device("cuda")
     eta = float(reference_impedance)
@@ -89,10 +90,15 @@ def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: 
                          f"(first face index {first}); the current SIE interface requires its full inverse")
     eye = torch.eye(4, dtype=torch.complex128, device=dev).expand(face_count, 4, 4)
     try:
-        if extraction_method == "reciprocal_lossless":
+        ldl = hermitian_solver == "ldl" or (hermitian_solver == "auto" and dev.type == "cpu")
+        if extraction_method == "reciprocal_lossless" and ldl:
             # B^H = -B, so i B is Hermitian and (i B) X = i I gives B^-1.
             LD, piv = torch.linalg.ldl_factor(1j * balanced, hermitian=True)
             binv = torch.linalg.ldl_solve(LD, piv, 1j * eye, hermitian=True)
+        elif extraction_method == "reciprocal_lossless":
+            # The same system by LU: torch has no complex Hermitian LDL^H solve
+            # on CUDA. The two-sided residual check below holds either way.
+            binv = torch.linalg.solve(1j * balanced, 1j * eye)
         else:
             binv = torch.linalg.inv(balanced)
     except RuntimeError as error:

@@ -19,13 +19,14 @@ def _params(maps):
     return {"Y_ee": m[:2, :2], "Y_em": m[:2, 2:], "Y_me": m[2:, :2], "Y_mm": m[2:, 2:]}
 
 
-def check_against_golden(device):
+def check_against_golden(device, hermitian_solver="auto"):
     from sieb200.records import prepare_tensor_records
     g = dict(np.load(RG))
     for name, (method, structure) in CASES.items():
         maps = g[f"{name}_maps"]
         rec, diag = prepare_tensor_records(_params(maps), maps.shape[0], reference_impedance=float(g["eta"]),
-                                           extraction_method=method, tensor_structure=structure, device=device)
+                                           extraction_method=method, tensor_structure=structure, device=device,
+                                           hermitian_solver=hermitian_solver)
         rec = rec.cpu().numpy()
         ref = g[f"{name}_records"]
         assert np.array_equal(rec[:, :16], ref[:, :16]), name  # the map is kept as given
@@ -37,8 +38,10 @@ def check_against_golden(device):
         assert abs(diag["maximum_map_condition_number"] / float(g[f"{name}_condition"]) - 1) < 1e-8
 
 
-def test_records_match_reference_on_cpu():
-    check_against_golden("cpu")
+@pytest.mark.parametrize("solver", ["auto", "lu"])
+def test_records_match_reference_on_cpu(solver):
+    # "lu" is the branch CUDA takes for lossless maps
+    check_against_golden("cpu", solver)
 
 
 def _one(matrix):
