@@ -26,7 +26,7 @@ from typing import Optional
 
 import numpy as np
 
-from .cli import EXTERIOR, INTERIOR, parse_integer, parse_real, parse_region, parse_vector, require_value
+from .cli import INTERIOR, parse_integer, parse_real, parse_region, parse_vector, require_value
 
 PROGRAM = "anisotropic_sphere_app"
 

@@ -4,7 +4,6 @@ formats (face_tensors.bin, currents.bin, OBJ), observation sampling and the
 JSON / CSV writers. The solve itself runs in tests/test_gpu_apps.py."""
 
 import json
-import math
 import subprocess
 import sys
 from pathlib import Path
