@@ -65,6 +65,7 @@ def reference() -> ctypes.CDLL | None:
     lib.ref_pair_blocks.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _P]
     lib.ref_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _i, _P]
     lib.ref_gauss_legendre.argtypes = [_i, _P, _P]
+    lib.ref_incident_fields.argtypes = [_i, _P, _P, _i, _d, _d, _i, _P, _P, _P]
     lib.ref_assemble.argtypes = _ASSEMBLE
     lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.ref_surface_fields.argtypes = _FIELDS
@@ -182,7 +183,9 @@ def surface_fields(lib, mesh, j, m, points, frequency_hz, eps_r=1.0, mu_r=1.0, e
 
 def incident_fields(lib, source: dict, k: float, eta: float, points):
     """Incident (E, H) at points (n x 3 complex) of a source dict as for rhs()
-    (plane-wave direction normalised here, as the library prepares it)."""
+    (plane-wave direction normalised here, as the library prepares it), from
+    the C restatement (lib = oracle()) or the reference's functors
+    (lib = reference())."""
     P = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
     a = np.ascontiguousarray(source["a"], dtype=np.float64)
     b = np.ascontiguousarray(source["b"], dtype=np.float64)
@@ -190,6 +193,7 @@ def incident_fields(lib, source: dict, k: float, eta: float, points):
         b = b / np.linalg.norm(b)
     E = np.zeros((P.shape[0], 3), np.complex128)
     H = np.zeros((P.shape[0], 3), np.complex128)
-    lib.so_incident_fields(int(source["kind"]), _p(a), _p(b), int(source.get("is_magnetic", 0)), float(k),
-                           float(eta), P.shape[0], _p(P), _p(E), _p(H))
+    fn = lib.so_incident_fields if hasattr(lib, "so_incident_fields") else lib.ref_incident_fields
+    fn(int(source["kind"]), _p(a), _p(b), int(source.get("is_magnetic", 0)), float(k), float(eta), P.shape[0],
+       _p(P), _p(E), _p(H))
     return E, H

@@ -680,6 +680,39 @@ double ref_lu_solve(int n, const double* A, const double* b, double* x, int nrhs
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+// The reference's source functors (include/sie_mom/excitation/source_functors.cuh:14-130)
+// at n points: kind 0 plane wave (a = E0, b = unit direction), 1 dipole
+// (a = moment, b = position). E, H complex interleaved, 3 per point.
+int ref_incident_fields(int kind, const double* a, const double* b, int is_magnetic, double k, double eta,
+                        int n, const double* pts, double* E, double* H) {
+    for (int i = 0; i < n; ++i) {
+        const vec3_t r = make_vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+        cvec3_t e, h;
+        if (kind == 0) {
+            sie_mom::cuda::PlaneWave pw;
+            pw.E0 = make_vec3(a[0], a[1], a[2]);
+            pw.propagation_k = make_vec3(b[0], b[1], b[2]);
+            pw.k = k;
+            pw.eta = eta;
+            pw(r, e, h);
+        } else {
+            sie_mom::cuda::DipoleSource d;
+            d.p_vec = make_vec3(a[0], a[1], a[2]);
+            d.r_0 = make_vec3(b[0], b[1], b[2]);
+            d.k = k;
+            d.eta = eta;
+            d.is_magnetic = is_magnetic != 0;
+            d(r, e, h);
+        }
+        const complex_t ec[3] = {e.x, e.y, e.z}, hc[3] = {h.x, h.y, h.z};
+        for (int c = 0; c < 3; ++c) {
+            E[2 * (3 * i + c)] = ec[c].x; E[2 * (3 * i + c) + 1] = ec[c].y;
+            H[2 * (3 * i + c)] = hc[c].x; H[2 * (3 * i + c) + 1] = hc[c].y;
+        }
+    }
+    return 0;
+}
+
 // The reference's Gauss-Legendre rule on [0, 1] (gauss_legendre_rule.cpp), doubles.
 int ref_gauss_legendre(int n, double* t, double* w) {
     if (n < 1 || n > gauss_legendre_max_points()) return -1;

@@ -104,6 +104,26 @@ def main() -> None:
     for p, (m, n) in enumerate(pairs):
         ref.ref_pair_blocks_n(L1.vertices.ctypes.data, L1.faces.ctypes.data, int(m), int(n), 6,
                               s["k1"], s["k2"], s["thr"], 12, blocks_line[p].ctypes.data)
+    # Incident fields of the reference's source functors at seeded points
+    # (plane wave, electric and magnetic dipoles; k, eta of a medium 3 / 1.5).
+    rng = np.random.default_rng(77)
+    P = rng.uniform(-1.0, 1.0, (40, 3))
+    k = 2 * np.pi * C0 * np.sqrt(1.25663706127e-6 * 1.5 * 8.8541878188e-12 * 3.0)
+    eta = np.sqrt(1.25663706127e-6 * 1.5 / (8.8541878188e-12 * 3.0))
+    srcs = [(0, [0.0, 2.0, 0.0], [1.0, 0.0, 0.0], 0), (1, [0.2, 0.0, 1.0], [0.1, 0.05, 0.0], 1),
+            (1, [0.0, 1.0, 0.0], [0.0, 0.0, 0.2], 0)]
+    for q, (kind, a, b, mag) in enumerate(srcs):
+        E = np.zeros((P.shape[0], 3), np.complex128)
+        H = np.zeros((P.shape[0], 3), np.complex128)
+        a = np.array(a)
+        b = np.array(b)
+        ref.ref_incident_fields(kind, a.ctypes.data, b.ctypes.data, mag, float(k), float(eta), P.shape[0],
+                                P.ctypes.data, E.ctypes.data, H.ctypes.data)
+        out[f"inc{q}_E"] = E
+        out[f"inc{q}_H"] = H
+        out[f"inc{q}_source"] = np.concatenate(([kind, mag], a, b))
+    out["inc_points"] = P
+    out["inc_k_eta"] = np.array([k, eta])
     out["pair_n_index"] = pairs
     out["pair_n_blocks"] = blocks
     out["pair_n_blocks_line12"] = blocks_line

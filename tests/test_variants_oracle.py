@@ -178,3 +178,24 @@ def test_python_options_map_reference_formulation_names():
     with pytest.raises(ValueError):
         to_c_options(sieb200.PecOptions(frequency_hz=1e9, formulation="NEfie", ntl_form="line",
                                         line_quadrature_points=21), _lib.PEC_EFIE)
+
+
+def test_incident_fields_match_reference_functors(vgolden, oracle_lib):
+    # so_incident_fields (the oracle of sieb200_incident_fields) against the
+    # reference's PlaneWave / DipoleSource functors (source_functors.cuh:14-130).
+    P = vgolden["inc_points"]
+    k, eta = (float(x) for x in vgolden["inc_k_eta"])
+    for q in range(3):
+        src = vgolden[f"inc{q}_source"]
+        spec = dict(kind=int(src[0]), is_magnetic=int(src[1]), a=src[2:5], b=src[5:8])
+        E, H = O.incident_fields(oracle_lib, spec, k, eta, P)
+        assert rel_err(E, vgolden[f"inc{q}_E"]) < 1e-14 and rel_err(H, vgolden[f"inc{q}_H"]) < 1e-14, q
+
+
+def test_incident_fields_match_live_reference(vgolden, oracle_lib, ref_lib):
+    rng = np.random.default_rng(5)
+    P = rng.uniform(-2, 2, (30, 3))
+    for spec in (dict(kind=0, a=[0, 0, 1.5], b=[0.6, 0.8, 0.0]), dict(kind=1, a=[1, 2, 3], b=[0, 0, 0], is_magnetic=1)):
+        Eo, Ho = O.incident_fields(oracle_lib, spec, 7.0, 300.0, P)
+        Er, Hr = O.incident_fields(ref_lib, spec, 7.0, 300.0, P)
+        assert rel_err(Eo, Er) < 1e-14 and rel_err(Ho, Hr) < 1e-14
