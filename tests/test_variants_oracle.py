@@ -199,3 +199,18 @@ def test_incident_fields_match_live_reference(vgolden, oracle_lib, ref_lib):
         Eo, Ho = O.incident_fields(oracle_lib, spec, 7.0, 300.0, P)
         Er, Hr = O.incident_fields(ref_lib, spec, 7.0, 300.0, P)
         assert rel_err(Eo, Er) < 1e-14 and rel_err(Ho, Hr) < 1e-14
+
+
+@pytest.mark.parametrize("name,rule,thr,freq", [("n_pmchwt", 1, 0.3, 2), ("n_muller", 20, 0.1, 1),
+                                                ("n_efie_line", 3, 0.5, 1), ("n_mfie", 13, 0.6, 1),
+                                                ("n_pmchwt_line", 2, 0.3, 2)])
+def test_variant_oracle_matches_harness_across_rules(name, rule, thr, freq, golden, oracle_lib, ref_lib):
+    # Dunavant rules 1-20 (one point up to 79), thresholds from self pairs
+    # only to most neighbours.
+    kind, variant, media, lp = CASES[name]
+    m = GoldenMesh(golden, "L1r05")
+    s = O.kernel_scalars(kind, freq * C0, **media, threshold_lambda0=thr)
+    Zo = O.assemble(oracle_lib, kind, m, rule, s, variant=variant, line_points=lp)
+    Zr = O.assemble(ref_lib, kind, m, rule, s, fn="ref_assemble", variant=variant, threads=1, line_points=lp)
+    assert np.isfinite(Zr).all()
+    assert rel_err(Zo, Zr) < 1e-13
