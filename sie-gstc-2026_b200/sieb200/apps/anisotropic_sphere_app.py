@@ -309,6 +309,9 @@ def write_field_outputs(directory: Path, observations: ObservationSamples, field
 
 def write_solver_metrics(path: Path, case_id: str, currents, metrics: dict, basis: str,
                          rhs_seconds: float) -> None:
+    """solver_metrics.json with the reference's keys (anisotropic_sphere_app.cpp:551-607).
+    The batched solve assembles the right-hand sides together with the matrix
+    (both inside matrix_assembly_seconds), so run() reports rhs_assembly_seconds 0."""
     mc = metrics["maximum_coefficient"]
     text = ("{\n"
             "  \"schema_version\": 2,\n"
@@ -346,6 +349,8 @@ def write_solver_metrics(path: Path, case_id: str, currents, metrics: dict, basi
 
 
 def write_batch_metrics(path: Path, mesh, metrics: dict, cases, basis: str, preparation_seconds: float) -> None:
+    """batch_metrics.json with the reference's keys (anisotropic_sphere_app.cpp:609-652);
+    device_preparation_seconds is the host loading of mesh and records."""
     ids = ", ".join(f'"{c.id}"' for c in cases)
     text = ("{\n"
             "  \"schema_version\": 2,\n"
