@@ -121,3 +121,40 @@ def test_python_layer_rejects_bad_inputs():
         sieb200.solvers._tensor_array(mesh, np.zeros(31), True)
     with pytest.raises(ValueError):
         sieb200.solvers.to_c_options(sieb200.GstcSieOptions(frequency_hz=1.0, basis="polar"), 2)
+
+
+def test_header_compiles_as_c_and_links(tmp_path):
+    # A plain C caller (the reference-side binding of INTEGRATION.md) built
+    # with gcc against include/sieb200.h and the in-tree library: struct
+    # layout, defaults of the variant fields and two host-only entry points.
+    import subprocess
+    import sieb200
+    src = tmp_path / "caller.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include "sieb200.h"
+int main(void) {
+    sieb200_options o;
+    if (sieb200_options_default(SIEB200_PMCHWT, &o) != SIEB200_OK) return 1;
+    if (o.variant != SIEB200_VARIANT_T || o.ntl_form != SIEB200_NTL_SURFACE || o.line_quadrature_points != 20)
+        return 2;
+    if (o.quadrature_rule != 17 || o.solver != SIEB200_SOLVER_LU_CUSOLVER) return 3;
+    if (sieb200_quadrature_rule(20, NULL, NULL) != 79) return 4;
+    const int32_t faces[12] = {0, 1, 2, 0, 3, 1, 1, 3, 2, 2, 3, 0};
+    int32_t edges[24], fe[12];
+    int64_t ne = 0;
+    if (sieb200_build_edges(faces, 4, edges, fe, &ne) != SIEB200_OK || ne != 6) return 5;
+    printf("%d %zu\n", sieb200_version(), sizeof(sieb200_options));
+    return 0;
+}
+""")
+    lib = sieb200.library_path()
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(ROOT / "include"), str(src), "-o", str(exe),
+                        str(lib), f"-Wl,-rpath,{lib.parent}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    import ctypes
+    from sieb200 import _lib
+    assert int(r.stdout.split()[1]) == ctypes.sizeof(_lib.Options)
