@@ -40,6 +40,9 @@ enum {
 
 /* Thread-local message of the last failing call on this host thread. */
 const char* sieb200_last_error(void);
+/* ABI version of the declarations below; a binding checks it on load.
+ * 2: sieb200_options gained variant, ntl_form, line_quadrature_points. */
+#define SIEB200_ABI_VERSION 2
 int sieb200_version(void);
 
 /* ----------------------------------------------------------- context ---- */

@@ -460,7 +460,7 @@ using namespace sieb200;
 extern "C" {
 
 const char* sieb200_last_error(void) { return g_last_error.c_str(); }
-int sieb200_version(void) { return 1; }
+int sieb200_version(void) { return SIEB200_ABI_VERSION; }
 
 int sieb200_ctx_create(int device, sieb200_ctx** out) {
     SIEB_CHECK(out, SIEB200_INVALID_ARG, "output pointer must not be null");

@@ -20,6 +20,7 @@ OK, INVALID_ARG, OVERFLOW, SINGULAR, NONFINITE, NOT_CONVERGED, CUDA_ERROR, TIMEO
 VARIANT_T, VARIANT_N, VARIANT_N_JUMP = 0, 1, 2
 NTL_SURFACE, NTL_LINE = 0, 1
 PEC_EFIE, PMCHWT, GSTC = 0, 1, 2
+ABI_VERSION = 2  # SIEB200_ABI_VERSION of include/sieb200.h
 SOLVER_LU_FP64, SOLVER_LU_CUSOLVER, SOLVER_MIXED_IR, SOLVER_GMRES_C64 = 0, 1, 2, 3
 
 _STATUS_NAMES = {
@@ -151,6 +152,9 @@ def lib() -> ctypes.CDLL:
                 fn = getattr(handle, name)
                 fn.argtypes = args
                 fn.restype = res
+            if handle.sieb200_version() != ABI_VERSION:
+                raise RuntimeError(f"{path} implements C ABI version {handle.sieb200_version()}, this binding "
+                                   f"needs {ABI_VERSION}: rebuild the library")
             _lib = handle
         return _lib
 

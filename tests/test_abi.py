@@ -144,6 +144,7 @@ int main(void) {
     int32_t edges[24], fe[12];
     int64_t ne = 0;
     if (sieb200_build_edges(faces, 4, edges, fe, &ne) != SIEB200_OK || ne != 6) return 5;
+    if (sieb200_version() != SIEB200_ABI_VERSION) return 6;
     printf("%d %zu\n", sieb200_version(), sizeof(sieb200_options));
     return 0;
 }
