@@ -377,8 +377,9 @@ def write_batch_metrics(path: Path, mesh, metrics: dict, cases, basis: str, prep
     path.write_text(text)
 
 
-def run(a: Arguments, out=sys.stdout) -> int:
+def run(a: Arguments, out=None) -> int:
     """anisotropic_sphere_app.cpp:676-775 on the C ABI."""
+    out = out if out is not None else sys.stdout
     import sieb200
     from ..io import load_face_tensors, write_physical_currents
     t_prep = time.perf_counter()

@@ -263,10 +263,11 @@ def write_field_csv(path: Path, obs: Observations, E: np.ndarray, H: np.ndarray,
     path.write_text("\n".join(lines) + "\n")
 
 
-def evaluate_fields(mesh, j2: np.ndarray, a: Arguments, options, source, out=sys.stdout, ctx=None) -> None:
+def evaluate_fields(mesh, j2: np.ndarray, a: Arguments, options, source, out=None, ctx=None) -> None:
     """Incident minus the surface integral of J2 (M = 0) in region 2's medium
     (pec_sphere_app.cpp:279-312)."""
     import sieb200
+    out = out if out is not None else sys.stdout
     obs = make_observations(a, sphere_radius(mesh))
     print(f"Evaluating {obs.points.shape[0]} field points inside and outside the sphere...", file=out, flush=True)
     QE, QH = sieb200.evaluate_surface_integral_fields(mesh, j2, np.zeros_like(j2), obs.points, a.frequency_hz,
@@ -284,7 +285,9 @@ def evaluate_fields(mesh, j2: np.ndarray, a: Arguments, options, source, out=sys
         print(f"radial_fields_csv=\"{root / 'radial_fields.csv'}\"", file=out)
 
 
-def run(a: Arguments, out=sys.stdout) -> int:
+def run(a: Arguments, out=None) -> int:
+    """pec_sphere_app.cpp:317-388 on the C ABI."""
+    out = out if out is not None else sys.stdout
     import sieb200
     mesh = sieb200.load_obj(a.mesh_path)
     options = options_of(a)

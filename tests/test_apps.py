@@ -241,3 +241,87 @@ def test_pec_observations():
     assert np.allclose(o.points[9:, 2], [0.0, 1.0, 2.0]) and list(o.regions[9:]) == [1, 2, 2]
     o = make_observations(Arguments(zx_grid_size=0, radial_points=0), 1.0)
     assert o.points.shape == (0, 3)
+
+
+def _fake_library(monkeypatch, ne_blocks):
+    """Stand-ins for the GPU calls, so that run() is exercised on the CPU."""
+    import sieb200
+    from sieb200 import solvers
+
+    class _Ctx:
+        pass
+
+    monkeypatch.setattr(sieb200, "default_context", lambda: _Ctx())
+
+    def solve_batch(mesh, tensors, options, cases, ctx=None):
+        assert tensors.shape == (mesh.num_faces, 32) and options.basis in ("face", "spherical")
+        n = ne_blocks * mesh.num_edges
+        metrics = dict(matrix_dimension=n, dense_matrix_bytes=16 * n * n, assembly_seconds=0.5,
+                       factorization_seconds=0.25, solve_seconds=0.125, residual_seconds=0.0625,
+                       residual_computed=1, rhs_norm=2.0, absolute_residual=2e-15, relative_residual=1e-15,
+                       maximum_coefficient=[1.0, 2.0, 3.0, 4.0])
+        return [solvers.SolveResult(np.arange(n) * (1 + 1j) * (c + 1), dict(metrics)) for c in range(len(cases))]
+
+    def solve_pec(mesh, options, source, ctx=None):
+        return solve_batch(mesh, np.zeros((mesh.num_faces, 32)), sieb200.GstcSieOptions(), [None])[0]
+
+    monkeypatch.setattr(sieb200, "solve_gstc_dense_batch", solve_batch)
+    monkeypatch.setattr(sieb200, "solve_pec_dense", solve_pec)
+    monkeypatch.setattr(sieb200, "assemble_matrix",
+                        lambda mesh, options, ctx=None: np.eye(mesh.num_edges, dtype=complex))
+    monkeypatch.setattr(sieb200, "evaluate_surface_integral_fields",
+                        lambda mesh, j, m, P, *a, **k: (np.ones((len(P), 3), complex), np.zeros((len(P), 3), complex)))
+    monkeypatch.setattr(sieb200, "incident_fields",
+                        lambda P, src, options, ctx=None: (3 * np.ones((len(P), 3), complex),
+                                                           np.ones((len(P), 3), complex)))
+
+
+def test_anisotropic_run_writes_the_reference_file_set(tmp_path, monkeypatch, capsys):
+    import sieb200
+    from sieb200.apps.anisotropic_sphere_app import main
+    from sieb200.io import read_physical_currents, save_face_tensors
+    _fake_library(monkeypatch, 4)
+    mesh = sieb200.icosphere(0.5, 0)
+    sieb200.save_obj(mesh, tmp_path / "s.obj")
+    save_face_tensors(tmp_path / "t.bin", np.zeros((mesh.num_faces, 32)), single=True)
+    out = tmp_path / "run"
+    rc = main(["app", "--mesh", str(tmp_path / "s.obj"), "--tensors", str(tmp_path / "t.bin"), "--output-dir",
+               str(out), "--frequency-hz", "1e8", "--epsilon-r-interior", "2", "--mu-r-interior", "1",
+               "--epsilon-r-exterior", "1", "--mu-r-exterior", "1", "--case", "a",
+               "--plane-wave", "exterior", "1", "0", "0", "0", "0", "1", "--case", "b",
+               "--dipole", "interior", "electric", "0", "0", "1", "0", "0", "0",
+               "--zx-grid-size", "4", "--radial-points", "3"])
+    assert rc == 0
+    assert json.loads((out / "batch_metrics.json").read_text())["solver"]["matrix_dimension"] == 120
+    for c, case in enumerate(("a", "b")):
+        d = out / "cases" / case
+        assert np.array_equal(read_physical_currents(d / "currents.bin"), np.arange(120) * (1 + 1j) * (c + 1))
+        assert json.loads((d / "solver_metrics.json").read_text())["case_id"] == case
+        for rep in ("interior_representation", "exterior_representation", "physical"):
+            assert len((d / "fields" / f"sie_{rep}_zx.csv").read_text().splitlines()) == 17
+            assert len((d / "fields" / f"sie_{rep}_radial.csv").read_text().splitlines()) == 4
+        rows = np.loadtxt(d / "fields" / "sie_physical_radial.csv", delimiter=",", skiprows=1)
+        # incident (3) minus surface integral (1) in the source's region, 0 - 1 elsewhere
+        inside = rows[:, 4] == 1
+        expect_inside = 2.0 if case == "b" else -1.0
+        expect_outside = 2.0 if case == "a" else -1.0
+        assert np.all(rows[inside, 5] == expect_inside) and np.all(rows[~inside, 5] == expect_outside)
+    assert "Starting dense CUDA solve..." in capsys.readouterr().out
+
+
+def test_pec_run_writes_the_reference_file_set(tmp_path, monkeypatch):
+    import sieb200
+    from sieb200.apps.pec_sphere_app import main
+    _fake_library(monkeypatch, 1)
+    mesh = sieb200.icosphere(0.5, 0)
+    sieb200.save_obj(mesh, tmp_path / "s.obj")
+    out = tmp_path / "run"
+    assert main(["pec", "--mesh", str(tmp_path / "s.obj"), "--output-dir", str(out), "--frequency-hz", "1e8",
+                 "--export-matrix", "--zx-grid-size", "2", "--radial-points", "2"]) == 0
+    lines = (out / "currents.csv").read_text().splitlines()
+    assert lines[0] == "edge,J2_real,J2_imag,J2_abs" and lines[2] == "1,1,1,1.4142135623730951"
+    assert np.array_equal(np.load(out / "matrix.npy"), np.eye(30))
+    assert (out / "matrix_edges.csv").read_text().splitlines()[0] == "edge,vertex_a,vertex_b"
+    f = (out / "radial_fields.csv").read_text().splitlines()
+    assert f[1].split(",")[4] == "2.000000000000e+00" and len(f) == 3
+    assert len((out / "zx_fields.csv").read_text().splitlines()) == 5
