@@ -35,7 +35,8 @@ enum {
     SIEB200_TIMEOUT = 7,
     SIEB200_NO_DEVICE = 8,
     SIEB200_OUT_OF_MEMORY = 9,
-    SIEB200_UNSUPPORTED = 10     /* a reference option this library does not build */
+    SIEB200_UNSUPPORTED = 10     /* reserved: a reference option this library does not build
+                                    (every option of the declared entry points is built) */
 };
 
 /* Thread-local message of the last failing call on this host thread. */

@@ -104,6 +104,24 @@ def test_validation_errors_mirror_reference(field, value, msg):
     assert msg in _lib.lib().sieb200_last_error().decode()
 
 
+@pytest.mark.parametrize("over,msg", [
+    (dict(variant=3), "unknown formulation variant"),
+    (dict(ntl_form=2), "unknown nTL integral form"),
+    (dict(variant=2, ntl_form=1), "line nTL form requires N-EFIE"),
+    (dict(variant=0, ntl_form=1), "line nTL form requires N-EFIE"),
+    (dict(variant=1, ntl_form=1, line_quadrature_points=0), "Gauss-Legendre point count must be in [1, 20]"),
+    (dict(variant=1, ntl_form=1, line_quadrature_points=21), "Gauss-Legendre point count must be in [1, 20]"),
+])
+def test_variant_validation_mirrors_reference(over, msg):
+    # pec_solver.cu:91-97: checked before any device work (null context here)
+    import sieb200
+    from sieb200 import _lib
+    mesh = sieb200.icosphere(1.0, 0)
+    assert _call_solve(mesh, **over) == _lib.INVALID_ARG
+    assert msg in _lib.lib().sieb200_last_error().decode()
+    assert "context" not in _lib.lib().sieb200_last_error().decode()
+
+
 def test_null_context_is_rejected_after_validation():
     import sieb200
     from sieb200 import _lib
