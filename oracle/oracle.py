@@ -66,6 +66,7 @@ def reference() -> ctypes.CDLL | None:
     lib.ref_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _i, _P]
     lib.ref_gauss_legendre.argtypes = [_i, _P, _P]
     lib.ref_incident_fields.argtypes = [_i, _P, _P, _i, _d, _d, _i, _P, _P, _P]
+    lib.ref_rhs_dipole.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.ref_assemble.argtypes = _ASSEMBLE
     lib.ref_rhs_plane_wave.argtypes = [_i, _P, _P, _P, _i, _i, _i, _P, _P, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.ref_surface_fields.argtypes = _FIELDS

@@ -194,6 +194,57 @@ void pair_n_efie(const double* V, const int* F, int m, int n, const Quad& q, flo
     }
 }
 
+// Right-hand side of one source functor as the reference RHS kernels place it
+// (see ref_rhs_plane_wave).
+template <class Source>
+int rhs_source(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+               const Source& pw, int region, double mu0_d, double eps0_d, double* b, int variant,
+               double eps_r_src, double mu_r_src) {
+    const bool rotated = variant != 0;
+    const Quad q = make_rule(rule);
+    const size_t N = (kind == 0) ? ne : (kind == 1 ? 2 * (size_t)ne : 4 * (size_t)ne);
+    std::memset(b, 0, sizeof(double) * 2 * N);
+    for (int m = 0; m < nf; ++m) {
+        const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
+        vec3_t tv[3];
+        for (int a = 0; a < 3; ++a)
+            tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
+        complex_t ve[3], vh[3];
+        if (rotated)
+            calculateExcitationQuadrature<TestingFunction::NxRWG>(tv, ti, q.pts.data(), q.w.data(),
+                                                                  q.n, pw, ve, vh);
+        else
+            calculateExcitationQuadrature<TestingFunction::RWG>(tv, ti, q.pts.data(), q.w.data(),
+                                                                q.n, pw, ve, vh);
+        for (int i = 0; i < 3; ++i) {
+            const size_t e = FE[3 * m + i];
+            if (kind == 0 && variant == 2) {
+                atomic_add(b, e, vh[i]);
+            } else if (kind == 0) {
+                atomic_add(b, e, ve[i]);
+            } else if (kind == 1 && variant == 2) {
+                const real_t eta0 = std::sqrt(mu0_d / eps0_d);
+                const real_t scale_e = static_cast<real_t>(eps_r_src * eps0_d);
+                const real_t scale_h = -static_cast<real_t>(mu_r_src * mu0_d) * eta0;
+                atomic_add(b, e, complexScale(ve[i], scale_e));
+                atomic_add(b, e + ne, complexScale(vh[i], scale_h));
+            } else if (kind == 1) {
+                const real_t eta0 = std::sqrt(mu0_d / eps0_d);
+                const real_t sign = region == 2 ? real_t(1) : real_t(-1);
+                atomic_add(b, e, complexScale(ve[i], sign));
+                atomic_add(b, e + ne, complexScale(vh[i], sign * eta0));
+            } else {
+                const float mu0 = (float)mu0_d, eps0 = (float)eps0_d;
+                const real_t eta0 = sqrt(static_cast<real_t>(mu0) / static_cast<real_t>(eps0));
+                const size_t off = region == 1 ? 0 : 2 * (size_t)ne;
+                atomic_add(b, e + off, ve[i]);
+                atomic_add(b, e + off + ne, complexScale(vh[i], eta0));
+            }
+        }
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -544,54 +595,26 @@ int ref_rhs_plane_wave(int kind, const double* V, const int* F, const int* FE, i
                        int rule, const double* E0, const double* khat, double k, double eta,
                        int region, double mu0_d, double eps0_d, double* b, int variant,
                        double eps_r_src, double mu_r_src) {
-    const bool rotated = variant != 0;
-    const Quad q = make_rule(rule);
-    const size_t N = (kind == 0) ? ne : (kind == 1 ? 2 * (size_t)ne : 4 * (size_t)ne);
-    std::memset(b, 0, sizeof(double) * 2 * N);
     sie_mom::cuda::PlaneWave pw;
     pw.E0 = make_vec3(E0[0], E0[1], E0[2]);
     pw.propagation_k = make_vec3(khat[0], khat[1], khat[2]);
     pw.k = k;
     pw.eta = eta;
-    for (int m = 0; m < nf; ++m) {
-        const int ti[3] = {F[3 * m], F[3 * m + 1], F[3 * m + 2]};
-        vec3_t tv[3];
-        for (int a = 0; a < 3; ++a)
-            tv[a] = make_vec3(V[3 * ti[a]], V[3 * ti[a] + 1], V[3 * ti[a] + 2]);
-        complex_t ve[3], vh[3];
-        if (rotated)
-            calculateExcitationQuadrature<TestingFunction::NxRWG>(tv, ti, q.pts.data(), q.w.data(),
-                                                                  q.n, pw, ve, vh);
-        else
-            calculateExcitationQuadrature<TestingFunction::RWG>(tv, ti, q.pts.data(), q.w.data(),
-                                                                q.n, pw, ve, vh);
-        for (int i = 0; i < 3; ++i) {
-            const size_t e = FE[3 * m + i];
-            if (kind == 0 && variant == 2) {
-                atomic_add(b, e, vh[i]);
-            } else if (kind == 0) {
-                atomic_add(b, e, ve[i]);
-            } else if (kind == 1 && variant == 2) {
-                const real_t eta0 = std::sqrt(mu0_d / eps0_d);
-                const real_t scale_e = static_cast<real_t>(eps_r_src * eps0_d);
-                const real_t scale_h = -static_cast<real_t>(mu_r_src * mu0_d) * eta0;
-                atomic_add(b, e, complexScale(ve[i], scale_e));
-                atomic_add(b, e + ne, complexScale(vh[i], scale_h));
-            } else if (kind == 1) {
-                const real_t eta0 = std::sqrt(mu0_d / eps0_d);
-                const real_t sign = region == 2 ? real_t(1) : real_t(-1);
-                atomic_add(b, e, complexScale(ve[i], sign));
-                atomic_add(b, e + ne, complexScale(vh[i], sign * eta0));
-            } else {
-                const float mu0 = (float)mu0_d, eps0 = (float)eps0_d;
-                const real_t eta0 = sqrt(static_cast<real_t>(mu0) / static_cast<real_t>(eps0));
-                const size_t off = region == 1 ? 0 : 2 * (size_t)ne;
-                atomic_add(b, e + off, ve[i]);
-                atomic_add(b, e + off + ne, complexScale(vh[i], eta0));
-            }
-        }
-    }
-    return 0;
+    return rhs_source(kind, V, F, FE, nf, ne, rule, pw, region, mu0_d, eps0_d, b, variant, eps_r_src, mu_r_src);
+}
+
+// The same for a dipole (source_functors.cuh:51-130): moment, position, type.
+int ref_rhs_dipole(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+                   const double* moment, const double* position, int is_magnetic, double k, double eta,
+                   int region, double mu0_d, double eps0_d, double* b, int variant, double eps_r_src,
+                   double mu_r_src) {
+    sie_mom::cuda::DipoleSource d;
+    d.p_vec = make_vec3(moment[0], moment[1], moment[2]);
+    d.r_0 = make_vec3(position[0], position[1], position[2]);
+    d.k = k;
+    d.eta = eta;
+    d.is_magnetic = is_magnetic != 0;
+    return rhs_source(kind, V, F, FE, nf, ne, rule, d, region, mu0_d, eps0_d, b, variant, eps_r_src, mu_r_src);
 }
 
 // Surface-integral field values Q_E = j w mu L[J] + K[M], Q_H = -K[J] + j w eps L[M]

@@ -123,6 +123,21 @@ def main() -> None:
         out[f"inc{q}_H"] = H
         out[f"inc{q}_source"] = np.concatenate(([kind, mag], a, b))
     out["inc_points"] = P
+    # Dipole right-hand sides on the unit icosahedron, every formulation and
+    # testing variant, interior and exterior sources (rule 5, f = C0).
+    for kind, variant, region, mag in [(0, 0, 2, 0), (0, 1, 2, 1), (0, 2, 2, 0), (1, 0, 1, 1), (1, 1, 1, 0),
+                                       (1, 2, 1, 1), (1, 2, 2, 0), (2, 0, 1, 0), (2, 0, 2, 1)]:
+        er, mr = (2.5, 1.5) if region == 1 else (1.0, 1.0)
+        kd = 2 * np.pi * C0 * np.sqrt(1.25663706212e-6 * mr * 8.8541878128e-12 * er)
+        etad = np.sqrt(1.25663706212e-6 * mr / (8.8541878128e-12 * er))
+        mom = np.array([0.3, -0.2, 1.0])
+        pos = np.array([0.1, 0.0, 0.05]) if region == 1 else np.array([0.4, 1.8, -0.3])
+        bd = np.zeros(O.dimension(kind, L0.edges.shape[0]), np.complex128)
+        ref.ref_rhs_dipole(kind, L0.vertices.ctypes.data, L0.faces.ctypes.data, L0.faces_edges.ctypes.data,
+                           L0.faces.shape[0], L0.edges.shape[0], 5, mom.ctypes.data, pos.ctypes.data, mag,
+                           float(kd), float(etad), region, 1.25663706212e-6, 8.8541878128e-12, bd.ctypes.data,
+                           variant, er, mr)
+        out[f"bdip_{kind}_{variant}_{region}_{mag}"] = bd
     out["inc_k_eta"] = np.array([k, eta])
     out["pair_n_index"] = pairs
     out["pair_n_blocks"] = blocks

@@ -214,3 +214,20 @@ def test_variant_oracle_matches_harness_across_rules(name, rule, thr, freq, gold
     Zr = O.assemble(ref_lib, kind, m, rule, s, fn="ref_assemble", variant=variant, threads=1, line_points=lp)
     assert np.isfinite(Zr).all()
     assert rel_err(Zo, Zr) < 1e-13
+
+
+@pytest.mark.parametrize("kind,variant,region,mag", [(0, 0, 2, 0), (0, 1, 2, 1), (0, 2, 2, 0), (1, 0, 1, 1),
+                                                     (1, 1, 1, 0), (1, 2, 1, 1), (1, 2, 2, 0), (2, 0, 1, 0),
+                                                     (2, 0, 2, 1)])
+def test_dipole_rhs_matches_reference(kind, variant, region, mag, vgolden, oracle_lib, mesh_l0):
+    # The oracle's dipole right-hand sides (every formulation, testing variant
+    # and region) against the reference's DipoleSource through its own
+    # calculateExcitationQuadrature and the RHS placements.
+    er, mr = (2.5, 1.5) if region == 1 else (1.0, 1.0)
+    mu0, eps0 = 1.25663706212e-6, 8.8541878128e-12
+    k = 2 * math.pi * C0 * math.sqrt(mu0 * mr * eps0 * er)
+    eta = math.sqrt(mu0 * mr / (eps0 * er))
+    pos = [0.1, 0.0, 0.05] if region == 1 else [0.4, 1.8, -0.3]
+    b = O.rhs(oracle_lib, kind, mesh_l0, 5, dict(kind=1, a=[0.3, -0.2, 1.0], b=pos, is_magnetic=mag, region=region),
+              k, eta, mu0, eps0, variant=variant, eps_r_src=er, mu_r_src=mr)
+    assert rel_err(b, vgolden[f"bdip_{kind}_{variant}_{region}_{mag}"]) < 1e-13
