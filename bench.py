@@ -46,9 +46,9 @@ C0 = 299792458.0
 METRIC = "solves/s mixed-prec+IR vs FP64 LU at rel.res≤1e-10 (1 B200); adjoint grads/s"
 WORKLOAD = ("T-PMCHWT dielectric sphere r=0.5 m, eps_r=4, mu_r=1, ka=pi; geodesic mesh 2000 faces / "
             "3000 RWG edges (N=6000); Dunavant rule 17; 1 plane-wave RHS")
-# DRAM bytes (read + write) per trailing-update launch, mean over the 92 launches of one
-# factorization of this workload, from one ncu capture
-# (profiles/gemm_tf32_sub_persistent_kernel_pmchwt_n6000.md, section 2).
+# DRAM bytes (read + write) per trailing-update launch, mean over the 92
+# launches of one factorization of this workload, from one ncu capture of
+# the trailing GEMM (dram__bytes_read.sum + dram__bytes_write.sum).
 GEMM_DRAM_BYTES_PER_LAUNCH = 163.7e6
 # FP64 flops per Green evaluation (one point pair, one wavenumber) of the
 # T-PMCHWT regular pass, counted from the kernel's source with an FMA as 2:
@@ -83,55 +83,111 @@ def build_problem(rule: int = 17):
     return mesh, opts
 
 
-class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+def bench_config(world: int) -> dict:
+    """The workload key both arms print (the driver compares them)."""
+    return {"workload": WORKLOAD, "N": 6000, "rule": 17, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (Z complex128 576 MB resident)"}
 
+
+class ClockSampler:
+    """SM clocks, power and clock-event reasons sampled during the timed
+    region: NVML polled every 10 ms from a thread (so that a short region
+    still gets many samples), nvidia-smi at 200 ms when NVML is missing."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.01):
         self.index = index
-        self.rows = []
+        self.period = period_s
+        self.rows = []  # (sm_mhz, max_mhz, power_w, reasons)
         self.proc = None
+        self.thread = None
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = u.decode() if isinstance(u, bytes) else u
+                if u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                    return pynvml, h
+        except Exception:
+            pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll_nvml(self, nv, h):
+        reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1e3
+                bits = reasons_fn(h)
+                self.rows.append((float(sm), float(mx), pw, [n for b, n in self.REASONS.items() if bits & b]))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
+
+    def _read_smi(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.proc.stdout:
+            r = [x.strip() for x in line.split(",")]
+            if len(r) > 8 and r[1].replace(".", "").isdigit():
+                reasons = [nm for nm, v in zip(names, r[5:9]) if v.lower() == "active"]
+                pw = float(r[3]) if r[3].replace(".", "").isdigit() else None
+                self.rows.append((float(r[1]), float(r[2]), pw, reasons))
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.source = "nvml 10 ms"
+            self.thread = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi 200 ms"
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
-
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
-    def summary(self, power_floor: float = 0.0) -> dict:
+    def summary(self) -> dict:
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            if len(r) > 8:
-                for nm, v in zip(names, r[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        pw = [r[2] for r in self.rows if r[2] is not None]
+        reasons = sorted({n for r in self.rows for n in r[3]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in self.rows),
+                "sm_min_mhz": min(sm), "power_w_median": statistics.median(pw) if pw else None,
+                "reasons": reasons, "samples": len(self.rows), "sampler": self.source}
 
 
 def measured_peaks() -> dict:
@@ -158,20 +214,27 @@ def cpu_reference_solve(Zh: np.ndarray, bh: np.ndarray, threads: int):
 
 
 def run_reference(args):
+    """The reference's CPU solve of the benchmark system, on the host cores.
+
+    Nothing of this library is loaded: the sphere comes from the oracle's own
+    generator (vertex- and index-equal to the library's), the system and the
+    right-hand side from the reference's host quadrature (oracle/_ref), the
+    solve is the reference's Eigen PartialPivLU."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     from oracle import oracle as O
     ref = O.reference()
-    mesh, _ = build_problem()
-    threads = os.cpu_count() or 1
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference host build (oracle/_ref) missing"}))
         return
-    # The reference's host assembly of this system (rule 17: ~3e10 Green
-    # evaluations) is far beyond a bounded CPU sample; the LU cost does not
-    # depend on the rule, so the system solved here is assembled by the
-    # reference harness with Dunavant rule 1 (same matrix size and structure).
+    mesh = O.geodesic_sphere(0.5, 10)
+    threads = os.cpu_count() or 1
+    # The reference's host assembly of this system at rule 17 (~3e10 Green
+    # evaluations) is far beyond a bounded CPU sample. The LU does not depend
+    # on the rule, so the solved system is assembled with Dunavant rule 1:
+    # same size, same block structure, same operator.
     s = O.kernel_scalars(1, C0, eps_r=(4.0, 1.0))
     t0 = time.perf_counter()
     Z = O.assemble(ref, 1, mesh, 1, s, threads=threads, fn="ref_assemble")
@@ -185,25 +248,30 @@ def run_reference(args):
     ref.ref_rhs_plane_wave(1, V.ctypes.data, mesh.faces.ctypes.data, mesh.faces_edges.ctypes.data,
                            mesh.num_faces, mesh.num_edges, 17, E0.ctypes.data, kh.ctypes.data, k, eta, 2,
                            s["mu0"], s["eps0"], b.ctypes.data, 0, 1.0, 1.0)
+    steps = args.steps if args.steps is not None else 20
     times = []
-    for i in range(args.warmup + args.steps):
+    x = None
+    for i in range(args.warmup + steps):
         secs, x, kind, desc = cpu_reference_solve(Z, b, threads)
         if i >= args.warmup:
             times.append(secs)
     tot = sum(times)
     value = len(times) / tot
     rres = float(np.linalg.norm(Z @ x - b) / np.linalg.norm(b))
-    sample = (f"one full N={Z.shape[0]} complex128 factor+solve per step; system assembled by the reference "
-              f"harness with Dunavant rule 1 in {t_asm:.1f} s (LU cost independent of the rule)")
+    sample = (f"one full N={Z.shape[0]} complex128 factor+solve per step ({desc}), {threads} host threads")
     print(json.dumps({
-        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "host CPU path"}, "impl": "reference",
+        "config": bench_config(world), "impl": "reference",
+        "solved_system": {"assembly": "reference host quadrature, Dunavant rule 1 (the LU cost does not depend "
+                                      "on the rule; rule 17 on the host is ~3e10 Green evaluations)",
+                          "assembly_seconds": t_asm, "N": int(Z.shape[0]), "faces": mesh.num_faces,
+                          "edges": mesh.num_edges},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "relative_residual": rres,
-    }))
+    }), flush=True)
 
 
 def run(args):
@@ -233,6 +301,31 @@ def run(args):
         return float(t.item())
 
     ctx = sieb200.Context(local)
+    try:
+        out = measure(args, ctx, rank, world, local, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        # Orderly teardown: every tensor and solver of measure() is gone once
+        # it returns; free torch's cached blocks (some were last used on the
+        # library's stream) while that stream still exists, then the context.
+        import gc
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+
+
+def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_ranks) -> dict:
+    """The timed work of one rank; returns rank 0's JSON line as a dict."""
+    import torch
+
+    import sieb200
+
+    if args.steps is None:
+        args.steps = 200
     stream = torch.cuda.ExternalStream(ctx.stream)
     mesh, opts = build_problem(args.rule)
     N = 2 * mesh.num_edges
@@ -418,6 +511,7 @@ def run(args):
         cpu = {"value": 1.0 / secs, "unit": "solves/s", "cores": threads, "kind": kind,
                "sample": f"one N={N} complex128 factor+solve of the same assembled system ({desc})"}
 
+    out = {}
     if rank == 0:
         peaks = measured_peaks()
         gemm_s = gemm["ms"] / 1e3
@@ -427,10 +521,23 @@ def run(args):
         tf32_peak = peaks["bf16_tflops"] / 2.0
         gemm_tflops = gemm["flops"] / gemm_s / 1e12 if gemm_s > 0 else 0.0
         gemm_gbs = gemm["bytes"] / gemm_s / 1e9 if gemm_s > 0 else 0.0
+        # Which roof binds: the kernel's algorithmic intensity (flops per
+        # byte of C read and written plus the packed operands) against the
+        # ridge of the two measured peaks.
+        intensity = gemm["flops"] / gemm["bytes"] if gemm["bytes"] else 0.0
+        ridge = tf32_peak * 1e12 / (peaks["hbm_gbs"] * 1e9)
+        hbm_bound = intensity < ridge
         roofline = {
             "kernel": "gemm_tf32_sub_persistent_kernel (split-TF32 trailing update, tcgen05)",
-            "bound": "tensor", "achieved": gemm_tflops, "peak": tf32_peak, "unit": "TFLOP/s",
-            "frac": gemm_tflops / tf32_peak, "traffic": GEMM_DRAM_BYTES_PER_LAUNCH,
+            "bound": "hbm" if hbm_bound else "tensor",
+            "achieved": gemm_gbs if hbm_bound else gemm_tflops,
+            "peak": peaks["hbm_gbs"] if hbm_bound else tf32_peak,
+            "unit": "GB/s" if hbm_bound else "TFLOP/s",
+            "frac": gemm_gbs / peaks["hbm_gbs"] if hbm_bound else gemm_tflops / tf32_peak,
+            "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
+            "tensor_tflops_achieved": gemm_tflops, "tensor_peak_tflops": tf32_peak,
+            "tensor_frac": gemm_tflops / tf32_peak,
+            "traffic": GEMM_DRAM_BYTES_PER_LAUNCH,
             "traffic_note": "mean dram read+write bytes per trailing-update launch, ncu over the 92 "
                             "launches of one N=6000 factorization",
             "algorithmic_bytes_per_launch": gemm["bytes"] / gemm["launches"] if gemm["launches"] else None,
@@ -449,8 +556,7 @@ def run(args):
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64+tf32x3/c128", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "N": N, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (Z complex128 576 MB resident)"},
+            "config": bench_config(world),
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": world * e2e_steps / t_e2e, "unit": "solves/s",
                     "h2d_bytes_per_step": int(16 * N * N + 16 * N), "d2h_bytes_per_step": int(16 * N),
@@ -473,14 +579,8 @@ def run(args):
             "adjoint": adjoint,
             "variants": variants,
         }
-        print(json.dumps(out), flush=True)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.destroy_process_group()
-    # Leave without running destructors of tensors that were used on the
-    # library's stream after that stream is gone.
-    sys.stderr.flush()
-    os._exit(0)
+    return out if rank == 0 else {}
 
 
 ADJOINT_WORKLOAD = ("SIE-GSTC adjoint synthesis: circular-arc spindle (arc radius 1.5 m, half-angle 60 deg), "
@@ -591,7 +691,8 @@ def adjoint_section(ctx, steps: int, max_over_ranks):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 200; the reference arm, one CPU solve per step, 20)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sieb200", choices=["sieb200", "reference"])
     ap.add_argument("--rule", type=int, default=17)

@@ -268,9 +268,13 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
  * its partial sums go to one fixed 2 MiB device array per device instead of
  * a per-call workspace, for callers that may not allocate device memory at
  * the point of the call. n <= 131072, else SIEB200_INVALID_ARG. The first
- * call on a device resolves the array's address (cudaGetSymbolAddress) and
- * should come before any stream capture. Calls whose kernels overlap in time
- * on one device (two host threads, two contexts) race on the array.
+ * call on a device does the set-up: it resolves the array's address
+ * (cudaGetSymbolAddress) and loads this path's kernels onto the device
+ * (lazy module loading would otherwise load them, and may allocate, at their
+ * first launch); make that first call before any stream capture. After a
+ * device reset the next call does the set-up again. Calls whose kernels
+ * overlap in time on one device (two host threads, two contexts) race on
+ * the array.
  * Synchronizes the context stream like sieb200_matvec. */
 int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                            const double* x, double beta, double* y);

@@ -198,3 +198,119 @@ def incident_fields(lib, source: dict, k: float, eta: float, points):
     fn(int(source["kind"]), _p(a), _p(b), int(source.get("is_magnetic", 0)), float(k), float(eta), P.shape[0],
        _p(P), _p(E), _p(H))
     return E, H
+
+
+# ------------------------------------------------------------------ meshes
+# The synthetic spheres of the benchmark workloads, generated here without
+# the library so that the reference arm of the benchmark and the checks that
+# compare against it never load libsieb200.so. Construction (the same as the
+# library's generator, asserted vertex- and index-equal by the tests):
+# SphericalSurface's icosahedron (src/sie_mom/mesh/spherical_surface.cpp:19-80),
+# each face split on a barycentric grid of the given frequency, projected to
+# the sphere by multiplying with the reciprocal length, faces oriented CCW
+# outward, RWG edges numbered by first appearance (so_build_edges).
+
+class OracleMesh:
+    def __init__(self, vertices: np.ndarray, faces: np.ndarray):
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
+        self.faces = np.ascontiguousarray(faces, dtype=np.int32)
+        nf = self.faces.shape[0]
+        fe = np.zeros((nf, 3), np.int32)
+        tmp = np.zeros((3 * nf, 2), np.int32)
+        ne = oracle().so_build_edges(_p(self.faces), nf, _p(tmp), _p(fe))
+        self.edges = tmp[:ne].copy()
+        self.faces_edges = fe
+
+    @property
+    def num_faces(self) -> int:
+        return int(self.faces.shape[0])
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.edges.shape[0])
+
+
+def _unit(v: np.ndarray) -> np.ndarray:
+    inv = 1.0 / np.sqrt(v[..., 0] * v[..., 0] + v[..., 1] * v[..., 1] + v[..., 2] * v[..., 2])
+    return v * inv[..., None]
+
+
+def _outward(vertices: np.ndarray, faces: np.ndarray) -> None:
+    v0, v1, v2 = (vertices[faces[:, i]] for i in range(3))
+    n = np.cross(v1 - v0, v2 - v0)
+    c = (v0 + v1 + v2) / 3.0
+    flip = np.einsum("ij,ij->i", n, c) < 0
+    faces[flip, 1], faces[flip, 2] = faces[flip, 2].copy(), faces[flip, 1].copy()
+
+
+def _icosahedron():
+    phi = (1.0 + np.sqrt(5.0)) / 2.0
+    V = np.array([(-1, phi, 0), (1, phi, 0), (-1, -phi, 0), (1, -phi, 0), (0, -1, phi), (0, 1, phi),
+                  (0, -1, -phi), (0, 1, -phi), (phi, 0, -1), (phi, 0, 1), (-phi, 0, -1), (-phi, 0, 1)],
+                 dtype=np.float64)
+    F = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+                  (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+                  (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)], dtype=np.int32)
+    V = _unit(V)
+    _outward(V, F)
+    return V, F
+
+
+def geodesic_sphere(radius: float, frequency: int) -> OracleMesh:
+    """Class-I geodesic sphere: 20 n^2 faces, 30 n^2 edges."""
+    BV, BF = _icosahedron()
+    n = int(frequency)
+    index: dict[tuple, int] = {}
+    verts: list[np.ndarray] = []
+
+    def vid(face, i: int, j: int) -> int:
+        corners = ((int(face[0]), n - i - j), (int(face[1]), i), (int(face[2]), j))
+        key = tuple(sorted((c, w) for c, w in corners if w > 0))
+        if key not in index:
+            p = 0
+            for c, w in corners:
+                p = p + BV[c] * (w / n)
+            verts.append(_unit(p) * radius)
+            index[key] = len(verts) - 1
+        return index[key]
+
+    faces = []
+    for face in BF:
+        for i in range(n):
+            for j in range(n - i):
+                faces.append((vid(face, i, j), vid(face, i + 1, j), vid(face, i, j + 1)))
+                if i + j < n - 1:
+                    faces.append((vid(face, i + 1, j), vid(face, i + 1, j + 1), vid(face, i, j + 1)))
+    V = np.array(verts)
+    F = np.array(faces, dtype=np.int32)
+    _outward(V, F)
+    return OracleMesh(V, F)
+
+
+def icosphere(radius: float, level: int) -> OracleMesh:
+    """SphericalSurface(radius, level): 20 * 4^level faces, midpoints
+    normalised, float radius (spherical_surface.cpp:19-80)."""
+    BV, _ = _icosahedron()
+    V = list(BV)
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+         (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+         (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        cache: dict[tuple[int, int], int] = {}
+
+        def mid(i: int, j: int) -> int:
+            key = (min(i, j), max(i, j))
+            if key not in cache:
+                V.append(_unit((V[i] + V[j]) * 0.5))
+                cache[key] = len(V) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in F:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca)]
+        F = nf
+    verts = np.array(V) * float(np.float32(radius))
+    faces = np.array(F, dtype=np.int32)
+    _outward(verts, faces)
+    return OracleMesh(verts, faces)

@@ -4,6 +4,7 @@
 // (src/sie_mom/solvers/gstc_sie.cu:398-457), and the solver object that
 // dispatches to the mixed-precision path (mixed.cu).
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -160,21 +161,68 @@ static __device__ __align__(256) cplx g_static_scratch[kStaticScratchElems];
 
 namespace {
 std::mutex g_static_scratch_mu;
-void* g_static_scratch_ptr[64] = {};  // device address of the array, per device
+// Per device: the array's device address and the id of the CUDA context it
+// was resolved in. A device reset (cudaDeviceReset) ends that context and
+// unloads the module, so a later call under a new context resolves again.
+struct StaticScratchSlot {
+    void* ptr = nullptr;
+    unsigned long long ctx_id = 0;
+};
+StaticScratchSlot g_static_scratch_slot[64];
+
+typedef CUresult (*PFN_ctxGetCurrent)(CUcontext*);
+typedef CUresult (*PFN_ctxGetId)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current CUDA context (0 if it cannot be read).
+unsigned long long current_context_id() {
+    static PFN_ctxGetCurrent get_current = nullptr;
+    static PFN_ctxGetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PFN_ctxGetCurrent>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_ctxGetId>(fn);
+        looked_up = true;
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS)
+        return id;
+    return 0;
+}
 }  // namespace
 
 int static_scratch_setup(int device, cplx** out) {
     SIEB_CHECK(device >= 0 && device < 64, SIEB200_INVALID_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-    if (!g_static_scratch_ptr[device]) {
-        // Called with `device` current: resolves this device's instance of
-        // the array (the first call per device may load the module).
+    StaticScratchSlot& slot = g_static_scratch_slot[device];
+    // The caller has made `device` current; its CUDA context exists (the
+    // library context owns a stream there).
+    const unsigned long long id = current_context_id();
+    if (!slot.ptr || slot.ctx_id != id) {
+        // This device's instance of the array; the first resolution loads the
+        // module on the device.
         void* p = nullptr;
         SIEB_TRY_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
         SIEB_CHECK(p != nullptr, SIEB200_CUDA_ERROR, "cudaGetSymbolAddress returned no address");
-        g_static_scratch_ptr[device] = p;
+        // With lazy loading (the default since CUDA 12.2) a kernel's code is
+        // put on the device at its first launch, which can allocate device
+        // memory; querying the three kernels of this path loads them now, in
+        // the set-up call.
+        cudaFuncAttributes fa;
+        SIEB_TRY_CUDA(cudaFuncGetAttributes(&fa, gemv_partial_kernel<double2>));
+        SIEB_TRY_CUDA(cudaFuncGetAttributes(&fa, gemv_partial_kernel<float2>));
+        SIEB_TRY_CUDA(cudaFuncGetAttributes(&fa, gemv_finish_kernel));
+        slot.ptr = p;
+        slot.ctx_id = id;
     }
-    *out = static_cast<cplx*>(g_static_scratch_ptr[device]);
+    *out = static_cast<cplx*>(slot.ptr);
     return SIEB200_OK;
 }
 
@@ -193,6 +241,9 @@ int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64
     const int64_t cpc = (n + chunks - 1) / chunks;
     chunks = (n + cpc - 1) / cpc;
     const dim3 grid((unsigned)row_blocks, (unsigned)chunks);
+    cudaEvent_t ev;
+    ctx->prof.begin(ctx->stream, 2, 8.0 * (double)n * (double)n,
+                    (prec == 0 ? 16.0 : 8.0) * (double)n * (double)n + 16.0 * 3.0 * n, &ev);
     if (prec == 0)
         gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(n, static_cast<const double2*>(A), lda, x,
                                                                           cpc, scratch);
@@ -203,6 +254,7 @@ int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64
     SIEB_TRY_CUDA(cudaGetLastError());
     gemv_finish_kernel<<<(unsigned)row_blocks, threads, 0, ctx->stream>>>(n, (int)chunks, scratch, beta, y);
     SIEB_NOTE_LAUNCH();
+    ctx->prof.end(ctx->stream, ev);
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;
 }

@@ -43,7 +43,9 @@ int main() {
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIE_REFERENCE")
+    if not ref:
+        raise SystemExit("usage: gen_dunavant_table.py /path/to/reference (or set SIE_REFERENCE)")
     src = os.path.join(ref, "src/sie_mom/quadrature/triangle_dunavant_rule.cpp")
     with tempfile.TemporaryDirectory() as tmp:
         dump = os.path.join(tmp, "dump.cpp")

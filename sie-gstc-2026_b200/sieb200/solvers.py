@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import threading
+import weakref
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -178,6 +179,8 @@ class Context:
         self._h = ctypes.c_void_p()
         _lib.check(_lib.lib().sieb200_ctx_create(int(device), ctypes.byref(self._h)))
         self.device = device
+        # Solvers made on this context; closed before it (they use its stream).
+        self._solvers = weakref.WeakSet()
 
     @property
     def handle(self) -> ctypes.c_void_p:
@@ -226,6 +229,8 @@ class Context:
 
     def close(self) -> None:
         if self._h:
+            for solver in list(self._solvers):
+                solver.close()
             _lib.lib().sieb200_ctx_destroy(self._h)
             self._h = ctypes.c_void_p()
 
@@ -425,6 +430,7 @@ class DenseLuSolver:
         self._h = ctypes.c_void_p()
         _lib.check(_lib.lib().sieb200_dense_solver_create(self.ctx.handle, int(n), SOLVERS[method],
                                                           ctypes.byref(self._h)))
+        self.ctx._solvers.add(self)
         self.n = n
         self.last_iterations = 0
 
@@ -442,9 +448,10 @@ class DenseLuSolver:
         return it.value
 
     def close(self) -> None:
-        if self._h:
+        # A solver whose context is already closed has nothing left to free.
+        if self._h and self.ctx.handle:
             _lib.lib().sieb200_dense_solver_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:

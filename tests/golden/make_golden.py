@@ -1,7 +1,8 @@
 """Regenerate tests/golden/golden.npz from the reference implementation itself.
 
-Run in a checkout that has the reference sources (default /root/reference):
-    python tests/golden/make_golden.py [/path/to/reference]
+Run in a checkout that has the reference sources, named by the first
+argument or the SIE_REFERENCE environment variable:
+    python tests/golden/make_golden.py /path/to/reference
 
 Sources of truth:
   * oracle/_ref/libsieref.so: the reference's own host-compiled quadrature
@@ -72,8 +73,17 @@ def reference_far_field(refdir: Path, mesh, currents, frequency_hz, theta, phi):
         return r_hat, th_hat, ph_hat, ft, fp, U, ev.k0, ev.eta0
 
 
+def reference_dir() -> Path:
+    """The reference checkout: first argument, else $SIE_REFERENCE."""
+    import os
+    d = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIE_REFERENCE")
+    if not d:
+        raise SystemExit("name the reference checkout: make_golden.py /path/to/reference (or set SIE_REFERENCE)")
+    return Path(d)
+
+
 def main() -> None:
-    refdir = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    refdir = reference_dir()
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "ref", f"REF={refdir}"], check=True)
     ref = O.reference()
     assert ref is not None, "reference harness did not build"

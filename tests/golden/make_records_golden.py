@@ -2,7 +2,7 @@
 surface-record preparation (src/sie_mom/gstc/tensor_io.py, imported from the
 reference checkout; pure numpy/scipy).
 
-    python tests/golden/make_records_golden.py [/path/to/reference]
+    python tests/golden/make_records_golden.py /path/to/reference   (or $SIE_REFERENCE)
 
 Seeded inputs: 64 reciprocal lossless maps with an ill-scaled spectrum, 32
 reciprocal complex maps, 16 diagonal lossless maps; each case stores the four
@@ -11,12 +11,13 @@ reciprocal complex maps, 16 diagonal lossless maps; each case stores the four
 
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIE_REFERENCE", ""))
 OUT = Path(__file__).resolve().parent / "records_golden.npz"
 ETA = 376.730313668
 
@@ -62,6 +63,8 @@ def complex_maps(rng, F):
 
 
 def main() -> None:
+    if not str(REF) or str(REF) == ".":
+        raise SystemExit("name the reference checkout: make_records_golden.py /path/to/reference (or set SIE_REFERENCE)")
     sys.path.insert(0, str(REF / "src"))
     from sie_mom.gstc import SurfaceParameters
     from sie_mom.gstc.tensor_io import prepare_tensor_records

@@ -142,7 +142,7 @@ def test_python_layer_rejects_bad_inputs():
 
 
 def test_header_compiles_as_c_and_links(tmp_path):
-    # A plain C caller (the reference-side binding of INTEGRATION.md) built
+    # A plain C caller (what a reference-side binding compiles against) built
     # with gcc against include/sieb200.h and the in-tree library: struct
     # layout, defaults of the variant fields and two host-only entry points.
     import subprocess

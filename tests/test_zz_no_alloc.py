@@ -55,3 +55,29 @@ def test_noalloc_matvec_rejects_oversize(gpu_ctx):
                                     y.data_ptr())
     assert st == _lib.INVALID_ARG
     assert b"131072" in lib.sieb200_last_error()
+
+
+def test_noalloc_matvec_allocates_nothing(gpu_ctx):
+    """After the set-up call, further calls leave the device's free memory
+    unchanged (no cudaMalloc, no lazily loaded kernel code) and launch exactly
+    the two kernels of the matvec each."""
+    import torch
+    from sieb200 import _lib
+    lib = _lib.lib()
+    n = 4096
+    rng = np.random.default_rng(7)
+    A = torch.from_numpy(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).cuda()
+    x = torch.from_numpy(rng.standard_normal(n) + 1j * rng.standard_normal(n)).cuda()
+    ys = [torch.empty(n, dtype=torch.complex128, device="cuda") for _ in range(4)]
+    _call(lib.sieb200_matvec_noalloc, gpu_ctx, n, A, n, 0, x, 0.0, ys[0])  # set-up call
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    launches0 = lib.sieb200_launch_count()
+    for y in ys[1:]:
+        _call(lib.sieb200_matvec_noalloc, gpu_ctx, n, A, n, 0, x, 0.0, y)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes"
+    assert lib.sieb200_launch_count() - launches0 == 2 * (len(ys) - 1)
+    for y in ys[1:]:
+        assert torch.equal(y, ys[0])
