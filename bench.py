@@ -421,6 +421,10 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
     rel_res = float(torch.linalg.vector_norm(r).item() / torch.linalg.vector_norm(b).item())
     x_mixed = x.clone()
 
+    # The solved sphere against the Mie series (discretization error of the
+    # far field; physical currents from the public solver call).
+    mie_err = rcs_error_vs_mie(ctx, mesh, opts, 0.5, 4.0)
+
     # FP64 LU (cuSOLVER) on the same system, for the speed-up and the error.
     fp64 = sieb200.DenseLuSolver(N, "lu_cusolver", ctx=ctx)
     Zw = torch.empty_like(Z)
@@ -500,6 +504,9 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
     # CPU baseline (rank 0, one GPU only): the reference's CPU solve of this system.
     fields = fields_section(ctx, mesh, fp64_peak, with_cpu=(rank == 0 and world == 1 and not args.no_cpu))
     adjoint = adjoint_section(ctx, args.adjoint_steps, max_over_ranks) if args.adjoint_steps > 0 else None
+    with_cpu = rank == 0 and world == 1 and not args.no_cpu
+    pec = pec_section(ctx, with_cpu) if not args.skip_sections else None
+    multi = multi_rhs_section(ctx, fp64_peak, max_over_ranks) if not args.skip_sections else None
     if adjoint is not None:
         adjoint["grads_per_s"] *= world
         adjoint["fp64_grads_per_s"] *= world
@@ -565,6 +572,7 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
             "gpu_launches": int(launches), "clocks": clocks.summary(),
             "fp64_lu_solves_per_s": world / t_fp64, "speedup_vs_fp64_lu": (value / world) * t_fp64,
             "relative_residual": rel_res, "rel_diff_vs_fp64_lu": rel_diff,
+            "rcs_rel_rms_error_vs_mie": mie_err,
             "refinement_iterations": max(iters), "assembly_seconds": t_asm,
             "assembly_green_evals_per_s": evals / t_asm,
             "assembly_roofline": {
@@ -576,6 +584,8 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
                 "z_write_gbs": 16.0 * N * N / t_asm / 1e9,
             },
             "fields": fields,
+            "pec_efie": pec,
+            "multi_rhs": multi,
             "adjoint": adjoint,
             "variants": variants,
         }
@@ -630,6 +640,234 @@ def fields_section(ctx, mesh, fp64_peak: float, with_cpu: bool) -> dict:
                                     "sample": f"{sample.shape[0]} of the cut's points, the reference's own "
                                               "per-face helpers on one host thread (oracle/_ref)"}
     return out
+
+
+def rcs_error_vs_mie(ctx, mesh, opts, radius: float, eps_r) -> dict:
+    """Relative RMS difference of the bistatic RCS (181 theta in the phi = 0
+    and 90 degree cuts) of the mixed solve from the Mie series (oracle/mie.py,
+    pinned to the reference's spherical-wave solver); eps_r None: PEC."""
+    import dataclasses as dc
+    import sieb200
+    from oracle import mie
+    o = dc.replace(opts, solver="mixed_ir")
+    if eps_r is None:
+        r = sieb200.solve_pec_dense(mesh, o, sieb200.PlaneWaveExcitation(), ctx=ctx)
+        J, M = r.currents, None
+    else:
+        r = sieb200.solve_dielectric_dense(mesh, o, sieb200.PlaneWaveExcitation(), ctx=ctx)
+        J, M = r.currents[:mesh.num_edges], r.currents[mesh.num_edges:]
+    mu0, eps0 = 1.25663706212e-6, 8.8541878128e-12
+    k = 2 * math.pi * C0 * math.sqrt(mu0 * eps0)
+    eta = math.sqrt(mu0 / eps0)
+    th = np.linspace(0.0, np.pi, 181)
+    num = den = 0.0
+    for phi in (0.0, np.pi / 2):
+        ph = np.full_like(th, phi)
+        r_hat, t_hat, p_hat = sieb200.spherical_frames(th, ph)
+        ft, fp, _ = sieb200.far_field(mesh, J, M, k, eta, r_hat, t_hat, p_hat, ctx=ctx)
+        rcs = 4 * np.pi * (np.abs(ft) ** 2 + np.abs(fp) ** 2)
+        ref = mie.bistatic_rcs(k, radius, eps_r, th, ph)
+        num += float(np.sum((rcs - ref) ** 2))
+        den += float(np.sum(ref ** 2))
+    return math.sqrt(num / den)
+
+
+PEC_WORKLOAD = ("PEC sphere r=1 m, T-EFIE, SphericalSurface(1, 3): 1280 faces / 1920 RWG edges (N=1920), "
+                "k=2 pi (f=c0), Dunavant rule 5 (7 points), threshold 0.1 lambda0, x-polarised plane wave along +z, "
+                "bistatic RCS at 181 theta in the phi=0 and phi=90 deg cuts")
+
+
+def pec_section(ctx, with_cpu: bool) -> dict:
+    """The PEC workload end to end through the public solver call (host mesh
+    in, host currents out: assembly, factorization, solve, residual), its
+    device-resident parts timed with CUDA events, the bistatic RCS cuts, and
+    the reference's host path on the same inputs (its quadrature and Eigen
+    LU from oracle/_ref; the far-field projection of its Python script as
+    the oracle's C restatement)."""
+    import torch
+    import sieb200
+    m = sieb200.icosphere(1.0, 3)
+    N = m.num_edges
+    th = np.linspace(0.0, np.pi, 181)
+    frames = [sieb200.spherical_frames(th, np.full_like(th, ph)) for ph in (0.0, np.pi / 2)]
+    r_hat = np.concatenate([f[0] for f in frames])
+    t_hat = np.concatenate([f[1] for f in frames])
+    p_hat = np.concatenate([f[2] for f in frames])
+    out = {"workload": PEC_WORKLOAD, "N": N}
+    for solver in ("lu_cusolver", "mixed_ir"):
+        o = sieb200.PecOptions(frequency_hz=C0, quadrature_rule=5, singularity_threshold_lambda0=0.1, solver=solver)
+        r = sieb200.solve_pec_dense(m, o, sieb200.PlaneWaveExcitation(), ctx=ctx)  # warm-up
+        reps = 5
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = sieb200.solve_pec_dense(m, o, sieb200.PlaneWaveExcitation(), ctx=ctx)
+        t = (time.perf_counter() - t0) / reps
+        out[solver] = {"end_to_end_seconds": t, "solves_per_s": 1.0 / t,
+                       "assembly_seconds": r.metrics["assembly_seconds"],
+                       "factorization_seconds": r.metrics["factorization_seconds"],
+                       "solve_seconds": r.metrics["solve_seconds"],
+                       "relative_residual": r.metrics["relative_residual"]}
+        if solver == "lu_cusolver":
+            x64 = r.currents
+        else:
+            out["mixed_vs_fp64_rel_diff"] = float(np.linalg.norm(r.currents - x64) / np.linalg.norm(x64))
+    s = {"mu0": 1.25663706212e-6, "eps0": 8.8541878128e-12}
+    k = 2 * math.pi * C0 * math.sqrt(s["mu0"] * s["eps0"])
+    eta = math.sqrt(s["mu0"] / s["eps0"])
+    sieb200.far_field(m, x64, None, k, eta, r_hat, t_hat, p_hat, ctx=ctx)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ft, fp, _ = sieb200.far_field(m, x64, None, k, eta, r_hat, t_hat, p_hat, ctx=ctx)
+    t_ff = (time.perf_counter() - t0) / reps
+    rcs = 4 * np.pi * (np.abs(ft) ** 2 + np.abs(fp) ** 2)
+    out["rcs"] = {"directions": int(r_hat.shape[0]), "seconds": t_ff,
+                  "monostatic_m2": float(rcs[180]), "forward_m2": float(rcs[0]),
+                  "rel_rms_error_vs_mie": rcs_error_vs_mie(
+                      ctx, m, sieb200.PecOptions(frequency_hz=C0, quadrature_rule=5,
+                                                 singularity_threshold_lambda0=0.1), 1.0, None)}
+    if with_cpu:
+        from oracle import oracle as O
+        ref = O.reference()
+        lib = O.oracle()
+        if ref is not None:
+            threads = os.cpu_count() or 1
+            sc = O.kernel_scalars(0, C0)
+            om = O.icosphere(1.0, 3)
+            t0 = time.perf_counter()
+            Z = O.assemble(ref, 0, om, 5, sc, threads=threads, fn="ref_assemble")
+            t_asm = time.perf_counter() - t0
+            b = np.zeros(N, np.complex128)
+            V = np.ascontiguousarray(om.vertices)
+            E0, kh = np.array([1.0, 0, 0]), np.array([0, 0, 1.0])
+            ref.ref_rhs_plane_wave(0, V.ctypes.data, om.faces.ctypes.data, om.faces_edges.ctypes.data,
+                                   om.num_faces, om.num_edges, 5, E0.ctypes.data, kh.ctypes.data, k, eta, 2,
+                                   sc["mu0"], sc["eps0"], b.ctypes.data, 0, 1.0, 1.0)
+            t_lu, xc, kind, desc = cpu_reference_solve(Z, b, threads)
+            t0 = time.perf_counter()
+            O.far_field(lib, om, xc, None, k, eta, r_hat, t_hat, p_hat)
+            t_ffc = time.perf_counter() - t0
+            tot = t_asm + t_lu + t_ffc
+            out["cpu_reference"] = {
+                "seconds": tot, "solves_per_s": 1.0 / tot, "assembly_seconds": t_asm, "lu_seconds": t_lu,
+                "far_field_seconds": t_ffc, "cores": threads, "kind": "reference",
+                "sample": "the whole workload once: the reference's host quadrature and Eigen PartialPivLU "
+                          "(oracle/_ref, all host threads), far field by the oracle's C restatement of "
+                          "plot_far_field.py (one thread)",
+                "currents_rel_diff_vs_gpu_fp64": float(np.linalg.norm(xc - x64) / np.linalg.norm(xc))}
+            out["gpu_vs_cpu_end_to_end"] = tot / out["mixed_ir"]["end_to_end_seconds"]
+    return out
+
+
+MULTI_WORKLOAD = ("SIE-GSTC omega-bianisotropic sphere r=1 m, geodesic mesh 2880 faces / 4320 RWG edges "
+                  "(N=17280: [J1, M1, J2, M2] per edge), f=c0 (ka=2 pi), Dunavant rule 17; per-face lossless "
+                  "omega records (B, X, chi uniform in [-2, 2], seeded, |chi^2-BX|>=0.25); 64 plane waves, "
+                  "theta uniform in [0, pi] (k in the xz-plane, E perpendicular in it), solved as one batch")
+
+
+def multi_rhs_section(ctx, fp64_peak: float, max_over_ranks) -> dict:
+    """Batch solves/s for 64 right-hand sides: the mixed factorization and
+    the tensor-core multi-right-hand-side refinement against cuSOLVER
+    Zgetrf + Zgetrs(nrhs = 64) on the same system, inputs resident."""
+    import torch
+    import sieb200
+    m = sieb200.geodesic_sphere(1.0, 12)
+    nf = m.num_faces
+    rng = np.random.default_rng(2026)
+    B_, X_, chi = (rng.uniform(-2, 2, nf) for _ in range(3))
+    bad = np.abs(chi ** 2 - B_ * X_) < 0.25
+    while bad.any():
+        B_[bad], X_[bad], chi[bad] = (rng.uniform(-2, 2, int(bad.sum())) for _ in range(3))
+        bad = np.abs(chi ** 2 - B_ * X_) < 0.25
+    t = sieb200.omega_records(B_, X_, chi).numpy().reshape(nf, 32)
+    o = sieb200.GstcSieOptions(frequency_hz=C0, quadrature_rule=17)
+    N = 4 * m.num_edges
+    nrhs = 64
+    th = np.linspace(0.0, np.pi, nrhs)
+    srcs = [sieb200.PlaneWaveExcitation(electric_amplitude=(np.cos(a), 0.0, -np.sin(a)),
+                                        propagation_direction=(np.sin(a), 0.0, np.cos(a))) for a in th]
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    Z = torch.empty((N, N), dtype=torch.complex128, device="cuda")
+    t0 = time.perf_counter()
+    sieb200.assemble_matrix_device(m, o, Z.data_ptr(), tensors=t, ctx=ctx)
+    ctx.synchronize()
+    t_asm = time.perf_counter() - t0
+    Bh = sieb200.assemble_rhs(m, o, srcs, ctx=ctx)  # (N, nrhs) column-major
+    B = torch.from_numpy(np.ascontiguousarray(Bh.T)).cuda()  # row c = column c: column-major N x nrhs
+    X = torch.empty_like(B)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            a, c = ev(), ev()
+            a.record(stream)
+            fn()
+            c.record(stream)
+            c.synchronize()
+            ts.append(a.elapsed_time(c) / 1e3)
+        return ts
+
+    mixed = sieb200.DenseLuSolver(N, "mixed_ir", ctx=ctx)
+    iters = []
+
+    def mixed_step():
+        mixed.factorize(Z.data_ptr())
+        with torch.cuda.stream(stream):
+            X.copy_(B)
+        iters.append(mixed.solve(X.data_ptr(), nrhs=nrhs, tolerance=1e-10, max_iterations=60))
+
+    timed(mixed_step, 2)
+    ctx.profile(True)
+    mixed_step()
+    prof = {name: ctx.profile_read(i) for i, name in [(0, "tf32_gemm"), (2, "fp64_gemm"), (5, "block_trsm"),
+                                                      (6, "factorization"), (7, "refined_solve")]}
+    ctx.profile(False)
+    t_mixed = max_over_ranks(statistics.mean(timed(mixed_step, 3)))
+    # accuracy: every column's FP64 residual
+    R = B.clone()
+    torch.cuda.synchronize()
+    sieb200.zgemm(N, nrhs, N, Z.data_ptr(), X.data_ptr(), R.data_ptr(), alpha=-1.0, beta=1.0, ctx=ctx)
+    res = (torch.linalg.vector_norm(R, dim=1) / torch.linalg.vector_norm(B, dim=1)).max().item()
+    X_mixed = X.clone()
+    mixed.close()
+    fp64 = sieb200.DenseLuSolver(N, "lu_cusolver", ctx=ctx)
+    Zw = torch.empty_like(Z)
+
+    def fp64_step():
+        with torch.cuda.stream(stream):
+            Zw.copy_(Z)
+            X.copy_(B)
+        fp64.factorize(Zw.data_ptr())
+        fp64.solve(X.data_ptr(), nrhs=nrhs)
+
+    timed(fp64_step, 1)
+    t_fp64 = max_over_ranks(statistics.mean(timed(fp64_step, 2)))
+    rel = (torch.linalg.vector_norm(X_mixed - X) / torch.linalg.vector_norm(X)).item()
+    fp64.close()
+    del Zw
+    np_ = ((N + 3) // 4) * 4
+    trsm = prof["block_trsm"]
+    gemm64 = prof["fp64_gemm"]
+    tri_tflops = trsm["flops"] / (trsm["ms"] / 1e3) / 1e12 if trsm["ms"] > 0 else None
+    return {
+        "workload": MULTI_WORKLOAD, "N": N, "nrhs": nrhs, "assembly_seconds": t_asm,
+        "batch_solves_per_s": 1.0 / t_mixed, "ms_per_batch": 1e3 * t_mixed,
+        "rhs_per_s": nrhs / t_mixed, "fp64_batch_solves_per_s": 1.0 / t_fp64,
+        "fp64_ms_per_batch": 1e3 * t_fp64, "speedup_vs_fp64_lu": t_fp64 / t_mixed,
+        "max_relative_residual": res, "rel_diff_vs_fp64_lu": rel, "refinement_iterations": max(iters),
+        "fp64": "cusolverDnZgetrf + Zgetrs with nrhs=64 on a copy of Z (the reference's batch solve path)",
+        "profile_ms": {k: v["ms"] for k, v in prof.items()},
+        "block_trsm": {"launches_of_applications": trsm["launches"],
+                       "tf32_tflops": tri_tflops,
+                       "packed_factor_gbs": trsm["bytes"] / (trsm["ms"] / 1e3) / 1e9 if trsm["ms"] > 0 else None,
+                       "work_note": f"24 np^2 nrhs TF32 flops and 48 np^2 bytes of packed factors per "
+                                    f"application, np={np_}"},
+        "fp64_gemm": {"launches": gemm64["launches"],
+                      "tflops": gemm64["flops"] / (gemm64["ms"] / 1e3) / 1e12 if gemm64["ms"] > 0 else None,
+                      "peak_tflops": fp64_peak,
+                      "frac": gemm64["flops"] / (gemm64["ms"] / 1e3) / 1e12 / fp64_peak if gemm64["ms"] > 0 else None},
+    }
 
 
 def adjoint_section(ctx, steps: int, max_over_ranks):
@@ -697,6 +935,8 @@ def main():
     ap.add_argument("--impl", default="sieb200", choices=["sieb200", "reference"])
     ap.add_argument("--rule", type=int, default=17)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline solve")
+    ap.add_argument("--skip-sections", action="store_true",
+                    help="time only the headline solve (no PEC or 64-right-hand-side sections)")
     ap.add_argument("--adjoint-steps", type=int, default=2,
                     help="timed adjoint gradients on the spindle workload (0 skips them)")
     args = ap.parse_args()

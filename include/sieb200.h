@@ -42,8 +42,10 @@ enum {
 /* Thread-local message of the last failing call on this host thread. */
 const char* sieb200_last_error(void);
 /* ABI version of the declarations below; a binding checks it on load.
- * 2: sieb200_options gained variant, ntl_form, line_quadrature_points. */
-#define SIEB200_ABI_VERSION 2
+ * 2: sieb200_options gained variant, ntl_form, line_quadrature_points.
+ * 3: sieb200_zgemm; the mixed solver solves several right-hand sides
+ *    together (profile kind 5). */
+#define SIEB200_ABI_VERSION 3
 int sieb200_version(void);
 
 /* ----------------------------------------------------------- context ---- */
@@ -279,12 +281,25 @@ int sieb200_matvec(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int 
 int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                            const double* x, double beta, double* y);
 
+/* FP64 complex product C = alpha A X + beta C on device data, column-major,
+ * complex interleaved: A m x k (lda), X k x nc (ldx), C m x nc (ldc); alpha
+ * and beta 2 doubles each (re, im); beta = 0 does not read C. The residual
+ * R = B - Z X and the Krylov products of the multi-right-hand-side mixed
+ * solve (hand-written SIMT FP64 kernel). Replaces, for a batch of cases,
+ * the one cublasZgemv per case of src/sie_mom/solvers/gstc_sie.cu:398-457.
+ * Synchronizes the context stream. */
+int sieb200_zgemm(sieb200_ctx* ctx, int64_t m, int64_t nc, int64_t k, const double* A, int64_t lda,
+                  const double* X, int64_t ldx, double* C, int64_t ldc, const double* alpha,
+                  const double* beta);
+
 /* Split-TF32 tensor-core contraction used by the mixed LU's trailing update
  * (no counterpart in the reference, which calls cuSOLVER): on device data,
  *   C[m2 x n] (fp32, column-major, ldc) -= A[m2 x k] * B[n x k]^T,
- * A and B K-major fp32, k a multiple of 32. mode 2: persistent tcgen05
- * kernel with TMA C epilogue (what the LU uses; C and ldc*4 16-byte aligned,
- * else mode 1), mode 1: one-CTA-per-tile tcgen05 kernel, mode 0: SIMT kernel
+ * A and B K-major fp32, k a multiple of 32. mode 3: persistent tcgen05
+ * kernel whose epilogue adds -A B^T to C by TMA reduction (no C load in the
+ * CTA), mode 2: persistent tcgen05 kernel that loads, subtracts and stores
+ * the C tile by TMA (modes 2 and 3 need C and ldc*4 16-byte aligned, else
+ * mode 1 runs), mode 1: one-CTA-per-tile tcgen05 kernel, mode 0: SIMT kernel
  * on the same operands (checking path). */
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode);
@@ -299,8 +314,11 @@ int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const 
  * 3: diagonal-block LU + inverses (with the previous block step's update
  * of the block; on the solver's lookahead stream); 4: block-step panels
  * (L21 with the previous step's update of its rows, and U12: one launch per
- * step); 5: unused; 6: whole mixed factorizations; 7: whole refined solves
- * (spans on the context stream unless stated). */
+ * step); 5: the two blocked triangular solves of a multi-right-hand-side
+ * preconditioner application (work = 24 np^2 nrhs TF32 flops and 48 np^2
+ * bytes of packed factors); 6: whole mixed factorizations; 7: whole refined
+ * solves (spans on the context stream unless stated). Kind 2 also counts the
+ * FP64 complex GEMMs (8 m nc k flops). */
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable);
 /* enable = 2 also keeps a timeline: per span its kernel kind and its start
  * and end in ms after the enable call (device timestamps, all streams).

@@ -45,6 +45,7 @@ def oracle() -> ctypes.CDLL:
     lib.so_pair_blocks_n.argtypes = [_P, _P, _i, _i, _i, _f, _f, _f, _i, _P]
     lib.so_gauss_legendre.argtypes = [_i, _P, _P]
     lib.so_assemble.argtypes = _ASSEMBLE
+    lib.so_assemble_rows.argtypes = _ASSEMBLE[:20] + [_P, _i, _P, _i, _P, _i, _i, _i]
     lib.so_rhs.argtypes = [_i, _i, _P, _P, _P, _i, _i, _i, _P, _P, _i, _d, _d, _i, _d, _d, _P, _i, _d, _d]
     lib.so_far_field.argtypes = [_P, _P, _i, _i, _P, _P, _d, _d, _i, _P, _P, _P, _P, _P, _P]
     lib.so_surface_fields.argtypes = _FIELDS
@@ -125,6 +126,32 @@ def assemble(lib, kind: int, mesh, rule: int, scalars: dict, tensors=None, unifo
                      s["mu_r2"], s["eps_r1"], s["eps_r2"], s["mu0"], s["eps0"], s["omega"], s["thr"],
                      _p(t), int(uniform), int(basis), _p(Z), int(threads), int(variant), int(line_points))
     return Z
+
+
+def assemble_rows(lib, kind: int, mesh, rule: int, scalars: dict, rows, tensors=None, uniform=False, basis=0,
+                  threads=0, variant: int = 0, line_points: int = 0) -> np.ndarray:
+    """Rows `rows` of the matrix assemble() gives (len(rows) x N), computed
+    from the test faces that hold their edges only."""
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
+    ne = int(mesh.edges.shape[0])
+    N = dimension(kind, ne)
+    rows = np.asarray(rows, dtype=np.int64)
+    rowmap = np.full(N, -1, np.int32)
+    rowmap[rows] = np.arange(rows.size, dtype=np.int32)
+    edges = np.unique(rows % ne)
+    faces = np.unique(np.nonzero(np.isin(FE, edges).any(axis=1))[0]).astype(np.int32)
+    out = np.zeros((rows.size, N), dtype=np.complex128, order="F")
+    t = None if tensors is None else np.ascontiguousarray(tensors, dtype=np.complex128)
+    s = scalars
+    rc = lib.so_assemble_rows(kind, _p(V), _p(F), _p(FE), F.shape[0], ne, rule, s["k1"], s["k2"], s["mu_r1"],
+                              s["mu_r2"], s["eps_r1"], s["eps_r2"], s["mu0"], s["eps0"], s["omega"], s["thr"],
+                              _p(t), int(uniform), int(basis), _p(faces), faces.size, _p(rowmap), rows.size,
+                              _p(out), int(threads), int(variant), int(line_points))
+    if rc != 0:
+        raise ValueError("oracle assembly: invalid rule")
+    return out
 
 
 def rhs(lib, kind: int, mesh, rule: int, source: dict, k: float, eta: float, mu0: float,

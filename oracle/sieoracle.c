@@ -13,6 +13,7 @@
 #include "sieoracle.h"
 
 #include <math.h>
+#include <omp.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -842,10 +843,20 @@ static void gram(const tri_t* T, const float* pts, const float* wts, int Q, doub
 }
 
 /* ------------------------------------------------------------ assembly -- */
-static inline void zadd(double* Z, size_t N, size_t r, size_t c, cx v) {
-    size_t idx = c * N + r;
-    Z[2 * idx] += v.re;
-    Z[2 * idx + 1] += v.im;
+/* Destination of an assembly: the whole matrix (rowmap NULL, ld = N) or
+ * selected rows of it (rowmap[r] = output row or -1, ld = output rows). */
+typedef struct { double* Z; size_t ld; const int* rowmap; } ztarget_t;
+
+static inline void zadd(const ztarget_t* T, size_t N, size_t r, size_t c, cx v) {
+    (void)N;
+    if (T->rowmap) {
+        const int rr = T->rowmap[r];
+        if (rr < 0) return;
+        r = (size_t)rr;
+    }
+    size_t idx = c * T->ld + r;
+    T->Z[2 * idx] += v.re;
+    T->Z[2 * idx + 1] += v.im;
 }
 
 /* kind 0: PEC T-EFIE (sie_kernels_assembly.cuh:610-705), with variant 1
@@ -857,11 +868,11 @@ static inline void zadd(double* Z, size_t N, size_t r, size_t c, cx v) {
  * kind 2: GSTC Calderon + mass, eta0-scaled (sie_kernels_assembly.cuh:156-272,
  *         460-594). Z: complex interleaved, column-major, overwritten.
  * Serial over faces so that the summation order is fixed. */
-int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
-                float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
-                float mu0, float eps0, float omega, float thr, const double* tensors,
-                int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points) {
-    (void)threads;
+static int assemble_impl(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+                         float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
+                         float mu0, float eps0, float omega, float thr, const double* tensors,
+                         int tensors_uniform, int basis, const ztarget_t* Zt, const int* test_faces, int ntest,
+                         int threads, int variant, int line_points) {
     float pts[2 * 80], wts[80];
     const int Q = so_rule(rule, pts, wts);
     if (Q < 0) return -1;
@@ -873,17 +884,32 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
     const line_t L = {lt, lw, NG};
     const size_t E = (size_t)ne;
     const size_t N = kind == 0 ? E : (kind == 1 ? 2 * E : 4 * E);
-    memset(Z, 0, sizeof(double) * 2 * N * N);
+    ztarget_t Zv = *Zt;
+    ztarget_t* Z = &Zv;
     tri_t* tris = (tri_t*)malloc(sizeof(tri_t) * (size_t)nf);
     for (int f = 0; f < nf; ++f) load_tri(V, F, f, &tris[f]);
+    if (threads <= 0) threads = omp_get_max_threads();
 
-    for (int m = 0; m < nf; ++m) {
-        for (int n = 0; n < nf; ++n) {
-            blocks_t B;
+    /* Face-pair blocks of a chunk of test faces in parallel, then placed
+     * serially in (test face, source face) order: the sums are the same,
+     * bit for bit, for any thread count. */
+    const int CH = 32;
+    blocks_t* buf = (blocks_t*)malloc(sizeof(blocks_t) * (size_t)CH * (size_t)nf);
+    for (int c0 = 0; c0 < ntest; c0 += CH) {
+        const int cn = ntest - c0 < CH ? ntest - c0 : CH;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+        for (long idx = 0; idx < (long)cn * nf; ++idx) {
+            const int mm = test_faces ? test_faces[c0 + idx / nf] : c0 + (int)(idx / nf);
+            const int nn = (int)(idx % nf);
             if (variant != 0)
-                pair_n(&tris[m], &tris[n], pts, wts, Q, &L, k1, k2, thr, kind == 0, &B);
+                pair_n(&tris[mm], &tris[nn], pts, wts, Q, &L, k1, k2, thr, kind == 0, &buf[idx]);
             else
-                pair(&tris[m], &tris[n], pts, wts, Q, k1, k2, thr, &B);
+                pair(&tris[mm], &tris[nn], pts, wts, Q, k1, k2, thr, &buf[idx]);
+        }
+      for (int ci = 0; ci < cn; ++ci) {
+        const int m = test_faces ? test_faces[c0 + ci] : c0 + ci;
+        for (int n = 0; n < nf; ++n) {
+            const blocks_t B = buf[(size_t)ci * nf + n];
             const int* te = &FE[3 * m];
             const int* se = &FE[3 * n];
             double G[3][3];
@@ -966,12 +992,15 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
                     }
                 }
         }
+      }
     }
+    free(buf);
 
     if (kind == 2) {
         const float eta0 = sqrtf(mu0 / eps0);
         const float eta0sq = eta0 * eta0;
-        for (int m = 0; m < nf; ++m) {
+        for (int ti = 0; ti < ntest; ++ti) {
+            const int m = test_faces ? test_faces[ti] : ti;
             const tri_t* T = &tris[m];
             v3 u, w;
             frame(T->v, basis, &u, &w);
@@ -1022,6 +1051,36 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
     }
     free(tris);
     return 0;
+}
+
+int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+                float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
+                float mu0, float eps0, float omega, float thr, const double* tensors,
+                int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points) {
+    const size_t E = (size_t)ne;
+    const size_t N = kind == 0 ? E : (kind == 1 ? 2 * E : 4 * E);
+    memset(Z, 0, sizeof(double) * 2 * N * N);
+    const ztarget_t T = {Z, N, NULL};
+    return assemble_impl(kind, V, F, FE, nf, ne, rule, k1, k2, mu_r1, mu_r2, eps_r1, eps_r2, mu0, eps0, omega,
+                         thr, tensors, tensors_uniform, basis, &T, NULL, nf, threads, variant, line_points);
+}
+
+/* The contributions of the listed test faces only, into the rows that
+ * rowmap selects (rowmap[r] = output row or -1; Zrows: nrows x N,
+ * column-major, overwritten). A row of Z is complete when every face that
+ * holds its edge is listed. */
+int so_assemble_rows(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+                     float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
+                     float mu0, float eps0, float omega, float thr, const double* tensors,
+                     int tensors_uniform, int basis, const int* test_faces, int ntest, const int* rowmap,
+                     int nrows, double* Zrows, int threads, int variant, int line_points) {
+    const size_t E = (size_t)ne;
+    const size_t N = kind == 0 ? E : (kind == 1 ? 2 * E : 4 * E);
+    memset(Zrows, 0, sizeof(double) * 2 * (size_t)nrows * N);
+    const ztarget_t T = {Zrows, (size_t)nrows, rowmap};
+    return assemble_impl(kind, V, F, FE, nf, ne, rule, k1, k2, mu_r1, mu_r2, eps_r1, eps_r2, mu0, eps0, omega,
+                         thr, tensors, tensors_uniform, basis, &T, test_faces, ntest, threads, variant,
+                         line_points);
 }
 
 /* ----------------------------------------------------------------- RHS -- */

@@ -20,6 +20,11 @@ int so_assemble(int kind, const double* V, const int* F, const int* FE, int nf, 
                 float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
                 float mu0, float eps0, float omega, float thr, const double* tensors,
                 int tensors_uniform, int basis, double* Z, int threads, int variant, int line_points);
+int so_assemble_rows(int kind, const double* V, const int* F, const int* FE, int nf, int ne, int rule,
+                float k1, float k2, float mu_r1, float mu_r2, float eps_r1, float eps_r2,
+                float mu0, float eps0, float omega, float thr, const double* tensors,
+                int tensors_uniform, int basis, const int* test_faces, int ntest, const int* rowmap,
+                     int nrows, double* Zrows, int threads, int variant, int line_points);
 int so_rhs(int kind, int source_kind, const double* V, const int* F, const int* FE, int nf, int ne,
            int rule, const double* a, const double* b, int is_magnetic, double k, double eta,
            int region, double mu0, double eps0, double* rhs, int variant, double eps_r_src,

@@ -413,9 +413,20 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
     if (o->compute_residual) {
         const auto t_res = Clock::now();
         const double* Zr = in_place ? Zcopy.as<double>() : Zb.as<double>();
-        SIEB_RETURN_IF(Rb.reserve(sizeof(cplx) * N * 2));
         DeviceBuffer scratch;
         std::vector<double> hr(2 * N);
+        if (ncols >= 2) {
+            // every column at once: R = B - Z X (one FP64 complex GEMM)
+            SIEB_RETURN_IF(Rb.reserve(sizeof(cplx) * N * ncols));
+            SIEB_TRY_CUDA(cudaMemcpyAsync(Rb.ptr, hb.data(), sizeof(cplx) * N * ncols, cudaMemcpyHostToDevice, st));
+            SIEB_RETURN_IF(zgemm_device(st, N, ncols, N, reinterpret_cast<const cplx*>(Zr), N, Bb.as<cplx>(), N,
+                                        Rb.as<cplx>(), N, cx(-1, 0), cx(1, 0)));
+            std::vector<double> hR(2 * N * ncols);
+            SIEB_TRY_CUDA(cudaMemcpyAsync(hR.data(), Rb.ptr, sizeof(cplx) * N * ncols, cudaMemcpyDeviceToHost, st));
+            SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+            for (int c = 0; c < ncols; ++c) abs_res[c] = host_norm(hR.data() + 2 * N * c, N);
+        } else {
+        SIEB_RETURN_IF(Rb.reserve(sizeof(cplx) * N * 2));
         for (int c = 0; c < ncols; ++c) {
             cplx* r = Rb.as<cplx>();
             SIEB_TRY_CUDA(cudaMemcpyAsync(r, hb.data() + 2 * N * c, sizeof(cplx) * N, cudaMemcpyHostToDevice, st));
@@ -424,6 +435,7 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
             SIEB_TRY_CUDA(cudaMemcpyAsync(hr.data(), r, sizeof(cplx) * N, cudaMemcpyDeviceToHost, st));
             SIEB_TRY_CUDA(cudaStreamSynchronize(st));
             abs_res[c] = host_norm(hr.data(), N);
+        }
         }
         res_s = seconds_since(t_res);
     }
@@ -780,6 +792,24 @@ int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t l
     return SIEB200_OK;
 }
 
+int sieb200_zgemm(sieb200_ctx* ctx, int64_t m, int64_t nc, int64_t k, const double* A, int64_t lda,
+                  const double* X, int64_t ldx, double* C, int64_t ldc, const double* alpha, const double* beta) {
+    SIEB_CHECK(ctx && alpha && beta && m >= 0 && nc >= 0 && k >= 0, SIEB200_INVALID_ARG, "invalid zgemm arguments");
+    if (m == 0 || nc == 0) return SIEB200_OK;
+    SIEB_CHECK(C && ldc >= m && (k == 0 || (A && X && lda >= m && ldx >= k)), SIEB200_INVALID_ARG,
+               "invalid zgemm arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaEvent_t ev;
+    ctx->prof.begin(ctx->stream, 2, 8.0 * (double)m * (double)nc * (double)k,
+                    16.0 * ((double)m * k + (double)k * nc + 2.0 * (double)m * nc), &ev);
+    SIEB_RETURN_IF(zgemm_device(ctx->stream, m, nc, k, reinterpret_cast<const cplx*>(A), lda,
+                                reinterpret_cast<const cplx*>(X), ldx, reinterpret_cast<cplx*>(C), ldc,
+                                cx(alpha[0], alpha[1]), cx(beta[0], beta[1])));
+    ctx->prof.end(ctx->stream, ev);
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
 int64_t sieb200_launch_count(void) { return (int64_t)g_launches.load(); }
 
 int sieb200_fp64_fma_peak(sieb200_ctx* ctx, double* tflops) {
@@ -832,7 +862,7 @@ int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double
 
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode) {
-    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 2, SIEB200_INVALID_ARG,
+    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 3, SIEB200_INVALID_ARG,
                "invalid GEMM arguments");
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     GemmTC* g = nullptr;

@@ -24,6 +24,9 @@ struct DenseSolver {
     DeviceBuffer flags;    // triangular-solve progress flags and error word
     DeviceBuffer gemv_scratch;
     void* gemm_state = nullptr;
+    // Cap on the SMs of the persistent trailing GEMM (0: all but one); a
+    // sweep running several systems concurrently gives each its share.
+    int sm_cap = 0;
 
     int factorize(double* A, int64_t lda);
     int solve(int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol, int maxit, int* iters);
@@ -46,6 +49,10 @@ int fp64_fma_rate(sieb200_ctx* ctx, double* tflops);
 int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                                const cplx* x, double beta, cplx* y);
 void destroy_cusolver(sieb200_ctx* ctx);
+// C = alpha A X + beta C, FP64 complex column-major (hand-written SIMT kernel,
+// block_solve.cu).
+int zgemm_device(cudaStream_t stream, int64_t m, int64_t nc, int64_t kdim, const cplx* A, int64_t lda,
+                 const cplx* X, int64_t ldx, cplx* C, int64_t ldc, cplx alpha, cplx beta);
 
 }  // namespace sieb200
 

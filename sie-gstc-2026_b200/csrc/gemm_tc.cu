@@ -231,6 +231,14 @@ constexpr int P_SMEM_BYTES = P_STAGES * (STAGE_A + STAGE_B) + C_TILE_BYTES + 102
 
 __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// REDUCE = true: the epilogue does not load C. It writes the negated
+// accumulator into the staging tile and adds it to C with a TMA reduction
+// (cp.reduce.async.bulk.tensor .add, performed at L2), so no CTA waits for a
+// 64 KB C load between tiles; the staging tile is reused once the previous
+// reduction has read it. C + (-acc) rounds exactly as C - acc, and each
+// element takes one reduction per launch, so results are unchanged and
+// deterministic.
+template <bool REDUCE>
 __global__ void __launch_bounds__(P_THREADS, 1)
 gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                                 const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, unsigned* err) {
@@ -325,14 +333,14 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
         const int rt = q * 32 + lane;      // row of the tile
         const bool e0 = et == 0;
         int t = blockIdx.x;
-        if (e0 && t < tiles) {
+        if (!REDUCE && e0 && t < tiles) {
             mbar_expect_tx(cfull, C_TILE_BYTES);
             tma_load_2d(sC, &tmC, cfull, (t % mt) * BM, (t / mt) * BN);
         }
         for (int li = 0; t < tiles; t += gridDim.x, ++li) {
             const int b = li & 1;
             const uint32_t u = (uint32_t)(li >> 1);
-            const bool okc = mbar_wait(cfull, (uint32_t)li & 1u, err);
+            const bool okc = REDUCE ? true : mbar_wait(cfull, (uint32_t)li & 1u, err);
             int got = 0;
             if (lane == 0) got = mbar_wait(accf0 + 8 * b, u & 1u, err) ? 1 : 0;
             got = __shfl_sync(0xffffffffu, got, 0);
@@ -343,8 +351,13 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
                 for (int chunk = 0; chunk < BN / 32; ++chunk) {
                     float v[32];
                     tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + chunk * 32), v);
+                    if (REDUCE) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] -= v[j];
+                        for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] = -v[j];
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] -= v[j];
+                    }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -354,15 +367,23 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             epilogue_bar();
             if (e0) {
-                tma_store_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
+                if (REDUCE) {
+                    // A tile whose accumulator wait failed adds nothing.
+                    if (got && okc) tma_reduce_add_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
+                } else {
+                    tma_store_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
+                }
                 bulk_commit();
                 bulk_wait_read_all();  // the buffer is free once the store has read it
                 const int tn = t + gridDim.x;
-                if (tn < tiles) {
+                if (!REDUCE && tn < tiles) {
                     mbar_expect_tx(cfull, C_TILE_BYTES);
                     tma_load_2d(sC, &tmC, cfull, (tn % mt) * BM, (tn / mt) * BN);
                 }
             }
+            // The staging tile is rewritten only after the reduction or store
+            // above has read it.
+            epilogue_bar();
         }
         if (e0) bulk_wait_all();
     }
@@ -452,6 +473,8 @@ int gemm_tc_create(GemmTC** out) {
     cudaMemset(g->err, 0, sizeof(unsigned));
     const char* env = getenv("SIEB200_GEMM_SIMT");
     if (env && env[0] == '1') g->mode = 0;
+    const char* mode_env = getenv("SIEB200_GEMM_MODE");
+    if (mode_env && mode_env[0] >= '0' && mode_env[0] <= '3' && mode_env[1] == 0) g->mode = mode_env[0] - '0';
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -486,9 +509,11 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
     SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
     // The persistent kernel moves C by TMA: its base and column stride must
     // be 16-byte aligned (otherwise the per-tile kernel below is used).
-    if (g->mode == 2 && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
+    if (g->mode >= 2 && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
         if (!g->attr_set_p) {
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel,
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
             g->attr_set_p = true;
         }
@@ -498,8 +523,12 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         const int64_t tiles = ((M2 + BM - 1) / BM) * ((N + BN - 1) / BN);
         const int cap = max_ctas > 0 ? std::min(max_ctas, g->sms) : g->sms;
         const unsigned grid = (unsigned)std::min<int64_t>(tiles, std::max(1, cap));
-        gemm_tf32_sub_persistent_kernel<<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2, (int)N, K,
-                                                                                 g->err);
+        if (g->mode == 3)
+            gemm_tf32_sub_persistent_kernel<true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2,
+                                                                                          (int)N, K, g->err);
+        else
+            gemm_tf32_sub_persistent_kernel<false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2,
+                                                                                           (int)N, K, g->err);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;

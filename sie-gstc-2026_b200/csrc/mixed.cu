@@ -27,15 +27,12 @@
 #include <cstring>
 #include <vector>
 
-#include "dense.cuh"
-#include "gemm_tc.cuh"
-#include "sm100.cuh"
+#include "mixed.cuh"
 
 namespace sieb200 {
 
 namespace {
 
-constexpr int NB = 64;  // LU block size (complex columns)
 // Dynamic shared memory of the block kernels (two NB x (NB+1) complex64
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
@@ -45,62 +42,6 @@ constexpr int kSmemPanel = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(flo
 constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
 constexpr int kDiagThreads = 256;  // diagonal-block kernel: 8 warps of NB / 8 columns
 
-struct MixedState {
-    int64_t n = 0, np = 0, ldw = 0, nbl = 0;
-    float2* W = nullptr;        // factors, np x np, ld = ldw
-    float2* Linv = nullptr;     // inverse unit-lower diagonal blocks, NB x NB each (col-major)
-    float2* Uinv = nullptr;     // inverse upper diagonal blocks
-    float* Apack[2] = {nullptr, nullptr};  // split realified L21: (2*np) x (6*NB), K-major; by step parity
-    float* Bpack = nullptr;     // split U12 columns: np x (6*NB), K-major
-    float2* panel = nullptr;    // NB x np scratch for U12 / np x NB for L21
-    double* diag = nullptr;     // butterfly diagonals: U (level1 a,b; level2 e,f) and V, 4*np each
-    unsigned* err = nullptr;    // error word (nonzero = failure code)
-    unsigned* tri_flags = nullptr;   // per block progress flags (2 * nbl) + 2 tickets
-    cplx* vecs = nullptr;       // FP64 work vectors
-    int use_tc = 1;
-    GemmTC* gemm = nullptr;
-    CUtensorMap tmW;                       // W for the triangular solves' tile loads
-    const void* tm_base = nullptr;
-    int64_t tm_np = 0;
-    // Conjugate-transpose solves (W^H = U^H L^H): W^H and the conjugate
-    // transposes of the diagonal-block inverses, built on first use after a
-    // factorization (in the solver's panel workspace).
-    cplx* dinv = nullptr;               // GMRES_C64: inverse diagonal of Z
-    bool adj_ready = false;
-    float2* WH = nullptr;
-    float2* LinvH = nullptr;
-    float2* UinvH = nullptr;
-    CUtensorMap tmWH;
-    cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
-    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr;
-    // The factorization's launches as one CUDA graph (both streams and the
-    // event edges between them), captured on the second call with an
-    // unchanged key and replayed while it stays so; not while the profiler
-    // is on (its per-kernel events run eagerly).
-    struct GraphKey {
-        const void* A = nullptr;
-        int64_t lda = -1, n = -1;
-        const void* W = nullptr;
-        const void* pack = nullptr;
-        int use_tc = -1, sms = -1;
-        bool operator==(const GraphKey& o) const {
-            return A == o.A && lda == o.lda && n == o.n && W == o.W && pack == o.pack && use_tc == o.use_tc &&
-                   sms == o.sms;
-        }
-    };
-    // Two graphs (for example one per buffer of a caller that uploads the
-    // next system while this one is solved); the two keys seen last decide
-    // what is worth capturing.
-    struct Graph {
-        GraphKey key;
-        cudaGraphExec_t exec = nullptr;
-        long long launches = 0;  // kernels per replay
-        uint64_t used = 0;
-    };
-    Graph graphs[2];
-    GraphKey seen[2];
-    uint64_t tick = 0;
-};
 
 static void drop_graphs(MixedState* st) {
     for (auto& g : st->graphs) {
@@ -124,52 +65,6 @@ __global__ void rbt_init_kernel(double* diag, int64_t np, uint64_t seed) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 8 * np) return;
     diag[i] = rbt_value(seed, i);
-}
-
-// Index quadruple of a depth-2 butterfly: {i, i+q, i+2q, i+3q}, q = np/4.
-// Transposed application T^T = L1^T L2^T (first the two level-2 blocks, then
-// level 1) of a butterfly with diagonals d = [a (h), b (h), e (h), f (h)],
-// h = np/2: level-2 block s pairs (s h + i, s h + i + q) with e[s q + i],
-// f[s q + i]; level 1 pairs (i', i' + h) with a[i'], b[i'].
-template <class T>
-__device__ __forceinline__ void bfly_T4(T x[4], const double* d, int64_t np, int64_t i) {
-    const int64_t h = np / 2, q = np / 4;
-    const double r = 0.70710678118654752440;
-    const double* a = d;
-    const double* b = d + h;
-    const double* e = d + 2 * h;
-    const double* f = d + 3 * h;
-    // level-2 transpose: halves s = 0 (x0,x1) and s = 1 (x2,x3)
-    T z[4];
-    z[0] = (x[0] + x[1]) * (e[i] * r);
-    z[1] = (x[0] - x[1]) * (f[i] * r);
-    z[2] = (x[2] + x[3]) * (e[q + i] * r);
-    z[3] = (x[2] - x[3]) * (f[q + i] * r);
-    // level-1 transpose: pairs (i, i+h) -> (z0, z2), (i+q, i+q+h) -> (z1, z3)
-    x[0] = (z[0] + z[2]) * (a[i] * r);
-    x[2] = (z[0] - z[2]) * (b[i] * r);
-    x[1] = (z[1] + z[3]) * (a[i + q] * r);
-    x[3] = (z[1] - z[3]) * (b[i + q] * r);
-}
-
-// Forward application T = L2 L1 (level 1, then level 2).
-template <class T>
-__device__ __forceinline__ void bfly_N4(T x[4], const double* d, int64_t np, int64_t i) {
-    const int64_t h = np / 2, q = np / 4;
-    const double r = 0.70710678118654752440;
-    const double* a = d;
-    const double* b = d + h;
-    const double* e = d + 2 * h;
-    const double* f = d + 3 * h;
-    T z[4];
-    z[0] = (x[0] * a[i] + x[2] * b[i]) * r;
-    z[2] = (x[0] * a[i] - x[2] * b[i]) * r;
-    z[1] = (x[1] * a[i + q] + x[3] * b[i + q]) * r;
-    z[3] = (x[1] * a[i + q] - x[3] * b[i + q]) * r;
-    x[0] = (z[0] * e[i] + z[1] * f[i]) * r;
-    x[1] = (z[0] * e[i] - z[1] * f[i]) * r;
-    x[2] = (z[2] * e[q + i] + z[3] * f[q + i]) * r;
-    x[3] = (z[2] * e[q + i] - z[3] * f[q + i]) * r;
 }
 
 // W = U^T A_pad V, read A (c128, n x n, lda) once, write W (c64).
@@ -421,11 +316,6 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __r
     }
 }
 
-__device__ __forceinline__ float tf32_hi(float x) {
-    uint32_t y;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
-    return __uint_as_float(y);
-}
 
 // L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
 // writes L21 back into W and the split realified rows into Apack.
@@ -1057,6 +947,7 @@ void mixed_release(DenseSolver* s) {
     MixedState* st = state_of(s);
     if (st) {
         drop_graphs(st);
+        block_solve_release(st);
         if (st->gemm) gemm_tc_destroy(st->gemm);
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
@@ -1106,6 +997,7 @@ int mixed_factorize(DenseSolver* s) {
     const int64_t nbl = (np + NB - 1) / NB;
     st->n = n; st->np = np; st->ldw = ldw; st->nbl = nbl;
     st->adj_ready = false;
+    block_solve_invalidate(st);
     const char* env = getenv("SIEB200_TRAILING_SIMT");
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
 
@@ -1150,7 +1042,8 @@ int mixed_factorize(DenseSolver* s) {
     // Replay, capture or run eagerly (see MixedState::graphs).
     MixedState::GraphKey key;
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
-    key.use_tc = st->use_tc; key.sms = ctx->sm_count;
+    const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
+    key.use_tc = st->use_tc; key.sms = gemm_sms;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -1286,7 +1179,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
             if (m > n1)
                 SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * K3,
-                                    ctx->sm_count - 1));
+                                    s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
             SIEB_RETURN_IF(panels(bk + 1, k0));
         } else {
@@ -1599,6 +1492,18 @@ int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoi
                "unsupported solver method");
     if (!(tol > 0)) tol = 1e-10;
     if (maxit <= 0) maxit = 50;
+    MixedState* st = state_of(s);
+    const char* per_column = getenv("SIEB200_PER_COLUMN_SOLVE");
+    if (nrhs >= 2 && !adjoint && s->method == SIEB200_SOLVER_MIXED_IR && st && st->use_tc &&
+        !(per_column && per_column[0] == '1')) {
+        // All columns together (tensor-core block triangular solves, batched
+        // FGMRES); -1: the packed factors do not fit, solve column by column.
+        cudaEvent_t ev;
+        s->ctx->prof.begin(s->ctx->stream, 7, 0.0, 0.0, &ev);
+        const int rc = block_solve(s, st, nrhs, B, ldb, tol, maxit, iters);
+        s->ctx->prof.end(s->ctx->stream, ev);
+        if (rc != -1) return rc;
+    }
     int total = 0;
     for (int64_t c = 0; c < nrhs; ++c) {
         int it = 0;

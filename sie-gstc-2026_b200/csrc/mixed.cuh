@@ -1,0 +1,139 @@
+// Internal state of the mixed-precision dense solver (mixed.cu) shared with
+// its multi-right-hand-side block solve (block_solve.cu).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "dense.cuh"
+#include "gemm_tc.cuh"
+#include "sm100.cuh"
+
+namespace sieb200 {
+
+constexpr int NB = 64;  // LU block size (complex columns)
+
+// Forward declaration: packed operands of the multi-right-hand-side solve.
+struct BlockSolveState;
+
+struct MixedState {
+    int64_t n = 0, np = 0, ldw = 0, nbl = 0;
+    float2* W = nullptr;        // factors, np x np, ld = ldw
+    float2* Linv = nullptr;     // inverse unit-lower diagonal blocks, NB x NB each (col-major)
+    float2* Uinv = nullptr;     // inverse upper diagonal blocks
+    float* Apack[2] = {nullptr, nullptr};  // split realified L21: (2*np) x (6*NB), K-major; by step parity
+    float* Bpack = nullptr;     // split U12 columns: np x (6*NB), K-major
+    float2* panel = nullptr;    // NB x np scratch for U12 / np x NB for L21
+    double* diag = nullptr;     // butterfly diagonals: U (level1 a,b; level2 e,f) and V, 4*np each
+    unsigned* err = nullptr;    // error word (nonzero = failure code)
+    unsigned* tri_flags = nullptr;   // per block progress flags (2 * nbl) + 2 tickets
+    cplx* vecs = nullptr;       // FP64 work vectors
+    int use_tc = 1;
+    GemmTC* gemm = nullptr;
+    CUtensorMap tmW;                       // W for the triangular solves' tile loads
+    const void* tm_base = nullptr;
+    int64_t tm_np = 0;
+    // Conjugate-transpose solves (W^H = U^H L^H): W^H and the conjugate
+    // transposes of the diagonal-block inverses, built on first use after a
+    // factorization (in the solver's panel workspace).
+    cplx* dinv = nullptr;               // GMRES_C64: inverse diagonal of Z
+    bool adj_ready = false;
+    float2* WH = nullptr;
+    float2* LinvH = nullptr;
+    float2* UinvH = nullptr;
+    CUtensorMap tmWH;
+    cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
+    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr;
+    // The factorization's launches as one CUDA graph (both streams and the
+    // event edges between them), captured on the second call with an
+    // unchanged key and replayed while it stays so; not while the profiler
+    // is on (its per-kernel events run eagerly).
+    struct GraphKey {
+        const void* A = nullptr;
+        int64_t lda = -1, n = -1;
+        const void* W = nullptr;
+        const void* pack = nullptr;
+        int use_tc = -1, sms = -1;
+        bool operator==(const GraphKey& o) const {
+            return A == o.A && lda == o.lda && n == o.n && W == o.W && pack == o.pack && use_tc == o.use_tc &&
+                   sms == o.sms;
+        }
+    };
+    // Two graphs (for example one per buffer of a caller that uploads the
+    // next system while this one is solved); the two keys seen last decide
+    // what is worth capturing.
+    struct Graph {
+        GraphKey key;
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;  // kernels per replay
+        uint64_t used = 0;
+    };
+    Graph graphs[2];
+    GraphKey seen[2];
+    uint64_t tick = 0;
+    // Multi-right-hand-side solve (block_solve.cu), built on first use after
+    // a factorization.
+    BlockSolveState* block = nullptr;
+};
+
+// Index quadruple of a depth-2 butterfly: {i, i+q, i+2q, i+3q}, q = np/4.
+// Transposed application T^T = L1^T L2^T (first the two level-2 blocks, then
+// level 1) of a butterfly with diagonals d = [a (h), b (h), e (h), f (h)],
+// h = np/2: level-2 block s pairs (s h + i, s h + i + q) with e[s q + i],
+// f[s q + i]; level 1 pairs (i', i' + h) with a[i'], b[i'].
+template <class T>
+__device__ __forceinline__ void bfly_T4(T x[4], const double* d, int64_t np, int64_t i) {
+    const int64_t h = np / 2, q = np / 4;
+    const double r = 0.70710678118654752440;
+    const double* a = d;
+    const double* b = d + h;
+    const double* e = d + 2 * h;
+    const double* f = d + 3 * h;
+    // level-2 transpose: halves s = 0 (x0,x1) and s = 1 (x2,x3)
+    T z[4];
+    z[0] = (x[0] + x[1]) * (e[i] * r);
+    z[1] = (x[0] - x[1]) * (f[i] * r);
+    z[2] = (x[2] + x[3]) * (e[q + i] * r);
+    z[3] = (x[2] - x[3]) * (f[q + i] * r);
+    // level-1 transpose: pairs (i, i+h) -> (z0, z2), (i+q, i+q+h) -> (z1, z3)
+    x[0] = (z[0] + z[2]) * (a[i] * r);
+    x[2] = (z[0] - z[2]) * (b[i] * r);
+    x[1] = (z[1] + z[3]) * (a[i + q] * r);
+    x[3] = (z[1] - z[3]) * (b[i + q] * r);
+}
+
+// Forward application T = L2 L1 (level 1, then level 2).
+template <class T>
+__device__ __forceinline__ void bfly_N4(T x[4], const double* d, int64_t np, int64_t i) {
+    const int64_t h = np / 2, q = np / 4;
+    const double r = 0.70710678118654752440;
+    const double* a = d;
+    const double* b = d + h;
+    const double* e = d + 2 * h;
+    const double* f = d + 3 * h;
+    T z[4];
+    z[0] = (x[0] * a[i] + x[2] * b[i]) * r;
+    z[2] = (x[0] * a[i] - x[2] * b[i]) * r;
+    z[1] = (x[1] * a[i + q] + x[3] * b[i + q]) * r;
+    z[3] = (x[1] * a[i + q] - x[3] * b[i + q]) * r;
+    x[0] = (z[0] * e[i] + z[1] * f[i]) * r;
+    x[1] = (z[0] * e[i] - z[1] * f[i]) * r;
+    x[2] = (z[2] * e[q + i] + z[3] * f[q + i]) * r;
+    x[3] = (z[2] * e[q + i] - z[3] * f[q + i]) * r;
+}
+
+__device__ __forceinline__ float tf32_hi(float x) {
+    uint32_t y;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
+    return __uint_as_float(y);
+}
+
+// Multi-right-hand-side solve with the mixed factors (block_solve.cu).
+int block_solve(DenseSolver* s, MixedState* st, int64_t nrhs, double* B, int64_t ldb, double tol, int maxit,
+                int* iters);
+// Frees the block-solve workspaces (on release of the solver).
+void block_solve_release(MixedState* st);
+// Marks the packed factors stale (a new factorization was enqueued).
+void block_solve_invalidate(MixedState* st);
+
+}  // namespace sieb200

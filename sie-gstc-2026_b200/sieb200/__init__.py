@@ -19,6 +19,6 @@ from .solvers import (EXTERIOR, INTERIOR, Context, DenseLuSolver, DielectricOpti
                       PecOptions, PlaneWaveExcitation, assemble_matrix, assemble_matrix_device,
                       assemble_rhs, default_context, incident_fields, matvec, matvec_matrix_free,
                       solve_dielectric_dense,
-                      solve_gstc_dense, solve_gstc_dense_batch, solve_pec_dense)
+                      solve_gstc_dense, solve_gstc_dense_batch, solve_pec_dense, zgemm)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

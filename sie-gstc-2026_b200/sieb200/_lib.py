@@ -20,7 +20,7 @@ OK, INVALID_ARG, OVERFLOW, SINGULAR, NONFINITE, NOT_CONVERGED, CUDA_ERROR, TIMEO
 VARIANT_T, VARIANT_N, VARIANT_N_JUMP = 0, 1, 2
 NTL_SURFACE, NTL_LINE = 0, 1
 PEC_EFIE, PMCHWT, GSTC = 0, 1, 2
-ABI_VERSION = 2  # SIEB200_ABI_VERSION of include/sieb200.h
+ABI_VERSION = 3  # SIEB200_ABI_VERSION of include/sieb200.h
 SOLVER_LU_FP64, SOLVER_LU_CUSOLVER, SOLVER_MIXED_IR, SOLVER_GMRES_C64 = 0, 1, 2, 3
 
 _STATUS_NAMES = {
@@ -128,6 +128,7 @@ _SIGNATURES = {
     "sieb200_launch_count": ([], ctypes.c_int64),
     "sieb200_profile_read": ([_P, ctypes.c_int, ctypes.POINTER(_I64), ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "sieb200_zgemm": ([_P, _I64, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P], ctypes.c_int),
     "sieb200_gemm_tf32_sub": ([_P, _I64, _I64, ctypes.c_int, _P, _P, _P, _I64, ctypes.c_int], ctypes.c_int),
     "sieb200_far_field": ([_P, ctypes.POINTER(Mesh), _P, _P, ctypes.c_double, ctypes.c_double, _I64,
                            _P, _P, _P, _P, _P, _P], ctypes.c_int),

@@ -218,8 +218,9 @@ class Context:
         return [(kinds[i], t0[i], t1[i]) for i in range(min(n, count.value))]
 
     def profile_read(self, kernel: int) -> dict:
-        """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec,
-        3: diagonal-block LU, 4: block-step panels (L21 and U12), 5: unused,
+        """kernel 0: split-TF32 trailing GEMM, 1: triangular solves, 2: FP64 matvec
+        and complex GEMM, 3: diagonal-block LU, 4: block-step panels (L21 and U12),
+        5: multi-right-hand-side block triangular solves,
         6: whole mixed factorizations, 7: whole refined solves."""
         n = ctypes.c_int64()
         ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
@@ -458,6 +459,17 @@ class DenseLuSolver:
             self.close()
         except Exception:
             pass
+
+
+def zgemm(m: int, nc: int, k: int, a_ptr: int, x_ptr: int, c_ptr: int, lda: Optional[int] = None,
+          ldx: Optional[int] = None, ldc: Optional[int] = None, alpha: complex = 1.0, beta: complex = 0.0,
+          ctx: Optional[Context] = None) -> None:
+    """C = alpha A X + beta C on device complex128 data (column-major)."""
+    ctx = ctx or default_context()
+    al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
+    _lib.check(_lib.lib().sieb200_zgemm(ctx.handle, int(m), int(nc), int(k), a_ptr, int(lda or m), x_ptr,
+                                        int(ldx or k), c_ptr, int(ldc or m), al, be))
 
 
 def matvec(n: int, a_ptr: int, x_ptr: int, y_ptr: int, lda: Optional[int] = None, prec: int = 0,

@@ -23,7 +23,7 @@ def _tf32(x):
     return b.view(np.float32)
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 @pytest.mark.parametrize("m2,n", [(256, 128), (300, 200), (1000, 517), (4096, 1500)])
 def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
     import torch
@@ -54,11 +54,13 @@ def _pmchwt(level=2, solver="lu_cusolver", rule=5):
     return m, o
 
 
-@pytest.mark.parametrize("trailing", ["tc", "simt"])
+@pytest.mark.parametrize("trailing", ["tc", "tc_load_store", "tc_reduce", "simt"])
 def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
     import sieb200
     if trailing == "simt":
         monkeypatch.setenv("SIEB200_TRAILING_SIMT", "1")
+    if trailing in ("tc_load_store", "tc_reduce"):
+        monkeypatch.setenv("SIEB200_GEMM_MODE", "2" if trailing == "tc_load_store" else "3")
     m, o = _pmchwt(2)
     ref = sieb200.solve_dielectric_dense(m, o, sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
     o.solver = "mixed_ir"
