@@ -441,11 +441,31 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
         c.synchronize()
         if i > 0:
             fp64_times.append(a.elapsed_time(c) / 1e3)
-    t_fp64 = max_over_ranks(statistics.mean(fp64_times))
+    t_cusolver = max_over_ranks(statistics.mean(fp64_times))
     x_fp64 = x.clone()
     rel_diff = float(torch.linalg.vector_norm(x_mixed - x_fp64).item() / torch.linalg.vector_norm(x_fp64).item())
     del Zw
     fp64.close()
+    # The library's own FP64 LU (complex128 butterfly LU, FP64 GEMM trailing
+    # update, FP64 refinement) on the same system; Z stays intact.
+    own = sieb200.DenseLuSolver(N, "lu_fp64", ctx=ctx)
+    own_times = []
+    for i in range(1 + max(2, min(args.steps, 5))):
+        with torch.cuda.stream(stream):
+            x.copy_(b)
+        a, c = ev(), ev()
+        a.record(stream)
+        own.factorize(Z.data_ptr())
+        own.solve(x.data_ptr(), tolerance=1e-10, max_iterations=5)
+        c.record(stream)
+        c.synchronize()
+        if i > 0:
+            own_times.append(a.elapsed_time(c) / 1e3)
+    own.close()
+    t_own = max_over_ranks(statistics.mean(own_times))
+    own_rel_diff = float(torch.linalg.vector_norm(x - x_fp64).item() / torch.linalg.vector_norm(x_fp64).item())
+    # the FP64 baseline is the faster of the two FP64 LUs
+    t_fp64 = min(t_cusolver, t_own)
 
     # End to end through the public API with host buffers, every step: the
     # H2D copy of that step's Z and b from pinned memory, factor + refine,
@@ -507,6 +527,7 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
     with_cpu = rank == 0 and world == 1 and not args.no_cpu
     pec = pec_section(ctx, with_cpu) if not args.skip_sections else None
     multi = multi_rhs_section(ctx, fp64_peak, max_over_ranks) if not args.skip_sections else None
+    sweep = sweep_section(ctx, max_over_ranks) if not args.skip_sections else None
     if adjoint is not None:
         adjoint["grads_per_s"] *= world
         adjoint["fp64_grads_per_s"] *= world
@@ -571,6 +592,9 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
                     "pipelining": "step i+1's H2D copy overlaps step i (copy stream, two device buffers)"},
             "gpu_launches": int(launches), "clocks": clocks.summary(),
             "fp64_lu_solves_per_s": world / t_fp64, "speedup_vs_fp64_lu": (value / world) * t_fp64,
+            "fp64_baseline": "own FP64 LU" if t_own <= t_cusolver else "cuSOLVER Zgetrf/Zgetrs",
+            "fp64_cusolver_solves_per_s": world / t_cusolver, "fp64_own_lu_solves_per_s": world / t_own,
+            "own_fp64_vs_cusolver_rel_diff": own_rel_diff,
             "relative_residual": rel_res, "rel_diff_vs_fp64_lu": rel_diff,
             "rcs_rel_rms_error_vs_mie": mie_err,
             "refinement_iterations": max(iters), "assembly_seconds": t_asm,
@@ -586,6 +610,7 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
             "fields": fields,
             "pec_efie": pec,
             "multi_rhs": multi,
+            "sweep": sweep,
             "adjoint": adjoint,
             "variants": variants,
         }
@@ -868,6 +893,59 @@ def multi_rhs_section(ctx, fp64_peak: float, max_over_ranks) -> dict:
                       "peak_tflops": fp64_peak,
                       "frac": gemm64["flops"] / (gemm64["ms"] / 1e3) / 1e12 / fp64_peak if gemm64["ms"] > 0 else None},
     }
+
+
+SWEEP_WORKLOAD = ("Batched sweep: 32 SIE-GSTC spheres r=1 m of uneven size (geodesic frequency n uniform in "
+                  "6..14: 1080-5880 RWG edges, N=4320-23520), ka uniform in [pi, 4 pi], per-face reciprocal 4x4 "
+                  "maps [[Y, K], [-K^T, Z]] with uniform complex entries (Y, Z symmetric, +2 I), seeded; Dunavant "
+                  "rule 5; one x-polarised plane wave each; mixed solve to rel. residual 1e-10")
+
+
+def sweep_instances(count: int = 32, seed: int = 4):
+    import sieb200
+    rng = np.random.default_rng(seed)
+    insts = []
+    for _ in range(count):
+        n = int(rng.integers(6, 15))
+        ka = float(rng.uniform(np.pi, 4 * np.pi))
+        m = sieb200.geodesic_sphere(1.0, n)
+        nf = m.num_faces
+        c = lambda *sh: rng.uniform(-1, 1, sh) + 1j * rng.uniform(-1, 1, sh)  # noqa: E731
+        Y = c(nf, 2, 2)
+        Y = (Y + Y.transpose(0, 2, 1)) / 2 + 2 * np.eye(2)
+        Zm = c(nf, 2, 2)
+        Zm = (Zm + Zm.transpose(0, 2, 1)) / 2 + 2 * np.eye(2)
+        K = 0.5 * c(nf, 2, 2)
+        L = np.concatenate([np.concatenate([Y, K], 2), np.concatenate([-K.transpose(0, 2, 1), Zm], 2)], 1)
+        t = np.concatenate([L.reshape(nf, 16), np.linalg.inv(L).reshape(nf, 16)], 1)
+        o = sieb200.GstcSieOptions(frequency_hz=ka * C0 / (2 * np.pi), quadrature_rule=5, solver="mixed_ir")
+        insts.append(sieb200.SweepInstance(m, t, o, exterior=sieb200.PlaneWaveExcitation()))
+    return insts
+
+
+def sweep_section(ctx, max_over_ranks) -> dict:
+    """Config-4 sweep through sieb200_solve_gstc_sweep: the instances one
+    after another (one lane) against the autotuned lane count (each
+    candidate timed once here and cached by sieb200.autotune)."""
+    import sieb200
+    from sieb200 import autotune
+    insts = sweep_instances()
+    sizes = [4 * i.mesh.num_edges for i in insts]
+    res, _ = sieb200.solve_gstc_sweep_batched(insts, concurrency=4, ctx=ctx)  # warm-up
+    best, timings = autotune.tune_sweep(insts, ctx=ctx)
+    t_seq = max_over_ranks(timings[1])
+    t_best = max_over_ranks(timings[best])
+    res, _ = sieb200.solve_gstc_sweep_batched(insts, concurrency=best, ctx=ctx)
+    flops = sum(8.0 * float(n) ** 3 for n in sizes)  # split-TF32 LU: 3 x (8/3) N^3
+    return {"workload": SWEEP_WORKLOAD, "instances": len(insts), "N_min": min(sizes), "N_max": max(sizes),
+            "sequential_seconds": t_seq, "sequential_solves_per_s": len(insts) / t_seq,
+            "batched_seconds": t_best, "batched_solves_per_s": len(insts) / t_best,
+            "speedup_vs_sequential": t_seq / t_best, "autotuned_concurrency": best,
+            "seconds_by_concurrency": {str(k): v for k, v in timings.items()},
+            "max_relative_residual": max(r.metrics["relative_residual"] for r in res),
+            "max_refinement_iterations": max(r.metrics["refinement_iterations"] for r in res),
+            "tf32_tflops_effective": flops / t_best / 1e12,
+            "timing": "wall clock around the library call (host tensors in, host currents out)"}
 
 
 def adjoint_section(ctx, steps: int, max_over_ranks):

@@ -43,8 +43,8 @@ enum {
 const char* sieb200_last_error(void);
 /* ABI version of the declarations below; a binding checks it on load.
  * 2: sieb200_options gained variant, ntl_form, line_quadrature_points.
- * 3: sieb200_zgemm; the mixed solver solves several right-hand sides
- *    together (profile kind 5). */
+ * 3: sieb200_zgemm, sieb200_solve_gstc_sweep; the mixed solver solves
+ *    several right-hand sides together (profile kind 5). */
 #define SIEB200_ABI_VERSION 3
 int sieb200_version(void);
 
@@ -91,7 +91,9 @@ typedef struct {
 /* --------------------------------------------------------- options ---- */
 enum { SIEB200_PEC_EFIE = 0, SIEB200_PMCHWT = 1, SIEB200_GSTC = 2 };
 enum {
-    SIEB200_SOLVER_LU_FP64 = 0,     /* own FP64 blocked LU (drop-in for the cuSOLVER path) */
+    SIEB200_SOLVER_LU_FP64 = 0,     /* own FP64 LU: butterfly transform + blocked LU without pivoting in
+                                       complex128 (own kernels, FP64 GEMM trailing update), FP64
+                                       refinement against the intact matrix; no adjoint solves */
     SIEB200_SOLVER_LU_CUSOLVER = 1, /* cusolverDnZgetrf/Zgetrs, as dense_lu_solver.cuh */
     SIEB200_SOLVER_MIXED_IR = 2,    /* split-FP32 tensor-core LU + FP64 GMRES refinement */
     SIEB200_SOLVER_GMRES_C64 = 3    /* Jacobi-preconditioned GMRES, complex64 copy of Z for the
@@ -198,6 +200,32 @@ int sieb200_solve_gstc_dense_batch(sieb200_ctx* ctx, const sieb200_mesh* mesh,
                                    const sieb200_source* sources, int num_cases,
                                    double* currents_out, sieb200_metrics* metrics);
 
+/* Batched sweep of independent SIE-GSTC systems (frequencies, meshes of
+ * uneven size, tensor records): what the reference's sweep workflows do by
+ * running solve_gstc_dense_batch once per instance
+ * (applications/anisotropic_gstc_sphere/sie_gstc_sphere.py:198-297 driving
+ * src/sie_mom/solvers/gstc_sie.cu:622), here in one call. The instances run
+ * largest first on `concurrency` lanes; each lane owns a context (stream,
+ * assembly workspaces) and device buffers sized by its first (largest)
+ * instance, and its trailing GEMMs use 1/concurrency of the SMs, so small
+ * systems' latency-bound steps overlap each other. Per instance: mesh,
+ * tensors (host, 32 per face or 32 if uniform), options (GSTC; solver
+ * SIEB200_SOLVER_MIXED_IR or SIEB200_SOLVER_LU_CUSOLVER), up to one interior
+ * and one exterior source (kind < 0 = absent), host output of 4*num_edges
+ * complex physical currents, optional metrics. seconds_out (optional): wall
+ * time of the sweep. The first failing instance's status and message are
+ * returned (NOT_CONVERGED does not stop the others). */
+typedef struct {
+    sieb200_mesh mesh;
+    const double* tensors;
+    sieb200_options opt;
+    sieb200_source source[2];
+    double* currents_out;
+    sieb200_metrics* metrics;
+} sieb200_sweep_instance;
+int sieb200_solve_gstc_sweep(sieb200_ctx* ctx, const sieb200_sweep_instance* instances, int count,
+                             int concurrency, double* seconds_out);
+
 /* ------------------------------------------------- assembly building blocks */
 /* Dense system matrix exactly as the reference kernels place it
  * (PEC: sie_kernels_assembly.cuh:610-705; PMCHWT: dielectric_kernels.cu:23-149;
@@ -247,8 +275,10 @@ typedef struct sieb200_dense_solver sieb200_dense_solver;
 int sieb200_dense_solver_create(sieb200_ctx* ctx, int64_t n, int method,
                                 sieb200_dense_solver** out);
 int sieb200_dense_solver_destroy(sieb200_dense_solver* s);
-/* A: device, n x n complex128, leading dimension lda. The FP64 methods factor
- * in place (as cusolverDnZgetrf does); the mixed method leaves A intact. */
+/* A: device, n x n complex128, leading dimension lda. SIEB200_SOLVER_LU_CUSOLVER
+ * factors in place (as cusolverDnZgetrf does); the own FP64 LU and the mixed
+ * method keep their factors apart and leave A intact (it must stay alive and
+ * unchanged: their solves refine against it). */
 int sieb200_dense_solver_factorize(sieb200_dense_solver* s, double* A, int64_t lda);
 /* B: device, n x nrhs complex128 (ldb), overwritten with the solution.
  * tolerance/max_iterations apply to the mixed method (relative residual of

@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
+#include <thread>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -381,7 +383,7 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
     SIEB_RETURN_IF(Bb.reserve(sizeof(cplx) * N * ncols));
     SIEB_TRY_CUDA(cudaMemcpyAsync(Bb.ptr, hb.data(), sizeof(cplx) * N * ncols, cudaMemcpyHostToDevice, st));
 
-    const bool in_place = method != SIEB200_SOLVER_MIXED_IR && method != SIEB200_SOLVER_GMRES_C64;
+    const bool in_place = method == SIEB200_SOLVER_LU_CUSOLVER;
     if (o->compute_residual && in_place) {
         SIEB_RETURN_IF(Zcopy.reserve(sizeof(cplx) * N * N));
         SIEB_TRY_CUDA(cudaMemcpyAsync(Zcopy.ptr, Zb.ptr, sizeof(cplx) * N * N, cudaMemcpyDeviceToDevice, st));
@@ -462,6 +464,112 @@ int solve_dense_common(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200
     }
     std::memcpy(out, hx.data(), sizeof(double) * 2 * N * ncols);
     return solve_status;
+}
+
+// ------------------------------------------------------------ batched sweep
+// Device buffers a sweep lane keeps across its instances (largest first, so
+// they are sized once and never freed mid-sweep: cudaFree would stall the
+// other lanes' streams).
+struct LaneBuffers {
+    DeviceBuffer Z, B, Src, R, scratch;
+};
+
+// One SIE-GSTC instance on a lane's own context: assembly, factorization
+// (trailing GEMM on at most sm_cap SMs), refined solve, FP64 residual,
+// physical currents. The same steps as solve_dense_common, without the
+// per-call allocations.
+int lane_solve(sieb200_ctx* ctx, DenseSolver& solver, LaneBuffers& lb, const sieb200_sweep_instance& in,
+               int sm_cap) {
+    const sieb200_options* o = &in.opt;
+    SIEB_CHECK(o->formulation == SIEB200_GSTC, SIEB200_INVALID_ARG, "sweep instances must be SIE-GSTC systems");
+    SIEB_RETURN_IF(validate(&in.mesh, o, in.tensors));
+    SIEB_CHECK(in.currents_out, SIEB200_INVALID_ARG, "sweep instance output must not be null");
+    std::vector<sieb200_source> src;
+    for (int slot = 0; slot < 2; ++slot) {
+        if (in.source[slot].kind < 0) continue;
+        SIEB_CHECK(in.source[slot].region == slot + 1, SIEB200_INVALID_ARG,
+                   "sweep instance excitation does not match its regional slot");
+        src.push_back(in.source[slot]);
+    }
+    SIEB_CHECK(!src.empty(), SIEB200_INVALID_ARG, "sweep instance needs at least one incident region");
+    const int64_t ne = in.mesh.num_edges;
+    const int64_t N = system_dimension(o->formulation, ne);
+    cudaStream_t st = ctx->stream;
+    const auto t_asm = Clock::now();
+    SIEB_RETURN_IF(lb.Z.reserve(sizeof(cplx) * N * N));
+    SIEB_RETURN_IF(assemble_device(ctx, in.mesh, *o, in.tensors, lb.Z.as<cplx>(), N));
+    SIEB_RETURN_IF(lb.Src.reserve(sizeof(cplx) * N * src.size()));
+    SIEB_RETURN_IF(assemble_rhs_device(ctx, in.mesh, *o, src.data(), (int)src.size(), lb.Src.as<cplx>(), N));
+    std::vector<double> hs(2 * N * src.size()), hb(2 * N, 0.0);
+    SIEB_TRY_CUDA(cudaMemcpyAsync(hs.data(), lb.Src.ptr, sizeof(cplx) * N * src.size(), cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    const double asm_s = seconds_since(t_asm);
+    for (size_t k = 0; k < src.size(); ++k)
+        for (int64_t i = 0; i < 2 * N; ++i) hb[i] += hs[2 * N * k + i];
+    const double rhs_norm = host_norm(hb.data(), N);
+    SIEB_CHECK(rhs_norm > 0.0 && std::isfinite(rhs_norm), SIEB200_INVALID_ARG,
+               "incident RHS norm must be finite and nonzero");
+    SIEB_RETURN_IF(lb.B.reserve(sizeof(cplx) * N));
+    SIEB_TRY_CUDA(cudaMemcpyAsync(lb.B.ptr, hb.data(), sizeof(cplx) * N, cudaMemcpyHostToDevice, st));
+    SIEB_CHECK(o->solver == SIEB200_SOLVER_MIXED_IR || o->solver == SIEB200_SOLVER_LU_CUSOLVER ||
+                   o->solver == SIEB200_SOLVER_LU_FP64,
+               SIEB200_INVALID_ARG, "sweep instances are solved by the mixed, the own FP64 or the cuSOLVER LU");
+    const bool in_place = o->solver == SIEB200_SOLVER_LU_CUSOLVER;
+    if (in_place && o->compute_residual) {
+        SIEB_RETURN_IF(lb.R.reserve(sizeof(cplx) * N * N + sizeof(cplx) * N));
+        SIEB_TRY_CUDA(cudaMemcpyAsync(lb.R.ptr, lb.Z.ptr, sizeof(cplx) * N * N, cudaMemcpyDeviceToDevice, st));
+    }
+    solver.ctx = ctx;
+    solver.n = N;
+    solver.method = o->solver;
+    solver.sm_cap = sm_cap;
+    const auto t_fac = Clock::now();
+    SIEB_RETURN_IF(solver.factorize(lb.Z.as<double>(), N));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    const double fac_s = seconds_since(t_fac);
+    const auto t_sol = Clock::now();
+    int iters = 0;
+    const int stt = solver.solve(1, lb.B.as<double>(), N, false, o->tolerance, o->max_iterations, &iters);
+    if (stt != SIEB200_OK && stt != SIEB200_NOT_CONVERGED) return stt;
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    const double sol_s = seconds_since(t_sol);
+    double abs_res = 0.0, res_s = 0.0;
+    if (o->compute_residual) {
+        const auto t_res = Clock::now();
+        const double* Zr = in_place ? lb.R.as<double>() : lb.Z.as<double>();
+        cplx* r = in_place ? lb.R.as<cplx>() + N * N : nullptr;
+        if (!in_place) {
+            SIEB_RETURN_IF(lb.R.reserve(sizeof(cplx) * N));
+            r = lb.R.as<cplx>();
+        }
+        SIEB_TRY_CUDA(cudaMemcpyAsync(r, hb.data(), sizeof(cplx) * N, cudaMemcpyHostToDevice, st));
+        SIEB_RETURN_IF(gemv_device(ctx, N, Zr, N, 0, lb.B.as<cplx>(), -1.0, r, lb.scratch));
+        std::vector<double> hr(2 * N);
+        SIEB_TRY_CUDA(cudaMemcpyAsync(hr.data(), r, sizeof(cplx) * N, cudaMemcpyDeviceToHost, st));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+        abs_res = host_norm(hr.data(), N);
+        res_s = seconds_since(t_res);
+    }
+    SIEB_TRY_CUDA(cudaMemcpyAsync(in.currents_out, lb.B.ptr, sizeof(cplx) * N, cudaMemcpyDeviceToHost, st));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(st));
+    sieb200_metrics* m = in.metrics;
+    if (m) {
+        std::memset(m, 0, sizeof(*m));
+        m->matrix_dimension = N;
+        m->dense_matrix_bytes = (int64_t)(sizeof(cplx) * N * N);
+        m->assembly_seconds = asm_s;
+        m->factorization_seconds = fac_s;
+        m->solve_seconds = sol_s;
+        m->residual_seconds = res_s;
+        m->residual_computed = o->compute_residual ? 1 : 0;
+        m->rhs_norm = rhs_norm;
+        m->absolute_residual = abs_res;
+        m->relative_residual = o->compute_residual ? abs_res / rhs_norm : 0.0;
+        m->refinement_iterations = iters;
+        m->solver = o->solver;
+    }
+    SIEB_RETURN_IF(finish_currents(*o, ne, in.currents_out, m));
+    return stt;
 }
 
 }  // namespace
@@ -639,6 +747,74 @@ int sieb200_solve_gstc_dense_batch(sieb200_ctx* ctx, const sieb200_mesh* mesh,
     }
     return solve_dense_common(ctx, mesh, opt, tensors, flat.data(), num_cases, cols.data(),
                               (int)flat.size(), currents_out, m);
+}
+
+int sieb200_solve_gstc_sweep(sieb200_ctx* ctx, const sieb200_sweep_instance* instances, int count,
+                             int concurrency, double* seconds_out) {
+    SIEB_CHECK(ctx && instances && count > 0, SIEB200_INVALID_ARG, "sweep needs a context and at least one instance");
+    SIEB_CHECK(concurrency >= 1, SIEB200_INVALID_ARG, "sweep concurrency must be at least 1");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    // Largest systems first (their cost grows as N^3): each lane takes the
+    // next one as it finishes, so the lanes end close together.
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return instances[a].mesh.num_edges > instances[b].mesh.num_edges;
+    });
+    const int lanes = std::min(concurrency, count);
+    const int sm_cap = lanes > 1 ? std::max(16, ctx->sm_count / lanes) : 0;
+    std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
+    std::mutex mu;
+    int status = SIEB200_OK;
+    std::string message;
+    const int device = ctx->device;
+    auto lane = [&]() {
+        sieb200_ctx* lctx = nullptr;
+        int rc = sieb200_ctx_create(device, &lctx);
+        if (rc == SIEB200_OK) {
+            DenseSolver solver;
+            LaneBuffers lb;
+            for (int k = next.fetch_add(1); k < count && !failed.load(); k = next.fetch_add(1)) {
+                rc = lane_solve(lctx, solver, lb, instances[order[k]], sm_cap);
+                if (rc != SIEB200_OK && rc != SIEB200_NOT_CONVERGED) {
+                    set_error("sweep instance " + std::to_string(order[k]) + ": " + g_last_error);
+                    break;
+                }
+                if (rc == SIEB200_NOT_CONVERGED) {
+                    std::lock_guard<std::mutex> lock(mu);
+                    if (status == SIEB200_OK) {
+                        status = rc;
+                        message = "sweep instance " + std::to_string(order[k]) + ": " + g_last_error;
+                    }
+                    rc = SIEB200_OK;
+                }
+            }
+            mixed_release(&solver);
+            lb.Z.release(); lb.B.release(); lb.Src.release(); lb.R.release(); lb.scratch.release();
+            sieb200_ctx_destroy(lctx);
+        }
+        if (rc != SIEB200_OK) {
+            failed.store(true);
+            std::lock_guard<std::mutex> lock(mu);
+            if (status == SIEB200_OK || status == SIEB200_NOT_CONVERGED) {
+                status = rc;
+                message = g_last_error;
+            }
+        }
+    };
+    const auto t0 = Clock::now();
+    if (lanes == 1) {
+        lane();
+    } else {
+        std::vector<std::thread> pool;
+        for (int l = 0; l < lanes; ++l) pool.emplace_back(lane);
+        for (auto& t : pool) t.join();
+    }
+    if (seconds_out) *seconds_out = seconds_since(t0);
+    if (status != SIEB200_OK) set_error(message);
+    return status;
 }
 
 int sieb200_assemble_matrix(sieb200_ctx* ctx, const sieb200_mesh* mesh, const sieb200_options* opt,

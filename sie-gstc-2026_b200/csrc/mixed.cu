@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "mixed.cuh"
@@ -41,6 +42,9 @@ constexpr int kSmemPanel = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(flo
 // blocks; its size also keeps it off SMs that hold a trailing-GEMM CTA.
 constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
 constexpr int kDiagThreads = 256;  // diagonal-block kernel: 8 warps of NB / 8 columns
+// The same two kernels in complex128 (own FP64 LU).
+constexpr int kSmemPanel64 = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(double2);
+constexpr int kSmemDiagUpd64 = 2 * NB * (NB + 1) * (int)sizeof(double2);
 
 
 static void drop_graphs(MixedState* st) {
@@ -68,9 +72,10 @@ __global__ void rbt_init_kernel(double* diag, int64_t np, uint64_t seed) {
 }
 
 // W = U^T A_pad V, read A (c128, n x n, lda) once, write W (c64).
+template <class T>
 __global__ void rbt_matrix_kernel(const cplx* __restrict__ A, int64_t lda, int64_t n, int64_t np,
                                   const double* __restrict__ du, const double* __restrict__ dv,
-                                  float2* __restrict__ W, int64_t ldw) {
+                                  T* __restrict__ W, int64_t ldw) {
     const int64_t q = np / 4;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t j = blockIdx.y;
@@ -108,7 +113,7 @@ __global__ void rbt_matrix_kernel(const cplx* __restrict__ A, int64_t lda, int64
     for (int t = 0; t < 4; ++t)
 #pragma unroll
         for (int s = 0; s < 4; ++s)
-            W[(i + s * q) + (j + t * q) * ldw] = make_float2((float)blk[s][t].re, (float)blk[s][t].im);
+            W[(i + s * q) + (j + t * q) * ldw] = T{(decltype(T::x))blk[s][t].re, (decltype(T::x))blk[s][t].im};
 }
 
 // y = U^T x_pad (vector); x has n entries (rest treated as 0).
@@ -164,6 +169,31 @@ __device__ __forceinline__ float2 shfl_c(float2 v, int src) {
     return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
 
+// The same helpers for complex128, so that the block kernels below run in
+// either precision (complex64 for the mixed LU, complex128 for the own FP64
+// LU).
+__device__ __forceinline__ double2 cmulf(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cnegf(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double2 cfmsf(double2 a, double2 c, double2 x) {
+    return make_double2(fma(-c.x, x.x, fma(c.y, x.y, a.x)), fma(-c.x, x.y, fma(-c.y, x.x, a.y)));
+}
+__device__ __forceinline__ double2 shfl_c(double2 v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+template <class T> struct RealOf;
+template <> struct RealOf<float2> { using type = float; };
+template <> struct RealOf<double2> { using type = double; };
+template <class T> __device__ __forceinline__ T cmk(double x, double y);
+template <> __device__ __forceinline__ float2 cmk<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+template <> __device__ __forceinline__ double2 cmk<double2>(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+// |pivot|^2 below this counts as a zero pivot.
+__device__ __forceinline__ float tiny_pivot(float) { return 1e-30f; }
+__device__ __forceinline__ double tiny_pivot(double) { return 1e-280; }
+
 // Diagonal block: LU without pivoting and both triangular inverses in one
 // pass of NB rank-1 steps over registers. Warp w holds columns
 // [kDiagCols w, kDiagCols (w+1)), lane l rows l and l+32. Step j takes the
@@ -188,23 +218,24 @@ constexpr int kDiagCols = NB / kDiagWarps;
 static_assert(kDiagCols % 2 == 0 && 32 % kDiagCols == 0, "diag column split");
 
 // Steps j = kDiagCols bp + u, u = 0 .. kDiagCols-1, all in row half H.
-template <int H>
-__device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, int w, int lane,
-                                           float2 (*cbuf)[NB], float2* rcps, unsigned* err) {
+template <class T, int H>
+__device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, int lane,
+                                           T (*cbuf)[NB], T* rcps, unsigned* err) {
+    using R = typename RealOf<T>::type;
     constexpr int CW = kDiagCols;
 #pragma unroll
     for (int u = 0; u < CW; ++u) {
         const int j = CW * bp + u, jl = j & 31, buf = u & 1;
         const bool g0 = lane > j, g1 = lane + 32 > j;  // rows below the pivot
-        const float2 z = make_float2(0.f, 0.f);
-        float2 ca0, ca1;
+        const T z = cmk<T>(0.f, 0.f);
+        T ca0, ca1;
         if (w == bp) {  // publish c_j, then update this warp's other columns
-            const float2 piv = shfl_c(a[u][H], jl);
-            const float pm = piv.x * piv.x + piv.y * piv.y;
-            const bool bad = !(pm > 1e-30f) || !isfinite(pm);
+            const T piv = shfl_c(a[u][H], jl);
+            const R pm = piv.x * piv.x + piv.y * piv.y;
+            const bool bad = !(pm > tiny_pivot(pm)) || !isfinite(pm);
             if (bad && lane == 0) atomicCAS(err, 0u, 1u);
-            const float inv = bad ? 0.f : __frcp_rn(pm);
-            const float2 rcp = make_float2(piv.x * inv, -piv.y * inv);
+            const R inv = bad ? R(0) : rcp_rn(pm);
+            const T rcp = cmk<T>(piv.x * inv, -piv.y * inv);
             ca0 = cmulf(a[u][0], rcp);
             ca1 = cmulf(a[u][1], rcp);
             if (lane == jl) {
@@ -216,11 +247,11 @@ __device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, in
             if (lane == 0) rcps[j] = rcp;
             a[u][0] = g0 ? cnegf(ca0) : a[u][0];
             a[u][1] = g1 ? cnegf(ca1) : a[u][1];
-            const float2 cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+            const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
 #pragma unroll
             for (int v = 0; v < CW; ++v) {
                 if (v == u) continue;
-                const float2 x = shfl_c(a[v][H], jl);
+                const T x = shfl_c(a[v][H], jl);
                 if (v < u) {
                     if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
                     a[v][1] = cfmsf(a[v][1], cl1, x);
@@ -235,17 +266,17 @@ __device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, in
             ca0 = cbuf[buf][lane];
             ca1 = cbuf[buf][lane + 32];
             if (w < bp) {  // columns left of the pivot: rows below j only
-                const float2 cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+                const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
 #pragma unroll
                 for (int v = 0; v < CW; ++v) {
-                    const float2 x = shfl_c(a[v][H], jl);
+                    const T x = shfl_c(a[v][H], jl);
                     if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
                     a[v][1] = cfmsf(a[v][1], cl1, x);
                 }
             } else {
 #pragma unroll
                 for (int v = 0; v < CW; ++v) {
-                    const float2 x = shfl_c(a[v][H], jl);
+                    const T x = shfl_c(a[v][H], jl);
                     a[v][0] = cfmsf(a[v][0], ca0, x);
                     a[v][1] = cfmsf(a[v][1], ca1, x);
                 }
@@ -258,58 +289,59 @@ __device__ __forceinline__ void diag_steps(float2 (&a)[kDiagCols][2], int bp, in
 // A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32 FMA), from the two
 // factor blocks staged in dynamic shared memory (kSmemDiagUpd; that size
 // also keeps the kernel off SMs that hold a trailing-GEMM CTA).
-__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __restrict__ W, int64_t ldw,
-                                                               int64_t k0, int kb, float2* __restrict__ Linv,
-                                                               float2* __restrict__ Uinv,
+template <class T>
+__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restrict__ W, int64_t ldw,
+                                                               int64_t k0, int kb, T* __restrict__ Linv,
+                                                               T* __restrict__ Uinv,
                                                                unsigned* __restrict__ err, int64_t kp) {
     constexpr int CW = kDiagCols;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    __shared__ float2 cbuf[2][NB];  // c_j, double-buffered across the step barrier
-    __shared__ float2 rcps[NB];     // 1 / p_j
+    __shared__ T cbuf[2][NB];  // c_j, double-buffered across the step barrier
+    __shared__ T rcps[NB];     // 1 / p_j
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    float2 a[CW][2];
+    T a[CW][2];
 #pragma unroll
     for (int v = 0; v < CW; ++v)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int r = lane + 32 * h, c = CW * w + v;
-            a[v][h] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : make_float2(r == c ? 1.f : 0.f, 0.f);
+            a[v][h] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : cmk<T>(r == c ? 1.f : 0.f, 0.f);
         }
     if (kp >= 0) {
-        float2(*Ls)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);           // [k][row]
-        float2(*Us)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem) + NB;      // [col][k]
+        T(*Ls)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem);           // [k][row]
+        T(*Us)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem) + NB;      // [col][k]
         for (int e = threadIdx.x; e < NB * NB; e += kDiagThreads) {
             const int i = e % NB, q = e / NB;  // i fastest: coalesced columns of W
-            Ls[q][i] = i < kb ? W[(k0 + i) + (kp + q) * ldw] : make_float2(0.f, 0.f);
-            Us[q][i] = q < kb ? W[(kp + i) + (k0 + q) * ldw] : make_float2(0.f, 0.f);
+            Ls[q][i] = i < kb ? W[(k0 + i) + (kp + q) * ldw] : cmk<T>(0.f, 0.f);
+            Us[q][i] = q < kb ? W[(kp + i) + (k0 + q) * ldw] : cmk<T>(0.f, 0.f);
         }
         __syncthreads();
         for (int kk = 0; kk < NB; ++kk) {
-            const float2 l0 = Ls[kk][lane], l1 = Ls[kk][lane + 32];
+            const T l0 = Ls[kk][lane], l1 = Ls[kk][lane + 32];
 #pragma unroll
             for (int v = 0; v < CW; ++v) {
-                const float2 u = Us[CW * w + v][kk];
+                const T u = Us[CW * w + v][kk];
                 a[v][0] = cfmsf(a[v][0], l0, u);
                 a[v][1] = cfmsf(a[v][1], l1, u);
             }
         }
     }
 #pragma unroll 1
-    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<0>(a, bp, w, lane, cbuf, rcps, err);
+    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cbuf, rcps, err);
 #pragma unroll 1
-    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<1>(a, bp, w, lane, cbuf, rcps, err);
+    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<T, 1>(a, bp, w, lane, cbuf, rcps, err);
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < CW; ++v) {
         const int c = CW * w + v;
-        const float2 rc = rcps[c];
+        const T rc = rcps[c];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int r = lane + 32 * h;
             const bool in = r < kb && c < kb;
-            const float2 one = make_float2(1.f, 0.f), z = make_float2(0.f, 0.f);
-            const float2 lv = r > c ? a[v][h] : (r == c ? one : z);
-            const float2 uv = r < c ? cnegf(cmulf(cmulf(a[v][h], rcps[r]), rc)) : (r == c ? rc : z);
+            const T one = cmk<T>(1.f, 0.f), z = cmk<T>(0.f, 0.f);
+            const T lv = r > c ? a[v][h] : (r == c ? one : z);
+            const T uv = r < c ? cnegf(cmulf(cmulf(a[v][h], rcps[r]), rc)) : (r == c ? rc : z);
             Linv[r + c * NB] = in ? lv : z;
             Uinv[r + c * NB] = in ? uv : z;
         }
@@ -326,42 +358,43 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const float2* __r
 // One CTA per 32 rows. Thread (ty, tx) computes rows 2ty, 2ty+1 and columns
 // 4tx .. 4tx+3 with k outermost; inv(U11) is upper triangular, so the k
 // loop stops at the thread's last column (tx is warp-uniform up to a pair).
-__device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                             int64_t r0, int64_t np, const float2* __restrict__ Uinv,
+template <class T>
+__device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                             int64_t r0, int64_t np, const T* __restrict__ Uinv,
                                              float* __restrict__ Apack, int pack, int bx, int64_t kp) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    float2(*Us)[NB + 4] = reinterpret_cast<float2(*)[NB + 4]>(dyn_smem);                       // [k][c]
-    float2(*Ar)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * 8);   // [row][k]
-    float2(*Lr)[NB + 1] = Ar + 32;                                                             // [row][k]
+    T(*Us)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(dyn_smem);                       // [k][c]
+    T(*Ar)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * sizeof(T));   // [row][k]
+    T(*Lr)[NB + 1] = Ar + 32;                                                             // [row][k]
     const int tid = threadIdx.x;
     const int64_t rb = r0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % 32, c = e / 32;
         const int64_t gr = rb + r;
-        Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+        Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
     }
     const int ty = tid & 15, tx = tid >> 4;
     if (kp >= 0) {
         for (int e = tid; e < NB * NB; e += blockDim.x) {
             const int kk = e % NB, c = e / NB;
-            Us[kk][c] = c < kb ? W[(kp + kk) + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+            Us[kk][c] = c < kb ? W[(kp + kk) + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
         }
         for (int e = tid; e < 32 * NB; e += blockDim.x) {
             const int r = e % 32, kk = e / 32;
             const int64_t gr = rb + r;
-            Lr[r][kk] = gr < np ? W[gr + (kp + kk) * ldw] : make_float2(0.f, 0.f);
+            Lr[r][kk] = gr < np ? W[gr + (kp + kk) * ldw] : cmk<T>(0.f, 0.f);
         }
         __syncthreads();
-        float2 upd[2][4];
+        T upd[2][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) upd[i][j] = Ar[2 * ty + i][4 * tx + j];
         for (int kk = 0; kk < NB; ++kk) {
-            const float2 l0 = Lr[2 * ty][kk], l1 = Lr[2 * ty + 1][kk];
+            const T l0 = Lr[2 * ty][kk], l1 = Lr[2 * ty + 1][kk];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const float2 u = Us[kk][4 * tx + j];
+                const T u = Us[kk][4 * tx + j];
                 upd[0][j] = cfmsf(upd[0][j], l0, u);
                 upd[1][j] = cfmsf(upd[1][j], l1, u);
             }
@@ -374,19 +407,19 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
     }
     for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];  // Uinv[k + c*NB]
     __syncthreads();
-    float2 acc[2][4];
+    T acc[2][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = make_float2(0.f, 0.f);
+        for (int j = 0; j < 4; ++j) acc[i][j] = cmk<T>(0.f, 0.f);
     const int kend = min(kb, 4 * tx + 4);
     for (int k = 0; k < kend; ++k) {
-        const float2 a0 = Ar[2 * ty][k], a1 = Ar[2 * ty + 1][k];
+        const T a0 = Ar[2 * ty][k], a1 = Ar[2 * ty + 1][k];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float2 u = Us[k][4 * tx + j];
-            acc[0][j] = make_float2(acc[0][j].x + a0.x * u.x - a0.y * u.y, acc[0][j].y + a0.x * u.y + a0.y * u.x);
-            acc[1][j] = make_float2(acc[1][j].x + a1.x * u.x - a1.y * u.y, acc[1][j].y + a1.x * u.y + a1.y * u.x);
+            const T u = Us[k][4 * tx + j];
+            acc[0][j] = cmk<T>(acc[0][j].x + a0.x * u.x - a0.y * u.y, acc[0][j].y + a0.x * u.y + a0.y * u.x);
+            acc[1][j] = cmk<T>(acc[1][j].x + a1.x * u.x - a1.y * u.y, acc[1][j].y + a1.x * u.y + a1.y * u.x);
         }
     }
     __syncthreads();
@@ -402,6 +435,7 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
         const int64_t gr = rb + rr;
         if (gr < np) W[gr + (k0 + c) * ldw] = Ar[rr][c];
     }
+    if constexpr (!std::is_same<T, float2>::value) return;
     if (!pack) return;
     // ... and to the split realified rows (K fastest: coalesced rows).
     // row 2i: [Re, -Im] per column, row 2i+1: [Im, Re]; layout [hi | hi | lo].
@@ -411,7 +445,7 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
         const int64_t gr = rb + rr;
         if (gr >= np) continue;
         const int c = kk >> 1, h = kk & 1;
-        const float2 v = Ar[rr][c];
+        const T v = Ar[rr][c];
         const float v0 = h == 0 ? v.x : -v.y;   // real row
         const float v1 = h == 0 ? v.y : v.x;    // imaginary row
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
@@ -427,35 +461,36 @@ __device__ __forceinline__ void panel_L_body(float2* __restrict__ W, int64_t ldw
 // columns. Thread (ty, tx) computes rows 4ty .. 4ty+3 and columns 2tx,
 // 2tx+1 with k outermost; inv(L11) is lower triangular, so the k loop stops
 // at the thread's last row (ty is warp-uniform up to a pair).
-__device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                             int64_t c0, int64_t np, const float2* __restrict__ Linv,
+template <class T>
+__device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                             int64_t c0, int64_t np, const T* __restrict__ Linv,
                                              float* __restrict__ Bpack, int pack, int bx) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    float2(*Ls)[NB + 4] = reinterpret_cast<float2(*)[NB + 4]>(dyn_smem);                       // [k][r]
-    float2(*Ac)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * 8);   // [col][k]
+    T(*Ls)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(dyn_smem);                       // [k][r]
+    T(*Ac)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * sizeof(T));   // [col][k]
     const int tid = threadIdx.x;
     for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];  // Linv[r + k*NB]
     const int64_t cb = c0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
-        Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : make_float2(0.f, 0.f);
+        Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : cmk<T>(0.f, 0.f);
     }
     __syncthreads();
     const int tx = tid & 15, ty = tid >> 4;
-    float2 acc[4][2];
+    T acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) acc[i][j] = make_float2(0.f, 0.f);
+        for (int j = 0; j < 2; ++j) acc[i][j] = cmk<T>(0.f, 0.f);
     const int kend = min(kb, 4 * ty + 4);
     for (int k = 0; k < kend; ++k) {
-        const float2 b0 = Ac[2 * tx][k], b1 = Ac[2 * tx + 1][k];
+        const T b0 = Ac[2 * tx][k], b1 = Ac[2 * tx + 1][k];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const float2 l = Ls[k][4 * ty + i];
-            acc[i][0] = make_float2(acc[i][0].x + l.x * b0.x - l.y * b0.y, acc[i][0].y + l.x * b0.y + l.y * b0.x);
-            acc[i][1] = make_float2(acc[i][1].x + l.x * b1.x - l.y * b1.y, acc[i][1].y + l.x * b1.y + l.y * b1.x);
+            const T l = Ls[k][4 * ty + i];
+            acc[i][0] = cmk<T>(acc[i][0].x + l.x * b0.x - l.y * b0.y, acc[i][0].y + l.x * b0.y + l.y * b0.x);
+            acc[i][1] = cmk<T>(acc[i][1].x + l.x * b1.x - l.y * b1.y, acc[i][1].y + l.x * b1.y + l.y * b1.x);
         }
     }
     __syncthreads();
@@ -469,9 +504,9 @@ __device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw
         const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
         if (gc >= np) continue;
-        const float2 v = Ac[c][r];
+        const T v = Ac[c][r];
         if (r < kb) W[(k0 + r) + gc * ldw] = v;
-        if (pack) {
+        if (std::is_same<T, float2>::value && pack) {
             float* col = Bpack + (gc - c0) * K3;
             const float h0 = tf32_hi(v.x), h1 = tf32_hi(v.y);
             col[2 * r] = h0; col[2 * r + 1] = h1;
@@ -484,9 +519,10 @@ __device__ __forceinline__ void panel_U_body(float2* __restrict__ W, int64_t ldw
 // Both panels of a block step in one launch: CTAs [0, nL) form L21 (rows
 // below the diagonal block, with the previous step's update when kp >= 0),
 // the rest U12 (columns right of it).
-__global__ void __launch_bounds__(256, 3) panels_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                                        int64_t s0, int64_t np, const float2* __restrict__ Uinv,
-                                                        const float2* __restrict__ Linv, float* __restrict__ Apack,
+template <class T>
+__global__ void __launch_bounds__(256, 3) panels_kernel(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                        int64_t s0, int64_t np, const T* __restrict__ Uinv,
+                                                        const T* __restrict__ Linv, float* __restrict__ Apack,
                                                         float* __restrict__ Bpack, int pack, int nL, int64_t kp) {
     if ((int)blockIdx.x < nL) panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x, kp);
     else panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x - nL);
@@ -937,6 +973,56 @@ __global__ void conj_transpose_blocks_kernel(const float2* __restrict__ in, floa
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Own FP64 LU: diagonal block k of a triangular solve, Y_k = Inv_k Y_k in
+// place for 16 columns per CTA (complex128; rows beyond the block's width
+// are left alone, the inverse is padded with the identity).
+__global__ void __launch_bounds__(256) fp64_diag_apply_kernel(cplx* __restrict__ Y, int64_t ldy, int64_t k0, int kb,
+                                                              int nrhs, const double2* __restrict__ Inv) {
+    __shared__ double2 ys[16][NB];
+    const int tid = threadIdx.x;
+    const int c0 = blockIdx.x * 16;
+    for (int e = tid; e < 16 * NB; e += blockDim.x) {
+        const int r = e % NB, c = e / NB;
+        const cplx v = (c0 + c < nrhs && r < kb) ? Y[(k0 + r) + (int64_t)(c0 + c) * ldy] : cx(0, 0);
+        ys[c][r] = make_double2(v.re, v.im);
+    }
+    __syncthreads();
+    const int c = tid / 16, r0 = (tid % 16) * 4;
+    double2 acc[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[u] = make_double2(0.0, 0.0);
+    for (int kk = 0; kk < NB; ++kk) {
+        const double2 y = ys[c][kk];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double2 a = __ldg(&Inv[(r0 + u) + kk * NB]);  // column-major, L1/L2 resident
+            acc[u].x = fma(a.x, y.x, fma(-a.y, y.y, acc[u].x));
+            acc[u].y = fma(a.x, y.y, fma(a.y, y.x, acc[u].y));
+        }
+    }
+    const int gc = c0 + c;
+    if (gc >= nrhs) return;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (r0 + u < kb) Y[(k0 + r0 + u) + (int64_t)gc * ldy] = cx(acc[u].x, acc[u].y);
+}
+
+// X(:, c) += D(:, c)
+__global__ void add_cols_kernel(int64_t n, const cplx* __restrict__ D, int64_t ldd, cplx* __restrict__ X,
+                                int64_t ldx) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r < n) X[r + c * ldx] += D[r + c * ldd];
+}
+
+// Y(:, c) = X(:, c) (rectangular copy between leading dimensions)
+__global__ void copy_cols_kernel(int64_t n, const cplx* __restrict__ X, int64_t ldx, cplx* __restrict__ Y,
+                                 int64_t ldy) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (r < n) Y[r + c * ldy] = X[r + c * ldx];
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ host side
@@ -981,9 +1067,11 @@ static int check_err(DenseSolver* s, const char* what) {
 
 static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3);
 
+static int fp64_factorize(DenseSolver* s);
+
 int mixed_factorize(DenseSolver* s) {
-    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG,
-               "own FP64 LU is not available in this build; use SIEB200_SOLVER_LU_CUSOLVER");
+    if (s->method == SIEB200_SOLVER_LU_FP64) return fp64_factorize(s);
+    SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR, SIEB200_INVALID_ARG, "unsupported solver method");
     sieb200_ctx* ctx = s->ctx;
     cudaStream_t stream = ctx->stream;
     MixedState* st = state_of(s);
@@ -1034,8 +1122,8 @@ int mixed_factorize(DenseSolver* s) {
     static bool attrs_set = false;
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiagUpd));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiagUpd));
         attrs_set = true;
     }
 
@@ -1103,7 +1191,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     const int64_t q = np / 4;
-    rbt_matrix_kernel<<<dim3(blocks_for(q, 128), (unsigned)q), 128, 0, stream>>>(
+    rbt_matrix_kernel<float2><<<dim3(blocks_for(q, 128), (unsigned)q), 128, 0, stream>>>(
         reinterpret_cast<const cplx*>(s->A), s->lda, n, np, st->diag, st->diag + 4 * np, st->W, ldw);
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
@@ -1115,7 +1203,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0),
                         8.0 * NB * NB * (kp >= 0 ? 5.0 : 3.0), &ev);
-        diag_lu_kernel<<<1, kDiagThreads, kSmemDiagUpd, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
+        diag_lu_kernel<float2><<<1, kDiagThreads, kSmemDiagUpd, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
                                                                st->Uinv + (size_t)bk * NB * NB, st->err, kp);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
@@ -1135,7 +1223,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         cudaEvent_t ev;
         ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m + (kp >= 0 ? 8.0 * NB * NB * (double)m : 0.0),
                         8.0 * 4.0 * NB * (double)m + (kp >= 0 ? 8.0 * NB * (double)m : 0.0), &ev);
-        panels_kernel<<<(unsigned)(2 * nL), 256, kSmemPanel, stream>>>(
+        panels_kernel<float2><<<(unsigned)(2 * nL), 256, kSmemPanel, stream>>>(
             st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB,
             st->Apack[bk & 1], st->Bpack, st->use_tc, nL, kp);
         SIEB_NOTE_LAUNCH();
@@ -1486,8 +1574,15 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     return check_err(s, "GMRES refinement");
 }
 
+static int fp64_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, double tol, int maxit, int* iters);
+
 int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoint, double tol,
                 int maxit, int* iters) {
+    if (s->method == SIEB200_SOLVER_LU_FP64) {
+        SIEB_CHECK(!adjoint, SIEB200_INVALID_ARG,
+                   "conjugate-transpose solves use the mixed or the cuSOLVER method, not the own FP64 LU");
+        return fp64_solve(s, nrhs, B, ldb, tol, maxit, iters);
+    }
     SIEB_CHECK(s->method == SIEB200_SOLVER_MIXED_IR || s->method == SIEB200_SOLVER_GMRES_C64, SIEB200_INVALID_ARG,
                "unsupported solver method");
     if (!(tol > 0)) tol = 1e-10;
@@ -1518,6 +1613,266 @@ int mixed_solve(DenseSolver* s, int64_t nrhs, double* B, int64_t ldb, bool adjoi
         }
     }
     if (iters) *iters = total;
+    return SIEB200_OK;
+}
+
+// ------------------------------------------------------------ own FP64 LU
+// SIEB200_SOLVER_LU_FP64: the drop-in for the reference's cusolverDnZgetrf /
+// Zgetrs path (include/sie_mom/cuda/dense_lu_solver.cuh:42-166) built from
+// this library's own kernels, all in complex128: the butterfly transform
+// W = U^T A V (A is left intact), blocked LU of W without pivoting (the
+// transform makes pivoting unnecessary with high probability; a zero or
+// non-finite pivot is reported as SIEB200_SINGULAR), the diagonal blocks and
+// both triangular inverses by diag_lu_kernel<double2>, the panels by
+// panels_kernel<double2>, the trailing update C -= L21 U12 by the FP64
+// complex GEMM (zgemm_device), with the same one-block lookahead on a side
+// stream as the mixed factorization. A solve applies V U^{-1} L^{-1} U^T
+// (blocked triangular solves: diagonal inverses plus FP64 GEMM updates) and
+// refines against the intact A in FP64 until the relative residual of every
+// column is <= tol (one correction at most, in practice).
+static int fp64_factorize(DenseSolver* s) {
+    sieb200_ctx* ctx = s->ctx;
+    cudaStream_t stream = ctx->stream;
+    MixedState* st = state_of(s);
+    if (!st) {
+        st = new MixedState();
+        s->gemm_state = st;
+    }
+    const int64_t n = s->n;
+    const int64_t np = ((n + 3) / 4) * 4;
+    const int64_t ldw = ((np + 31) / 32) * 32;
+    const int64_t nbl = (np + NB - 1) / NB;
+    st->n = n; st->np = np; st->ldw = ldw; st->nbl = nbl;
+    st->adj_ready = false;
+    block_solve_invalidate(st);
+    auto up = [](size_t b) { return ((b + 255) / 256) * 256; };
+    const size_t bW = sizeof(double2) * ldw * np;
+    const size_t bInv = sizeof(double2) * NB * NB * nbl;
+    const size_t bDiag = sizeof(double) * 8 * np;
+    const size_t bFlags = sizeof(unsigned) * 16;
+    SIEB_RETURN_IF(s->lu.reserve(up(bW) + 2 * up(bInv) + up(bDiag) + up(bFlags)));
+    char* base = s->lu.as<char>();
+    st->W64 = reinterpret_cast<double2*>(base);
+    st->Linv64 = reinterpret_cast<double2*>(base + up(bW));
+    st->Uinv64 = reinterpret_cast<double2*>(base + up(bW) + up(bInv));
+    st->diag = reinterpret_cast<double*>(base + up(bW) + 2 * up(bInv));
+    st->err = reinterpret_cast<unsigned*>(base + up(bW) + 2 * up(bInv) + up(bDiag));
+    if (!st->side) {
+        int least = 0, greatest = 0;
+        SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
+    }
+    static bool attrs64 = false;
+    if (!attrs64) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemPanel64));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagUpd64));
+        attrs64 = true;
+    }
+    cudaEvent_t ev_fact;
+    ctx->prof.begin(stream, 6, (8.0 / 3.0) * (double)np * np * np, 0.0, &ev_fact);
+    SIEB_TRY_CUDA(cudaMemsetAsync(st->err, 0, bFlags, stream));
+    rbt_init_kernel<<<blocks_for(8 * np, 256), 256, 0, stream>>>(st->diag, np, 0x5EB200ull);
+    SIEB_NOTE_LAUNCH();
+    const int64_t q = np / 4;
+    rbt_matrix_kernel<double2><<<dim3(blocks_for(q, 128), (unsigned)q), 128, 0, stream>>>(
+        reinterpret_cast<const cplx*>(s->A), s->lda, n, np, st->diag, st->diag + 4 * np, st->W64, ldw);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    auto diag_blk = [&](int64_t bk, int64_t kp, cudaStream_t sm) -> int {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        cudaEvent_t ev;
+        ctx->prof.begin(sm, 3, (16.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0), 0.0, &ev);
+        diag_lu_kernel<double2><<<1, kDiagThreads, kSmemDiagUpd64, sm>>>(
+            st->W64, ldw, k0, kb, st->Linv64 + (size_t)bk * NB * NB, st->Uinv64 + (size_t)bk * NB * NB, st->err, kp);
+        SIEB_NOTE_LAUNCH();
+        ctx->prof.end(sm, ev);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    };
+    auto panels = [&](int64_t bk, int64_t kp) -> int {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        const int64_t s0 = k0 + kb;
+        if (s0 >= np) return SIEB200_OK;
+        const int64_t m = np - s0;
+        const int nL = (int)blocks_for(m, 32);
+        cudaEvent_t ev;
+        ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m * (kp >= 0 ? 2.0 : 1.0), 0.0, &ev);
+        panels_kernel<double2><<<(unsigned)(2 * nL), 256, kSmemPanel64, stream>>>(
+            st->W64, ldw, k0, kb, s0, np, st->Uinv64 + (size_t)bk * NB * NB, st->Linv64 + (size_t)bk * NB * NB,
+            nullptr, nullptr, 0, nL, kp);
+        SIEB_NOTE_LAUNCH();
+        ctx->prof.end(stream, ev);
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    };
+    SIEB_RETURN_IF(diag_blk(0, -1, stream));
+    SIEB_RETURN_IF(panels(0, -1));
+    cplx* W = reinterpret_cast<cplx*>(st->W64);
+    for (int64_t bk = 0; bk < nbl; ++bk) {
+        const int64_t k0 = bk * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        const int64_t s0 = k0 + kb;
+        if (s0 >= np) break;
+        const int64_t m = np - s0;
+        const int64_t n1 = std::min<int64_t>(NB, m);
+        SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
+        SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
+        SIEB_RETURN_IF(diag_blk(bk + 1, k0, st->side));
+        SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
+        if (m > n1) {
+            cudaEvent_t ev;
+            ctx->prof.begin(stream, 0, 8.0 * (double)m * (double)(m - n1) * kb,
+                            16.0 * (2.0 * (double)m * (m - n1) + (double)(m + m - n1) * kb), &ev);
+            SIEB_RETURN_IF(zgemm_device(stream, m, m - n1, kb, W + s0 + k0 * ldw, ldw, W + k0 + (s0 + n1) * ldw, ldw,
+                                        W + s0 + (s0 + n1) * ldw, ldw, cx(-1, 0), cx(1, 0)));
+            ctx->prof.end(stream, ev);
+        }
+        SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
+        SIEB_RETURN_IF(panels(bk + 1, k0));
+    }
+    ctx->prof.end(stream, ev_fact);
+    unsigned e = 0;
+    SIEB_TRY_CUDA(cudaMemcpyAsync(&e, st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (e != 0u) {
+        set_error("own FP64 LU: zero or non-finite pivot in a diagonal block (the matrix is singular or the "
+                  "butterfly transform met an unlucky pivot)");
+        return SIEB200_SINGULAR;
+    }
+    return SIEB200_OK;
+}
+
+// Y (np x nrhs, ldy) <- W^{-1} Y with the complex128 factors.
+static int fp64_triangular(DenseSolver* s, MixedState* st, cplx* Y, int64_t ldy, int nrhs) {
+    cudaStream_t stream = s->ctx->stream;
+    const int64_t np = st->np, nbl = st->nbl, ldw = st->ldw;
+    const cplx* W = reinterpret_cast<const cplx*>(st->W64);
+    const unsigned g = blocks_for(nrhs, 16);
+    for (int64_t k = 0; k < nbl; ++k) {
+        const int64_t k0 = k * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        fp64_diag_apply_kernel<<<g, 256, 0, stream>>>(Y, ldy, k0, kb, nrhs, st->Linv64 + (size_t)k * NB * NB);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        const int64_t s0 = k0 + kb;
+        if (s0 < np)
+            SIEB_RETURN_IF(zgemm_device(stream, np - s0, nrhs, kb, W + s0 + k0 * ldw, ldw, Y + k0, ldy, Y + s0, ldy,
+                                        cx(-1, 0), cx(1, 0)));
+    }
+    for (int64_t k = nbl - 1; k >= 0; --k) {
+        const int64_t k0 = k * NB;
+        const int kb = (int)std::min<int64_t>(NB, np - k0);
+        fp64_diag_apply_kernel<<<g, 256, 0, stream>>>(Y, ldy, k0, kb, nrhs, st->Uinv64 + (size_t)k * NB * NB);
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        if (k0 > 0)
+            SIEB_RETURN_IF(zgemm_device(stream, k0, nrhs, kb, W + k0 * ldw, ldw, Y + k0, ldy, Y, ldy, cx(-1, 0),
+                                        cx(1, 0)));
+    }
+    return SIEB200_OK;
+}
+
+static int fp64_solve(DenseSolver* s, int64_t nrhs64, double* Bd, int64_t ldb, double tol, int maxit, int* iters) {
+    MixedState* st = state_of(s);
+    SIEB_CHECK(st && st->W64, SIEB200_INVALID_ARG, "own FP64 LU: factorize() has not run");
+    sieb200_ctx* ctx = s->ctx;
+    cudaStream_t stream = ctx->stream;
+    const int nrhs = (int)nrhs64;
+    const int64_t n = st->n, np = st->np, q = np / 4;
+    const int64_t ldy = ((np + 31) / 32) * 32;
+    if (!(tol > 0)) tol = 1e-10;
+    if (maxit <= 0) maxit = 5;
+    // Y (ldy x nrhs) | X | R | B0 (n x nrhs each)
+    const size_t blk = (size_t)n * nrhs;
+    SIEB_RETURN_IF(s->krylov.reserve(sizeof(cplx) * ((size_t)ldy * nrhs + 3 * blk)));
+    cplx* Y = s->krylov.as<cplx>();
+    cplx* X = Y + (size_t)ldy * nrhs;
+    cplx* R = X + blk;
+    cplx* B0 = R + blk;
+    cplx* B = reinterpret_cast<cplx*>(Bd);
+    const dim3 gv(blocks_for(n, 256), (unsigned)nrhs);
+    copy_cols_kernel<<<gv, 256, 0, stream>>>(n, B, ldb, B0, n);
+    SIEB_NOTE_LAUNCH();
+    copy_cols_kernel<<<gv, 256, 0, stream>>>(n, B, ldb, R, n);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaMemsetAsync(X, 0, sizeof(cplx) * blk, stream));
+    std::vector<cplx> hb(blk);
+    SIEB_TRY_CUDA(cudaMemcpyAsync(hb.data(), B0, sizeof(cplx) * blk, cudaMemcpyDeviceToHost, stream));
+    SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+    std::vector<double> bnorm(nrhs);
+    for (int c = 0; c < nrhs; ++c) {
+        long double acc = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const cplx v = hb[(size_t)c * n + i];
+            acc += (long double)v.re * v.re + (long double)v.im * v.im;
+        }
+        bnorm[c] = std::sqrt((double)acc);
+        SIEB_CHECK(bnorm[c] > 0 && std::isfinite(bnorm[c]), SIEB200_INVALID_ARG,
+                   "right-hand side norm must be finite and nonzero");
+    }
+    int it = 0;
+    std::vector<cplx> hr(blk);
+    for (;;) {
+        // correction D = V W^{-1} U^T R, X += D
+        for (int c = 0; c < nrhs; ++c) {
+            rbt_vec_T_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(R + (size_t)c * n, n, np, st->diag,
+                                                                     Y + (size_t)c * ldy);
+            SIEB_NOTE_LAUNCH();
+        }
+        cudaEvent_t ev;
+        ctx->prof.begin(stream, 1, 0.0, 16.0 * (double)np * np, &ev);
+        SIEB_RETURN_IF(fp64_triangular(s, st, Y, ldy, nrhs));
+        ctx->prof.end(stream, ev);
+        for (int c = 0; c < nrhs; ++c) {
+            rbt_vec_N_kernel<<<blocks_for(q, 256), 256, 0, stream>>>(Y + (size_t)c * ldy, n, np, st->diag + 4 * np,
+                                                                     R + (size_t)c * n);
+            SIEB_NOTE_LAUNCH();
+        }
+        add_cols_kernel<<<gv, 256, 0, stream>>>(n, R, n, X, n);
+        SIEB_NOTE_LAUNCH();
+        ++it;
+        // R = B - A X in FP64 against the intact matrix
+        copy_cols_kernel<<<gv, 256, 0, stream>>>(n, B0, n, R, n);
+        SIEB_NOTE_LAUNCH();
+        ctx->prof.begin(stream, 2, 8.0 * (double)n * n * nrhs, 16.0 * (double)n * n, &ev);
+        SIEB_RETURN_IF(zgemm_device(stream, n, nrhs, n, reinterpret_cast<const cplx*>(s->A), s->lda, X, n, R, n,
+                                    cx(-1, 0), cx(1, 0)));
+        ctx->prof.end(stream, ev);
+        SIEB_TRY_CUDA(cudaMemcpyAsync(hr.data(), R, sizeof(cplx) * blk, cudaMemcpyDeviceToHost, stream));
+        SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+        bool done = true;
+        for (int c = 0; c < nrhs && done; ++c) {
+            long double acc = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                const cplx v = hr[(size_t)c * n + i];
+                acc += (long double)v.re * v.re + (long double)v.im * v.im;
+            }
+            const double rn = std::sqrt((double)acc);
+            if (!std::isfinite(rn)) {
+                set_error("own FP64 LU produced a non-finite residual");
+                return SIEB200_NONFINITE;
+            }
+            done = rn <= tol * bnorm[c];
+        }
+        if (done) break;
+        if (it >= maxit) {
+            copy_cols_kernel<<<gv, 256, 0, stream>>>(n, X, n, B, ldb);
+            SIEB_NOTE_LAUNCH();
+            if (iters) *iters = it;
+            set_error("own FP64 LU refinement did not reach the tolerance within max_iterations");
+            return SIEB200_NOT_CONVERGED;
+        }
+    }
+    copy_cols_kernel<<<gv, 256, 0, stream>>>(n, X, n, B, ldb);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    if (iters) *iters = it;
     return SIEB200_OK;
 }
 

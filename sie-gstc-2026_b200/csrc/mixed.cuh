@@ -74,6 +74,11 @@ struct MixedState {
     // Multi-right-hand-side solve (block_solve.cu), built on first use after
     // a factorization.
     BlockSolveState* block = nullptr;
+    // Own FP64 LU (SIEB200_SOLVER_LU_FP64): the same butterfly transform and
+    // blocked schedule in complex128, factors in W64 (np x np, ld ldw).
+    double2* W64 = nullptr;
+    double2* Linv64 = nullptr;
+    double2* Uinv64 = nullptr;
 };
 
 // Index quadruple of a depth-2 butterfly: {i, i+q, i+2q, i+3q}, q = np/4.

@@ -14,11 +14,13 @@ from .farfield import (MetasurfaceFarFieldEvaluator, bistatic_rcs, evaluate_surf
                        spherical_frames)
 from .mesh import MeshData, build_edges, geodesic_sphere, icosphere, infer_sphere_radius, load_obj, make_mesh, \
     revolved_spindle, save_obj
+from . import autotune  # noqa: F401
 from .solvers import (EXTERIOR, INTERIOR, Context, DenseLuSolver, DielectricOptions,
                       DipoleExcitation, GstcExcitationCase, GstcSieOptions, IsotropicMedium,
                       PecOptions, PlaneWaveExcitation, assemble_matrix, assemble_matrix_device,
                       assemble_rhs, default_context, incident_fields, matvec, matvec_matrix_free,
                       solve_dielectric_dense,
-                      solve_gstc_dense, solve_gstc_dense_batch, solve_pec_dense, zgemm)
+                      solve_gstc_dense, solve_gstc_dense_batch, solve_gstc_sweep_batched, solve_pec_dense,
+                      SweepInstance, zgemm)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -82,6 +82,11 @@ class Metrics(ctypes.Structure):
         return d
 
 
+class SweepInstance(ctypes.Structure):
+    _fields_ = [("mesh", Mesh), ("tensors", ctypes.c_void_p), ("opt", Options), ("source", Source * 2),
+                ("currents_out", ctypes.c_void_p), ("metrics", ctypes.POINTER(Metrics))]
+
+
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _SIGNATURES = {
@@ -128,6 +133,8 @@ _SIGNATURES = {
     "sieb200_launch_count": ([], ctypes.c_int64),
     "sieb200_profile_read": ([_P, ctypes.c_int, ctypes.POINTER(_I64), ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "sieb200_solve_gstc_sweep": ([_P, _P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)],
+                                 ctypes.c_int),
     "sieb200_zgemm": ([_P, _I64, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P], ctypes.c_int),
     "sieb200_gemm_tf32_sub": ([_P, _I64, _I64, ctypes.c_int, _P, _P, _P, _I64, ctypes.c_int], ctypes.c_int),
     "sieb200_far_field": ([_P, ctypes.POINTER(Mesh), _P, _P, ctypes.c_double, ctypes.c_double, _I64,

@@ -331,6 +331,58 @@ def solve_gstc_dense(mesh: MeshData, tensors, options: GstcSieOptions, source,
     return solve_gstc_dense_batch(mesh, tensors, options, [case], ctx)[0]
 
 
+@dataclass
+class SweepInstance:
+    """One system of a batched sweep: a mesh, its tensor records, GSTC
+    options and up to one interior and one exterior source."""
+    mesh: MeshData
+    tensors: object
+    options: "GstcSieOptions"
+    exterior: Optional[object] = None
+    interior: Optional[object] = None
+
+
+def solve_gstc_sweep_batched(instances: Sequence[SweepInstance], concurrency="auto",
+                             ctx: Optional[Context] = None):
+    """All instances in one library call (sieb200_solve_gstc_sweep): largest
+    first over `concurrency` lanes that run concurrently on the GPU, each
+    lane's trailing GEMMs on its share of the SMs. concurrency "auto" takes
+    the autotuned lane count for these sizes (sieb200.autotune). Returns
+    (list of SolveResult in input order, wall seconds)."""
+    ctx = ctx or default_context()
+    if len(instances) == 0:
+        raise ValueError("a sweep needs at least one instance")
+    if concurrency == "auto":
+        from .autotune import sweep_concurrency
+        concurrency = sweep_concurrency([4 * inst.mesh.num_edges for inst in instances], ctx=ctx)
+    arr = (_lib.SweepInstance * len(instances))()
+    keep = []
+    outs = []
+    metrics = (_lib.Metrics * len(instances))()
+    for i, inst in enumerate(instances):
+        if inst.interior is None and inst.exterior is None:
+            raise ValueError(f"sweep instance {i}: at least one incident region is required")
+        t = _tensor_array(inst.mesh, inst.tensors, inst.options.tensors_are_uniform)
+        out = np.zeros(4 * inst.mesh.num_edges, dtype=np.complex128)
+        keep.append(t)
+        outs.append(out)
+        a = arr[i]
+        a.mesh = inst.mesh.as_c()
+        a.tensors = t.ctypes.data
+        a.opt = to_c_options(inst.options, _lib.GSTC)
+        for slot, src in enumerate((inst.interior, inst.exterior)):
+            if src is None:
+                a.source[slot].kind = -1
+            else:
+                a.source[slot] = src.as_c()
+        a.currents_out = out.ctypes.data
+        a.metrics = ctypes.pointer(metrics[i])
+    secs = ctypes.c_double()
+    _lib.check(_lib.lib().sieb200_solve_gstc_sweep(ctx.handle, arr, len(instances), int(concurrency),
+                                                   ctypes.byref(secs)))
+    return [SolveResult(outs[i], metrics[i].as_dict()) for i in range(len(instances))], secs.value
+
+
 def _formulation_of(options) -> int:
     if isinstance(options, PecOptions):
         return _lib.PEC_EFIE
@@ -420,9 +472,10 @@ def matvec_matrix_free(mesh: MeshData, options, x: np.ndarray, tensors=None,
 class DenseLuSolver:
     """Factorize once, solve many (dense_lu_solver.cuh:17-184).
 
-    Works on device memory addresses (e.g. torch tensors' data_ptr()); the
-    FP64 methods factor in place, the mixed method keeps the matrix intact
-    and refines every solve to `tolerance` against it."""
+    Works on device memory addresses (e.g. torch tensors' data_ptr()).
+    "lu_cusolver" factors in place; "lu_fp64" (own complex128 LU) and
+    "mixed_ir" keep the matrix intact and refine every solve to `tolerance`
+    against it."""
 
     def __init__(self, n: int, method: str = "lu_cusolver", ctx: Optional[Context] = None):
         self.ctx = ctx or default_context()

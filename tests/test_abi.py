@@ -149,6 +149,7 @@ def test_header_compiles_as_c_and_links(tmp_path):
     import sieb200
     src = tmp_path / "caller.c"
     src.write_text(r"""
+#include <stddef.h>
 #include <stdio.h>
 #include "sieb200.h"
 int main(void) {
@@ -163,7 +164,8 @@ int main(void) {
     int64_t ne = 0;
     if (sieb200_build_edges(faces, 4, edges, fe, &ne) != SIEB200_OK || ne != 6) return 5;
     if (sieb200_version() != SIEB200_ABI_VERSION) return 6;
-    printf("%d %zu\n", sieb200_version(), sizeof(sieb200_options));
+    printf("%d %zu %zu %zu\n", sieb200_version(), sizeof(sieb200_options), sizeof(sieb200_sweep_instance),
+           offsetof(sieb200_sweep_instance, currents_out));
     return 0;
 }
 """)
@@ -177,3 +179,19 @@ int main(void) {
     import ctypes
     from sieb200 import _lib
     assert int(r.stdout.split()[1]) == ctypes.sizeof(_lib.Options)
+    assert int(r.stdout.split()[2]) == ctypes.sizeof(_lib.SweepInstance)
+    assert int(r.stdout.split()[3]) == _lib.SweepInstance.currents_out.offset
+
+
+def test_sweep_validation_without_gpu_work():
+    """The sweep refuses empty input and a zero lane count before any work."""
+    import ctypes
+    import sieb200
+    from sieb200 import _lib
+    lib = _lib.lib()
+    arr = (_lib.SweepInstance * 1)()
+    assert lib.sieb200_solve_gstc_sweep(None, arr, 1, 1, None) == _lib.INVALID_ARG
+    assert lib.sieb200_solve_gstc_sweep(None, arr, 0, 1, None) == _lib.INVALID_ARG
+    secs = ctypes.c_double()
+    assert lib.sieb200_solve_gstc_sweep(None, None, 1, 1, ctypes.byref(secs)) == _lib.INVALID_ARG
+    _ = sieb200  # the package exposes the call as solve_gstc_sweep_batched
