@@ -43,7 +43,8 @@ enum {
 const char* sieb200_last_error(void);
 /* ABI version of the declarations below; a binding checks it on load.
  * 2: sieb200_options gained variant, ntl_form, line_quadrature_points.
- * 3: sieb200_zgemm, sieb200_solve_gstc_sweep; the mixed solver solves
+ * 3: sieb200_zgemm, sieb200_solve_gstc_sweep, sieb200_prepare_records,
+ *    the own FP64 LU (SIEB200_SOLVER_LU_FP64); the mixed solver solves
  *    several right-hand sides together (profile kind 5). */
 #define SIEB200_ABI_VERSION 3
 int sieb200_version(void);
@@ -321,6 +322,22 @@ int sieb200_matvec_noalloc(sieb200_ctx* ctx, int64_t n, const void* A, int64_t l
 int sieb200_zgemm(sieb200_ctx* ctx, int64_t m, int64_t nc, int64_t k, const double* A, int64_t lda,
                   const double* X, int64_t ldx, double* C, int64_t ldc, const double* alpha,
                   const double* beta);
+
+/* Surface-parameter record preparation on the device: the per-face checks
+ * and inversion of prepare_tensor_records
+ * (src/sie_mom/gstc/tensor_io.py:17-132), one thread per face in FP64.
+ * maps: device, faces x 16 complex (row-major physical 4x4 map per face).
+ * records_out: device, faces x 32 complex (the map, then its inverse: the
+ * record layout of face_tensors.bin). diag_out: device, faces x 8 doubles:
+ * reciprocity defect, skew-Hermitian defect and off-diagonal size of the
+ * impedance-balanced map (each relative to its largest entry), its largest
+ * and smallest singular values (one-sided Jacobi), the balanced two-sided
+ * inverse residual, the physical inverse residual (Frobenius), and flags
+ * (1 balanced map non-finite, 2 zero pivot, 4 inverse non-finite,
+ * 8 balanced inverse non-finite). The caller applies the reference's
+ * tolerances and messages (sieb200.records). Synchronizes the stream. */
+int sieb200_prepare_records(sieb200_ctx* ctx, int64_t faces, const double* maps, double reference_impedance,
+                            double* records_out, double* diag_out);
 
 /* Split-TF32 tensor-core contraction used by the mixed LU's trailing update
  * (no counterpart in the reference, which calls cuSOLVER): on device data,

@@ -30,6 +30,8 @@ int far_field_device(sieb200_ctx* ctx, const sieb200_mesh& mesh, const double* j
                      double* intensity);
 int incident_fields_device(sieb200_ctx* ctx, const sieb200_options& opt, const sieb200_source& source, int64_t n,
                            const double* points, double* E_out, double* H_out);
+int prepare_records_device(sieb200_ctx* ctx, int64_t faces, const double* maps, double eta, double* records,
+                           double* diag);
 
 namespace {
 thread_local std::string g_last_error;
@@ -982,6 +984,19 @@ int sieb200_zgemm(sieb200_ctx* ctx, int64_t m, int64_t nc, int64_t k, const doub
                                 reinterpret_cast<const cplx*>(X), ldx, reinterpret_cast<cplx*>(C), ldc,
                                 cx(alpha[0], alpha[1]), cx(beta[0], beta[1])));
     ctx->prof.end(ctx->stream, ev);
+    SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SIEB200_OK;
+}
+
+int sieb200_prepare_records(sieb200_ctx* ctx, int64_t faces, const double* maps, double reference_impedance,
+                            double* records_out, double* diag_out) {
+    SIEB_CHECK(ctx && faces >= 0, SIEB200_INVALID_ARG, "invalid record preparation arguments");
+    SIEB_CHECK(std::isfinite(reference_impedance) && reference_impedance > 0, SIEB200_INVALID_ARG,
+               "reference_impedance must be finite and positive");
+    if (faces == 0) return SIEB200_OK;
+    SIEB_CHECK(maps && records_out && diag_out, SIEB200_INVALID_ARG, "record arrays must not be null");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    SIEB_RETURN_IF(prepare_records_device(ctx, faces, maps, reference_impedance, records_out, diag_out));
     SIEB_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     return SIEB200_OK;
 }

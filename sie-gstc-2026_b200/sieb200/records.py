@@ -1,7 +1,10 @@
 """Surface-parameter record preparation on the device, for loops that rebuild
 the GSTC records every step (adjoint design, sweeps): the checks, the
 impedance-balanced inversion and the 32-value record layout of
-src/sie_mom/gstc/tensor_io.py:13-132, batched over faces in torch.
+src/sie_mom/gstc/tensor_io.py:13-132. On a CUDA device one library kernel
+(sieb200_prepare_records, one thread per face: balanced map, constraint
+defects, one-sided Jacobi singular values, pivoted 4x4 inverse, residuals)
+does the per-face work; on the CPU the same steps run batched in torch.
 
 Records: per face the row-major 4x4 map [[Y_ee, Y_em], [Y_me, Y_mm]] followed
 by its full inverse (complex128), the layout face_tensors.bin and the
@@ -38,9 +41,10 @@ def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: 
     losslessness (extraction_method "reciprocal_lossless"), diagonal
     structure (tensor_structure "diagonal"), numerical singularity
     (s_min <= 4 eps s_max) and the two-sided inverse residual (1e-8).
-    Lossless maps are inverted as the Hermitian system (i B) X = i I (LDL^H
-    on the CPU, LU on CUDA; hermitian_solver "ldl" or "lu" forces one), the
-    others by LU."""
+    On CUDA the library's record kernel inverts every map by pivoted
+    elimination (hermitian_solver is not used there); on the CPU lossless
+    maps are inverted as the Hermitian system (i B) X = i I by LDL^H
+    (hermitian_solver "lu" forces LU), the others by LU."""
     torch = _torch()
     dev = torch.device(device) if device is not None else torch.device("cuda")
     eta = float(reference_impedance)
@@ -56,6 +60,8 @@ def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: 
     top = torch.cat((blocks[0], blocks[1]), dim=1)
     bottom = torch.cat((blocks[2], blocks[3]), dim=1)
     matrix = torch.cat((top, bottom), dim=0).permute(2, 0, 1).contiguous()  # (F, 4, 4)
+    if dev.type == "cuda":
+        return _prepare_on_device(matrix, face_count, eta, extraction_method, tensor_structure, dev)
     # impedance balance: eta on the Y_ee block, 1/eta on the Y_mm block
     balanced = matrix.clone()
     balanced[:, :2, :2] *= eta
@@ -126,6 +132,61 @@ def prepare_tensor_records(parameters, face_count: int, *, reference_impedance: 
         "maximum_relative_reciprocity_residual": reciprocity,
         "maximum_relative_skew_hermitian_residual": losslessness,
         "maximum_map_condition_number": float((sv[:, 0] / sv[:, -1]).max()),
+        "maximum_balanced_inverse_residual": residual,
+        "maximum_inverse_residual": physical_residual,
+    }
+
+
+def _prepare_on_device(matrix, face_count: int, eta: float, extraction_method: str, tensor_structure: str, dev):
+    """The checks and inversion by the library's record kernel
+    (sieb200_prepare_records, one thread per face), then the reference's
+    tolerances and messages in the reference's order."""
+    import ctypes
+    from . import _lib
+    from .solvers import Context, default_context
+    torch = _torch()
+    ctx = default_context() if (dev.index or 0) == 0 else Context(dev.index)
+    records = torch.empty((face_count, 32), dtype=torch.complex128, device=dev)
+    diag = torch.empty((face_count, 8), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    _lib.check(_lib.lib().sieb200_prepare_records(ctx.handle, face_count, matrix.data_ptr(), ctypes.c_double(eta),
+                                                  records.data_ptr(), diag.data_ptr()))
+    d = diag.cpu().numpy()
+    flags = d[:, 7].astype(np.int64)
+    if (flags & 1).any():
+        raise ValueError("impedance-balanced surface maps must be finite")
+    reciprocity = float(d[:, 0].max()) if face_count else 0.0
+    losslessness = float(d[:, 1].max()) if face_count else 0.0
+    if reciprocity > CONSTRAINT_TOLERANCE:
+        raise ValueError("surface maps do not satisfy reciprocity")
+    if extraction_method == "reciprocal_lossless" and losslessness > CONSTRAINT_TOLERANCE:
+        raise ValueError("surface maps do not satisfy losslessness")
+    if tensor_structure == "diagonal" and face_count and float(d[:, 2].max()) > CONSTRAINT_TOLERANCE:
+        raise ValueError("surface maps do not satisfy the configured diagonal structure")
+    singular = d[:, 4] <= 4 * np.finfo(float).eps * d[:, 3]
+    if singular.any():
+        raise ValueError(f"surface map is numerically singular at {int(singular.sum())} faces "
+                         f"(first face index {int(np.flatnonzero(singular)[0])}); the current SIE interface "
+                         "requires its full inverse")
+    if (flags & 2).any():
+        raise ValueError("surface map is singular; the current SIE interface requires its full inverse")
+    if (flags & 4).any():
+        raise ValueError("surface map inverse must be finite")
+    if (flags & 8).any():
+        raise ValueError("impedance-balanced inverse must be finite")
+    residual = float(d[:, 5].max()) if face_count else 0.0
+    if not math.isfinite(residual) or residual > INVERSE_TOLERANCE:
+        raise ValueError(f"surface map inversion residual {residual:.3g} exceeds {INVERSE_TOLERANCE}")
+    physical_residual = float(d[:, 6].max()) if face_count else 0.0
+    if not math.isfinite(physical_residual):
+        raise ValueError("physical surface map inversion residual must be finite")
+    return records, {
+        "all_tensors_finite": True,
+        "relative_constraint_tolerance": CONSTRAINT_TOLERANCE,
+        "balanced_inverse_tolerance": INVERSE_TOLERANCE,
+        "maximum_relative_reciprocity_residual": reciprocity,
+        "maximum_relative_skew_hermitian_residual": losslessness,
+        "maximum_map_condition_number": float((d[:, 3] / d[:, 4]).max()) if face_count else 0.0,
         "maximum_balanced_inverse_residual": residual,
         "maximum_inverse_residual": physical_residual,
     }
