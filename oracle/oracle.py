@@ -77,6 +77,39 @@ def reference() -> ctypes.CDLL | None:
     return lib
 
 
+REF_GPU_SO = HERE / "_ref" / "libsieref_gpu.so"
+
+
+def reference_gpu() -> ctypes.CDLL | None:
+    """The reference's own GPU dielectric solver (oracle/ref_gpu_harness.cu,
+    make -C oracle ref_gpu), or None when it has not been built."""
+    if not REF_GPU_SO.exists():
+        return None
+    lib = ctypes.CDLL(str(REF_GPU_SO))
+    lib.ref_gpu_last_error.restype = ctypes.c_char_p
+    lib.ref_gpu_solve_dielectric.argtypes = [_P, _i, _P, _i, _P, _P, _i, _d, _d, _i, _P, _P]
+    lib.ref_gpu_solve_dielectric.restype = _i
+    return lib
+
+
+def reference_gpu_dielectric(lib, mesh, frequency_hz: float, eps_r: float, rule: int):
+    """(physical interior-oriented currents [J, M], timings dict) of the
+    reference's solve_dielectric_dense for an x-polarised plane wave along +z."""
+    V = np.ascontiguousarray(mesh.vertices, dtype=np.float64)
+    F = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    E = np.ascontiguousarray(mesh.edges, dtype=np.int32)
+    FE = np.ascontiguousarray(mesh.faces_edges, dtype=np.int32)
+    ne = E.shape[0]
+    cur = np.zeros(2 * ne, np.complex128)
+    t = np.zeros(6)
+    rc = lib.ref_gpu_solve_dielectric(_p(V), V.shape[0], _p(F), F.shape[0], _p(E), _p(FE), ne, float(frequency_hz),
+                                      float(eps_r), int(rule), _p(cur), _p(t))
+    if rc != 0:
+        raise RuntimeError("reference GPU solve failed: " + lib.ref_gpu_last_error().decode(errors="replace"))
+    return cur, {"device_preparation_seconds": t[0], "assembly_seconds": t[1], "solve_seconds": t[2],
+                 "residual_seconds": t[3], "call_seconds": t[4], "relative_residual": t[5]}
+
+
 def _p(a):
     return None if a is None else a.ctypes.data
 
