@@ -1044,6 +1044,50 @@ def adjoint_section(ctx, steps: int, max_over_ranks):
     }
 
 
+def run_case(args):
+    """One small workload for a profiler capture (ncu -k <kernel> -c <n>):
+    no timing, one short JSON summary. Cases:
+      assembly       T-PMCHWT assembly of the 2000-face sphere, Dunavant rule 17 (twice)
+      factorization  mixed factorization of that system (N = 6000), twice
+      multi_rhs      mixed solve of 64 plane-wave right-hand sides of it
+      fp64_lu        own FP64 LU factorization and solve of it
+    """
+    import torch
+    import sieb200
+    ctx = sieb200.Context(0)
+    mesh, opts = build_problem(17)
+    N = 2 * mesh.num_edges
+    Z = torch.empty((N, N), dtype=torch.complex128, device="cuda")
+    for _ in range(2 if args.case == "assembly" else 1):
+        sieb200.assemble_matrix_device(mesh, opts, Z.data_ptr(), ctx=ctx)
+    ctx.synchronize()
+    out = {"case": args.case, "N": N}
+    if args.case == "factorization":
+        s = sieb200.DenseLuSolver(N, "mixed_ir", ctx=ctx)
+        for _ in range(2):
+            s.factorize(Z.data_ptr())
+        ctx.synchronize()
+        s.close()
+    elif args.case in ("multi_rhs", "fp64_lu"):
+        th = np.linspace(0.0, np.pi, 64 if args.case == "multi_rhs" else 1)
+        srcs = [sieb200.PlaneWaveExcitation(electric_amplitude=(np.cos(a), 0.0, -np.sin(a)),
+                                            propagation_direction=(np.sin(a), 0.0, np.cos(a))) for a in th]
+        B = torch.from_numpy(np.ascontiguousarray(sieb200.assemble_rhs(mesh, opts, srcs, ctx=ctx).T)).cuda()
+        s = sieb200.DenseLuSolver(N, "mixed_ir" if args.case == "multi_rhs" else "lu_fp64", ctx=ctx)
+        s.factorize(Z.data_ptr())
+        torch.cuda.synchronize()
+        out["iterations"] = s.solve(B.data_ptr(), nrhs=len(srcs), tolerance=1e-10, max_iterations=60)
+        ctx.synchronize()
+        s.close()
+    elif args.case != "assembly":
+        raise SystemExit(f"unknown case {args.case}")
+    del Z
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    ctx.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1057,8 +1101,11 @@ def main():
                     help="time only the headline solve (no PEC or 64-right-hand-side sections)")
     ap.add_argument("--adjoint-steps", type=int, default=2,
                     help="timed adjoint gradients on the spindle workload (0 skips them)")
+    ap.add_argument("--case", default=None, help="run one small profiling workload (see run_case) and exit")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run(args)
