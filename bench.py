@@ -1048,6 +1048,7 @@ def run_case(args):
     """One small workload for a profiler capture (ncu -k <kernel> -c <n>):
     no timing, one short JSON summary. Cases:
       assembly       T-PMCHWT assembly of the 2000-face sphere, Dunavant rule 17 (twice)
+      assembly_small T-PMCHWT assembly of a 320-face icosphere (r = 0.5), rule 17 (twice)
       factorization  mixed factorization of that system (N = 6000), twice
       multi_rhs      mixed solve of 64 plane-wave right-hand sides of it
       fp64_lu        own FP64 LU factorization and solve of it
@@ -1056,9 +1057,11 @@ def run_case(args):
     import sieb200
     ctx = sieb200.Context(0)
     mesh, opts = build_problem(17)
+    if args.case == "assembly_small":
+        mesh = sieb200.icosphere(0.5, 2)
     N = 2 * mesh.num_edges
     Z = torch.empty((N, N), dtype=torch.complex128, device="cuda")
-    for _ in range(2 if args.case == "assembly" else 1):
+    for _ in range(2 if args.case.startswith("assembly") else 1):
         sieb200.assemble_matrix_device(mesh, opts, Z.data_ptr(), ctx=ctx)
     ctx.synchronize()
     out = {"case": args.case, "N": N}
@@ -1079,7 +1082,7 @@ def run_case(args):
         out["iterations"] = s.solve(B.data_ptr(), nrhs=len(srcs), tolerance=1e-10, max_iterations=60)
         ctx.synchronize()
         s.close()
-    elif args.case != "assembly":
+    elif not args.case.startswith("assembly"):
         raise SystemExit(f"unknown case {args.case}")
     del Z
     torch.cuda.synchronize()

@@ -11,7 +11,8 @@ functions psi_n(z) = z j_n(z) and xi_n(z) = z h_n^(1)(z) from scipy:
         / [mu1 psi_n(mx) xi_n'(x) - m xi_n(x) psi_n'(mx)]
   (relative permeability mu1 inside, 1 outside; m = sqrt(eps_r mu1);
   B&H eqs. 4.53-4.54 multiplied through by x)
-  PEC: a_n = psi_n(x) / xi_n(x), b_n = psi_n'(x) / xi_n'(x)
+  PEC (the limit m -> infinity of the above): a_n = psi_n'(x) / xi_n'(x),
+  b_n = psi_n(x) / xi_n(x)
 
   S1(theta) = sum_n (2n+1)/(n(n+1)) (a_n pi_n + b_n tau_n)
   S2(theta) = sum_n (2n+1)/(n(n+1)) (a_n tau_n + b_n pi_n)
@@ -57,7 +58,7 @@ def coefficients(x: float, eps_r: complex | None, mu_r: complex = 1.0, n_max: in
     n = np.arange(1, n_max + 1)
     psi, dpsi, xi, dxi = _riccati(n, x)
     if eps_r is None:
-        return psi / xi, dpsi / dxi
+        return dpsi / dxi, psi / xi
     m = np.sqrt(complex(eps_r) * complex(mu_r))
     mx = m * x
     jm = spherical_jn(n, mx)

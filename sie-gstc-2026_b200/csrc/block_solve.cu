@@ -636,7 +636,7 @@ int block_solve(DenseSolver* s, MixedState* st, int64_t nrhs64, double* Bd, int6
         bscale_kernel<<<gv, 256, 0, stream>>>(n, R, n, sd, V, n);
         SIEB_NOTE_LAUNCH();
         std::fill(g.begin(), g.end(), cx(0, 0));
-        for (int c = 0; c < nrhs; ++c) g[c] = cx(active[c] ? beta[c] : 0.0, 0);
+        for (int c = 0; c < nrhs; ++c) g[(size_t)c * (m + 1)] = cx(active[c] ? beta[c] : 0.0, 0);
         int j = 0;
         for (; j < m && total < maxit; ++j, ++total) {
             cplx* vj = V + (size_t)j * blk;

@@ -24,7 +24,10 @@ def _dev(a):
 
 
 def _host(t, rows, cols):
-    return t.cpu().numpy().T.reshape(cols, rows).T
+    # the tensor is (cols, rows): column-major storage of a rows x cols matrix
+    a = t.cpu().numpy().T
+    assert a.shape == (rows, cols)
+    return a
 
 
 @pytest.mark.parametrize("m,nc,k", [(1, 1, 1), (130, 7, 77), (1000, 64, 999), (257, 33, 300), (64, 1, 2000)])

@@ -78,7 +78,9 @@ def test_config1_pec_currents_and_rcs(solver, tol, config1, gpu_ctx, oracle_lib)
         rcs = 4 * np.pi * (np.abs(ft) ** 2 + np.abs(fp) ** 2)
         rcs_o = 4 * np.pi * (np.abs(fto) ** 2 + np.abs(fpo) ** 2)
         assert rel_err(rcs, rcs_o) < 10 * tol
-        assert rel_err(ft, fto) < tol and rel_err(fp, fpo) < tol
+        # both components against the larger field (F_phi vanishes in the phi = 0 cut)
+        scale = max(np.abs(fto).max(), np.abs(fpo).max())
+        assert max(np.abs(ft - fto).max(), np.abs(fp - fpo).max()) < tol * scale
 
 
 def test_config1_matrix_free_product(config1, gpu_ctx):
@@ -191,13 +193,13 @@ def _rcs_vs_mie(m, currents_j, currents_m, eps_r, ctx):
 
 def test_config1_rcs_against_mie(gpu_ctx):
     """Discretization error of the PEC workload's bistatic RCS against the
-    Mie series of a perfectly conducting sphere: a few percent on 1280 faces
-    at ka = 2 pi (the reference's accuracy for this mesh, not a parity bar)."""
+    Mie series of a perfectly conducting sphere: about 1 % on 1280 faces at
+    ka = 2 pi (the oracle's solution shows the same; not a parity bar)."""
     import sieb200
     m = sieb200.icosphere(1.0, 3)
     r = sieb200.solve_pec_dense(m, _pec_options("mixed_ir"), sieb200.PlaneWaveExcitation(), ctx=gpu_ctx)
     err = _rcs_vs_mie(m, r.currents, None, None, gpu_ctx)
-    assert err < 0.1, err
+    assert err < 0.03, err
 
 
 def test_config2_rcs_against_mie(gpu_ctx):
@@ -209,4 +211,4 @@ def test_config2_rcs_against_mie(gpu_ctx):
                                        ctx=gpu_ctx)
     ne = m.num_edges
     err = _rcs_vs_mie(m, r.currents[:ne], r.currents[ne:], 4.0, gpu_ctx)
-    assert err < 0.05, err
+    assert err < 0.03, err

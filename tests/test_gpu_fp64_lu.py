@@ -24,7 +24,10 @@ def _dev(a):
 
 
 def _host(t, rows, cols):
-    return t.cpu().numpy().T.reshape(cols, rows).T
+    # the tensor is (cols, rows): column-major storage of a rows x cols matrix
+    a = t.cpu().numpy().T
+    assert a.shape == (rows, cols)
+    return a
 
 
 @pytest.mark.parametrize("n,nrhs", [(5, 1), (50, 2), (130, 1), (997, 3), (2100, 1)])

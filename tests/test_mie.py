@@ -26,5 +26,13 @@ def test_mie_limits():
     # Rayleigh backscatter: 4 pi k^4 a^6 |(eps-1)/(eps+2)|^2, PEC 9 pi k^4 a^6
     assert abs(mie.bistatic_rcs(k, a, 4.0, np.pi, 0.0) / (4 * np.pi * k ** 4 * a ** 6 * 0.25) - 1) < 1e-4
     assert abs(mie.bistatic_rcs(k, a, None, np.pi, 0.0) / (9 * np.pi * k ** 4 * a ** 6) - 1) < 1e-4
+    # small PEC sphere at theta = 90 degrees: the H-plane (phi = 90) cross
+    # section is 4 times the E-plane one (amplitudes 1 - cos/2 and cos - 1/2);
+    # backscatter alone cannot tell a_n from b_n
+    e = mie.bistatic_rcs(k, a, None, np.pi / 2, 0.0)
+    h = mie.bistatic_rcs(k, a, None, np.pi / 2, np.pi / 2)
+    assert abs(h / e - 4.0) < 1e-3
+    # dielectric Rayleigh sphere: the E-plane cross section vanishes at 90 degrees
+    assert mie.bistatic_rcs(k, a, 4.0, np.pi / 2, 0.0) < 1e-6 * mie.bistatic_rcs(k, a, 4.0, np.pi / 2, np.pi / 2)
     # optical limit of the monostatic PEC cross section: pi a^2
     assert abs(mie.bistatic_rcs(1.0, 60.0, None, np.pi, 0.0, n_max=120) / (np.pi * 60 ** 2) - 1) < 1e-2
