@@ -285,15 +285,16 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
     }
 }
 
-// With kp >= 0 the block first takes the previous block step's update,
-// A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32 FMA), from the two
-// factor blocks staged in dynamic shared memory (kSmemDiagUpd; that size
-// also keeps the kernel off SMs that hold a trailing-GEMM CTA).
+// With kp1 >= 0 (and kp2 >= 0) the block first takes those earlier block
+// steps' updates, A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32
+// FMA), from the factor blocks staged in dynamic shared memory (kSmemDiagUpd;
+// that size also keeps the kernel off SMs that hold a trailing-GEMM CTA).
 template <class T>
 __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restrict__ W, int64_t ldw,
                                                                int64_t k0, int kb, T* __restrict__ Linv,
                                                                T* __restrict__ Uinv,
-                                                               unsigned* __restrict__ err, int64_t kp) {
+                                                               unsigned* __restrict__ err, int64_t kp1,
+                                                               int64_t kp2) {
     constexpr int CW = kDiagCols;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ T cbuf[2][NB];  // c_j, double-buffered across the step barrier
@@ -307,9 +308,12 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
             const int r = lane + 32 * h, c = CW * w + v;
             a[v][h] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw] : cmk<T>(r == c ? 1.f : 0.f, 0.f);
         }
-    if (kp >= 0) {
+    for (int q = 0; q < 2; ++q) {
+        const int64_t kp = q == 0 ? kp1 : kp2;
+        if (kp < 0) continue;
         T(*Ls)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem);           // [k][row]
         T(*Us)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem) + NB;      // [col][k]
+        __syncthreads();  // the previous update's tiles are no longer read
         for (int e = threadIdx.x; e < NB * NB; e += kDiagThreads) {
             const int i = e % NB, q = e / NB;  // i fastest: coalesced columns of W
             Ls[q][i] = i < kb ? W[(k0 + i) + (kp + q) * ldw] : cmk<T>(0.f, 0.f);
@@ -349,19 +353,37 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
 }
 
 
-// L21 = A21 * inv(U11) for rows [r0, np) of the panel columns [k0, k0+kb);
+// Arguments of one block step's panels launch.
+//   kp[0], kp[1]: earlier block steps (column offsets, -1 = none) whose
+//     updates the L rows take first; kpu: the step whose update the U
+//     columns take first (the trailing GEMM runs every second step, so these
+//     columns can lag one step behind);
+//   Apack (at its K offset), a_ld (row stride in floats), a_r0 (first row
+//     packed: pack row 2 (r - a_r0)); Bpack, b_ld, b_c0 likewise for columns.
+struct PanelArgs {
+    int64_t k0 = 0, s0 = 0, np = 0;
+    int kb = 0, nL = 0, pack = 0;
+    int64_t kp[2] = {-1, -1};
+    int64_t kpu = -1;
+    float* Apack = nullptr;
+    int64_t a_ld = 0, a_r0 = 0;
+    float* Bpack = nullptr;
+    int64_t b_ld = 0, b_c0 = 0;
+};
+
+// L21 = A21 * inv(U11) for rows [s0, np) of the panel columns [k0, k0+kb);
 // writes L21 back into W and the split realified rows into Apack.
-// With kp >= 0 the rows first take the previous block step's update of
-// these columns, A21 -= L21(kp) U12(kp)[:, k0:k0+kb] (FP32 FMA; the two
-// factors are the previous step's panels in W), so no separate GEMM
-// launch stands between the steps.
+// The rows first take the updates of the earlier steps in kp,
+// A21 -= L21(kp) U12(kp)[:, k0:k0+kb] (FP32 FMA; the factors are those
+// steps' panels in W), so no separate GEMM launch stands between the steps.
 // One CTA per 32 rows. Thread (ty, tx) computes rows 2ty, 2ty+1 and columns
 // 4tx .. 4tx+3 with k outermost; inv(U11) is upper triangular, so the k
 // loop stops at the thread's last column (tx is warp-uniform up to a pair).
 template <class T>
-__device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                             int64_t r0, int64_t np, const T* __restrict__ Uinv,
-                                             float* __restrict__ Apack, int pack, int bx, int64_t kp) {
+__device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, const PanelArgs& pa,
+                                             const T* __restrict__ Uinv, int bx) {
+    const int64_t k0 = pa.k0, r0 = pa.s0, np = pa.np;
+    const int kb = pa.kb;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     T(*Us)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(dyn_smem);                       // [k][c]
     T(*Ar)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * sizeof(T));   // [row][k]
@@ -374,7 +396,9 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, int
         Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
     }
     const int ty = tid & 15, tx = tid >> 4;
-    if (kp >= 0) {
+    for (int q = 0; q < 2; ++q) {
+        const int64_t kp = pa.kp[q];
+        if (kp < 0) continue;
         for (int e = tid; e < NB * NB; e += blockDim.x) {
             const int kk = e % NB, c = e / NB;
             Us[kk][c] = c < kb ? W[(kp + kk) + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
@@ -436,48 +460,84 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, int
         if (gr < np) W[gr + (k0 + c) * ldw] = Ar[rr][c];
     }
     if constexpr (!std::is_same<T, float2>::value) return;
-    if (!pack) return;
+    if (!pa.pack) return;
     // ... and to the split realified rows (K fastest: coalesced rows).
     // row 2i: [Re, -Im] per column, row 2i+1: [Im, Re]; layout [hi | hi | lo].
-    const int K3 = 6 * NB;
     for (int e = tid; e < 32 * 2 * NB; e += blockDim.x) {
         const int rr = e / (2 * NB), kk = e % (2 * NB);
         const int64_t gr = rb + rr;
-        if (gr >= np) continue;
+        if (gr >= np || gr < pa.a_r0) continue;
         const int c = kk >> 1, h = kk & 1;
         const T v = Ar[rr][c];
         const float v0 = h == 0 ? v.x : -v.y;   // real row
         const float v1 = h == 0 ? v.y : v.x;    // imaginary row
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
-        float* row0 = Apack + (2 * (gr - r0)) * K3;
-        float* row1 = row0 + K3;
+        float* row0 = pa.Apack + (2 * (gr - pa.a_r0)) * pa.a_ld;
+        float* row1 = row0 + pa.a_ld;
         row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
         row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
     }
 }
 
-// U12 = inv(L11) * A12 for columns [c0, np) of the panel rows [k0, k0+kb);
-// writes U12 back into W and the split columns into Bpack. One CTA per 32
+// U12 = inv(L11) * A12 for columns [s0, np) of the panel rows [k0, k0+kb);
+// writes U12 back into W and the split columns into Bpack. With kpu >= 0 the
+// columns first take that step's update, A12 -= L21(kpu)[k0:k0+kb, :]
+// U12(kpu)[:, these columns] (FP32 FMA, both factors from W). One CTA per 32
 // columns. Thread (ty, tx) computes rows 4ty .. 4ty+3 and columns 2tx,
 // 2tx+1 with k outermost; inv(L11) is lower triangular, so the k loop stops
 // at the thread's last row (ty is warp-uniform up to a pair).
 template <class T>
-__device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                             int64_t c0, int64_t np, const T* __restrict__ Linv,
-                                             float* __restrict__ Bpack, int pack, int bx) {
+__device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, const PanelArgs& pa,
+                                             const T* __restrict__ Linv, int bx) {
+    const int64_t k0 = pa.k0, c0 = pa.s0, np = pa.np;
+    const int kb = pa.kb;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     T(*Ls)[NB + 4] = reinterpret_cast<T(*)[NB + 4]>(dyn_smem);                       // [k][r]
     T(*Ac)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(dyn_smem + NB * (NB + 4) * sizeof(T));   // [col][k]
+    T(*Uc)[NB + 1] = Ac + 32;                                                           // [col][k]
     const int tid = threadIdx.x;
-    for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];  // Linv[r + k*NB]
     const int64_t cb = c0 + (int64_t)bx * 32;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
         Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : cmk<T>(0.f, 0.f);
     }
-    __syncthreads();
     const int tx = tid & 15, ty = tid >> 4;
+    if (pa.kpu >= 0) {
+        const int64_t kp = pa.kpu;
+        // L21(kp) rows of this block as Ls[r][kk], U12(kp) columns as Uc[c][kk]
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+            const int r = e % NB, kk = e / NB;
+            Ls[r][kk] = r < kb ? W[(k0 + r) + (kp + kk) * ldw] : cmk<T>(0.f, 0.f);
+        }
+        for (int e = tid; e < 32 * NB; e += blockDim.x) {
+            const int kk = e % NB, c = e / NB;
+            const int64_t gc = cb + c;
+            Uc[c][kk] = gc < np ? W[(kp + kk) + gc * ldw] : cmk<T>(0.f, 0.f);
+        }
+        __syncthreads();
+        T upd[4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) upd[i][j] = Ac[2 * tx + j][4 * ty + i];
+        for (int kk = 0; kk < NB; ++kk) {
+            const T u0 = Uc[2 * tx][kk], u1 = Uc[2 * tx + 1][kk];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const T l = Ls[4 * ty + i][kk];
+                upd[i][0] = cfmsf(upd[i][0], l, u0);
+                upd[i][1] = cfmsf(upd[i][1], l, u1);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) Ac[2 * tx + j][4 * ty + i] = upd[i][j];
+    }
+    for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];  // Linv[r + k*NB]
+    __syncthreads();
     T acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -499,15 +559,14 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, int
 #pragma unroll
         for (int j = 0; j < 2; ++j) Ac[2 * tx + j][4 * ty + i] = acc[i][j];
     __syncthreads();
-    const int K3 = 6 * NB;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % NB, c = e / NB;
         const int64_t gc = cb + c;
         if (gc >= np) continue;
         const T v = Ac[c][r];
         if (r < kb) W[(k0 + r) + gc * ldw] = v;
-        if (std::is_same<T, float2>::value && pack) {
-            float* col = Bpack + (gc - c0) * K3;
+        if (std::is_same<T, float2>::value && pa.pack && gc >= pa.b_c0) {
+            float* col = pa.Bpack + (gc - pa.b_c0) * pa.b_ld;
             const float h0 = tf32_hi(v.x), h1 = tf32_hi(v.y);
             col[2 * r] = h0; col[2 * r + 1] = h1;
             col[2 * NB + 2 * r] = v.x - h0; col[2 * NB + 2 * r + 1] = v.y - h1;
@@ -517,15 +576,13 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, int
 }
 
 // Both panels of a block step in one launch: CTAs [0, nL) form L21 (rows
-// below the diagonal block, with the previous step's update when kp >= 0),
-// the rest U12 (columns right of it).
+// below the diagonal block, after the updates of the steps in kp), the rest
+// U12 (columns right of it, after the update of step kpu).
 template <class T>
-__global__ void __launch_bounds__(256, 3) panels_kernel(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
-                                                        int64_t s0, int64_t np, const T* __restrict__ Uinv,
-                                                        const T* __restrict__ Linv, float* __restrict__ Apack,
-                                                        float* __restrict__ Bpack, int pack, int nL, int64_t kp) {
-    if ((int)blockIdx.x < nL) panel_L_body(W, ldw, k0, kb, s0, np, Uinv, Apack, pack, blockIdx.x, kp);
-    else panel_U_body(W, ldw, k0, kb, s0, np, Linv, Bpack, pack, blockIdx.x - nL);
+__global__ void __launch_bounds__(256, 3) panels_kernel(T* __restrict__ W, int64_t ldw, const T* __restrict__ Uinv,
+                                                        const T* __restrict__ Linv, const PanelArgs pa) {
+    if ((int)blockIdx.x < pa.nL) panel_L_body(W, ldw, pa, Uinv, blockIdx.x);
+    else panel_U_body(W, ldw, pa, Linv, blockIdx.x - pa.nL);
 }
 
 // SIMT trailing update C -= L21 U12 in complex64 (checking path).
@@ -1088,6 +1145,8 @@ int mixed_factorize(DenseSolver* s) {
     block_solve_invalidate(st);
     const char* env = getenv("SIEB200_TRAILING_SIMT");
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
+    const char* pair_env = getenv("SIEB200_PAIR_UPDATE");
+    st->pair = (pair_env && pair_env[0] == '0') ? 0 : 1;
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -1106,7 +1165,7 @@ int mixed_factorize(DenseSolver* s) {
     const int K3 = 6 * NB;
     const size_t bApack = ((sizeof(float) * 2 * np * K3 + 255) / 256) * 256;
     SIEB_RETURN_IF(s->gemm_a.reserve(2 * bApack));
-    SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * K3));
+    SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * 2 * K3));  // the pair schedule's K = 2 x 384
     st->Apack[0] = s->gemm_a.as<float>();
     st->Apack[1] = reinterpret_cast<float*>(s->gemm_a.as<char>() + bApack);
     st->Bpack = s->gemm_b.as<float>();
@@ -1131,7 +1190,7 @@ int mixed_factorize(DenseSolver* s) {
     MixedState::GraphKey key;
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
-    key.use_tc = st->use_tc; key.sms = gemm_sms;
+    key.use_tc = st->use_tc + 2 * st->pair; key.sms = gemm_sms;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -1196,63 +1255,86 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
 
-    // Diagonal block bk (kp >= 0: after the update of step kp / NB).
-    auto diag_blk = [&](int64_t bk, int64_t kp, cudaStream_t sm) -> int {
+    // Diagonal block bk after the updates of the block steps at column
+    // offsets kp1, kp2 (-1 = none).
+    auto diag_blk = [&](int64_t bk, int64_t kp1, int64_t kp2, cudaStream_t sm) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
+        const int nupd = (kp1 >= 0) + (kp2 >= 0);
         cudaEvent_t ev;
-        ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0),
-                        8.0 * NB * NB * (kp >= 0 ? 5.0 : 3.0), &ev);
-        diag_lu_kernel<float2><<<1, kDiagThreads, kSmemDiagUpd, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
-                                                               st->Uinv + (size_t)bk * NB * NB, st->err, kp);
+        ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + nupd * 8.0 * NB * NB * NB,
+                        8.0 * NB * NB * (3.0 + 2.0 * nupd), &ev);
+        diag_lu_kernel<float2><<<1, kDiagThreads, kSmemDiagUpd, sm>>>(
+            st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB, st->Uinv + (size_t)bk * NB * NB, st->err, kp1, kp2);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     };
-    // Both panels of block bk on the context stream (L21 into the A pack of
-    // step bk, after the update of step kp / NB when kp >= 0; U12 into the
-    // B pack).
-    auto panels = [&](int64_t bk, int64_t kp) -> int {
+    // Both panels of block bk on the context stream: L21 after the updates
+    // of the steps kp1, kp2 into the A pack, U12 after the update of step
+    // kpu into the B pack. Pair schedule: the trailing GEMM of an odd step q
+    // applies steps q - 1 and q together (K = 2 x 384), so step j's packs go
+    // to K half j & 1 of one buffer, rows from s0(q) and columns from
+    // s0(q) + NB (q = j | 1); single-step schedule: one K = 384 pack per
+    // step, rows from s0(j), all columns (the GEMM offsets them).
+    const bool pair = st->use_tc && st->pair;
+    const int64_t KP = pair ? 2 * K3 : K3;
+    auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         const int64_t s0 = k0 + kb;
         if (s0 >= np) return SIEB200_OK;
         const int64_t m = np - s0;
-        const int nL = (int)blocks_for(m, 32);
+        PanelArgs pa;
+        pa.k0 = k0; pa.kb = kb; pa.s0 = s0; pa.np = np;
+        pa.nL = (int)blocks_for(m, 32);
+        pa.pack = st->use_tc;
+        pa.kp[0] = kp1; pa.kp[1] = kp2; pa.kpu = kpu;
+        if (pair) {
+            const int half = (int)(bk & 1);
+            const int64_t q_s0 = half ? s0 : s0 + NB;  // s0 of the step whose GEMM uses this pack
+            pa.Apack = st->Apack[0] + half * K3; pa.a_ld = KP; pa.a_r0 = q_s0;
+            pa.Bpack = st->Bpack + half * K3; pa.b_ld = KP; pa.b_c0 = q_s0 + NB;
+        } else {
+            pa.Apack = st->Apack[bk & 1]; pa.a_ld = K3; pa.a_r0 = s0;
+            pa.Bpack = st->Bpack; pa.b_ld = K3; pa.b_c0 = s0;
+        }
+        const int nupd = (kp1 >= 0) + (kp2 >= 0) + (kpu >= 0);
         cudaEvent_t ev;
-        ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m + (kp >= 0 ? 8.0 * NB * NB * (double)m : 0.0),
-                        8.0 * 4.0 * NB * (double)m + (kp >= 0 ? 8.0 * NB * (double)m : 0.0), &ev);
-        panels_kernel<float2><<<(unsigned)(2 * nL), 256, kSmemPanel, stream>>>(
-            st->W, ldw, k0, kb, s0, np, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB,
-            st->Apack[bk & 1], st->Bpack, st->use_tc, nL, kp);
+        ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m * (2 + nupd), 8.0 * NB * (double)m * (4 + nupd), &ev);
+        panels_kernel<float2><<<(unsigned)(2 * pa.nL), 256, kSmemPanel, stream>>>(
+            st->W, ldw, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB, pa);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(stream, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     };
-    auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B,
+    auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B, int K,
                     int max_ctas) -> int {
         const int64_t m = np - s0;
         float* C = reinterpret_cast<float*>(st->W + s0 + c0 * ldw);
         cudaEvent_t ev;
-        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * K3,
-                        4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K3), &ev);
-        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K3, max_ctas));
+        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * K,
+                        4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K), &ev);
+        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K, max_ctas));
         ctx->prof.end(stream, ev);
         return SIEB200_OK;
     };
+    const int gemm_ctas = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
 
     // Right-looking block LU with a lookahead of one block. Step bk: the
     // panels of block bk are formed on the context stream; the next
-    // diagonal block takes its update from them and is factored on the side
-    // stream while the tensor-core trailing update (all columns but the
-    // next block's) runs here; then the next panels, whose L21 part applies
-    // step bk's update to the next block's remaining rows. The persistent
-    // GEMM leaves one SM to the diagonal kernel (whose shared memory keeps it
-    // off the GEMM's SMs).
-    SIEB_RETURN_IF(diag_blk(0, -1, stream));
-    SIEB_RETURN_IF(panels(0, -1));
+    // diagonal block takes its update(s) from them and is factored on the
+    // side stream while the tensor-core trailing update runs here; then the
+    // next panels, which apply the pending updates to the next block's
+    // column (and, in the pair schedule after an even step, to its row).
+    // The trailing update skips the next block column; in the pair schedule
+    // it runs after odd steps only, for both steps of the pair at once
+    // (half the C traffic per flop). The persistent GEMM leaves one SM to the
+    // diagonal kernel (whose shared memory keeps it off the GEMM's SMs).
+    SIEB_RETURN_IF(diag_blk(0, -1, -1, stream));
+    SIEB_RETURN_IF(panels(0, -1, -1, -1));
     for (int64_t bk = 0; bk < nbl; ++bk) {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
@@ -1261,22 +1343,30 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         const int64_t m = np - s0;
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
+            const bool odd = pair && (bk & 1);
+            const int64_t kprev = odd ? k0 - NB : -1;      // the first step of the pair
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
-            SIEB_RETURN_IF(diag_blk(bk + 1, k0, st->side));
+            SIEB_RETURN_IF(diag_blk(bk + 1, k0, kprev, st->side));
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
-            if (m > n1)
-                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * K3,
-                                    s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1));
+            if (!pair) {
+                if (m > n1)
+                    SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * K3, (int)K3,
+                                        gemm_ctas));
+            } else if (odd && m > n1) {
+                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas));
+            }
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
-            SIEB_RETURN_IF(panels(bk + 1, k0));
+            // after an even step of the pair schedule the next block row
+            // has not had this step's update yet
+            SIEB_RETURN_IF(panels(bk + 1, k0, kprev, pair && !odd ? k0 : -1));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
-            SIEB_RETURN_IF(diag_blk(bk + 1, -1, stream));
-            SIEB_RETURN_IF(panels(bk + 1, -1));
+            SIEB_RETURN_IF(diag_blk(bk + 1, -1, -1, stream));
+            SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1));
         }
     }
     ctx->prof.end(stream, ev_fact);
@@ -1688,7 +1778,8 @@ static int fp64_factorize(DenseSolver* s) {
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, (16.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0), 0.0, &ev);
         diag_lu_kernel<double2><<<1, kDiagThreads, kSmemDiagUpd64, sm>>>(
-            st->W64, ldw, k0, kb, st->Linv64 + (size_t)bk * NB * NB, st->Uinv64 + (size_t)bk * NB * NB, st->err, kp);
+            st->W64, ldw, k0, kb, st->Linv64 + (size_t)bk * NB * NB, st->Uinv64 + (size_t)bk * NB * NB, st->err, kp,
+            -1);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
@@ -1703,9 +1794,11 @@ static int fp64_factorize(DenseSolver* s) {
         const int nL = (int)blocks_for(m, 32);
         cudaEvent_t ev;
         ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m * (kp >= 0 ? 2.0 : 1.0), 0.0, &ev);
+        PanelArgs pa;
+        pa.k0 = k0; pa.kb = kb; pa.s0 = s0; pa.np = np; pa.nL = nL; pa.pack = 0;
+        pa.kp[0] = kp;
         panels_kernel<double2><<<(unsigned)(2 * nL), 256, kSmemPanel64, stream>>>(
-            st->W64, ldw, k0, kb, s0, np, st->Uinv64 + (size_t)bk * NB * NB, st->Linv64 + (size_t)bk * NB * NB,
-            nullptr, nullptr, 0, nL, kp);
+            st->W64, ldw, st->Uinv64 + (size_t)bk * NB * NB, st->Linv64 + (size_t)bk * NB * NB, pa);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(stream, ev);
         SIEB_TRY_CUDA(cudaGetLastError());

@@ -54,11 +54,13 @@ def _pmchwt(level=2, solver="lu_cusolver", rule=5):
     return m, o
 
 
-@pytest.mark.parametrize("trailing", ["tc", "tc_load_store", "tc_reduce", "simt"])
+@pytest.mark.parametrize("trailing", ["tc", "tc_single_step", "tc_load_store", "tc_reduce", "simt"])
 def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
     import sieb200
     if trailing == "simt":
         monkeypatch.setenv("SIEB200_TRAILING_SIMT", "1")
+    if trailing == "tc_single_step":
+        monkeypatch.setenv("SIEB200_PAIR_UPDATE", "0")
     if trailing in ("tc_load_store", "tc_reduce"):
         monkeypatch.setenv("SIEB200_GEMM_MODE", "2" if trailing == "tc_load_store" else "3")
     m, o = _pmchwt(2)
