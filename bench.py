@@ -1052,6 +1052,7 @@ def run_case(args):
       factorization  mixed factorization of that system (N = 6000), twice
       multi_rhs      mixed solve of 64 plane-wave right-hand sides of it
       fp64_lu        own FP64 LU factorization and solve of it
+      residual       four FP64 residual matvecs b - Z x of that system (576 MB each)
     """
     import torch
     import sieb200
@@ -1082,6 +1083,15 @@ def run_case(args):
         out["iterations"] = s.solve(B.data_ptr(), nrhs=len(srcs), tolerance=1e-10, max_iterations=60)
         ctx.synchronize()
         s.close()
+    elif args.case == "residual":
+        g = torch.Generator(device="cuda").manual_seed(5)
+        x = torch.randn(N, dtype=torch.complex128, device="cuda", generator=g)
+        y = torch.randn(N, dtype=torch.complex128, device="cuda", generator=g)
+        torch.cuda.synchronize()
+        for _ in range(4):
+            sieb200.matvec(N, Z.data_ptr(), x.data_ptr(), y.data_ptr(), beta=-1.0, ctx=ctx)
+        ctx.synchronize()
+        out["y_norm"] = float(y.norm())
     elif not args.case.startswith("assembly"):
         raise SystemExit(f"unknown case {args.case}")
     del Z

@@ -212,12 +212,20 @@ __device__ __forceinline__ void accumulate(Moments<NK, TK>& M, const d3& pl, con
 // Regular (or extracted-kernel) double quadrature of all face pairs (m, n)
 // with m in [m0, m1). Output blocks: NB = NK (TL only) or 2*NK (TL then TK),
 // each 3x3 complex, per pair at pairs[((m-m0)*nf + n) * NB*9].
-template <int NK, bool TK>
-__global__ void __launch_bounds__(kWarps * 32, 1)
+// SPLIT: blockIdx.y picks one of the NK wavenumbers and the CTA accumulates
+// that one only. The geometry of a point pair (R, 1/R, p.q, p x q) is then
+// formed once per wavenumber instead of once, but the moments of one
+// wavenumber (18 complex) fit in half the registers, so two CTAs share an SM
+// and the FP64 pipe sees twice the warps; each wavenumber's sums run in the
+// same order as without the split.
+template <int NK, bool TK, bool SPLIT = false>
+__global__ void __launch_bounds__(kWarps * 32, SPLIT ? 2 : 1)
 pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
                     const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
                     float thr, cplx* __restrict__ pairs) {
     constexpr int NB = TK ? 2 * NK : NK;
+    constexpr int NKC = SPLIT ? 1 : NK;  // wavenumbers accumulated by this CTA
+    const int a_base = SPLIT ? (int)blockIdx.y : 0;
     __shared__ d3 s_tp[kMaxQ], s_tl[kMaxQ];
     __shared__ double s_w[kMaxQ];
     __shared__ d3 s_sp[kWarps][kMaxQ], s_sl[kWarps][kMaxQ];
@@ -233,7 +241,10 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
         s_w[t] = (double)qw_g[t];
     }
     __syncthreads();
-    const double kk[2] = {k0, k1};
+    const double kall[2] = {k0, k1};
+    double kk[NKC];
+#pragma unroll
+    for (int a = 0; a < NKC; ++a) kk[a] = kall[a_base + a];
     const int QQ = Q * Q;
 
     for (int n = warp; n < nf; n += kWarps) {
@@ -249,9 +260,9 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
         const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] &&
                            gm.idx[2] == gn.idx[2];
 
-        Moments<NK, TK> M;
+        Moments<NKC, TK> M;
 #pragma unroll
-        for (int a = 0; a < NK; ++a) {
+        for (int a = 0; a < NKC; ++a) {
             M.S0[a] = cx(0, 0); M.Spq[a] = cx(0, 0);
 #pragma unroll
             for (int c = 0; c < 3; ++c) { M.Sp[a][c] = cx(0, 0); M.Sq[a][c] = cx(0, 0); }
@@ -278,23 +289,23 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
                 const double inv_R = 1.0 / R;
                 const double i4pR = 1.0 / (4.0 * kPi * R);
 #pragma unroll
-                for (int a = 0; a < NK; ++a) {
+                for (int a = 0; a < NKC; ++a) {
                     cplx G, g;
                     green_std(R, inv_R, i4pR, kk[a], G, g);
-                    accumulate<NK, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
+                    accumulate<NKC, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
                 }
             } else {
 #pragma unroll
-                for (int a = 0; a < NK; ++a) {
+                for (int a = 0; a < NKC; ++a) {
                     cplx G, g;
                     green_reg(R, kk[a], G, g);
-                    accumulate<NK, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
+                    accumulate<NKC, TK>(M, pl, ql, pq, pxq, ww, a, G, g);
                 }
             }
         }
         // Butterfly: every lane ends with the totals.
 #pragma unroll
-        for (int a = 0; a < NK; ++a) {
+        for (int a = 0; a < NKC; ++a) {
             warp_sum(M.S0[a]); warp_sum(M.Spq[a]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) { warp_sum(M.Sp[a][c]); warp_sum(M.Sq[a][c]); }
@@ -314,14 +325,14 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
             const double AB = dot3(A, B);
             cplx* out = pairs + ((size_t)blockIdx.x * nf + n) * (NB * 9);
 #pragma unroll
-            for (int a = 0; a < NK; ++a) {
+            for (int a = 0; a < NKC; ++a) {
                 // TL_ji = l_j l_i [ 1/4 (Spq - Sp.B - A.Sq + (A.B) S0) - S0 / k^2 ]
                 cplx t = M.Spq[a];
                 t = t - (M.Sp[a][0] * B.x + M.Sp[a][1] * B.y + M.Sp[a][2] * B.z);
                 t = t - (M.Sq[a][0] * A.x + M.Sq[a][1] * A.y + M.Sq[a][2] * A.z);
                 t += M.S0[a] * AB;
                 const cplx tl = (t * 0.25 - M.S0[a] * (1.0 / (kk[a] * kk[a]))) * scale;
-                out[a * 9 + lane] = tl;
+                out[(a_base + a) * 9 + lane] = tl;
                 if (TK) {
                     cplx tk = cx(0, 0);
                     if (!coinc) {
@@ -335,7 +346,7 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
                         u += M.T0[a] * axbd;
                         tk = u * (0.25 * scale);
                     }
-                    out[(NK + a) * 9 + lane] = tk;
+                    out[(NK + a_base + a) * 9 + lane] = tk;
                 }
             }
         }
@@ -1470,6 +1481,10 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
     gp.eps_f = ap.eps_f; gp.mu_f = ap.mu_f;
     gp.gram = dgram;
 
+    // Two-wavenumber regular pass as one CTA per (face, wavenumber), two CTAs
+    // per SM; SIEB200_ASM_SPLIT=0 keeps one CTA per face over both.
+    const char* split_env = getenv("SIEB200_ASM_SPLIT");
+    const bool split_wavenumbers = !(split_env && split_env[0] == '0');
     for (int m0 = 0; m0 < nf; m0 += slab) {
         const int m1 = std::min(nf, m0 + slab);
         const int rows = m1 - m0;
@@ -1491,6 +1506,9 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
         else if (opt.formulation == SIEB200_PEC_EFIE)
             pair_regular_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, pairs);
+        else if (split_wavenumbers)
+            pair_regular_kernel<2, true, true><<<dim3(rows, 2), kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
         else
             pair_regular_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);

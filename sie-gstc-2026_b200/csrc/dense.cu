@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "dense.cuh"
+#include "sm100.cuh"
 
 namespace sieb200 {
 
@@ -94,6 +95,120 @@ __global__ void gemv_h_kernel(int64_t n, const TA* __restrict__ A, int64_t lda, 
     }
 }
 
+// y = A x, TMA-staged. Each CTA owns GV_ROWS rows and one column chunk; a
+// producer warp streams 16 KB tiles (GV_ROWS rows x the chunk's next CB
+// columns, one cp.async.bulk.tensor per tile) through a GV_STAGES-deep ring
+// in shared memory, and each of the GV_ROWS consumer threads accumulates its
+// row from the tiles in FP64, in the same column order as
+// gemv_partial_kernel. The tensor map views A as reals: inner extent 2n
+// (re, im of n rows), outer extent n columns, row stride lda elements.
+// Every wait is bounded: past timeout_ns the CTA stops streaming and writes
+// NaN partial sums, so the caller's residual shows the failure.
+constexpr int GV_ROWS = 128;
+constexpr int GV_STAGES = 6;
+constexpr int GV_TILE_BYTES = 16384;
+constexpr int GV_THREADS = GV_ROWS + 32;
+constexpr int GV_SMEM = GV_STAGES * GV_TILE_BYTES + 1024;
+
+__device__ __forceinline__ bool gv_wait(uint32_t bar, uint32_t parity, uint64_t deadline) {
+    int it = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if ((++it & 255) == 0 && global_ns() > deadline) return false;
+    }
+    return true;
+}
+
+template <class TA>
+__global__ void __launch_bounds__(GV_THREADS, 2)
+gemv_tma_kernel(const __grid_constant__ CUtensorMap tmA, int64_t n, const cplx* __restrict__ x,
+                int64_t cols_per_chunk, cplx* __restrict__ partial, unsigned long long timeout_ns) {
+    constexpr int CB = GV_TILE_BYTES / (GV_ROWS * (int)sizeof(TA));  // columns per tile
+    extern __shared__ __align__(16) unsigned char gv_smem[];
+    const uint32_t raw = smem_u32(gv_smem);
+    unsigned char* base = gv_smem + (((raw + 1023u) & ~1023u) - raw);
+    const uint32_t ring = smem_u32(base);
+    __shared__ __align__(8) uint64_t bars[2 * GV_STAGES];
+    __shared__ volatile int s_abort;
+    const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[GV_STAGES]);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t i0 = (int64_t)blockIdx.x * GV_ROWS;
+    const int64_t c0 = (int64_t)blockIdx.y * cols_per_chunk;
+    const int64_t c1 = min(n, c0 + cols_per_chunk);
+    const int ntile = (int)((c1 - c0 + CB - 1) / CB);
+    if (tid == 0) {
+        s_abort = 0;
+        for (int st = 0; st < GV_STAGES; ++st) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, GV_ROWS / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    const uint64_t deadline = global_ns() + timeout_ns;
+
+    if (warp == GV_ROWS / 32) {  // producer
+        if (lane == 0) {
+            for (int i = 0; i < ntile; ++i) {
+                const int st = i % GV_STAGES;
+                const uint32_t ph = (uint32_t)(i / GV_STAGES) & 1u;
+                if (!gv_wait(empty0 + 8 * st, ph ^ 1u, deadline)) {
+                    s_abort = 1;
+                    break;
+                }
+                mbar_expect_tx(full0 + 8 * st, GV_TILE_BYTES);
+                tma_load_2d(ring + st * GV_TILE_BYTES, &tmA, full0 + 8 * st, (int)(2 * i0), (int)(c0 + (int64_t)i * CB));
+            }
+        }
+        return;
+    }
+
+    double re = 0.0, im = 0.0;
+    bool ok = true;
+    for (int i = 0; i < ntile; ++i) {
+        const int st = i % GV_STAGES;
+        const uint32_t ph = (uint32_t)(i / GV_STAGES) & 1u;
+        if (s_abort || !gv_wait(full0 + 8 * st, ph, deadline)) {
+            ok = false;
+            break;
+        }
+        const TA* tile = reinterpret_cast<const TA*>(base + st * GV_TILE_BYTES);
+        const int64_t cb = c0 + (int64_t)i * CB;
+        const int ncol = (int)min((int64_t)CB, c1 - cb);
+#pragma unroll 4
+        for (int j = 0; j < ncol; ++j) {
+            const TA a = tile[j * GV_ROWS + tid];
+            const cplx xv = x[cb + j];
+            const double ar = (double)a.x, ai = (double)a.y;
+            re += ar * xv.re - ai * xv.im;
+            im += ar * xv.im + ai * xv.re;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * st);
+    }
+    if (i0 + tid < n) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        partial[(int64_t)blockIdx.y * n + i0 + tid] = ok ? cx(re, im) : cx(nan, nan);
+    }
+}
+
+template <class TA>
+int gemv_tma_launch(sieb200_ctx* ctx, const CUtensorMap* tm, int64_t n, const cplx* x, int64_t cpc, int chunks,
+                    cplx* partial) {
+    static bool attr_set[64] = {};  // per device
+    const int dev = ctx->device & 63;
+    if (!attr_set[dev]) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(gemv_tma_kernel<TA>, cudaFuncAttributeMaxDynamicSharedMemorySize, GV_SMEM));
+        attr_set[dev] = true;
+    }
+    const dim3 grid((unsigned)((n + GV_ROWS - 1) / GV_ROWS), (unsigned)chunks);
+    gemv_tma_kernel<TA><<<grid, GV_THREADS, GV_SMEM, ctx->stream>>>(*tm, n, x, cpc, partial, 2000000000ull);
+    SIEB_NOTE_LAUNCH();
+    SIEB_TRY_CUDA(cudaGetLastError());
+    return SIEB200_OK;
+}
+
 }  // namespace
 
 int gemv_h_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, const cplx* x, double beta,
@@ -114,27 +229,68 @@ int gemv_h_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, const
 int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec, const cplx* x,
                 double beta, cplx* y, DeviceBuffer& scratch) {
     const int threads = 256;
-    const int64_t row_blocks = (n + threads - 1) / threads;
-    // Aim for ~4 CTAs per SM.
-    int64_t chunks = std::max<int64_t>(1, (int64_t)ctx->sm_count * 4 / std::max<int64_t>(1, row_blocks));
-    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / 64));
-    const int64_t cpc = (n + chunks - 1) / chunks;
-    chunks = (n + cpc - 1) / cpc;
+    // The TMA-staged kernel needs a 16-byte aligned A whose column stride is a
+    // multiple of 16 bytes; other operands (and SIEB200_GEMV_TMA=0) take the
+    // per-thread-load kernel.
+    const size_t esz = prec == 0 ? 16 : 8;
+    const char* tma_env = getenv("SIEB200_GEMV_TMA");
+    bool tma_ok = !(tma_env && tma_env[0] == '0') && n >= 2 * GV_ROWS && n <= (int64_t)1 << 30 &&
+                  (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((size_t)lda * esz) % 16 == 0;
+    CUtensorMap tm;
+    int64_t row_blocks, chunks, cpc;
+    if (tma_ok) {
+        SIEB_RETURN_IF(encode_tensor_map_2d(&tm, prec == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                            A, (uint64_t)(2 * n), (uint64_t)n, (uint64_t)lda * esz, 2 * GV_ROWS,
+                                            (uint32_t)(GV_TILE_BYTES / (GV_ROWS * esz)), CU_TENSOR_MAP_SWIZZLE_NONE));
+        // Two CTAs per SM. The column chunk count maximises the filled share of
+        // the CTA waves times the streaming share of a CTA (a CTA pays about
+        // two tiles' time to fill its ring), with chunks of whole tiles, at
+        // least four tiles each; the smaller count wins within 1 %.
+        const int64_t cb = GV_TILE_BYTES / (GV_ROWS * (int64_t)esz);
+        const int64_t slots = 2 * (int64_t)std::max(1, ctx->sm_count);
+        row_blocks = (n + GV_ROWS - 1) / GV_ROWS;
+        const int64_t max_chunks = std::max<int64_t>(1, std::min<int64_t>(32, n / (4 * cb)));
+        double best = -1.0;
+        chunks = 1;
+        for (int64_t c = 1; c <= max_chunks; ++c) {
+            const int64_t t = row_blocks * c;
+            const double tiles = (double)((n + c - 1) / c) / (double)cb;
+            const double fill = (double)t / (double)(((t + slots - 1) / slots) * slots) * tiles / (tiles + 2.0);
+            if (fill > best + 0.01) {
+                best = fill;
+                chunks = c;
+            }
+        }
+        cpc = ((n + chunks - 1) / chunks + cb - 1) / cb * cb;
+        chunks = (n + cpc - 1) / cpc;
+    } else {
+        row_blocks = (n + threads - 1) / threads;
+        // Aim for ~4 CTAs per SM.
+        chunks = std::max<int64_t>(1, (int64_t)ctx->sm_count * 4 / std::max<int64_t>(1, row_blocks));
+        chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / 64));
+        cpc = (n + chunks - 1) / chunks;
+        chunks = (n + cpc - 1) / cpc;
+    }
     SIEB_RETURN_IF(scratch.reserve(sizeof(cplx) * n * chunks));
     const dim3 grid((unsigned)row_blocks, (unsigned)chunks);
     cudaEvent_t ev;
     ctx->prof.begin(ctx->stream, 2, 8.0 * (double)n * (double)n,
                     (prec == 0 ? 16.0 : 8.0) * (double)n * (double)n + 16.0 * 3.0 * n, &ev);
-    if (prec == 0)
-        gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(
-            n, static_cast<const double2*>(A), lda, x, cpc, scratch.as<cplx>());
-    else
-        gemv_partial_kernel<float2><<<grid, threads, 0, ctx->stream>>>(
-            n, static_cast<const float2*>(A), lda, x, cpc, scratch.as<cplx>());
-    SIEB_NOTE_LAUNCH();
-    SIEB_TRY_CUDA(cudaGetLastError());
-    gemv_finish_kernel<<<(unsigned)row_blocks, threads, 0, ctx->stream>>>(n, (int)chunks,
-                                                                          scratch.as<cplx>(), beta, y);
+    if (tma_ok) {
+        SIEB_RETURN_IF(prec == 0 ? gemv_tma_launch<double2>(ctx, &tm, n, x, cpc, (int)chunks, scratch.as<cplx>())
+                                 : gemv_tma_launch<float2>(ctx, &tm, n, x, cpc, (int)chunks, scratch.as<cplx>()));
+    } else {
+        if (prec == 0)
+            gemv_partial_kernel<double2><<<grid, threads, 0, ctx->stream>>>(
+                n, static_cast<const double2*>(A), lda, x, cpc, scratch.as<cplx>());
+        else
+            gemv_partial_kernel<float2><<<grid, threads, 0, ctx->stream>>>(
+                n, static_cast<const float2*>(A), lda, x, cpc, scratch.as<cplx>());
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+    }
+    gemv_finish_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, ctx->stream>>>(
+        n, (int)chunks, scratch.as<cplx>(), beta, y);
     SIEB_NOTE_LAUNCH();
     ctx->prof.end(ctx->stream, ev);
     SIEB_TRY_CUDA(cudaGetLastError());

@@ -217,15 +217,34 @@ constexpr int kDiagWarps = kDiagThreads / 32;
 constexpr int kDiagCols = NB / kDiagWarps;
 static_assert(kDiagCols % 2 == 0 && 32 % kDiagCols == 0, "diag column split");
 
+// Bounded wait for step j's coefficient column (error word 2 past the bound).
+__device__ __forceinline__ void diag_wait(uint32_t bar, uint64_t deadline, unsigned* err) {
+    int it = 0;
+    while (!mbar_try_wait(bar, 0)) {
+        if ((++it & 255) == 0 && global_ns() > deadline) {
+            atomicCAS(err, 0u, 2u);
+            return;
+        }
+    }
+}
+
 // Steps j = kDiagCols bp + u, u = 0 .. kDiagCols-1, all in row half H.
+// Dataflow instead of block barriers: the owning warp writes c_j into
+// column j of cols (every step keeps its own column, so nothing is
+// overwritten) and releases step j's mbarrier; every other warp acquires
+// that mbarrier when it reaches step j. The owner only waits for the steps
+// before j, so a warp runs ahead of the warps that are still applying
+// earlier columns, and the chain per step is the owner's pivot, reciprocal,
+// scaling and the update of its own next column.
 template <class T, int H>
 __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, int lane,
-                                           T (*cbuf)[NB], T* rcps, unsigned* err) {
+                                           T (*cols)[NB], T* rcps, uint32_t bar0, uint64_t deadline,
+                                           unsigned* err) {
     using R = typename RealOf<T>::type;
     constexpr int CW = kDiagCols;
 #pragma unroll
     for (int u = 0; u < CW; ++u) {
-        const int j = CW * bp + u, jl = j & 31, buf = u & 1;
+        const int j = CW * bp + u, jl = j & 31;
         const bool g0 = lane > j, g1 = lane + 32 > j;  // rows below the pivot
         const T z = cmk<T>(0.f, 0.f);
         T ca0, ca1;
@@ -242,9 +261,14 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
                 if (H) ca1 = z;
                 else ca0 = z;
             }
-            cbuf[buf][lane] = ca0;
-            cbuf[buf][lane + 32] = ca1;
+            cols[j][lane] = ca0;
+            cols[j][lane + 32] = ca1;
             if (lane == 0) rcps[j] = rcp;
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                mbar_arrive(bar0 + 8 * j);
+            }
             a[u][0] = g0 ? cnegf(ca0) : a[u][0];
             a[u][1] = g1 ? cnegf(ca1) : a[u][1];
             const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
@@ -260,11 +284,10 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
                     a[v][1] = cfmsf(a[v][1], ca1, x);
                 }
             }
-        }
-        __syncthreads();
-        if (w != bp) {
-            ca0 = cbuf[buf][lane];
-            ca1 = cbuf[buf][lane + 32];
+        } else {
+            diag_wait(bar0 + 8 * j, deadline, err);
+            ca0 = cols[j][lane];
+            ca1 = cols[j][lane + 32];
             if (w < bp) {  // columns left of the pivot: rows below j only
                 const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
 #pragma unroll
@@ -297,9 +320,15 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
                                                                int64_t kp2) {
     constexpr int CW = kDiagCols;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    __shared__ T cbuf[2][NB];  // c_j, double-buffered across the step barrier
-    __shared__ T rcps[NB];     // 1 / p_j
+    __shared__ T rcps[NB];                      // 1 / p_j
+    __shared__ __align__(8) uint64_t bars[NB];  // step j's column published
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t bar0 = smem_u32(&bars[0]);
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < NB; ++j) mbar_init(bar0 + 8 * j, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const uint64_t deadline = global_ns() + 1000000000ull;
     T a[CW][2];
 #pragma unroll
     for (int v = 0; v < CW; ++v)
@@ -330,10 +359,15 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
             }
         }
     }
+    // The coefficient columns reuse the update's staging area (NB x NB <=
+    // kSmemDiagUpd); the barrier also publishes the mbarrier initialisation.
+    __syncthreads();
+    T(*cols)[NB] = reinterpret_cast<T(*)[NB]>(dyn_smem);
 #pragma unroll 1
-    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cbuf, rcps, err);
+    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cols, rcps, bar0, deadline, err);
 #pragma unroll 1
-    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<T, 1>(a, bp, w, lane, cbuf, rcps, err);
+    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp)
+        diag_steps<T, 1>(a, bp, w, lane, cols, rcps, bar0, deadline, err);
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < CW; ++v) {
@@ -1112,7 +1146,7 @@ static int check_err(DenseSolver* s, const char* what) {
         return SIEB200_SINGULAR;
     }
     if (e == 2u) {
-        set_error(std::string(what) + ": a triangular-solve block waited past its bound");
+        set_error(std::string(what) + ": a diagonal-block or triangular-solve kernel waited past its bound");
         return SIEB200_TIMEOUT;
     }
     if (e != 0u) {
@@ -1833,6 +1867,10 @@ static int fp64_factorize(DenseSolver* s) {
     unsigned e = 0;
     SIEB_TRY_CUDA(cudaMemcpyAsync(&e, st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (e == 2u) {
+        set_error("own FP64 LU: a diagonal-block kernel waited past its bound");
+        return SIEB200_TIMEOUT;
+    }
     if (e != 0u) {
         set_error("own FP64 LU: zero or non-finite pivot in a diagonal block (the matrix is singular or the "
                   "butterfly transform met an unlucky pivot)");

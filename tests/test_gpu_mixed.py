@@ -207,13 +207,16 @@ def test_mixed_adjoint_matches_cusolver_on_pmchwt(gpu_ctx):
     mix.close()
 
 
-def test_profile_timeline_orders_the_block_steps(gpu_ctx):
+@pytest.mark.parametrize("pair", ["0", "1"])
+def test_profile_timeline_orders_the_block_steps(pair, gpu_ctx, monkeypatch):
     """The profiler's timeline: one span per hot launch with start <= end,
     every chain kernel inside the factorization span, one diagonal-block
     kernel per block, one panels launch per block step and one tensor-core
-    trailing update per step but the last."""
+    trailing update per step but the last two (single-step schedule) or per
+    odd step among those (pair schedule)."""
     import torch
     import sieb200
+    monkeypatch.setenv("SIEB200_PAIR_UPDATE", pair)
     n = 1000
     rng = np.random.default_rng(7)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
@@ -234,8 +237,9 @@ def test_profile_timeline_orders_the_block_steps(gpu_ctx):
     nbl = -(-n // 64)
     assert sum(1 for sp in spans if sp[0] == 3) == nbl
     assert sum(1 for sp in spans if sp[0] == 4) == nbl - 1
-    # one trailing update per block step but the last (whose next block is the last one)
-    assert sum(1 for sp in spans if sp[0] == 0) == nbl - 2
+    # the last two steps have no columns right of the next block
+    expect = (nbl - 2) // 2 if pair == "1" else nbl - 2
+    assert sum(1 for sp in spans if sp[0] == 0) == expect
     diag = sorted(t0 for k, t0, _ in spans if k == 3)
     assert diag == [t0 for k, t0, _ in spans if k == 3]  # recorded in step order
 
