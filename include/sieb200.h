@@ -347,7 +347,11 @@ int sieb200_prepare_records(sieb200_ctx* ctx, int64_t faces, const double* maps,
  * CTA), mode 2: persistent tcgen05 kernel that loads, subtracts and stores
  * the C tile by TMA (modes 2 and 3 need C and ldc*4 16-byte aligned, else
  * mode 1 runs), mode 1: one-CTA-per-tile tcgen05 kernel, mode 0: SIMT kernel
- * on the same operands (checking path). */
+ * on the same operands (checking path). Modes 4 and 5 (the epilogues of
+ * modes 2 and 3) take split operands instead: A = [A_hi | A_lo] and
+ * B = [B_hi | B_lo] along k (k a multiple of 64, C and ldc*4 16-byte
+ * aligned), C -= A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T, each operand read
+ * once per tile. */
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode);
 

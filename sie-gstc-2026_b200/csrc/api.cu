@@ -1053,13 +1053,13 @@ int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double
 
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode) {
-    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 3, SIEB200_INVALID_ARG,
+    SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 5, SIEB200_INVALID_ARG,
                "invalid GEMM arguments");
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     GemmTC* g = nullptr;
     SIEB_RETURN_IF(gemm_tc_create(&g));
-    gemm_tc_set_mode(g, mode);
-    int st = gemm_tc_sub(g, ctx->stream, C, ldc, A, B, m2, n, k);
+    gemm_tc_set_mode(g, mode >= 4 ? mode - 2 : mode);
+    int st = gemm_tc_sub(g, ctx->stream, C, ldc, A, B, m2, n, k, 0, mode >= 4 ? 1 : 0);
     if (st == SIEB200_OK) st = gemm_tc_check(g, ctx->stream);
     gemm_tc_destroy(g);
     return st;

@@ -97,10 +97,10 @@ __global__ void gemv_h_kernel(int64_t n, const TA* __restrict__ A, int64_t lda, 
 
 // y = A x, TMA-staged. Each CTA owns GV_ROWS rows and one column chunk; a
 // producer warp streams 16 KB tiles (GV_ROWS rows x the chunk's next CB
-// columns, one cp.async.bulk.tensor per tile) through a GV_STAGES-deep ring
-// in shared memory, and each of the GV_ROWS consumer threads accumulates its
-// row from the tiles in FP64, in the same column order as
-// gemv_partial_kernel. The tensor map views A as reals: inner extent 2n
+// columns, one cp.async.bulk.tensor per tile) and the CB entries of x they
+// multiply (one cp.async.bulk) through a GV_STAGES-deep ring in shared
+// memory, and each of the GV_ROWS consumer threads accumulates its row from
+// the tiles in FP64, in the same column order as gemv_partial_kernel. The tensor map views A as reals: inner extent 2n
 // (re, im of n rows), outer extent n columns, row stride lda elements.
 // Every wait is bounded: past timeout_ns the CTA stops streaming and writes
 // NaN partial sums, so the caller's residual shows the failure.
@@ -108,7 +108,8 @@ constexpr int GV_ROWS = 128;
 constexpr int GV_STAGES = 6;
 constexpr int GV_TILE_BYTES = 16384;
 constexpr int GV_THREADS = GV_ROWS + 32;
-constexpr int GV_SMEM = GV_STAGES * GV_TILE_BYTES + 1024;
+constexpr int GV_XSLOT = 256;  // bytes of x per stage (16 complex128 at most)
+constexpr int GV_SMEM = GV_STAGES * (GV_TILE_BYTES + GV_XSLOT) + 1024;
 
 __device__ __forceinline__ bool gv_wait(uint32_t bar, uint32_t parity, uint64_t deadline) {
     int it = 0;
@@ -127,6 +128,8 @@ gemv_tma_kernel(const __grid_constant__ CUtensorMap tmA, int64_t n, const cplx* 
     const uint32_t raw = smem_u32(gv_smem);
     unsigned char* base = gv_smem + (((raw + 1023u) & ~1023u) - raw);
     const uint32_t ring = smem_u32(base);
+    const uint32_t xring = ring + GV_STAGES * GV_TILE_BYTES;
+    static_assert(CB * (int)sizeof(cplx) <= GV_XSLOT, "x slot");
     __shared__ __align__(8) uint64_t bars[2 * GV_STAGES];
     __shared__ volatile int s_abort;
     const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[GV_STAGES]);
@@ -157,8 +160,11 @@ gemv_tma_kernel(const __grid_constant__ CUtensorMap tmA, int64_t n, const cplx* 
                     s_abort = 1;
                     break;
                 }
-                mbar_expect_tx(full0 + 8 * st, GV_TILE_BYTES);
-                tma_load_2d(ring + st * GV_TILE_BYTES, &tmA, full0 + 8 * st, (int)(2 * i0), (int)(c0 + (int64_t)i * CB));
+                const int64_t cb = c0 + (int64_t)i * CB;
+                const uint32_t xbytes = (uint32_t)(min((int64_t)CB, c1 - cb) * (int64_t)sizeof(cplx));
+                mbar_expect_tx(full0 + 8 * st, GV_TILE_BYTES + xbytes);
+                tma_load_2d(ring + st * GV_TILE_BYTES, &tmA, full0 + 8 * st, (int)(2 * i0), (int)cb);
+                bulk_load_1d(xring + st * GV_XSLOT, x + cb, xbytes, full0 + 8 * st);
             }
         }
         return;
@@ -174,12 +180,13 @@ gemv_tma_kernel(const __grid_constant__ CUtensorMap tmA, int64_t n, const cplx* 
             break;
         }
         const TA* tile = reinterpret_cast<const TA*>(base + st * GV_TILE_BYTES);
+        const cplx* xs = reinterpret_cast<const cplx*>(base + GV_STAGES * GV_TILE_BYTES + st * GV_XSLOT);
         const int64_t cb = c0 + (int64_t)i * CB;
         const int ncol = (int)min((int64_t)CB, c1 - cb);
 #pragma unroll 4
         for (int j = 0; j < ncol; ++j) {
             const TA a = tile[j * GV_ROWS + tid];
-            const cplx xv = x[cb + j];
+            const cplx xv = xs[j];
             const double ar = (double)a.x, ai = (double)a.y;
             re += ar * xv.re - ai * xv.im;
             im += ar * xv.im + ai * xv.re;
@@ -235,7 +242,8 @@ int gemv_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int pre
     const size_t esz = prec == 0 ? 16 : 8;
     const char* tma_env = getenv("SIEB200_GEMV_TMA");
     bool tma_ok = !(tma_env && tma_env[0] == '0') && n >= 2 * GV_ROWS && n <= (int64_t)1 << 30 &&
-                  (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((size_t)lda * esz) % 16 == 0;
+                  (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((size_t)lda * esz) % 16 == 0 &&
+                  (reinterpret_cast<uintptr_t>(x) & 15) == 0;
     CUtensorMap tm;
     int64_t row_blocks, chunks, cpc;
     if (tma_ok) {

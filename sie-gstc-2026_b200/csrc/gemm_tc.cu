@@ -62,15 +62,19 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
 
 // Instruction descriptor: D f32 [4,6)=1, A tf32 [7,10)=2, B tf32 [10,13)=2,
 // both K-major, N>>3 at [17,23), M>>4 at [24,29).
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                            ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t idesc_tf32(int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+constexpr uint32_t kIdesc = idesc_tf32(BN);
+constexpr uint32_t kIdesc2 = idesc_tf32(2 * BN);  // N = 256: B_hi and B_lo in one MMA
 
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate,
+                                          uint32_t idesc = kIdesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -228,9 +232,20 @@ constexpr int P_STAGES = 4;
 constexpr int P_THREADS = 192;
 constexpr int C_TILE_BYTES = BM * BN * 4;
 constexpr int P_SMEM_BYTES = P_STAGES * (STAGE_A + STAGE_B) + C_TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+// Split-operand layout (HILO): two stages of [A_hi | A_lo] and [B_hi | B_lo]
+// k-blocks, the same shared memory as four single stages.
+constexpr int H_STAGES = 2;
+static_assert(H_STAGES * 2 * (STAGE_A + STAGE_B) == P_STAGES * (STAGE_A + STAGE_B), "HILO stage budget");
 
 __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// HILO = true: A = [A_hi | A_lo] and B = [B_hi | B_lo] along K (K/2 columns
+// each) and the tile takes A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T. A stage
+// holds one k-block of all four; B_hi and B_lo sit back to back as one
+// 256-row operand, so a single N = 256 MMA forms A_hi [B_hi; B_lo]^T into
+// 256 accumulator columns and an N = 128 MMA adds A_lo B_hi^T to the first
+// 128. Each operand crosses from L2 once per tile (two thirds of the bytes
+// of the three-product sweep); the epilogue sums the two halves.
 // REDUCE = true: the epilogue does not load C. It writes the negated
 // accumulator into the staging tile and adds it to C with a TMA reduction
 // (cp.reduce.async.bulk.tensor .add, performed at L2), so no CTA waits for a
@@ -238,33 +253,38 @@ __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;"
 // reduction has read it. C + (-acc) rounds exactly as C - acc, and each
 // element takes one reduction per launch, so results are unchanged and
 // deterministic.
-template <bool REDUCE>
+template <bool REDUCE, bool HILO>
 __global__ void __launch_bounds__(P_THREADS, 1)
 gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                                 const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, unsigned* err) {
+    constexpr int NS = HILO ? H_STAGES : P_STAGES;     // ring stages
+    constexpr int SA = HILO ? 2 * STAGE_A : STAGE_A;   // A bytes per stage
+    constexpr int SB = HILO ? 2 * STAGE_B : STAGE_B;   // B bytes per stage
+    constexpr int ACC = HILO ? 2 * BN : BN;            // accumulator columns per buffer
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     unsigned char* gbase = smem_raw + (base - raw);
     const uint32_t sA = base;
-    const uint32_t sB = base + P_STAGES * STAGE_A;
-    const uint32_t sC = base + P_STAGES * (STAGE_A + STAGE_B);
-    float* cs = reinterpret_cast<float*>(gbase + P_STAGES * (STAGE_A + STAGE_B));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + P_STAGES * (STAGE_A + STAGE_B) + C_TILE_BYTES);
+    const uint32_t sB = base + NS * SA;
+    const uint32_t sC = base + NS * (SA + SB);
+    float* cs = reinterpret_cast<float*>(gbase + NS * (SA + SB));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + NS * (SA + SB) + C_TILE_BYTES);
     const uint32_t full0 = smem_u32(&bars[0]);
-    const uint32_t empty0 = smem_u32(&bars[P_STAGES]);
-    const uint32_t accf0 = smem_u32(&bars[2 * P_STAGES]);      // accumulator b ready (MMA -> epilogue)
-    const uint32_t acce0 = smem_u32(&bars[2 * P_STAGES + 2]);  // accumulator b drained (epilogue -> MMA)
-    const uint32_t cfull = smem_u32(&bars[2 * P_STAGES + 4]);  // C tile in shared memory
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * P_STAGES + 5]);
+    const uint32_t empty0 = smem_u32(&bars[NS]);
+    const uint32_t accf0 = smem_u32(&bars[2 * NS]);      // accumulator b ready (MMA -> epilogue)
+    const uint32_t acce0 = smem_u32(&bars[2 * NS + 2]);  // accumulator b drained (epilogue -> MMA)
+    const uint32_t cfull = smem_u32(&bars[2 * NS + 4]);  // C tile in shared memory
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * NS + 5]);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (M2 + BM - 1) / BM, nt = (N + BN - 1) / BN;
     const int tiles = mt * nt;
-    const int kblocks = K / BK;
+    const int KR = HILO ? K / 2 : K;  // columns of one K sweep (the hi half)
+    const int kblocks = KR / BK;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < P_STAGES; ++s) {
+        for (int s = 0; s < NS; ++s) {
             mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
@@ -278,7 +298,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(2 * BN));
+                     "r"(2 * ACC));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -293,12 +313,16 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
             for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int m0 = (t % mt) * BM, n0 = (t / mt) * BN;
                 for (int kb = 0; kb < kblocks; ++kb, ++g) {
-                    const int s = g % P_STAGES;
-                    const uint32_t ph = (uint32_t)(g / P_STAGES) & 1u;
+                    const int s = g % NS;
+                    const uint32_t ph = (uint32_t)(g / NS) & 1u;
                     if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, err)) { ok = false; break; }
-                    mbar_expect_tx(full0 + 8 * s, STAGE_A + STAGE_B);
-                    tma_load_2d(sA + s * STAGE_A, &tmA, full0 + 8 * s, kb * BK, m0);
-                    tma_load_2d(sB + s * STAGE_B, &tmB, full0 + 8 * s, kb * BK, n0);
+                    mbar_expect_tx(full0 + 8 * s, SA + SB);
+                    tma_load_2d(sA + s * SA, &tmA, full0 + 8 * s, kb * BK, m0);
+                    tma_load_2d(sB + s * SB, &tmB, full0 + 8 * s, kb * BK, n0);
+                    if (HILO) {
+                        tma_load_2d(sA + s * SA + STAGE_A, &tmA, full0 + 8 * s, KR + kb * BK, m0);
+                        tma_load_2d(sB + s * SB + STAGE_B, &tmB, full0 + 8 * s, KR + kb * BK, n0);
+                    }
                 }
             }
         }
@@ -311,17 +335,26 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
                 const uint32_t u = (uint32_t)(li >> 1);
                 if (!mbar_wait(acce0 + 8 * b, (u & 1u) ^ 1u, err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                const uint32_t acc = tmem + (uint32_t)(b * ACC);
                 for (int kb = 0; kb < kblocks; ++kb, ++g) {
-                    const int s = g % P_STAGES;
-                    const uint32_t ph = (uint32_t)(g / P_STAGES) & 1u;
+                    const int s = g % NS;
+                    const uint32_t ph = (uint32_t)(g / NS) & 1u;
                     if (!mbar_wait(full0 + 8 * s, ph, err)) { ok = false; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint64_t ad = smem_desc_sw128(sA + s * STAGE_A);
-                    const uint64_t bd = smem_desc_sw128(sB + s * STAGE_B);
+                    const uint64_t ad = smem_desc_sw128(sA + s * SA);
+                    const uint64_t bd = smem_desc_sw128(sB + s * SB);
+                    if (HILO) {
+                        const uint64_t adl = smem_desc_sw128(sA + s * SA + STAGE_A);
 #pragma unroll
-                    for (int k = 0; k < BK / 8; ++k)
-                        umma_tf32(acc, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u);
+                        for (int k = 0; k < BK / 8; ++k) {
+                            umma_tf32(acc, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u, kIdesc2);
+                            umma_tf32(acc, adl + 2 * k, bd + 2 * k, 1u, kIdesc);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < BK / 8; ++k)
+                            umma_tf32(acc, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u);
+                    }
                     umma_commit(empty0 + 8 * s);
                 }
                 if (ok) umma_commit(accf0 + 8 * b);  // fires when the tile's MMAs have completed
@@ -350,7 +383,14 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
 #pragma unroll 1
                 for (int chunk = 0; chunk < BN / 32; ++chunk) {
                     float v[32];
-                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + chunk * 32), v);
+                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * ACC + chunk * 32);
+                    tmem_ld32(ta, v);
+                    if (HILO) {
+                        float w[32];
+                        tmem_ld32(ta + BN, w);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) v[j] += w[j];
+                    }
                     if (REDUCE) {
 #pragma unroll
                         for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] = -v[j];
@@ -390,30 +430,43 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 1) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ACC));
     }
 }
 
 // SIMT reference on the same packed operands (checking path).
+// hilo: A = [A_hi | A_lo], B = [B_hi | B_lo] along K; the sum is
+// a_hi (b_hi + b_lo) + a_lo b_hi per k of the first half.
 __global__ void gemm_simt_sub_kernel(const float* __restrict__ A, const float* __restrict__ B,
-                                     float* __restrict__ C, int64_t ldc, int M2, int N, int K) {
-    __shared__ float As[64][33], Bs[64][33];
+                                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, int hilo) {
+    __shared__ float As[64][33], Bs[64][33], Al[64][33], Bl[64][33];
     const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
     const int tr = threadIdx.x & 63, tc = threadIdx.x >> 6;  // 256 threads: 64 rows x 4 col groups
+    const int KR = hilo ? K / 2 : K;
     float acc[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) acc[j] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += 32) {
+    for (int k0 = 0; k0 < KR; k0 += 32) {
         for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {
             const int r = e / 32, k = e % 32;
             As[r][k] = (r0 + r < M2) ? A[(int64_t)(r0 + r) * K + k0 + k] : 0.f;
             Bs[r][k] = (c0 + r < N) ? B[(int64_t)(c0 + r) * K + k0 + k] : 0.f;
+            if (hilo) {
+                Al[r][k] = (r0 + r < M2) ? A[(int64_t)(r0 + r) * K + KR + k0 + k] : 0.f;
+                Bl[r][k] = (c0 + r < N) ? B[(int64_t)(c0 + r) * K + KR + k0 + k] : 0.f;
+            }
         }
         __syncthreads();
         for (int k = 0; k < 32; ++k) {
             const float a = As[tr][k];
+            if (hilo) {
+                const float al = Al[tr][k];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) acc[j] += a * Bs[tc * 16 + j][k];
+                for (int j = 0; j < 16; ++j) acc[j] += a * Bs[tc * 16 + j][k] + a * Bl[tc * 16 + j][k] + al * Bs[tc * 16 + j][k];
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[j] += a * Bs[tc * 16 + j][k];
+            }
         }
         __syncthreads();
     }
@@ -492,14 +545,16 @@ void gemm_tc_destroy(GemmTC* g) {
 void gemm_tc_set_mode(GemmTC* g, int mode) { g->mode = mode; }
 
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A, const float* B,
-                int64_t M2, int64_t N, int K, int max_ctas) {
+                int64_t M2, int64_t N, int K, int max_ctas, int layout) {
     SIEB_CHECK(K % BK == 0 && K > 0, SIEB200_INVALID_ARG, "GEMM K must be a positive multiple of 32");
+    SIEB_CHECK(layout == 0 || (layout == 1 && K % (2 * BK) == 0), SIEB200_INVALID_ARG,
+               "split-operand GEMM: K must be a positive multiple of 64");
     SIEB_CHECK(M2 > 0 && N > 0 && M2 < (1ll << 31) && N < (1ll << 31), SIEB200_INVALID_ARG, "GEMM size out of range");
     SIEB_CHECK(((uintptr_t)A % 16) == 0 && ((uintptr_t)B % 16) == 0, SIEB200_INVALID_ARG,
                "GEMM operands must be 16-byte aligned");
     if (g->mode == 0) {
         gemm_simt_sub_kernel<<<dim3((unsigned)((M2 + 63) / 64), (unsigned)((N + 63) / 64)), 256, 0, stream>>>(
-            A, B, C, ldc, (int)M2, (int)N, K);
+            A, B, C, ldc, (int)M2, (int)N, K, layout);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
@@ -509,11 +564,18 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
     SIEB_RETURN_IF(make_map(&mb, B, K, N, BN));
     // The persistent kernel moves C by TMA: its base and column stride must
     // be 16-byte aligned (otherwise the per-tile kernel below is used).
-    if (g->mode >= 2 && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
+    // The split-operand layout runs on the persistent kernel only.
+    SIEB_CHECK(layout == 0 || (((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0), SIEB200_INVALID_ARG,
+               "split-operand GEMM: C and its column stride must be 16-byte aligned");
+    if ((g->mode >= 2 || layout == 1) && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
         if (!g->attr_set_p) {
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false>,
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false, false>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true>,
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true, false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true, true>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
             g->attr_set_p = true;
         }
@@ -523,12 +585,19 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         const int64_t tiles = ((M2 + BM - 1) / BM) * ((N + BN - 1) / BN);
         const int cap = max_ctas > 0 ? std::min(max_ctas, g->sms) : g->sms;
         const unsigned grid = (unsigned)std::min<int64_t>(tiles, std::max(1, cap));
-        if (g->mode == 3)
-            gemm_tf32_sub_persistent_kernel<true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2,
-                                                                                          (int)N, K, g->err);
+        const bool red = g->mode == 3;
+        if (layout == 1 && red)
+            gemm_tf32_sub_persistent_kernel<true, true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
+                ma, mb, mc, (int)M2, (int)N, K, g->err);
+        else if (layout == 1)
+            gemm_tf32_sub_persistent_kernel<false, true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
+                ma, mb, mc, (int)M2, (int)N, K, g->err);
+        else if (red)
+            gemm_tf32_sub_persistent_kernel<true, false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
+                ma, mb, mc, (int)M2, (int)N, K, g->err);
         else
-            gemm_tf32_sub_persistent_kernel<false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, (int)M2,
-                                                                                           (int)N, K, g->err);
+            gemm_tf32_sub_persistent_kernel<false, false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
+                ma, mb, mc, (int)M2, (int)N, K, g->err);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;

@@ -17,8 +17,10 @@ void gemm_tc_destroy(GemmTC* g);
 // error word checked on the next synchronization (gemm_tc_check).
 // max_ctas > 0 caps the persistent kernel's grid, leaving the other SMs to
 // concurrent work on other streams.
+// layout 0: A and B are one K sweep; layout 1: [hi | lo] halves along K,
+// C -= A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T (persistent kernel).
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A,
-                const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0);
+                const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0, int layout = 0);
 int gemm_tc_check(GemmTC* g, cudaStream_t stream);
 // Selects the implementation: 3 = persistent tcgen05 kernel whose epilogue
 // adds -acc to C by TMA reduction, 2 = persistent kernel that loads,

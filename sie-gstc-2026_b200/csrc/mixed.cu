@@ -217,34 +217,15 @@ constexpr int kDiagWarps = kDiagThreads / 32;
 constexpr int kDiagCols = NB / kDiagWarps;
 static_assert(kDiagCols % 2 == 0 && 32 % kDiagCols == 0, "diag column split");
 
-// Bounded wait for step j's coefficient column (error word 2 past the bound).
-__device__ __forceinline__ void diag_wait(uint32_t bar, uint64_t deadline, unsigned* err) {
-    int it = 0;
-    while (!mbar_try_wait(bar, 0)) {
-        if ((++it & 255) == 0 && global_ns() > deadline) {
-            atomicCAS(err, 0u, 2u);
-            return;
-        }
-    }
-}
-
 // Steps j = kDiagCols bp + u, u = 0 .. kDiagCols-1, all in row half H.
-// Dataflow instead of block barriers: the owning warp writes c_j into
-// column j of cols (every step keeps its own column, so nothing is
-// overwritten) and releases step j's mbarrier; every other warp acquires
-// that mbarrier when it reaches step j. The owner only waits for the steps
-// before j, so a warp runs ahead of the warps that are still applying
-// earlier columns, and the chain per step is the owner's pivot, reciprocal,
-// scaling and the update of its own next column.
 template <class T, int H>
 __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, int lane,
-                                           T (*cols)[NB], T* rcps, uint32_t bar0, uint64_t deadline,
-                                           unsigned* err) {
+                                           T (*cbuf)[NB], T* rcps, unsigned* err) {
     using R = typename RealOf<T>::type;
     constexpr int CW = kDiagCols;
 #pragma unroll
     for (int u = 0; u < CW; ++u) {
-        const int j = CW * bp + u, jl = j & 31;
+        const int j = CW * bp + u, jl = j & 31, buf = u & 1;
         const bool g0 = lane > j, g1 = lane + 32 > j;  // rows below the pivot
         const T z = cmk<T>(0.f, 0.f);
         T ca0, ca1;
@@ -261,14 +242,9 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
                 if (H) ca1 = z;
                 else ca0 = z;
             }
-            cols[j][lane] = ca0;
-            cols[j][lane + 32] = ca1;
+            cbuf[buf][lane] = ca0;
+            cbuf[buf][lane + 32] = ca1;
             if (lane == 0) rcps[j] = rcp;
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence_block();
-                mbar_arrive(bar0 + 8 * j);
-            }
             a[u][0] = g0 ? cnegf(ca0) : a[u][0];
             a[u][1] = g1 ? cnegf(ca1) : a[u][1];
             const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
@@ -284,10 +260,11 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
                     a[v][1] = cfmsf(a[v][1], ca1, x);
                 }
             }
-        } else {
-            diag_wait(bar0 + 8 * j, deadline, err);
-            ca0 = cols[j][lane];
-            ca1 = cols[j][lane + 32];
+        }
+        __syncthreads();
+        if (w != bp) {
+            ca0 = cbuf[buf][lane];
+            ca1 = cbuf[buf][lane + 32];
             if (w < bp) {  // columns left of the pivot: rows below j only
                 const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
 #pragma unroll
@@ -320,15 +297,9 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
                                                                int64_t kp2) {
     constexpr int CW = kDiagCols;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    __shared__ T rcps[NB];                      // 1 / p_j
-    __shared__ __align__(8) uint64_t bars[NB];  // step j's column published
+    __shared__ T cbuf[2][NB];  // c_j, double-buffered across the step barrier
+    __shared__ T rcps[NB];     // 1 / p_j
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t bar0 = smem_u32(&bars[0]);
-    if (threadIdx.x == 0) {
-        for (int j = 0; j < NB; ++j) mbar_init(bar0 + 8 * j, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    const uint64_t deadline = global_ns() + 1000000000ull;
     T a[CW][2];
 #pragma unroll
     for (int v = 0; v < CW; ++v)
@@ -359,15 +330,10 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
             }
         }
     }
-    // The coefficient columns reuse the update's staging area (NB x NB <=
-    // kSmemDiagUpd); the barrier also publishes the mbarrier initialisation.
-    __syncthreads();
-    T(*cols)[NB] = reinterpret_cast<T(*)[NB]>(dyn_smem);
 #pragma unroll 1
-    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cols, rcps, bar0, deadline, err);
+    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cbuf, rcps, err);
 #pragma unroll 1
-    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp)
-        diag_steps<T, 1>(a, bp, w, lane, cols, rcps, bar0, deadline, err);
+    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<T, 1>(a, bp, w, lane, cbuf, rcps, err);
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < CW; ++v) {
@@ -393,7 +359,9 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
 //     columns take first (the trailing GEMM runs every second step, so these
 //     columns can lag one step behind);
 //   Apack (at its K offset), a_ld (row stride in floats), a_r0 (first row
-//     packed: pack row 2 (r - a_r0)); Bpack, b_ld, b_c0 likewise for columns.
+//     packed: pack row 2 (r - a_r0)); Bpack, b_ld, b_c0 likewise for columns;
+//   a_lo, b_lo: offset of the lo part from the hi part in the split layout
+//     [hi | lo] (0: the three-product layout [hi | hi | lo] / [hi | lo | hi]).
 struct PanelArgs {
     int64_t k0 = 0, s0 = 0, np = 0;
     int kb = 0, nL = 0, pack = 0;
@@ -403,6 +371,7 @@ struct PanelArgs {
     int64_t a_ld = 0, a_r0 = 0;
     float* Bpack = nullptr;
     int64_t b_ld = 0, b_c0 = 0;
+    int64_t a_lo = 0, b_lo = 0;
 };
 
 // L21 = A21 * inv(U11) for rows [s0, np) of the panel columns [k0, k0+kb);
@@ -508,8 +477,13 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
         float* row0 = pa.Apack + (2 * (gr - pa.a_r0)) * pa.a_ld;
         float* row1 = row0 + pa.a_ld;
-        row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
-        row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
+        if (pa.a_lo) {
+            row0[kk] = h0; row0[pa.a_lo + kk] = v0 - h0;
+            row1[kk] = h1; row1[pa.a_lo + kk] = v1 - h1;
+        } else {
+            row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
+            row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
+        }
     }
 }
 
@@ -603,8 +577,12 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
             float* col = pa.Bpack + (gc - pa.b_c0) * pa.b_ld;
             const float h0 = tf32_hi(v.x), h1 = tf32_hi(v.y);
             col[2 * r] = h0; col[2 * r + 1] = h1;
-            col[2 * NB + 2 * r] = v.x - h0; col[2 * NB + 2 * r + 1] = v.y - h1;
-            col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
+            if (pa.b_lo) {
+                col[pa.b_lo + 2 * r] = v.x - h0; col[pa.b_lo + 2 * r + 1] = v.y - h1;
+            } else {
+                col[2 * NB + 2 * r] = v.x - h0; col[2 * NB + 2 * r + 1] = v.y - h1;
+                col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
+            }
         }
     }
 }
@@ -1146,7 +1124,7 @@ static int check_err(DenseSolver* s, const char* what) {
         return SIEB200_SINGULAR;
     }
     if (e == 2u) {
-        set_error(std::string(what) + ": a diagonal-block or triangular-solve kernel waited past its bound");
+        set_error(std::string(what) + ": a triangular-solve block waited past its bound");
         return SIEB200_TIMEOUT;
     }
     if (e != 0u) {
@@ -1180,7 +1158,9 @@ int mixed_factorize(DenseSolver* s) {
     const char* env = getenv("SIEB200_TRAILING_SIMT");
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
     const char* pair_env = getenv("SIEB200_PAIR_UPDATE");
-    st->pair = (pair_env && pair_env[0] == '0') ? 0 : 1;
+    st->pair = (pair_env && pair_env[0] == '1') ? 1 : 0;
+    const char* hilo_env = getenv("SIEB200_GEMM_HILO");
+    st->hilo = (hilo_env && hilo_env[0] == '0') ? 0 : 1;
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -1224,7 +1204,7 @@ int mixed_factorize(DenseSolver* s) {
     MixedState::GraphKey key;
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
-    key.use_tc = st->use_tc + 2 * st->pair; key.sms = gemm_sms;
+    key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo; key.sms = gemm_sms;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -1312,8 +1292,14 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // to K half j & 1 of one buffer, rows from s0(q) and columns from
     // s0(q) + NB (q = j | 1); single-step schedule: one K = 384 pack per
     // step, rows from s0(j), all columns (the GEMM offsets them).
+    // Split layout (hilo): a step's pack is [hi | lo], 2 x 2NB = 256 wide,
+    // and the GEMM forms the three products from it; in the pair schedule
+    // the two steps' hi parts come first, then their lo parts.
     const bool pair = st->use_tc && st->pair;
-    const int64_t KP = pair ? 2 * K3 : K3;
+    const bool hilo = st->hilo != 0;
+    const int64_t KS = hilo ? 4 * NB : K3;  // pack width of one step
+    const int64_t KP = pair ? 2 * KS : KS;
+    const int layout = hilo ? 1 : 0;
     auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
@@ -1328,11 +1314,14 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         if (pair) {
             const int half = (int)(bk & 1);
             const int64_t q_s0 = half ? s0 : s0 + NB;  // s0 of the step whose GEMM uses this pack
-            pa.Apack = st->Apack[0] + half * K3; pa.a_ld = KP; pa.a_r0 = q_s0;
-            pa.Bpack = st->Bpack + half * K3; pa.b_ld = KP; pa.b_c0 = q_s0 + NB;
+            const int64_t off = half * (hilo ? 2 * NB : K3);
+            pa.Apack = st->Apack[0] + off; pa.a_ld = KP; pa.a_r0 = q_s0;
+            pa.Bpack = st->Bpack + off; pa.b_ld = KP; pa.b_c0 = q_s0 + NB;
+            pa.a_lo = pa.b_lo = hilo ? 4 * NB : 0;
         } else {
-            pa.Apack = st->Apack[bk & 1]; pa.a_ld = K3; pa.a_r0 = s0;
-            pa.Bpack = st->Bpack; pa.b_ld = K3; pa.b_c0 = s0;
+            pa.Apack = st->Apack[bk & 1]; pa.a_ld = KS; pa.a_r0 = s0;
+            pa.Bpack = st->Bpack; pa.b_ld = KS; pa.b_c0 = s0;
+            pa.a_lo = pa.b_lo = hilo ? 2 * NB : 0;
         }
         const int nupd = (kp1 >= 0) + (kp2 >= 0) + (kpu >= 0);
         cudaEvent_t ev;
@@ -1349,9 +1338,11 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         const int64_t m = np - s0;
         float* C = reinterpret_cast<float*>(st->W + s0 + c0 * ldw);
         cudaEvent_t ev;
-        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * K,
+        // tensor work: three products of K/3 (one sweep) or K/2 (split) columns
+        const double keff = hilo ? 1.5 * K : (double)K;
+        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * keff,
                         4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K), &ev);
-        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K, max_ctas));
+        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K, max_ctas, layout));
         ctx->prof.end(stream, ev);
         return SIEB200_OK;
     };
@@ -1367,6 +1358,11 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // it runs after odd steps only, for both steps of the pair at once
     // (half the C traffic per flop). The persistent GEMM leaves one SM to the
     // diagonal kernel (whose shared memory keeps it off the GEMM's SMs).
+    // The single-step schedule is the default (SIEB200_PAIR_UPDATE=1 selects
+    // the pair schedule): on the 6016-unknown system the pair schedule's
+    // GEMM runs at 360 TFLOP/s against 297, but the steps without a GEMM put
+    // the panels and the diagonal block back to back and the extra updates
+    // lengthen that chain, so the factorization takes longer overall.
     SIEB_RETURN_IF(diag_blk(0, -1, -1, stream));
     SIEB_RETURN_IF(panels(0, -1, -1, -1));
     for (int64_t bk = 0; bk < nbl; ++bk) {
@@ -1385,7 +1381,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
             if (!pair) {
                 if (m > n1)
-                    SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * K3, (int)K3,
+                    SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * KS, (int)KS,
                                         gemm_ctas));
             } else if (odd && m > n1) {
                 SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas));
@@ -1867,10 +1863,6 @@ static int fp64_factorize(DenseSolver* s) {
     unsigned e = 0;
     SIEB_TRY_CUDA(cudaMemcpyAsync(&e, st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
-    if (e == 2u) {
-        set_error("own FP64 LU: a diagonal-block kernel waited past its bound");
-        return SIEB200_TIMEOUT;
-    }
     if (e != 0u) {
         set_error("own FP64 LU: zero or non-finite pivot in a diagonal block (the matrix is singular or the "
                   "butterfly transform met an unlucky pivot)");

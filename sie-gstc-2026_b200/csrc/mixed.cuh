@@ -29,7 +29,8 @@ struct MixedState {
     unsigned* tri_flags = nullptr;   // per block progress flags (2 * nbl) + 2 tickets
     cplx* vecs = nullptr;       // FP64 work vectors
     int use_tc = 1;
-    int pair = 1;               // trailing update every second block step (K = 2 x 384)
+    int hilo = 1;               // split [hi | lo] packs, three products per GEMM k-block
+    int pair = 0;               // trailing update every second block step (K = 2 x 384)
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;

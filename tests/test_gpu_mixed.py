@@ -46,6 +46,36 @@ def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
     assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
 
 
+@pytest.mark.parametrize("mode", [4, 5])
+@pytest.mark.parametrize("m2,n,K", [(256, 128, 256), (300, 200, 256), (1000, 517, 512), (4096, 1500, 256)])
+def test_gemm_tf32_sub_split_operands(mode, m2, n, K, gpu_ctx):
+    """Split operands [hi | lo] along k (modes 4 and 5): C -= A_hi B_hi^T +
+    A_hi B_lo^T + A_lo B_hi^T with TF32 hi parts and FP32 remainders, against
+    the FP64 product of the unsplit FP32 operands. Tolerance 1e-5 (the
+    dropped lo*lo term and FP32 accumulation; a plain TF32 product of these
+    operands is off by ~1e-3)."""
+    import torch
+    from sieb200 import _lib
+    rng = np.random.default_rng(m2 + n + K)
+    KR = K // 2
+    A = rng.standard_normal((m2, KR)).astype(np.float32)
+    B = rng.standard_normal((n, KR)).astype(np.float32)
+    Ah, Bh = _tf32(A), _tf32(B)
+    Ap = np.concatenate([Ah, A - Ah], axis=1)
+    Bp = np.concatenate([Bh, B - Bh], axis=1)
+    ldc = m2 + 8
+    C = rng.standard_normal((n, ldc)).astype(np.float32)
+    dA, dB, dC = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (Ap, Bp, C))
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().sieb200_gemm_tf32_sub(gpu_ctx.handle, m2, n, K, dA.data_ptr(), dB.data_ptr(),
+                                                 dC.data_ptr(), ldc, mode))
+    out = dC.cpu().numpy()
+    ref = C.astype(np.float64).copy()
+    ref[:, :m2] -= (A.astype(np.float64) @ B.astype(np.float64).T).T
+    assert rel_err(out[:, :m2], ref[:, :m2]) < 1e-5
+    assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
+
+
 def _pmchwt(level=2, solver="lu_cusolver", rule=5):
     import sieb200
     m = sieb200.icosphere(0.5, level)
@@ -54,13 +84,16 @@ def _pmchwt(level=2, solver="lu_cusolver", rule=5):
     return m, o
 
 
-@pytest.mark.parametrize("trailing", ["tc", "tc_single_step", "tc_load_store", "tc_reduce", "simt"])
+@pytest.mark.parametrize("trailing", ["tc", "tc_pair", "tc_three_product", "tc_load_store", "tc_reduce",
+                                      "simt"])
 def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
     import sieb200
     if trailing == "simt":
         monkeypatch.setenv("SIEB200_TRAILING_SIMT", "1")
-    if trailing == "tc_single_step":
-        monkeypatch.setenv("SIEB200_PAIR_UPDATE", "0")
+    if trailing == "tc_pair":
+        monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1")
+    if trailing == "tc_three_product":
+        monkeypatch.setenv("SIEB200_GEMM_HILO", "0")
     if trailing in ("tc_load_store", "tc_reduce"):
         monkeypatch.setenv("SIEB200_GEMM_MODE", "2" if trailing == "tc_load_store" else "3")
     m, o = _pmchwt(2)
@@ -120,14 +153,19 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
     s.close()
 
 
+@pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
-def test_mixed_ragged_sizes_one_step(n, gpu_ctx):
+def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
-    sub-block, and fewer rows than one block. One preconditioned step must
-    already reach 1e-5 (the factors are single precision), and the full
-    refinement 1e-12: a wrong triangular solve fails the first bound."""
+    sub-block, and fewer rows than one block, under both trailing-update
+    schedules (pair / single step) and both pack layouts (split [hi | lo] /
+    three-product). One preconditioned step must already reach 1e-5 (the
+    factors are single precision), and the full refinement 1e-12: a wrong
+    triangular solve fails the first bound."""
     import torch
     import sieb200
+    monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1" if schedule.startswith("pair") else "0")
+    monkeypatch.setenv("SIEB200_GEMM_HILO", "1" if schedule.endswith("split") else "0")
     rng = np.random.default_rng(n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
