@@ -253,7 +253,7 @@ __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;"
 // reduction has read it. C + (-acc) rounds exactly as C - acc, and each
 // element takes one reduction per launch, so results are unchanged and
 // deterministic.
-template <bool REDUCE, bool HILO>
+template <bool REDUCE, bool HILO, int CH>
 __global__ void __launch_bounds__(P_THREADS, 1)
 gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                                 const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, unsigned* err) {
@@ -274,8 +274,10 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
     const uint32_t empty0 = smem_u32(&bars[NS]);
     const uint32_t accf0 = smem_u32(&bars[2 * NS]);      // accumulator b ready (MMA -> epilogue)
     const uint32_t acce0 = smem_u32(&bars[2 * NS + 2]);  // accumulator b drained (epilogue -> MMA)
-    const uint32_t cfull = smem_u32(&bars[2 * NS + 4]);  // C tile in shared memory
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * NS + 5]);
+    const uint32_t cfull0 = smem_u32(&bars[2 * NS + 4]);  // C slot c in shared memory (CH of them)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * NS + 4 + CH]);
+    static_assert(CH == 1 || CH == 2 || CH == 4, "C slots");
+    static_assert((2 * NS + 4 + CH) * 8 + 4 <= 256, "barrier area");
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (M2 + BM - 1) / BM, nt = (N + BN - 1) / BN;
@@ -292,7 +294,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
             mbar_init(accf0 + 8 * b, 1);
             mbar_init(acce0 + 8 * b, 4);
         }
-        mbar_init(cfull, 1);
+        for (int c = 0; c < CH; ++c) mbar_init(cfull0 + 8 * c, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -361,69 +363,87 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
             }
         }
     } else {
+        // C moves through CH slots of BN / CH columns: a slot's store (or
+        // reduction) is followed at once by the load of the same columns of
+        // the CTA's next tile, so with CH > 1 the next tile's first columns
+        // are already in flight while this tile's last ones are processed.
+        constexpr int CC = BN / CH;
+        constexpr int CHUNK_BYTES = BM * CC * 4;
         const int q = warp & 3;            // TMEM lane quarter of this warp
         const int et = threadIdx.x - 64;   // 0..127
         const int rt = q * 32 + lane;      // row of the tile
         const bool e0 = et == 0;
         int t = blockIdx.x;
         if (!REDUCE && e0 && t < tiles) {
-            mbar_expect_tx(cfull, C_TILE_BYTES);
-            tma_load_2d(sC, &tmC, cfull, (t % mt) * BM, (t / mt) * BN);
+            for (int c = 0; c < CH; ++c) {
+                mbar_expect_tx(cfull0 + 8 * c, CHUNK_BYTES);
+                tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (t % mt) * BM, (t / mt) * BN + c * CC);
+            }
         }
         for (int li = 0; t < tiles; t += gridDim.x, ++li) {
             const int b = li & 1;
             const uint32_t u = (uint32_t)(li >> 1);
-            const bool okc = REDUCE ? true : mbar_wait(cfull, (uint32_t)li & 1u, err);
+            const int tn = t + gridDim.x;
             int got = 0;
             if (lane == 0) got = mbar_wait(accf0 + 8 * b, u & 1u, err) ? 1 : 0;
             got = __shfl_sync(0xffffffffu, got, 0);
             __syncwarp();
-            if (got && okc) {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (got) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-                for (int chunk = 0; chunk < BN / 32; ++chunk) {
-                    float v[32];
-                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * ACC + chunk * 32);
-                    tmem_ld32(ta, v);
-                    if (HILO) {
-                        float w[32];
-                        tmem_ld32(ta + BN, w);
+            for (int c = 0; c < CH; ++c) {
+                const bool okc = REDUCE ? true : mbar_wait(cfull0 + 8 * c, (uint32_t)li & 1u, err);
+                float* cc = cs + c * (BM * CC);
+                if (got && okc) {
+#pragma unroll 1
+                    for (int sub = 0; sub < CC / 32; ++sub) {
+                        float v[32];
+                        const uint32_t ta =
+                            tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * ACC + c * CC + sub * 32);
+                        tmem_ld32(ta, v);
+                        if (HILO) {
+                            float w[32];
+                            tmem_ld32(ta + BN, w);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) v[j] += w[j];
+                            for (int j = 0; j < 32; ++j) v[j] += w[j];
+                        }
+                        if (REDUCE) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) cc[(sub * 32 + j) * BM + rt] = -v[j];
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) cc[(sub * 32 + j) * BM + rt] -= v[j];
+                        }
                     }
+                }
+                if (c == CH - 1) {  // every TMEM column of accumulator b has been read
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(acce0 + 8 * b);
+                }
+                // Generic-proxy writes of the slot, then the async-proxy store.
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                epilogue_bar();
+                if (e0) {
+                    const int x = (t % mt) * BM, y = (t / mt) * BN + c * CC;
                     if (REDUCE) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] = -v[j];
+                        // A tile whose accumulator wait failed adds nothing.
+                        if (got) tma_reduce_add_2d(&tmC, sC + c * CHUNK_BYTES, x, y);
                     } else {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) cs[(chunk * 32 + j) * BM + rt] -= v[j];
+                        tma_store_2d(&tmC, sC + c * CHUNK_BYTES, x, y);
+                    }
+                    bulk_commit();
+                    bulk_wait_read_all();  // the slot is free once the store has read it
+                    if (!REDUCE && tn < tiles) {
+                        mbar_expect_tx(cfull0 + 8 * c, CHUNK_BYTES);
+                        tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (tn % mt) * BM,
+                                    (tn / mt) * BN + c * CC);
                     }
                 }
+                // REDUCE: the slot is rewritten (next tile) only after its
+                // reduction has read it. Otherwise the next tile's writes
+                // wait for the slot's new load (cfull), issued after the read.
+                if (REDUCE) epilogue_bar();
             }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acce0 + 8 * b);
-            // Generic-proxy writes of the tile, then the async-proxy store.
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            epilogue_bar();
-            if (e0) {
-                if (REDUCE) {
-                    // A tile whose accumulator wait failed adds nothing.
-                    if (got && okc) tma_reduce_add_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
-                } else {
-                    tma_store_2d(&tmC, sC, (t % mt) * BM, (t / mt) * BN);
-                }
-                bulk_commit();
-                bulk_wait_read_all();  // the buffer is free once the store has read it
-                const int tn = t + gridDim.x;
-                if (!REDUCE && tn < tiles) {
-                    mbar_expect_tx(cfull, C_TILE_BYTES);
-                    tma_load_2d(sC, &tmC, cfull, (tn % mt) * BM, (tn / mt) * BN);
-                }
-            }
-            // The staging tile is rewritten only after the reduction or store
-            // above has read it.
-            epilogue_bar();
         }
         if (e0) bulk_wait_all();
     }
@@ -511,9 +531,40 @@ int encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType type, const void*
 struct GemmTC {
     unsigned* err = nullptr;
     int mode = 2;
-    bool attr_set = false, attr_set_p = false;
+    int c_slots = 4;  // C slots of the persistent kernel's epilogue (1 or 4)
+    bool attr_set = false;
+    bool attr_set_p[8] = {};
     int sms = 148;
 };
+
+template <bool REDUCE, bool HILO, int CH>
+int launch_one(unsigned grid, cudaStream_t stream, const CUtensorMap& ma, const CUtensorMap& mb,
+               const CUtensorMap& mc, int M2, int N, int K, unsigned* err, bool& attr_set) {
+    if (!attr_set) {
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<REDUCE, HILO, CH>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+        attr_set = true;
+    }
+    gemm_tf32_sub_persistent_kernel<REDUCE, HILO, CH><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, M2, N,
+                                                                                                K, err);
+    return SIEB200_OK;
+}
+
+// variant bit 0: reduction epilogue, bit 1: split operands, bit 2: four C slots.
+int launch_persistent(int variant, unsigned grid, cudaStream_t stream, const CUtensorMap& ma, const CUtensorMap& mb,
+                      const CUtensorMap& mc, int M2, int N, int K, unsigned* err, bool (&attr_set)[8]) {
+    bool& a = attr_set[variant];
+    switch (variant) {
+        case 0: return launch_one<false, false, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 1: return launch_one<true, false, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 2: return launch_one<false, true, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 3: return launch_one<true, true, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 4: return launch_one<false, false, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 5: return launch_one<true, false, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 6: return launch_one<false, true, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        default: return launch_one<true, true, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+    }
+}
 
 int gemm_tc_create(GemmTC** out) {
     GemmTC* g = new GemmTC();
@@ -528,6 +579,8 @@ int gemm_tc_create(GemmTC** out) {
     if (env && env[0] == '1') g->mode = 0;
     const char* mode_env = getenv("SIEB200_GEMM_MODE");
     if (mode_env && mode_env[0] >= '0' && mode_env[0] <= '3' && mode_env[1] == 0) g->mode = mode_env[0] - '0';
+    const char* slots_env = getenv("SIEB200_GEMM_C_SLOTS");
+    if (slots_env && slots_env[0] == '1' && slots_env[1] == 0) g->c_slots = 1;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -568,36 +621,17 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
     SIEB_CHECK(layout == 0 || (((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0), SIEB200_INVALID_ARG,
                "split-operand GEMM: C and its column stride must be 16-byte aligned");
     if ((g->mode >= 2 || layout == 1) && ((uintptr_t)C % 16) == 0 && ((ldc * 4) % 16) == 0) {
-        if (!g->attr_set_p) {
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false, false>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true, false>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<false, true>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
-            SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<true, true>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
-            g->attr_set_p = true;
-        }
+        const int ch = g->c_slots;
         CUtensorMap mc;
         SIEB_RETURN_IF(encode_tensor_map_2d(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, C, (uint64_t)M2, (uint64_t)N,
-                                            (uint64_t)ldc * sizeof(float), BM, BN, CU_TENSOR_MAP_SWIZZLE_NONE));
+                                            (uint64_t)ldc * sizeof(float), BM, BN / ch, CU_TENSOR_MAP_SWIZZLE_NONE));
         const int64_t tiles = ((M2 + BM - 1) / BM) * ((N + BN - 1) / BN);
         const int cap = max_ctas > 0 ? std::min(max_ctas, g->sms) : g->sms;
         const unsigned grid = (unsigned)std::min<int64_t>(tiles, std::max(1, cap));
         const bool red = g->mode == 3;
-        if (layout == 1 && red)
-            gemm_tf32_sub_persistent_kernel<true, true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
-                ma, mb, mc, (int)M2, (int)N, K, g->err);
-        else if (layout == 1)
-            gemm_tf32_sub_persistent_kernel<false, true><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
-                ma, mb, mc, (int)M2, (int)N, K, g->err);
-        else if (red)
-            gemm_tf32_sub_persistent_kernel<true, false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
-                ma, mb, mc, (int)M2, (int)N, K, g->err);
-        else
-            gemm_tf32_sub_persistent_kernel<false, false><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(
-                ma, mb, mc, (int)M2, (int)N, K, g->err);
+        const int variant = (red ? 1 : 0) + (layout == 1 ? 2 : 0) + (ch == 4 ? 4 : 0);
+        SIEB_RETURN_IF(launch_persistent(variant, grid, stream, ma, mb, mc, (int)M2, (int)N, K, g->err,
+                                         g->attr_set_p));
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;

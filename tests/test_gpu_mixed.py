@@ -23,12 +23,18 @@ def _tf32(x):
     return b.view(np.float32)
 
 
+@pytest.mark.parametrize("slots", ["4", "1"])
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
 @pytest.mark.parametrize("m2,n", [(256, 128), (300, 200), (1000, 517), (4096, 1500)])
-def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
+def test_gemm_tf32_sub(mode, m2, n, slots, gpu_ctx, monkeypatch):
+    """Every kernel mode, with the persistent kernel's C tile in four slots of
+    32 columns (default) or one slot of 128 (SIEB200_GEMM_C_SLOTS=1)."""
     import torch
     import sieb200
     from sieb200 import _lib
+    if mode < 2 and slots == "1":
+        pytest.skip("the slot count applies to the persistent kernel only")
+    monkeypatch.setenv("SIEB200_GEMM_C_SLOTS", slots)
     rng = np.random.default_rng(m2 + n)
     K = 384
     A = _tf32(rng.standard_normal((m2, K)))
@@ -46,9 +52,10 @@ def test_gemm_tf32_sub(mode, m2, n, gpu_ctx):
     assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
 
 
+@pytest.mark.parametrize("slots", ["4", "1"])
 @pytest.mark.parametrize("mode", [4, 5])
 @pytest.mark.parametrize("m2,n,K", [(256, 128, 256), (300, 200, 256), (1000, 517, 512), (4096, 1500, 256)])
-def test_gemm_tf32_sub_split_operands(mode, m2, n, K, gpu_ctx):
+def test_gemm_tf32_sub_split_operands(mode, m2, n, K, slots, gpu_ctx, monkeypatch):
     """Split operands [hi | lo] along k (modes 4 and 5): C -= A_hi B_hi^T +
     A_hi B_lo^T + A_lo B_hi^T with TF32 hi parts and FP32 remainders, against
     the FP64 product of the unsplit FP32 operands. Tolerance 1e-5 (the
@@ -56,6 +63,7 @@ def test_gemm_tf32_sub_split_operands(mode, m2, n, K, gpu_ctx):
     operands is off by ~1e-3)."""
     import torch
     from sieb200 import _lib
+    monkeypatch.setenv("SIEB200_GEMM_C_SLOTS", slots)
     rng = np.random.default_rng(m2 + n + K)
     KR = K // 2
     A = rng.standard_normal((m2, KR)).astype(np.float32)
