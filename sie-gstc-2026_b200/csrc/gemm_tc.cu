@@ -530,7 +530,7 @@ int encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType type, const void*
 
 struct GemmTC {
     unsigned* err = nullptr;
-    int mode = 2;
+    int mode = 3;  // persistent kernel, reduction epilogue
     int c_slots = 4;  // C slots of the persistent kernel's epilogue (1 or 4)
     bool attr_set = false;
     bool attr_set_p[8] = {};

@@ -23,10 +23,12 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
                 const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0, int layout = 0);
 int gemm_tc_check(GemmTC* g, cudaStream_t stream);
 // Selects the implementation: 3 = persistent tcgen05 kernel whose epilogue
-// adds -acc to C by TMA reduction, 2 = persistent kernel that loads,
-// subtracts and stores the C tile by TMA (default), 1 = one CTA per tile
+// adds -acc to C by TMA reduction (default), 2 = persistent kernel that
+// loads, subtracts and stores the C tile by TMA, 1 = one CTA per tile
 // tcgen05 kernel, 0 = SIMT on the same packed operands (checking path).
-// SIEB200_GEMM_MODE=<0..3> in the environment overrides the default.
+// SIEB200_GEMM_MODE=<0..3> in the environment overrides the default;
+// SIEB200_GEMM_C_SLOTS=1 moves C in one 128-column slot instead of four
+// 32-column ones.
 void gemm_tc_set_mode(GemmTC* g, int mode);
 
 }  // namespace sieb200
