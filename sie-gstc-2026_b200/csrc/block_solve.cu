@@ -388,6 +388,138 @@ __global__ void bcopy_kernel(int64_t n, const cplx* __restrict__ X, int64_t ldx,
     Y[r + (int64_t)c * ldy] = X[r + (int64_t)c * ldx];
 }
 
+// The same product on the FP64 tensor cores (mma.sync m8n8k4 .f64, 256 FMAs
+// per warp instruction): CTA tile 64 x 64 complex, four warps of 32 x 32,
+// K stages of 16 complex columns brought by cp.async (16 bytes per complex
+// entry, zero-filled outside the operands) into a 3-deep ring. Each 8 x 8
+// output block keeps its real and imaginary parts in two accumulators:
+//   Re += Ar Br + (-Ai) Bi,  Im += Ar Bi + Ai Br,
+// four MMAs per block and k-step of 4. Fragments (PTX m8n8k4 .f64 layout):
+// lane l holds A(l / 4, l % 4), B(l % 4, l / 4) and D(l / 4, 2 (l % 4) + {0, 1}).
+// Shared layouts: A as [k][row] with rows padded to 66 (conflict-free
+// 16-byte fragment loads), X as [col][k] with k padded to 20.
+constexpr int ZD_BM = 64, ZD_BN = 64, ZD_BK = 16, ZD_THREADS = 128, ZD_STAGES = 3;
+constexpr int ZD_ALD = ZD_BM + 2, ZD_XLD = ZD_BK + 4;
+constexpr int ZD_STAGE_A = ZD_BK * ZD_ALD, ZD_STAGE_X = ZD_BN * ZD_XLD;  // complex entries
+constexpr int kSmemZgemmDmma = ZD_STAGES * (ZD_STAGE_A + ZD_STAGE_X) * 16;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool in) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(ZD_THREADS, 2) zgemm_dmma_kernel(int64_t m, int64_t nc, int64_t kdim,
+                                                                   const double2* __restrict__ A, int64_t lda,
+                                                                   const double2* __restrict__ X, int64_t ldx,
+                                                                   double2* __restrict__ C, int64_t ldc,
+                                                                   double2 alpha, double2 beta) {
+    extern __shared__ __align__(16) double2 zd_smem[];
+    double2* As = zd_smem;                                // [stage][k][ZD_ALD]
+    double2* Xs = zd_smem + ZD_STAGES * ZD_STAGE_A;       // [stage][col][ZD_XLD]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t row0 = (int64_t)blockIdx.x * ZD_BM, col0 = (int64_t)blockIdx.y * ZD_BN;
+    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;  // warp tile origin in the CTA tile
+    const int nk = (int)((kdim + ZD_BK - 1) / ZD_BK);
+
+    auto issue = [&](int kt) {
+        const int st = kt % ZD_STAGES;
+        const int64_t k0 = (int64_t)kt * ZD_BK;
+        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(As + st * ZD_STAGE_A);
+        const uint32_t sx = (uint32_t)__cvta_generic_to_shared(Xs + st * ZD_STAGE_X);
+#pragma unroll
+        for (int u = 0; u < ZD_BM * ZD_BK / ZD_THREADS; ++u) {  // A: rows fastest
+            const int e = tid + u * ZD_THREADS;
+            const int r = e % ZD_BM, kk = e / ZD_BM;
+            const int64_t gr = row0 + r, gk = k0 + kk;
+            const bool in = gr < m && gk < kdim;
+            cp_async16(sa + (uint32_t)(kk * ZD_ALD + r) * 16u, in ? (const void*)(A + gr + gk * lda) : (const void*)A,
+                       in);
+        }
+#pragma unroll
+        for (int u = 0; u < ZD_BN * ZD_BK / ZD_THREADS; ++u) {  // X: k fastest
+            const int e = tid + u * ZD_THREADS;
+            const int kk = e % ZD_BK, c = e / ZD_BK;
+            const int64_t gk = k0 + kk, gc = col0 + c;
+            const bool in = gk < kdim && gc < nc;
+            cp_async16(sx + (uint32_t)(c * ZD_XLD + kk) * 16u, in ? (const void*)(X + gk + gc * ldx) : (const void*)X,
+                       in);
+        }
+    };
+
+    double re[4][4][2], im[4][4][2];  // [row block][col block][fragment pair]
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < ZD_STAGES - 1; ++s) {
+        if (s < nk) issue(s);
+        cp_async_commit();
+    }
+    const int fr = lane >> 2, fk = lane & 3;
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<ZD_STAGES - 2>();
+        __syncthreads();  // stage kt is in; stage kt - 1 is no longer read
+        if (kt + ZD_STAGES - 1 < nk) issue(kt + ZD_STAGES - 1);
+        cp_async_commit();
+        const double2* as = As + (kt % ZD_STAGES) * ZD_STAGE_A;
+        const double2* xs = Xs + (kt % ZD_STAGES) * ZD_STAGE_X;
+#pragma unroll
+        for (int k4 = 0; k4 < ZD_BK; k4 += 4) {
+            double2 af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = as[(k4 + fk) * ZD_ALD + wr + 8 * i + fr];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bf[j] = xs[(wc + 8 * j + fr) * ZD_XLD + k4 + fk];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double nai = -af[i].y;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dmma(re[i][j][0], re[i][j][1], af[i].x, bf[j].x);
+                    dmma(re[i][j][0], re[i][j][1], nai, bf[j].y);
+                    dmma(im[i][j][0], im[i][j][1], af[i].x, bf[j].y);
+                    dmma(im[i][j][0], im[i][j][1], af[i].y, bf[j].x);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+    const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t gr = row0 + wr + 8 * i + fr;
+        if (gr >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int64_t gc = col0 + wc + 8 * j + 2 * fk + h;
+                if (gc >= nc) continue;
+                const double vr = re[i][j][h], vi = im[i][j][h];
+                double2 out = make_double2(alpha.x * vr - alpha.y * vi, alpha.x * vi + alpha.y * vr);
+                if (use_beta) {
+                    const double2 c = C[gr + gc * ldc];
+                    out.x += beta.x * c.x - beta.y * c.y;
+                    out.y += beta.x * c.y + beta.y * c.x;
+                }
+                C[gr + gc * ldc] = out;
+            }
+        }
+    }
+}
+
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -398,6 +530,28 @@ int zgemm_device(cudaStream_t stream, int64_t m, int64_t nc, int64_t kdim, const
                  const cplx* X, int64_t ldx, cplx* C, int64_t ldc, cplx alpha, cplx beta) {
     if (m <= 0 || nc <= 0) return SIEB200_OK;
     SIEB_CHECK(nc < 65536ll * ZG_BN && m < (1ll << 40), SIEB200_INVALID_ARG, "zgemm: size out of range");
+    // The tensor-core kernel needs 16-byte aligned operands (cp.async of one
+    // complex entry); SIEB200_ZGEMM_DMMA=0 selects the FMA kernel.
+    const char* dm_env = getenv("SIEB200_ZGEMM_DMMA");
+    const bool aligned = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(X) |
+                           reinterpret_cast<uintptr_t>(C)) & 15) == 0;
+    if (!(dm_env && dm_env[0] == '0') && aligned && nc < 65536ll * ZD_BN) {
+        static bool attr_set[64] = {};
+        int dev = 0;
+        SIEB_TRY_CUDA(cudaGetDevice(&dev));
+        if (!attr_set[dev & 63]) {
+            SIEB_TRY_CUDA(cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSmemZgemmDmma));
+            attr_set[dev & 63] = true;
+        }
+        const dim3 grid(nblk(m, ZD_BM), nblk(nc, ZD_BN));
+        zgemm_dmma_kernel<<<grid, ZD_THREADS, kSmemZgemmDmma, stream>>>(
+            m, nc, kdim, reinterpret_cast<const double2*>(A), lda, reinterpret_cast<const double2*>(X), ldx,
+            reinterpret_cast<double2*>(C), ldc, make_double2(alpha.re, alpha.im), make_double2(beta.re, beta.im));
+        SIEB_NOTE_LAUNCH();
+        SIEB_TRY_CUDA(cudaGetLastError());
+        return SIEB200_OK;
+    }
     const dim3 grid(nblk(m, ZG_BM), nblk(nc, ZG_BN));
     zgemm_kernel<<<grid, ZG_THREADS, 0, stream>>>(m, nc, kdim, reinterpret_cast<const double2*>(A), lda,
                                                   reinterpret_cast<const double2*>(X), ldx,

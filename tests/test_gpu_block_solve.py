@@ -1,8 +1,8 @@
 """GPU: the multi-right-hand-side mixed solve (tensor-core block triangular
 solves inside a batched FGMRES) and the FP64 complex GEMM it refines with.
 
-Tolerances: the FP64 GEMM <= 1e-13 (max-entry error over the largest entry)
-against numpy; every column of a block solve reaches the requested relative
+Tolerances: both FP64 GEMM kernels <= 1e-13 (max-entry error over the
+largest entry) against numpy; every column of a block solve reaches the requested relative
 residual (1e-10, with the FP64 GEMM) and agrees with numpy's FP64 solution
 to <= 1e-9 (forward error bounded by the condition of these systems times
 the residual), as does the column-by-column solve it replaces."""
@@ -30,10 +30,15 @@ def _host(t, rows, cols):
     return a
 
 
-@pytest.mark.parametrize("m,nc,k", [(1, 1, 1), (130, 7, 77), (1000, 64, 999), (257, 33, 300), (64, 1, 2000)])
-def test_zgemm_matches_numpy(m, nc, k, gpu_ctx):
+@pytest.mark.parametrize("kernel", ["dmma", "fma"])
+@pytest.mark.parametrize("m,nc,k", [(1, 1, 1), (130, 7, 77), (1000, 64, 999), (257, 33, 300), (64, 1, 2000),
+                                    (600, 700, 64)])
+def test_zgemm_matches_numpy(m, nc, k, kernel, gpu_ctx, monkeypatch):
+    """Both FP64 complex GEMM kernels: the tensor-core one (mma.sync .f64)
+    and the FMA one (SIEB200_ZGEMM_DMMA=0)."""
     import torch
     import sieb200
+    monkeypatch.setenv("SIEB200_ZGEMM_DMMA", "1" if kernel == "dmma" else "0")
     rng = np.random.default_rng(m + 7 * nc + k)
     A = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
     X = rng.standard_normal((k, nc)) + 1j * rng.standard_normal((k, nc))
