@@ -49,7 +49,7 @@ WORKLOAD = ("T-PMCHWT dielectric sphere r=0.5 m, eps_r=4, mu_r=1, ka=pi; geodesi
 # DRAM bytes (read + write) per trailing-update launch, mean over the 92
 # launches of one factorization of this workload, from one ncu capture of
 # the trailing GEMM (dram__bytes_read.sum + dram__bytes_write.sum).
-GEMM_DRAM_BYTES_PER_LAUNCH = 163.7e6
+GEMM_DRAM_BYTES_PER_LAUNCH = 155.5e6
 # FP64 flops per Green evaluation (one point pair, one wavenumber) of the
 # T-PMCHWT regular pass, counted from the kernel's source with an FMA as 2:
 # the point-pair geometry shared by the two wavenumbers (distance, r_p.r_q,
