@@ -1044,6 +1044,32 @@ def adjoint_section(ctx, steps: int, max_over_ranks):
     }
 
 
+def timeline_summary(spans):
+    """Critical path of one factorization and solve from the library's
+    timeline [(kind, start_ms, end_ms)]: kinds 0 trailing GEMM, 1 triangular
+    solve, 2 FP64 matvec, 3 diagonal block, 4 panels, 6 factorization,
+    7 refined solve. A block step runs panels(k), then the GEMM of step k
+    beside the next diagonal block."""
+    span = {k: [(a, b) for kk, a, b in spans if kk == k] for k in range(8)}
+    total = {name: sum(b - a for a, b in span[k]) for k, name in
+             [(0, "gemm_ms"), (1, "trsv_ms"), (2, "matvec_ms"), (3, "diag_ms"), (4, "panels_ms")]}
+    pan, gem, dia = span[4], span[0], span[3]
+    steps = []
+    for k in range(len(pan) - 1):
+        g = [b - a for a, b in gem if pan[k][1] - 1e-6 <= a < pan[k + 1][0]]
+        d = [b - a for a, b in dia if pan[k][0] - 1e-6 <= a < pan[k + 1][0]]
+        steps.append((pan[k + 1][0] - pan[k][1], g[0] if g else 0.0, d[0] if d else 0.0))
+    fact = span[6][0][1] - span[6][0][0] if span[6] else None
+    solve = span[7][0][1] - span[7][0][0] if span[7] else None
+    return {"factorization_ms": fact, "refined_solve_ms": solve, **total,
+            "steps_bound_by_gemm": sum(1 for _, g, d in steps if g > d),
+            "steps_bound_by_diag": sum(1 for _, g, d in steps if g <= d),
+            "sum_max_gemm_diag_ms": sum(max(g, d) for _, g, d in steps),
+            "gaps_ms": sum(t - max(g, d) for t, g, d in steps),
+            "trsv_us": [round(1e3 * (b - a), 1) for a, b in span[1]],
+            "matvec_us": [round(1e3 * (b - a), 1) for a, b in span[2]]}
+
+
 def run_case(args):
     """One small workload for a profiler capture (ncu -k <kernel> -c <n>):
     no timing, one short JSON summary. Cases:
@@ -1053,6 +1079,9 @@ def run_case(args):
       multi_rhs      mixed solve of 64 plane-wave right-hand sides of it
       fp64_lu        own FP64 LU factorization and solve of it
       residual       four FP64 residual matvecs b - Z x of that system (576 MB each)
+      timeline       one mixed factorization and refined solve of it with the
+                     library's per-launch timeline (after three warm-up solves);
+                     prints the critical-path summary
     """
     import torch
     import sieb200
@@ -1092,6 +1121,22 @@ def run_case(args):
             sieb200.matvec(N, Z.data_ptr(), x.data_ptr(), y.data_ptr(), beta=-1.0, ctx=ctx)
         ctx.synchronize()
         out["y_norm"] = float(y.norm())
+    elif args.case == "timeline":
+        b = torch.from_numpy(sieb200.assemble_rhs(mesh, opts, [sieb200.PlaneWaveExcitation()], ctx=ctx)[:, 0]
+                             .copy()).cuda()
+        s = sieb200.DenseLuSolver(N, "mixed_ir", ctx=ctx)
+        for i in range(4):
+            if i == 3:
+                ctx.profile(True, timeline=True)
+            s.factorize(Z.data_ptr())
+            x = b.clone()
+            torch.cuda.synchronize()
+            s.solve(x.data_ptr(), tolerance=1e-10, max_iterations=60)
+            ctx.synchronize()
+        spans = sorted(ctx.profile_timeline(), key=lambda v: v[1])
+        ctx.profile(False)
+        s.close()
+        out.update(timeline_summary(spans))
     elif not args.case.startswith("assembly"):
         raise SystemExit(f"unknown case {args.case}")
     del Z
