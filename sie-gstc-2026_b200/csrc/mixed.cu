@@ -154,11 +154,6 @@ __global__ void rbt_vec_N_kernel(const cplx* __restrict__ y, int64_t n, int64_t 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 crecipf(float2 a) {
-    const float inv = __frcp_rn(a.x * a.x + a.y * a.y);
-    return make_float2(a.x * inv, -a.y * inv);
-}
 
 __device__ __forceinline__ float2 cnegf(float2 a) { return make_float2(-a.x, -a.y); }
 // a - c x with fused multiply-adds.
@@ -626,11 +621,6 @@ __global__ void __launch_bounds__(256) trailing_simt_kernel(float2* __restrict__
 }
 
 // ------------------------------------------------------------ triangular solves
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 // Published solution entries: every 8-byte word of the publication buffer
 // starts as all ones (a NaN payload arithmetic does not produce) and is
 // written once; each word is single-copy atomic, so an entry whose two
@@ -780,7 +770,6 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     for (int i = 0, g = 0; i < n_off; ++g) {
         const int sb = (tile_k(i) * TR_COLS) / NB;
         const int cnt = (i + 1 < n_off && (tile_k(i + 1) * TR_COLS) / NB == sb) ? 2 : 1;
-        const unsigned need = lower ? (unsigned)sb + 1u : (unsigned)(nsb - sb);
         cplx* xg = xstage + (g & 1) * NB;
         if (warp == 0) {
             // Each lane polls its entries of the sub-block in the publication
@@ -976,11 +965,6 @@ __global__ void combo_kernel(int64_t n, int k, const cplx* __restrict__ V, int64
 __global__ void add_kernel(int64_t n, const cplx* __restrict__ a, cplx* __restrict__ x) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] += a[i];
-}
-
-__global__ void conj_kernel(int64_t n, cplx* __restrict__ x) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x[i].im = -x[i].im;
 }
 
 // Adjoint support: W^H solves are done on the conjugate transpose factors.
@@ -1512,11 +1496,6 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     return SIEB200_OK;
 }
 
-static double host_norm2(const std::vector<cplx>& v) {
-    long double s = 0;
-    for (const cplx& c : v) s += (long double)c.re * c.re + (long double)c.im * c.im;
-    return std::sqrt((double)s);
-}
 
 // Restarted flexible GMRES on A x = b or A^H x = b (FP64, A the intact complex128 matrix)
 // with right preconditioner M^{-1}, started from x = 0. The preconditioned
@@ -1535,8 +1514,9 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     const int m = std::max(1, std::min(maxit, 100));
     const int parts = 64;
     // vectors: x, r, w, work(np), V (n x (m+1)), Z (n x m), partial, h
+    // h: two CGS passes of up to m + 1 coefficients each and ||w||^2
     const size_t vbytes =
-        sizeof(cplx) * (4 * np + (int64_t)(m + 1) * n + (int64_t)m * n + parts * (m + 1) + (m + 2));
+        sizeof(cplx) * (4 * np + (int64_t)(m + 1) * n + (int64_t)m * n + parts * (m + 1) + (2 * m + 4));
     SIEB_RETURN_IF(s->krylov.reserve(vbytes));
     cplx* x = s->krylov.as<cplx>();
     cplx* r = x + np;
@@ -1549,16 +1529,12 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
     const double* A = s->A;
     const int64_t lda = s->lda;
 
-    // ||b||
-    std::vector<cplx> hb(n);
-    SIEB_TRY_CUDA(cudaMemcpyAsync(hb.data(), b, sizeof(cplx) * n, cudaMemcpyDeviceToHost, stream));
-    SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
-    const double bnorm = host_norm2(hb);
-    SIEB_CHECK(bnorm > 0 && std::isfinite(bnorm), SIEB200_INVALID_ARG, "right-hand side norm must be finite and nonzero");
+    // ||b|| is the first residual norm (x0 = 0), read with it below.
+    double bnorm = 0.0;
 
     SIEB_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(cplx) * n, stream));
     int total = 0;
-    std::vector<cplx> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), hh(m + 2);
+    std::vector<cplx> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), hh(2 * m + 4);
     for (int outer = 0; outer < 1000; ++outer) {
         // r = A x - b (for x = 0 simply -b)
         if (outer == 0) {
@@ -1579,6 +1555,11 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
         SIEB_TRY_CUDA(cudaMemcpyAsync(&rr, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
         SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
         const double beta = std::sqrt(std::max(rr.re, 0.0));
+        if (outer == 0) {
+            bnorm = beta;
+            SIEB_CHECK(bnorm > 0 && std::isfinite(bnorm), SIEB200_INVALID_ARG,
+                       "right-hand side norm must be finite and nonzero");
+        }
         if (!std::isfinite(beta)) {
             set_error("GMRES refinement produced a non-finite residual");
             return SIEB200_NONFINITE;
@@ -1614,28 +1595,29 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
                 else
                     SIEB_RETURN_IF(gemv_device(ctx, n, A, lda, 0, zj, 0.0, w, s->gemv_scratch));
             }
-            // Classical Gram-Schmidt with one reorthogonalization (CGS2).
-            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = cx(0, 0);
+            // Classical Gram-Schmidt with one reorthogonalization (CGS2): the
+            // two passes' coefficients (h, h + j + 1) and ||w||^2 (h + 2j + 2)
+            // stay on the device and come back in one copy.
+            const int fin_threads = std::min(1024, ((j + 1 + 31) / 32) * 32);
             for (int pass = 0; pass < 2; ++pass) {
+                cplx* hp = h + pass * (j + 1);
                 dot_partial_kernel<<<dim3(parts, j + 1), 256, 0, stream>>>(n, j + 1, V, n, w, partial);
                 SIEB_NOTE_LAUNCH();
-                dot_finish_kernel<<<1, 64, 0, stream>>>(j + 1, parts, partial, h);
+                dot_finish_kernel<<<1, fin_threads, 0, stream>>>(j + 1, parts, partial, hp);
                 SIEB_NOTE_LAUNCH();
-                axpy_multi_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j + 1, V, n, h, w);
+                axpy_multi_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, j + 1, V, n, hp, w);
                 SIEB_NOTE_LAUNCH();
                 SIEB_TRY_CUDA(cudaGetLastError());
-                SIEB_TRY_CUDA(cudaMemcpyAsync(hh.data(), h, sizeof(cplx) * (j + 1), cudaMemcpyDeviceToHost,
-                                              stream));
-                SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
-                for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = H[(size_t)i * m + j] + hh[i];
             }
             dot_partial_kernel<<<dim3(parts, 1), 256, 0, stream>>>(n, 1, w, n, w, partial);
             SIEB_NOTE_LAUNCH();
-            dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h);
+            dot_finish_kernel<<<1, 32, 0, stream>>>(1, parts, partial, h + 2 * (j + 1));
             SIEB_NOTE_LAUNCH();
-            cplx ww;
-            SIEB_TRY_CUDA(cudaMemcpyAsync(&ww, h, sizeof(cplx), cudaMemcpyDeviceToHost, stream));
+            SIEB_TRY_CUDA(cudaMemcpyAsync(hh.data(), h, sizeof(cplx) * (2 * (j + 1) + 1), cudaMemcpyDeviceToHost,
+                                          stream));
             SIEB_TRY_CUDA(cudaStreamSynchronize(stream));
+            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hh[i] + hh[j + 1 + i];
+            const cplx ww = hh[2 * (j + 1)];
             const double hn = std::sqrt(std::max(ww.re, 0.0));
             cplx hj1 = cx(hn, 0);
             if (j + 1 <= m) {
