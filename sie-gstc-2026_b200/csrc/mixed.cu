@@ -1028,36 +1028,43 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 // Own FP64 LU: diagonal block k of a triangular solve, Y_k = Inv_k Y_k in
 // place for 16 columns per CTA (complex128; rows beyond the block's width
-// are left alone, the inverse is padded with the identity).
+// are left alone, the inverse is padded with the identity). Thread (r, p)
+// holds row r of Inv_k over columns 16p .. 16p+15 in registers (all its
+// loads issued at once), forms that quarter of each column's product, and
+// the four quarters are summed through shared memory.
 __global__ void __launch_bounds__(256) fp64_diag_apply_kernel(cplx* __restrict__ Y, int64_t ldy, int64_t k0, int kb,
                                                               int nrhs, const double2* __restrict__ Inv) {
     __shared__ double2 ys[16][NB];
+    __shared__ double2 red[4][NB];
     const int tid = threadIdx.x;
     const int c0 = blockIdx.x * 16;
+    const int r = tid & (NB - 1), p = tid >> 6;
+    double2 inv[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) inv[u] = __ldg(&Inv[r + (16 * p + u) * NB]);  // column-major
     for (int e = tid; e < 16 * NB; e += blockDim.x) {
-        const int r = e % NB, c = e / NB;
-        const cplx v = (c0 + c < nrhs && r < kb) ? Y[(k0 + r) + (int64_t)(c0 + c) * ldy] : cx(0, 0);
-        ys[c][r] = make_double2(v.re, v.im);
+        const int rr = e % NB, c = e / NB;
+        const cplx v = (c0 + c < nrhs && rr < kb) ? Y[(k0 + rr) + (int64_t)(c0 + c) * ldy] : cx(0, 0);
+        ys[c][rr] = make_double2(v.re, v.im);
     }
     __syncthreads();
-    const int c = tid / 16, r0 = (tid % 16) * 4;
-    double2 acc[4];
+    const int ncol = min(16, nrhs - c0);
+    for (int c = 0; c < ncol; ++c) {
+        double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) acc[u] = make_double2(0.0, 0.0);
-    for (int kk = 0; kk < NB; ++kk) {
-        const double2 y = ys[c][kk];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const double2 a = __ldg(&Inv[(r0 + u) + kk * NB]);  // column-major, L1/L2 resident
-            acc[u].x = fma(a.x, y.x, fma(-a.y, y.y, acc[u].x));
-            acc[u].y = fma(a.x, y.y, fma(a.y, y.x, acc[u].y));
+        for (int u = 0; u < 16; ++u) {
+            const double2 y = ys[c][16 * p + u];
+            acc.x = fma(inv[u].x, y.x, fma(-inv[u].y, y.y, acc.x));
+            acc.y = fma(inv[u].x, y.y, fma(inv[u].y, y.x, acc.y));
         }
+        red[p][r] = acc;
+        __syncthreads();
+        if (p == 0 && r < kb) {
+            const double2 s1 = red[1][r], s2 = red[2][r], s3 = red[3][r];
+            Y[(k0 + r) + (int64_t)(c0 + c) * ldy] = cx(acc.x + s1.x + s2.x + s3.x, acc.y + s1.y + s2.y + s3.y);
+        }
+        __syncthreads();
     }
-    const int gc = c0 + c;
-    if (gc >= nrhs) return;
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-        if (r0 + u < kb) Y[(k0 + r0 + u) + (int64_t)gc * ldy] = cx(acc[u].x, acc[u].y);
 }
 
 // X(:, c) += D(:, c)
