@@ -382,6 +382,10 @@ int64_t sieb200_launch_count(void);
  * flops; dependent-FMA chains on every SM, best of 5 timed launches): the
  * denominator of the assembly's FP64-pipe roofline (no reference counterpart). */
 int sieb200_fp64_fma_peak(sieb200_ctx* ctx, double* tflops);
+/* The same for the FP64 tensor cores (mma.sync m8n8k4 .f64, independent
+ * accumulators on every SM): the denominator of the FP64 complex GEMM's
+ * roofline (sieb200_zgemm; no reference counterpart). */
+int sieb200_fp64_mma_peak(sieb200_ctx* ctx, double* tflops);
 int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double* total_ms,
                          double* flops, double* bytes);
 

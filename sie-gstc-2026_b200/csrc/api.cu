@@ -1009,6 +1009,12 @@ int sieb200_fp64_fma_peak(sieb200_ctx* ctx, double* tflops) {
     return fp64_fma_rate(ctx, tflops);
 }
 
+int sieb200_fp64_mma_peak(sieb200_ctx* ctx, double* tflops) {
+    SIEB_CHECK(ctx && tflops, SIEB200_INVALID_ARG, "invalid FP64 probe arguments");
+    SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
+    return fp64_mma_rate(ctx, tflops);
+}
+
 int sieb200_profile_enable(sieb200_ctx* ctx, int enable) {
     SIEB_CHECK(ctx && enable >= 0 && enable <= 2, SIEB200_INVALID_ARG, "invalid profile mode");
     ctx->prof.collect();

@@ -522,7 +522,27 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* out, int it
     if (sum == -1.0) out[0] = sum;
 }
 
-int fp64_fma_rate(sieb200_ctx* ctx, double* tflops) {
+// The same with the FP64 tensor cores: eight independent accumulators of
+// mma.sync m8n8k4 .f64 per warp (256 FMAs per instruction).
+__global__ void __launch_bounds__(256) fp64_mma_probe_kernel(double* out, int iters) {
+    const double a = 1e-3 * (threadIdx.x & 31), b = 1e-3 * blockIdx.x;
+    double d[8][2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) d[j][0] = d[j][1] = 0.0;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                         : "+d"(d[j][0]), "+d"(d[j][1])
+                         : "d"(a), "d"(b));
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sum += d[j][0] + d[j][1];
+    if (sum == -1.0) out[0] = sum;
+}
+
+static int fp64_probe(sieb200_ctx* ctx, bool mma, double* tflops) {
     const int iters = 8192;
     const unsigned grid = (unsigned)ctx->sm_count * 4u;
     DeviceBuffer sink;
@@ -533,7 +553,10 @@ int fp64_fma_rate(sieb200_ctx* ctx, double* tflops) {
     float best = 1e30f;
     for (int rep = 0; rep < 6; ++rep) {
         cudaEventRecord(a, ctx->stream);
-        fp64_fma_probe_kernel<<<grid, 256, 0, ctx->stream>>>(sink.as<double>(), iters);
+        if (mma)
+            fp64_mma_probe_kernel<<<grid, 256, 0, ctx->stream>>>(sink.as<double>(), iters / 8);
+        else
+            fp64_fma_probe_kernel<<<grid, 256, 0, ctx->stream>>>(sink.as<double>(), iters);
         SIEB_NOTE_LAUNCH();
         cudaEventRecord(b, ctx->stream);
         cudaEventSynchronize(b);
@@ -543,9 +566,14 @@ int fp64_fma_rate(sieb200_ctx* ctx, double* tflops) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     SIEB_TRY_CUDA(cudaGetLastError());
-    const double flops = 2.0 * 8.0 * iters * (double)grid * 256.0;
+    // FMA: 8 chains per thread; MMA: 8 accumulators per warp, 256 FMAs each
+    const double flops = mma ? 2.0 * 256.0 * 8.0 * (iters / 8) * (double)grid * 8.0
+                             : 2.0 * 8.0 * iters * (double)grid * 256.0;
     *tflops = flops / (best * 1e-3) / 1e12;
     return SIEB200_OK;
 }
+
+int fp64_fma_rate(sieb200_ctx* ctx, double* tflops) { return fp64_probe(ctx, false, tflops); }
+int fp64_mma_rate(sieb200_ctx* ctx, double* tflops) { return fp64_probe(ctx, true, tflops); }
 
 }  // namespace sieb200

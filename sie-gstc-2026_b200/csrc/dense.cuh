@@ -46,6 +46,7 @@ int gemv_h_device(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, const
 // Same product with its partial sums in a fixed device array (no allocation).
 // Measured FP64 FMA throughput of the device (TFLOP/s; FMA = 2 flops).
 int fp64_fma_rate(sieb200_ctx* ctx, double* tflops);
+int fp64_mma_rate(sieb200_ctx* ctx, double* tflops);
 int gemv_device_static_scratch(sieb200_ctx* ctx, int64_t n, const void* A, int64_t lda, int prec,
                                const cplx* x, double beta, cplx* y);
 void destroy_cusolver(sieb200_ctx* ctx);

@@ -128,6 +128,7 @@ _SIGNATURES = {
     "sieb200_incident_fields": ([_P, _P, _P, _I64, _P, _P, _P], ctypes.c_int),
     "sieb200_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "sieb200_fp64_fma_peak": ([_P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "sieb200_fp64_mma_peak": ([_P, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     "sieb200_profile_timeline": ([_P, _I64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I64)], ctypes.c_int),
     "sieb200_launch_count": ([], ctypes.c_int64),

@@ -205,6 +205,12 @@ class Context:
         _lib.check(_lib.lib().sieb200_fp64_fma_peak(self._h, ctypes.byref(t)))
         return t.value
 
+    def fp64_mma_peak(self) -> float:
+        """Measured FP64 tensor-core (mma.sync .f64) throughput, TFLOP/s."""
+        t = ctypes.c_double()
+        _lib.check(_lib.lib().sieb200_fp64_mma_peak(self._h, ctypes.byref(t)))
+        return t.value
+
     def profile_timeline(self) -> list:
         """[(kernel kind, start_ms, end_ms)] of the spans since profile(timeline=True),
         times relative to that call (kinds as in profile_read)."""

@@ -344,3 +344,6 @@ def test_fp64_fma_peak_is_plausible(gpu_ctx):
     few tens of TFLOP/s of FP64 FMA, far from zero and from tensor rates."""
     t = gpu_ctx.fp64_fma_peak()
     assert 5.0 < t < 200.0
+    # the FP64 tensor cores of a B200 run at about the FMA rate
+    tm = gpu_ctx.fp64_mma_peak()
+    assert 0.5 * t < tm < 4.0 * t
