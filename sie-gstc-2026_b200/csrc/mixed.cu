@@ -1097,6 +1097,7 @@ void mixed_release(DenseSolver* s) {
         if (st->gemm) gemm_tc_destroy(st->gemm);
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
+        if (st->ev_pan) cudaEventDestroy(st->ev_pan);
         if (st->side) cudaStreamDestroy(st->side);
         delete st;
     }
@@ -1126,6 +1127,10 @@ static int check_err(DenseSolver* s, const char* what) {
 }
 
 static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3);
+// Overlapped block steps (see mixed_enqueue): trailing updates at least this
+// many columns wide (0: none), and the SMs they leave to the panels.
+constexpr int kOverlapMinDefault = 0;
+constexpr int kOverlapSmsDefault = 20;
 
 static int fp64_factorize(DenseSolver* s);
 
@@ -1152,6 +1157,10 @@ int mixed_factorize(DenseSolver* s) {
     st->pair = (pair_env && pair_env[0] == '1') ? 1 : 0;
     const char* hilo_env = getenv("SIEB200_GEMM_HILO");
     st->hilo = (hilo_env && hilo_env[0] == '0') ? 0 : 1;
+    const char* ovl_env = getenv("SIEB200_OVERLAP_MIN");
+    st->ovl_min = ovl_env ? std::max(0, atoi(ovl_env)) : kOverlapMinDefault;
+    const char* ovs_env = getenv("SIEB200_OVERLAP_SMS");
+    st->ovl_sms = ovs_env ? std::max(2, std::min(s->ctx->sm_count / 2, atoi(ovs_env))) : kOverlapSmsDefault;
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -1170,7 +1179,8 @@ int mixed_factorize(DenseSolver* s) {
     const int K3 = 6 * NB;
     const size_t bApack = ((sizeof(float) * 2 * np * K3 + 255) / 256) * 256;
     SIEB_RETURN_IF(s->gemm_a.reserve(2 * bApack));
-    SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * 2 * K3));  // the pair schedule's K = 2 x 384
+    // two step buffers (single-step schedule) or the pair schedule's K = 2 x 384
+    SIEB_RETURN_IF(s->gemm_b.reserve(sizeof(float) * np * 2 * K3));
     st->Apack[0] = s->gemm_a.as<float>();
     st->Apack[1] = reinterpret_cast<float*>(s->gemm_a.as<char>() + bApack);
     st->Bpack = s->gemm_b.as<float>();
@@ -1181,6 +1191,7 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_pan, cudaEventDisableTiming));
     }
 
     static bool attrs_set = false;
@@ -1196,6 +1207,7 @@ int mixed_factorize(DenseSolver* s) {
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
     key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo; key.sms = gemm_sms;
+    key.ovl = st->ovl_min * 1000 + st->ovl_sms;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -1291,7 +1303,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     const int64_t KS = hilo ? 4 * NB : K3;  // pack width of one step
     const int64_t KP = pair ? 2 * KS : KS;
     const int layout = hilo ? 1 : 0;
-    auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu) -> int {
+    auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu, cudaStream_t ps) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         const int64_t s0 = k0 + kb;
@@ -1310,17 +1322,19 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             pa.Bpack = st->Bpack + off; pa.b_ld = KP; pa.b_c0 = q_s0 + NB;
             pa.a_lo = pa.b_lo = hilo ? 4 * NB : 0;
         } else {
+            // both packs double-buffered by step parity: an overlapped GEMM
+            // still reads step bk - 1's while these are written
             pa.Apack = st->Apack[bk & 1]; pa.a_ld = KS; pa.a_r0 = s0;
-            pa.Bpack = st->Bpack; pa.b_ld = KS; pa.b_c0 = s0;
+            pa.Bpack = st->Bpack + (bk & 1) * np * KS; pa.b_ld = KS; pa.b_c0 = s0;
             pa.a_lo = pa.b_lo = hilo ? 2 * NB : 0;
         }
         const int nupd = (kp1 >= 0) + (kp2 >= 0) + (kpu >= 0);
         cudaEvent_t ev;
-        ctx->prof.begin(stream, 4, 8.0 * NB * NB * (double)m * (2 + nupd), 8.0 * NB * (double)m * (4 + nupd), &ev);
-        panels_kernel<float2><<<(unsigned)(2 * pa.nL), 256, kSmemPanel, stream>>>(
+        ctx->prof.begin(ps, 4, 8.0 * NB * NB * (double)m * (2 + nupd), 8.0 * NB * (double)m * (4 + nupd), &ev);
+        panels_kernel<float2><<<(unsigned)(2 * pa.nL), 256, kSmemPanel, ps>>>(
             st->W, ldw, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB, pa);
         SIEB_NOTE_LAUNCH();
-        ctx->prof.end(stream, ev);
+        ctx->prof.end(ps, ev);
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     };
@@ -1354,8 +1368,17 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // GEMM runs at 360 TFLOP/s against 297, but the steps without a GEMM put
     // the panels and the diagonal block back to back and the extra updates
     // lengthen that chain, so the factorization takes longer overall.
+    //
+    // Overlapped steps (single-step schedule, trailing update at least
+    // st->ovl_min columns wide): the trailing GEMM skips the next block row
+    // as well and runs on all but st->ovl_sms SMs, the next panels take this
+    // step's update of that row themselves (kpu, as after an even pair step)
+    // and run on the side stream right after the next diagonal block, on the
+    // SMs the GEMM leaves free; so the panels leave the critical path while
+    // the GEMM is the longer of the two. The next GEMM waits for them (event).
     SIEB_RETURN_IF(diag_blk(0, -1, -1, stream));
-    SIEB_RETURN_IF(panels(0, -1, -1, -1));
+    SIEB_RETURN_IF(panels(0, -1, -1, -1, stream));
+    bool pan_side = false;  // the last panels ran on the side stream
     for (int64_t bk = 0; bk < nbl; ++bk) {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
@@ -1369,27 +1392,42 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
             SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
             SIEB_RETURN_IF(diag_blk(bk + 1, k0, kprev, st->side));
+            const bool ovl = !pair && st->ovl_min > 0 && m - n1 >= st->ovl_min && m > 2 * n1;
+            if (pan_side) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_pan, 0));  // GEMM operands
+            if (ovl) {
+                const int octas = std::max(1, std::min(gemm_ctas, ctx->sm_count - st->ovl_sms));
+                SIEB_RETURN_IF(gemm(s0 + n1, s0 + n1, m - n1, st->Apack[bk & 1] + 2 * n1 * KS,
+                                    st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, octas));
+                SIEB_RETURN_IF(panels(bk + 1, k0, -1, k0, st->side));
+                SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
+                pan_side = true;
+                continue;
+            }
+            pan_side = false;
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
             if (!pair) {
                 if (m > n1)
-                    SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1], st->Bpack + n1 * KS, (int)KS,
-                                        gemm_ctas));
+                    SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1],
+                                        st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, gemm_ctas));
             } else if (odd && m > n1) {
                 SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas));
             }
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
             // after an even step of the pair schedule the next block row
             // has not had this step's update yet
-            SIEB_RETURN_IF(panels(bk + 1, k0, kprev, pair && !odd ? k0 : -1));
+            SIEB_RETURN_IF(panels(bk + 1, k0, kprev, pair && !odd ? k0 : -1, stream));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             SIEB_RETURN_IF(diag_blk(bk + 1, -1, -1, stream));
-            SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1));
+            SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1, stream));
         }
     }
+    // Join the side stream (its last panels or diagonal block).
+    SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
+    SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_pan, 0));
     ctx->prof.end(stream, ev_fact);
     return SIEB200_OK;
 }
@@ -1772,6 +1810,7 @@ static int fp64_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side, cudaStreamNonBlocking, greatest));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_cols, cudaEventDisableTiming));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_pan, cudaEventDisableTiming));
     }
     static bool attrs64 = false;
     if (!attrs64) {

@@ -31,6 +31,8 @@ struct MixedState {
     int use_tc = 1;
     int hilo = 1;               // split [hi | lo] packs, three products per GEMM k-block
     int pair = 0;               // trailing update every second block step (K = 2 x 384)
+    int ovl_min = 0;            // overlap the next panels with GEMMs at least this wide (0: off)
+    int ovl_sms = 20;           // SMs the overlapped GEMMs leave to the panels
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
@@ -45,7 +47,7 @@ struct MixedState {
     float2* UinvH = nullptr;
     CUtensorMap tmWH;
     cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
-    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr;
+    cudaEvent_t ev_cols = nullptr, ev_diag = nullptr, ev_pan = nullptr;
     // The factorization's launches as one CUDA graph (both streams and the
     // event edges between them), captured on the second call with an
     // unchanged key and replayed while it stays so; not while the profiler
@@ -56,9 +58,10 @@ struct MixedState {
         const void* W = nullptr;
         const void* pack = nullptr;
         int use_tc = -1, sms = -1;
+        int64_t ovl = -1;
         bool operator==(const GraphKey& o) const {
             return A == o.A && lda == o.lda && n == o.n && W == o.W && pack == o.pack && use_tc == o.use_tc &&
-                   sms == o.sms;
+                   sms == o.sms && ovl == o.ovl;
         }
     };
     // Two graphs (for example one per buffer of a caller that uploads the

@@ -93,7 +93,7 @@ def _pmchwt(level=2, solver="lu_cusolver", rule=5):
 
 
 @pytest.mark.parametrize("trailing", ["tc", "tc_pair", "tc_three_product", "tc_load_store", "tc_reduce",
-                                      "simt"])
+                                      "tc_overlap", "simt"])
 def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
     import sieb200
     if trailing == "simt":
@@ -102,6 +102,8 @@ def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
         monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1")
     if trailing == "tc_three_product":
         monkeypatch.setenv("SIEB200_GEMM_HILO", "0")
+    if trailing == "tc_overlap":
+        monkeypatch.setenv("SIEB200_OVERLAP_MIN", "64")
     if trailing in ("tc_load_store", "tc_reduce"):
         monkeypatch.setenv("SIEB200_GEMM_MODE", "2" if trailing == "tc_load_store" else "3")
     m, o = _pmchwt(2)
@@ -161,19 +163,25 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
     s.close()
 
 
-@pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three"])
+@pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three",
+                                      "single_split_overlap"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
     sub-block, and fewer rows than one block, under both trailing-update
-    schedules (pair / single step) and both pack layouts (split [hi | lo] /
-    three-product). One preconditioned step must already reach 1e-5 (the
+    schedules (pair / single step), both pack layouts (split [hi | lo] /
+    three-product) and with overlapped steps (panels beside the GEMM). One
+    preconditioned step must already reach 1e-5 (the
     factors are single precision), and the full refinement 1e-12: a wrong
     triangular solve fails the first bound."""
     import torch
     import sieb200
     monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1" if schedule.startswith("pair") else "0")
-    monkeypatch.setenv("SIEB200_GEMM_HILO", "1" if schedule.endswith("split") else "0")
+    monkeypatch.setenv("SIEB200_GEMM_HILO", "0" if schedule.endswith("three") else "1")
+    # overlapped steps: every trailing update at least 64 columns wide skips
+    # the next block row, whose update the next panels take on the side stream
+    monkeypatch.setenv("SIEB200_OVERLAP_MIN", "64" if schedule.endswith("overlap") else "0")
+    monkeypatch.setenv("SIEB200_OVERLAP_SMS", "16")
     rng = np.random.default_rng(n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
