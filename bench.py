@@ -411,6 +411,12 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
     gemv = ctx.profile_read(2)
     prof = {name: ctx.profile_read(i) for i, name in
             [(3, "diag_lu"), (4, "panels"), (6, "factorization"), (7, "refined_solve")]}
+    # One more step with the per-launch timeline: the largest trailing update
+    # (block step 0) on its own, against its roofline.
+    ctx.profile(True, timeline=True)
+    step()
+    ctx.synchronize()
+    first_gemm = next(((a, b2) for k, a, b2 in sorted(ctx.profile_timeline(), key=lambda v: v[1]) if k == 0), None)
     ctx.profile(False)
 
     # Accuracy of the mixed solution against the FP64 matrix.
@@ -596,6 +602,7 @@ def measure(args, ctx, rank: int, world: int, local: int, barrier, max_over_rank
             # two phases of a step (spans on the launching streams)
             "mean_ms": {k: (v["ms"] / v["launches"] if v["launches"] else None)
                         for k, v in [("tf32_gemm", gemm), ("trsv", trsv), *prof.items()]},
+            "largest_launch": largest_launch_roofline(first_gemm, peaks, tf32_peak),
         }
         value = world * args.steps / t_mixed
         out = {
@@ -1045,6 +1052,24 @@ def adjoint_section(ctx, steps: int, max_over_ranks):
         "grad_rel_diff_vs_fp64": float((g_mx - g_64).norm() / g_64.norm()),
         "timing": "CUDA events around device-synchronized gradient evaluations",
     }
+
+
+def largest_launch_roofline(span, peaks, tf32_peak):
+    """The first trailing update of the N = 6016 factorization (block step
+    0: C = 2m x (m - 64) real with m = 5952, split packs 256 wide) from its
+    in-situ timeline span: time against max(bytes / HBM, flops / TF32)."""
+    if not span:
+        return None
+    np_, nb = 6016, 64
+    m = np_ - nb
+    rows, cols, k = 2 * m, m - nb, 256
+    alg_bytes = 4.0 * (2.0 * rows * cols + (rows + cols) * k)
+    flops = 2.0 * rows * cols * 384
+    t = (span[1] - span[0]) / 1e3
+    roof = max(alg_bytes / (peaks["hbm_gbs"] * 1e9), flops / (tf32_peak * 1e12))
+    return {"us": t * 1e6, "algorithmic_bytes": alg_bytes, "tf32_flops": flops, "roofline_us": roof * 1e6,
+            "frac_of_roofline": roof / t, "hbm_frac": alg_bytes / t / (peaks["hbm_gbs"] * 1e9),
+            "tensor_frac": flops / t / (tf32_peak * 1e12)}
 
 
 def timeline_summary(spans):
