@@ -666,6 +666,14 @@ constexpr int TR_CONSUMERS = 256;
 constexpr int TR_THREADS = TR_CONSUMERS + 32;
 constexpr int kSmemTrsv = 1024 + TR_STAGES * TR_TILE_BYTES + 2 * NB * TR_DLD * 8 +
                           (2 * TR_ROWS + 3 * NB) * (int)sizeof(cplx) + 2 * TR_STAGES * 8;
+// Stages of the tile ring for CTAs of `rows` rows (32 KB tiles of 128 rows,
+// 16 KB tiles of 64) and the shared memory of that variant.
+__host__ __device__ constexpr int tr_stages(int rows) { return rows == 2 * NB ? TR_STAGES : 8; }
+__host__ __device__ constexpr int trsv_smem(int rows) {
+    return 1024 + tr_stages(rows) * rows * TR_COLS * 8 + (rows / NB) * NB * TR_DLD * 8 +
+           ((TR_CONSUMERS / rows - 1) * rows + rows + 3 * NB) * (int)sizeof(cplx) + 2 * tr_stages(rows) * 8;
+}
+static_assert(trsv_smem(2 * NB) == kSmemTrsv, "128-row layout");
 
 __device__ __forceinline__ void consumer_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
@@ -678,21 +686,28 @@ __device__ __forceinline__ bool tr_wait(uint32_t bar, uint32_t parity, uint64_t 
     return true;
 }
 
+template <int ROWS>
 __global__ void __launch_bounds__(TR_THREADS, 1)
 trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, int lower,
                 const float2* __restrict__ Dinv, cplx* __restrict__ x, cplx* __restrict__ xpub,
                 unsigned* __restrict__ progress, unsigned* __restrict__ err, unsigned long long timeout_ns) {
+    constexpr int SUBS = ROWS / NB;                 // diagonal sub-blocks per CTA (1 or 2)
+    constexpr int HG = TR_CONSUMERS / ROWS;         // consumer threads per row
+    constexpr int CPT = TR_COLS / HG;               // tile columns per consumer thread
+    constexpr int STG = tr_stages(ROWS);
+    constexpr int TILE = ROWS * TR_COLS;            // float2 per tile
+    constexpr int TILE_BYTES = TILE * 8;
     extern __shared__ __align__(16) unsigned char dyn_smem[];  // aligned to 1024 below
     const uint32_t raw = smem_u32(dyn_smem);
     unsigned char* base = dyn_smem + (((raw + 1023u) & ~1023u) - raw);
     const uint32_t ring = smem_u32(base);
     const float2* ringp = reinterpret_cast<const float2*>(base);
-    float2* Ds = reinterpret_cast<float2*>(base + TR_STAGES * TR_TILE_BYTES);  // 2 x [NB cols][TR_DLD]
-    cplx* red = reinterpret_cast<cplx*>(Ds + 2 * NB * TR_DLD);                  // TR_ROWS
-    cplx* ys = red + TR_ROWS;                                                      // TR_ROWS
-    cplx* xs = ys + TR_ROWS;                                                       // NB
+    float2* Ds = reinterpret_cast<float2*>(base + STG * TILE_BYTES);  // SUBS x [NB cols][TR_DLD]
+    cplx* red = reinterpret_cast<cplx*>(Ds + SUBS * NB * TR_DLD);              // (HG - 1) x ROWS
+    cplx* ys = red + (HG - 1) * ROWS;                                           // ROWS
+    cplx* xs = ys + ROWS;                                                       // NB
     cplx* xstage = xs + NB;                                                        // 2 x NB
-    const uint32_t full0 = smem_u32(xstage + 2 * NB), empty0 = full0 + 8 * TR_STAGES;
+    const uint32_t full0 = smem_u32(xstage + 2 * NB), empty0 = full0 + 8 * STG;
     __shared__ int s_t, s_go;
     __shared__ volatile int s_abort;
 
@@ -700,7 +715,7 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     if (tid == 0) {
         s_t = (int)atomicAdd(&progress[1], 1u);
         s_abort = 0;
-        for (int st = 0; st < TR_STAGES; ++st) {
+        for (int st = 0; st < STG; ++st) {
             mbar_init(full0 + 8 * st, 1);
             mbar_init(empty0 + 8 * st, TR_CONSUMERS / 32);
         }
@@ -709,13 +724,13 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     }
     __syncthreads();
     const uint64_t deadline = global_ns() + timeout_ns;
-    const int ncta = (int)((np + TR_ROWS - 1) / TR_ROWS);
+    const int ncta = (int)((np + ROWS - 1) / ROWS);
     const int t = s_t;
     if (t >= ncta) return;  // block-uniform
     const int rb = lower ? t : ncta - 1 - t;
-    const int64_t R0 = (int64_t)rb * TR_ROWS;
-    const int sbA = 2 * rb, sbB = 2 * rb + 1;
-    const bool has_bot = sbB < nsb;
+    const int64_t R0 = (int64_t)rb * ROWS;
+    const int sbA = SUBS * rb, sbB = SUBS * rb + 1;
+    const bool has_bot = SUBS == 2 && sbB < nsb;
     // Streamed tiles: the off-diagonal ones in publication order, then the
     // two tiles holding the coupling block between the sub-blocks.
     const int ntile_all = (int)((np + TR_COLS - 1) / TR_COLS);
@@ -723,7 +738,7 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     if (lower) {
         n_off = (int)(R0 / TR_COLS);
     } else {
-        const int kmin = (int)((R0 + TR_ROWS) / TR_COLS);
+        const int kmin = (int)((R0 + ROWS) / TR_COLS);
         n_off = ntile_all > kmin ? ntile_all - kmin : 0;
     }
     const int n_tiles = n_off + (has_bot ? 2 : 0);
@@ -736,15 +751,15 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     if (warp == TR_CONSUMERS / 32) {  // producer
         if (lane == 0) {
             for (int i = 0; i < n_tiles; ++i) {
-                const int st = i % TR_STAGES;
-                const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
+                const int st = i % STG;
+                const uint32_t ph = (uint32_t)(i / STG) & 1u;
                 if (!tr_wait(empty0 + 8 * st, ph ^ 1u, deadline)) {
                     atomicCAS(err, 0u, 2u);
                     s_abort = 1;
                     break;
                 }
-                mbar_expect_tx(full0 + 8 * st, TR_TILE_BYTES);
-                tma_load_2d(ring + st * TR_TILE_BYTES, &tmW, full0 + 8 * st, (int)R0, tile_k(i) * TR_COLS);
+                mbar_expect_tx(full0 + 8 * st, TILE_BYTES);
+                tma_load_2d(ring + st * TILE_BYTES, &tmW, full0 + 8 * st, (int)R0, tile_k(i) * TR_COLS);
             }
         }
         return;
@@ -754,10 +769,11 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     for (int e = tid; e < NB * NB; e += TR_CONSUMERS) {
         const int r = e & (NB - 1), c = e >> 6;
         Ds[c * TR_DLD + r] = Dinv[(size_t)sbA * NB * NB + e];
-        Ds[(NB + c) * TR_DLD + r] = has_bot ? Dinv[(size_t)sbB * NB * NB + e] : make_float2(0.f, 0.f);
+        if (SUBS == 2)
+            Ds[(NB + c) * TR_DLD + r] = has_bot ? Dinv[(size_t)sbB * NB * NB + e] : make_float2(0.f, 0.f);
     }
-    // Thread (r, h): row r of the block, columns h*16 .. h*16+15 of a tile.
-    const int r = tid & (TR_ROWS - 1), h = tid >> 7;
+    // Thread (r, h): row r of the block, columns h*CPT .. h*CPT+CPT-1 of a tile.
+    const int r = tid & (ROWS - 1), h = tid / ROWS;
     const int64_t grow = R0 + r;
     cplx b = cx(0, 0);  // written only by this CTA: final from the start
     if (h == 0 && grow < np) b = cx(__ldcg(&x[grow].re), __ldcg(&x[grow].im));
@@ -802,8 +818,8 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
         }
         consumer_bar();
         for (int j = 0; j < cnt; ++j, ++i) {
-            const int st = i % TR_STAGES;
-            const uint32_t ph = (uint32_t)(i / TR_STAGES) & 1u;
+            const int st = i % STG;
+            const uint32_t ph = (uint32_t)(i / STG) & 1u;
             // Every issued tile is waited for and released, also after an
             // abort, so that no copy is in flight when the CTA exits.
             bool ok = !s_abort;
@@ -813,11 +829,11 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
                 ok = false;
             }
             if (ok) {
-                const float2* tile = ringp + st * TR_TILE;
-                const cplx* xt = xg + (tile_k(i) * TR_COLS - sb * NB) + h * 16;
+                const float2* tile = ringp + st * TILE;
+                const cplx* xt = xg + (tile_k(i) * TR_COLS - sb * NB) + h * CPT;
 #pragma unroll
-                for (int u = 0; u < 16; ++u) {
-                    const float2 w = tile[(h * 16 + u) * TR_ROWS + r];
+                for (int u = 0; u < CPT; ++u) {
+                    const float2 w = tile[(h * CPT + u) * ROWS + r];
                     const cplx xv = xt[u];
                     acc_re += (double)w.x * xv.re - (double)w.y * xv.im;
                     acc_im += (double)w.x * xv.im + (double)w.y * xv.re;
@@ -827,9 +843,16 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
             if (lane == 0) mbar_arrive(empty0 + 8 * st);
         }
     }
-    if (h == 1) red[r] = cx(acc_re, acc_im);
+    if (h >= 1) red[(h - 1) * ROWS + r] = cx(acc_re, acc_im);
     consumer_bar();
-    if (h == 0) ys[r] = cx(b.re - acc_re - red[r].re, b.im - acc_im - red[r].im);
+    if (h == 0) {
+#pragma unroll
+        for (int g2 = 0; g2 < HG - 1; ++g2) {
+            acc_re += red[g2 * ROWS + r].re;
+            acc_im += red[g2 * ROWS + r].im;
+        }
+        ys[r] = cx(b.re - acc_re, b.im - acc_im);
+    }
     if (tid == 0) s_go = !s_abort;
     consumer_bar();
     if (!s_go) return;  // block-uniform
@@ -877,7 +900,7 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     bool ok = true;
     for (int j = 0; j < 2; ++j) {
         const int i = n_off + j;
-        ok = tr_wait(full0 + 8 * (i % TR_STAGES), (uint32_t)(i / TR_STAGES) & 1u, deadline) && ok;
+        ok = tr_wait(full0 + 8 * (i % STG), (uint32_t)(i / STG) & 1u, deadline) && ok;
     }
     if (!ok && tid == 0) atomicCAS(err, 0u, 2u);
     const int roff = second * NB;
@@ -886,8 +909,8 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
 #pragma unroll
         for (int u = 0; u < NB / 4; ++u) {
             const int c = part + 4 * u;
-            const float2* tile = ringp + ((n_off + (c >> 5)) % TR_STAGES) * TR_TILE;
-            const float2 w = tile[(c & 31) * TR_ROWS + roff + dr];
+            const float2* tile = ringp + ((n_off + (c >> 5)) % STG) * TILE;
+            const float2 w = tile[(c & 31) * ROWS + roff + dr];
             const cplx xv = xs[c];
             re += (double)w.x * xv.re - (double)w.y * xv.im;
             im += (double)w.x * xv.im + (double)w.y * xv.re;
@@ -1478,11 +1501,21 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     SIEB_TRY_CUDA(cudaGetLastError());
     unsigned* fl = st->tri_flags;
     const int nbl = (int)st->nbl;
+    // Rows per triangular-solve CTA: 128 (two 64-row sub-blocks and their
+    // coupling tiles) or 64 (SIEB200_TRSV_ROWS=64: one sub-block, twice the
+    // CTAs, each hop one sub-block).
+    const char* rows_env = getenv("SIEB200_TRSV_ROWS");
+    const int rows = (rows_env && atoi(rows_env) == 64) ? NB : TR_ROWS;
+    if (st->tm_rows != rows) {
+        st->tm_base = nullptr;
+        st->adj_ready = false;
+        st->tm_rows = rows;
+    }
     if (st->tm_base != st->W || st->tm_np != np) {
         // W as 8-byte elements: rows inner, 128 x 32 boxes; rows/columns
         // beyond np read as zero.
         SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmW, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->W, (uint64_t)np,
-                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
+                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), (uint32_t)rows,
                                             TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
         st->tm_base = st->W;
         st->tm_np = np;
@@ -1507,17 +1540,19 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         SIEB_RETURN_IF(encode_tensor_map_2d(&st->tmWH, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, st->WH, (uint64_t)np,
-                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), TR_ROWS,
+                                            (uint64_t)np, (uint64_t)st->ldw * sizeof(float2), (uint32_t)rows,
                                             TR_COLS, CU_TENSOR_MAP_SWIZZLE_NONE));
         st->adj_ready = true;
     }
     static bool attr_set = false;
     if (!attr_set) {
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemTrsv));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel<TR_ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           trsv_smem(TR_ROWS)));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           trsv_smem(NB)));
         attr_set = true;
     }
-    const unsigned ncta = (unsigned)((np + TR_ROWS - 1) / TR_ROWS);
+    const unsigned ncta = (unsigned)((np + rows - 1) / rows);
     const unsigned long long timeout_ns = 2000000000ull;
     // algorithmic bytes: the triangle of c64 factors plus the diagonal inverses
     const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
@@ -1529,8 +1564,12 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
         SIEB_TRY_CUDA(cudaMemsetAsync(xpub, 0xFF, sizeof(cplx) * (size_t)np, stream));
         cudaEvent_t ev;
         s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
-        trsv_tma_kernel<<<ncta, TR_THREADS, kSmemTrsv, stream>>>(adjoint ? st->tmWH : st->tmW, np, nbl, lower,
-                                                                 dinv, work, xpub, fl, st->err, timeout_ns);
+        if (rows == NB)
+            trsv_tma_kernel<NB><<<ncta, TR_THREADS, trsv_smem(NB), stream>>>(
+                adjoint ? st->tmWH : st->tmW, np, nbl, lower, dinv, work, xpub, fl, st->err, timeout_ns);
+        else
+            trsv_tma_kernel<TR_ROWS><<<ncta, TR_THREADS, trsv_smem(TR_ROWS), stream>>>(
+                adjoint ? st->tmWH : st->tmW, np, nbl, lower, dinv, work, xpub, fl, st->err, timeout_ns);
         SIEB_NOTE_LAUNCH();
         s->ctx->prof.end(stream, ev);
         SIEB_TRY_CUDA(cudaGetLastError());

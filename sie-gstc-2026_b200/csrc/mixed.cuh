@@ -36,6 +36,7 @@ struct MixedState {
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
+    int tm_rows = 0;                       // rows per box of tmW / tmWH
     int64_t tm_np = 0;
     // Conjugate-transpose solves (W^H = U^H L^H): W^H and the conjugate
     // transposes of the diagonal-block inverses, built on first use after a

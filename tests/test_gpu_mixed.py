@@ -164,14 +164,14 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
 
 
 @pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three",
-                                      "single_split_overlap"])
+                                      "single_split_overlap", "single_split_trsv64"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
     sub-block, and fewer rows than one block, under both trailing-update
     schedules (pair / single step), both pack layouts (split [hi | lo] /
-    three-product) and with overlapped steps (panels beside the GEMM). One
-    preconditioned step must already reach 1e-5 (the
+    three-product), with overlapped steps (panels beside the GEMM) and with
+    64-row triangular-solve CTAs. One preconditioned step must already reach 1e-5 (the
     factors are single precision), and the full refinement 1e-12: a wrong
     triangular solve fails the first bound."""
     import torch
@@ -182,6 +182,8 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     # the next block row, whose update the next panels take on the side stream
     monkeypatch.setenv("SIEB200_OVERLAP_MIN", "64" if schedule.endswith("overlap") else "0")
     monkeypatch.setenv("SIEB200_OVERLAP_SMS", "16")
+    # triangular solves with 64-row CTAs (one sub-block each) or 128-row ones
+    monkeypatch.setenv("SIEB200_TRSV_ROWS", "64" if schedule.endswith("trsv64") else "128")
     rng = np.random.default_rng(n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
@@ -204,12 +206,15 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     s.close()
 
 
+@pytest.mark.parametrize("rows", ["128", "64"])
 @pytest.mark.parametrize("n", [5, 129, 300, 1000])
-def test_mixed_adjoint_solve(n, gpu_ctx):
+def test_mixed_adjoint_solve(n, rows, gpu_ctx, monkeypatch):
     """Conjugate-transpose solve A^H x = b with the mixed factors: one
-    preconditioned step reaches 1e-5, the refinement 1e-12, as for A x = b."""
+    preconditioned step reaches 1e-5, the refinement 1e-12, as for A x = b
+    (triangular solves with 128- and 64-row CTAs)."""
     import torch
     import sieb200
+    monkeypatch.setenv("SIEB200_TRSV_ROWS", rows)
     rng = np.random.default_rng(100 + n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     A[0, n - 1] += 5.0  # make A far from Hermitian
