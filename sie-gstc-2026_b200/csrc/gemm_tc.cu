@@ -432,16 +432,22 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
                         tma_store_2d(&tmC, sC + c * CHUNK_BYTES, x, y);
                     }
                     bulk_commit();
-                    bulk_wait_read_all();  // the slot is free once the store has read it
+                    if (REDUCE)
+                        // the slot written next was last reduced CH - 1 groups
+                        // ago: only that read has to be complete
+                        bulk_wait_read<CH - 1>();
+                    else
+                        bulk_wait_read_all();  // the slot is reloaded at once
                     if (!REDUCE && tn < tiles) {
                         mbar_expect_tx(cfull0 + 8 * c, CHUNK_BYTES);
                         tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (tn % mt) * BM,
                                     (tn / mt) * BN + c * CC);
                     }
                 }
-                // REDUCE: the slot is rewritten (next tile) only after its
-                // reduction has read it. Otherwise the next tile's writes
-                // wait for the slot's new load (cfull), issued after the read.
+                // REDUCE: the next slot is written only after its previous
+                // reduction has read it (the wait above). Otherwise the next
+                // tile's writes wait for the slot's new load (cfull), issued
+                // after the read.
                 if (REDUCE) epilogue_bar();
             }
         }
