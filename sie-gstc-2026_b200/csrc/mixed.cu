@@ -788,32 +788,32 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
         const int cnt = (i + 1 < n_off && (tile_k(i + 1) * TR_COLS) / NB == sb) ? 2 : 1;
         cplx* xg = xstage + (g & 1) * NB;
         if (warp == 0) {
-            // Each lane polls its entries of the sub-block in the publication
-            // buffer: the value is the flag, one L2 round trip per entry.
+            // Each lane polls its two entries of the sub-block (lane, lane +
+            // 32) in the publication buffer, both in every round: the value is
+            // the flag, one L2 round trip per round for all 64 entries.
+            static_assert(NB == 64, "two entries per lane");
+            const int64_t c0 = (int64_t)sb * NB + lane, c1 = c0 + 32;
+            bool need0 = c0 < np, need1 = c1 < np;
+            cplx v0 = cx(0, 0), v1 = cx(0, 0);
             bool okp = !s_abort;
-            for (int e = lane; e < NB; e += 32) {
-                const int64_t c = (int64_t)sb * NB + e;
-                cplx v = cx(0, 0);
-                if (okp && c < np) {
-                    int it = 0;
-                    while (true) {
-                        const double vr = ld_relaxed_f64(&xpub[c].re), vi = ld_relaxed_f64(&xpub[c].im);
-                        if (!unpublished(vr) && !unpublished(vi)) {
-                            v = cx(vr, vi);
-                            break;
-                        }
-                        if (++it > 16) __nanosleep(64);
-                        if ((it & 63) == 0 &&
-                            (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
-                            atomicCAS(err, 0u, 2u);
-                            s_abort = 1;
-                            okp = false;
-                            break;
-                        }
-                    }
+            int it = 0;
+            while (okp && (need0 || need1)) {
+                double r0 = 0, i0 = 0, r1 = 0, i1 = 0;
+                if (need0) { r0 = ld_relaxed_f64(&xpub[c0].re); i0 = ld_relaxed_f64(&xpub[c0].im); }
+                if (need1) { r1 = ld_relaxed_f64(&xpub[c1].re); i1 = ld_relaxed_f64(&xpub[c1].im); }
+                if (need0 && !unpublished(r0) && !unpublished(i0)) { v0 = cx(r0, i0); need0 = false; }
+                if (need1 && !unpublished(r1) && !unpublished(i1)) { v1 = cx(r1, i1); need1 = false; }
+                if (!need0 && !need1) break;
+                if (++it > 16) __nanosleep(64);
+                if ((it & 63) == 0 &&
+                    (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
+                    atomicCAS(err, 0u, 2u);
+                    s_abort = 1;
+                    okp = false;
                 }
-                xg[e] = v;
             }
+            xg[lane] = v0;
+            xg[lane + 32] = v1;
             __syncwarp();
         }
         consumer_bar();
