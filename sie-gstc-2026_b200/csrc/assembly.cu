@@ -354,6 +354,183 @@ pair_regular_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp
     }
 }
 
+// The same double quadrature with a test point held per lane. Lane l works
+// on test point p (G lanes per point when Q < 32, each taking every G-th
+// source point) and sums over its source points only the moments that do not
+// carry p: per wavenumber S0_p = sum w_q G, Sq_p = sum w_q G q, and for TK
+// T0_p = sum w_q g, Tq_p = sum w_q g q (8 complex for both). The moments
+// with p are folded in once per point,
+//   S0 += w_p S0_p,  Sp += w_p S0_p p,  Sq += w_p Sq_p,  Spq += w_p p.Sq_p,
+//   T0 += w_p T0_p,  Tp += w_p T0_p p,  Tq += w_p Tq_p,  Tpq += w_p p x Tq_p,
+// reduced over the warp and accumulated in shared memory. Per point pair and
+// wavenumber that is 20 FP64 accumulation instructions instead of 40 and no
+// p.q or p x q, and the accumulators fit in half the registers (two CTAs per
+// SM). Each moment is the same sum as in pair_regular_kernel in another
+// order.
+template <int NK, bool TK>
+__global__ void __launch_bounds__(kWarps * 32, 2)
+pair_regular_pq_kernel(const FaceGeom* __restrict__ geom, const d3* __restrict__ qp,
+                       const float* __restrict__ qw_g, int Q, int nf, int m0, double k0, double k1,
+                       float thr, cplx* __restrict__ pairs) {
+    constexpr int NB = TK ? 2 * NK : NK;
+    constexpr int NM = TK ? 18 : 8;  // complex moments per wavenumber
+    __shared__ d3 s_tp[kMaxQ], s_tl[kMaxQ];
+    __shared__ double s_w[kMaxQ];
+    __shared__ d3 s_sp[kWarps][kMaxQ], s_sl[kWarps][kMaxQ];
+    __shared__ cplx s_tot[kWarps][NK * NM];
+
+    const int m = m0 + blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const FaceGeom& gm = geom[m];
+    const d3 cm = gm.c;
+    for (int t = threadIdx.x; t < Q; t += blockDim.x) {
+        const d3 r = qp[(size_t)m * Q + t];
+        s_tp[t] = r;
+        s_tl[t] = r - cm;
+        s_w[t] = (double)qw_g[t];
+    }
+    __syncthreads();
+    const double kk[2] = {k0, k1};
+    const int G = Q >= 32 ? 1 : 32 / Q;  // lanes per test point
+    const int PL = 32 / G;               // test points per round
+    const int lp = lane / G, lq = lane - (lane / G) * G;
+    cplx* tot = s_tot[warp];
+
+    for (int n = warp; n < nf; n += kWarps) {
+        const FaceGeom& gn = geom[n];
+        const d3 cn = gn.c;
+        for (int t = lane; t < Q; t += 32) {
+            const d3 r = ldg3(&qp[(size_t)n * Q + t]);
+            s_sp[warp][t] = r;
+            s_sl[warp][t] = r - cn;
+        }
+        for (int t = lane; t < NK * NM; t += 32) tot[t] = cx(0, 0);
+        __syncwarp();
+        const bool regular = centroid_distance(gm, gn) < thr;  // warp-uniform
+        const bool coinc = gm.idx[0] == gn.idx[0] && gm.idx[1] == gn.idx[1] &&
+                           gm.idx[2] == gn.idx[2];
+
+        for (int p0 = 0; p0 < Q; p0 += PL) {
+            const int p = p0 + lp;
+            const bool act = p < Q;
+            cplx S0[NK], Sq[NK][3], T0[TK ? NK : 1], Tq[TK ? NK : 1][3];
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                S0[a] = cx(0, 0);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) Sq[a][c] = cx(0, 0);
+                if (TK) {
+                    T0[a] = cx(0, 0);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) Tq[a][c] = cx(0, 0);
+                }
+            }
+            if (act) {
+                const d3 rp = s_tp[p];
+                for (int q = lq; q < Q; q += G) {
+                    const d3 rq = s_sp[warp][q], ql = s_sl[warp][q];
+                    const double wq = s_w[q];
+                    const d3 Rv = rp - rq;
+                    const double R = sqrt(Rv.x * Rv.x + Rv.y * Rv.y + Rv.z * Rv.z);
+                    cplx Gk[NK], gk[NK];
+                    if (!regular) {
+                        if (R < 1e-12) continue;
+                        const double inv_R = 1.0 / R;
+                        const double i4pR = 1.0 / (4.0 * kPi * R);
+#pragma unroll
+                        for (int a = 0; a < NK; ++a) green_std(R, inv_R, i4pR, kk[a], Gk[a], gk[a]);
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < NK; ++a) green_reg(R, kk[a], Gk[a], gk[a]);
+                    }
+#pragma unroll
+                    for (int a = 0; a < NK; ++a) {
+                        const cplx Gw = Gk[a] * wq;
+                        S0[a] += Gw;
+                        Sq[a][0] += Gw * ql.x; Sq[a][1] += Gw * ql.y; Sq[a][2] += Gw * ql.z;
+                        if (TK) {
+                            const cplx gw = gk[a] * wq;
+                            T0[a] += gw;
+                            Tq[a][0] += gw * ql.x; Tq[a][1] += gw * ql.y; Tq[a][2] += gw * ql.z;
+                        }
+                    }
+                }
+            }
+            // Fold the test point in, reduce over the warp, accumulate.
+            const d3 pl = act ? s_tl[p] : mk3(0, 0, 0);
+            const double wp = act ? s_w[p] : 0.0;
+            auto put = [&](int idx, cplx v) {
+                warp_sum(v);
+                if (lane == 0) tot[idx] += v;
+            };
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                const int b0 = a * NM;
+                const cplx s0 = S0[a] * wp;
+                const cplx sq[3] = {Sq[a][0] * wp, Sq[a][1] * wp, Sq[a][2] * wp};
+                put(b0 + 0, s0);
+                put(b0 + 1, s0 * pl.x); put(b0 + 2, s0 * pl.y); put(b0 + 3, s0 * pl.z);
+                put(b0 + 4, sq[0]); put(b0 + 5, sq[1]); put(b0 + 6, sq[2]);
+                put(b0 + 7, sq[0] * pl.x + sq[1] * pl.y + sq[2] * pl.z);
+                if (TK) {
+                    const cplx t0 = T0[a] * wp;
+                    const cplx tq[3] = {Tq[a][0] * wp, Tq[a][1] * wp, Tq[a][2] * wp};
+                    put(b0 + 8, t0);
+                    put(b0 + 9, t0 * pl.x); put(b0 + 10, t0 * pl.y); put(b0 + 11, t0 * pl.z);
+                    put(b0 + 12, tq[0]); put(b0 + 13, tq[1]); put(b0 + 14, tq[2]);
+                    // p x Tq
+                    put(b0 + 15, tq[2] * pl.y - tq[1] * pl.z);
+                    put(b0 + 16, tq[0] * pl.z - tq[2] * pl.x);
+                    put(b0 + 17, tq[1] * pl.x - tq[0] * pl.y);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < 9) {
+            const int j = lane / 3, i = lane - 3 * j;
+            const d3 A = gm.A[j], B = gn.A[i];
+            const d3 d = gm.fv[j] - gn.fv[i];
+            const double scale = gm.len[j] * gn.len[i];
+            const double AB = dot3(A, B);
+            cplx* out = pairs + ((size_t)blockIdx.x * nf + n) * (NB * 9);
+#pragma unroll
+            for (int a = 0; a < NK; ++a) {
+                const cplx* M = tot + a * NM;
+                // TL_ji = l_j l_i [ 1/4 (Spq - Sp.B - A.Sq + (A.B) S0) - S0 / k^2 ]
+                cplx t = M[7];
+                t = t - (M[1] * B.x + M[2] * B.y + M[3] * B.z);
+                t = t - (M[4] * A.x + M[5] * A.y + M[6] * A.z);
+                t += M[0] * AB;
+                out[a * 9 + lane] = (t * 0.25 - M[0] * (1.0 / (kk[a] * kk[a]))) * scale;
+                if (TK) {
+                    cplx tk = cx(0, 0);
+                    if (!coinc) {
+                        const d3 BxD = cross3(B, d);
+                        const d3 DxA = cross3(d, A);
+                        const double axbd = dot3(cross3(A, B), d);
+                        cplx u = M[15] * d.x + M[16] * d.y + M[17] * d.z;
+                        u = u - (M[9] * BxD.x + M[10] * BxD.y + M[11] * BxD.z);
+                        u = u - (M[12] * DxA.x + M[13] * DxA.y + M[14] * DxA.z);
+                        u += M[8] * axbd;
+                        tk = u * (0.25 * scale);
+                    }
+                    out[(NK + a) * 9 + lane] = tk;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Lane slots used by pair_regular_pq_kernel for Q points: its lanes do useful
+// work for this share of their iterations (1 for the flat kernel's Q x Q
+// index space up to the last partial round).
+inline double pq_lane_use(int Q) {
+    const int G = Q >= 32 ? 1 : 32 / Q, PL = 32 / G;
+    const int rounds = (Q + PL - 1) / PL, iters = (Q + G - 1) / G;
+    return (double)Q * Q / (32.0 * rounds * iters);
+}
+
 // ------------------------------------------------------------ Wilton ----
 struct Pots {
     double phi0, phi2, d;
@@ -1487,6 +1664,11 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
     // geometry twice), so the default is one CTA per face over both.
     const char* split_env = getenv("SIEB200_ASM_SPLIT");
     const bool split_wavenumbers = split_env && split_env[0] == '1';
+    // Test point per lane (pair_regular_pq_kernel) where its lanes stay busy
+    // (>= 75 % of their iterations); SIEB200_ASM_PER_POINT=0 keeps the flat
+    // point-pair kernel everywhere.
+    const char* pp_env = getenv("SIEB200_ASM_PER_POINT");
+    const bool per_point = !(pp_env && pp_env[0] == '0') && pq_lane_use(Q) >= 0.75;
     for (int m0 = 0; m0 < nf; m0 += slab) {
         const int m1 = std::min(nf, m0 + slab);
         const int rows = m1 - m0;
@@ -1505,11 +1687,17 @@ static int assemble_or_apply(sieb200_ctx* ctx, const sieb200_mesh& mesh, const s
         else if (variant != 0)
             pair_regular_n_kernel<2, true, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, exact, pairs);
+        else if (opt.formulation == SIEB200_PEC_EFIE && per_point)
+            pair_regular_pq_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, pairs);
         else if (opt.formulation == SIEB200_PEC_EFIE)
             pair_regular_kernel<1, false><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[1], ap.k[1], ap.threshold, pairs);
         else if (split_wavenumbers)
             pair_regular_kernel<2, true, true><<<dim3(rows, 2), kWarps * 32, 0, st>>>(
+                geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
+        else if (per_point)
+            pair_regular_pq_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(
                 geom, qp, dw, Q, nf, m0, ap.k[0], ap.k[1], ap.threshold, pairs);
         else
             pair_regular_kernel<2, true><<<rows, kWarps * 32, 0, st>>>(

@@ -55,10 +55,16 @@ def test_assembly_matches_reference_golden(name, golden, gpu_ctx, mesh_l0):
     assert rel_err(b, golden[f"b_{name}_L0"]) < Z_TOL
 
 
+@pytest.mark.parametrize("kernel", ["per_point", "flat"])
 @pytest.mark.parametrize("kind,rule,thr,level", [
-    (0, 7, 0.1, 2), (0, 5, 0.35, 1), (1, 17, 0.1, 1), (1, 4, 0.3, 1), (2, 5, 0.3, 1), (2, 17, 0.1, 1)])
-def test_assembly_matches_oracle(kind, rule, thr, level, gpu_ctx, oracle_lib):
+    (0, 7, 0.1, 2), (0, 5, 0.35, 1), (1, 17, 0.1, 1), (1, 4, 0.3, 1), (2, 5, 0.3, 1), (2, 17, 0.1, 1),
+    (1, 8, 0.1, 1), (0, 20, 0.2, 1)])
+def test_assembly_matches_oracle(kind, rule, thr, level, kernel, gpu_ctx, oracle_lib, monkeypatch):
+    """Both regular-pass kernels (a test point per lane where its lanes stay
+    busy, or the flat point-pair kernel: SIEB200_ASM_PER_POINT=0) against the
+    oracle's assembly."""
     import sieb200
+    monkeypatch.setenv("SIEB200_ASM_PER_POINT", "1" if kernel == "per_point" else "0")
     m = sieb200.icosphere(0.5, level)
     eps = (4.0, 1.0) if kind == 1 else (2.5, 1.0)
     freq = 2 * C0 if kind == 2 else C0
