@@ -1153,6 +1153,9 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3);
 // Overlapped block steps (see mixed_enqueue): trailing updates at least this
 // many columns wide (0: none), and the SMs they leave to the panels.
 constexpr int kOverlapMinDefault = 0;
+// Pair schedule for block steps whose paired GEMM is at least this wide (0:
+// none, unless SIEB200_PAIR_UPDATE=1 makes every step a pair step).
+constexpr int kPairMinDefault = 0;
 constexpr int kOverlapSmsDefault = 20;
 
 static int fp64_factorize(DenseSolver* s);
@@ -1178,6 +1181,8 @@ int mixed_factorize(DenseSolver* s) {
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
     const char* pair_env = getenv("SIEB200_PAIR_UPDATE");
     st->pair = (pair_env && pair_env[0] == '1') ? 1 : 0;
+    const char* pmin_env = getenv("SIEB200_PAIR_MIN");
+    st->pair_min = pmin_env ? std::max(0, atoi(pmin_env)) : kPairMinDefault;
     const char* hilo_env = getenv("SIEB200_GEMM_HILO");
     st->hilo = (hilo_env && hilo_env[0] == '0') ? 0 : 1;
     const char* ovl_env = getenv("SIEB200_OVERLAP_MIN");
@@ -1230,7 +1235,7 @@ int mixed_factorize(DenseSolver* s) {
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
     key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo; key.sms = gemm_sms;
-    key.ovl = st->ovl_min * 1000 + st->ovl_sms;
+    key.ovl = ((int64_t)st->pair_min << 32) | (int64_t)(st->ovl_min * 1000 + st->ovl_sms);
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -1321,10 +1326,22 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // Split layout (hilo): a step's pack is [hi | lo], 2 x 2NB = 256 wide,
     // and the GEMM forms the three products from it; in the pair schedule
     // the two steps' hi parts come first, then their lo parts.
-    const bool pair = st->use_tc && st->pair;
+    // Block step bk runs the pair schedule when SIEB200_PAIR_UPDATE=1, or
+    // when the GEMM of its pair (at the odd step bk | 1) is at least
+    // st->pair_min columns wide: the early, wide updates of a large system,
+    // where the GEMM rather than the chain sets the pace; both steps of a
+    // pair decide alike, and once a pair is too narrow every later one is.
+    auto pair_at = [&](int64_t bk) -> bool {
+        if (!st->use_tc) return false;
+        if (st->pair) return true;
+        if (st->pair_min <= 0) return false;
+        const int64_t q = bk | 1;
+        const int64_t mq = np - std::min(np, (q + 1) * NB);  // rows below block q
+        return mq - NB >= st->pair_min;
+    };
     const bool hilo = st->hilo != 0;
     const int64_t KS = hilo ? 4 * NB : K3;  // pack width of one step
-    const int64_t KP = pair ? 2 * KS : KS;
+    const int64_t KP = 2 * KS;              // pack width of a pair
     const int layout = hilo ? 1 : 0;
     auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu, cudaStream_t ps) -> int {
         const int64_t k0 = bk * NB;
@@ -1337,7 +1354,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         pa.nL = (int)blocks_for(m, 32);
         pa.pack = st->use_tc;
         pa.kp[0] = kp1; pa.kp[1] = kp2; pa.kpu = kpu;
-        if (pair) {
+        if (pair_at(bk)) {
             const int half = (int)(bk & 1);
             const int64_t q_s0 = half ? s0 : s0 + NB;  // s0 of the step whose GEMM uses this pack
             const int64_t off = half * (hilo ? 2 * NB : K3);
@@ -1410,6 +1427,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         const int64_t m = np - s0;
         if (st->use_tc) {
             const int64_t n1 = std::min<int64_t>(NB, m);  // the next block's columns
+            const bool pair = pair_at(bk);
             const bool odd = pair && (bk & 1);
             const int64_t kprev = odd ? k0 - NB : -1;      // the first step of the pair
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));

@@ -31,6 +31,7 @@ struct MixedState {
     int use_tc = 1;
     int hilo = 1;               // split [hi | lo] packs, three products per GEMM k-block
     int pair = 0;               // trailing update every second block step (K = 2 x 384)
+    int pair_min = 0;           // pair schedule for steps whose paired GEMM is at least this wide
     int ovl_min = 0;            // overlap the next panels with GEMMs at least this wide (0: off)
     int ovl_sms = 20;           // SMs the overlapped GEMMs leave to the panels
     GemmTC* gemm = nullptr;

@@ -164,19 +164,23 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
 
 
 @pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three",
-                                      "single_split_overlap", "single_split_trsv64"])
+                                      "single_split_overlap", "single_split_trsv64", "pair_then_single"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
     sub-block, and fewer rows than one block, under both trailing-update
     schedules (pair / single step), both pack layouts (split [hi | lo] /
-    three-product), with overlapped steps (panels beside the GEMM) and with
-    64-row triangular-solve CTAs. One preconditioned step must already reach 1e-5 (the
+    three-product), with overlapped steps (panels beside the GEMM), with
+    64-row triangular-solve CTAs, and switching from the pair to the single
+    schedule part way. One preconditioned step must already reach 1e-5 (the
     factors are single precision), and the full refinement 1e-12: a wrong
     triangular solve fails the first bound."""
     import torch
     import sieb200
-    monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1" if schedule.startswith("pair") else "0")
+    monkeypatch.setenv("SIEB200_PAIR_UPDATE", "1" if schedule.startswith("pair_") and schedule != "pair_then_single"
+                       else "0")
+    # pair steps while the paired update is at least 128 columns wide, single steps after
+    monkeypatch.setenv("SIEB200_PAIR_MIN", "128" if schedule == "pair_then_single" else "0")
     monkeypatch.setenv("SIEB200_GEMM_HILO", "0" if schedule.endswith("three") else "1")
     # overlapped steps: every trailing update at least 64 columns wide skips
     # the next block row, whose update the next panels take on the side stream
