@@ -60,6 +60,8 @@ struct BlockSolveState {
     Key graph_key, seen_key;
     cudaGraphExec_t graph = nullptr;
     long long graph_launches = 0;
+    // lookahead triangular solves: side-stream fork/join and per-step events
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_x[2] = {nullptr, nullptr}, ev_b[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -164,12 +166,23 @@ __global__ void rbt_block_N_kernel(const float2* __restrict__ Y, int64_t ldy, in
 // into Y and packed as the GEMM's B operand: column j of Xpack is
 // [Re, Im] per row, split [hi | lo | hi] along K. Rows beyond the block's
 // width are zero in Xpack (the inverse is padded with the identity).
+// With Fb != null the block first takes the previous step's update itself,
+// Y_k -= F X_prev (F the 64 x 64 factor block between the two, column-major
+// with leading dimension ldf; X_prev the previous block's solved rows of Y,
+// kbp of them): the trailing GEMM of the previous step skips this block, so
+// that this kernel and that GEMM run side by side.
 constexpr int DA_COLS = 16;
+constexpr int kSmemDiagApply = (2 * NB * (NB + 1) + 2 * DA_COLS * NB) * (int)sizeof(float2);
 __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y, int64_t ldy, int64_t k0, int kb,
                                                          int nrhs, const float2* __restrict__ Inv,
-                                                         float* __restrict__ Xpack) {
-    __shared__ float2 inv[NB][NB + 1];  // [row][col]
-    __shared__ float2 ys[DA_COLS][NB];
+                                                         float* __restrict__ Xpack,
+                                                         const float2* __restrict__ Fb, int64_t ldf,
+                                                         const float2* __restrict__ Xprev, int kbp) {
+    extern __shared__ __align__(16) float2 da_smem[];
+    float2(*inv)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(da_smem);              // [row][col]
+    float2(*fb)[NB + 1] = inv + NB;                                                    // [row][col]
+    float2(*ys)[NB] = reinterpret_cast<float2(*)[NB]>(da_smem + 2 * NB * (NB + 1));   // [col][row]
+    float2(*xp)[NB] = ys + DA_COLS;                                                    // [col][row]
     const int tid = threadIdx.x;
     const int c0 = blockIdx.x * DA_COLS;
     for (int e = tid; e < NB * NB; e += blockDim.x) inv[e % NB][e / NB] = Inv[e];  // Inv[r + c NB]
@@ -177,9 +190,38 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
         const int r = e % NB, c = e / NB;
         ys[c][r] = (c0 + c < nrhs && r < kb) ? Y[(k0 + r) + (int64_t)(c0 + c) * ldy] : make_float2(0.f, 0.f);
     }
+    if (Fb) {
+        for (int e = tid; e < NB * NB; e += blockDim.x) {
+            const int r = e % NB, c = e / NB;
+            fb[r][c] = (r < kb && c < kbp) ? Fb[r + (int64_t)c * ldf] : make_float2(0.f, 0.f);
+        }
+        for (int e = tid; e < DA_COLS * NB; e += blockDim.x) {
+            const int r = e % NB, c = e / NB;
+            xp[c][r] = (c0 + c < nrhs && r < kbp) ? Xprev[r + (int64_t)(c0 + c) * ldy] : make_float2(0.f, 0.f);
+        }
+    }
     __syncthreads();
     const int c = tid / 16;         // column of this thread
     const int r0 = (tid % 16) * 4;  // its four rows
+    if (Fb) {
+        double fr[4] = {0, 0, 0, 0}, fi[4] = {0, 0, 0, 0};
+        for (int kk = 0; kk < NB; ++kk) {
+            const float2 x = xp[c][kk];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float2 a = fb[r0 + u][kk];
+                fr[u] += (double)a.x * x.x - (double)a.y * x.y;
+                fi[u] += (double)a.x * x.y + (double)a.y * x.x;
+            }
+        }
+        // each thread owns rows r0 .. r0+3 of column c of ys
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float2 y = ys[c][r0 + u];
+            ys[c][r0 + u] = make_float2((float)((double)y.x - fr[u]), (float)((double)y.y - fi[u]));
+        }
+        __syncthreads();
+    }
     double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
     for (int kk = 0; kk < NB; ++kk) {
         const float2 y = ys[c][kk];
@@ -564,7 +606,10 @@ int zgemm_device(cudaStream_t stream, int64_t m, int64_t nc, int64_t kdim, const
 
 void block_solve_release(MixedState* st) {
     if (!st || !st->block) return;
-    if (st->block->graph) cudaGraphExecDestroy(st->block->graph);
+    BlockSolveState* bs = st->block;
+    if (bs->graph) cudaGraphExecDestroy(bs->graph);
+    for (cudaEvent_t e : {bs->ev_fork, bs->ev_join, bs->ev_x[0], bs->ev_x[1], bs->ev_b[0], bs->ev_b[1]})
+        if (e) cudaEventDestroy(e);
     delete st->block;
     st->block = nullptr;
 }
@@ -597,7 +642,13 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
     bs->Up = reinterpret_cast<float*>(bs->packs.as<char>() + ((bL + 255) / 256) * 256);
     const int64_t ldy = ((np + 31) / 32) * 32;
     const size_t bY = ((sizeof(float2) * (size_t)ldy * nrhs + 255) / 256) * 256;
-    SIEB_RETURN_IF(bs->work.reserve(bY + sizeof(float) * (size_t)nrhs * K3));
+    SIEB_RETURN_IF(bs->work.reserve(bY + 2 * sizeof(float) * (size_t)nrhs * K3));  // two Xpack buffers
+    if (!bs->ev_fork) {
+        for (cudaEvent_t* e : {&bs->ev_fork, &bs->ev_join, &bs->ev_x[0], &bs->ev_x[1], &bs->ev_b[0], &bs->ev_b[1]})
+            SIEB_TRY_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagApply));
+    }
     bs->Y = bs->work.as<float2>();
     bs->Xpack = reinterpret_cast<float*>(bs->work.as<char>() + bY);
     bs->ldy = ldy;
@@ -616,37 +667,110 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
 }
 
 // The two blocked triangular solves on Y (np x nrhs) in place.
+// Lookahead (default): the trailing GEMM of step k skips the next block,
+// whose diagonal kernel takes step k's update itself (the fold), so the
+// diagonal kernel of step k + 1 runs on the side stream beside the trailing
+// GEMM of step k, which leaves it a few SMs; the diagonal kernel of step k
+// waits for the trailing GEMM of step k - 2 (the last one that reaches its
+// block and the last reader of its Xpack buffer, double-buffered by step).
+// SIEB200_BLOCK_LOOKAHEAD=0: one stream, every GEMM over all rows below.
 static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* bs, int nrhs) {
     cudaStream_t stream = s->ctx->stream;
     const int64_t np = st->np, nbl = st->nbl;
     const unsigned gda = nblk(nrhs, DA_COLS);
-    for (int64_t k = 0; k < nbl; ++k) {
-        const int64_t k0 = k * NB;
-        const int kb = (int)std::min<int64_t>(NB, np - k0);
-        diag_apply_kernel<<<gda, 256, 0, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs, st->Linv + (size_t)k * NB * NB,
-                                                   bs->Xpack);
-        SIEB_NOTE_LAUNCH();
-        SIEB_TRY_CUDA(cudaGetLastError());
-        const int64_t s0 = k0 + kb;
-        if (s0 < np) {
-            const float* A = bs->Lp + 2 * lower_pack_rows_before(k, np) * K3;
-            SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y + s0), 2 * bs->ldy, A,
-                                       bs->Xpack, 2 * (np - s0), nrhs, K3, 0));
+    const char* la_env = getenv("SIEB200_BLOCK_LOOKAHEAD");
+    const bool la = !(la_env && la_env[0] == '0') && st->side != nullptr;
+    float* Xbuf[2] = {bs->Xpack, bs->Xpack + (size_t)nrhs * K3};
+    if (!la) {
+        for (int64_t k = 0; k < nbl; ++k) {
+            const int64_t k0 = k * NB;
+            const int kb = (int)std::min<int64_t>(NB, np - k0);
+            diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
+                                                                     st->Linv + (size_t)k * NB * NB, Xbuf[0],
+                                                                     nullptr, 0, nullptr, 0);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+            const int64_t s0 = k0 + kb;
+            if (s0 < np) {
+                const float* A = bs->Lp + 2 * lower_pack_rows_before(k, np) * K3;
+                SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y + s0), 2 * bs->ldy, A,
+                                           Xbuf[0], 2 * (np - s0), nrhs, K3, 0));
+            }
         }
-    }
-    for (int64_t k = nbl - 1; k >= 0; --k) {
-        const int64_t k0 = k * NB;
-        const int kb = (int)std::min<int64_t>(NB, np - k0);
-        diag_apply_kernel<<<gda, 256, 0, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs, st->Uinv + (size_t)k * NB * NB,
-                                                   bs->Xpack);
-        SIEB_NOTE_LAUNCH();
-        SIEB_TRY_CUDA(cudaGetLastError());
-        if (k0 > 0) {
-            const float* A = bs->Up + 2 * upper_pack_rows_before(k) * K3;
-            SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y), 2 * bs->ldy, A, bs->Xpack,
-                                       2 * k0, nrhs, K3, 0));
+        for (int64_t k = nbl - 1; k >= 0; --k) {
+            const int64_t k0 = k * NB;
+            const int kb = (int)std::min<int64_t>(NB, np - k0);
+            diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
+                                                                     st->Uinv + (size_t)k * NB * NB, Xbuf[0],
+                                                                     nullptr, 0, nullptr, 0);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+            if (k0 > 0) {
+                const float* A = bs->Up + 2 * upper_pack_rows_before(k) * K3;
+                SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y), 2 * bs->ldy, A,
+                                           Xbuf[0], 2 * k0, nrhs, K3, 0));
+            }
         }
+        return SIEB200_OK;
     }
+    cudaStream_t side = st->side;
+    const int cap = std::max(1, s->ctx->sm_count - 4);  // SMs left to the diagonal kernels
+    SIEB_TRY_CUDA(cudaEventRecord(bs->ev_fork, stream));
+    SIEB_TRY_CUDA(cudaStreamWaitEvent(side, bs->ev_fork, 0));
+    for (int pass = 0; pass < 2; ++pass) {  // 0: L (forward), 1: U (backward)
+        for (int64_t t = 0; t < nbl; ++t) {
+            const int64_t k = pass == 0 ? t : nbl - 1 - t;
+            const int64_t k0 = k * NB;
+            const int kb = (int)std::min<int64_t>(NB, np - k0);
+            float* Xk = Xbuf[t & 1];
+            if (t >= 2) SIEB_TRY_CUDA(cudaStreamWaitEvent(side, bs->ev_b[t & 1], 0));
+            // the previous step's update of this block, folded in
+            const float2* Fb = nullptr;
+            const float2* Xprev = nullptr;
+            int kbp = 0;
+            if (t >= 1) {
+                const int64_t kprev = pass == 0 ? k - 1 : k + 1;
+                const int64_t p0 = kprev * NB;
+                Fb = st->W + k0 + p0 * st->ldw;
+                Xprev = bs->Y + p0;
+                kbp = (int)std::min<int64_t>(NB, np - p0);
+            }
+            diag_apply_kernel<<<gda, 256, kSmemDiagApply, side>>>(
+                bs->Y, bs->ldy, k0, kb, nrhs, (pass == 0 ? st->Linv : st->Uinv) + (size_t)k * NB * NB, Xk, Fb,
+                st->ldw, Xprev, kbp);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+            SIEB_TRY_CUDA(cudaEventRecord(bs->ev_x[t & 1], side));
+            // trailing update of every block but the next one
+            const float* A;
+            float* C;
+            int64_t rows;
+            if (pass == 0) {
+                const int64_t s0 = k0 + kb, n1 = std::min<int64_t>(NB, np - s0);
+                rows = np - s0 - n1;
+                A = bs->Lp + 2 * (lower_pack_rows_before(k, np) + n1) * K3;
+                C = reinterpret_cast<float*>(bs->Y + s0 + n1);
+            } else {
+                rows = k0 - NB;  // rows above the previous block
+                A = bs->Up + 2 * upper_pack_rows_before(k) * K3;
+                C = reinterpret_cast<float*>(bs->Y);
+            }
+            if (rows > 0) {
+                SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, bs->ev_x[t & 1], 0));
+                SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * bs->ldy, A, Xk, 2 * rows, nrhs, K3, cap));
+            }
+            // recorded every step, so that the wait two steps later sees
+            // this step's GEMM (or, without one, everything before it)
+            SIEB_TRY_CUDA(cudaEventRecord(bs->ev_b[t & 1], stream));
+        }
+        // the second pass starts from the whole first one
+        SIEB_TRY_CUDA(cudaEventRecord(bs->ev_join, side));
+        SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, bs->ev_join, 0));
+        SIEB_TRY_CUDA(cudaEventRecord(bs->ev_fork, stream));
+        SIEB_TRY_CUDA(cudaStreamWaitEvent(side, bs->ev_fork, 0));
+    }
+    SIEB_TRY_CUDA(cudaEventRecord(bs->ev_join, side));
+    SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, bs->ev_join, 0));
     return SIEB200_OK;
 }
 

@@ -1154,8 +1154,12 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3);
 // many columns wide (0: none), and the SMs they leave to the panels.
 constexpr int kOverlapMinDefault = 0;
 // Pair schedule for block steps whose paired GEMM is at least this wide (0:
-// none, unless SIEB200_PAIR_UPDATE=1 makes every step a pair step).
-constexpr int kPairMinDefault = 0;
+// none; SIEB200_PAIR_UPDATE=1 makes every step a pair step). Measured with
+// every step paired: N = 6000 factor + solve 9.75 against 8.99 ms (the chain
+// of the steps without a GEMM is exposed), N = 17280 factorization 106 against
+// 117 ms and the N = 58,800 adjoint gradient 5.21 against 5.96 s (the GEMM
+// sets the pace there): so only updates at least this wide are paired.
+constexpr int kPairMinDefault = 8192;
 constexpr int kOverlapSmsDefault = 20;
 
 static int fp64_factorize(DenseSolver* s);

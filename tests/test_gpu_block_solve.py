@@ -86,8 +86,13 @@ def _solve(A, B, method="mixed_ir", per_column=False, gpu_ctx=None):
     return X
 
 
-@pytest.mark.parametrize("n,nrhs", [(50, 2), (130, 7), (997, 64), (2100, 17)])
-def test_block_solve_matches_numpy(n, nrhs, gpu_ctx):
+@pytest.mark.parametrize("lookahead", ["1", "0"])
+@pytest.mark.parametrize("n,nrhs", [(50, 2), (130, 7), (997, 64), (2100, 17), (4099, 33)])
+def test_block_solve_matches_numpy(n, nrhs, lookahead, gpu_ctx, monkeypatch):
+    """Block triangular solves with the lookahead (each diagonal block takes
+    the previous step's update itself, beside the trailing GEMM on another
+    stream) and without (SIEB200_BLOCK_LOOKAHEAD=0)."""
+    monkeypatch.setenv("SIEB200_BLOCK_LOOKAHEAD", lookahead)
     A = _system(n, n)
     rng = np.random.default_rng(n + 1)
     B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
