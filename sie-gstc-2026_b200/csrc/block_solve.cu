@@ -667,19 +667,23 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
 }
 
 // The two blocked triangular solves on Y (np x nrhs) in place.
-// Lookahead (default): the trailing GEMM of step k skips the next block,
+// Lookahead (optional): the trailing GEMM of step k skips the next block,
 // whose diagonal kernel takes step k's update itself (the fold), so the
 // diagonal kernel of step k + 1 runs on the side stream beside the trailing
 // GEMM of step k, which leaves it a few SMs; the diagonal kernel of step k
 // waits for the trailing GEMM of step k - 2 (the last one that reaches its
 // block and the last reader of its Xpack buffer, double-buffered by step).
-// SIEB200_BLOCK_LOOKAHEAD=0: one stream, every GEMM over all rows below.
+// The default is one stream, every GEMM over all rows below: on the config-3
+// system (N = 17280, 64 columns) the lookahead measured 18.8 against 16.7 ms
+// per application (the diagonal kernels with the fold and the cross-stream
+// hand-offs are slower than the GEMMs they overlap); SIEB200_BLOCK_LOOKAHEAD=1
+// selects it.
 static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* bs, int nrhs) {
     cudaStream_t stream = s->ctx->stream;
     const int64_t np = st->np, nbl = st->nbl;
     const unsigned gda = nblk(nrhs, DA_COLS);
     const char* la_env = getenv("SIEB200_BLOCK_LOOKAHEAD");
-    const bool la = !(la_env && la_env[0] == '0') && st->side != nullptr;
+    const bool la = la_env && la_env[0] == '1' && st->side != nullptr;
     float* Xbuf[2] = {bs->Xpack, bs->Xpack + (size_t)nrhs * K3};
     if (!la) {
         for (int64_t k = 0; k < nbl; ++k) {
