@@ -1158,8 +1158,12 @@ constexpr int kOverlapMinDefault = 0;
 // every step paired: N = 6000 factor + solve 9.75 against 8.99 ms (the chain
 // of the steps without a GEMM is exposed), N = 17280 factorization 106 against
 // 117 ms and the N = 58,800 adjoint gradient 5.21 against 5.96 s (the GEMM
-// sets the pace there): so only updates at least this wide are paired.
-constexpr int kPairMinDefault = 8192;
+// sets the pace there): so only updates at least this wide are paired. The
+// paired updates also leave slightly less accurate factors: with 8192 the
+// config-3 system (N = 17280, 64 right-hand sides) needed one refinement
+// iteration more (6 instead of 5), which cost more than the faster
+// factorization gained; 20000 keeps such systems on single steps.
+constexpr int kPairMinDefault = 20000;
 constexpr int kOverlapSmsDefault = 20;
 
 static int fp64_factorize(DenseSolver* s);
