@@ -354,6 +354,13 @@ int sieb200_prepare_records(sieb200_ctx* ctx, int64_t faces, const double* maps,
  * once per tile. */
 int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
                           const float* B, float* C, int64_t ldc, int mode);
+/* The same contraction with the first 128 rows of C (one 64-unknown block row
+ * of a realified complex matrix) restricted to columns [col_shift, n): those
+ * rows' first col_shift columns are left untouched. This is the shape of the
+ * mixed LU's trailing update, which leaves the next diagonal block to a
+ * kernel running at the same time. 0 <= col_shift < n. */
+int sieb200_gemm_tf32_sub_shifted(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
+                                  const float* B, float* C, int64_t ldc, int mode, int64_t col_shift);
 
 /* Per-context kernel timing (no counterpart in the reference, which times
  * phases with std::chrono): when enabled, the library brackets each launch

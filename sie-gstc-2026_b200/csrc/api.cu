@@ -1057,18 +1057,23 @@ int sieb200_profile_read(sieb200_ctx* ctx, int kernel, int64_t* launches, double
     return SIEB200_OK;
 }
 
-int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
-                          const float* B, float* C, int64_t ldc, int mode) {
+int sieb200_gemm_tf32_sub_shifted(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
+                                  const float* B, float* C, int64_t ldc, int mode, int64_t col_shift) {
     SIEB_CHECK(ctx && A && B && C && ldc >= m2 && mode >= 0 && mode <= 5, SIEB200_INVALID_ARG,
                "invalid GEMM arguments");
     SIEB_TRY_CUDA(cudaSetDevice(ctx->device));
     GemmTC* g = nullptr;
     SIEB_RETURN_IF(gemm_tc_create(&g));
     gemm_tc_set_mode(g, mode >= 4 ? mode - 2 : mode);
-    int st = gemm_tc_sub(g, ctx->stream, C, ldc, A, B, m2, n, k, 0, mode >= 4 ? 1 : 0);
+    int st = gemm_tc_sub(g, ctx->stream, C, ldc, A, B, m2, n, k, 0, mode >= 4 ? 1 : 0, col_shift);
     if (st == SIEB200_OK) st = gemm_tc_check(g, ctx->stream);
     gemm_tc_destroy(g);
     return st;
+}
+
+int sieb200_gemm_tf32_sub(sieb200_ctx* ctx, int64_t m2, int64_t n, int k, const float* A,
+                          const float* B, float* C, int64_t ldc, int mode) {
+    return sieb200_gemm_tf32_sub_shifted(ctx, m2, n, k, A, B, C, ldc, mode, 0);
 }
 
 int sieb200_far_field(sieb200_ctx* ctx, const sieb200_mesh* mesh, const double* j_cur,

@@ -84,7 +84,8 @@ __host__ __device__ inline int64_t upper_pack_rows_before(int64_t k) {
 // are coalesced. Row 2r: [Re, -Im] per column, row 2r + 1: [Im, Re];
 // layout [hi | hi | lo] along K; columns beyond the block's width are zero.
 __global__ void __launch_bounds__(256) pack_factors_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
-                                                           float* __restrict__ Lp, float* __restrict__ Up) {
+                                                           float* __restrict__ Lp, float* __restrict__ Up,
+                                                           int lo_rn) {
     __shared__ float2 tile[32][NB + 1];
     const int64_t k = blockIdx.y;
     const int64_t k0 = k * NB;
@@ -113,8 +114,8 @@ __global__ void __launch_bounds__(256) pack_factors_kernel(const float2* __restr
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
         float* row0 = base + (2 * (gr - r_begin)) * K3;
         float* row1 = row0 + K3;
-        row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
-        row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
+        row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = tf32_lo(v0, h0, lo_rn);
+        row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = tf32_lo(v1, h1, lo_rn);
     }
 }
 
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
                                                          int nrhs, const float2* __restrict__ Inv,
                                                          float* __restrict__ Xpack,
                                                          const float2* __restrict__ Fb, int64_t ldf,
-                                                         const float2* __restrict__ Xprev, int kbp) {
+                                                         const float2* __restrict__ Xprev, int kbp, int lo_rn) {
     extern __shared__ __align__(16) float2 da_smem[];
     float2(*inv)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(da_smem);              // [row][col]
     float2(*fb)[NB + 1] = inv + NB;                                                    // [row][col]
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
         if (in) Y[(k0 + r) + (int64_t)gc * ldy] = make_float2(vx, vy);
         const float h0 = tf32_hi(vx), h1 = tf32_hi(vy);
         col[2 * r] = h0; col[2 * r + 1] = h1;
-        col[2 * NB + 2 * r] = vx - h0; col[2 * NB + 2 * r + 1] = vy - h1;
+        col[2 * NB + 2 * r] = tf32_lo(vx, h0, lo_rn); col[2 * NB + 2 * r + 1] = tf32_lo(vy, h1, lo_rn);
         col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
     }
 }
@@ -657,7 +658,7 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
     // The packs are built once per factorization (which clears `packed`).
     if (!bs->packed) {
         const dim3 grid(nblk(np, 32), (unsigned)nbl, 2);
-        pack_factors_kernel<<<grid, 256, 0, s->ctx->stream>>>(st->W, st->ldw, np, bs->Lp, bs->Up);
+        pack_factors_kernel<<<grid, 256, 0, s->ctx->stream>>>(st->W, st->ldw, np, bs->Lp, bs->Up, st->lo_rn);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         bs->packed = true;
@@ -691,7 +692,7 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             const int kb = (int)std::min<int64_t>(NB, np - k0);
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
                                                                      st->Linv + (size_t)k * NB * NB, Xbuf[0],
-                                                                     nullptr, 0, nullptr, 0);
+                                                                     nullptr, 0, nullptr, 0, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             const int64_t s0 = k0 + kb;
@@ -706,7 +707,7 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             const int kb = (int)std::min<int64_t>(NB, np - k0);
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
                                                                      st->Uinv + (size_t)k * NB * NB, Xbuf[0],
-                                                                     nullptr, 0, nullptr, 0);
+                                                                     nullptr, 0, nullptr, 0, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             if (k0 > 0) {
@@ -741,7 +742,7 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             }
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, side>>>(
                 bs->Y, bs->ldy, k0, kb, nrhs, (pass == 0 ? st->Linv : st->Uinv) + (size_t)k * NB * NB, Xk, Fb,
-                st->ldw, Xprev, kbp);
+                st->ldw, Xprev, kbp, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             SIEB_TRY_CUDA(cudaEventRecord(bs->ev_x[t & 1], side));

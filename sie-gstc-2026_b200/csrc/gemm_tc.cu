@@ -101,7 +101,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 __global__ void __launch_bounds__(128, 2)
 gemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, unsigned* err) {
+                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, int shift0, unsigned* err) {
+    // The first row tile starts shift0 columns in (see gemm_tc_sub); a tile
+    // left wholly past the last column has nothing to do.
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN + (blockIdx.x == 0 ? shift0 : 0);
+    if (n0 >= N) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte aligned stage area (required by the 128B swizzle atoms).
     const uint32_t raw = smem_u32(smem_raw);
@@ -116,7 +120,6 @@ gemm_tf32_sub_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_const
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(&bars[2 * STAGES + 1]);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int kblocks = K / BK;
 
     if (threadIdx.x == 0) {
@@ -256,7 +259,8 @@ __device__ __forceinline__ void epilogue_bar() { asm volatile("bar.sync 1, 128;"
 template <bool REDUCE, bool HILO, int CH>
 __global__ void __launch_bounds__(P_THREADS, 1)
 gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                                const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, unsigned* err) {
+                                const __grid_constant__ CUtensorMap tmC, int M2, int N, int K, int shift0,
+                                int lolo, unsigned* err) {
     constexpr int NS = HILO ? H_STAGES : P_STAGES;     // ring stages
     constexpr int SA = HILO ? 2 * STAGE_A : STAGE_A;   // A bytes per stage
     constexpr int SB = HILO ? 2 * STAGE_B : STAGE_B;   // B bytes per stage
@@ -284,6 +288,24 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
     const int tiles = mt * nt;
     const int KR = HILO ? K / 2 : K;  // columns of one K sweep (the hi half)
     const int kblocks = KR / BK;
+    // A_lo against B_hi only (N = 128), or against the stacked [B_hi; B_lo]
+    // as well (lolo: the fourth product lo.lo lands beside hi.lo)
+    const uint32_t idesc_lo = lolo ? kIdesc2 : kIdesc;
+    // Tile t covers rows (t % mt) BM and columns (t / mt) BN, the first row
+    // tile shift0 columns further right; a tile wholly past the last column
+    // is skipped alike by all three roles (first: this CTA's first tile,
+    // next: its tile after t).
+    auto col0 = [&](int t) { return (t / mt) * BN + ((t % mt) == 0 ? shift0 : 0); };
+    auto first = [&]() {
+        int t = blockIdx.x;
+        while (t < tiles && col0(t) >= N) t += gridDim.x;
+        return t;
+    };
+    auto next = [&](int t) {
+        t += gridDim.x;
+        while (t < tiles && col0(t) >= N) t += gridDim.x;
+        return t;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; ++s) {
@@ -312,8 +334,8 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
         if (lane == 0) {
             int g = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int m0 = (t % mt) * BM, n0 = (t / mt) * BN;
+            for (int t = first(); t < tiles && ok; t = next(t)) {
+                const int m0 = (t % mt) * BM, n0 = col0(t);
                 for (int kb = 0; kb < kblocks; ++kb, ++g) {
                     const int s = g % NS;
                     const uint32_t ph = (uint32_t)(g / NS) & 1u;
@@ -332,7 +354,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
         if (lane == 0) {
             int g = 0, li = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++li) {
+            for (int t = first(); t < tiles && ok; t = next(t), ++li) {
                 const int b = li & 1;
                 const uint32_t u = (uint32_t)(li >> 1);
                 if (!mbar_wait(acce0 + 8 * b, (u & 1u) ^ 1u, err)) break;
@@ -350,7 +372,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
 #pragma unroll
                         for (int k = 0; k < BK / 8; ++k) {
                             umma_tf32(acc, ad + 2 * k, bd + 2 * k, (kb | k) != 0 ? 1u : 0u, kIdesc2);
-                            umma_tf32(acc, adl + 2 * k, bd + 2 * k, 1u, kIdesc);
+                            umma_tf32(acc, adl + 2 * k, bd + 2 * k, 1u, idesc_lo);
                         }
                     } else {
 #pragma unroll
@@ -373,17 +395,17 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
         const int et = threadIdx.x - 64;   // 0..127
         const int rt = q * 32 + lane;      // row of the tile
         const bool e0 = et == 0;
-        int t = blockIdx.x;
+        int t = first();
         if (!REDUCE && e0 && t < tiles) {
             for (int c = 0; c < CH; ++c) {
                 mbar_expect_tx(cfull0 + 8 * c, CHUNK_BYTES);
-                tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (t % mt) * BM, (t / mt) * BN + c * CC);
+                tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (t % mt) * BM, col0(t) + c * CC);
             }
         }
-        for (int li = 0; t < tiles; t += gridDim.x, ++li) {
+        for (int li = 0; t < tiles; t = next(t), ++li) {
             const int b = li & 1;
             const uint32_t u = (uint32_t)(li >> 1);
-            const int tn = t + gridDim.x;
+            const int tn = next(t);
             int got = 0;
             if (lane == 0) got = mbar_wait(accf0 + 8 * b, u & 1u, err) ? 1 : 0;
             got = __shfl_sync(0xffffffffu, got, 0);
@@ -424,7 +446,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 epilogue_bar();
                 if (e0) {
-                    const int x = (t % mt) * BM, y = (t / mt) * BN + c * CC;
+                    const int x = (t % mt) * BM, y = col0(t) + c * CC;
                     if (REDUCE) {
                         // A tile whose accumulator wait failed adds nothing.
                         if (got) tma_reduce_add_2d(&tmC, sC + c * CHUNK_BYTES, x, y);
@@ -441,7 +463,7 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
                     if (!REDUCE && tn < tiles) {
                         mbar_expect_tx(cfull0 + 8 * c, CHUNK_BYTES);
                         tma_load_2d(sC + c * CHUNK_BYTES, &tmC, cfull0 + 8 * c, (tn % mt) * BM,
-                                    (tn / mt) * BN + c * CC);
+                                    col0(tn) + c * CC);
                     }
                 }
                 // REDUCE: the next slot is written only after its previous
@@ -464,9 +486,12 @@ gemm_tf32_sub_persistent_kernel(const __grid_constant__ CUtensorMap tmA, const _
 // hilo: A = [A_hi | A_lo], B = [B_hi | B_lo] along K; the sum is
 // a_hi (b_hi + b_lo) + a_lo b_hi per k of the first half.
 __global__ void gemm_simt_sub_kernel(const float* __restrict__ A, const float* __restrict__ B,
-                                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, int hilo) {
+                                     float* __restrict__ C, int64_t ldc, int M2, int N, int K, int hilo,
+                                     int shift0) {
     __shared__ float As[64][33], Bs[64][33], Al[64][33], Bl[64][33];
-    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+    // rows [0, BM) start shift0 columns in, like the tensor-core kernels
+    const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64 + (r0 < BM ? shift0 : 0);
+    if (c0 >= N) return;
     const int tr = threadIdx.x & 63, tc = threadIdx.x >> 6;  // 256 threads: 64 rows x 4 col groups
     const int KR = hilo ? K / 2 : K;
     float acc[16];
@@ -538,6 +563,7 @@ struct GemmTC {
     unsigned* err = nullptr;
     int mode = 3;  // persistent kernel, reduction epilogue
     int c_slots = 4;  // C slots of the persistent kernel's epilogue (1 or 4)
+    int lolo = 0;     // split operands: also the product A_lo B_lo^T
     bool attr_set = false;
     bool attr_set_p[8] = {};
     int sms = 148;
@@ -545,30 +571,32 @@ struct GemmTC {
 
 template <bool REDUCE, bool HILO, int CH>
 int launch_one(unsigned grid, cudaStream_t stream, const CUtensorMap& ma, const CUtensorMap& mb,
-               const CUtensorMap& mc, int M2, int N, int K, unsigned* err, bool& attr_set) {
+               const CUtensorMap& mc, int M2, int N, int K, int shift0, int lolo, unsigned* err,
+               bool& attr_set) {
     if (!attr_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(gemm_tf32_sub_persistent_kernel<REDUCE, HILO, CH>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
         attr_set = true;
     }
     gemm_tf32_sub_persistent_kernel<REDUCE, HILO, CH><<<grid, P_THREADS, P_SMEM_BYTES, stream>>>(ma, mb, mc, M2, N,
-                                                                                                K, err);
+                                                                                                K, shift0, lolo, err);
     return SIEB200_OK;
 }
 
 // variant bit 0: reduction epilogue, bit 1: split operands, bit 2: four C slots.
 int launch_persistent(int variant, unsigned grid, cudaStream_t stream, const CUtensorMap& ma, const CUtensorMap& mb,
-                      const CUtensorMap& mc, int M2, int N, int K, unsigned* err, bool (&attr_set)[8]) {
+                      const CUtensorMap& mc, int M2, int N, int K, int shift0, int lolo, unsigned* err,
+                      bool (&attr_set)[8]) {
     bool& a = attr_set[variant];
     switch (variant) {
-        case 0: return launch_one<false, false, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 1: return launch_one<true, false, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 2: return launch_one<false, true, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 3: return launch_one<true, true, 1>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 4: return launch_one<false, false, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 5: return launch_one<true, false, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        case 6: return launch_one<false, true, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
-        default: return launch_one<true, true, 4>(grid, stream, ma, mb, mc, M2, N, K, err, a);
+        case 0: return launch_one<false, false, 1>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 1: return launch_one<true, false, 1>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 2: return launch_one<false, true, 1>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 3: return launch_one<true, true, 1>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 4: return launch_one<false, false, 4>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 5: return launch_one<true, false, 4>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        case 6: return launch_one<false, true, 4>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
+        default: return launch_one<true, true, 4>(grid, stream, ma, mb, mc, M2, N, K, shift0, lolo, err, a);
     }
 }
 
@@ -587,6 +615,8 @@ int gemm_tc_create(GemmTC** out) {
     if (mode_env && mode_env[0] >= '0' && mode_env[0] <= '3' && mode_env[1] == 0) g->mode = mode_env[0] - '0';
     const char* slots_env = getenv("SIEB200_GEMM_C_SLOTS");
     if (slots_env && slots_env[0] == '1' && slots_env[1] == 0) g->c_slots = 1;
+    const char* lolo_env = getenv("SIEB200_GEMM_LOLO");
+    g->lolo = (lolo_env && lolo_env[0] == '1') ? 1 : 0;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&g->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -604,16 +634,17 @@ void gemm_tc_destroy(GemmTC* g) {
 void gemm_tc_set_mode(GemmTC* g, int mode) { g->mode = mode; }
 
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A, const float* B,
-                int64_t M2, int64_t N, int K, int max_ctas, int layout) {
+                int64_t M2, int64_t N, int K, int max_ctas, int layout, int64_t shift0) {
     SIEB_CHECK(K % BK == 0 && K > 0, SIEB200_INVALID_ARG, "GEMM K must be a positive multiple of 32");
     SIEB_CHECK(layout == 0 || (layout == 1 && K % (2 * BK) == 0), SIEB200_INVALID_ARG,
                "split-operand GEMM: K must be a positive multiple of 64");
     SIEB_CHECK(M2 > 0 && N > 0 && M2 < (1ll << 31) && N < (1ll << 31), SIEB200_INVALID_ARG, "GEMM size out of range");
+    SIEB_CHECK(shift0 >= 0 && shift0 < N, SIEB200_INVALID_ARG, "GEMM first-row-tile column shift out of range");
     SIEB_CHECK(((uintptr_t)A % 16) == 0 && ((uintptr_t)B % 16) == 0, SIEB200_INVALID_ARG,
                "GEMM operands must be 16-byte aligned");
     if (g->mode == 0) {
         gemm_simt_sub_kernel<<<dim3((unsigned)((M2 + 63) / 64), (unsigned)((N + 63) / 64)), 256, 0, stream>>>(
-            A, B, C, ldc, (int)M2, (int)N, K, layout);
+            A, B, C, ldc, (int)M2, (int)N, K, layout, (int)shift0);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
@@ -636,8 +667,8 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         const unsigned grid = (unsigned)std::min<int64_t>(tiles, std::max(1, cap));
         const bool red = g->mode == 3;
         const int variant = (red ? 1 : 0) + (layout == 1 ? 2 : 0) + (ch == 4 ? 4 : 0);
-        SIEB_RETURN_IF(launch_persistent(variant, grid, stream, ma, mb, mc, (int)M2, (int)N, K, g->err,
-                                         g->attr_set_p));
+        SIEB_RETURN_IF(launch_persistent(variant, grid, stream, ma, mb, mc, (int)M2, (int)N, K, (int)shift0,
+                                         layout == 1 ? g->lolo : 0, g->err, g->attr_set_p));
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
@@ -648,7 +679,7 @@ int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const flo
         g->attr_set = true;
     }
     const dim3 grid((unsigned)((M2 + BM - 1) / BM), (unsigned)((N + BN - 1) / BN));
-    gemm_tf32_sub_kernel<<<grid, 128, SMEM_BYTES, stream>>>(ma, mb, C, ldc, (int)M2, (int)N, K, g->err);
+    gemm_tf32_sub_kernel<<<grid, 128, SMEM_BYTES, stream>>>(ma, mb, C, ldc, (int)M2, (int)N, K, (int)shift0, g->err);
     SIEB_NOTE_LAUNCH();
     SIEB_TRY_CUDA(cudaGetLastError());
     return SIEB200_OK;

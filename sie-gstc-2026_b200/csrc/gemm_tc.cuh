@@ -19,8 +19,13 @@ void gemm_tc_destroy(GemmTC* g);
 // concurrent work on other streams.
 // layout 0: A and B are one K sweep; layout 1: [hi | lo] halves along K,
 // C -= A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T (persistent kernel).
+// shift0 > 0 leaves the first shift0 columns of the first 128 rows (one row
+// tile) untouched: those rows take columns [shift0, N), the others [0, N)
+// (the trailing update of a block LU whose next diagonal block is factored
+// concurrently).
 int gemm_tc_sub(GemmTC* g, cudaStream_t stream, float* C, int64_t ldc, const float* A,
-                const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0, int layout = 0);
+                const float* B, int64_t M2, int64_t N, int K, int max_ctas = 0, int layout = 0,
+                int64_t shift0 = 0);
 int gemm_tc_check(GemmTC* g, cudaStream_t stream);
 // Selects the implementation: 3 = persistent tcgen05 kernel whose epilogue
 // adds -acc to C by TMA reduction (default), 2 = persistent kernel that

@@ -47,6 +47,21 @@ constexpr int kSmemPanel64 = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(d
 constexpr int kSmemDiagUpd64 = 2 * NB * (NB + 1) * (int)sizeof(double2);
 
 
+// SIEB200_DIAG_SPLIT=0 folds the diagonal blocks' updates back into the LU
+// kernel.
+static int diag_split_env() {
+    const char* e = getenv("SIEB200_DIAG_SPLIT");
+    return (e && e[0] == '0') ? 0 : 1;
+}
+
+// SIEB200_DIAG_PANELS=1: the diagonal-block elimination with one named
+// barrier per panel instead of one block barrier per step (measured ~2 us
+// per launch slower in the N = 6000 factorization).
+static int diag_panels_env() {
+    const char* e = getenv("SIEB200_DIAG_PANELS");
+    return (e && e[0] == '1') ? 1 : 0;
+}
+
 static void drop_graphs(MixedState* st) {
     for (auto& g : st->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -280,11 +295,141 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
     }
 }
 
+// The same steps, one panel of kDiagCols columns at a time: the warp that
+// owns columns [kDiagCols p, kDiagCols (p+1)) runs the panel's steps alone
+// (its own columns only, through shuffles), leaving each coefficient column
+// c_j in cbuf[j], and signals named barrier 1 + p without waiting on it
+// (bar.arrive); every other warp waits there (bar.sync) and then applies the
+// panel's steps to its columns. So while the others apply panel p, the warp
+// owning panel p + 1 applies it to its own columns and goes on to factor
+// them: one barrier per panel instead of one per step, and no warp waits for
+// a panel's update of columns other than its own. Each column takes the
+// same updates in the same order as in diag_steps (same results). cbuf
+// holds all NB coefficient columns ([j][row]); every barrier id is used
+// once, and warp p arrives at its barrier only after passing those of
+// panels 0 .. p-1, whose owners arrive unconditionally: no wait can hang.
+__device__ __forceinline__ void named_bar_arrive(int id, int threads) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+__device__ __forceinline__ void named_bar_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+template <class T, int H>
+__device__ __forceinline__ void diag_panel(T (&a)[kDiagCols][2], int p, int w, int lane, T (*cbuf)[NB],
+                                           T* rcps, unsigned* err) {
+    using R = typename RealOf<T>::type;
+    constexpr int CW = kDiagCols;
+    const T z = cmk<T>(0.f, 0.f);
+    if (w == p) {
+#pragma unroll
+        for (int u = 0; u < CW; ++u) {
+            const int j = CW * p + u, jl = j & 31;
+            const bool g0 = lane > j, g1 = lane + 32 > j;
+            const T piv = shfl_c(a[u][H], jl);
+            const R pm = piv.x * piv.x + piv.y * piv.y;
+            const bool bad = !(pm > tiny_pivot(pm)) || !isfinite(pm);
+            if (bad && lane == 0) atomicCAS(err, 0u, 1u);
+            const R inv = bad ? R(0) : rcp_rn(pm);
+            const T rcp = cmk<T>(piv.x * inv, -piv.y * inv);
+            T ca0 = cmulf(a[u][0], rcp);
+            T ca1 = cmulf(a[u][1], rcp);
+            if (lane == jl) {
+                if (H) ca1 = z;
+                else ca0 = z;
+            }
+            cbuf[j][lane] = ca0;
+            cbuf[j][lane + 32] = ca1;
+            if (lane == 0) rcps[j] = rcp;
+            a[u][0] = g0 ? cnegf(ca0) : a[u][0];
+            a[u][1] = g1 ? cnegf(ca1) : a[u][1];
+            const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+#pragma unroll
+            for (int v = 0; v < CW; ++v) {
+                if (v == u) continue;
+                const T x = shfl_c(a[v][H], jl);
+                if (v < u) {
+                    if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
+                    a[v][1] = cfmsf(a[v][1], cl1, x);
+                } else {
+                    a[v][0] = cfmsf(a[v][0], ca0, x);
+                    a[v][1] = cfmsf(a[v][1], ca1, x);
+                }
+            }
+        }
+        __syncwarp();
+        named_bar_arrive(1 + p, kDiagThreads);
+    } else {
+        named_bar_sync(1 + p, kDiagThreads);
+#pragma unroll
+        for (int u = 0; u < CW; ++u) {
+            const int j = CW * p + u, jl = j & 31;
+            const bool g0 = lane > j, g1 = lane + 32 > j;
+            const T ca0 = cbuf[j][lane], ca1 = cbuf[j][lane + 32];
+            if (w < p) {  // columns left of the pivot: rows below j only
+                const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+#pragma unroll
+                for (int v = 0; v < CW; ++v) {
+                    const T x = shfl_c(a[v][H], jl);
+                    if (H == 0) a[v][0] = cfmsf(a[v][0], cl0, x);
+                    a[v][1] = cfmsf(a[v][1], cl1, x);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < CW; ++v) {
+                    const T x = shfl_c(a[v][H], jl);
+                    a[v][0] = cfmsf(a[v][0], ca0, x);
+                    a[v][1] = cfmsf(a[v][1], ca1, x);
+                }
+            }
+        }
+    }
+}
+
+// The update of a diagonal block by the earlier block steps kp1 (and kp2,
+// -1 = none), A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb], in place in
+// W, on 16 CTAs of 16 x 16 entries (one per thread, the k order and FP32
+// FMAs of the update inside diag_lu_kernel, so the result is the same bit
+// for bit). Run ahead of diag_lu_kernel it takes the product off that
+// kernel's single SM: 64 x 64 x 64 complex FMAs are at least 4.2 us of FP32
+// issue on one SM, here spread over 16.
+template <class T>
+__global__ void __launch_bounds__(256) diag_update_kernel(T* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                          int64_t kp1, int64_t kp2) {
+    __shared__ T Ls[NB][17];      // [k][row]
+    __shared__ T Us[16][NB + 1];  // [col][k]
+    const int tid = threadIdx.x;
+    const int r = tid & 15, c = tid >> 4;
+    const int row = 16 * blockIdx.x + r, col = 16 * blockIdx.y + c;
+    const bool in = row < kb && col < kb;
+    T a = in ? W[(k0 + row) + (k0 + col) * ldw] : cmk<T>(0.f, 0.f);
+    for (int q = 0; q < 2; ++q) {
+        const int64_t kp = q == 0 ? kp1 : kp2;
+        if (kp < 0) continue;
+        __syncthreads();  // the previous update's tiles are no longer read
+        for (int e = tid; e < NB * 16; e += 256) {
+            const int i = e & 15, kk = e >> 4;  // rows fastest: coalesced columns of L21
+            const int gr = 16 * blockIdx.x + i;
+            Ls[kk][i] = gr < kb ? W[(k0 + gr) + (kp + kk) * ldw] : cmk<T>(0.f, 0.f);
+            const int kk2 = e % NB, j = e / NB;  // k fastest: coalesced columns of U12
+            const int gc = 16 * blockIdx.y + j;
+            Us[j][kk2] = gc < kb ? W[(kp + kk2) + (k0 + gc) * ldw] : cmk<T>(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < NB; ++kk) a = cfmsf(a, Ls[kk][r], Us[c][kk]);
+    }
+    if (in) W[(k0 + row) + (k0 + col) * ldw] = a;
+}
+
 // With kp1 >= 0 (and kp2 >= 0) the block first takes those earlier block
 // steps' updates, A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32
 // FMA), from the factor blocks staged in dynamic shared memory (kSmemDiagUpd;
 // that size also keeps the kernel off SMs that hold a trailing-GEMM CTA).
-template <class T>
+// PANELS: diag_panel (one named barrier per panel) instead of diag_steps
+// (one block barrier per step); the coefficient columns then live in the
+// dynamic shared memory, after the update tiles are no longer read.
+template <class T, bool PANELS>
 __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restrict__ W, int64_t ldw,
                                                                int64_t k0, int kb, T* __restrict__ Linv,
                                                                T* __restrict__ Uinv,
@@ -325,10 +470,19 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
             }
         }
     }
+    if (PANELS) {
+        T(*cb)[NB] = reinterpret_cast<T(*)[NB]>(dyn_smem);
+        __syncthreads();  // the update tiles are no longer read
 #pragma unroll 1
-    for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cbuf, rcps, err);
+        for (int p = 0; p < kDiagWarps / 2; ++p) diag_panel<T, 0>(a, p, w, lane, cb, rcps, err);
 #pragma unroll 1
-    for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<T, 1>(a, bp, w, lane, cbuf, rcps, err);
+        for (int p = kDiagWarps / 2; p < kDiagWarps; ++p) diag_panel<T, 1>(a, p, w, lane, cb, rcps, err);
+    } else {
+#pragma unroll 1
+        for (int bp = 0; bp < kDiagWarps / 2; ++bp) diag_steps<T, 0>(a, bp, w, lane, cbuf, rcps, err);
+#pragma unroll 1
+        for (int bp = kDiagWarps / 2; bp < kDiagWarps; ++bp) diag_steps<T, 1>(a, bp, w, lane, cbuf, rcps, err);
+    }
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < CW; ++v) {
@@ -367,6 +521,7 @@ struct PanelArgs {
     float* Bpack = nullptr;
     int64_t b_ld = 0, b_c0 = 0;
     int64_t a_lo = 0, b_lo = 0;
+    int lo_rn = 0;  // lo parts rounded to the nearest TF32
 };
 
 // L21 = A21 * inv(U11) for rows [s0, np) of the panel columns [k0, k0+kb);
@@ -472,12 +627,13 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
         float* row0 = pa.Apack + (2 * (gr - pa.a_r0)) * pa.a_ld;
         float* row1 = row0 + pa.a_ld;
+        const float l0 = tf32_lo(v0, h0, pa.lo_rn), l1 = tf32_lo(v1, h1, pa.lo_rn);
         if (pa.a_lo) {
-            row0[kk] = h0; row0[pa.a_lo + kk] = v0 - h0;
-            row1[kk] = h1; row1[pa.a_lo + kk] = v1 - h1;
+            row0[kk] = h0; row0[pa.a_lo + kk] = l0;
+            row1[kk] = h1; row1[pa.a_lo + kk] = l1;
         } else {
-            row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = v0 - h0;
-            row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = v1 - h1;
+            row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = l0;
+            row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = l1;
         }
     }
 }
@@ -571,15 +727,72 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
         if (std::is_same<T, float2>::value && pa.pack && gc >= pa.b_c0) {
             float* col = pa.Bpack + (gc - pa.b_c0) * pa.b_ld;
             const float h0 = tf32_hi(v.x), h1 = tf32_hi(v.y);
+            const float l0 = tf32_lo(v.x, h0, pa.lo_rn), l1 = tf32_lo(v.y, h1, pa.lo_rn);
             col[2 * r] = h0; col[2 * r + 1] = h1;
             if (pa.b_lo) {
-                col[pa.b_lo + 2 * r] = v.x - h0; col[pa.b_lo + 2 * r + 1] = v.y - h1;
+                col[pa.b_lo + 2 * r] = l0; col[pa.b_lo + 2 * r + 1] = l1;
             } else {
-                col[2 * NB + 2 * r] = v.x - h0; col[2 * NB + 2 * r + 1] = v.y - h1;
+                col[2 * NB + 2 * r] = l0; col[2 * NB + 2 * r + 1] = l1;
                 col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
             }
         }
     }
+}
+
+// Rows [r0, np) of block column k0 (kb columns) take the update of step kp,
+// A21 -= L21(kp)[rows, :] U12(kp)[:, k0:k0+kb], written back to W: the FP32
+// FMAs of panel_L_body's update in the same order (same results), ahead of
+// a panels launch that then only forms L21 = A21 inv(U11). One CTA per 32
+// rows, thread (ty, tx) rows 2ty, 2ty+1 and columns 4tx .. 4tx+3 as there;
+// the K range is staged in two halves so that the shared memory (25.8 KB)
+// leaves a CTA room beside a trailing-GEMM CTA on its SM.
+constexpr int kColUpdK = NB / 2;
+__global__ void __launch_bounds__(256) col_update_kernel(float2* __restrict__ W, int64_t ldw, int64_t k0, int kb,
+                                                         int64_t r0, int64_t np, int64_t kp) {
+    __shared__ float2 Us[kColUpdK][NB + 4];  // [k][c]
+    __shared__ float2 Lr[32][kColUpdK + 1];  // [row][k]
+    const int tid = threadIdx.x;
+    const int ty = tid & 15, tx = tid >> 4;
+    const int64_t rb = r0 + (int64_t)blockIdx.x * 32;
+    float2 upd[2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t gr = rb + 2 * ty + i;
+            const int c = 4 * tx + j;
+            upd[i][j] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+        }
+    for (int h = 0; h < NB; h += kColUpdK) {
+        __syncthreads();  // the previous half is no longer read
+        for (int e = tid; e < kColUpdK * NB; e += blockDim.x) {
+            const int kk = e % kColUpdK, c = e / kColUpdK;  // k fastest: coalesced columns of U12
+            Us[kk][c] = c < kb ? W[(kp + h + kk) + (k0 + c) * ldw] : make_float2(0.f, 0.f);
+        }
+        for (int e = tid; e < 32 * kColUpdK; e += blockDim.x) {
+            const int r = e % 32, kk = e / 32;  // rows fastest: coalesced columns of L21
+            const int64_t gr = rb + r;
+            Lr[r][kk] = gr < np ? W[gr + (kp + h + kk) * ldw] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        for (int kk = 0; kk < kColUpdK; ++kk) {
+            const float2 l0 = Lr[2 * ty][kk], l1 = Lr[2 * ty + 1][kk];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 u = Us[kk][4 * tx + j];
+                upd[0][j] = cfmsf(upd[0][j], l0, u);
+                upd[1][j] = cfmsf(upd[1][j], l1, u);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t gr = rb + 2 * ty + i;
+            const int c = 4 * tx + j;
+            if (gr < np && c < kb) W[gr + (k0 + c) * ldw] = upd[i][j];
+        }
 }
 
 // Both panels of a block step in one launch: CTAs [0, nL) form L21 (rows
@@ -1121,7 +1334,9 @@ void mixed_release(DenseSolver* s) {
         if (st->ev_cols) cudaEventDestroy(st->ev_cols);
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
         if (st->ev_pan) cudaEventDestroy(st->ev_pan);
+        if (st->ev_lcol) cudaEventDestroy(st->ev_lcol);
         if (st->side) cudaStreamDestroy(st->side);
+        if (st->side2) cudaStreamDestroy(st->side2);
         delete st;
     }
     s->gemm_state = nullptr;
@@ -1197,6 +1412,12 @@ int mixed_factorize(DenseSolver* s) {
     st->ovl_min = ovl_env ? std::max(0, atoi(ovl_env)) : kOverlapMinDefault;
     const char* ovs_env = getenv("SIEB200_OVERLAP_SMS");
     st->ovl_sms = ovs_env ? std::max(2, std::min(s->ctx->sm_count / 2, atoi(ovs_env))) : kOverlapSmsDefault;
+    const char* lcol_env = getenv("SIEB200_GEMM_LCOL");
+    st->lcol = (lcol_env && lcol_env[0] >= '0' && lcol_env[0] <= '3' && lcol_env[1] == 0) ? lcol_env[0] - '0' : 1;
+    const char* lorn_env = getenv("SIEB200_TF32_LO_RN");
+    st->lo_rn = (lorn_env && lorn_env[0] == '1') ? 1 : 0;
+    st->diag_split = diag_split_env();
+    st->diag_panels = diag_panels_env();
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -1229,12 +1450,21 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_diag, cudaEventDisableTiming));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_pan, cudaEventDisableTiming));
     }
+    if (!st->side2) {
+        int least = 0, greatest = 0;
+        SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side2, cudaStreamNonBlocking, greatest));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_lcol, cudaEventDisableTiming));
+    }
 
     static bool attrs_set = false;
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiagUpd));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagUpd));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagUpd));
         attrs_set = true;
     }
 
@@ -1242,7 +1472,9 @@ int mixed_factorize(DenseSolver* s) {
     MixedState::GraphKey key;
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
-    key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo; key.sms = gemm_sms;
+    key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo + 8 * st->lcol + 16 * st->lo_rn + 32 * st->diag_split +
+                 64 * st->diag_panels;
+    key.sms = gemm_sms;
     key.ovl = ((int64_t)st->pair_min << 32) | (int64_t)(st->ovl_min * 1000 + st->ovl_sms);
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
@@ -1317,7 +1549,14 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + nupd * 8.0 * NB * NB * NB,
                         8.0 * NB * NB * (3.0 + 2.0 * nupd), &ev);
-        diag_lu_kernel<float2><<<1, kDiagThreads, kSmemDiagUpd, sm>>>(
+        if (nupd > 0 && st->diag_split) {
+            diag_update_kernel<float2><<<dim3(NB / 16, NB / 16), 256, 0, sm>>>(st->W, ldw, k0, kb, kp1, kp2);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+            kp1 = kp2 = -1;
+        }
+        (st->diag_panels ? diag_lu_kernel<float2, true> : diag_lu_kernel<float2, false>)<<<1, kDiagThreads,
+                                                                                            kSmemDiagUpd, sm>>>(
             st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB, st->Uinv + (size_t)bk * NB * NB, st->err, kp1, kp2);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
@@ -1362,6 +1601,7 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         pa.nL = (int)blocks_for(m, 32);
         pa.pack = st->use_tc;
         pa.kp[0] = kp1; pa.kp[1] = kp2; pa.kpu = kpu;
+        pa.lo_rn = st->lo_rn;
         if (pair_at(bk)) {
             const int half = (int)(bk & 1);
             const int64_t q_s0 = half ? s0 : s0 + NB;  // s0 of the step whose GEMM uses this pack
@@ -1386,16 +1626,17 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         SIEB_TRY_CUDA(cudaGetLastError());
         return SIEB200_OK;
     };
+    // shift: the first block row (128 real rows) starts that many columns in
     auto gemm = [&](int64_t s0, int64_t c0, int64_t ncols, const float* A, const float* B, int K,
-                    int max_ctas) -> int {
+                    int max_ctas, int64_t shift) -> int {
         const int64_t m = np - s0;
         float* C = reinterpret_cast<float*>(st->W + s0 + c0 * ldw);
         cudaEvent_t ev;
         // tensor work: three products of K/3 (one sweep) or K/2 (split) columns
         const double keff = hilo ? 1.5 * K : (double)K;
-        ctx->prof.begin(stream, 0, 2.0 * (2.0 * m) * ncols * keff,
-                        4.0 * (2.0 * (2.0 * m) * ncols + (2.0 * m + ncols) * K), &ev);
-        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K, max_ctas, layout));
+        const double elems = (2.0 * m) * ncols - (double)std::min<int64_t>(128, 2 * m) * shift;
+        ctx->prof.begin(stream, 0, 2.0 * elems * keff, 4.0 * (2.0 * elems + (2.0 * m + ncols) * K), &ev);
+        SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * ldw, A, B, 2 * m, ncols, K, max_ctas, layout, shift));
         ctx->prof.end(stream, ev);
         return SIEB200_OK;
     };
@@ -1407,10 +1648,24 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // side stream while the tensor-core trailing update runs here; then the
     // next panels, which apply the pending updates to the next block's
     // column (and, in the pair schedule after an even step, to its row).
-    // The trailing update skips the next block column; in the pair schedule
-    // it runs after odd steps only, for both steps of the pair at once
-    // (half the C traffic per flop). The persistent GEMM leaves one SM to the
-    // diagonal kernel (whose shared memory keeps it off the GEMM's SMs).
+    // In a single step the trailing update skips only the next diagonal
+    // block (the side stream factors it meanwhile): its first block row
+    // starts one block column further right and its other rows cover the
+    // next block column too, so the next L21 panel is only a triangular
+    // product (SIEB200_GEMM_LCOL=1, default). On the 6016-unknown system
+    // this takes the factorization from 6.93 to 5.99 ms (with the diagonal
+    // block's update in its own kernel). That column's last update then
+    // comes from TF32 products accumulated on the tensor cores instead of
+    // FP32 FMAs, and the 17280-unknown GSTC batch needs a sixth refinement
+    // iteration (about 20 of 235 ms). The alternatives keep the FP32 update
+    // (same factors as the panels, bit for bit): =0 the panels apply it,
+    // =2 col_update_kernel on a third stream beside the GEMM (its CTAs
+    // crowd the diagonal kernel's SM: 6.7-6.9 ms), =3 col_update_kernel
+    // ahead of the GEMM (6.72 ms); the GEMM then skips the whole next block
+    // column. In the pair schedule the update skips the next block column
+    // and runs after odd steps only, for both steps of the pair at once
+    // (half the C traffic per flop). The persistent GEMM leaves one SM to
+    // the diagonal kernel (whose shared memory keeps it off the GEMM's SMs).
     // The single-step schedule is the default (SIEB200_PAIR_UPDATE=1 selects
     // the pair schedule): on the 6016-unknown system the pair schedule's
     // GEMM runs at 360 TFLOP/s against 297, but the steps without a GEMM put
@@ -1446,25 +1701,56 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             if (ovl) {
                 const int octas = std::max(1, std::min(gemm_ctas, ctx->sm_count - st->ovl_sms));
                 SIEB_RETURN_IF(gemm(s0 + n1, s0 + n1, m - n1, st->Apack[bk & 1] + 2 * n1 * KS,
-                                    st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, octas));
+                                    st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, octas, 0));
                 SIEB_RETURN_IF(panels(bk + 1, k0, -1, k0, st->side));
                 SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
                 pan_side = true;
                 continue;
             }
+            const bool pan_was_side = pan_side;
             pan_side = false;
             SIEB_TRY_CUDA(cudaEventRecord(st->ev_diag, st->side));
+            // lcol 1: the GEMM covers the next block column below its
+            // diagonal block; lcol 2: col_update_kernel does, on the
+            // third stream beside the GEMM (which skips that column);
+            // lcol 3: col_update_kernel on this stream before the GEMM
+            const bool lcol = !pair && st->lcol == 1;
+            const bool lside = !pair && st->lcol == 2;
+            const bool lmain = !pair && st->lcol == 3;
+            if (lmain && m > n1) {  // lcol 3: the same kernel here, ahead of the GEMM, on the whole GPU
+                col_update_kernel<<<(unsigned)blocks_for(m - n1, 32), 256, 0, stream>>>(st->W, ldw, s0, (int)n1,
+                                                                                       s0 + n1, np, k0);
+                SIEB_NOTE_LAUNCH();
+                SIEB_TRY_CUDA(cudaGetLastError());
+            }
+            if (lside && m > n1) {
+                // after panels (stream order of the context stream, or the
+                // side stream after an overlapped step)
+                SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side2, st->ev_cols, 0));
+                if (pan_was_side) SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side2, st->ev_pan, 0));
+                col_update_kernel<<<(unsigned)blocks_for(m - n1, 32), 256, 0, st->side2>>>(st->W, ldw, s0, (int)n1,
+                                                                                           s0 + n1, np, k0);
+                SIEB_NOTE_LAUNCH();
+                SIEB_TRY_CUDA(cudaGetLastError());
+                SIEB_TRY_CUDA(cudaEventRecord(st->ev_lcol, st->side2));
+            }
             if (!pair) {
-                if (m > n1)
+                if (m > n1 && lcol)
+                    SIEB_RETURN_IF(gemm(s0, s0, m, st->Apack[bk & 1], st->Bpack + (bk & 1) * np * KS, (int)KS,
+                                        gemm_ctas, n1));
+                else if (m > n1)
                     SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[bk & 1],
-                                        st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, gemm_ctas));
+                                        st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, gemm_ctas, 0));
             } else if (odd && m > n1) {
-                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas));
+                SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas, 0));
             }
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
-            // after an even step of the pair schedule the next block row
-            // has not had this step's update yet
-            SIEB_RETURN_IF(panels(bk + 1, k0, kprev, pair && !odd ? k0 : -1, stream));
+            if (lside && m > n1) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_lcol, 0));
+            // The next L21 rows take this step's update themselves unless
+            // the GEMM or col_update_kernel applied it (lcol, lside); after
+            // an even step of the pair schedule the next block row has not
+            // had it either.
+            SIEB_RETURN_IF(panels(bk + 1, (lcol || lside || lmain) ? -1 : k0, kprev, pair && !odd ? k0 : -1, stream));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
@@ -1869,6 +2155,8 @@ static int fp64_factorize(DenseSolver* s) {
     st->Uinv64 = reinterpret_cast<double2*>(base + up(bW) + up(bInv));
     st->diag = reinterpret_cast<double*>(base + up(bW) + 2 * up(bInv));
     st->err = reinterpret_cast<unsigned*>(base + up(bW) + 2 * up(bInv) + up(bDiag));
+    st->diag_split = diag_split_env();
+    st->diag_panels = diag_panels_env();
     if (!st->side) {
         int least = 0, greatest = 0;
         SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -1881,7 +2169,9 @@ static int fp64_factorize(DenseSolver* s) {
     if (!attrs64) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kSmemPanel64));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagUpd64));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kSmemDiagUpd64));
         attrs64 = true;
     }
@@ -1900,7 +2190,14 @@ static int fp64_factorize(DenseSolver* s) {
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, (16.0 / 3.0) * NB * NB * NB + (kp >= 0 ? 8.0 * NB * NB * NB : 0.0), 0.0, &ev);
-        diag_lu_kernel<double2><<<1, kDiagThreads, kSmemDiagUpd64, sm>>>(
+        if (kp >= 0 && st->diag_split) {
+            diag_update_kernel<double2><<<dim3(NB / 16, NB / 16), 256, 0, sm>>>(st->W64, ldw, k0, kb, kp, -1);
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+            kp = -1;
+        }
+        (st->diag_panels ? diag_lu_kernel<double2, true> : diag_lu_kernel<double2, false>)<<<1, kDiagThreads,
+                                                                                              kSmemDiagUpd64, sm>>>(
             st->W64, ldw, k0, kb, st->Linv64 + (size_t)bk * NB * NB, st->Uinv64 + (size_t)bk * NB * NB, st->err, kp,
             -1);
         SIEB_NOTE_LAUNCH();

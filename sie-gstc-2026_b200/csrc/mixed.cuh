@@ -34,6 +34,12 @@ struct MixedState {
     int pair_min = 0;           // pair schedule for steps whose paired GEMM is at least this wide
     int ovl_min = 0;            // overlap the next panels with GEMMs at least this wide (0: off)
     int ovl_sms = 20;           // SMs the overlapped GEMMs leave to the panels
+    int lcol = 1;               // single steps: the next block column below its diagonal block takes the
+                                // step's update from the panels (0), the GEMM (1, TF32) or col_update_kernel
+                                // (FP32) on the third stream (2) or ahead of the GEMM (3)
+    int lo_rn = 0;              // split packs: lo parts rounded to the nearest TF32 (else truncated by the MMA)
+    int diag_split = 1;         // diagonal blocks take their update in a 16-CTA kernel ahead of the LU kernel
+    int diag_panels = 0;        // diagonal-block elimination synchronised per panel of 8 steps, not per step
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
@@ -50,6 +56,8 @@ struct MixedState {
     CUtensorMap tmWH;
     cudaStream_t side = nullptr;           // high-priority stream of the lookahead panel
     cudaEvent_t ev_cols = nullptr, ev_diag = nullptr, ev_pan = nullptr;
+    cudaStream_t side2 = nullptr;          // third stream: the next block column's update beside the GEMM
+    cudaEvent_t ev_lcol = nullptr;
     // The factorization's launches as one CUDA graph (both streams and the
     // event edges between them), captured on the second call with an
     // unchanged key and replayed while it stays so; not while the profiler
@@ -138,6 +146,12 @@ __device__ __forceinline__ float tf32_hi(float x) {
     uint32_t y;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
     return __uint_as_float(y);
+}
+// The remainder x - hi of the split: rounded to the nearest TF32 (rn != 0),
+// or left in FP32, whose last 13 mantissa bits the tensor core ignores.
+__device__ __forceinline__ float tf32_lo(float x, float hi, int rn) {
+    const float l = x - hi;
+    return rn ? tf32_hi(l) : l;
 }
 
 // Multi-right-hand-side solve with the mixed factors (block_solve.cu).

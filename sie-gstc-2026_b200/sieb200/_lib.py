@@ -139,6 +139,8 @@ _SIGNATURES = {
     "sieb200_prepare_records": ([_P, _I64, _P, ctypes.c_double, _P, _P], ctypes.c_int),
     "sieb200_zgemm": ([_P, _I64, _I64, _I64, _P, _I64, _P, _I64, _P, _I64, _P, _P], ctypes.c_int),
     "sieb200_gemm_tf32_sub": ([_P, _I64, _I64, ctypes.c_int, _P, _P, _P, _I64, ctypes.c_int], ctypes.c_int),
+    "sieb200_gemm_tf32_sub_shifted": ([_P, _I64, _I64, ctypes.c_int, _P, _P, _P, _I64, ctypes.c_int, _I64],
+                                      ctypes.c_int),
     "sieb200_far_field": ([_P, ctypes.POINTER(Mesh), _P, _P, ctypes.c_double, ctypes.c_double, _I64,
                            _P, _P, _P, _P, _P, _P], ctypes.c_int),
 }

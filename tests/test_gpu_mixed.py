@@ -84,6 +84,59 @@ def test_gemm_tf32_sub_split_operands(mode, m2, n, K, slots, gpu_ctx, monkeypatc
     assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
 
 
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("m2,n,shift", [(256, 128, 64), (384, 448, 64), (1000, 517, 64), (300, 200, 137),
+                                        (4096, 1600, 64)])
+def test_gemm_tf32_sub_shifted(mode, m2, n, shift, gpu_ctx):
+    """The first 128 rows of C take columns [shift, n) only (the trailing
+    update that leaves the next diagonal block alone); the other rows take
+    all n. (384, 448, 64) and (4096, 1600, 64) leave the first row tile's
+    last column tile wholly past n (448 - 64 and 1600 - 64 fit in one tile
+    fewer), which the kernels skip. Every mode, plain (0-3, K = 384) and
+    split (4-5, K = 256) operands; tolerance 1e-5 as above, the untouched
+    block bit-exact."""
+    import torch
+    from sieb200 import _lib
+    rng = np.random.default_rng(m2 + n + shift + mode)
+    if mode >= 4:
+        K = 256
+        A32 = rng.standard_normal((m2, K // 2)).astype(np.float32)
+        B32 = rng.standard_normal((n, K // 2)).astype(np.float32)
+        Ah, Bh = _tf32(A32), _tf32(B32)
+        A = np.concatenate([Ah, A32 - Ah], axis=1)
+        B = np.concatenate([Bh, B32 - Bh], axis=1)
+        prod = A32.astype(np.float64) @ B32.astype(np.float64).T
+    else:
+        K = 384
+        A = _tf32(rng.standard_normal((m2, K)))
+        B = _tf32(rng.standard_normal((n, K)))
+        prod = A.astype(np.float64) @ B.astype(np.float64).T
+    ldc = m2 + 8
+    C = rng.standard_normal((n, ldc)).astype(np.float32)
+    dA, dB, dC = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (A, B, C))
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().sieb200_gemm_tf32_sub_shifted(gpu_ctx.handle, m2, n, K, dA.data_ptr(), dB.data_ptr(),
+                                                         dC.data_ptr(), ldc, mode, shift))
+    out = dC.cpu().numpy()
+    ref = C.astype(np.float64).copy()
+    ref[:, :m2] -= prod.T
+    r1 = min(128, m2)
+    ref[:shift, :r1] = C[:shift, :r1]
+    assert np.array_equal(out[:shift, :r1], C[:shift, :r1])  # the skipped block
+    assert rel_err(out[:, :m2], ref[:, :m2]) < 1e-5
+    assert np.array_equal(out[:, m2:], C[:, m2:])  # padding rows untouched
+
+
+def test_gemm_shift_out_of_range_refused(gpu_ctx):
+    import torch
+    import sieb200
+    from sieb200 import _lib
+    d = torch.zeros(256 * 128, device="cuda")
+    with pytest.raises(sieb200.SiebError):
+        _lib.check(_lib.lib().sieb200_gemm_tf32_sub_shifted(gpu_ctx.handle, 256, 128, 256, d.data_ptr(),
+                                                             d.data_ptr(), d.data_ptr(), 256, 3, 128))
+
+
 def _pmchwt(level=2, solver="lu_cusolver", rule=5):
     import sieb200
     m = sieb200.icosphere(0.5, level)
@@ -93,9 +146,15 @@ def _pmchwt(level=2, solver="lu_cusolver", rule=5):
 
 
 @pytest.mark.parametrize("trailing", ["tc", "tc_pair", "tc_three_product", "tc_load_store", "tc_reduce",
-                                      "tc_overlap", "simt"])
+                                      "tc_overlap", "tc_no_lcol", "tc_lcol_gemm", "tc_simt_gemm", "simt"])
 def test_mixed_solver_matches_fp64(trailing, gpu_ctx, monkeypatch):
     import sieb200
+    if trailing == "tc_no_lcol":  # the next panels update the next block column
+        monkeypatch.setenv("SIEB200_GEMM_LCOL", "0")
+    if trailing == "tc_lcol_gemm":  # the GEMM does, its first block row shifted
+        monkeypatch.setenv("SIEB200_GEMM_LCOL", "1")
+    if trailing == "tc_simt_gemm":  # GEMM mode 0 on the same packs and shapes
+        monkeypatch.setenv("SIEB200_GEMM_MODE", "0")
     if trailing == "simt":
         monkeypatch.setenv("SIEB200_TRAILING_SIMT", "1")
     if trailing == "tc_pair":
@@ -164,13 +223,18 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
 
 
 @pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three",
-                                      "single_split_overlap", "single_split_trsv64", "pair_then_single"])
+                                      "single_split_overlap", "single_split_trsv64", "pair_then_single",
+                                      "single_split_no_lcol", "single_split_lcol_gemm",
+                                      "single_split_lcol_side"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
     sub-block, and fewer rows than one block, under both trailing-update
     schedules (pair / single step), both pack layouts (split [hi | lo] /
-    three-product), with overlapped steps (panels beside the GEMM), with
+    three-product), the next block column's update in single steps from the
+    column kernel before the GEMM (default) or beside it, the GEMM or the
+    panels,
+    with overlapped steps (panels beside the GEMM), with
     64-row triangular-solve CTAs, and switching from the pair to the single
     schedule part way. One preconditioned step must already reach 1e-5 (the
     factors are single precision), and the full refinement 1e-12: a wrong
@@ -188,6 +252,12 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     monkeypatch.setenv("SIEB200_OVERLAP_SMS", "16")
     # triangular solves with 64-row CTAs (one sub-block each) or 128-row ones
     monkeypatch.setenv("SIEB200_TRSV_ROWS", "64" if schedule.endswith("trsv64") else "128")
+    # who updates the next block column below its diagonal block in a single
+    # step: the next panels (0), the GEMM (1), col_update_kernel on the third
+    # stream (2) or before the GEMM (3, default)
+    monkeypatch.setenv("SIEB200_GEMM_LCOL", "0" if schedule.endswith("no_lcol")
+                       else "1" if schedule.endswith("lcol_gemm")
+                       else "2" if schedule.endswith("lcol_side") else "3")
     rng = np.random.default_rng(n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
@@ -208,6 +278,51 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     xs = x.cpu().numpy()
     assert np.linalg.norm(A @ xs - b) / np.linalg.norm(b) <= 1e-12
     s.close()
+
+
+_CHAIN_VARIANTS = {
+    # (SIEB200_GEMM_LCOL, SIEB200_DIAG_SPLIT, SIEB200_DIAG_PANELS)
+    "default": ("3", "1", "0"),
+    "panel_updates_column": ("0", "1", "0"),
+    "column_update_third_stream": ("2", "1", "0"),
+    "fused_diag_update": ("3", "0", "0"),
+    "diag_barrier_per_panel": ("3", "1", "1"),
+    "all_previous": ("0", "0", "0"),
+}
+
+
+@pytest.mark.parametrize("n", [64, 200, 1000, 2100])
+def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
+    """The chain variants only move work between kernels and streams: the
+    next block column's update by col_update_kernel (before the GEMM or on
+    a third stream beside it) or by the panels, the diagonal block's update
+    by diag_update_kernel or inside the LU kernel, and the elimination with
+    a barrier per step or per panel all run the
+    same FP32 operations in the same order, so the factors, and with them
+    the one-step solution, are the same bit for bit."""
+    import torch
+    import sieb200
+    rng = np.random.default_rng(300 + n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()
+    monkeypatch.setenv("SIEB200_PAIR_MIN", "0")
+    out = {}
+    for name, (lcol, split, panels) in _CHAIN_VARIANTS.items():
+        monkeypatch.setenv("SIEB200_GEMM_LCOL", lcol)
+        monkeypatch.setenv("SIEB200_DIAG_SPLIT", split)
+        monkeypatch.setenv("SIEB200_DIAG_PANELS", panels)
+        s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+        s.factorize(Z.data_ptr())
+        x = torch.from_numpy(b.copy()).cuda()
+        torch.cuda.synchronize()
+        s.solve(x.data_ptr(), tolerance=1e-5, max_iterations=1)
+        gpu_ctx.synchronize()
+        out[name] = x.cpu().numpy()
+        s.close()
+    assert np.linalg.norm(A @ out["default"] - b) / np.linalg.norm(b) <= 1e-5
+    for name, xs in out.items():
+        assert np.array_equal(xs, out["default"]), name
 
 
 @pytest.mark.parametrize("rows", ["128", "64"])
