@@ -49,7 +49,7 @@ WORKLOAD = ("T-PMCHWT dielectric sphere r=0.5 m, eps_r=4, mu_r=1, ka=pi; geodesi
 # DRAM bytes (read + write) per trailing-update launch, mean over the 92
 # launches of one factorization of this workload, from one ncu capture of
 # the trailing GEMM (dram__bytes_read.sum + dram__bytes_write.sum).
-GEMM_DRAM_BYTES_PER_LAUNCH = 155.5e6
+GEMM_DRAM_BYTES_PER_LAUNCH = 158.4e6
 # FP64 flops per Green evaluation (one point pair, one wavenumber) of the
 # T-PMCHWT regular pass, counted from the kernel's source with an FMA as 2:
 # the point-pair geometry shared by the two wavenumbers (distance, r_p.r_q,
@@ -935,8 +935,8 @@ def multi_rhs_section(ctx, fp64_peak: float, max_over_ranks) -> dict:
         "block_trsm": {"launches_of_applications": trsm["launches"],
                        "tf32_tflops": tri_tflops,
                        "packed_factor_gbs": trsm["bytes"] / (trsm["ms"] / 1e3) / 1e9 if trsm["ms"] > 0 else None,
-                       "work_note": f"24 np^2 nrhs TF32 flops and 48 np^2 bytes of packed factors per "
-                                    f"application, np={np_}"},
+                       "work_note": f"24 np^2 nrhs TF32 flops and 32 np^2 bytes of split [hi | lo] packed "
+                                    f"factors per application, np={np_}"},
         "fp64_gemm": {"launches": gemm64["launches"],
                       "tflops": gemm64["flops"] / (gemm64["ms"] / 1e3) / 1e12 if gemm64["ms"] > 0 else None,
                       "peak_tflops": fp64_peak,

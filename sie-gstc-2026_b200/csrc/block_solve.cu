@@ -12,11 +12,13 @@
 //     then the rest of Y takes the block's contribution as one split-TF32
 //     tcgen05 GEMM, Y[rows] -= L[rows, k] X_k (lower) or U[rows, k] X_k
 //     (upper), with FP32 accumulation: 3 products hi*hi + hi*lo + lo*hi
-//     along K = 3 * 128 (the realified complex columns);
+//     of K = 128 (the realified complex columns) from split [hi | lo]
+//     operands, each read once per tile;
 //   * the GEMM's A operands (realified split rows of every L21 and every
 //     column block of U above the diagonal) are packed from the factors once
-//     per factorization, 48 np^2 bytes; when they do not fit, the caller
-//     solves column by column instead.
+//     per factorization, 32 np^2 bytes (48 np^2 with the three-product
+//     layout [hi | hi | lo], SIEB200_BLOCK_HILO=0); when they do not fit, the
+//     caller solves column by column instead.
 // FGMRES: every column keeps its own Krylov space (classical Gram-Schmidt
 // twice, Givens rotations on the host), but the columns advance in lockstep,
 // so each iteration is one multi-column preconditioner application and one
@@ -37,6 +39,7 @@ namespace sieb200 {
 struct BlockSolveState {
     int64_t np = 0, nbl = 0, ldy = 0;
     int nrhs_cap = 0;
+    int kw = 0;           // pack width: KH (split [hi | lo], default) or K3 (SIEB200_BLOCK_HILO=0)
     DeviceBuffer packs;   // L packs | U packs (fp32)
     DeviceBuffer work;    // Y (np x nrhs c64) | Xpack (nrhs x 384 fp32)
     DeviceBuffer krylov;  // FP64 FGMRES vectors
@@ -52,9 +55,9 @@ struct BlockSolveState {
         const void* packs = nullptr;
         const void* W = nullptr;
         int64_t np = 0;
-        int nrhs = 0;
+        int nrhs = 0, kw = 0;
         bool operator==(const Key& o) const {
-            return Y == o.Y && packs == o.packs && W == o.W && np == o.np && nrhs == o.nrhs;
+            return Y == o.Y && packs == o.packs && W == o.W && np == o.np && nrhs == o.nrhs && kw == o.kw;
         }
     };
     Key graph_key, seen_key;
@@ -66,7 +69,8 @@ struct BlockSolveState {
 
 namespace {
 
-constexpr int K3 = 6 * NB;  // packed K: [hi | hi | lo] (A) or [hi | lo | hi] (B) of 2 NB reals
+constexpr int K3 = 6 * NB;  // three-product packs: [hi | hi | lo] (A) or [hi | lo | hi] (B) of 2 NB reals
+constexpr int KH = 4 * NB;  // split packs: [hi | lo] of 2 NB reals (A and B)
 
 __host__ __device__ inline int64_t lower_pack_rows_before(int64_t k, int64_t np) {
     // sum over j < k of (np - NB (j + 1)): rows below diagonal block j
@@ -82,10 +86,11 @@ __host__ __device__ inline int64_t upper_pack_rows_before(int64_t k) {
 // of U[0:k0, k] (grid.z = 1), 32 rows per CTA (grid.x), staged through
 // shared memory so that both the column reads and the K-major row writes
 // are coalesced. Row 2r: [Re, -Im] per column, row 2r + 1: [Im, Re];
-// layout [hi | hi | lo] along K; columns beyond the block's width are zero.
+// layout [hi | lo] along K (kw = KH) or [hi | hi | lo] (kw = K3); columns
+// beyond the block's width are zero.
 __global__ void __launch_bounds__(256) pack_factors_kernel(const float2* __restrict__ W, int64_t ldw, int64_t np,
                                                            float* __restrict__ Lp, float* __restrict__ Up,
-                                                           int lo_rn) {
+                                                           int kw, int lo_rn) {
     __shared__ float2 tile[32][NB + 1];
     const int64_t k = blockIdx.y;
     const int64_t k0 = k * NB;
@@ -95,7 +100,7 @@ __global__ void __launch_bounds__(256) pack_factors_kernel(const float2* __restr
     const int64_t r_end = upper ? k0 : np;
     const int64_t rb = r_begin + (int64_t)blockIdx.x * 32;
     if (rb >= r_end) return;
-    float* base = upper ? Up + 2 * upper_pack_rows_before(k) * K3 : Lp + 2 * lower_pack_rows_before(k, np) * K3;
+    float* base = upper ? Up + 2 * upper_pack_rows_before(k) * kw : Lp + 2 * lower_pack_rows_before(k, np) * kw;
     const int tid = threadIdx.x;
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % 32, c = e / 32;
@@ -112,10 +117,16 @@ __global__ void __launch_bounds__(256) pack_factors_kernel(const float2* __restr
         const float v0 = h == 0 ? v.x : -v.y;
         const float v1 = h == 0 ? v.y : v.x;
         const float h0 = tf32_hi(v0), h1 = tf32_hi(v1);
-        float* row0 = base + (2 * (gr - r_begin)) * K3;
-        float* row1 = row0 + K3;
-        row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = tf32_lo(v0, h0, lo_rn);
-        row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = tf32_lo(v1, h1, lo_rn);
+        float* row0 = base + (2 * (gr - r_begin)) * kw;
+        float* row1 = row0 + kw;
+        const float l0 = tf32_lo(v0, h0, lo_rn), l1 = tf32_lo(v1, h1, lo_rn);
+        if (kw == KH) {
+            row0[kk] = h0; row0[2 * NB + kk] = l0;
+            row1[kk] = h1; row1[2 * NB + kk] = l1;
+        } else {
+            row0[kk] = h0; row0[2 * NB + kk] = h0; row0[4 * NB + kk] = l0;
+            row1[kk] = h1; row1[2 * NB + kk] = h1; row1[4 * NB + kk] = l1;
+        }
     }
 }
 
@@ -178,7 +189,8 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
                                                          int nrhs, const float2* __restrict__ Inv,
                                                          float* __restrict__ Xpack,
                                                          const float2* __restrict__ Fb, int64_t ldf,
-                                                         const float2* __restrict__ Xprev, int kbp, int lo_rn) {
+                                                         const float2* __restrict__ Xprev, int kbp, int kw,
+                                                         int lo_rn) {
     extern __shared__ __align__(16) float2 da_smem[];
     float2(*inv)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(da_smem);              // [row][col]
     float2(*fb)[NB + 1] = inv + NB;                                                    // [row][col]
@@ -235,7 +247,7 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
     }
     const int gc = c0 + c;
     if (gc >= nrhs) return;
-    float* col = Xpack + (int64_t)gc * K3;
+    float* col = Xpack + (int64_t)gc * kw;  // [hi | lo] (KH) or [hi | lo | hi] (K3)
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         const int r = r0 + u;
@@ -245,7 +257,7 @@ __global__ void __launch_bounds__(256) diag_apply_kernel(float2* __restrict__ Y,
         const float h0 = tf32_hi(vx), h1 = tf32_hi(vy);
         col[2 * r] = h0; col[2 * r + 1] = h1;
         col[2 * NB + 2 * r] = tf32_lo(vx, h0, lo_rn); col[2 * NB + 2 * r + 1] = tf32_lo(vy, h1, lo_rn);
-        col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1;
+        if (kw == K3) { col[4 * NB + 2 * r] = h0; col[4 * NB + 2 * r + 1] = h1; }
     }
 }
 
@@ -624,8 +636,12 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
     const int64_t np = st->np, nbl = st->nbl;
     const int64_t l_rows = lower_pack_rows_before(nbl - 1, np);  // every L21 (the last block has none)
     const int64_t u_rows = upper_pack_rows_before(nbl);
-    const size_t bL = sizeof(float) * 2 * (size_t)l_rows * K3;
-    const size_t bU = sizeof(float) * 2 * (size_t)u_rows * K3;
+    const char* hilo_env = getenv("SIEB200_BLOCK_HILO");
+    const int kw = (hilo_env && hilo_env[0] == '0') ? K3 : KH;
+    if (kw != bs->kw) bs->packed = false;
+    bs->kw = kw;
+    const size_t bL = sizeof(float) * 2 * (size_t)l_rows * kw;
+    const size_t bU = sizeof(float) * 2 * (size_t)u_rows * kw;
     const size_t need = ((bL + 255) / 256) * 256 + bU;
     if (bs->packs.bytes < need) {
         size_t free_b = 0, total_b = 0;
@@ -643,7 +659,7 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
     bs->Up = reinterpret_cast<float*>(bs->packs.as<char>() + ((bL + 255) / 256) * 256);
     const int64_t ldy = ((np + 31) / 32) * 32;
     const size_t bY = ((sizeof(float2) * (size_t)ldy * nrhs + 255) / 256) * 256;
-    SIEB_RETURN_IF(bs->work.reserve(bY + 2 * sizeof(float) * (size_t)nrhs * K3));  // two Xpack buffers
+    SIEB_RETURN_IF(bs->work.reserve(bY + 2 * sizeof(float) * (size_t)nrhs * kw));  // two Xpack buffers
     if (!bs->ev_fork) {
         for (cudaEvent_t* e : {&bs->ev_fork, &bs->ev_join, &bs->ev_x[0], &bs->ev_x[1], &bs->ev_b[0], &bs->ev_b[1]})
             SIEB_TRY_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
@@ -658,7 +674,7 @@ static int prepare(DenseSolver* s, MixedState* st, int nrhs, bool* fits) {
     // The packs are built once per factorization (which clears `packed`).
     if (!bs->packed) {
         const dim3 grid(nblk(np, 32), (unsigned)nbl, 2);
-        pack_factors_kernel<<<grid, 256, 0, s->ctx->stream>>>(st->W, st->ldw, np, bs->Lp, bs->Up, st->lo_rn);
+        pack_factors_kernel<<<grid, 256, 0, s->ctx->stream>>>(st->W, st->ldw, np, bs->Lp, bs->Up, kw, st->lo_rn);
         SIEB_NOTE_LAUNCH();
         SIEB_TRY_CUDA(cudaGetLastError());
         bs->packed = true;
@@ -685,21 +701,22 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
     const unsigned gda = nblk(nrhs, DA_COLS);
     const char* la_env = getenv("SIEB200_BLOCK_LOOKAHEAD");
     const bool la = la_env && la_env[0] == '1' && st->side != nullptr;
-    float* Xbuf[2] = {bs->Xpack, bs->Xpack + (size_t)nrhs * K3};
+    const int kw = bs->kw, layout = kw == KH ? 1 : 0;
+    float* Xbuf[2] = {bs->Xpack, bs->Xpack + (size_t)nrhs * kw};
     if (!la) {
         for (int64_t k = 0; k < nbl; ++k) {
             const int64_t k0 = k * NB;
             const int kb = (int)std::min<int64_t>(NB, np - k0);
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
                                                                      st->Linv + (size_t)k * NB * NB, Xbuf[0],
-                                                                     nullptr, 0, nullptr, 0, st->lo_rn);
+                                                                     nullptr, 0, nullptr, 0, kw, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             const int64_t s0 = k0 + kb;
             if (s0 < np) {
-                const float* A = bs->Lp + 2 * lower_pack_rows_before(k, np) * K3;
+                const float* A = bs->Lp + 2 * lower_pack_rows_before(k, np) * kw;
                 SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y + s0), 2 * bs->ldy, A,
-                                           Xbuf[0], 2 * (np - s0), nrhs, K3, 0));
+                                           Xbuf[0], 2 * (np - s0), nrhs, kw, 0, layout));
             }
         }
         for (int64_t k = nbl - 1; k >= 0; --k) {
@@ -707,13 +724,13 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             const int kb = (int)std::min<int64_t>(NB, np - k0);
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, stream>>>(bs->Y, bs->ldy, k0, kb, nrhs,
                                                                      st->Uinv + (size_t)k * NB * NB, Xbuf[0],
-                                                                     nullptr, 0, nullptr, 0, st->lo_rn);
+                                                                     nullptr, 0, nullptr, 0, kw, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             if (k0 > 0) {
-                const float* A = bs->Up + 2 * upper_pack_rows_before(k) * K3;
+                const float* A = bs->Up + 2 * upper_pack_rows_before(k) * kw;
                 SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, reinterpret_cast<float*>(bs->Y), 2 * bs->ldy, A,
-                                           Xbuf[0], 2 * k0, nrhs, K3, 0));
+                                           Xbuf[0], 2 * k0, nrhs, kw, 0, layout));
             }
         }
         return SIEB200_OK;
@@ -742,7 +759,7 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             }
             diag_apply_kernel<<<gda, 256, kSmemDiagApply, side>>>(
                 bs->Y, bs->ldy, k0, kb, nrhs, (pass == 0 ? st->Linv : st->Uinv) + (size_t)k * NB * NB, Xk, Fb,
-                st->ldw, Xprev, kbp, st->lo_rn);
+                st->ldw, Xprev, kbp, kw, st->lo_rn);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             SIEB_TRY_CUDA(cudaEventRecord(bs->ev_x[t & 1], side));
@@ -753,16 +770,16 @@ static int enqueue_triangular(DenseSolver* s, MixedState* st, BlockSolveState* b
             if (pass == 0) {
                 const int64_t s0 = k0 + kb, n1 = std::min<int64_t>(NB, np - s0);
                 rows = np - s0 - n1;
-                A = bs->Lp + 2 * (lower_pack_rows_before(k, np) + n1) * K3;
+                A = bs->Lp + 2 * (lower_pack_rows_before(k, np) + n1) * kw;
                 C = reinterpret_cast<float*>(bs->Y + s0 + n1);
             } else {
                 rows = k0 - NB;  // rows above the previous block
-                A = bs->Up + 2 * upper_pack_rows_before(k) * K3;
+                A = bs->Up + 2 * upper_pack_rows_before(k) * kw;
                 C = reinterpret_cast<float*>(bs->Y);
             }
             if (rows > 0) {
                 SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, bs->ev_x[t & 1], 0));
-                SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * bs->ldy, A, Xk, 2 * rows, nrhs, K3, cap));
+                SIEB_RETURN_IF(gemm_tc_sub(st->gemm, stream, C, 2 * bs->ldy, A, Xk, 2 * rows, nrhs, kw, cap, layout));
             }
             // recorded every step, so that the wait two steps later sees
             // this step's GEMM (or, without one, everything before it)
@@ -791,9 +808,9 @@ static int apply_block_precond(DenseSolver* s, MixedState* st, BlockSolveState* 
     SIEB_TRY_CUDA(cudaGetLastError());
     cudaEvent_t ev;
     ctx->prof.begin(stream, 5, 2.0 * 3.0 * 8.0 * (double)np * (double)np / 2.0 * nrhs,
-                    2.0 * (4.0 * 2.0 * K3 * (double)np * (double)np / (2.0 * NB)), &ev);
+                    2.0 * (4.0 * 2.0 * bs->kw * (double)np * (double)np / (2.0 * NB)), &ev);
     BlockSolveState::Key key;
-    key.Y = bs->Y; key.packs = bs->packs.ptr; key.W = st->W; key.np = np; key.nrhs = nrhs;
+    key.Y = bs->Y; key.packs = bs->packs.ptr; key.W = st->W; key.np = np; key.nrhs = nrhs; key.kw = bs->kw;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs && bs->graph && bs->graph_key == key) {

@@ -86,13 +86,16 @@ def _solve(A, B, method="mixed_ir", per_column=False, gpu_ctx=None):
     return X
 
 
+@pytest.mark.parametrize("packs", ["split", "three"])
 @pytest.mark.parametrize("lookahead", ["1", "0"])
 @pytest.mark.parametrize("n,nrhs", [(50, 2), (130, 7), (997, 64), (2100, 17), (4099, 33)])
-def test_block_solve_matches_numpy(n, nrhs, lookahead, gpu_ctx, monkeypatch):
+def test_block_solve_matches_numpy(n, nrhs, lookahead, packs, gpu_ctx, monkeypatch):
     """Block triangular solves with the lookahead (each diagonal block takes
     the previous step's update itself, beside the trailing GEMM on another
-    stream) and without (SIEB200_BLOCK_LOOKAHEAD=0)."""
+    stream) and without (SIEB200_BLOCK_LOOKAHEAD=0), on split [hi | lo]
+    packs (default) and on three-product packs (SIEB200_BLOCK_HILO=0)."""
     monkeypatch.setenv("SIEB200_BLOCK_LOOKAHEAD", lookahead)
+    monkeypatch.setenv("SIEB200_BLOCK_HILO", "0" if packs == "three" else "1")
     A = _system(n, n)
     rng = np.random.default_rng(n + 1)
     B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
@@ -105,15 +108,17 @@ def test_block_solve_matches_numpy(n, nrhs, lookahead, gpu_ctx, monkeypatch):
     assert np.linalg.norm(X - Xc) / np.linalg.norm(Xc) < 1e-9
 
 
-def test_block_solve_after_refactorization(gpu_ctx):
-    """The packed factors follow a new factorization of the same solver."""
+def test_block_solve_after_refactorization(gpu_ctx, monkeypatch):
+    """The packed factors follow a new factorization of the same solver, and
+    a change of pack layout between solves (the packs are rebuilt)."""
     import torch
     import sieb200
     n, nrhs = 700, 5
     rng = np.random.default_rng(3)
     B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
     s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
-    for seed in (1, 2, 1):
+    for seed, hilo in ((1, "1"), (2, "1"), (1, "0"), (1, "1")):
+        monkeypatch.setenv("SIEB200_BLOCK_HILO", hilo)
         A = _system(n, seed)
         dA, dB = _dev(A), _dev(B)
         torch.cuda.synchronize()
