@@ -889,6 +889,7 @@ int block_solve(DenseSolver* s, MixedState* st, int64_t nrhs64, double* Bd, int6
     SIEB_NOTE_LAUNCH();
     SIEB_RETURN_IF(fetch(stream, hh.data(), hd, sizeof(cplx) * nrhs));
     std::vector<double> bnorm(nrhs);
+    const double est_factor = gmres_est_factor();
     for (int c = 0; c < nrhs; ++c) {
         bnorm[c] = std::sqrt(std::max(hh[c].re, 0.0));
         SIEB_CHECK(bnorm[c] > 0 && std::isfinite(bnorm[c]), SIEB200_INVALID_ARG,
@@ -995,7 +996,7 @@ int block_solve(DenseSolver* s, MixedState* st, int64_t nrhs64, double* Bd, int6
                 gc[j + 1] = cx(-(conj_s * gj).re, -(conj_s * gj).im);
                 used[c] = j + 1;
                 const double est = std::hypot(gc[j + 1].re, gc[j + 1].im);
-                if (est <= 0.5 * tol * bnorm[c] || hn == 0.0) {
+                if (est <= est_factor * tol * bnorm[c] || hn == 0.0) {
                     active[c] = 0;  // converged within this cycle: no further directions
                 } else {
                     scale[c] = 1.0 / hn;

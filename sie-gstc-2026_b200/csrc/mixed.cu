@@ -62,6 +62,14 @@ static int diag_panels_env() {
     return (e && e[0] == '1') ? 1 : 0;
 }
 
+// SIEB200_DIAG_COMPACT=1: diag_steps_compact instead of the fully unrolled
+// elimination (11 % faster alone under ncu, 31.2 against 35.0 us, but the
+// factorization measured 6.05 against 5.98 ms at N = 6016 in situ).
+static int diag_compact_env() {
+    const char* e = getenv("SIEB200_DIAG_COMPACT");
+    return (e && e[0] == '1') ? 1 : 0;
+}
+
 static void drop_graphs(MixedState* st) {
     for (auto& g : st->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -295,7 +303,74 @@ __device__ __forceinline__ void diag_steps(T (&a)[kDiagCols][2], int bp, int w, 
     }
 }
 
-// The same steps, one panel of kDiagCols columns at a time: the warp that
+// diag_steps with the row half H a runtime value and the two non-owner
+// cases (columns left or right of the pivot block) in one code path through
+// warp-uniform selects: the same FMAs on the same values in the same order
+// (same results), in about a third of the instructions of the unrolled
+// code, whose fetch was the kernel's top stall (no_instruction).
+template <class T>
+__device__ __forceinline__ void diag_steps_compact(T (&a)[kDiagCols][2], int bp, int H, int w, int lane,
+                                                   T (*cbuf)[NB], T* rcps, unsigned* err) {
+    using R = typename RealOf<T>::type;
+    constexpr int CW = kDiagCols;
+    const bool left = w < bp;   // this warp's columns lie left of the pivot block
+    const bool keep0 = H != 0;  // rows 0..31 are above every pivot of this half
+#pragma unroll
+    for (int u = 0; u < CW; ++u) {
+        const int j = CW * bp + u, jl = j & 31, buf = u & 1;
+        const bool g0 = lane > j, g1 = lane + 32 > j;  // rows below the pivot
+        const T z = cmk<T>(0.f, 0.f);
+        if (w == bp) {  // publish c_j, then update this warp's other columns
+            const T piv = shfl_c(keep0 ? a[u][1] : a[u][0], jl);
+            const R pm = piv.x * piv.x + piv.y * piv.y;
+            const bool bad = !(pm > tiny_pivot(pm)) || !isfinite(pm);
+            if (bad && lane == 0) atomicCAS(err, 0u, 1u);
+            const R inv = bad ? R(0) : rcp_rn(pm);
+            const T rcp = cmk<T>(piv.x * inv, -piv.y * inv);
+            T ca0 = cmulf(a[u][0], rcp);
+            T ca1 = cmulf(a[u][1], rcp);
+            if (lane == jl) {
+                if (keep0) ca1 = z;
+                else ca0 = z;
+            }
+            cbuf[buf][lane] = ca0;
+            cbuf[buf][lane + 32] = ca1;
+            if (lane == 0) rcps[j] = rcp;
+            a[u][0] = g0 ? cnegf(ca0) : a[u][0];
+            a[u][1] = g1 ? cnegf(ca1) : a[u][1];
+            const T cl0 = g0 ? ca0 : z, cl1 = g1 ? ca1 : z;
+#pragma unroll
+            for (int v = 0; v < CW; ++v) {
+                if (v == u) continue;
+                const T x = shfl_c(keep0 ? a[v][1] : a[v][0], jl);
+                if (v < u) {
+                    a[v][0] = keep0 ? a[v][0] : cfmsf(a[v][0], cl0, x);
+                    a[v][1] = cfmsf(a[v][1], cl1, x);
+                } else {
+                    a[v][0] = cfmsf(a[v][0], ca0, x);
+                    a[v][1] = cfmsf(a[v][1], ca1, x);
+                }
+            }
+        }
+        __syncthreads();
+        if (w != bp) {
+            const T ca0 = cbuf[buf][lane], ca1 = cbuf[buf][lane + 32];
+            // left of the pivot block: rows below j only, and nothing in
+            // rows 0..31 once the pivots are in the lower half
+            const T k0 = left ? (g0 ? ca0 : z) : ca0;
+            const T k1 = left ? (g1 ? ca1 : z) : ca1;
+            const bool skip0 = left && keep0;
+#pragma unroll
+            for (int v = 0; v < CW; ++v) {
+                const T x = shfl_c(keep0 ? a[v][1] : a[v][0], jl);
+                a[v][0] = skip0 ? a[v][0] : cfmsf(a[v][0], k0, x);
+                a[v][1] = cfmsf(a[v][1], k1, x);
+            }
+        }
+    }
+}
+
+// The same steps, one panel of kDiagCols columns at a time: the warp that// The same steps, one panel of kDiagCols columns at a time: the warp that
 // owns columns [kDiagCols p, kDiagCols (p+1)) runs the panel's steps alone
 // (its own columns only, through shuffles), leaving each coefficient column
 // c_j in cbuf[j], and signals named barrier 1 + p without waiting on it
@@ -386,6 +461,182 @@ __device__ __forceinline__ void diag_panel(T (&a)[kDiagCols][2], int p, int w, i
     }
 }
 
+// ---- diagonal block by 2 x 2 recursion over 32 x 32 blocks ----
+// LU without pivoting of A = [A11 A12; A21 A22] and both inverses:
+//   A11 = L11 U11 (one warp), U12 = inv(L11) A12, L21 = A21 inv(U11),
+//   A22 - L21 U12 = L22 U22 (one warp),
+//   inv(L) = [inv(L11) 0; -inv(L22) L21 inv(L11)  inv(L22)],
+//   inv(U) = [inv(U11)  -inv(U11) U12 inv(U22); 0 inv(U22)].
+// Each 32 x 32 factorization is the one-pass scheme of diag_steps run by a
+// single warp, lane r holding row r: no block barrier per step, and the
+// coupling products run on all eight warps from shared memory (the two
+// that need only the first block, L21 inv(L11) and inv(U11) U12, beside the
+// second factorization).
+constexpr int RB = NB / 2;       // 32
+constexpr int kRecLd = RB + 1;   // row stride of the 32 x 32 shared-memory blocks (float2)
+constexpr int kSmemDiagRec = (NB * (NB + 1) + 8 * RB * kRecLd + 2 * RB) * (int)sizeof(float2);
+
+// One warp: LU and both inverses of the 32 x 32 block whose row `lane` is
+// in a[0..31] (column c in a[c]), 32 rank-1 steps as in diag_steps: step j
+// takes c_j = col_j / p_j (entry j zeroed) and applies
+// a(r, c) -= c_j(r) a(j, c) to every column c != j, rows r > j only when
+// c < j; column j becomes -c_j below the pivot. a(j, c) comes from lane j
+// by shuffle. The steps run in groups of four over a register window that
+// is rotated by four columns after each group (a[u] holds the group's
+// column j0 + u, a[c] column (j0 + c) mod 32), so that every register index
+// is static while the group loop stays rolled (the fully unrolled 32 steps
+// would be ~9 k instructions of straight-line code). Ends with a[c] = column
+// c: inv(L)(r, c) below the diagonal, the pivot p_r on it, S(r, c) =
+// -p_r inv(U~)(r, c) above; rcps[j] = 1 / p_j (lane 0 writes).
+__device__ __forceinline__ void leaf32(float2 (&a)[RB], int lane, float2* rcps, unsigned* err) {
+    const float2 z = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int j0 = 0; j0 < RB; j0 += 4) {
+        const int rlim = RB - j0;  // a[c] holds a column right of the pivot iff u < c < rlim
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            const float2 piv = shfl_c(a[u], j);
+            const float pm = piv.x * piv.x + piv.y * piv.y;
+            const bool bad = !(pm > tiny_pivot(pm)) || !isfinite(pm);
+            if (bad && lane == 0) atomicCAS(err, 0u, 1u);
+            const float inv = bad ? 0.f : rcp_rn(pm);
+            const float2 rcp = make_float2(piv.x * inv, -piv.y * inv);
+            float2 cj = cmulf(a[u], rcp);
+            if (lane == j) cj = z;
+            const float2 cl = lane > j ? cj : z;
+#pragma unroll
+            for (int c = 0; c < RB; ++c) {
+                if (c == u) continue;
+                const float2 x = shfl_c(a[c], j);
+                const float2 k = (c > u && c < rlim) ? cj : cl;
+                a[c] = cfmsf(a[c], k, x);
+            }
+            a[u] = lane > j ? cnegf(cj) : a[u];
+            if (lane == 0) rcps[j] = rcp;
+        }
+        const float2 t0 = a[0], t1 = a[1], t2 = a[2], t3 = a[3];
+#pragma unroll
+        for (int c = 0; c < RB - 4; ++c) a[c] = a[c + 4];
+        a[RB - 4] = t0;
+        a[RB - 3] = t1;
+        a[RB - 2] = t2;
+        a[RB - 1] = t3;
+    }
+    __syncwarp();
+}
+
+// Z = X Y (MODE 0), Z = -X Y (MODE 1) or Z -= X Y (MODE 2) for 32 x 32
+// complex64 blocks in shared memory (row-major, strides ldx / ldy / ldz),
+// by NT threads (t = 0 .. NT-1): thread t forms the entries of row t % 32
+// in columns t / 32 + (NT / 32) i, k ascending, FP32 FMAs.
+template <int NT, int MODE>
+__device__ __forceinline__ void mm32(const float2* X, int ldx, const float2* Y, int ldy, float2* Z, int ldz,
+                                     int t) {
+    constexpr int E = RB * RB / NT;   // entries per thread
+    constexpr int CS = NT / RB;       // column stride between them
+    const int r = t % RB, c0 = t / RB;
+    float2 acc[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) acc[i] = MODE == 2 ? Z[r * ldz + c0 + CS * i] : make_float2(0.f, 0.f);
+    for (int k = 0; k < RB; ++k) {
+        const float2 x = X[r * ldx + k];
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+            const float2 y = Y[k * ldy + c0 + CS * i];
+            if (MODE == 2) acc[i] = cfmsf(acc[i], x, y);
+            else acc[i] = make_float2(fmaf(x.x, y.x, fmaf(-x.y, y.y, acc[i].x)), fmaf(x.x, y.y, fmaf(x.y, y.x, acc[i].y)));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < E; ++i) Z[r * ldz + c0 + CS * i] = MODE == 1 ? cnegf(acc[i]) : acc[i];
+}
+
+// Writes the 32 x 32 inverses of the block leaf32 left in a (lane r = row
+// r): IL = inv(L) (unit diagonal), IU = inv(U) = -S(r, c) / (p_r p_c) above
+// the diagonal, 1 / p_r on it.
+__device__ __forceinline__ void leaf32_store(const float2 (&a)[RB], int lane, const float2* rcps, float2* IL,
+                                             float2* IU) {
+    const float2 z = make_float2(0.f, 0.f), one = make_float2(1.f, 0.f);
+    const float2 rr = rcps[lane];
+#pragma unroll
+    for (int c = 0; c < RB; ++c) {
+        IL[lane * kRecLd + c] = c < lane ? a[c] : (c == lane ? one : z);
+        IU[lane * kRecLd + c] = c > lane ? cnegf(cmulf(cmulf(a[c], rr), rcps[c])) : (c == lane ? rr : z);
+    }
+}
+
+// Diagonal block k0 (kb rows and columns, padded to NB with the identity)
+// by the 2 x 2 recursion above; writes Linv and Uinv (NB x NB column-major,
+// zero outside kb) and reads the block of W only. The block's update by the
+// previous step is done before (diag_update_kernel). A zero or non-finite
+// pivot sets the error word and continues with a zero reciprocal.
+__global__ void __launch_bounds__(256) diag_lu_rec_kernel(const float2* __restrict__ W, int64_t ldw, int64_t k0,
+                                                          int kb, float2* __restrict__ Linv,
+                                                          float2* __restrict__ Uinv, unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* A = reinterpret_cast<float2*>(dyn_smem);  // NB x (NB + 1), row-major
+    float2* blk = A + NB * (NB + 1);
+    float2* IL1 = blk;
+    float2* IU1 = blk + 1 * RB * kRecLd;
+    float2* IL2 = blk + 2 * RB * kRecLd;
+    float2* IU2 = blk + 3 * RB * kRecLd;
+    float2* U12 = blk + 4 * RB * kRecLd;  // later -inv(U11) U12 inv(U22)
+    float2* L21 = blk + 5 * RB * kRecLd;  // later -inv(L22) L21 inv(L11)
+    float2* T1 = blk + 6 * RB * kRecLd;   // L21 inv(L11)
+    float2* T2 = blk + 7 * RB * kRecLd;   // inv(U11) U12
+    float2* rc1 = blk + 8 * RB * kRecLd;
+    float2* rc2 = rc1 + RB;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    constexpr int LD = NB + 1;
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int r = e % NB, c = e / NB;  // rows fastest: coalesced columns of W
+        A[r * LD + c] = (r < kb && c < kb) ? W[(k0 + r) + (k0 + c) * ldw]
+                                           : make_float2(r == c ? 1.f : 0.f, 0.f);
+    }
+    __syncthreads();
+    if (w == 0) {
+        float2 a[RB];
+#pragma unroll
+        for (int c = 0; c < RB; ++c) a[c] = A[lane * LD + c];
+        leaf32(a, lane, rc1, err);
+        leaf32_store(a, lane, rc1, IL1, IU1);
+    }
+    __syncthreads();
+    if (w < 4) mm32<128, 0>(IL1, kRecLd, A + RB, LD, U12, kRecLd, tid);             // U12 = inv(L11) A12
+    else mm32<128, 0>(A + RB * LD, LD, IU1, kRecLd, L21, kRecLd, tid - 128);         // L21 = A21 inv(U11)
+    __syncthreads();
+    mm32<256, 2>(L21, kRecLd, U12, kRecLd, A + RB * LD + RB, LD, tid);               // A22 -= L21 U12
+    __syncthreads();
+    if (w == 0) {
+        float2 a[RB];
+#pragma unroll
+        for (int c = 0; c < RB; ++c) a[c] = A[(RB + lane) * LD + RB + c];
+        leaf32(a, lane, rc2, err);
+        leaf32_store(a, lane, rc2, IL2, IU2);
+    } else if (w >= 4) {
+        mm32<128, 0>(L21, kRecLd, IL1, kRecLd, T1, kRecLd, tid - 128);                // T1 = L21 inv(L11)
+        mm32<128, 0>(IU1, kRecLd, U12, kRecLd, T2, kRecLd, tid - 128);                // T2 = inv(U11) U12
+    }
+    __syncthreads();
+    if (w < 4) mm32<128, 1>(IL2, kRecLd, T1, kRecLd, L21, kRecLd, tid);              // -inv(L22) T1
+    else mm32<128, 1>(T2, kRecLd, IU2, kRecLd, U12, kRecLd, tid - 128);              // -T2 inv(U22)
+    __syncthreads();
+    const float2 z = make_float2(0.f, 0.f);
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int r = e % NB, c = e / NB;
+        const bool in = r < kb && c < kb;
+        const int rl = r % RB, cl = c % RB;
+        float2 lv, uv;
+        if (r < RB && c < RB) { lv = IL1[rl * kRecLd + cl]; uv = IU1[rl * kRecLd + cl]; }
+        else if (r >= RB && c >= RB) { lv = IL2[rl * kRecLd + cl]; uv = IU2[rl * kRecLd + cl]; }
+        else if (r >= RB) { lv = L21[rl * kRecLd + cl]; uv = z; }
+        else { lv = z; uv = U12[rl * kRecLd + cl]; }
+        Linv[r + c * NB] = in ? lv : z;
+        Uinv[r + c * NB] = in ? uv : z;
+    }
+}
+
 // The update of a diagonal block by the earlier block steps kp1 (and kp2,
 // -1 = none), A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb], in place in
 // W, on 16 CTAs of 16 x 16 entries (one per thread, the k order and FP32
@@ -426,10 +677,11 @@ __global__ void __launch_bounds__(256) diag_update_kernel(T* __restrict__ W, int
 // steps' updates, A11 -= L21(kp)[k0:k0+kb, :] U12(kp)[:, k0:k0+kb] (FP32
 // FMA), from the factor blocks staged in dynamic shared memory (kSmemDiagUpd;
 // that size also keeps the kernel off SMs that hold a trailing-GEMM CTA).
-// PANELS: diag_panel (one named barrier per panel) instead of diag_steps
-// (one block barrier per step); the coefficient columns then live in the
-// dynamic shared memory, after the update tiles are no longer read.
-template <class T, bool PANELS>
+// ELIM 0: diag_steps (one block barrier per step, fully unrolled per row
+// half); 1: diag_panel (one named barrier per panel; the coefficient
+// columns then live in the dynamic shared memory, after the update tiles
+// are no longer read); 2: diag_steps_compact (as 0, one code path).
+template <class T, int ELIM>
 __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restrict__ W, int64_t ldw,
                                                                int64_t k0, int kb, T* __restrict__ Linv,
                                                                T* __restrict__ Uinv,
@@ -470,7 +722,11 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
             }
         }
     }
-    if (PANELS) {
+    if (ELIM == 2) {
+#pragma unroll 1
+        for (int bp = 0; bp < kDiagWarps; ++bp)
+            diag_steps_compact<T>(a, bp, bp >= kDiagWarps / 2 ? 1 : 0, w, lane, cbuf, rcps, err);
+    } else if (ELIM == 1) {
         T(*cb)[NB] = reinterpret_cast<T(*)[NB]>(dyn_smem);
         __syncthreads();  // the update tiles are no longer read
 #pragma unroll 1
@@ -501,6 +757,23 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(const T* __restri
     }
 }
 
+
+template <class T>
+using DiagKernel = void (*)(const T*, int64_t, int64_t, int, T*, T*, unsigned*, int64_t, int64_t);
+
+// The elimination variant the switches select (diag_lu_kernel's ELIM).
+template <class T>
+static DiagKernel<T> diag_kernel_for(const MixedState* st) {
+    if (st->diag_panels) return diag_lu_kernel<T, 1>;
+    return st->diag_compact ? diag_lu_kernel<T, 2> : diag_lu_kernel<T, 0>;
+}
+
+template <class T>
+static int diag_set_smem(int bytes) {
+    for (DiagKernel<T> k : {diag_lu_kernel<T, 0>, diag_lu_kernel<T, 1>, diag_lu_kernel<T, 2>})
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return SIEB200_OK;
+}
 
 // Arguments of one block step's panels launch.
 //   kp[0], kp[1]: earlier block steps (column offsets, -1 = none) whose
@@ -1379,6 +1652,10 @@ constexpr int kOverlapMinDefault = 0;
 // iteration more (6 instead of 5), which cost more than the faster
 // factorization gained; 20000 keeps such systems on single steps.
 constexpr int kPairMinDefault = 20000;
+// Stop an FGMRES cycle at an Arnoldi residual estimate of this fraction of
+// the tolerance (the true residual is checked after the cycle; 0.5 cost the
+// 17280-unknown GSTC batch 16 ms more per solve, 129 against 113 ms).
+constexpr double kGmresEstFactorDefault = 0.9;
 constexpr int kOverlapSmsDefault = 20;
 
 static int fp64_factorize(DenseSolver* s);
@@ -1418,6 +1695,9 @@ int mixed_factorize(DenseSolver* s) {
     st->lo_rn = (lorn_env && lorn_env[0] == '1') ? 1 : 0;
     st->diag_split = diag_split_env();
     st->diag_panels = diag_panels_env();
+    st->diag_compact = diag_compact_env();
+    const char* rec_env = getenv("SIEB200_DIAG_REC");
+    st->diag_rec = (rec_env && rec_env[0] == '1') ? 1 : 0;
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -1461,10 +1741,9 @@ int mixed_factorize(DenseSolver* s) {
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemDiagUpd));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemDiagUpd));
+        SIEB_RETURN_IF(diag_set_smem<float2>(kSmemDiagUpd));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_rec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemDiagRec));
         attrs_set = true;
     }
 
@@ -1473,7 +1752,7 @@ int mixed_factorize(DenseSolver* s) {
     key.A = s->A; key.lda = s->lda; key.n = n; key.W = st->W; key.pack = st->Apack[0];
     const int gemm_sms = s->sm_cap > 0 ? std::min(s->sm_cap, ctx->sm_count - 1) : ctx->sm_count - 1;
     key.use_tc = st->use_tc + 2 * st->pair + 4 * st->hilo + 8 * st->lcol + 16 * st->lo_rn + 32 * st->diag_split +
-                 64 * st->diag_panels;
+                 64 * st->diag_panels + 128 * st->diag_rec + 256 * st->diag_compact;
     key.sms = gemm_sms;
     key.ovl = ((int64_t)st->pair_min << 32) | (int64_t)(st->ovl_min * 1000 + st->ovl_sms);
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
@@ -1549,14 +1828,21 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         cudaEvent_t ev;
         ctx->prof.begin(sm, 3, (8.0 / 3.0 + 8.0 / 3.0) * NB * NB * NB + nupd * 8.0 * NB * NB * NB,
                         8.0 * NB * NB * (3.0 + 2.0 * nupd), &ev);
-        if (nupd > 0 && st->diag_split) {
+        if (nupd > 0 && (st->diag_split || st->diag_rec)) {
             diag_update_kernel<float2><<<dim3(NB / 16, NB / 16), 256, 0, sm>>>(st->W, ldw, k0, kb, kp1, kp2);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             kp1 = kp2 = -1;
         }
-        (st->diag_panels ? diag_lu_kernel<float2, true> : diag_lu_kernel<float2, false>)<<<1, kDiagThreads,
-                                                                                            kSmemDiagUpd, sm>>>(
+        if (st->diag_rec) {
+            diag_lu_rec_kernel<<<1, 256, kSmemDiagRec, sm>>>(st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB,
+                                                             st->Uinv + (size_t)bk * NB * NB, st->err);
+            SIEB_NOTE_LAUNCH();
+            ctx->prof.end(sm, ev);
+            SIEB_TRY_CUDA(cudaGetLastError());
+            return SIEB200_OK;
+        }
+        diag_kernel_for<float2>(st)<<<1, kDiagThreads, kSmemDiagUpd, sm>>>(
             st->W, ldw, k0, kb, st->Linv + (size_t)bk * NB * NB, st->Uinv + (size_t)bk * NB * NB, st->err, kp1, kp2);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(sm, ev);
@@ -1897,6 +2183,12 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
 // with right preconditioner M^{-1}, started from x = 0. The preconditioned
 // directions z_j = M^{-1} v_j are kept, so the update x += Z y costs no
 // further preconditioner application.
+double gmres_est_factor() {
+    const char* e = getenv("SIEB200_GMRES_EST_FACTOR");
+    const double f = e ? atof(e) : kGmresEstFactorDefault;
+    return (f > 0.0 && f <= 1.0) ? f : kGmresEstFactorDefault;
+}
+
 static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int maxit, bool adjoint,
                     int* iters) {
     (void)ldb_unused;
@@ -1927,6 +2219,7 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
 
     // ||b|| is the first residual norm (x0 = 0), read with it below.
     double bnorm = 0.0;
+    const double est_factor = gmres_est_factor();
 
     SIEB_TRY_CUDA(cudaMemsetAsync(x, 0, sizeof(cplx) * n, stream));
     int total = 0;
@@ -2048,7 +2341,7 @@ static int gmres_ir(DenseSolver* s, cplx* b, int64_t ldb_unused, double tol, int
             g[j] = cx(cs[j].re * gj.re, cs[j].re * gj.im);
             g[j + 1] = cx(-(conj_s * gj).re, -(conj_s * gj).im);
             est = std::hypot(g[j + 1].re, g[j + 1].im);
-            if (est <= 0.5 * tol * bnorm || hn == 0.0) { ++j; ++total; break; }
+            if (est <= est_factor * tol * bnorm || hn == 0.0) { ++j; ++total; break; }
         }
         // y = H^{-1} g (upper triangular j x j)
         std::vector<cplx> y(j);
@@ -2157,6 +2450,8 @@ static int fp64_factorize(DenseSolver* s) {
     st->err = reinterpret_cast<unsigned*>(base + up(bW) + 2 * up(bInv) + up(bDiag));
     st->diag_split = diag_split_env();
     st->diag_panels = diag_panels_env();
+    st->diag_compact = diag_compact_env();
+    st->diag_rec = 0;  // complex64 only
     if (!st->side) {
         int least = 0, greatest = 0;
         SIEB_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -2169,10 +2464,7 @@ static int fp64_factorize(DenseSolver* s) {
     if (!attrs64) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kSmemPanel64));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemDiagUpd64));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemDiagUpd64));
+        SIEB_RETURN_IF(diag_set_smem<double2>(kSmemDiagUpd64));
         attrs64 = true;
     }
     cudaEvent_t ev_fact;
@@ -2196,8 +2488,7 @@ static int fp64_factorize(DenseSolver* s) {
             SIEB_TRY_CUDA(cudaGetLastError());
             kp = -1;
         }
-        (st->diag_panels ? diag_lu_kernel<double2, true> : diag_lu_kernel<double2, false>)<<<1, kDiagThreads,
-                                                                                              kSmemDiagUpd64, sm>>>(
+        diag_kernel_for<double2>(st)<<<1, kDiagThreads, kSmemDiagUpd64, sm>>>(
             st->W64, ldw, k0, kb, st->Linv64 + (size_t)bk * NB * NB, st->Uinv64 + (size_t)bk * NB * NB, st->err, kp,
             -1);
         SIEB_NOTE_LAUNCH();

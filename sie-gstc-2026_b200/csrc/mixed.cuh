@@ -40,6 +40,8 @@ struct MixedState {
     int lo_rn = 0;              // split packs: lo parts rounded to the nearest TF32 (else truncated by the MMA)
     int diag_split = 1;         // diagonal blocks take their update in a 16-CTA kernel ahead of the LU kernel
     int diag_panels = 0;        // diagonal-block elimination synchronised per panel of 8 steps, not per step
+    int diag_rec = 0;           // diagonal block by 2 x 2 recursion over 32 x 32 warp-level factorizations
+    int diag_compact = 0;       // diagonal-block elimination in one code path (runtime row half)
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
@@ -153,6 +155,11 @@ __device__ __forceinline__ float tf32_lo(float x, float hi, int rn) {
     const float l = x - hi;
     return rn ? tf32_hi(l) : l;
 }
+
+// The FGMRES cycles stop once the Arnoldi residual estimate is at most
+// this fraction of tol * ||b||; the restart then checks the true FP64
+// residual against tol * ||b|| itself (SIEB200_GMRES_EST_FACTOR, in (0, 1]).
+double gmres_est_factor();
 
 // Multi-right-hand-side solve with the mixed factors (block_solve.cu).
 int block_solve(DenseSolver* s, MixedState* st, int64_t nrhs, double* B, int64_t ldb, double tol, int maxit,

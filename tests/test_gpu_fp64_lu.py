@@ -30,7 +30,7 @@ def _host(t, rows, cols):
     return a
 
 
-@pytest.mark.parametrize("diag", ["split_panels", "split_steps", "fused_steps"])
+@pytest.mark.parametrize("diag", ["split_panels", "split_steps", "fused_steps", "split_compact"])
 @pytest.mark.parametrize("n,nrhs", [(5, 1), (50, 2), (130, 1), (997, 3), (2100, 1)])
 def test_fp64_lu_matches_numpy(n, nrhs, diag, gpu_ctx, monkeypatch):
     """Against numpy at 1e-12, with the diagonal block's update in its own
@@ -40,6 +40,7 @@ def test_fp64_lu_matches_numpy(n, nrhs, diag, gpu_ctx, monkeypatch):
     import sieb200
     monkeypatch.setenv("SIEB200_DIAG_SPLIT", "0" if diag.startswith("fused") else "1")
     monkeypatch.setenv("SIEB200_DIAG_PANELS", "1" if diag.endswith("panels") else "0")
+    monkeypatch.setenv("SIEB200_DIAG_COMPACT", "1" if diag.endswith("compact") else "0")
     rng = np.random.default_rng(n)
     A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
     A += np.diag(2.0 + rng.uniform(0, 1, n))

@@ -225,15 +225,17 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
 @pytest.mark.parametrize("schedule", ["pair_split", "single_split", "pair_three", "single_three",
                                       "single_split_overlap", "single_split_trsv64", "pair_then_single",
                                       "single_split_no_lcol", "single_split_lcol_gemm",
-                                      "single_split_lcol_side"])
+                                      "single_split_lcol_side", "single_split_diag_rec",
+                                      "single_split_diag_compact"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
     sub-block, and fewer rows than one block, under both trailing-update
     schedules (pair / single step), both pack layouts (split [hi | lo] /
     three-product), the next block column's update in single steps from the
-    column kernel before the GEMM (default) or beside it, the GEMM or the
-    panels,
+    GEMM (default), the column kernel before or beside it or the panels,
+    diagonal blocks by the one-pass 64 x 64 kernel (unrolled or compact)
+    or the 32 x 32 recursion,
     with overlapped steps (panels beside the GEMM), with
     64-row triangular-solve CTAs, and switching from the pair to the single
     schedule part way. One preconditioned step must already reach 1e-5 (the
@@ -245,7 +247,7 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
                        else "0")
     # pair steps while the paired update is at least 128 columns wide, single steps after
     monkeypatch.setenv("SIEB200_PAIR_MIN", "128" if schedule == "pair_then_single" else "0")
-    monkeypatch.setenv("SIEB200_GEMM_HILO", "0" if schedule.endswith("three") else "1")
+    monkeypatch.setenv("SIEB200_GEMM_HILO", "0" if "_three" in schedule else "1")
     # overlapped steps: every trailing update at least 64 columns wide skips
     # the next block row, whose update the next panels take on the side stream
     monkeypatch.setenv("SIEB200_OVERLAP_MIN", "64" if schedule.endswith("overlap") else "0")
@@ -253,11 +255,16 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     # triangular solves with 64-row CTAs (one sub-block each) or 128-row ones
     monkeypatch.setenv("SIEB200_TRSV_ROWS", "64" if schedule.endswith("trsv64") else "128")
     # who updates the next block column below its diagonal block in a single
-    # step: the next panels (0), the GEMM (1), col_update_kernel on the third
-    # stream (2) or before the GEMM (3, default)
+    # step: the next panels (0), the GEMM (1, default), col_update_kernel on
+    # the third stream (2) or before the GEMM (3)
     monkeypatch.setenv("SIEB200_GEMM_LCOL", "0" if schedule.endswith("no_lcol")
                        else "1" if schedule.endswith("lcol_gemm")
-                       else "2" if schedule.endswith("lcol_side") else "3")
+                       else "2" if schedule.endswith("lcol_side") else "1")
+    # diagonal blocks by the one-pass 64 x 64 kernel, fully unrolled
+    # (default) or in one code path, or by the 2 x 2 recursion over 32 x 32
+    # warp factorizations
+    monkeypatch.setenv("SIEB200_DIAG_REC", "1" if schedule.endswith("diag_rec") else "0")
+    monkeypatch.setenv("SIEB200_DIAG_COMPACT", "1" if schedule.endswith("diag_compact") else "0")
     rng = np.random.default_rng(n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
@@ -281,13 +288,14 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
 
 
 _CHAIN_VARIANTS = {
-    # (SIEB200_GEMM_LCOL, SIEB200_DIAG_SPLIT, SIEB200_DIAG_PANELS)
-    "default": ("3", "1", "0"),
-    "panel_updates_column": ("0", "1", "0"),
-    "column_update_third_stream": ("2", "1", "0"),
-    "fused_diag_update": ("3", "0", "0"),
-    "diag_barrier_per_panel": ("3", "1", "1"),
-    "all_previous": ("0", "0", "0"),
+    # (SIEB200_GEMM_LCOL, SIEB200_DIAG_SPLIT, SIEB200_DIAG_PANELS, SIEB200_DIAG_COMPACT)
+    "reference": ("3", "1", "0", "1"),
+    "panel_updates_column": ("0", "1", "0", "1"),
+    "column_update_third_stream": ("2", "1", "0", "1"),
+    "fused_diag_update": ("3", "0", "0", "1"),
+    "diag_barrier_per_panel": ("3", "1", "1", "1"),
+    "diag_unrolled": ("3", "1", "0", "0"),
+    "all_previous": ("0", "0", "0", "0"),
 }
 
 
@@ -297,9 +305,9 @@ def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
     next block column's update by col_update_kernel (before the GEMM or on
     a third stream beside it) or by the panels, the diagonal block's update
     by diag_update_kernel or inside the LU kernel, and the elimination with
-    a barrier per step or per panel all run the
-    same FP32 operations in the same order, so the factors, and with them
-    the one-step solution, are the same bit for bit."""
+    a barrier per step (unrolled or in one code path) or per panel all run
+    the same FP32 operations in the same order, so the factors, and with
+    them the one-step solution, are the same bit for bit."""
     import torch
     import sieb200
     rng = np.random.default_rng(300 + n)
@@ -307,11 +315,13 @@ def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
     b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
     Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()
     monkeypatch.setenv("SIEB200_PAIR_MIN", "0")
+    monkeypatch.setenv("SIEB200_DIAG_REC", "0")  # the one-pass 64 x 64 kernel in every variant
     out = {}
-    for name, (lcol, split, panels) in _CHAIN_VARIANTS.items():
+    for name, (lcol, split, panels, compact) in _CHAIN_VARIANTS.items():
         monkeypatch.setenv("SIEB200_GEMM_LCOL", lcol)
         monkeypatch.setenv("SIEB200_DIAG_SPLIT", split)
         monkeypatch.setenv("SIEB200_DIAG_PANELS", panels)
+        monkeypatch.setenv("SIEB200_DIAG_COMPACT", compact)
         s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
         s.factorize(Z.data_ptr())
         x = torch.from_numpy(b.copy()).cuda()
@@ -320,9 +330,9 @@ def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
         gpu_ctx.synchronize()
         out[name] = x.cpu().numpy()
         s.close()
-    assert np.linalg.norm(A @ out["default"] - b) / np.linalg.norm(b) <= 1e-5
+    assert np.linalg.norm(A @ out["reference"] - b) / np.linalg.norm(b) <= 1e-5
     for name, xs in out.items():
-        assert np.array_equal(xs, out["default"]), name
+        assert np.array_equal(xs, out["reference"]), name
 
 
 @pytest.mark.parametrize("rows", ["128", "64"])
