@@ -23,6 +23,7 @@ struct DenseSolver {
     DeviceBuffer vec;      // residual / work vectors
     DeviceBuffer flags;    // triangular-solve progress flags and error word
     DeviceBuffer gemv_scratch;
+    DeviceBuffer couple;   // triangular-solve coupling products (mixed)
     void* gemm_state = nullptr;
     // Cap on the SMs of the persistent trailing GEMM (0: all but one); a
     // sweep running several systems concurrently gives each its share.

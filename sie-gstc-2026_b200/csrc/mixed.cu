@@ -1413,6 +1413,347 @@ trsv_tma_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, in
     solve_sub(second);
 }
 
+// Coupling products for trsv_fold_kernel: for sub-block k and its
+// neighbours at distance d in solve order (lower: k - d, upper: k + d),
+// Pd[k] = Dinv_k F(k, k -/+ d), F the factor (W or its conjugate transpose;
+// rows and columns beyond np read as zero), Dinv_k the sub-block's inverse
+// (NB x NB column-major). grid (nsb, D): blockIdx.y + 1 is d (zero where
+// the neighbour does not exist); P = P1 (nsb blocks), P2, .., each NB x NB
+// column-major complex64, accumulated in FP64.
+constexpr int kSmemCouple = 2 * NB * (NB + 1) * (int)sizeof(float2);
+__global__ void __launch_bounds__(256) trsv_couple_kernel(const float2* __restrict__ M, int64_t ldm, int64_t np,
+                                                          int nsb, int lower, const float2* __restrict__ Dinv,
+                                                          float2* __restrict__ P) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2(*Ds)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(dyn_smem);  // [row][q]
+    float2(*Fs)[NB + 1] = Ds + NB;                                           // [q][col]
+    const int k = blockIdx.x, dist = blockIdx.y + 1;
+    const int nb = lower ? k - dist : k + dist;  // neighbour sub-block
+    float2* out = P + ((size_t)blockIdx.y * nsb + k) * NB * NB;
+    const int tid = threadIdx.x;
+    if (nb < 0 || nb >= nsb) {
+        for (int e = tid; e < NB * NB; e += 256) out[e] = make_float2(0.f, 0.f);
+        return;
+    }
+    for (int e = tid; e < NB * NB; e += 256) {
+        const int r = e % NB, c = e / NB;  // rows fastest: coalesced columns
+        Ds[r][c] = Dinv[(size_t)k * NB * NB + e];
+        const int64_t gr = (int64_t)k * NB + r, gc = (int64_t)nb * NB + c;
+        Fs[r][c] = (gr < np && gc < np) ? M[gr + gc * ldm] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int r = tid % NB, c0 = tid / NB;  // columns c0 + 4i
+    double re[NB / 4], im[NB / 4];
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i) re[i] = im[i] = 0.0;
+    for (int q = 0; q < NB; ++q) {
+        const float2 d = Ds[r][q];
+#pragma unroll
+        for (int i = 0; i < NB / 4; ++i) {
+            const float2 f = Fs[q][c0 + 4 * i];
+            re[i] += (double)d.x * f.x - (double)d.y * f.y;
+            im[i] += (double)d.x * f.y + (double)d.y * f.x;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NB / 4; ++i) out[r + (c0 + 4 * i) * NB] = make_float2((float)re[i], (float)im[i]);
+}
+
+// trsv_tma_kernel for 128-row CTAs with the coupling to the newest
+// sub-block folded into precomputed products (trsv_couple_kernel). A CTA's
+// sub-blocks in solve order are s1, s2; p is the one published just before
+// s1 (its neighbour). Then
+//   x_s1 = Dinv_s1 y_s1 - P1[s1] x_p,
+//   x_s2 = (Dinv_s2 y_s2 - P2[s2] x_p) - P1[s2] x_s1,
+// y the CTA's right-hand side less the contributions of every sub-block
+// published before p, which are streamed and accumulated as before, and
+// Dinv y formed while p is still awaited. Once x_p is in, s1 is one 64 x 64
+// product away from publication and s2 one more, with no coupling tiles
+// (the P slices are read into registers at the start): 203 against 213 us
+// per solve at N = 6016. Folding the previous CTA's first sub-block as well
+// (P3, one poll for both) measured slower, 246-254 us: the longer FP64
+// product then sits on the chain. The same bounded waits, abort and
+// publication protocol as trsv_tma_kernel.
+constexpr int kSmemTrsvFold = kSmemTrsv + NB * (int)sizeof(cplx);
+// Registers are granted to 288 threads in units of four warps (12 warps'
+// worth), which caps a thread at 168.
+__global__ void __launch_bounds__(TR_THREADS, 1)
+trsv_fold_kernel(const __grid_constant__ CUtensorMap tmW, int64_t np, int nsb, int lower,
+                 const float2* __restrict__ Dinv, const float2* __restrict__ P, cplx* __restrict__ x,
+                 cplx* __restrict__ xpub, unsigned* __restrict__ progress, unsigned* __restrict__ err,
+                 unsigned long long timeout_ns) {
+    constexpr int ROWS = TR_ROWS, STG = TR_STAGES, TILE = TR_TILE, TILE_BYTES = TR_TILE_BYTES;
+    constexpr int HG = TR_CONSUMERS / ROWS;  // consumer threads per row (2)
+    constexpr int CPT = TR_COLS / HG;        // tile columns per consumer thread
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const uint32_t raw = smem_u32(dyn_smem);
+    unsigned char* base = dyn_smem + (((raw + 1023u) & ~1023u) - raw);
+    const uint32_t ring = smem_u32(base);
+    const float2* ringp = reinterpret_cast<const float2*>(base);
+    float2* Ds = reinterpret_cast<float2*>(base + STG * TILE_BYTES);  // 2 x [NB cols][TR_DLD]
+    cplx* red = reinterpret_cast<cplx*>(Ds + 2 * NB * TR_DLD);        // ROWS: partial sums, then Dinv y
+    cplx* ys = red + (HG - 1) * ROWS;                                   // ROWS
+    cplx* xs = ys + ROWS;                                               // NB: x_s1
+    cplx* xstage = xs + NB;                                             // 2 x NB
+    const uint32_t full0 = smem_u32(xstage + 2 * NB), empty0 = full0 + 8 * STG;
+    cplx* ts = reinterpret_cast<cplx*>(xstage + 2 * NB) + STG;          // NB: s2 before its last term
+    __shared__ int s_t, s_go;
+    __shared__ volatile int s_abort;
+    static_assert(HG == 2, "two consumer threads per row");
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        s_t = (int)atomicAdd(&progress[1], 1u);
+        s_abort = 0;
+        for (int st = 0; st < STG; ++st) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, TR_CONSUMERS / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    const uint64_t deadline = global_ns() + timeout_ns;
+    const int ncta = (int)((np + ROWS - 1) / ROWS);
+    const int t = s_t;
+    if (t >= ncta) return;  // block-uniform
+    const int rb = lower ? t : ncta - 1 - t;
+    const int64_t R0 = (int64_t)rb * ROWS;
+    const int sbA = 2 * rb, sbB = 2 * rb + 1;
+    const bool has_bot = sbB < nsb;
+    const int s1 = (lower || !has_bot) ? sbA : sbB;   // solve order within the CTA
+    const int s2 = lower ? sbB : sbA;
+    const int w1 = s1 - sbA, w2 = s2 - sbA;           // 0 (rows 0..63) or 1 (rows 64..127)
+    const int pnb = lower ? s1 - 1 : s1 + 1;          // the neighbour published just before s1
+    const bool has_p = pnb >= 0 && pnb < nsb;
+    // Streamed tiles: the off-diagonal ones of every sub-block before pnb,
+    // in publication order.
+    const int ntile_all = (int)((np + TR_COLS - 1) / TR_COLS);
+    int n_off;
+    if (lower) {
+        n_off = R0 >= NB ? (int)((R0 - NB) / TR_COLS) : 0;
+    } else {
+        const int64_t c_first = R0 + ROWS + NB;  // columns from here on come before pnb
+        n_off = c_first < np ? ntile_all - (int)(c_first / TR_COLS) : 0;
+    }
+    auto tile_k = [&](int i) -> int { return lower ? i : ntile_all - 1 - i; };
+
+    if (warp == TR_CONSUMERS / 32) {  // producer
+        if (lane == 0) {
+            for (int i = 0; i < n_off; ++i) {
+                const int st = i % STG;
+                const uint32_t ph = (uint32_t)(i / STG) & 1u;
+                if (!tr_wait(empty0 + 8 * st, ph ^ 1u, deadline)) {
+                    atomicCAS(err, 0u, 2u);
+                    s_abort = 1;
+                    break;
+                }
+                mbar_expect_tx(full0 + 8 * st, TILE_BYTES);
+                tma_load_2d(ring + st * TILE_BYTES, &tmW, full0 + 8 * st, (int)R0, tile_k(i) * TR_COLS);
+            }
+        }
+        return;
+    }
+    // Consumers. Inverses of the two diagonal sub-blocks into shared memory.
+    for (int e = tid; e < NB * NB; e += TR_CONSUMERS) {
+        const int r = e & (NB - 1), c = e >> 6;
+        Ds[c * TR_DLD + r] = Dinv[(size_t)sbA * NB * NB + e];
+        Ds[(NB + c) * TR_DLD + r] = has_bot ? Dinv[(size_t)sbB * NB * NB + e] : make_float2(0.f, 0.f);
+    }
+    // The coupling slices, read at the start. Phase 1 (x_p): threads 0..127
+    // form P1[s1] x_p for the s1 rows, threads 128..255 P2[s2] x_p for the
+    // s2 rows, thread (row q >> 1, half q & 1) over columns (q & 1) + 2u.
+    // Phase 2: P1[s2] x_s1, thread (row tid >> 2, part tid & 3) over
+    // columns (tid & 3) + 4u.
+    const int q1 = tid & 127, r1 = q1 >> 1, c1 = q1 & 1;
+    const bool ph1_s2 = tid >= 128;
+    const int kk1 = ph1_s2 ? s2 : s1;
+    const int d1 = ph1_s2 ? 2 : 1;  // distance of p from kk1
+    const float2* srca = P + ((size_t)(d1 - 1) * nsb + kk1) * NB * NB;  // P1[s1] or P2[s2]
+    const bool use_a = ph1_s2 ? (has_bot && has_p) : has_p;
+    float2 pa[NB / 2], pb[NB / 4];
+    {
+#pragma unroll
+        for (int u = 0; u < NB / 2; ++u) pa[u] = use_a ? __ldg(&srca[r1 + (c1 + 2 * u) * NB]) : make_float2(0.f, 0.f);
+        const float2* src2 = P + (size_t)s2 * NB * NB;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u)
+            pb[u] = has_bot ? __ldg(&src2[(tid >> 2) + ((tid & 3) + 4 * u) * NB]) : make_float2(0.f, 0.f);
+    }
+    // Thread (r, h): row r of the block, columns h*CPT .. h*CPT+CPT-1 of a tile.
+    const int r = tid & (ROWS - 1), h = tid / ROWS;
+    const int64_t grow = R0 + r;
+    cplx b = cx(0, 0);  // written only by this CTA: final from the start
+    if (h == 0 && grow < np) b = cx(__ldcg(&x[grow].re), __ldcg(&x[grow].im));
+    double acc_re = 0.0, acc_im = 0.0;
+    // Polls the NB entries of sub-block sb, and of sub-block sb2 as well
+    // when sb2 >= 0 (warp 0, two entries of each per lane, all in every
+    // round) into dst / dst2; false on abort or timeout.
+    auto poll_sub = [&](int sb, cplx* dst, int sb2, cplx* dst2) -> bool {
+        int64_t e[4];
+        bool need[4];
+        cplx v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int sbq = q < 2 ? sb : sb2;
+            e[q] = (int64_t)sbq * NB + lane + 32 * (q & 1);
+            need[q] = sbq >= 0 && e[q] < np;
+            v[q] = cx(0, 0);
+        }
+        bool okp = !s_abort;
+        int it = 0;
+        while (okp && (need[0] || need[1] || need[2] || need[3])) {
+            double a[4], b2[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q] = 0; b2[q] = 0;
+                if (need[q]) { a[q] = ld_relaxed_f64(&xpub[e[q]].re); b2[q] = ld_relaxed_f64(&xpub[e[q]].im); }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (need[q] && !unpublished(a[q]) && !unpublished(b2[q])) { v[q] = cx(a[q], b2[q]); need[q] = false; }
+            if (!(need[0] || need[1] || need[2] || need[3])) break;
+            if (++it > 16) __nanosleep(64);
+            if ((it & 63) == 0 && (s_abort || global_ns() > deadline || *reinterpret_cast<volatile unsigned*>(err))) {
+                atomicCAS(err, 0u, 2u);
+                s_abort = 1;
+                okp = false;
+            }
+        }
+        dst[lane] = v[0];
+        dst[lane + 32] = v[1];
+        if (sb2 >= 0) {
+            dst2[lane] = v[2];
+            dst2[lane + 32] = v[3];
+        }
+        __syncwarp();
+        return okp;
+    };
+    // Off-diagonal tiles of the sub-blocks before pnb, a group of one NB
+    // sub-block (two tiles, or one at a ragged end) per poll.
+    for (int i = 0, g = 0; i < n_off; ++g) {
+        const int sb = (tile_k(i) * TR_COLS) / NB;
+        const int cnt = (i + 1 < n_off && (tile_k(i + 1) * TR_COLS) / NB == sb) ? 2 : 1;
+        cplx* xg = xstage + (g & 1) * NB;
+        if (warp == 0) poll_sub(sb, xg, -1, nullptr);
+        consumer_bar();
+        for (int j = 0; j < cnt; ++j, ++i) {
+            const int st = i % STG;
+            const uint32_t ph = (uint32_t)(i / STG) & 1u;
+            bool ok = !s_abort;
+            if (!tr_wait(full0 + 8 * st, ph, deadline)) {
+                if (lane == 0) atomicCAS(err, 0u, 2u);
+                s_abort = 1;
+                ok = false;
+            }
+            if (ok) {
+                const float2* tile = ringp + st * TILE;
+                const cplx* xt = xg + (tile_k(i) * TR_COLS - sb * NB) + h * CPT;
+#pragma unroll
+                for (int u = 0; u < CPT; ++u) {
+                    const float2 w = tile[(h * CPT + u) * ROWS + r];
+                    const cplx xv = xt[u];
+                    acc_re += (double)w.x * xv.re - (double)w.y * xv.im;
+                    acc_im += (double)w.x * xv.im + (double)w.y * xv.re;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty0 + 8 * st);
+        }
+    }
+    if (h >= 1) red[(h - 1) * ROWS + r] = cx(acc_re, acc_im);
+    consumer_bar();
+    if (h == 0) ys[r] = cx(b.re - (acc_re + red[r].re), b.im - (acc_im + red[r].im));
+    consumer_bar();
+    // z = Dinv y for both sub-blocks (into red), thread (row dr, part) of
+    // sub-block `which` over columns part + 4u.
+    const int dr = tid >> 2, part = tid & 3;
+    auto dinv_apply = [&](int which) {
+        const float2* D = Ds + which * NB * TR_DLD;
+        const cplx* y = ys + which * NB;
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = part + 4 * u;
+            const float2 d = D[c * TR_DLD + dr];
+            const cplx yv = y[c];
+            re += (double)d.x * yv.re - (double)d.y * yv.im;
+            im += (double)d.x * yv.im + (double)d.y * yv.re;
+        }
+        re += __shfl_xor_sync(0xffffffffu, re, 1);
+        im += __shfl_xor_sync(0xffffffffu, im, 1);
+        re += __shfl_xor_sync(0xffffffffu, re, 2);
+        im += __shfl_xor_sync(0xffffffffu, im, 2);
+        if (part == 0) red[which * NB + dr] = cx(re, im);
+    };
+    dinv_apply(0);
+    if (has_bot) dinv_apply(1);
+    // The neighbour's NB entries.
+    cplx* xp = xstage;  // both group buffers are free once the loop is done
+    if (warp == 0 && has_p) poll_sub(pnb, xp, -1, nullptr);
+    if (tid == 0) s_go = !s_abort;
+    consumer_bar();
+    if (!s_go) return;  // block-uniform
+    {
+        double re = 0.0, im = 0.0;
+        if (use_a) {
+#pragma unroll
+            for (int u = 0; u < NB / 2; ++u) {
+                const cplx xv = xp[c1 + 2 * u];
+                re += (double)pa[u].x * xv.re - (double)pa[u].y * xv.im;
+                im += (double)pa[u].x * xv.im + (double)pa[u].y * xv.re;
+            }
+        }
+        re += __shfl_xor_sync(0xffffffffu, re, 1);
+        im += __shfl_xor_sync(0xffffffffu, im, 1);
+        if (c1 == 0) {
+            if (!ph1_s2) {
+                const cplx z = red[w1 * NB + r1];
+                const cplx v = cx(z.re - re, z.im - im);
+                xs[r1] = v;
+                const int64_t gr = R0 + w1 * NB + r1;
+                if (gr < np) {
+                    __stcg(&x[gr].re, v.re);
+                    __stcg(&x[gr].im, v.im);
+                    __stcg(&xpub[gr].re, v.re);
+                    __stcg(&xpub[gr].im, v.im);
+                }
+            } else if (has_bot) {
+                const cplx z = red[w2 * NB + r1];
+                ts[r1] = cx(z.re - re, z.im - im);
+            }
+        }
+    }
+    consumer_bar();  // orders the stores of s1 before the release
+    if (tid == 0) st_release_gpu(&progress[0], lower ? (unsigned)s1 + 1u : (unsigned)(nsb - s1));
+    if (!has_bot) return;
+    {
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int u = 0; u < NB / 4; ++u) {
+            const cplx xv = xs[part + 4 * u];
+            re += (double)pb[u].x * xv.re - (double)pb[u].y * xv.im;
+            im += (double)pb[u].x * xv.im + (double)pb[u].y * xv.re;
+        }
+        re += __shfl_xor_sync(0xffffffffu, re, 1);
+        im += __shfl_xor_sync(0xffffffffu, im, 1);
+        re += __shfl_xor_sync(0xffffffffu, re, 2);
+        im += __shfl_xor_sync(0xffffffffu, im, 2);
+        if (part == 0) {
+            const cplx v = cx(ts[dr].re - re, ts[dr].im - im);
+            const int64_t gr = R0 + w2 * NB + dr;
+            if (gr < np) {
+                __stcg(&x[gr].re, v.re);
+                __stcg(&x[gr].im, v.im);
+                __stcg(&xpub[gr].re, v.re);
+                __stcg(&xpub[gr].im, v.im);
+            }
+        }
+    }
+    consumer_bar();
+    if (tid == 0) st_release_gpu(&progress[0], lower ? (unsigned)s2 + 1u : (unsigned)(nsb - s2));
+}
+
 // ------------------------------------------------------------ small vector ops
 __global__ void dot_partial_kernel(int64_t n, int k, const cplx* __restrict__ V, int64_t ldv,
                                    const cplx* __restrict__ w, cplx* __restrict__ out) {
@@ -1614,7 +1955,7 @@ void mixed_release(DenseSolver* s) {
     }
     s->gemm_state = nullptr;
     s->lu.release(); s->perm.release(); s->panel.release(); s->gemm_a.release(); s->gemm_b.release();
-    s->krylov.release(); s->vec.release(); s->flags.release(); s->gemv_scratch.release();
+    s->krylov.release(); s->vec.release(); s->flags.release(); s->gemv_scratch.release(); s->couple.release();
 }
 
 static int check_err(DenseSolver* s, const char* what) {
@@ -1676,6 +2017,7 @@ int mixed_factorize(DenseSolver* s) {
     const int64_t nbl = (np + NB - 1) / NB;
     st->n = n; st->np = np; st->ldw = ldw; st->nbl = nbl;
     st->adj_ready = false;
+    st->couple_ready[0] = st->couple_ready[1] = false;
     block_solve_invalidate(st);
     const char* env = getenv("SIEB200_TRAILING_SIMT");
     st->use_tc = (env && env[0] == '1') ? 0 : 1;
@@ -2107,8 +2449,14 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     if (st->tm_rows != rows) {
         st->tm_base = nullptr;
         st->adj_ready = false;
+        st->couple_ready[0] = st->couple_ready[1] = false;
         st->tm_rows = rows;
     }
+    // 128-row CTAs fold the coupling to the newest sub-blocks into
+    // precomputed products (trsv_fold_kernel; SIEB200_TRSV_FOLD=0 streams
+    // those tiles as well, trsv_tma_kernel).
+    const char* fold_env = getenv("SIEB200_TRSV_FOLD");
+    const bool fold = rows == TR_ROWS && !(fold_env && fold_env[0] == '0');
     if (st->tm_base != st->W || st->tm_np != np) {
         // W as 8-byte elements: rows inner, 128 x 32 boxes; rows/columns
         // beyond np read as zero.
@@ -2148,6 +2496,10 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
                                            trsv_smem(TR_ROWS)));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_tma_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            trsv_smem(NB)));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemTrsvFold));
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(trsv_couple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemCouple));
         attr_set = true;
     }
     const unsigned ncta = (unsigned)((np + rows - 1) / rows);
@@ -2156,13 +2508,32 @@ static int apply_precond(DenseSolver* s, const cplx* r, cplx* z, cplx* work, boo
     const double tri_bytes = 8.0 * (double)np * (double)np / 2.0 + 8.0 * NB * NB * nbl;
     SIEB_RETURN_IF(s->flags.reserve(sizeof(cplx) * (size_t)np));
     cplx* xpub = s->flags.as<cplx>();
+    // Coupling products: [adjoint][lower] x (P1, P2) x nbl blocks, formed
+    // once per factorization and direction.
+    const size_t per_dir = (size_t)2 * nbl * NB * NB;
+    auto couple_of = [&](int lower) { return s->couple.as<float2>() + ((adjoint ? 2 : 0) + lower) * per_dir; };
+    if (fold && !st->couple_ready[adjoint ? 1 : 0]) {
+        SIEB_RETURN_IF(s->couple.reserve(sizeof(float2) * per_dir * 4));
+        for (int lower = 1; lower >= 0; --lower) {
+            const float2* dinv = adjoint ? (lower ? st->UinvH : st->LinvH) : (lower ? st->Linv : st->Uinv);
+            trsv_couple_kernel<<<dim3((unsigned)nbl, 2), 256, kSmemCouple, stream>>>(
+                adjoint ? st->WH : st->W, st->ldw, np, nbl, lower, dinv, couple_of(lower));
+            SIEB_NOTE_LAUNCH();
+            SIEB_TRY_CUDA(cudaGetLastError());
+        }
+        st->couple_ready[adjoint ? 1 : 0] = true;
+    }
     for (int lower = 1; lower >= 0; --lower) {
         const float2* dinv = adjoint ? (lower ? st->UinvH : st->LinvH) : (lower ? st->Linv : st->Uinv);
         SIEB_TRY_CUDA(cudaMemsetAsync(fl, 0, sizeof(unsigned) * 2, stream));
         SIEB_TRY_CUDA(cudaMemsetAsync(xpub, 0xFF, sizeof(cplx) * (size_t)np, stream));
         cudaEvent_t ev;
         s->ctx->prof.begin(stream, 1, 0.0, tri_bytes, &ev);
-        if (rows == NB)
+        if (fold)
+            trsv_fold_kernel<<<ncta, TR_THREADS, kSmemTrsvFold, stream>>>(
+                adjoint ? st->tmWH : st->tmW, np, nbl, lower, dinv, couple_of(lower), work, xpub, fl, st->err,
+                timeout_ns);
+        else if (rows == NB)
             trsv_tma_kernel<NB><<<ncta, TR_THREADS, trsv_smem(NB), stream>>>(
                 adjoint ? st->tmWH : st->tmW, np, nbl, lower, dinv, work, xpub, fl, st->err, timeout_ns);
         else

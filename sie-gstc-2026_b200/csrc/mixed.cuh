@@ -52,6 +52,7 @@ struct MixedState {
     // factorization (in the solver's panel workspace).
     cplx* dinv = nullptr;               // GMRES_C64: inverse diagonal of Z
     bool adj_ready = false;
+    bool couple_ready[2] = {false, false};  // trsv_fold_kernel's products (forward, adjoint)
     float2* WH = nullptr;
     float2* LinvH = nullptr;
     float2* UinvH = nullptr;

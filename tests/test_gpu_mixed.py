@@ -226,7 +226,7 @@ def test_dense_solver_object_on_device_memory(gpu_ctx):
                                       "single_split_overlap", "single_split_trsv64", "pair_then_single",
                                       "single_split_no_lcol", "single_split_lcol_gemm",
                                       "single_split_lcol_side", "single_split_diag_rec",
-                                      "single_split_diag_compact"])
+                                      "single_split_diag_compact", "single_split_trsv_stream"])
 @pytest.mark.parametrize("n", [5, 64, 100, 129, 190, 256, 300, 1000, 2100])
 def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     """Sizes that leave partial sub-blocks, a last row block with one
@@ -254,6 +254,9 @@ def test_mixed_ragged_sizes_one_step(n, schedule, gpu_ctx, monkeypatch):
     monkeypatch.setenv("SIEB200_OVERLAP_SMS", "16")
     # triangular solves with 64-row CTAs (one sub-block each) or 128-row ones
     monkeypatch.setenv("SIEB200_TRSV_ROWS", "64" if schedule.endswith("trsv64") else "128")
+    # 128-row triangular solves with the newest coupling folded into
+    # precomputed products (default) or streamed as tiles
+    monkeypatch.setenv("SIEB200_TRSV_FOLD", "0" if schedule.endswith("trsv_stream") else "1")
     # who updates the next block column below its diagonal block in a single
     # step: the next panels (0), the GEMM (1, default), col_update_kernel on
     # the third stream (2) or before the GEMM (3)
@@ -335,15 +338,17 @@ def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
         assert np.array_equal(xs, out["reference"]), name
 
 
-@pytest.mark.parametrize("rows", ["128", "64"])
+@pytest.mark.parametrize("rows", ["128", "128_stream", "64"])
 @pytest.mark.parametrize("n", [5, 129, 300, 1000])
 def test_mixed_adjoint_solve(n, rows, gpu_ctx, monkeypatch):
     """Conjugate-transpose solve A^H x = b with the mixed factors: one
     preconditioned step reaches 1e-5, the refinement 1e-12, as for A x = b
-    (triangular solves with 128- and 64-row CTAs)."""
+    (triangular solves with 128-row CTAs, the newest coupling folded into
+    precomputed products or streamed, and with 64-row CTAs)."""
     import torch
     import sieb200
-    monkeypatch.setenv("SIEB200_TRSV_ROWS", rows)
+    monkeypatch.setenv("SIEB200_TRSV_ROWS", rows.split("_")[0])
+    monkeypatch.setenv("SIEB200_TRSV_FOLD", "0" if rows.endswith("stream") else "1")
     rng = np.random.default_rng(100 + n)
     A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
     A[0, n - 1] += 5.0  # make A far from Hermitian
