@@ -1077,11 +1077,19 @@ def timeline_summary(spans):
     timeline [(kind, start_ms, end_ms)]: kinds 0 trailing GEMM, 1 triangular
     solve, 2 FP64 matvec, 3 diagonal block, 4 panels, 6 factorization,
     7 refined solve. A block step runs panels(k), then the GEMM of step k
-    beside the next diagonal block."""
+    beside the next diagonal block. Split panels (a head launch on the
+    lookahead stream beside the rest) overlap in time and count as one
+    panels span of their step."""
     span = {k: [(a, b) for kk, a, b in spans if kk == k] for k in range(8)}
     total = {name: sum(b - a for a, b in span[k]) for k, name in
              [(0, "gemm_ms"), (1, "trsv_ms"), (2, "matvec_ms"), (3, "diag_ms"), (4, "panels_ms")]}
-    pan, gem, dia = span[4], span[0], span[3]
+    pan = []
+    for a, b in sorted(span[4]):
+        if pan and a <= pan[-1][1] + 0.005:
+            pan[-1] = (pan[-1][0], max(pan[-1][1], b))
+        else:
+            pan.append((a, b))
+    gem, dia = span[0], span[3]
     steps = []
     for k in range(len(pan) - 1):
         g = [b - a for a, b in gem if pan[k][1] - 1e-6 <= a < pan[k + 1][0]]

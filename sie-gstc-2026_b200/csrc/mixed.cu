@@ -38,6 +38,10 @@ namespace {
 // tiles, or one plus a 32-row slab).
 constexpr int kSmemDiag = (2 * NB * (NB + 1) + NB * NB / 4) * (int)sizeof(float2);
 constexpr int kSmemPanel = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(float2);
+// Upper bound of a split panels head's dynamic shared memory: asking for
+// more than kSmemPanel keeps the other panels' CTAs (kSmemPanel each) off
+// the head's SMs (228 KB per SM).
+constexpr int kSmemPanelHeadMax = 200 * 1024;
 // The diagonal-block kernel stages the previous step's two 64 x 64 factor
 // blocks; its size also keeps it off SMs that hold a trailing-GEMM CTA.
 constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
@@ -795,6 +799,9 @@ struct PanelArgs {
     int64_t b_ld = 0, b_c0 = 0;
     int64_t a_lo = 0, b_lo = 0;
     int lo_rn = 0;  // lo parts rounded to the nearest TF32
+    // CTA range of one launch: L21 row blocks and U12 column blocks
+    // [b_first, b_first + nl_run) of 32 each (nl_run 0: all nL from 0)
+    int b_first = 0, nl_run = 0;
 };
 
 // L21 = A21 * inv(U11) for rows [s0, np) of the panel columns [k0, k0+kb);
@@ -1068,14 +1075,18 @@ __global__ void __launch_bounds__(256) col_update_kernel(float2* __restrict__ W,
         }
 }
 
-// Both panels of a block step in one launch: CTAs [0, nL) form L21 (rows
-// below the diagonal block, after the updates of the steps in kp), the rest
-// U12 (columns right of it, after the update of step kpu).
+// Both panels of a block step in one launch: the first nl_run CTAs form
+// L21 (rows below the diagonal block, after the updates of the steps in kp),
+// the rest U12 (columns right of it, after the update of step kpu), both
+// over the 32-row (32-column) blocks from b_first. A block's result does
+// not depend on the launch it runs in, so the panels can be split between
+// launches (the next block's rows and columns first) bit for bit.
 template <class T>
 __global__ void __launch_bounds__(256, 3) panels_kernel(T* __restrict__ W, int64_t ldw, const T* __restrict__ Uinv,
                                                         const T* __restrict__ Linv, const PanelArgs pa) {
-    if ((int)blockIdx.x < pa.nL) panel_L_body(W, ldw, pa, Uinv, blockIdx.x);
-    else panel_U_body(W, ldw, pa, Linv, blockIdx.x - pa.nL);
+    const int nl = pa.nl_run > 0 ? pa.nl_run : pa.nL;
+    if ((int)blockIdx.x < nl) panel_L_body(W, ldw, pa, Uinv, pa.b_first + (int)blockIdx.x);
+    else panel_U_body(W, ldw, pa, Linv, pa.b_first + (int)blockIdx.x - nl);
 }
 
 // SIMT trailing update C -= L21 U12 in complex64 (checking path).
@@ -1949,6 +1960,8 @@ void mixed_release(DenseSolver* s) {
         if (st->ev_diag) cudaEventDestroy(st->ev_diag);
         if (st->ev_pan) cudaEventDestroy(st->ev_pan);
         if (st->ev_lcol) cudaEventDestroy(st->ev_lcol);
+        if (st->ev_gemm) cudaEventDestroy(st->ev_gemm);
+        if (st->ev_head) cudaEventDestroy(st->ev_head);
         if (st->side) cudaStreamDestroy(st->side);
         if (st->side2) cudaStreamDestroy(st->side2);
         delete st;
@@ -1998,6 +2011,8 @@ constexpr int kPairMinDefault = 20000;
 // 17280-unknown GSTC batch 16 ms more per solve, 129 against 113 ms).
 constexpr double kGmresEstFactorDefault = 0.9;
 constexpr int kOverlapSmsDefault = 20;
+// Split panels (SIEB200_PANEL_HEAD_MAX): 0 = off.
+constexpr int kPanelHeadMaxDefault = 0;
 
 static int fp64_factorize(DenseSolver* s);
 
@@ -2040,6 +2055,10 @@ int mixed_factorize(DenseSolver* s) {
     st->diag_compact = diag_compact_env();
     const char* rec_env = getenv("SIEB200_DIAG_REC");
     st->diag_rec = (rec_env && rec_env[0] == '1') ? 1 : 0;
+    const char* head_env = getenv("SIEB200_PANEL_HEAD_MAX");
+    st->head_max = head_env ? std::max(0, atoi(head_env)) : kPanelHeadMaxDefault;
+    const char* hsm_env = getenv("SIEB200_PANEL_HEAD_SMEM");
+    st->head_smem = hsm_env ? std::max(kSmemPanel, std::min(kSmemPanelHeadMax, atoi(hsm_env))) : kSmemPanel;
 
     // Workspace layout in s->lu: W | Linv | Uinv | diag | err+flags ; packs separate.
     const size_t bW = sizeof(float2) * ldw * np;
@@ -2078,11 +2097,17 @@ int mixed_factorize(DenseSolver* s) {
         SIEB_TRY_CUDA(cudaStreamCreateWithPriority(&st->side2, cudaStreamNonBlocking, greatest));
         SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_lcol, cudaEventDisableTiming));
     }
+    if (!st->ev_gemm) {
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_gemm, cudaEventDisableTiming));
+        SIEB_TRY_CUDA(cudaEventCreateWithFlags(&st->ev_head, cudaEventDisableTiming));
+    }
 
     static bool attrs_set = false;
     if (!attrs_set) {
         SIEB_TRY_CUDA(cudaFuncSetAttribute(trailing_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemDiag));
-        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemPanel));
+        // (a head launch may ask for more, up to kSmemPanelHeadMax)
+        SIEB_TRY_CUDA(cudaFuncSetAttribute(panels_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kSmemPanelHeadMax));
         SIEB_RETURN_IF(diag_set_smem<float2>(kSmemDiagUpd));
         SIEB_TRY_CUDA(cudaFuncSetAttribute(diag_lu_rec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kSmemDiagRec));
@@ -2097,6 +2122,7 @@ int mixed_factorize(DenseSolver* s) {
                  64 * st->diag_panels + 128 * st->diag_rec + 256 * st->diag_compact;
     key.sms = gemm_sms;
     key.ovl = ((int64_t)st->pair_min << 32) | (int64_t)(st->ovl_min * 1000 + st->ovl_sms);
+    key.head = ((int64_t)st->head_max << 20) | (int64_t)st->head_smem;
     const char* no_graphs = getenv("SIEB200_NO_GRAPHS");
     const bool graphs = !ctx->prof.enabled && !(no_graphs && no_graphs[0] == '1');
     if (graphs) {
@@ -2218,7 +2244,10 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     const int64_t KS = hilo ? 4 * NB : K3;  // pack width of one step
     const int64_t KP = 2 * KS;              // pack width of a pair
     const int layout = hilo ? 1 : 0;
-    auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu, cudaStream_t ps) -> int {
+    // part 0: all of the panels; 1: the head, the rows and columns of the
+    // next block (the next diagonal block's update needs only these); 2: the
+    // rest (none when the head is all).
+    auto panels = [&](int64_t bk, int64_t kp1, int64_t kp2, int64_t kpu, cudaStream_t ps, int part) -> int {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
         const int64_t s0 = k0 + kb;
@@ -2227,6 +2256,15 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         PanelArgs pa;
         pa.k0 = k0; pa.kb = kb; pa.s0 = s0; pa.np = np;
         pa.nL = (int)blocks_for(m, 32);
+        const int nhead = std::min(pa.nL, NB / 32);
+        if (part == 1) {
+            pa.b_first = 0; pa.nl_run = nhead;
+        } else if (part == 2) {
+            if (pa.nL <= nhead) return SIEB200_OK;
+            pa.b_first = nhead; pa.nl_run = pa.nL - nhead;
+        }
+        const int run = pa.nl_run > 0 ? pa.nl_run : pa.nL;
+        const double share = (double)run / (double)pa.nL;
         pa.pack = st->use_tc;
         pa.kp[0] = kp1; pa.kp[1] = kp2; pa.kpu = kpu;
         pa.lo_rn = st->lo_rn;
@@ -2246,8 +2284,9 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
         }
         const int nupd = (kp1 >= 0) + (kp2 >= 0) + (kpu >= 0);
         cudaEvent_t ev;
-        ctx->prof.begin(ps, 4, 8.0 * NB * NB * (double)m * (2 + nupd), 8.0 * NB * (double)m * (4 + nupd), &ev);
-        panels_kernel<float2><<<(unsigned)(2 * pa.nL), 256, kSmemPanel, ps>>>(
+        ctx->prof.begin(ps, 4, share * 8.0 * NB * NB * (double)m * (2 + nupd),
+                        share * 8.0 * NB * (double)m * (4 + nupd), &ev);
+        panels_kernel<float2><<<(unsigned)(2 * run), 256, part == 1 ? st->head_smem : kSmemPanel, ps>>>(
             st->W, ldw, st->Uinv + (size_t)bk * NB * NB, st->Linv + (size_t)bk * NB * NB, pa);
         SIEB_NOTE_LAUNCH();
         ctx->prof.end(ps, ev);
@@ -2308,8 +2347,21 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
     // SMs the GEMM leaves free; so the panels leave the critical path while
     // the GEMM is the longer of the two. The next GEMM waits for them (event).
     SIEB_RETURN_IF(diag_blk(0, -1, -1, stream));
-    SIEB_RETURN_IF(panels(0, -1, -1, -1, stream));
+    SIEB_RETURN_IF(panels(0, -1, -1, -1, stream, 0));
     bool pan_side = false;  // the last panels ran on the side stream
+    // Split panels (single steps with the GEMM covering the next block
+    // column, no overlapped steps): when the next panels are at most
+    // st->head_max wide, their head runs on the side stream right after the
+    // next diagonal block and the GEMM, followed there by the diagonal block
+    // after it, while the rest of the panels run here; the chain of a step
+    // whose diagonal block outlasts the GEMM is then head + diagonal block
+    // instead of all of the panels + diagonal block.
+    const int64_t head_max = (st->ovl_min > 0 || st->lcol != 1) ? 0 : st->head_max;
+    bool head_prev = false;  // this step's panels ran split (head on the side stream, ev_head)
+    // The side stream joins only after it has been forked from this one: a
+    // system of one block has no lookahead, and under stream capture a wait
+    // on an event of the never-forked side stream is refused.
+    bool side_forked = false;
     for (int64_t bk = 0; bk < nbl; ++bk) {
         const int64_t k0 = bk * NB;
         const int kb = (int)std::min<int64_t>(NB, np - k0);
@@ -2321,16 +2373,21 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             const bool pair = pair_at(bk);
             const bool odd = pair && (bk & 1);
             const int64_t kprev = odd ? k0 - NB : -1;      // the first step of the pair
-            SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
-            SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
+            if (!head_prev) {  // (else the head went before on the side stream)
+                SIEB_TRY_CUDA(cudaEventRecord(st->ev_cols, stream));
+                SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_cols, 0));
+                side_forked = true;
+            }
             SIEB_RETURN_IF(diag_blk(bk + 1, k0, kprev, st->side));
             const bool ovl = !pair && st->ovl_min > 0 && m - n1 >= st->ovl_min && m > 2 * n1;
             if (pan_side) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_pan, 0));  // GEMM operands
+            if (head_prev) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_head, 0));  // the head's packs
+            head_prev = false;
             if (ovl) {
                 const int octas = std::max(1, std::min(gemm_ctas, ctx->sm_count - st->ovl_sms));
                 SIEB_RETURN_IF(gemm(s0 + n1, s0 + n1, m - n1, st->Apack[bk & 1] + 2 * n1 * KS,
                                     st->Bpack + (bk & 1) * np * KS + n1 * KS, (int)KS, octas, 0));
-                SIEB_RETURN_IF(panels(bk + 1, k0, -1, k0, st->side));
+                SIEB_RETURN_IF(panels(bk + 1, k0, -1, k0, st->side, 0));
                 SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
                 pan_side = true;
                 continue;
@@ -2372,25 +2429,41 @@ static int mixed_enqueue(DenseSolver* s, MixedState* st, size_t bFlags, int K3) 
             } else if (odd && m > n1) {
                 SIEB_RETURN_IF(gemm(s0, s0 + n1, m - n1, st->Apack[0], st->Bpack, (int)KP, gemm_ctas, 0));
             }
+            const int64_t m1 = m - n1;  // width of the next panels
+            if (lcol && head_max > 0 && m1 > 0 && m1 <= head_max) {
+                // split: the head after this GEMM and the next diagonal block
+                // (side stream order), the rest here after both
+                SIEB_TRY_CUDA(cudaEventRecord(st->ev_gemm, stream));
+                SIEB_TRY_CUDA(cudaStreamWaitEvent(st->side, st->ev_gemm, 0));
+                SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1, st->side, 1));
+                SIEB_TRY_CUDA(cudaEventRecord(st->ev_head, st->side));
+                SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
+                SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1, stream, 2));
+                head_prev = true;
+                continue;
+            }
             SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_diag, 0));
             if (lside && m > n1) SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_lcol, 0));
             // The next L21 rows take this step's update themselves unless
             // the GEMM or col_update_kernel applied it (lcol, lside); after
             // an even step of the pair schedule the next block row has not
             // had it either.
-            SIEB_RETURN_IF(panels(bk + 1, (lcol || lside || lmain) ? -1 : k0, kprev, pair && !odd ? k0 : -1, stream));
+            SIEB_RETURN_IF(panels(bk + 1, (lcol || lside || lmain) ? -1 : k0, kprev, pair && !odd ? k0 : -1, stream,
+                                  0));
         } else {
             trailing_simt_kernel<<<dim3(blocks_for(m, 64), blocks_for(m, 64)), 256, kSmemDiag, stream>>>(
                 st->W, ldw, k0, kb, s0, np);
             SIEB_NOTE_LAUNCH();
             SIEB_TRY_CUDA(cudaGetLastError());
             SIEB_RETURN_IF(diag_blk(bk + 1, -1, -1, stream));
-            SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1, stream));
+            SIEB_RETURN_IF(panels(bk + 1, -1, -1, -1, stream, 0));
         }
     }
     // Join the side stream (its last panels or diagonal block).
-    SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
-    SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_pan, 0));
+    if (side_forked) {
+        SIEB_TRY_CUDA(cudaEventRecord(st->ev_pan, st->side));
+        SIEB_TRY_CUDA(cudaStreamWaitEvent(stream, st->ev_pan, 0));
+    }
     ctx->prof.end(stream, ev_fact);
     return SIEB200_OK;
 }

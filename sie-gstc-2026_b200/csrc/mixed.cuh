@@ -42,6 +42,10 @@ struct MixedState {
     int diag_panels = 0;        // diagonal-block elimination synchronised per panel of 8 steps, not per step
     int diag_rec = 0;           // diagonal block by 2 x 2 recursion over 32 x 32 warp-level factorizations
     int diag_compact = 0;       // diagonal-block elimination in one code path (runtime row half)
+    int head_max = 0;           // single steps: panels whose trailing width is at most this split into a
+                                // head (the next block's rows and columns) on the lookahead stream and the
+                                // rest on the context stream (0: one panels launch)
+    int head_smem = 0;          // dynamic shared memory of a head launch (bytes)
     GemmTC* gemm = nullptr;
     CUtensorMap tmW;                       // W for the triangular solves' tile loads
     const void* tm_base = nullptr;
@@ -61,6 +65,7 @@ struct MixedState {
     cudaEvent_t ev_cols = nullptr, ev_diag = nullptr, ev_pan = nullptr;
     cudaStream_t side2 = nullptr;          // third stream: the next block column's update beside the GEMM
     cudaEvent_t ev_lcol = nullptr;
+    cudaEvent_t ev_gemm = nullptr, ev_head = nullptr;  // split panels: trailing GEMM done; head done
     // The factorization's launches as one CUDA graph (both streams and the
     // event edges between them), captured on the second call with an
     // unchanged key and replayed while it stays so; not while the profiler
@@ -72,9 +77,10 @@ struct MixedState {
         const void* pack = nullptr;
         int use_tc = -1, sms = -1;
         int64_t ovl = -1;
+        int64_t head = -1;
         bool operator==(const GraphKey& o) const {
             return A == o.A && lda == o.lda && n == o.n && W == o.W && pack == o.pack && use_tc == o.use_tc &&
-                   sms == o.sms && ovl == o.ovl;
+                   sms == o.sms && ovl == o.ovl && head == o.head;
         }
     };
     // Two graphs (for example one per buffer of a caller that uploads the

@@ -302,6 +302,50 @@ _CHAIN_VARIANTS = {
 }
 
 
+@pytest.mark.parametrize("n", [64, 130, 1000, 2100])
+def test_mixed_split_panels_bit_identical(n, gpu_ctx, monkeypatch):
+    """Split panels (SIEB200_PANEL_HEAD_MAX): the next block's rows and
+    columns of L21 / U12 in a head launch on the lookahead stream, the rest
+    on the context stream. Every 32-row block of the panels runs the same
+    code whichever launch it is in, so the factors, and with them the
+    one-step solution, are the same bit for bit as with one panels launch:
+    for every step split, for the narrower steps only (the switch inside
+    the factorization), and with the head's larger shared-memory request."""
+    import torch
+    import sieb200
+    rng = np.random.default_rng(400 + n)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * math.sqrt(n) * np.eye(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    Z = torch.from_numpy(np.asfortranarray(A).T.copy()).cuda()
+    monkeypatch.setenv("SIEB200_PAIR_MIN", "0")
+    monkeypatch.setenv("SIEB200_GEMM_LCOL", "1")
+    variants = {"one_launch": ("0", "0"), "all_split": ("1000000", "0"),
+                "narrow_split": (str(max(1, n // 2)), "0"), "all_split_big_smem": ("1000000", str(200 * 1024))}
+    out = {}
+    for name, (head_max, smem) in variants.items():
+        monkeypatch.setenv("SIEB200_PANEL_HEAD_MAX", head_max)
+        if smem == "0":
+            monkeypatch.delenv("SIEB200_PANEL_HEAD_SMEM", raising=False)
+        else:
+            monkeypatch.setenv("SIEB200_PANEL_HEAD_SMEM", smem)
+        s = sieb200.DenseLuSolver(n, "mixed_ir", ctx=gpu_ctx)
+        xs = []
+        for _ in range(3):  # eager, captured, replayed
+            s.factorize(Z.data_ptr())
+            x = torch.from_numpy(b.copy()).cuda()
+            torch.cuda.synchronize()
+            s.solve(x.data_ptr(), tolerance=1e-5, max_iterations=1)
+            gpu_ctx.synchronize()
+            xs.append(x.cpu().numpy())
+        s.close()
+        for x in xs[1:]:
+            assert np.array_equal(x, xs[0]), name
+        out[name] = xs[0]
+    assert np.linalg.norm(A @ out["one_launch"] - b) / np.linalg.norm(b) <= 1e-5
+    for name, xs in out.items():
+        assert np.array_equal(xs, out["one_launch"]), name
+
+
 @pytest.mark.parametrize("n", [64, 200, 1000, 2100])
 def test_mixed_chain_variants_bit_identical(n, gpu_ctx, monkeypatch):
     """The chain variants only move work between kernels and streams: the
