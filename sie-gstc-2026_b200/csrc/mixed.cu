@@ -42,6 +42,11 @@ constexpr int kSmemPanel = (NB * (NB + 4) + 2 * 32 * (NB + 1)) * (int)sizeof(flo
 // more than kSmemPanel keeps the other panels' CTAs (kSmemPanel each) off
 // the head's SMs (228 KB per SM).
 constexpr int kSmemPanelHeadMax = 200 * 1024;
+// Panel CTAs: 256 threads; a 32-row (32-column) slab of NB entries and an
+// NB x NB inverse are 8 and 16 entries per thread.
+constexpr int kPanelThreads = 256;
+constexpr int kPanelSlab = 32 * NB / kPanelThreads;
+constexpr int kPanelInv = NB * NB / kPanelThreads;
 // The diagonal-block kernel stages the previous step's two 64 x 64 factor
 // blocks; its size also keeps it off SMs that hold a trailing-GEMM CTA.
 constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
@@ -823,10 +828,35 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
     T(*Lr)[NB + 1] = Ar + 32;                                                             // [row][k]
     const int tid = threadIdx.x;
     const int64_t rb = r0 + (int64_t)bx * 32;
-    for (int e = tid; e < 32 * NB; e += blockDim.x) {
-        const int r = e % 32, c = e / 32;
-        const int64_t gr = rb + r;
-        Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
+    // All of this thread's loads go out before the first shared-memory store
+    // (one memory latency per CTA instead of one per loop trip): its A21
+    // entries and, in complex64, its entries of inv(U11), which stay in
+    // registers until the update phase no longer needs Us.
+    // (complex128, the own FP64 LU: the plain loop, which needs no spill)
+    constexpr bool kPre = std::is_same<T, float2>::value;
+    T ui[kPre ? kPanelInv : 1];
+    if constexpr (kPre) {
+        T ra[kPanelSlab];
+#pragma unroll
+        for (int i = 0; i < kPanelSlab; ++i) {
+            const int e = tid + kPanelThreads * i;
+            const int r = e % 32, c = e / 32;
+            const int64_t gr = rb + r;
+            ra[i] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < kPanelInv; ++i) ui[i] = Uinv[tid + kPanelThreads * i];
+#pragma unroll
+        for (int i = 0; i < kPanelSlab; ++i) {
+            const int e = tid + kPanelThreads * i;
+            Ar[e % 32][e / 32] = ra[i];
+        }
+    } else {
+        for (int e = tid; e < 32 * NB; e += blockDim.x) {
+            const int r = e % 32, c = e / 32;
+            const int64_t gr = rb + r;
+            Ar[r][c] = (gr < np && c < kb) ? W[gr + (k0 + c) * ldw] : cmk<T>(0.f, 0.f);
+        }
     }
     const int ty = tid & 15, tx = tid >> 4;
     for (int q = 0; q < 2; ++q) {
@@ -862,7 +892,15 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
 #pragma unroll
             for (int j = 0; j < 4; ++j) Ar[2 * ty + i][4 * tx + j] = upd[i][j];
     }
-    for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];  // Uinv[k + c*NB]
+    if constexpr (kPre) {
+#pragma unroll
+        for (int i = 0; i < kPanelInv; ++i) {
+            const int e = tid + kPanelThreads * i;
+            Us[e % NB][e / NB] = ui[i];  // Uinv[k + c*NB]
+        }
+    } else {
+        for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];
+    }
     __syncthreads();
     T acc[2][4];
 #pragma unroll
@@ -936,10 +974,31 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
     T(*Uc)[NB + 1] = Ac + 32;                                                           // [col][k]
     const int tid = threadIdx.x;
     const int64_t cb = c0 + (int64_t)bx * 32;
-    for (int e = tid; e < 32 * NB; e += blockDim.x) {
-        const int r = e % NB, c = e / NB;
-        const int64_t gc = cb + c;
-        Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : cmk<T>(0.f, 0.f);
+    // As in panel_L_body: every load of the thread before the first store.
+    constexpr bool kPre = std::is_same<T, float2>::value;
+    T li[kPre ? kPanelInv : 1];
+    if constexpr (kPre) {
+        T ra[kPanelSlab];
+#pragma unroll
+        for (int i = 0; i < kPanelSlab; ++i) {
+            const int e = tid + kPanelThreads * i;
+            const int r = e % NB, c = e / NB;
+            const int64_t gc = cb + c;
+            ra[i] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : cmk<T>(0.f, 0.f);
+        }
+#pragma unroll
+        for (int i = 0; i < kPanelInv; ++i) li[i] = Linv[tid + kPanelThreads * i];
+#pragma unroll
+        for (int i = 0; i < kPanelSlab; ++i) {
+            const int e = tid + kPanelThreads * i;
+            Ac[e / NB][e % NB] = ra[i];
+        }
+    } else {
+        for (int e = tid; e < 32 * NB; e += blockDim.x) {
+            const int r = e % NB, c = e / NB;
+            const int64_t gc = cb + c;
+            Ac[c][r] = (gc < np && r < kb) ? W[(k0 + r) + gc * ldw] : cmk<T>(0.f, 0.f);
+        }
     }
     const int tx = tid & 15, ty = tid >> 4;
     if (pa.kpu >= 0) {
@@ -975,7 +1034,15 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
 #pragma unroll
             for (int j = 0; j < 2; ++j) Ac[2 * tx + j][4 * ty + i] = upd[i][j];
     }
-    for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];  // Linv[r + k*NB]
+    if constexpr (kPre) {
+#pragma unroll
+        for (int i = 0; i < kPanelInv; ++i) {
+            const int e = tid + kPanelThreads * i;
+            Ls[e / NB][e % NB] = li[i];  // Linv[r + k*NB]
+        }
+    } else {
+        for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];
+    }
     __syncthreads();
     T acc[4][2];
 #pragma unroll
