@@ -47,6 +47,7 @@ constexpr int kSmemPanelHeadMax = 200 * 1024;
 constexpr int kPanelThreads = 256;
 constexpr int kPanelSlab = 32 * NB / kPanelThreads;
 constexpr int kPanelInv = NB * NB / kPanelThreads;
+static_assert(NB == 64 && kPanelThreads == 256, "panel threads: 16 x 16, four columns (rows) of 64 each");
 // The diagonal-block kernel stages the previous step's two 64 x 64 factor
 // blocks; its size also keeps it off SMs that hold a trailing-GEMM CTA.
 constexpr int kSmemDiagUpd = 2 * NB * (NB + 1) * (int)sizeof(float2);
@@ -815,8 +816,8 @@ struct PanelArgs {
 // A21 -= L21(kp) U12(kp)[:, k0:k0+kb] (FP32 FMA; the factors are those
 // steps' panels in W), so no separate GEMM launch stands between the steps.
 // One CTA per 32 rows. Thread (ty, tx) computes rows 2ty, 2ty+1 and columns
-// 4tx .. 4tx+3 with k outermost; inv(U11) is upper triangular, so the k
-// loop stops at the thread's last column (tx is warp-uniform up to a pair).
+// 2tx, 2tx+1, 62-2tx, 63-2tx with k outermost; inv(U11) is upper
+// triangular, so each column pair's k loop stops at its last column.
 template <class T>
 __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, const PanelArgs& pa,
                                              const T* __restrict__ Uinv, int bx) {
@@ -902,17 +903,33 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
         for (int e = tid; e < NB * NB; e += blockDim.x) Us[e % NB][e / NB] = Uinv[e];
     }
     __syncthreads();
+    // Columns of thread tx: the pair 2tx, 2tx+1 and the pair 62-2tx, 63-2tx,
+    // so that every warp runs about the same number of k steps of the
+    // triangle (2tx+2 with all four columns, then up to 64-2tx with the high
+    // pair) instead of the last warps running all 64 while the first wait at
+    // the barrier. Each column still sums its k in ascending order.
     T acc[2][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = cmk<T>(0.f, 0.f);
-    const int kend = min(kb, 4 * tx + 4);
-    for (int k = 0; k < kend; ++k) {
+    int col[4];
+    col[0] = 2 * tx; col[1] = 2 * tx + 1; col[2] = 62 - 2 * tx; col[3] = 63 - 2 * tx;
+    const int kend_lo = min(kb, 2 * tx + 2), kend_hi = min(kb, 64 - 2 * tx);
+    for (int k = 0; k < kend_lo; ++k) {
         const T a0 = Ar[2 * ty][k], a1 = Ar[2 * ty + 1][k];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const T u = Us[k][4 * tx + j];
+            const T u = Us[k][col[j]];
+            acc[0][j] = cmk<T>(acc[0][j].x + a0.x * u.x - a0.y * u.y, acc[0][j].y + a0.x * u.y + a0.y * u.x);
+            acc[1][j] = cmk<T>(acc[1][j].x + a1.x * u.x - a1.y * u.y, acc[1][j].y + a1.x * u.y + a1.y * u.x);
+        }
+    }
+    for (int k = kend_lo; k < kend_hi; ++k) {
+        const T a0 = Ar[2 * ty][k], a1 = Ar[2 * ty + 1][k];
+#pragma unroll
+        for (int j = 2; j < 4; ++j) {
+            const T u = Us[k][col[j]];
             acc[0][j] = cmk<T>(acc[0][j].x + a0.x * u.x - a0.y * u.y, acc[0][j].y + a0.x * u.y + a0.y * u.x);
             acc[1][j] = cmk<T>(acc[1][j].x + a1.x * u.x - a1.y * u.y, acc[1][j].y + a1.x * u.y + a1.y * u.x);
         }
@@ -922,7 +939,7 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) Ar[2 * ty + i][4 * tx + j] = acc[i][j];
+        for (int j = 0; j < 4; ++j) Ar[2 * ty + i][col[j]] = acc[i][j];
     __syncthreads();
     // ... to W (rows fastest: coalesced columns) ...
     for (int e = tid; e < 32 * kb; e += blockDim.x) {
@@ -960,9 +977,9 @@ __device__ __forceinline__ void panel_L_body(T* __restrict__ W, int64_t ldw, con
 // writes U12 back into W and the split columns into Bpack. With kpu >= 0 the
 // columns first take that step's update, A12 -= L21(kpu)[k0:k0+kb, :]
 // U12(kpu)[:, these columns] (FP32 FMA, both factors from W). One CTA per 32
-// columns. Thread (ty, tx) computes rows 4ty .. 4ty+3 and columns 2tx,
-// 2tx+1 with k outermost; inv(L11) is lower triangular, so the k loop stops
-// at the thread's last row (ty is warp-uniform up to a pair).
+// columns. Thread (ty, tx) computes rows 2ty, 2ty+1, 62-2ty, 63-2ty and
+// columns 2tx, 2tx+1 with k outermost; inv(L11) is lower triangular, so each
+// row pair's k loop stops at its last row.
 template <class T>
 __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, const PanelArgs& pa,
                                              const T* __restrict__ Linv, int bx) {
@@ -1044,17 +1061,30 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
         for (int e = tid; e < NB * NB; e += blockDim.x) Ls[e / NB][e % NB] = Linv[e];
     }
     __syncthreads();
+    // Rows of thread ty: the pairs 2ty, 2ty+1 and 62-2ty, 63-2ty (balanced
+    // triangle, as the columns in panel_L_body), each summed in ascending k.
     T acc[4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j] = cmk<T>(0.f, 0.f);
-    const int kend = min(kb, 4 * ty + 4);
-    for (int k = 0; k < kend; ++k) {
+    int row[4];
+    row[0] = 2 * ty; row[1] = 2 * ty + 1; row[2] = 62 - 2 * ty; row[3] = 63 - 2 * ty;
+    const int kend_lo = min(kb, 2 * ty + 2), kend_hi = min(kb, 64 - 2 * ty);
+    for (int k = 0; k < kend_lo; ++k) {
         const T b0 = Ac[2 * tx][k], b1 = Ac[2 * tx + 1][k];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const T l = Ls[k][4 * ty + i];
+            const T l = Ls[k][row[i]];
+            acc[i][0] = cmk<T>(acc[i][0].x + l.x * b0.x - l.y * b0.y, acc[i][0].y + l.x * b0.y + l.y * b0.x);
+            acc[i][1] = cmk<T>(acc[i][1].x + l.x * b1.x - l.y * b1.y, acc[i][1].y + l.x * b1.y + l.y * b1.x);
+        }
+    }
+    for (int k = kend_lo; k < kend_hi; ++k) {
+        const T b0 = Ac[2 * tx][k], b1 = Ac[2 * tx + 1][k];
+#pragma unroll
+        for (int i = 2; i < 4; ++i) {
+            const T l = Ls[k][row[i]];
             acc[i][0] = cmk<T>(acc[i][0].x + l.x * b0.x - l.y * b0.y, acc[i][0].y + l.x * b0.y + l.y * b0.x);
             acc[i][1] = cmk<T>(acc[i][1].x + l.x * b1.x - l.y * b1.y, acc[i][1].y + l.x * b1.y + l.y * b1.x);
         }
@@ -1063,7 +1093,7 @@ __device__ __forceinline__ void panel_U_body(T* __restrict__ W, int64_t ldw, con
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) Ac[2 * tx + j][4 * ty + i] = acc[i][j];
+        for (int j = 0; j < 2; ++j) Ac[2 * tx + j][row[i]] = acc[i][j];
     __syncthreads();
     for (int e = tid; e < 32 * NB; e += blockDim.x) {
         const int r = e % NB, c = e / NB;
